@@ -1,0 +1,205 @@
+"""ctypes mirror of include/crowdphot_b200.h (structs, constants, prototypes).
+
+The struct layouts here must match the C header field for field; the
+`test_abi.py` suite checks every declared symbol and the struct sizes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+CPB_OK = 0
+CPB_ERR_ARGUMENT = -1
+CPB_ERR_CUDA = -2
+CPB_ERR_OOM = -3
+CPB_ERR_TIMEOUT = -4
+CPB_ERR_INTERNAL = -5
+CPB_ERR_NO_DEVICE = -6
+
+CPB_F32 = 1
+CPB_F64 = 2
+
+CPB_PSF_GRIDDED_IMAGE = 1
+CPB_PSF_IMAGE = 2
+CPB_PSF_CIRCULAR_GAUSSIAN = 3
+
+CPB_FREE_Y = 1
+CPB_FREE_X = 2
+CPB_FREE_FLUX = 4
+CPB_FREE_BKG = 8
+CPB_FREE_FWHM = 16
+
+CPB_PREC_FP64 = 0
+CPB_PREC_MIXED = 1
+
+CPB_COV_AUTO = 0
+CPB_COV_KNOWN_WEIGHTS = 1
+CPB_COV_REWEIGHTED = 2
+
+CPB_DAMP_MARQUARDT = 0
+CPB_DAMP_LEVENBERG = 1
+CPB_DAMP_NONE = 2
+
+CPB_SOLVER_LSQR = 0
+CPB_SOLVER_LSMR = 1
+
+_dp = C.POINTER(C.c_double)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class PsfDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("n_nodes", C.c_int32),
+        ("eltype", C.c_int32),
+        ("reserved", C.c_int32),
+        ("node_data", C.POINTER(C.c_void_p)),
+        ("node_ny", _i64p),
+        ("node_nx", _i64p),
+        ("node_os", _i64p),
+        ("node_origin", _dp),
+        ("node_fill_value", _dp),
+        ("grid_y", _dp),
+        ("grid_x", _dp),
+        ("fwhm", C.c_double),
+    ]
+
+
+class SimParams(C.Structure):
+    _fields_ = [
+        ("fit_rad", C.c_double),
+        ("free_mask", C.c_int32),
+        ("inner_iterations", C.c_int32),
+        ("fixed_y", C.c_double),
+        ("fixed_x", C.c_double),
+        ("fixed_flux", C.c_double),
+        ("fixed_bkg", C.c_double),
+        ("fixed_fwhm", C.c_double),
+        ("linear_tol", C.c_double),
+        ("model_rad_auto", C.c_int32),
+        ("max_trials", C.c_int32),
+        ("model_rad", C.c_double),
+        ("model_rad_max", C.c_double),
+        ("model_rad_nsigma", C.c_double),
+        ("max_step", C.c_double),
+        ("max_iter", C.c_int32),
+        ("covariance", C.c_int32),
+        ("x_tol", C.c_double),
+        ("f_tol", C.c_double),
+        ("g_tol", C.c_double),
+        ("lambda_init", C.c_double),
+        ("lambda_up", C.c_double),
+        ("lambda_down", C.c_double),
+        ("lambda_min", C.c_double),
+        ("lambda_max", C.c_double),
+        ("precision", C.c_int32),
+        ("solver", C.c_int32),
+        ("damping", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class SimResult(C.Structure):
+    _fields_ = [
+        ("y", _dp), ("x", _dp), ("flux", _dp), ("bkg", _dp),
+        ("y_err", _dp), ("x_err", _dp), ("flux_err", _dp), ("bkg_err", _dp),
+        ("converged", _u8p), ("valid", _u8p),
+        ("chisq", _dp),
+        ("qfit", _dp), ("qfit_expected", _dp), ("qfit_z", _dp), ("crowding", _dp),
+        ("n_iter", _i32p),
+        ("residual", _dp),
+        ("dbg_active", _i32p),
+        ("dbg_pixels", _i32p),
+        ("dbg_model_R", _i32p),
+        ("n_passes", C.c_int32),
+        ("n_failed", C.c_int32),
+        ("n_active", C.c_int64),
+        ("n_union", C.c_int64),
+        ("n_trials", C.c_int64),
+        ("n_lsqr_iters", C.c_int64),
+        ("model_px_evals", C.c_double),
+        ("lsqr_px_macs", C.c_double),
+        ("device_seconds", C.c_double),
+    ]
+
+
+class LMParams(C.Structure):
+    _fields_ = [
+        ("free_mask", C.c_int32),
+        ("max_iter", C.c_int32),
+        ("fixed_y", C.c_double),
+        ("fixed_x", C.c_double),
+        ("fixed_flux", C.c_double),
+        ("fixed_bkg", C.c_double),
+        ("fixed_fwhm", C.c_double),
+        ("x_tol", C.c_double),
+        ("f_tol", C.c_double),
+        ("g_tol", C.c_double),
+        ("lambda_init", C.c_double),
+        ("lambda_up", C.c_double),
+        ("lambda_down", C.c_double),
+        ("lambda_min", C.c_double),
+        ("lambda_max", C.c_double),
+        ("min_diagonal", C.c_double),
+        ("damping", C.c_int32),
+        ("covariance", C.c_int32),
+        ("precision", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class LMResultC(C.Structure):
+    _fields_ = [
+        ("params", _dp),
+        ("cov", _dp),
+        ("cost", _dp), ("cost_init", _dp), ("chisq", _dp), ("lambda_final", _dp),
+        ("converged", _u8p), ("x_converged", _u8p), ("f_converged", _u8p), ("g_converged", _u8p),
+        ("iterations", _i32p),
+        ("status", _i32p),
+        ("device_seconds", C.c_double),
+    ]
+
+
+# Every entry point declared in include/crowdphot_b200.h: name -> (restype, argtypes)
+PROTOTYPES = {
+    "cpb_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "cpb_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "cpb_last_error": (C.c_char_p, [C.c_void_p]),
+    "cpb_version": (C.c_char_p, []),
+    "cpb_psf_upload": (C.c_int, [C.c_void_p, C.POINTER(PsfDesc), C.POINTER(C.c_void_p)]),
+    "cpb_psf_free": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cpb_fit_simultaneous": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_void_p, C.c_int32,
+                                       C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, _dp, _dp, _dp,
+                                       C.POINTER(SimResult)]),
+    "cpb_fit_simultaneous_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_void_p, C.c_int32,
+                                              C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.POINTER(SimResult)]),
+    "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
+                                   _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
+}
+
+PACKAGE_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PACKAGE_DIR, "lib", "libcrowdphot_b200.so")
+
+_lib = None
+
+
+def load_library(path: str | None = None) -> C.CDLL:
+    """Loads libcrowdphot_b200.so and binds every prototype.  Raises when absent:
+    there is no CPU fallback for the product path."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"libcrowdphot_b200.so not found at {p}; build it with __graft_entry__.build()")
+    lib = C.CDLL(p)
+    for name, (res, args) in PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib

@@ -1,0 +1,523 @@
+"""Host mirror of CrowdPhot's photometry entry points over the B200 C-ABI.
+
+``fit_all_stars_simultaneous`` mirrors
+src/photometry/psf_photometry_simultaneous.jl:953-981 (same positional
+arguments, keyword names, defaults and ArgumentError texts) and returns a
+``MultiPassPhotResult`` (psf_photometry_single.jl:99-122).  ``fit_star``
+mirrors src/psf/psf_fitting.jl:229-250 and returns ``(best_model, LMResult)``
+(levenberg_marquardt.jl:28-41).  ``fit_star_batch`` runs many independent
+fit_star calls in one launch.
+
+Differences from the Julia API, all deliberate:
+  * the device computes in FP64 and results are returned as float64 arrays
+    (Float32 cannot hold 1e-4 px at 2048 px);
+  * ``background`` (image-shaped, optional) is subtracted on the device;
+  * ``solver=:lsmr``, ``model_rad=:auto``, IRLS ``reweight`` and PSF types
+    other than CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF}
+    raise ArgumentError -- there is no CPU fallback;
+  * ``spread_model`` / ``spread_model_err`` are NaN.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import threading
+import weakref
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from .psf import (ArgumentError, CircularGaussianPSF, GriddedPSFModel, ImagePSF, replace_params)
+
+_tls_lock = threading.Lock()
+
+
+class CudaError(RuntimeError):
+    pass
+
+
+class Context:
+    """A device context (cpb_ctx) with an upload cache for PSFs."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _abi.load_library()
+        h = C.c_void_p()
+        rc = self.lib.cpb_ctx_create(int(device), C.byref(h))
+        if rc != _abi.CPB_OK:
+            raise CudaError(f"cpb_ctx_create(device={device}) failed with status {rc}")
+        self.handle = h
+        self.device = device
+        self._psfs: dict[int, tuple] = {}
+
+    def close(self):
+        if self.handle:
+            for _, (hp, _ref) in list(self._psfs.items()):
+                self.lib.cpb_psf_free(self.handle, hp)
+            self._psfs.clear()
+            self.lib.cpb_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def error(self) -> str:
+        return self.lib.cpb_last_error(self.handle).decode()
+
+    def raise_for(self, rc: int, what: str):
+        if rc == _abi.CPB_OK:
+            return
+        msg = self.error()
+        if rc == _abi.CPB_ERR_ARGUMENT:
+            raise ArgumentError(msg)
+        if rc == _abi.CPB_ERR_OOM:
+            raise MemoryError(f"{what}: {msg}")
+        raise CudaError(f"{what} failed ({rc}): {msg}")
+
+    def psf_handle(self, psf, fwhm_override=None):
+        key = id(psf)
+        hit = self._psfs.get(key)
+        if hit is not None and hit[1]() is psf:
+            return hit[0]
+        desc, keep = psf_descriptor(psf)
+        hp = C.c_void_p()
+        rc = self.lib.cpb_psf_upload(self.handle, C.byref(desc), C.byref(hp))
+        self.raise_for(rc, "cpb_psf_upload")
+        del keep
+        self._psfs[key] = (hp, weakref.ref(psf))
+        return hp
+
+
+_default_ctx: Context | None = None
+
+
+def get_context(device: int = 0) -> Context:
+    global _default_ctx
+    with _tls_lock:
+        if _default_ctx is None or _default_ctx.device != device:
+            _default_ctx = Context(device)
+        return _default_ctx
+
+
+def psf_descriptor(psf):
+    """Builds a cpb_psf_desc for a supported PSF; returns (desc, keepalive)."""
+    d = _abi.PsfDesc()
+    keep = []
+    if isinstance(psf, CircularGaussianPSF):
+        d.kind = _abi.CPB_PSF_CIRCULAR_GAUSSIAN
+        d.n_nodes = 0
+        d.eltype = _abi.CPB_F64
+        d.fwhm = float(psf.fwhm)
+        return d, keep
+    if isinstance(psf, ImagePSF):
+        nodes, gy, gx, kind = [psf], [0.0], [0.0], _abi.CPB_PSF_IMAGE
+    elif isinstance(psf, GriddedPSFModel):
+        nodes, gy, gx, kind = psf.psfs, list(psf.grid_y), list(psf.grid_x), _abi.CPB_PSF_GRIDDED_IMAGE
+    else:
+        raise ArgumentError(f"unsupported PSF type {type(psf).__name__} for the B200 path")
+    n = len(nodes)
+    datas = [np.asfortranarray(nd.data, dtype=np.float64) for nd in nodes]
+    keep += datas
+    ptrs = (C.c_void_p * n)(*[a.ctypes.data for a in datas])
+    ny = np.array([a.shape[0] for a in datas], dtype=np.int64)
+    nx = np.array([a.shape[1] for a in datas], dtype=np.int64)
+    os_ = np.array([v for nd in nodes for v in nd.oversampling], dtype=np.int64)
+    org = np.array([v for nd in nodes for v in (nd.origin["y"], nd.origin["x"])], dtype=np.float64)
+    fill = np.array([nd.fill_value for nd in nodes], dtype=np.float64)
+    gya = np.asarray(gy, dtype=np.float64)
+    gxa = np.asarray(gx, dtype=np.float64)
+    keep += [ptrs, ny, nx, os_, org, fill, gya, gxa]
+    d.kind = kind
+    d.n_nodes = n
+    d.eltype = _abi.CPB_F64
+    d.node_data = C.cast(ptrs, C.POINTER(C.c_void_p))
+    d.node_ny = ny.ctypes.data_as(_abi._i64p)
+    d.node_nx = nx.ctypes.data_as(_abi._i64p)
+    d.node_os = os_.ctypes.data_as(_abi._i64p)
+    d.node_origin = org.ctypes.data_as(_abi._dp)
+    d.node_fill_value = fill.ctypes.data_as(_abi._dp)
+    d.grid_y = gya.ctypes.data_as(_abi._dp)
+    d.grid_x = gxa.ctypes.data_as(_abi._dp)
+    return d, keep
+
+
+@dataclass
+class MultiPassPhotResult:
+    """MultiPassPhotResult (psf_photometry_single.jl:99-122)."""
+    y: np.ndarray
+    x: np.ndarray
+    y_err: np.ndarray
+    x_err: np.ndarray
+    flux: np.ndarray
+    flux_err: np.ndarray
+    bkg: np.ndarray
+    bkg_err: np.ndarray
+    converged: np.ndarray
+    valid: np.ndarray
+    chisq: np.ndarray
+    qfit: np.ndarray
+    qfit_expected: np.ndarray
+    qfit_z: np.ndarray
+    crowding: np.ndarray
+    spread_model: np.ndarray
+    spread_model_err: np.ndarray
+    n_iter: np.ndarray
+    n_passes: int
+    n_failed: int
+    failure_msgs: list
+    residual: np.ndarray
+    stats: dict | None = None
+    debug: dict | None = None
+
+
+@dataclass
+class LMResult:
+    """LMResult (levenberg_marquardt.jl:28-41)."""
+    minimizer: np.ndarray
+    minimum: float
+    cost_init: float
+    converged: bool
+    x_converged: bool
+    f_converged: bool
+    g_converged: bool
+    iterations: int
+    lambda_final: float
+    sigma_final: float
+    cov: np.ndarray
+    chisq: float
+
+
+_DAMPING = {"marquardt": _abi.CPB_DAMP_MARQUARDT, "levenberg": _abi.CPB_DAMP_LEVENBERG,
+            "none": _abi.CPB_DAMP_NONE}
+_COV = {None: _abi.CPB_COV_AUTO, "known_weights": _abi.CPB_COV_KNOWN_WEIGHTS,
+        "reweighted": _abi.CPB_COV_REWEIGHTED}
+_PREC = {"fp64": _abi.CPB_PREC_FP64, "mixed": _abi.CPB_PREC_MIXED}
+
+
+def _props(psf):
+    if isinstance(psf, CircularGaussianPSF):
+        return ("y", "x", "fwhm", "flux", "bkg")
+    if isinstance(psf, (ImagePSF, GriddedPSFModel)):
+        return ("y", "x", "flux", "bkg")
+    raise ArgumentError(f"unsupported PSF type {type(psf).__name__} for the B200 path")
+
+
+_BITS = {"y": _abi.CPB_FREE_Y, "x": _abi.CPB_FREE_X, "flux": _abi.CPB_FREE_FLUX, "bkg": _abi.CPB_FREE_BKG,
+         "fwhm": _abi.CPB_FREE_FWHM}
+
+
+def _free_mask(psf, fixed):
+    mask = 0
+    for k in _props(psf):
+        if k not in fixed:
+            mask |= _BITS[k]
+    return mask
+
+
+def _image_arrays(image, inv_var, background):
+    img = np.asarray(image)
+    if img.ndim != 2:
+        raise ArgumentError("`image` must be a matrix")
+    dt = np.float32 if img.dtype == np.float32 else np.float64
+    imgf = np.asfortranarray(img, dtype=dt)
+    ivf = None
+    if inv_var is not None:
+        iv = np.asarray(inv_var)
+        if iv.shape != img.shape:
+            raise ArgumentError("`inv_var` must be the same size as `image`")
+        ivf = np.asfortranarray(iv, dtype=dt)
+    bkf = None
+    if background is not None:
+        bk = np.asarray(background)
+        if bk.ndim == 0:
+            bk = np.full(img.shape, float(bk))
+        if bk.shape != img.shape:
+            raise ArgumentError("`background` must be the same size as `image`")
+        bkf = np.asfortranarray(bk, dtype=dt)
+    et = _abi.CPB_F32 if dt == np.float32 else _abi.CPB_F64
+    return imgf, ivf, bkf, et
+
+
+def _catalog(sources):
+    """_extract_source_catalog for NamedTuple-like catalogues (psf_photometry_single.jl:167-181)."""
+    get = (lambda k: sources[k]) if isinstance(sources, dict) else (lambda k: getattr(sources, k))
+    has = (lambda k: k in sources) if isinstance(sources, dict) else (lambda k: hasattr(sources, k))
+    y = np.ascontiguousarray(np.asarray(get("y"), dtype=np.float64).ravel())
+    x = np.ascontiguousarray(np.asarray(get("x"), dtype=np.float64).ravel())
+    n = y.size
+    f = np.ascontiguousarray(np.asarray(get("flux"), dtype=np.float64).ravel()) if has("flux") else np.ones(n)
+    if x.size != n or f.size != n:
+        raise ArgumentError("source y/x/flux lengths must match")
+    return y, x, f
+
+
+def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_iterations=10, linear_tol=1.0e-6,
+               model_rad="auto", model_rad_max=None, model_rad_nsigma=1.0, max_step=0.25, max_trials=8, max_iter=40,
+               x_tol=1.0e-5, f_tol=1.0e-4, g_tol=1.0e-4, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0,
+               lambda_min=1.0e-12, lambda_max=1.0e12, damping="marquardt", covariance_estimator=None,
+               precision="fp64"):
+    """Keyword arguments -> cpb_sim_params (shared by the device path and the oracle)."""
+    P = _abi.SimParams()
+    P.fit_rad = float(fit_rad)
+    P.free_mask = _free_mask(psf, fixed)
+    P.inner_iterations = int(inner_iterations)
+    P.fixed_y = float(fixed.get("y", 0.0))
+    P.fixed_x = float(fixed.get("x", 0.0))
+    P.fixed_flux = float(fixed.get("flux", 1.0))
+    P.fixed_bkg = float(fixed.get("bkg", 0.0))
+    P.fixed_fwhm = float(fixed.get("fwhm", getattr(psf, "fwhm", 0.0)))
+    P.linear_tol = float(linear_tol)
+    if isinstance(model_rad, str):
+        if model_rad != "auto":
+            raise ArgumentError(f"model_rad must be :auto or a positive real, got :{model_rad}")
+        P.model_rad_auto = 1
+        P.model_rad = 0.0
+    else:
+        P.model_rad_auto = 0
+        P.model_rad = float(model_rad)
+    P.max_trials = int(max_trials)
+    P.model_rad_max = float(10 * fit_rad if model_rad_max is None else model_rad_max)
+    P.model_rad_nsigma = float(model_rad_nsigma)
+    P.max_step = float(max_step)
+    P.max_iter = int(max_iter)
+    P.covariance = _COV[covariance_estimator]
+    P.x_tol, P.f_tol, P.g_tol = float(x_tol), float(f_tol), float(g_tol)
+    P.lambda_init, P.lambda_up, P.lambda_down = float(lambda_init), float(lambda_up), float(lambda_down)
+    P.lambda_min, P.lambda_max = float(lambda_min), float(lambda_max)
+    P.precision = _PREC[precision]
+    if solver not in ("lsqr", "lsmr"):
+        raise ArgumentError(f"solver must be :lsqr or :lsmr, got :{solver}")
+    P.solver = _abi.CPB_SOLVER_LSQR if solver == "lsqr" else _abi.CPB_SOLVER_LSMR
+    P.damping = _DAMPING[damping]
+    return P
+
+
+class SimOutputs:
+    """Caller-owned output arrays for one cpb_sim_result."""
+
+    def __init__(self, n, ny, nx, S2, residual=True, debug=False):
+        self.n = n
+        z = lambda: np.zeros(max(n, 1), dtype=np.float64)
+        self.y, self.x, self.flux, self.bkg = z(), z(), z(), z()
+        self.y_err, self.x_err, self.flux_err, self.bkg_err = z(), z(), z(), z()
+        self.chisq, self.qfit, self.qfit_expected, self.qfit_z, self.crowding = z(), z(), z(), z(), z()
+        self.converged = np.zeros(max(n, 1), dtype=np.uint8)
+        self.valid = np.zeros(max(n, 1), dtype=np.uint8)
+        self.n_iter = np.zeros(max(n, 1), dtype=np.int32)
+        self.residual = np.zeros((ny, nx), dtype=np.float64, order="F") if residual else None
+        self.debug = debug
+        if debug:
+            self.dbg_active = np.full(max(n, 1), -1, dtype=np.int32)
+            self.dbg_pixels = np.zeros(max(S2 * n, 1), dtype=np.int32)
+            self.dbg_model_R = np.zeros(max(n, 1), dtype=np.int32)
+        r = _abi.SimResult()
+        dp = lambda a: a.ctypes.data_as(_abi._dp)
+        r.y, r.x, r.flux, r.bkg = dp(self.y), dp(self.x), dp(self.flux), dp(self.bkg)
+        r.y_err, r.x_err, r.flux_err, r.bkg_err = dp(self.y_err), dp(self.x_err), dp(self.flux_err), dp(self.bkg_err)
+        r.converged = self.converged.ctypes.data_as(_abi._u8p)
+        r.valid = self.valid.ctypes.data_as(_abi._u8p)
+        r.chisq, r.qfit, r.qfit_expected = dp(self.chisq), dp(self.qfit), dp(self.qfit_expected)
+        r.qfit_z, r.crowding = dp(self.qfit_z), dp(self.crowding)
+        r.n_iter = self.n_iter.ctypes.data_as(_abi._i32p)
+        if residual:
+            r.residual = dp(self.residual)
+        if debug:
+            r.dbg_active = self.dbg_active.ctypes.data_as(_abi._i32p)
+            r.dbg_pixels = self.dbg_pixels.ctypes.data_as(_abi._i32p)
+            r.dbg_model_R = self.dbg_model_R.ctypes.data_as(_abi._i32p)
+        self.c = r
+
+    def result(self, ny, nx, S2) -> MultiPassPhotResult:
+        n = self.n
+        r = self.c
+        valid = self.valid[:n].astype(bool)
+        msgs = [f"star {i + 1}: excluded before the solve (no usable pixels or non-finite initial parameters)"
+                for i in range(n) if not valid[i] and r.n_active < n]
+        if r.n_active == n:
+            msgs = []
+        nan = np.full(n, np.nan)
+        res = MultiPassPhotResult(
+            y=self.y[:n].copy(), x=self.x[:n].copy(), y_err=self.y_err[:n].copy(), x_err=self.x_err[:n].copy(),
+            flux=self.flux[:n].copy(), flux_err=self.flux_err[:n].copy(), bkg=self.bkg[:n].copy(),
+            bkg_err=self.bkg_err[:n].copy(), converged=self.converged[:n].astype(bool), valid=valid,
+            chisq=self.chisq[:n].copy(), qfit=self.qfit[:n].copy(), qfit_expected=self.qfit_expected[:n].copy(),
+            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(), spread_model=nan.copy(),
+            spread_model_err=nan.copy(), n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes),
+            n_failed=int(r.n_failed), failure_msgs=msgs,
+            residual=self.residual if self.residual is not None else np.zeros((ny, nx)),
+            stats=dict(n_active=int(r.n_active), n_union=int(r.n_union), n_trials=int(r.n_trials),
+                       n_lsqr_iters=int(r.n_lsqr_iters), model_px_evals=float(r.model_px_evals),
+                       lsqr_px_macs=float(r.lsqr_px_macs), device_seconds=float(r.device_seconds)))
+        if self.debug:
+            na = int(r.n_active)
+            res.debug = dict(active=self.dbg_active[:na].copy(),
+                             pixels=self.dbg_pixels[:S2 * na].reshape(na, S2).copy(),
+                             model_R=self.dbg_model_R[:na].copy())
+        return res
+
+
+def fit_all_stars_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_var=None, background=None,
+                               spread_model_fwhm=None, solver="lsqr", inner_iterations=10, linear_tol=1.0e-6,
+                               model_rad="auto", model_rad_max=None, model_rad_nsigma=1.0, max_step=0.25,
+                               max_trials=8, max_iter=40, x_tol=1.0e-5, f_tol=1.0e-4, g_tol=1.0e-4,
+                               lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
+                               lambda_max=1.0e12, damping="marquardt", show_trace=False, covariance_estimator=None,
+                               precision="fp64", ctx: Context | None = None, debug=False,
+                               residual=True) -> MultiPassPhotResult:
+    """CrowdPhot.fit_all_stars_simultaneous on the B200 (psf_photometry_simultaneous.jl:953-1431)."""
+    fixed = dict(fixed or {})
+    ctx = ctx or get_context()
+    imgf, ivf, bkf, et = _image_arrays(image, inv_var, background)
+    y0, x0, f0 = _catalog(sources)
+    P = sim_params(psf, fit_rad, fixed, inv_var_given=ivf is not None, solver=solver,
+                   inner_iterations=inner_iterations, linear_tol=linear_tol, model_rad=model_rad,
+                   model_rad_max=model_rad_max, model_rad_nsigma=model_rad_nsigma, max_step=max_step,
+                   max_trials=max_trials, max_iter=max_iter, x_tol=x_tol, f_tol=f_tol, g_tol=g_tol,
+                   lambda_init=lambda_init, lambda_up=lambda_up, lambda_down=lambda_down, lambda_min=lambda_min,
+                   lambda_max=lambda_max, damping=damping, covariance_estimator=covariance_estimator,
+                   precision=precision)
+    ny, nx = imgf.shape
+    R = int(np.ceil(fit_rad)) if fit_rad > 0 else 0
+    S2 = (2 * R + 1) ** 2
+    outs = SimOutputs(y0.size, ny, nx, S2, residual=residual, debug=debug)
+    hp = ctx.psf_handle(psf)
+    vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    rc = ctx.lib.cpb_fit_simultaneous(ctx.handle, hp, C.byref(P), vp(imgf), et, ny, nx, vp(ivf), vp(bkf),
+                                      y0.size, y0.ctypes.data_as(_abi._dp), x0.ctypes.data_as(_abi._dp),
+                                      f0.ctypes.data_as(_abi._dp), C.byref(outs.c))
+    ctx.raise_for(rc, "cpb_fit_simultaneous")
+    return outs.result(ny, nx, S2)
+
+
+def lm_params(model, fixed, *, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
+              lambda_max=1.0e12, damping="marquardt", max_iter=200, x_tol=1.0e-8, f_tol=1.0e-4, g_tol=1.0e-4,
+              covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64"):
+    P = _abi.LMParams()
+    P.free_mask = _free_mask(model, fixed)
+    P.max_iter = int(max_iter)
+    P.fixed_y = float(fixed.get("y", model.y))
+    P.fixed_x = float(fixed.get("x", model.x))
+    P.fixed_flux = float(fixed.get("flux", model.flux))
+    P.fixed_bkg = float(fixed.get("bkg", model.bkg))
+    P.fixed_fwhm = float(fixed.get("fwhm", getattr(model, "fwhm", 0.0)))
+    P.x_tol, P.f_tol, P.g_tol = float(x_tol), float(f_tol), float(g_tol)
+    P.lambda_init, P.lambda_up, P.lambda_down = float(lambda_init), float(lambda_up), float(lambda_down)
+    P.lambda_min, P.lambda_max = float(lambda_min), float(lambda_max)
+    P.min_diagonal = float(min_diagonal)
+    P.damping = _DAMPING[damping]
+    P.covariance = _COV[covariance_estimator]
+    P.precision = _PREC[precision]
+    return P
+
+
+def _model_vector(model):
+    return np.array([getattr(model, k) for k in _props(model)], dtype=np.float64)
+
+
+def fit_star_batch(model, cutouts, *, inv_vars=None, origins, inits=None, fixed=None, ctx: Context | None = None,
+                   **kw):
+    """Many independent fit_star calls in one launch.
+
+    cutouts: list of 2-D arrays (each image[inds]); origins: list of (y1, x1),
+    the 1-based image coordinates of each cutout's first pixel; inits: list of
+    model parameter vectors (defaults to the model's own values).
+    Returns a dict of arrays (params, cov, cost, ..., status).
+    """
+    fixed = dict(fixed or {})
+    if kw.get("reweight") is not None:
+        raise ArgumentError("IRLS reweighting is not supported by the B200 path")
+    kw.pop("reweight", None)
+    kw.pop("scale_estimator", None)
+    kw.pop("weight_reset_tol", None)
+    kw.pop("show_trace", None)
+    ctx = ctx or get_context()
+    P = lm_params(model, fixed, **kw)
+    n = len(cutouts)
+    np_ = len(_props(model))
+    dt = np.float32 if all(np.asarray(c).dtype == np.float32 for c in cutouts) else np.float64
+    sizes = [np.asarray(c).shape for c in cutouts]
+    offs = np.zeros(n, dtype=np.int64)
+    tot = 0
+    for i, s in enumerate(sizes):
+        offs[i] = tot
+        tot += s[0] * s[1]
+    pix = np.empty(max(tot, 1), dtype=dt)
+    for i, c in enumerate(cutouts):
+        pix[offs[i]:offs[i] + c.size] = np.asarray(c, dtype=dt).ravel(order="F")
+    iv = None
+    if inv_vars is not None:
+        iv = np.empty(max(tot, 1), dtype=dt)
+        for i, c in enumerate(inv_vars):
+            if np.asarray(c).shape != sizes[i]:
+                raise ArgumentError("`inv_var` must be the same size as `image`")
+            iv[offs[i]:offs[i] + sizes[i][0] * sizes[i][1]] = np.asarray(c, dtype=dt).ravel(order="F")
+    nyv = np.array([s[0] for s in sizes], dtype=np.int32)
+    nxv = np.array([s[1] for s in sizes], dtype=np.int32)
+    y1 = np.array([o[0] for o in origins], dtype=np.int32)
+    x1 = np.array([o[1] for o in origins], dtype=np.int32)
+    init = np.ascontiguousarray(np.stack(inits) if inits is not None else np.tile(_model_vector(model), (n, 1)),
+                                dtype=np.float64)
+    nf = bin(P.free_mask).count("1")
+    out = dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), cost=np.zeros(n), cost_init=np.zeros(n),
+               chisq=np.zeros(n), lambda_final=np.zeros(n), converged=np.zeros(n, np.uint8),
+               x_converged=np.zeros(n, np.uint8), f_converged=np.zeros(n, np.uint8),
+               g_converged=np.zeros(n, np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
+    r = _abi.LMResultC()
+    dp = lambda a: a.ctypes.data_as(_abi._dp)
+    u8 = lambda a: a.ctypes.data_as(_abi._u8p)
+    r.params, r.cov, r.cost, r.cost_init = dp(out["params"]), dp(out["cov"]), dp(out["cost"]), dp(out["cost_init"])
+    r.chisq, r.lambda_final = dp(out["chisq"]), dp(out["lambda_final"])
+    r.converged, r.x_converged = u8(out["converged"]), u8(out["x_converged"])
+    r.f_converged, r.g_converged = u8(out["f_converged"]), u8(out["g_converged"])
+    r.iterations = out["iterations"].ctypes.data_as(_abi._i32p)
+    r.status = out["status"].ctypes.data_as(_abi._i32p)
+    hp = ctx.psf_handle(model)
+    et = _abi.CPB_F32 if dt == np.float32 else _abi.CPB_F64
+    rc = ctx.lib.cpb_fit_lm_batch(ctx.handle, hp, C.byref(P), n, offs.ctypes.data_as(_abi._i64p),
+                                  nyv.ctypes.data_as(_abi._i32p), nxv.ctypes.data_as(_abi._i32p),
+                                  y1.ctypes.data_as(_abi._i32p), x1.ctypes.data_as(_abi._i32p),
+                                  pix.ctypes.data_as(C.c_void_p),
+                                  et, None if iv is None else iv.ctypes.data_as(C.c_void_p),
+                                  init.ctypes.data_as(_abi._dp), C.byref(r))
+    ctx.raise_for(rc, "cpb_fit_lm_batch")
+    out["device_seconds"] = float(r.device_seconds)
+    out["names"] = _props(model)
+    return out
+
+
+def fit_star(model, image, inds=None, *, fixed=None, inv_var=None, ctx: Context | None = None, **kw):
+    """CrowdPhot.PSF.fit_star on the B200 (psf_fitting.jl:229-308) -> (best_model, LMResult).
+
+    inds: ((y_first, y_last), (x_first, x_last)), 1-based inclusive; default the whole image.
+    """
+    fixed = dict(fixed or {})
+    img = np.asarray(image)
+    if inv_var is not None and np.asarray(inv_var).shape != img.shape:
+        raise ArgumentError("`inv_var` must be the same size as `image`")
+    if inds is None:
+        inds = ((1, img.shape[0]), (1, img.shape[1]))
+    (ya, yb), (xa, xb) = inds
+    cut = img[ya - 1:yb, xa - 1:xb]
+    ivc = None if inv_var is None else [np.asarray(inv_var)[ya - 1:yb, xa - 1:xb]]
+    out = fit_star_batch(model, [cut], inv_vars=ivc, origins=[(ya, xa)], fixed=fixed, ctx=ctx, **kw)
+    if out["status"][0] != 0:
+        nf = bin(_free_mask(model, fixed)).count("1")
+        if ivc is not None:
+            iv = ivc[0]
+            nvalid = int(np.sum(np.isfinite(iv) & (iv > 0)))
+            if not nvalid > nf:
+                raise ArgumentError(f"too few valid inv_var pixels ({nvalid}) for {nf} free parameters")
+        raise ArgumentError(f"degrees of freedom must be positive; too many free parameters ({nf}) for the number "
+                            f"of observations ({cut.size})")
+    names = out["names"]
+    params = out["params"][0]
+    best = replace_params(model, **{k: params[i] for i, k in enumerate(names)})
+    free = [i for i, k in enumerate(names) if k not in fixed]
+    res = LMResult(minimizer=params[free].copy(), minimum=float(out["cost"][0]), cost_init=float(out["cost_init"][0]),
+                   converged=bool(out["converged"][0]), x_converged=bool(out["x_converged"][0]),
+                   f_converged=bool(out["f_converged"][0]), g_converged=bool(out["g_converged"][0]),
+                   iterations=int(out["iterations"][0]), lambda_final=float(out["lambda_final"][0]),
+                   sigma_final=float("nan"), cov=out["cov"][0].copy(), chisq=float(out["chisq"][0]))
+    return best, res

@@ -1,0 +1,305 @@
+// cpb_api.cu -- the extern "C" boundary (include/crowdphot_b200.h).
+//
+// Context and PSF handles, argument validation that mirrors the reference's
+// constructors, host<->device staging, and error translation: C++ exceptions
+// never cross the ABI; every entry point returns a CPB_* status and leaves a
+// message for cpb_last_error().
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "cpb_internal.cuh"
+
+namespace cpb {
+
+void* scratch(cpb_ctx* ctx, const char* name, size_t bytes) {
+    auto& b = ctx->bufs[name];
+    if (b.bytes >= bytes && b.p) return b.p;
+    if (b.p) {
+        check(cudaStreamSynchronize(ctx->stream), "sync before realloc");
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = std::max<size_t>(bytes, 256);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        throw OomError{std::string("device memory exhausted allocating ") + name};
+    }
+    check(e, "cudaMalloc");
+    b.p = p;
+    b.bytes = want;
+    return p;
+}
+
+template <typename F>
+int guarded(cpb_ctx* ctx, F&& f) {
+    if (!ctx) return CPB_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->err.clear();
+    try {
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        return f();
+    } catch (const ArgError& e) {
+        ctx->err = e.msg;
+        return CPB_ERR_ARGUMENT;
+    } catch (const OomError& e) {
+        ctx->err = e.msg;
+        return CPB_ERR_OOM;
+    } catch (const CudaError& e) {
+        ctx->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);
+        return CPB_ERR_CUDA;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return CPB_ERR_INTERNAL;
+    }
+}
+
+}  // namespace cpb
+
+using namespace cpb;
+
+extern "C" {
+
+const char* cpb_version(void) { return "crowdphot_b200 0.1 (sm_100a)"; }
+
+int cpb_ctx_create(int device, cpb_ctx** out) {
+    if (!out) return CPB_ERR_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return CPB_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return CPB_ERR_ARGUMENT;
+    auto* ctx = new cpb_ctx();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaMallocHost(&ctx->pinned, 4096) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return CPB_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
+    *out = ctx;
+    return CPB_OK;
+}
+
+int cpb_ctx_destroy(cpb_ctx* ctx) {
+    if (!ctx) return CPB_OK;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        for (auto& kv : ctx->bufs)
+            if (kv.second.p) cudaFree(kv.second.p);
+        ctx->bufs.clear();
+        if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+        if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return CPB_OK;
+}
+
+const char* cpb_last_error(const cpb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
+    return guarded(ctx, [&]() -> int {
+        if (!d || !out) throw ArgError{"null argument"};
+        *out = nullptr;
+        auto* ps = new cpb_psf();
+        DevPsf& dp = ps->dev;
+        std::memset(&dp, 0, sizeof(dp));
+        dp.kind = d->kind;
+        dp.fwhm = d->fwhm;
+        try {
+            if (d->kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+                if (!(std::isfinite(d->fwhm))) throw ArgError{"CircularGaussianPSF fwhm must be finite"};
+                dp.n_nodes = 0;
+                *out = ps;
+                return CPB_OK;
+            }
+            if (d->kind != CPB_PSF_GRIDDED_IMAGE && d->kind != CPB_PSF_IMAGE) throw ArgError{"unsupported PSF kind"};
+            const int nn = d->n_nodes;
+            if (nn < 1) throw ArgError{"`psfs` must be non-empty"};
+            if (d->kind == CPB_PSF_IMAGE && nn != 1) throw ArgError{"ImagePSF takes exactly one node"};
+            if (nn > kMaxNodes) throw ArgError{"too many PSF nodes"};
+            if (d->eltype != CPB_F32 && d->eltype != CPB_F64) throw ArgError{"unsupported PSF eltype"};
+            // ImagePSF checks (empirical_models.jl:101-140)
+            std::vector<double> h64;
+            std::vector<DevNode> nodes(nn);
+            int64_t off = 0;
+            for (int k = 0; k < nn; ++k) {
+                DevNode& nd = nodes[k];
+                const int64_t nyd = d->node_ny[k], nxd = d->node_nx[k];
+                if (nyd < 4 || nxd < 4) throw ArgError{"each axis of `data` must have at least 4 samples"};
+                nd.ny = (int32_t)nyd;
+                nd.nx = (int32_t)nxd;
+                nd.off = off;
+                nd.sx = (double)d->node_os[2 * k];
+                nd.sy = (double)d->node_os[2 * k + 1];
+                if (!(nd.sx > 0 && nd.sy > 0)) throw ArgError{"`oversampling` values must be positive"};
+                nd.oy = d->node_origin[2 * k];
+                nd.ox = d->node_origin[2 * k + 1];
+                if (!std::isfinite(nd.oy) || !std::isfinite(nd.ox)) throw ArgError{"`origin` must be finite"};
+                nd.fill = d->node_fill_value ? d->node_fill_value[k] : 0.0;
+                const int64_t ne = nyd * nxd;
+                const int64_t padded = (ne + 3) / 4 * 4;  // 32-byte (FP64) / 16-byte (FP32) node alignment
+                h64.resize(off + padded, 0.0);
+                for (int64_t q = 0; q < ne; ++q) {
+                    double v = d->eltype == CPB_F64 ? ((const double*)d->node_data[k])[q]
+                                                    : (double)((const float*)d->node_data[k])[q];
+                    if (!std::isfinite(v)) throw ArgError{"all elements of `data` must be finite"};
+                    h64[off + q] = v;
+                }
+                off += padded;
+            }
+            // node grid (gridded_psf.jl:106-134)
+            std::vector<double> yg, xg;
+            std::vector<int32_t> ig;
+            if (nn == 1 || d->kind == CPB_PSF_IMAGE) {
+                yg = {d->grid_y ? d->grid_y[0] : 0.0};
+                xg = {d->grid_x ? d->grid_x[0] : 0.0};
+                ig = {0};
+            } else {
+                for (int k = 0; k < nn; ++k)
+                    if (!std::isfinite(d->grid_y[k]) || !std::isfinite(d->grid_x[k]))
+                        throw ArgError{"`grid_y` and `grid_x` must be finite"};
+                std::set<double> ys(d->grid_y, d->grid_y + nn), xs(d->grid_x, d->grid_x + nn);
+                yg.assign(ys.begin(), ys.end());
+                xg.assign(xs.begin(), xs.end());
+                if (yg.size() < 2 || xg.size() < 2)
+                    throw ArgError{
+                        "`grid_y` and `grid_x` must each contain at least 2 unique values unless a single PSF is "
+                        "supplied"};
+                if ((size_t)nn != yg.size() * xg.size())
+                    throw ArgError{"`grid_y`/`grid_x` positions do not form a complete rectangular grid"};
+                ig.assign(yg.size() * xg.size(), -1);
+                for (int k = 0; k < nn; ++k) {
+                    size_t iy = std::lower_bound(yg.begin(), yg.end(), d->grid_y[k]) - yg.begin();
+                    size_t ix = std::lower_bound(xg.begin(), xg.end(), d->grid_x[k]) - xg.begin();
+                    int32_t& slot = ig[iy + ix * yg.size()];
+                    if (slot != -1) throw ArgError{"duplicate node position"};
+                    slot = k;
+                }
+            }
+            std::vector<float> h32(h64.size());
+            for (size_t q = 0; q < h64.size(); ++q) h32[q] = (float)h64[q];
+            check(cudaMalloc(&ps->d_data64, sizeof(double) * h64.size()), "cudaMalloc");
+            check(cudaMalloc(&ps->d_data32, sizeof(float) * h32.size()), "cudaMalloc");
+            check(cudaMalloc(&ps->d_nodes, sizeof(DevNode) * nn), "cudaMalloc");
+            check(cudaMalloc(&ps->d_ygrid, sizeof(double) * yg.size()), "cudaMalloc");
+            check(cudaMalloc(&ps->d_xgrid, sizeof(double) * xg.size()), "cudaMalloc");
+            check(cudaMalloc(&ps->d_index_grid, sizeof(int32_t) * ig.size()), "cudaMalloc");
+            check(cudaMemcpy(ps->d_data64, h64.data(), sizeof(double) * h64.size(), cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_data32, h32.data(), sizeof(float) * h32.size(), cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_nodes, nodes.data(), sizeof(DevNode) * nn, cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_ygrid, yg.data(), sizeof(double) * yg.size(), cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_xgrid, xg.data(), sizeof(double) * xg.size(), cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_index_grid, ig.data(), sizeof(int32_t) * ig.size(), cudaMemcpyHostToDevice), "h2d");
+            dp.n_nodes = nn;
+            dp.gny = (int32_t)yg.size();
+            dp.gnx = (int32_t)xg.size();
+            dp.data64 = ps->d_data64;
+            dp.data32 = ps->d_data32;
+            dp.nodes = ps->d_nodes;
+            dp.ygrid = ps->d_ygrid;
+            dp.xgrid = ps->d_xgrid;
+            dp.index_grid = ps->d_index_grid;
+            dp.total_elems = (int64_t)h64.size();
+            ps->h_nodes = nodes;
+            ps->smem_bytes64 = (int64_t)h64.size() * 8;
+            ps->smem_bytes32 = (int64_t)h64.size() * 4;
+        } catch (...) {
+            cudaFree(ps->d_data64);
+            cudaFree(ps->d_data32);
+            cudaFree(ps->d_nodes);
+            cudaFree(ps->d_ygrid);
+            cudaFree(ps->d_xgrid);
+            cudaFree(ps->d_index_grid);
+            delete ps;
+            throw;
+        }
+        *out = ps;
+        return CPB_OK;
+    });
+}
+
+int cpb_psf_free(cpb_ctx* ctx, cpb_psf* ps) {
+    if (!ps) return CPB_OK;
+    return guarded(ctx, [&]() -> int {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ps->d_data64);
+        cudaFree(ps->d_data32);
+        cudaFree(ps->d_nodes);
+        cudaFree(ps->d_ygrid);
+        cudaFree(ps->d_xgrid);
+        cudaFree(ps->d_index_grid);
+        delete ps;
+        return CPB_OK;
+    });
+}
+
+int cpb_fit_simultaneous_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params, const void* d_image,
+                                int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var,
+                                const void* d_background, int64_t n, const double* d_y0, const double* d_x0,
+                                const double* d_flux0, cpb_sim_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || (n > 0 && (!d_y0 || !d_x0 || !d_flux0)) || !d_image)
+            throw ArgError{"null argument"};
+        return fit_simultaneous_dev(ctx, psf, params, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0,
+                                    d_flux0, out);
+    });
+}
+
+int cpb_fit_simultaneous(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params, const void* image,
+                         int32_t eltype, int64_t ny, int64_t nx, const void* inv_var, const void* background,
+                         int64_t n, const double* y0, const double* x0, const double* flux0, cpb_sim_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || !image || (n > 0 && (!y0 || !x0 || !flux0))) throw ArgError{"null argument"};
+        if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
+        if (ny <= 0 || nx <= 0) throw ArgError{"image must be non-empty"};
+        const size_t esz = eltype == CPB_F64 ? 8 : 4;
+        const size_t bytes = esz * (size_t)ny * (size_t)nx;
+        cudaStream_t st = ctx->stream;
+        void* d_img = scratch(ctx, "in_image", bytes);
+        void* d_iv = inv_var ? scratch(ctx, "in_inv_var", bytes) : nullptr;
+        void* d_bk = background ? scratch(ctx, "in_background", bytes) : nullptr;
+        double* d_y = (double*)scratch(ctx, "in_y", sizeof(double) * std::max<int64_t>(n, 1));
+        double* d_x = (double*)scratch(ctx, "in_x", sizeof(double) * std::max<int64_t>(n, 1));
+        double* d_f = (double*)scratch(ctx, "in_flux", sizeof(double) * std::max<int64_t>(n, 1));
+        check(cudaMemcpyAsync(d_img, image, bytes, cudaMemcpyHostToDevice, st), "h2d image");
+        if (d_iv) check(cudaMemcpyAsync(d_iv, inv_var, bytes, cudaMemcpyHostToDevice, st), "h2d inv_var");
+        if (d_bk) check(cudaMemcpyAsync(d_bk, background, bytes, cudaMemcpyHostToDevice, st), "h2d background");
+        if (n > 0) {
+            check(cudaMemcpyAsync(d_y, y0, sizeof(double) * n, cudaMemcpyHostToDevice, st), "h2d y");
+            check(cudaMemcpyAsync(d_x, x0, sizeof(double) * n, cudaMemcpyHostToDevice, st), "h2d x");
+            check(cudaMemcpyAsync(d_f, flux0, sizeof(double) * n, cudaMemcpyHostToDevice, st), "h2d flux");
+        }
+        return fit_simultaneous_dev(ctx, psf, params, d_img, eltype, ny, nx, d_iv, d_bk, n, d_y, d_x, d_f, out);
+    });
+}
+
+int cpb_fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, int64_t n_cutouts,
+                     const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,
+                     const int32_t* x_origin, const void* pixels, int32_t eltype, const void* inv_var,
+                     const double* init, cpb_lm_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || (n_cutouts > 0 && (!offsets || !ny || !nx || !y_origin || !x_origin ||
+                                                          !pixels || !init || !out->params || !out->iterations ||
+                                                          !out->status)))
+            throw ArgError{"null argument"};
+        return fit_lm_batch(ctx, psf, params, n_cutouts, offsets, ny, nx, y_origin, x_origin, pixels, eltype, inv_var,
+                            init, out);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,320 @@
+// cpb_internal.cuh -- shared host/device definitions of the B200 PSF-fitting library.
+//
+// Device PSF arithmetic restates CrowdPhot.jl:
+//   bicubic_interpolate / _cubic4        src/psf/empirical_models.jl:185-292
+//   _gridded_corner_bicubic_pass!        src/psf/psf_fitting.jl:1233-1321
+//   _grid_corners_dw                     src/psf/gridded_psf.jl:176-208
+//   CircularGaussianPSF evaluate(_fg)    src/psf/parametric_models.jl:79-115
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/crowdphot_b200.h"
+
+namespace cpb {
+
+// ---------------------------------------------------------------------------
+// device-side PSF description (passed by value to kernels)
+// ---------------------------------------------------------------------------
+struct DevNode {
+    int64_t off;        // element offset of this node in the concatenated data
+    int32_t ny, nx;
+    double oy, ox;      // origin.y, origin.x
+    double sx, sy;      // oversampling x, y
+    double fill;
+};
+
+constexpr int kMaxNodes = 64;
+
+struct DevPsf {
+    int32_t kind;       // CPB_PSF_*
+    int32_t n_nodes;
+    int32_t gny, gnx;   // node grid size
+    double fwhm;        // CircularGaussianPSF FWHM (the fixed value of the fit)
+    const double* data64;
+    const float* data32;
+    const DevNode* nodes;     // n_nodes
+    const double* ygrid;      // gny
+    const double* xgrid;      // gnx
+    const int32_t* index_grid;  // gny x gnx column-major, 0-based
+    int64_t total_elems;      // sum of padded node sizes
+};
+
+// Per-star model coefficients for one parameter vector (theta or theta+delta).
+struct StarCoef {
+    double y, x, flux, bkg;
+    double w[4], dwdy[4], dwdx[4];
+    int32_t idx[4];           // node index, -1 = inactive corner
+};
+
+// ---------------------------------------------------------------------------
+// device math
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// _grid_corners_dw (gridded_psf.jl:176-208).
+__device__ inline void grid_corners_dw(const DevPsf& P, double Y, double X, StarCoef& c) {
+    if (P.n_nodes == 1 || P.kind != CPB_PSF_GRIDDED_IMAGE) {
+        c.idx[0] = 0;
+        c.w[0] = 1.0;
+        c.dwdy[0] = 0.0;
+        c.dwdx[0] = 0.0;
+        for (int k = 1; k < 4; ++k) {
+            c.idx[k] = -1;
+            c.w[k] = 0.0;
+            c.dwdy[k] = 0.0;
+            c.dwdx[k] = 0.0;
+        }
+        return;
+    }
+    int iy = 0, ix = 0;  // searchsortedlast (1-based count of elements <= value)
+    for (int k = 0; k < P.gny; ++k) iy += (P.ygrid[k] <= Y) ? 1 : 0;
+    for (int k = 0; k < P.gnx; ++k) ix += (P.xgrid[k] <= X) ? 1 : 0;
+    iy = clampi(iy, 1, P.gny - 1);
+    ix = clampi(ix, 1, P.gnx - 1);
+    double y0 = P.ygrid[iy - 1], y1 = P.ygrid[iy], x0 = P.xgrid[ix - 1], x1 = P.xgrid[ix];
+    double Yc = fmin(fmax(Y, y0), y1), Xc = fmin(fmax(X, x0), x1);
+    double cy = (Y > y0 && Y < y1) ? 1.0 : 0.0;
+    double cx = (X > x0 && X < x1) ? 1.0 : 0.0;
+    double invnorm = 1.0 / ((x1 - x0) * (y1 - y0));
+    double dy1 = y1 - Yc, dy0 = Yc - y0, dx1 = x1 - Xc, dx0 = Xc - x0;
+    const int32_t* ig = P.index_grid;
+    int g = P.gny;
+    c.idx[0] = ig[(iy - 1) + (ix - 1) * g];
+    c.w[0] = dx1 * dy1 * invnorm;
+    c.dwdy[0] = -dx1 * cy * invnorm;
+    c.dwdx[0] = -dy1 * cx * invnorm;
+    c.idx[1] = ig[(iy - 1) + ix * g];
+    c.w[1] = dx0 * dy1 * invnorm;
+    c.dwdy[1] = -dx0 * cy * invnorm;
+    c.dwdx[1] = dy1 * cx * invnorm;
+    c.idx[2] = ig[iy + (ix - 1) * g];
+    c.w[2] = dx1 * dy0 * invnorm;
+    c.dwdy[2] = dx1 * cy * invnorm;
+    c.dwdx[2] = -dy0 * cx * invnorm;
+    c.idx[3] = ig[iy + ix * g];
+    c.w[3] = dx0 * dy0 * invnorm;
+    c.dwdy[3] = dx0 * cy * invnorm;
+    c.dwdx[3] = dy0 * cx * invnorm;
+    for (int k = 0; k < 4; ++k)
+        if (c.w[k] == 0.0 && c.dwdy[k] == 0.0 && c.dwdx[k] == 0.0) c.idx[k] = -1;
+}
+
+// One node's bicubic value and grid derivatives at detector pixel (py, px)
+// for a star centred at (Y, X) -- the per-pixel body of
+// _gridded_corner_bicubic_pass!.  D = element type of the tabulated data,
+// M = arithmetic type.  NEED_D = false skips the derivative arithmetic.
+template <typename D, typename M, bool NEED_D>
+__device__ __forceinline__ void corner_eval(const D* __restrict__ data, const DevNode& nd, M Y, M X, M py, M px, M& pv,
+                                            M& pdv, M& pdu) {
+    const M u = (M)nd.sx * (px - X) + (M)nd.ox;
+    const M v = (M)nd.sy * (py - Y) + (M)nd.oy;
+    const int nyd = nd.ny, nxd = nd.nx;
+    const bool inb = isfinite(u) && isfinite(v) && u >= (M)1 && u <= (M)nxd && v >= (M)1 && v <= (M)nyd;
+    const M uc = inb ? u : (M)1, vc = inb ? v : (M)1;
+    const int lx = clampi((int)floor(uc), 1, nxd - 1);
+    const int ly = clampi((int)floor(vc), 1, nyd - 1);
+    const M du = uc - (M)lx, dv = vc - (M)ly;
+    const int ix0 = clampi(lx - 1, 1, nxd) - 1, ix1 = lx - 1, ix2 = lx, ix3 = clampi(lx + 2, 1, nxd) - 1;
+    const int iy0 = clampi(ly - 1, 1, nyd) - 1, iy1 = ly - 1, iy2 = ly, iy3 = clampi(ly + 2, 1, nyd) - 1;
+    const D* c0 = data + (int64_t)ix0 * nyd;
+    const D* c1 = data + (int64_t)ix1 * nyd;
+    const D* c2 = data + (int64_t)ix2 * nyd;
+    const D* c3 = data + (int64_t)ix3 * nyd;
+    M row[4], drow[4];
+    const int iys[4] = {iy0, iy1, iy2, iy3};
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const M a = (M)c0[iys[r]], b = (M)c1[iys[r]], c = (M)c2[iys[r]], e = (M)c3[iys[r]];
+        const M k1 = (c - a) / 2;
+        const M k4 = c - b - k1;
+        const M k2 = 3 * k4 - (e - b) / 2 + k1;
+        const M k3 = k4 - k2;
+        row[r] = du * (du * (du * k3 + k2) + k1) + b;
+        if (NEED_D) drow[r] = du * (3 * du * k3 + 2 * k2) + k1;
+    }
+    const M v1 = (row[2] - row[0]) / 2;
+    const M v4 = row[2] - row[1] - v1;
+    const M v2 = 3 * v4 - (row[3] - row[1]) / 2 + v1;
+    const M v3 = v4 - v2;
+    const M val = dv * (dv * (dv * v3 + v2) + v1) + row[1];
+    pv = inb ? val : (M)nd.fill;
+    if (NEED_D) {
+        const M dpdv = dv * (3 * dv * v3 + 2 * v2) + v1;
+        const M u1 = (drow[2] - drow[0]) / 2;
+        const M u4 = drow[2] - drow[1] - u1;
+        const M u2 = 3 * u4 - (drow[3] - drow[1]) / 2 + u1;
+        const M u3 = u4 - u2;
+        const M dpdu = dv * (dv * (dv * u3 + u2) + u1) + drow[1];
+        pdv = inb ? dpdv : (M)0;
+        pdu = inb ? dpdu : (M)0;
+    }
+}
+
+template <typename D>
+__device__ __forceinline__ const D* node_data(const DevPsf& P);
+template <>
+__device__ __forceinline__ const double* node_data<double>(const DevPsf& P) { return P.data64; }
+template <>
+__device__ __forceinline__ const float* node_data<float>(const DevPsf& P) { return P.data32; }
+
+// Unit-flux profile s and ds/dY, ds/dX (gridded chain rule, psf_photometry_simultaneous.jl:500-512).
+// `base` points at the (possibly shared-memory) concatenated node data.
+template <typename D, typename M, bool NEED_D>
+__device__ __forceinline__ void grid_profile(const DevPsf& P, const D* __restrict__ base, const StarCoef& c, M py,
+                                             M px, M& s, M& dsdY, M& dsdX) {
+    s = 0;
+    dsdY = 0;
+    dsdX = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (c.idx[k] < 0) continue;
+        const DevNode nd = P.nodes[c.idx[k]];
+        M pv, pdv = 0, pdu = 0;
+        corner_eval<D, M, NEED_D>(base + nd.off, nd, (M)c.y, (M)c.x, py, px, pv, pdv, pdu);
+        s += (M)c.w[k] * pv;
+        if (NEED_D) {
+            dsdY += (M)c.dwdy[k] * pv - (M)c.w[k] * (M)nd.sy * pdv;
+            dsdX += (M)c.dwdx[k] * pv - (M)c.w[k] * (M)nd.sx * pdu;
+        }
+    }
+}
+
+// CircularGaussianPSF profile (parametric_models.jl:79-115): f and (df/dy, df/dx, df/dflux).
+template <typename M, bool NEED_D>
+__device__ __forceinline__ M gauss_eval(M fwhm, const StarCoef& c, M py, M px, M& gy, M& gx, M& gf) {
+    const M gp = (M)(-2.772588722239781);  // -4 log(2)
+    const M dx = px - (M)c.x, dy = py - (M)c.y;
+    const M f2 = fwhm * fwhm;
+    const M sq = (dx * dx + dy * dy) / f2;
+    const M norm = -((M)3.141592653589793 * f2 / gp);
+    const M amp = (M)c.flux / norm;
+    const M g = exp(gp * sq);
+    if (NEED_D) {
+        const M Ag = amp * g;
+        const M gf2 = gp / f2;
+        gy = -2 * Ag * gf2 * dy;
+        gx = -2 * Ag * gf2 * dx;
+        gf = g / norm;
+    }
+    return amp * g + (M)c.bkg;
+}
+
+// Model value flux*s + bkg at one pixel for either PSF family.
+template <typename D, typename M>
+__device__ __forceinline__ M model_value(const DevPsf& P, const D* __restrict__ base, const StarCoef& c, M py, M px) {
+    if (P.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        M a, b, e;
+        return gauss_eval<M, false>((M)P.fwhm, c, py, px, a, b, e);
+    }
+    M s, dY, dX;
+    grid_profile<D, M, false>(P, base, c, py, px, s, dY, dX);
+    return (M)c.flux * s + (M)c.bkg;
+}
+
+// Gradient (df/dy, df/dx, df/dflux) at one pixel.
+template <typename D, typename M>
+__device__ __forceinline__ void model_grad(const DevPsf& P, const D* __restrict__ base, const StarCoef& c, M py, M px,
+                                           M g[3]) {
+    if (P.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        gauss_eval<M, true>((M)P.fwhm, c, py, px, g[0], g[1], g[2]);
+        return;
+    }
+    M s, dY, dX;
+    grid_profile<D, M, true>(P, base, c, py, px, s, dY, dX);
+    g[0] = (M)c.flux * dY;
+    g[1] = (M)c.flux * dX;
+    g[2] = s;
+}
+
+// ---------------------------------------------------------------------------
+// warp helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// max that propagates NaN like Julia's max (fmax would drop it).
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+}  // namespace cpb
+
+// ---------------------------------------------------------------------------
+// host-side handles
+// ---------------------------------------------------------------------------
+struct cpb_psf {
+    cpb::DevPsf dev;
+    double* d_data64 = nullptr;
+    float* d_data32 = nullptr;
+    cpb::DevNode* d_nodes = nullptr;
+    double* d_ygrid = nullptr;
+    double* d_xgrid = nullptr;
+    int32_t* d_index_grid = nullptr;
+    std::vector<cpb::DevNode> h_nodes;
+    int64_t smem_bytes64 = 0;  // padded bytes of all nodes in FP64
+    int64_t smem_bytes32 = 0;
+};
+
+struct cpb_ctx {
+    int device = 0;
+    int n_sm = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    struct Buf {
+        void* p = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buf> bufs;  // grow-only scratch arena, reused across calls
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    void* pinned = nullptr;  // small pinned staging for scalar readbacks
+};
+
+namespace cpb {
+
+// Scratch arena: returns a device buffer of at least `bytes` under `name`.
+void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
+
+struct CudaError {
+    cudaError_t e;
+    const char* what;
+};
+
+inline void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError{e, what};
+}
+
+struct ArgError {
+    std::string msg;
+};
+struct OomError {
+    std::string msg;
+};
+
+// Simultaneous fit driver (cpb_sim.cu).  Inputs are device pointers.
+int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
+                         int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var, const void* d_background,
+                         int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
+                         cpb_sim_result* out);
+
+// Batched LM driver (cpb_lm.cu).  Host inputs.
+int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cutouts,
+                 const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,
+                 const int32_t* x_origin, const void* pixels, int32_t eltype, const void* inv_var,
+                 const double* init, cpb_lm_result* out);
+
+}  // namespace cpb

@@ -1,0 +1,454 @@
+// cpb_lm.cu -- batched per-star Levenberg-Marquardt (CrowdPhot.PSF.fit_star).
+//
+// Device restatement of
+//   _prepare_fit_star_inputs                src/psf/psf_fitting.jl:36-101
+//   _accum_circular_gaussian!               :354-451
+//   _accum_image_psf!                       :1115-1173
+//   _accum_gridded_imagepsf!                :1383-1517
+//   lm_irls (without IRLS), damp!, covariance!  src/levenberg_marquardt.jl:64-99, 361-680
+// One warp owns one cutout for the whole fit: lanes stride over the cutout's
+// pixels, the normal equations are reduced with warp shuffles (every lane
+// ends with the same A, b, cost), and every lane runs the identical small
+// Cholesky / accept-reject logic, so there is no divergence and no shared
+// state between cutouts.  Warps are persistent over a cutout queue.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "cpb_internal.cuh"
+
+namespace cpb {
+namespace {
+
+struct LMConst {
+    int np, nf;
+    int fidx[5];
+    int gauss;
+    int damping;
+    int max_iter;
+    int reweighted;
+    double fixv[5];  // fixed value per model parameter
+    double x_tol, f_tol, g_tol;
+    double lambda_init, lambda_up, lambda_down, lambda_min, lambda_max, min_diagonal;
+};
+
+// Normal equations at the full parameter vector fv (projected onto the free set).
+template <typename TI>
+__device__ double lm_accum(const DevPsf& P, const LMConst& L, const TI* __restrict__ pix, const TI* __restrict__ iv,
+                           int ny, int nx, int y1, int x1, const double* fv, double* A, double* b) {
+    const int lane = threadIdx.x & 31;
+    double Af[15], bf[5], cost = 0;
+#pragma unroll
+    for (int q = 0; q < 15; ++q) Af[q] = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) bf[q] = 0;
+    const int npx = ny * nx;
+    if (L.gauss) {
+        const double gp = -2.772588722239781;
+        const double Y = fv[0], X = fv[1], fwhm = fv[2], flux = fv[3], bkg = fv[4];
+        const double f2 = fwhm * fwhm;
+        const double norm = -(3.141592653589793 * f2 / gp);
+        const double amp = flux / norm, gf2 = gp / f2;
+        for (int e = lane; e < npx; e += 32) {
+            const int i = e % ny, j = e / ny;
+            const double dx = (double)(x1 + j) - X, dy = (double)(y1 + i) - Y;
+            const double sq = (dx * dx + dy * dy) / f2;
+            const double g = exp(gp * sq);
+            const double Ag = amp * g;
+            const double r = (amp * g + bkg) - (double)pix[e];
+            double w = 1.0;
+            if (iv) {
+                double v = (double)iv[e];
+                w = (isfinite(v) && v > 0) ? v : 0.0;
+            }
+            const double wr = w * r;
+            cost = wr * r + cost;
+            const double gv[5] = {-2 * Ag * gf2 * dy, -2 * Ag * gf2 * dx, -2 * Ag * (1 + gp * sq) / fwhm, g / norm,
+                                  1.0};
+            int t = 0;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                bf[q] = wr * gv[q] + bf[q];
+#pragma unroll
+                for (int pq = 0; pq <= q; ++pq) {
+                    Af[t] = (w * gv[pq]) * gv[q] + Af[t];
+                    ++t;
+                }
+            }
+        }
+    } else {
+        const double Y = fv[0], X = fv[1], flux = fv[2], bkg = fv[3];
+        StarCoef c;
+        c.y = Y;
+        c.x = X;
+        c.flux = flux;
+        c.bkg = bkg;
+        grid_corners_dw(P, Y, X, c);
+        for (int e = lane; e < npx; e += 32) {
+            const int i = e % ny, j = e / ny;
+            double s, dY, dX;
+            grid_profile<double, double, true>(P, P.data64, c, (double)(y1 + i), (double)(x1 + j), s, dY, dX);
+            const double r = (flux * s + bkg) - (double)pix[e];
+            double w = 1.0;
+            if (iv) {
+                double v = (double)iv[e];
+                w = (isfinite(v) && v > 0) ? v : 0.0;
+            }
+            const double wr = w * r;
+            cost = wr * r + cost;
+            const double gv[4] = {flux * dY, flux * dX, s, 1.0};
+            int t = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                bf[q] = wr * gv[q] + bf[q];
+#pragma unroll
+                for (int pq = 0; pq <= q; ++pq) {
+                    Af[t] = (w * gv[pq]) * gv[q] + Af[t];
+                    ++t;
+                }
+            }
+        }
+    }
+    cost = warp_sum(cost);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) bf[q] = warp_sum(bf[q]);
+#pragma unroll
+    for (int q = 0; q < 15; ++q) Af[q] = warp_sum(Af[q]);
+    // packed upper triangle: entry (pq, q), pq <= q, at q*(q+1)/2 + pq
+    for (int jq = 0; jq < L.nf; ++jq) {
+        b[jq] = bf[L.fidx[jq]];
+        for (int iq = 0; iq < L.nf; ++iq) {
+            int a = L.fidx[iq], bb = L.fidx[jq];
+            int lo = min(a, bb), hi = max(a, bb);
+            A[iq + jq * L.nf] = Af[hi * (hi + 1) / 2 + lo];
+        }
+    }
+    return cost;
+}
+
+__device__ bool lm_chol_solve(const double* A, int n, const double* b, double* x) {
+    double U[25];
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            double s = A[i + j * n];
+            for (int k = 0; k < i; ++k) s -= U[k + i * n] * U[k + j * n];
+            if (i == j) {
+                if (!(s > 0)) return false;
+                U[j + j * n] = sqrt(s);
+            } else {
+                U[i + j * n] = s / U[i + i * n];
+            }
+        }
+    double y[5];
+    for (int i = 0; i < n; ++i) {
+        double s = b[i];
+        for (int k = 0; k < i; ++k) s -= U[k + i * n] * y[k];
+        y[i] = s / U[i + i * n];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = y[i];
+        for (int k = i + 1; k < n; ++k) s -= U[i + k * n] * x[k];
+        x[i] = s / U[i + i * n];
+    }
+    return true;
+}
+
+// covariance! with the pinv fallback (levenberg_marquardt.jl:366-388).
+__device__ void lm_cov(const double* A0, int n, double* cov) {
+    double e[5];
+    bool ok = true;
+    for (int c = 0; c < n && ok; ++c) {
+        for (int i = 0; i < n; ++i) e[i] = (i == c) ? 1.0 : 0.0;
+        double x[5];
+        ok = lm_chol_solve(A0, n, e, x);
+        for (int i = 0; i < n; ++i) cov[i + c * n] = x[i];
+    }
+    if (ok) return;
+    // Jacobi pseudo-inverse of the symmetric matrix
+    double A[25], V[25];
+    for (int i = 0; i < n * n; ++i) A[i] = A0[i];
+    for (int i = 0; i < n * n; ++i) V[i] = 0;
+    for (int i = 0; i < n; ++i) V[i + i * n] = 1;
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            double s = 0.5 * (A[i + j * n] + A[j + i * n]);
+            A[i + j * n] = A[j + i * n] = s;
+        }
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0;
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j) off += A[i + j * n] * A[i + j * n];
+        if (off < 1e-300) break;
+        for (int pp = 0; pp < n; ++pp)
+            for (int q = pp + 1; q < n; ++q) {
+                double apq = A[pp + q * n];
+                if (apq == 0) continue;
+                double tau = (A[q + q * n] - A[pp + pp * n]) / (2 * apq);
+                double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+                double c = 1 / sqrt(1 + t * t), s = t * c;
+                for (int k = 0; k < n; ++k) {
+                    double akp = A[k + pp * n], akq = A[k + q * n];
+                    A[k + pp * n] = c * akp - s * akq;
+                    A[k + q * n] = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double apk = A[pp + k * n], aqk = A[q + k * n];
+                    A[pp + k * n] = c * apk - s * aqk;
+                    A[q + k * n] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double vkp = V[k + pp * n], vkq = V[k + q * n];
+                    V[k + pp * n] = c * vkp - s * vkq;
+                    V[k + q * n] = s * vkp + c * vkq;
+                }
+            }
+    }
+    double smax = 0;
+    for (int i = 0; i < n; ++i) smax = fmax(smax, fabs(A[i + i * n]));
+    double tol = 2.220446049250313e-16 * n * smax;
+    for (int i = 0; i < n * n; ++i) cov[i] = 0;
+    for (int ev = 0; ev < n; ++ev) {
+        double lam = A[ev + ev * n];
+        if (!(fabs(lam) > tol)) continue;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) cov[i + j * n] += V[i + ev * n] * V[j + ev * n] / lam;
+    }
+}
+
+struct LMOut {
+    double* params;   // n x np
+    double* cov;      // n x nf x nf
+    double* scal;     // n x 4: cost, cost_init, chisq, lambda
+    uint8_t* flags;   // n x 4: converged, x, f, g
+    int32_t* iters;
+    int32_t* status;
+};
+
+template <typename TI>
+__global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, const int64_t* __restrict__ offs,
+                                            const int32_t* __restrict__ cny, const int32_t* __restrict__ cnx,
+                                            const int32_t* __restrict__ cy1, const int32_t* __restrict__ cx1,
+                                            const TI* __restrict__ pixels, const TI* __restrict__ ivs,
+                                            const double* __restrict__ init, LMOut out) {
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int np = L.np, nf = L.nf;
+    for (int64_t c = warp; c < n_cut; c += nwarps) {
+        const int ny = cny[c], nx = cnx[c], y1 = cy1[c], x1 = cx1[c];
+        const TI* pix = pixels + offs[c];
+        const TI* iv = ivs ? ivs + offs[c] : nullptr;
+        const int64_t nobs = (int64_t)ny * nx;
+        // _prepare_fit_star_inputs checks (psf_fitting.jl:61-90) and lm_irls dof (:461-467)
+        int bad = 0;
+        if (iv) {
+            int nvalid = 0;
+            for (int64_t e = lane; e < nobs; e += 32) {
+                double v = (double)iv[e];
+                nvalid += (isfinite(v) && v > 0) ? 1 : 0;
+            }
+            nvalid = warp_sum(nvalid);
+            if (!(nvalid > nf)) bad = 1;
+        }
+        if (!(nobs - nf > 0)) bad = 1;
+        if (bad) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
+        double fv[5], x[5], xc[5], A[25], b[5], Ac[25], bc[5], Ad[25], d[5], D[5];
+        for (int q = 0; q < np; ++q) fv[q] = init[c * np + q];
+        for (int q = 0; q < np; ++q) {
+            bool fr = false;
+            for (int k = 0; k < nf; ++k) fr |= (L.fidx[k] == q);
+            if (!fr) fv[q] = L.fixv[q];
+        }
+        for (int k = 0; k < nf; ++k) x[k] = fv[L.fidx[k]];
+        double cost = lm_accum<TI>(P, L, pix, iv, ny, nx, y1, x1, fv, A, b);
+        const double cost_init = cost;
+        for (int k = 0; k < nf; ++k) D[k] = sqrt(fmax(A[k + k * nf], 1.0e-6));
+        double lam = L.lambda_init;
+        bool xconv = false, fconv = false, gconv = false, conv = false;
+        int iter = 0;
+        while (iter < L.max_iter) {
+            ++iter;
+            double gcos = 0;
+            for (int k = 0; k < nf; ++k)
+                gcos = nan_max(gcos, fabs(b[k]) / (sqrt(A[k + k * nf] * cost) + 2.220446049250313e-16));
+            if (gcos <= L.g_tol) {
+                gconv = conv = true;
+                break;
+            }
+            for (int k = 0; k < nf * nf; ++k) Ad[k] = A[k];
+            if (L.damping == CPB_DAMP_MARQUARDT)
+                for (int k = 0; k < nf; ++k) Ad[k + k * nf] += lam * fmax(Ad[k + k * nf], L.min_diagonal);
+            else if (L.damping == CPB_DAMP_LEVENBERG)
+                for (int k = 0; k < nf; ++k) Ad[k + k * nf] += lam;
+            if (!lm_chol_solve(Ad, nf, b, d)) {
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+                continue;
+            }
+            for (int k = 0; k < nf; ++k) d[k] = -d[k];
+            double db = 0, dAd = 0;
+            for (int k = 0; k < nf; ++k) db += d[k] * b[k];
+            for (int k = 0; k < nf; ++k)
+                for (int r = 0; r < nf; ++r) dAd += d[k] * A[k + r * nf] * d[r];
+            const double prered = -2 * db - dAd;
+            for (int k = 0; k < nf; ++k) xc[k] = x[k] + d[k];
+            double fc[5];
+            for (int q = 0; q < np; ++q) fc[q] = fv[q];
+            for (int k = 0; k < nf; ++k) fc[L.fidx[k]] = xc[k];
+            const double cost_c = lm_accum<TI>(P, L, pix, iv, ny, nx, y1, x1, fc, Ac, bc);
+            const bool accepted = cost_c < cost;
+            const double dcost = cost - cost_c;
+            const double ratio = prered > 0 ? dcost / prered : 0.0;
+            fconv = fabs(dcost) <= L.f_tol * (fabs(cost) + L.f_tol) && prered <= L.f_tol * (fabs(cost) + L.f_tol) &&
+                    0.5 * ratio <= 1;
+            double nd = 0, nxv = 0;
+            for (int k = 0; k < nf; ++k) {
+                nd += (D[k] * d[k]) * (D[k] * d[k]);
+                nxv += (D[k] * x[k]) * (D[k] * x[k]);
+            }
+            xconv = sqrt(nd) <= L.x_tol * (sqrt(nxv) + L.x_tol) && (accepted || fconv);
+            if (accepted) {
+                cost = cost_c;
+                lam = fmax(lam / L.lambda_down, L.lambda_min);
+                for (int k = 0; k < nf; ++k) x[k] = xc[k];
+                for (int k = 0; k < nf * nf; ++k) A[k] = Ac[k];
+                for (int k = 0; k < nf; ++k) b[k] = bc[k];
+                for (int q = 0; q < np; ++q) fv[q] = fc[q];
+                for (int k = 0; k < nf; ++k) D[k] = fmax(D[k], sqrt(A[k + k * nf]));
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+            } else {
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+            }
+        }
+        if (lane == 0) {
+            const double dof = (double)(nobs - nf);
+            double cov[25];
+            lm_cov(A, nf, cov);
+            const double f = L.reweighted ? cost / dof : 1.0;
+            if (out.cov)
+                for (int k = 0; k < nf * nf; ++k) out.cov[c * nf * nf + k] = cov[k] * f;
+            for (int q = 0; q < np; ++q) out.params[c * np + q] = fv[q];
+            out.scal[c * 4 + 0] = cost;
+            out.scal[c * 4 + 1] = cost_init;
+            out.scal[c * 4 + 2] = cost / dof;
+            out.scal[c * 4 + 3] = lam;
+            out.flags[c * 4 + 0] = conv;
+            out.flags[c * 4 + 1] = xconv;
+            out.flags[c * 4 + 2] = fconv;
+            out.flags[c * 4 + 3] = gconv;
+            out.iters[c] = iter;
+            out.status[c] = 0;
+        }
+    }
+}
+
+}  // namespace
+
+void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
+
+int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
+                 const int32_t* ny, const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,
+                 const void* pixels, int32_t eltype, const void* inv_var, const double* init, cpb_lm_result* out) {
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
+    if (P->precision != CPB_PREC_FP64) throw ArgError{"only the FP64 precision form is built for fit_star"};
+    if (n_cut <= 0) return 0;
+    LMConst L{};
+    L.gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    L.np = L.gauss ? 5 : 4;
+    const int bits_g[5] = {CPB_FREE_Y, CPB_FREE_X, CPB_FREE_FWHM, CPB_FREE_FLUX, CPB_FREE_BKG};
+    const int bits_i[4] = {CPB_FREE_Y, CPB_FREE_X, CPB_FREE_FLUX, CPB_FREE_BKG};
+    const double fix_g[5] = {P->fixed_y, P->fixed_x, P->fixed_fwhm, P->fixed_flux, P->fixed_bkg};
+    const double fix_i[4] = {P->fixed_y, P->fixed_x, P->fixed_flux, P->fixed_bkg};
+    L.nf = 0;
+    for (int q = 0; q < L.np; ++q) {
+        L.fixv[q] = L.gauss ? fix_g[q] : fix_i[q];
+        if (P->free_mask & (L.gauss ? bits_g[q] : bits_i[q])) L.fidx[L.nf++] = q;
+    }
+    if (L.nf == 0) throw ArgError{"all model parameters are fixed; nothing to fit"};
+    L.damping = P->damping;
+    L.max_iter = P->max_iter;
+    L.reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && inv_var == nullptr);
+    L.x_tol = P->x_tol;
+    L.f_tol = P->f_tol;
+    L.g_tol = P->g_tol;
+    L.lambda_init = P->lambda_init;
+    L.lambda_up = P->lambda_up;
+    L.lambda_down = P->lambda_down;
+    L.lambda_min = P->lambda_min;
+    L.lambda_max = P->lambda_max;
+    L.min_diagonal = P->min_diagonal;
+    cudaStream_t st = ctx->stream;
+    int64_t total = 0;
+    for (int64_t c = 0; c < n_cut; ++c) {
+        if (ny[c] <= 0 || nx[c] <= 0) throw ArgError{"cutout dimensions must be positive"};
+        total = std::max<int64_t>(total, offsets[c] + (int64_t)ny[c] * nx[c]);
+    }
+    const size_t esz = eltype == CPB_F64 ? 8 : 4;
+    auto up = [&](const char* name, const void* h, size_t bytes) {
+        void* d = scratch(ctx, name, std::max<size_t>(bytes, 8));
+        check(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st), "h2d");
+        return d;
+    };
+    check(cudaEventRecord(ctx->ev0, st), "event");
+    const int64_t* d_off = (const int64_t*)up("lm_off", offsets, sizeof(int64_t) * n_cut);
+    const int32_t* d_ny = (const int32_t*)up("lm_ny", ny, sizeof(int32_t) * n_cut);
+    const int32_t* d_nx = (const int32_t*)up("lm_nx", nx, sizeof(int32_t) * n_cut);
+    const int32_t* d_y1 = (const int32_t*)up("lm_y1", y_origin, sizeof(int32_t) * n_cut);
+    const int32_t* d_x1 = (const int32_t*)up("lm_x1", x_origin, sizeof(int32_t) * n_cut);
+    const void* d_pix = up("lm_pix", pixels, esz * total);
+    const void* d_iv = inv_var ? up("lm_iv", inv_var, esz * total) : nullptr;
+    const double* d_init = (const double*)up("lm_init", init, sizeof(double) * n_cut * L.np);
+    LMOut o;
+    o.params = (double*)scratch(ctx, "lm_params", sizeof(double) * n_cut * L.np);
+    o.cov = out->cov ? (double*)scratch(ctx, "lm_cov", sizeof(double) * n_cut * L.nf * L.nf) : nullptr;
+    o.scal = (double*)scratch(ctx, "lm_scal", sizeof(double) * n_cut * 4);
+    o.flags = (uint8_t*)scratch(ctx, "lm_flags", n_cut * 4);
+    o.iters = (int32_t*)scratch(ctx, "lm_iters", sizeof(int32_t) * n_cut);
+    o.status = (int32_t*)scratch(ctx, "lm_status", sizeof(int32_t) * n_cut);
+    const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
+    if (eltype == CPB_F64)
+        k_lm<double><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
+                                             (const double*)d_pix, (const double*)d_iv, d_init, o);
+    else
+        k_lm<float><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1, (const float*)d_pix,
+                                            (const float*)d_iv, d_init, o);
+    check(cudaGetLastError(), "k_lm");
+    check(cudaEventRecord(ctx->ev1, st), "event");
+    std::vector<double> scal(n_cut * 4);
+    std::vector<uint8_t> flags(n_cut * 4);
+    check(cudaMemcpyAsync(out->params, o.params, sizeof(double) * n_cut * L.np, cudaMemcpyDeviceToHost, st), "d2h");
+    if (out->cov)
+        check(cudaMemcpyAsync(out->cov, o.cov, sizeof(double) * n_cut * L.nf * L.nf, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(scal.data(), o.scal, sizeof(double) * n_cut * 4, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(flags.data(), o.flags, n_cut * 4, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(out->iterations, o.iters, sizeof(int32_t) * n_cut, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(out->status, o.status, sizeof(int32_t) * n_cut, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    out->device_seconds = ms * 1e-3;
+    for (int64_t c = 0; c < n_cut; ++c) {
+        if (out->cost) out->cost[c] = scal[c * 4 + 0];
+        if (out->cost_init) out->cost_init[c] = scal[c * 4 + 1];
+        if (out->chisq) out->chisq[c] = scal[c * 4 + 2];
+        if (out->lambda_final) out->lambda_final[c] = scal[c * 4 + 3];
+        if (out->converged) out->converged[c] = flags[c * 4 + 0];
+        if (out->x_converged) out->x_converged[c] = flags[c * 4 + 1];
+        if (out->f_converged) out->f_converged[c] = flags[c * 4 + 2];
+        if (out->g_converged) out->g_converged[c] = flags[c * 4 + 3];
+    }
+    return 0;
+}
+
+}  // namespace cpb

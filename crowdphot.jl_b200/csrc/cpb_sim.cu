@@ -1,0 +1,1524 @@
+// cpb_sim.cu -- B200 simultaneous damped Gauss-Newton / LSQR PSF fit.
+//
+// Device restatement of CrowdPhot.fit_all_stars_simultaneous
+// (src/photometry/psf_photometry_simultaneous.jl:953-1431).  Layout in HBM:
+//   * per-pixel vectors (data, data_work, w, sqrt(w), union mask, residual,
+//     LSQR u) are column-major npix arrays, as in the reference;
+//   * stamp derivatives V are star-major: star j owns a contiguous block of
+//     VS >= p*S2 values in the reference's (k fastest, then stamp pixel m)
+//     order (StampDerivatives.values, :19-43), padded to 128 bytes;
+//   * stamp pixel indices are not stored: they follow from the integer anchor
+//     and the fit-box offset (the reference's `pixels` matrix is rebuilt only
+//     for the bit-exact debug export);
+//   * per-tile star lists (32 x 8 pixel tiles, stars in Morton order) turn the
+//     reference's scatter-adds (apply_J!, _render_model!) into deterministic
+//     pixel gathers with no atomics.
+// Control flow per outer iteration follows :1186-1284; the LSQR inner solve
+// runs entirely on the device with its stopping tests evaluated in-kernel.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "cpb_internal.cuh"
+#include "cpb_reduce.cuh"
+
+namespace cpb {
+namespace {
+
+constexpr int TY = 32;   // tile rows (y, contiguous in memory)
+constexpr int TX = 8;    // tile columns
+constexpr int NT = 256;  // threads of the tile kernels (one pixel each)
+constexpr double kEps64 = 2.220446049250313e-16;
+
+enum RenderMode { MODE_CUR = 0, MODE_CAND = 1, MODE_FREEZE = 2, MODE_FINAL = 3 };
+
+// Device-resident scalars of one fit.
+struct Scalars {
+    double cost;       // current residual cost (over U)
+    double cost_cand;  // candidate cost
+    double gnorm;      // global gradient cosine
+    double beta1;      // ||mrhs||
+    // LSQR state (Krylov.jl lsqr recurrences)
+    double alpha, beta, inv_alpha, inv_beta;
+    double Anorm2, dNorm2, xNorm, xNorm2, c2, s2, z, xENorm2, res2, rhobar, phibar, ArNorm0;
+    double err_vec[5];
+    double wnorm2;
+    double lambda, atol, btol;
+    int iter, itmax, stopped, status;
+    int n_new_frozen;
+};
+
+// ---------------------------------------------------------------------------
+// setup kernels
+// ---------------------------------------------------------------------------
+template <typename TI>
+__global__ void k_prepare(const TI* __restrict__ img, const TI* __restrict__ iv, const TI* __restrict__ bkg,
+                          int64_t npix, double* data, double* data_work, double* w, double* sw,
+                          unsigned* nonfinite) {
+    int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q >= npix) return;
+    double d = (double)img[q] - (bkg ? (double)bkg[q] : 0.0);
+    double wv = 1.0;
+    if (iv) {
+        double v = (double)iv[q];
+        wv = (isfinite(v) && v > 0) ? v : 0.0;
+    }
+    if (!isfinite(d)) {
+        if (!iv) atomicAdd(nonfinite, 1u);
+        d = 0.0;
+        wv = 0.0;
+    }
+    data[q] = d;
+    data_work[q] = d;
+    w[q] = wv;
+    sw[q] = sqrt(wv);
+}
+
+__device__ __forceinline__ uint64_t spread_bits(uint64_t v) {
+    v &= 0x00000000ffffffffULL;
+    v = (v | (v << 16)) & 0x0000ffff0000ffffULL;
+    v = (v | (v << 8)) & 0x00ff00ff00ff00ffULL;
+    v = (v | (v << 4)) & 0x0f0f0f0f0f0f0f0fULL;
+    v = (v | (v << 2)) & 0x3333333333333333ULL;
+    v = (v | (v << 1)) & 0x5555555555555555ULL;
+    return v;
+}
+
+// _build_stamps! per catalogue star (:262-295): anchors (round half to even),
+// usable-pixel test, active flag and Morton key (:163-174).
+__global__ void k_anchor(int64_t n, const double* y0, const double* x0, const double* f0, int R, int ny, int nx,
+                         const double* __restrict__ w, int32_t* ay, int32_t* ax, uint8_t* ok, uint64_t* key,
+                         unsigned* neg) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool fin = isfinite(y0[i]) && isfinite(x0[i]);
+    const int a_y = fin ? (int)__double2ll_rn(y0[i]) : 0;
+    const int a_x = fin ? (int)__double2ll_rn(x0[i]) : 0;
+    bool any = false;
+    if (fin) {
+        for (int dx = -R; dx <= R && !any; ++dx) {
+            int gx = a_x + dx;
+            if (gx < 1 || gx > nx) continue;
+            for (int dy = -R; dy <= R; ++dy) {
+                int gy = a_y + dy;
+                if (gy < 1 || gy > ny) continue;
+                if (w[(gy - 1) + (int64_t)(gx - 1) * ny] > 0) {
+                    any = true;
+                    break;
+                }
+            }
+        }
+    }
+    const bool good = any && fin && isfinite(f0[i]);
+    ay[i] = a_y;
+    ax[i] = a_x;
+    ok[i] = good;
+    if (good && (a_y < 0 || a_x < 0)) atomicAdd(neg, 1u);
+    key[i] = spread_bits((uint64_t)(uint32_t)a_y) | (spread_bits((uint64_t)(uint32_t)a_x) << 1);
+}
+
+__global__ void k_gather_active(int64_t n_act, const int32_t* act, const int32_t* ay_c, const int32_t* ax_c,
+                                const double* y0, const double* x0, const double* f0, int p, int3 gc,
+                                int32_t* ay, int32_t* ax, double* theta) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    int i = act[j];
+    ay[j] = ay_c[i];
+    ax[j] = ax_c[i];
+    int g[3] = {gc.x, gc.y, gc.z};
+    for (int k = 0; k < p; ++k) theta[j * p + k] = g[k] == 1 ? y0[i] : (g[k] == 2 ? x0[i] : f0[i]);
+}
+
+// Union of usable stamp pixels (_touched_pixels, :329-335) and, on request,
+// the reference's `pixels` matrix (1-based, 0 = unusable).
+__global__ void k_union(int64_t n_act, const int32_t* ay, const int32_t* ax, int R, int ny, int nx,
+                        const double* __restrict__ w, uint8_t* umask, int32_t* dbg_pixels) {
+    int64_t j = blockIdx.x;
+    const int S = 2 * R + 1, S2 = S * S;
+    for (int m = threadIdx.x; m < S2; m += blockDim.x) {
+        int gy = ay[j] + (m % S) - R, gx = ax[j] + (m / S) - R;
+        int32_t fi = 0;
+        if (gy >= 1 && gy <= ny && gx >= 1 && gx <= nx) {
+            int64_t q = (gy - 1) + (int64_t)(gx - 1) * ny;
+            if (w[q] > 0) {
+                umask[q] = 1;
+                fi = (int32_t)(q + 1);
+            }
+        }
+        if (dbg_pixels) dbg_pixels[m + (int64_t)S2 * j] = fi;
+    }
+}
+
+__global__ void k_count_u8(const uint8_t* m, int64_t n, unsigned long long* cnt) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    unsigned c = (i < n && m[i]) ? 1u : 0u;
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(cnt, (unsigned long long)c);
+}
+
+// ---- per-tile star lists -------------------------------------------------
+__device__ __forceinline__ bool star_tiles(int ay, int ax, int Rj, int ny, int nx, int& ty0, int& ty1, int& tx0,
+                                           int& tx1) {
+    int ylo = max(ay - Rj, 1), yhi = min(ay + Rj, ny), xlo = max(ax - Rj, 1), xhi = min(ax + Rj, nx);
+    if (ylo > yhi || xlo > xhi) return false;
+    ty0 = (ylo - 1) / TY;
+    ty1 = (yhi - 1) / TY;
+    tx0 = (xlo - 1) / TX;
+    tx1 = (xhi - 1) / TX;
+    return true;
+}
+
+__global__ void k_tile_count(int64_t n_act, const int32_t* ay, const int32_t* ax, const int32_t* Rs, int Rconst,
+                             int ny, int nx, int32_t* cnt) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    int Rj = Rs ? Rs[j] : Rconst, a, b, c, d;
+    cnt[j] = star_tiles(ay[j], ax[j], Rj, ny, nx, a, b, c, d) ? (b - a + 1) * (d - c + 1) : 0;
+}
+
+__global__ void k_tile_emit(int64_t n_act, const int32_t* ay, const int32_t* ax, const int32_t* Rs, int Rconst,
+                            int ny, int nx, int nty, const int32_t* offs, uint32_t* keys, int32_t* vals) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    int Rj = Rs ? Rs[j] : Rconst, ty0, ty1, tx0, tx1;
+    if (!star_tiles(ay[j], ax[j], Rj, ny, nx, ty0, ty1, tx0, tx1)) return;
+    int o = offs[j];
+    for (int tx = tx0; tx <= tx1; ++tx)
+        for (int ty = ty0; ty <= ty1; ++ty) {
+            keys[o] = (uint32_t)(ty + tx * nty);
+            vals[o] = (int32_t)j;
+            ++o;
+        }
+}
+
+__global__ void k_tile_bounds(int64_t npairs, const uint32_t* keys, int32_t* start, int32_t* end) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= npairs) return;
+    uint32_t k = keys[i];
+    if (i == 0 || keys[i - 1] != k) start[k] = (int32_t)i;
+    if (i == npairs - 1 || keys[i + 1] != k) end[k] = (int32_t)(i + 1);
+}
+
+// ---------------------------------------------------------------------------
+// per-iteration kernels
+// ---------------------------------------------------------------------------
+struct FitConst {
+    int p;
+    int gc[3];     // grad_col of free param k (1 = dy, 2 = dx, 3 = dflux)
+    int ky, kx;    // index of y / x in the free list, -1 if fixed
+    double fixed_y, fixed_x, fixed_flux, fixed_bkg;
+    int R, S, S2, VS;
+    int ny, nx;
+    int nty, ntx;
+};
+
+// model_from_vector for star j: theta (+ delta when cand).
+__global__ void k_coef(int64_t n_act, FitConst fc, DevPsf P, const double* theta, const double* delta,
+                       StarCoef* coef) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    StarCoef c;
+    c.y = fc.fixed_y;
+    c.x = fc.fixed_x;
+    c.flux = fc.fixed_flux;
+    c.bkg = fc.fixed_bkg;
+    for (int k = 0; k < fc.p; ++k) {
+        double v = theta[j * fc.p + k];
+        if (delta) v = v + delta[j * fc.p + k];
+        if (fc.gc[k] == 1) c.y = v;
+        else if (fc.gc[k] == 2) c.x = v;
+        else c.flux = v;
+    }
+    grid_corners_dw(P, c.y, c.x, c);
+    coef[j] = c;
+}
+
+// _fill_stamps! (:342-399, :437-543) for the stars in `list`: one block per
+// star; raw = sqrt(w) * gradient, colnorm = max(||raw||, eps), V = raw / colnorm.
+// When `gram` is non-null it instead accumulates the unscaled p x p Gram
+// block sum(raw raw') per star for the error estimate (:1305-1318).
+template <int NTF, int MAXE>
+__global__ void __launch_bounds__(NTF) k_fill(const int32_t* __restrict__ list, int64_t nlist, FitConst fc, DevPsf P,
+                                              const StarCoef* __restrict__ coef, const int32_t* __restrict__ ay,
+                                              const int32_t* __restrict__ ax, const double* __restrict__ w,
+                                              const double* __restrict__ sw, double* __restrict__ V,
+                                              double* __restrict__ colnorm, double* __restrict__ gram) {
+    __shared__ double sh[32];
+    __shared__ double cn_sh[3];
+    const double* base = P.data64;
+    for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
+        const int j = list ? list[li] : (int)li;
+        const StarCoef c = coef[j];
+        const int a_y = ay[j], a_x = ax[j];
+        double raw[MAXE][3];
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int e = 0; e < MAXE; ++e) {
+            const int m = threadIdx.x + e * NTF;
+            raw[e][0] = raw[e][1] = raw[e][2] = 0.0;
+            if (m >= fc.S2) continue;
+            const int gy = a_y + (m % fc.S) - fc.R, gx = a_x + (m / fc.S) - fc.R;
+            if (gy < 1 || gy > fc.ny || gx < 1 || gx > fc.nx) continue;
+            const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
+            if (!(w[q] > 0)) continue;
+            double g[3];
+            model_grad<double, double>(P, base, c, (double)gy, (double)gx, g);
+            const double s = sw[q];
+            for (int k = 0; k < fc.p; ++k) raw[e][k] = s * g[fc.gc[k] - 1];
+            if (gram) {
+                int t = 0;
+                for (int k = 0; k < fc.p; ++k)
+                    for (int l = k; l < fc.p; ++l) acc[t++] += raw[e][k] * raw[e][l];
+            } else {
+                for (int k = 0; k < fc.p; ++k) acc[k] += raw[e][k] * raw[e][k];
+            }
+        }
+        const int nacc = gram ? fc.p * (fc.p + 1) / 2 : fc.p;
+        for (int t = 0; t < nacc; ++t) {
+            double tot = block_sum<NTF>(acc[t], sh);
+            if (threadIdx.x == 0) {
+                if (gram) gram[(int64_t)j * 6 + t] = tot;
+                else cn_sh[t] = tot;
+            }
+        }
+        __syncthreads();
+        if (!gram) {
+            double inv[3];
+            for (int k = 0; k < fc.p; ++k) {
+                double cn = sqrt(cn_sh[k]);
+                cn = cn < kEps64 ? kEps64 : cn;
+                inv[k] = 1.0 / cn;
+                if (threadIdx.x == 0) colnorm[(int64_t)j * fc.p + k] = cn;
+            }
+            double* Vj = V + (int64_t)j * fc.VS;
+#pragma unroll
+            for (int e = 0; e < MAXE; ++e) {
+                const int m = threadIdx.x + e * NTF;
+                if (m >= fc.S2) continue;
+                for (int k = 0; k < fc.p; ++k) Vj[m * fc.p + k] = raw[e][k] * inv[k];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Model gather over one 32x8 tile: each pixel sums flux*s + bkg over the
+// stars of the tile list that cover it (mode selects the stars and the
+// epilogue).  Replaces the scatter of _render_model! (:545-577, :605-673),
+// _residual_cost! (:675-684), _cost! (:686-693) and _freeze_star! (:739-754).
+template <int MODE>
+__global__ void __launch_bounds__(NT) k_render(FitConst fc, DevPsf P, const int32_t* __restrict__ tstart,
+                                               const int32_t* __restrict__ tend, const int32_t* __restrict__ tlist,
+                                               const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
+                                               const int32_t* __restrict__ Rs, int Rconst,
+                                               const uint8_t* __restrict__ incl, const StarCoef* __restrict__ coef,
+                                               const uint8_t* __restrict__ umask, const double* __restrict__ w,
+                                               const double* __restrict__ sw, const double* __restrict__ data_ref,
+                                               double* __restrict__ out, Reducer red, double* result) {
+    __shared__ double sh[32];
+    const int tile = blockIdx.x;
+    const int ty = tile % fc.nty, tx = tile / fc.nty;
+    const int gy = ty * TY + (threadIdx.x & 31) + 1;
+    const int gx = tx * TX + (threadIdx.x >> 5) + 1;
+    const bool inside = gy <= fc.ny && gx <= fc.nx;
+    const double* base = P.data64;
+    double model = 0.0;
+    const int s0 = tstart[tile], s1 = tend[tile];
+    for (int li = s0; li < s1; ++li) {
+        const int j = tlist[li];
+        if (incl && !incl[j]) continue;
+        const int Rj = Rs ? Rs[j] : Rconst;
+        const int dxo = gx - ax[j];
+        if (dxo < -Rj || dxo > Rj) continue;  // warp-uniform: one column per warp
+        const int dyo = gy - ay[j];
+        if (dyo < -Rj || dyo > Rj || !inside) continue;
+        model += model_value<double, double>(P, base, coef[j], (double)gy, (double)gx);
+    }
+    double part = 0.0;
+    if (inside) {
+        const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
+        if (MODE == MODE_CUR) {
+            double wr = 0.0;
+            if (umask[q]) {
+                wr = sw[q] * (model - data_ref[q]);
+                part = wr * wr;
+            }
+            out[q] = wr;  // wt_resid (zero outside U)
+        } else if (MODE == MODE_CAND) {
+            if (umask[q]) {
+                double r = model - data_ref[q];
+                part = w[q] * r * r;
+            }
+        } else if (MODE == MODE_FREEZE) {
+            out[q] -= model;  // data_work
+        } else {
+            out[q] = data_ref[q] - model;  // residual against the original data
+        }
+    }
+    if (MODE == MODE_CUR || MODE == MODE_CAND) grid_reduce<NT>(part, red, sh, result);
+}
+
+// J^T u for the stars of `list` (apply_JT!, :55-85): one warp per star,
+// coalesced reads of the star's V block, gathers of u.  Writes z[j*p+k] =
+// scale * sum_m V[j,m,k] u[pix(m)] (u already scaled when uscale != 1).
+// LSQR form (lsqr != 0): v_new = z - beta * v_old * inv_alpha_old, and the
+// grid reduction of ||v_new||^2 gives alpha (Krylov lsqr step 2).
+template <bool LSQR>
+__global__ void __launch_bounds__(256) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+                                            const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
+                                            const double* __restrict__ V, const double* __restrict__ u,
+                                            double* __restrict__ z, Scalars* sc, Reducer red) {
+    __shared__ double sh[32];
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
+    double uscale = 1.0, beta = 0.0, inv_alpha = 0.0;
+    if (LSQR) {
+        if (sc->stopped || sc->beta == 0.0) return;  // uniform across the grid
+        uscale = sc->inv_beta;
+        beta = sc->beta;
+        inv_alpha = sc->inv_alpha;
+    }
+    double part = 0.0;
+    for (int64_t li = warp; li < nlist; li += nwarps) {
+        const int j = list[li];
+        const int a_y = ay[j], a_x = ax[j];
+        const double* Vj = V + (int64_t)j * fc.VS;
+        double acc0 = 0, acc1 = 0, acc2 = 0;
+        for (int m = lane; m < fc.S2; m += 32) {
+            const int gy = a_y + (m % fc.S) - fc.R, gx = a_x + (m / fc.S) - fc.R;
+            if (gy < 1 || gy > fc.ny || gx < 1 || gx > fc.nx) continue;
+            const double uv = LSQR ? u[(gy - 1) + (int64_t)(gx - 1) * fc.ny] * uscale
+                                   : u[(gy - 1) + (int64_t)(gx - 1) * fc.ny];
+            const double* vm = Vj + m * fc.p;
+            acc0 += vm[0] * uv;
+            if (fc.p > 1) acc1 += vm[1] * uv;
+            if (fc.p > 2) acc2 += vm[2] * uv;
+        }
+        acc0 = warp_sum(acc0);
+        acc1 = warp_sum(acc1);
+        acc2 = warp_sum(acc2);
+        if (lane == 0) {
+            double a[3] = {acc0, acc1, acc2};
+            for (int k = 0; k < fc.p; ++k) {
+                double val = a[k];
+                if (LSQR) {
+                    val = val - beta * (z[(int64_t)j * fc.p + k] * inv_alpha);
+                    part += val * val;
+                }
+                z[(int64_t)j * fc.p + k] = val;
+            }
+        }
+    }
+    if (LSQR) {
+        double tot;
+        if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) {
+            double alpha = sqrt(tot);
+            sc->alpha = alpha;
+            sc->inv_alpha = alpha != 0.0 ? 1.0 / alpha : 0.0;
+        }
+    }
+}
+
+// J v gather (apply_J!, :95-137) fused with the LSQR update
+// u_new = J v - alpha u (Krylov lsqr step 1) and beta = ||u_new||.
+__global__ void __launch_bounds__(NT) k_Jv(FitConst fc, const int32_t* __restrict__ tstart,
+                                           const int32_t* __restrict__ tend, const int32_t* __restrict__ tlist,
+                                           const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
+                                           const uint8_t* __restrict__ live, const double* __restrict__ V,
+                                           const double* __restrict__ vt, const double* __restrict__ u_src,
+                                           double u_src_scale_sign, double* __restrict__ u_dst, Scalars* sc,
+                                           Reducer red) {
+    __shared__ double sh[32];
+    if (sc->stopped) return;
+    const double inv_alpha = sc->inv_alpha, alpha = sc->alpha;
+    // first iteration reads mrhs = -wt_resid with 1/beta1; later ones u_dst with 1/beta
+    const double uscale = u_src_scale_sign * sc->inv_beta;
+    const int tile = blockIdx.x;
+    const int ty = tile % fc.nty, tx = tile / fc.nty;
+    const int gy = ty * TY + (threadIdx.x & 31) + 1;
+    const int gx = tx * TX + (threadIdx.x >> 5) + 1;
+    const bool inside = gy <= fc.ny && gx <= fc.nx;
+    double acc = 0.0;
+    const int s0 = tstart[tile], s1 = tend[tile];
+    for (int li = s0; li < s1; ++li) {
+        const int j = tlist[li];
+        if (!live[j]) continue;
+        const int dxo = gx - ax[j];
+        if (dxo < -fc.R || dxo > fc.R) continue;
+        const int dyo = gy - ay[j];
+        if (dyo < -fc.R || dyo > fc.R || !inside) continue;
+        const int m = (dyo + fc.R) + (dxo + fc.R) * fc.S;
+        const double* vm = V + (int64_t)j * fc.VS + m * fc.p;
+        const double* vj = vt + (int64_t)j * fc.p;
+        double s = vm[0] * (vj[0] * inv_alpha);
+        if (fc.p > 1) s += vm[1] * (vj[1] * inv_alpha);
+        if (fc.p > 2) s += vm[2] * (vj[2] * inv_alpha);
+        acc += s;
+    }
+    double part = 0.0;
+    if (inside) {
+        const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
+        const double un = acc - alpha * (u_src[q] * uscale);
+        u_dst[q] = un;
+        part = un * un;
+    }
+    double tot;
+    if (grid_reduce<NT>(part, red, sh, &tot) && threadIdx.x == 0) {
+        double beta = sqrt(tot);
+        sc->beta = beta;
+        if (beta != 0.0) {
+            sc->inv_beta = 1.0 / beta;
+            sc->Anorm2 = sc->Anorm2 + alpha * alpha + beta * beta;
+            if (sc->lambda > 0) sc->Anorm2 += sc->lambda * sc->lambda;
+        }
+    }
+}
+
+__device__ __forceinline__ double sgn(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
+__device__ __forceinline__ void sym_givens(double a, double b, double& c, double& s, double& rho) {
+    if (b == 0) {
+        c = (a == 0) ? 1.0 : sgn(a);
+        s = 0;
+        rho = fabs(a);
+    } else if (a == 0) {
+        c = 0;
+        s = sgn(b);
+        rho = fabs(b);
+    } else if (fabs(b) > fabs(a)) {
+        double t = a / b;
+        s = sgn(b) / sqrt(1.0 + t * t);
+        c = s * t;
+        rho = b / s;
+    } else {
+        double t = b / a;
+        c = sgn(a) / sqrt(1.0 + t * t);
+        s = c * t;
+        rho = a / c;
+    }
+}
+
+// LSQR init after b_scaled: v1 = A'u1 = -b_scaled / beta1 (the first
+// adjoint product reuses the gradient pass), alpha1 = ||v1||, x = 0.
+__global__ void k_lsqr_v0(int64_t n, const double* b_scaled, double* vt, double* x, Scalars* sc, Reducer red) {
+    __shared__ double sh[32];
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double inv_b1 = sc->inv_beta;
+    double part = 0.0;
+    if (i < n) {
+        double v = -(b_scaled[i] * inv_b1);
+        vt[i] = v;
+        x[i] = 0.0;
+        part = v * v;
+    }
+    double tot;
+    if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) {
+        double alpha = sqrt(tot);
+        sc->alpha = alpha;
+        sc->Anorm2 = tot;
+        sc->inv_alpha = alpha != 0.0 ? 1.0 / alpha : 0.0;
+        sc->ArNorm0 = alpha * sc->beta1;
+        sc->rhobar = alpha;
+        sc->phibar = sc->beta1;
+        if (alpha == 0.0) {
+            sc->stopped = 1;
+            sc->status = 4;
+        } else {
+            double Anorm = alpha, rNorm = sc->beta1;
+            double t = sc->ArNorm0 / (Anorm * rNorm);
+            if (t <= 1.4901161193847656e-08 || 1.0 + t <= 1.0) {
+                sc->stopped = 1;
+                sc->status = 1;
+            }
+        }
+    }
+}
+
+__global__ void k_lsqr_w0(int64_t n, const double* vt, double* wl, Scalars* sc, Reducer red) {
+    __shared__ double sh[32];
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double ia = sc->inv_alpha;
+    double part = 0.0;
+    if (i < n) {
+        double v = vt[i] * ia;
+        wl[i] = v;
+        part = v * v;
+    }
+    double tot;
+    if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) sc->wnorm2 = tot;
+}
+
+// QR continuation, x / w update and stopping tests (Krylov lsqr main loop
+// after the Golub-Kahan step).  Every thread evaluates the same scalar
+// recurrence from the state; the last block commits it.
+__global__ void k_lsqr_update(int64_t n, const double* vt, double* x, double* wl, Scalars* sc, Reducer red) {
+    __shared__ double sh[32];
+    if (sc->stopped) return;
+    const double alpha = sc->alpha, beta = sc->beta, lambda = sc->lambda;
+    double c1, s1, rhobar1;
+    sym_givens(sc->rhobar, lambda, c1, s1, rhobar1);
+    double phibar = sc->phibar;
+    const double psi = s1 * phibar;
+    phibar = c1 * phibar;
+    double c, s, rho;
+    sym_givens(rhobar1, beta, c, s, rho);
+    const double phi = c * phibar;
+    phibar = s * phibar;
+    const double theta = s * alpha;
+    const double sigma = phi / rho, tr = -theta / rho;
+    const double ia = sc->inv_alpha;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double part = 0.0;
+    if (i < n) {
+        double wi = wl[i];
+        x[i] = x[i] + sigma * wi;
+        double wn = vt[i] * ia + tr * wi;
+        wl[i] = wn;
+        part = wn * wn;
+    }
+    double tot;
+    if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) {
+        const double axtol = 1.4901161193847656e-08, etol = axtol, ctol = axtol;
+        int iter = sc->iter + 1;
+        double xENorm2 = sc->xENorm2 + phi * phi;
+        sc->err_vec[iter % 5] = phi;
+        double err_lbnd = 0;
+        if (iter >= 5) {
+            double e2 = 0;
+            for (int k = 0; k < 5; ++k) e2 += sc->err_vec[k] * sc->err_vec[k];
+            err_lbnd = sqrt(e2);
+        }
+        const double tau = s * phi;
+        double dNorm2 = sc->dNorm2 + sc->wnorm2 / (rho * rho);
+        double delta = sc->s2 * rho;
+        double gambar = -sc->c2 * rho;
+        double rhs = phi - delta * sc->z;
+        double zbar = rhs / gambar;
+        double xNorm = sqrt(sc->xNorm2 + zbar * zbar);
+        double c2, s2, gamma;
+        sym_givens(gambar, theta, c2, s2, gamma);
+        double z = rhs / gamma;
+        double xNorm2 = sc->xNorm2 + z * z;
+        double Anorm = sqrt(sc->Anorm2);
+        double Acond = Anorm * sqrt(dNorm2);
+        double res1 = phibar * phibar;
+        double res2 = sc->res2 + psi * psi;
+        double rNorm = sqrt(res1 + res2);
+        double ArNorm = alpha * fabs(tau);
+        double test1 = rNorm / sc->beta1;
+        double test2 = ArNorm / (Anorm * rNorm);
+        double test3 = 1.0 / Acond;
+        double t1 = test1 / (1.0 + Anorm * xNorm / sc->beta1);
+        double rNormtol = sc->btol + axtol * Anorm * xNorm / sc->beta1;
+        bool ill = (1.0 + test3 <= 1.0) || (test3 <= ctol);
+        bool zr = (1.0 + t1 <= 1.0) || (test1 <= rNormtol);
+        bool fwd = iter >= 5 && err_lbnd <= etol * sqrt(xENorm2);
+        bool solved = (1.0 + test2 <= 1.0) || (test2 <= axtol) || (ArNorm <= sc->atol) || zr || fwd;
+        bool tired = iter >= sc->itmax;
+        sc->rhobar = -c * alpha;
+        sc->phibar = phibar;
+        sc->xENorm2 = xENorm2;
+        sc->dNorm2 = dNorm2;
+        sc->xNorm = xNorm;
+        sc->xNorm2 = xNorm2;
+        sc->c2 = c2;
+        sc->s2 = s2;
+        sc->z = z;
+        sc->res2 = res2;
+        sc->wnorm2 = tot;
+        sc->iter = iter;
+        if (solved || tired || ill) {
+            sc->stopped = 1;
+            sc->status = solved ? (zr ? 2 : 1) : (ill ? 3 : 0);
+        }
+    }
+}
+
+// delta = x / colnorm, position step cap (_cap_position_step!, :700-716),
+// delta_scaled = colnorm * delta.
+__global__ void k_step(int64_t n_act, FitConst fc, double max_step, const double* x, const double* cn, double* delta,
+                       double* dsc) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    const int p = fc.p;
+    double d[3];
+    for (int k = 0; k < p; ++k) d[k] = x[j * p + k] / cn[j * p + k];
+    if (fc.ky >= 0 || fc.kx >= 0) {
+        double dy = fc.ky < 0 ? 0.0 : d[fc.ky];
+        double dx = fc.kx < 0 ? 0.0 : d[fc.kx];
+        double len = sqrt(dy * dy + dx * dx);
+        if (len > max_step) {
+            double scl = max_step / len;
+            if (fc.ky >= 0) d[fc.ky] *= scl;
+            if (fc.kx >= 0) d[fc.kx] *= scl;
+        }
+    }
+    for (int k = 0; k < p; ++k) {
+        delta[j * p + k] = d[k];
+        dsc[j * p + k] = cn[j * p + k] * d[k];
+    }
+}
+
+// global gradient cosine (:1199-1213), max over all parameters
+__global__ void k_gnorm(int64_t n, const double* cn, const double* b, double dof, Scalars* sc, Reducer red) {
+    __shared__ double sh[32];
+    const double C_r = sc->cost / dof;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double g = 0.0;
+    if (i < n) {
+        double bt = cn[i] * b[i];
+        double Aii = cn[i] * cn[i];
+        g = fabs(bt) / (sqrt(Aii * C_r) + kEps64);
+    }
+    double tot;
+    if (grid_reduce<256, true>(g, red, sh, &tot) && threadIdx.x == 0) sc->gnorm = tot;
+}
+
+// Accepted step (:1245-1251) and per-star freeze tests (:1265-1283,
+// _x_tol_local :810-823, _g_tol_local :789-801).
+__global__ void k_accept_freeze(int64_t n_act, FitConst fc, double x_tol, double g_tol, double dof, int iter,
+                                double* theta, const double* delta, const double* dsc, const double* cn, double* D,
+                                const double* b, uint8_t* live, uint8_t* newf, int32_t* frozen_at, uint8_t* conv,
+                                Scalars* sc) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    const int p = fc.p;
+    for (int k = 0; k < p; ++k) {
+        int64_t i = j * p + k;
+        theta[i] = theta[i] + delta[i];
+        D[i] = fmax(D[i], cn[i]);
+    }
+    newf[j] = 0;
+    if (!live[j]) return;
+    const double C_r = sc->cost / dof;
+    double num = 0, xn = 0, gn = 0;
+    for (int k = 0; k < p; ++k) {
+        int64_t i = j * p + k;
+        double v = (D[i] / cn[i]) * dsc[i];
+        num += v * v;
+        double xv = D[i] * theta[i];
+        xn += xv * xv;
+        double bt = cn[i] * b[i];
+        double Aii = cn[i] * cn[i];
+        gn = nan_max(gn, fabs(bt) / (sqrt(Aii * C_r) + kEps64));
+    }
+    bool xt = sqrt(num) <= x_tol * (sqrt(xn) + x_tol);
+    bool gt = gn <= g_tol;
+    if (xt || gt) {
+        live[j] = 0;
+        newf[j] = 1;
+        frozen_at[j] = iter;
+        conv[j] = 1;
+        atomicAdd(&sc->n_new_frozen, 1);
+    }
+}
+
+__global__ void k_freeze_all(int64_t n_act, int iter, uint8_t* live, int32_t* frozen_at, uint8_t* conv) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act || !live[j]) return;
+    live[j] = 0;
+    frozen_at[j] = iter;
+    conv[j] = 1;
+}
+
+__global__ void k_zero_nonlive(int64_t n_act, int p, const uint8_t* live, double* v) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act || live[j]) return;
+    for (int k = 0; k < p; ++k) v[j * p + k] = 0.0;
+}
+
+// Per-star p x p covariance from the Gram block (:1305-1329,
+// levenberg_marquardt.jl:366-388): ridge 1e-12 tr, Cholesky inverse,
+// Jacobi pseudo-inverse fallback, reweighted scaling by cost/dof.
+__device__ void pinv_small(double* A, int n, double* inv) {
+    double V[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    for (int i = 0; i < n; ++i)
+        for (int j = i + 1; j < n; ++j) {
+            double s = 0.5 * (A[i + j * n] + A[j + i * n]);
+            A[i + j * n] = A[j + i * n] = s;
+        }
+    for (int i = 0; i < 9; ++i) V[i] = 0;
+    for (int i = 0; i < n; ++i) V[i + i * n] = 1;
+    for (int sweep = 0; sweep < 60; ++sweep) {
+        double off = 0;
+        for (int i = 0; i < n; ++i)
+            for (int j = i + 1; j < n; ++j) off += A[i + j * n] * A[i + j * n];
+        if (off < 1e-300) break;
+        for (int pp = 0; pp < n; ++pp)
+            for (int q = pp + 1; q < n; ++q) {
+                double apq = A[pp + q * n];
+                if (apq == 0) continue;
+                double tau = (A[q + q * n] - A[pp + pp * n]) / (2 * apq);
+                double t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1 + tau * tau));
+                double c = 1 / sqrt(1 + t * t), s = t * c;
+                for (int k = 0; k < n; ++k) {
+                    double akp = A[k + pp * n], akq = A[k + q * n];
+                    A[k + pp * n] = c * akp - s * akq;
+                    A[k + q * n] = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double apk = A[pp + k * n], aqk = A[q + k * n];
+                    A[pp + k * n] = c * apk - s * aqk;
+                    A[q + k * n] = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {
+                    double vkp = V[k + pp * n], vkq = V[k + q * n];
+                    V[k + pp * n] = c * vkp - s * vkq;
+                    V[k + q * n] = s * vkp + c * vkq;
+                }
+            }
+    }
+    double smax = 0;
+    for (int i = 0; i < n; ++i) smax = fmax(smax, fabs(A[i + i * n]));
+    double tol = kEps64 * n * smax;
+    for (int i = 0; i < n * n; ++i) inv[i] = 0;
+    for (int e = 0; e < n; ++e) {
+        double lam = A[e + e * n];
+        if (!(fabs(lam) > tol)) continue;
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) inv[i + j * n] += V[i + e * n] * V[j + e * n] / lam;
+    }
+}
+
+__device__ bool chol_inv_small(const double* A, int n, double* inv) {
+    double U[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) {
+            double s = A[i + j * n];
+            for (int k = 0; k < i; ++k) s -= U[k + i * n] * U[k + j * n];
+            if (i == j) {
+                if (!(s > 0)) return false;
+                U[j + j * n] = sqrt(s);
+            } else {
+                U[i + j * n] = s / U[i + i * n];
+            }
+        }
+    for (int c = 0; c < n; ++c) {
+        double y[3], xx[3];
+        for (int i = 0; i < n; ++i) {
+            double s = (i == c) ? 1.0 : 0.0;
+            for (int k = 0; k < i; ++k) s -= U[k + i * n] * y[k];
+            y[i] = s / U[i + i * n];
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double s = y[i];
+            for (int k = i + 1; k < n; ++k) s -= U[i + k * n] * xx[k];
+            xx[i] = s / U[i + i * n];
+        }
+        for (int i = 0; i < n; ++i) inv[i + c * n] = xx[i];
+    }
+    return true;
+}
+
+__global__ void k_errors(int64_t n_act, int p, const double* gram, bool reweighted, double dof, const Scalars* sc,
+                         double* err) {
+    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (j >= n_act) return;
+    double A[9], inv[9];
+    int t = 0;
+    for (int k = 0; k < p; ++k)
+        for (int l = k; l < p; ++l) {
+            double v = gram[j * 6 + t++];
+            A[k + l * p] = v;
+            A[l + k * p] = v;
+        }
+    double tr = 0;
+    for (int k = 0; k < p; ++k) tr += A[k + k * p];
+    for (int k = 0; k < p; ++k) A[k + k * p] += 1.0e-12 * tr;
+    if (!chol_inv_small(A, p, inv)) pinv_small(A, p, inv);
+    double f = reweighted ? sc->cost / dof : 1.0;
+    for (int k = 0; k < p; ++k) err[j * p + k] = sqrt(fmax(0.0, inv[k + k * p] * f));
+}
+
+// chisq and the qfit / crowding diagnostics per active star (:1358-1397,
+// psf_photometry_diagnostics.jl:154-231); one warp per star.
+template <typename TI>
+__global__ void k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad, const StarCoef* __restrict__ coef,
+                       const double* __restrict__ resid, const TI* __restrict__ img, const TI* __restrict__ bkgimg,
+                       const TI* __restrict__ iv, double* out /* n_act x 5: chisq qfit qfit_exp qfit_z crowding */) {
+    const int lane = threadIdx.x & 31;
+    const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (j >= n_act) return;
+    const StarCoef c = coef[j];
+    const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+    double* o = out + j * 5;
+    const bool validp = isfinite(c.y) && isfinite(c.x) && isfinite(c.flux) && c.flux > 0;
+    if (!validp) {
+        if (lane == 0) {
+            o[0] = 0.0;
+            o[1] = o[2] = o[3] = o[4] = NaN;
+        }
+        return;
+    }
+    int ylo = max((int)floor(c.y - fit_rad), 1), yhi = min((int)ceil(c.y + fit_rad), fc.ny);
+    int xlo = max((int)floor(c.x - fit_rad), 1), xhi = min((int)ceil(c.x + fit_rad), fc.nx);
+    double num = 0, qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
+    int ng = 0, ngi = 0;
+    const int h = yhi - ylo + 1, wd = xhi - xlo + 1;
+    const double inv_flux = 1.0 / c.flux;
+    if (h > 0 && wd > 0) {
+        for (int e = lane; e < h * wd; e += 32) {
+            const int gy = ylo + e % h, gx = xlo + e / h;
+            const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
+            const double r = resid[q];
+            const double wp = iv ? (double)iv[q] : 1.0;
+            if (isfinite(wp) && wp > 0) {
+                num += wp * (r * r);
+                ng += 1;
+                double mv = model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
+                qv += fabs(r);
+                double Pp = (mv - c.bkg) * inv_flux;
+                double wP = wp * Pp;
+                ncl += wP * (r + mv - c.bkg);
+                double im = (double)img[q] - (bkgimg ? (double)bkgimg[q] : 0.0);
+                ndi += wP * (im - c.bkg);
+                den += wP * Pp;
+                if (iv) {
+                    double si = 1.0 / sqrt(wp);
+                    ss += si;
+                    ss2 += si * si;
+                    ngi += 1;
+                }
+            }
+        }
+    }
+    num = warp_sum(num);
+    qv = warp_sum(qv);
+    ncl = warp_sum(ncl);
+    ndi = warp_sum(ndi);
+    den = warp_sum(den);
+    ss = warp_sum(ss);
+    ss2 = warp_sum(ss2);
+    ng = warp_sum(ng);
+    ngi = warp_sum(ngi);
+    if (lane == 0) {
+        o[0] = (ng - fc.p > 0) ? num / (double)(ng - fc.p) : 0.0;
+        o[1] = qv * inv_flux;
+        o[4] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
+        if (iv) {
+            o[2] = sqrt(2.0 / 3.141592653589793) * ss * inv_flux;
+            if (ss2 > 0 && ngi > fc.p) {
+                double dfac = sqrt(1.0 - (double)fc.p / (double)ngi);
+                o[3] = (qv - sqrt(2.0 / 3.141592653589793) * dfac * ss) /
+                       (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
+            } else {
+                o[3] = NaN;
+            }
+        } else {
+            o[2] = o[3] = NaN;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+template <typename T>
+T* S(cpb_ctx* ctx, const char* name, size_t count) {
+    return (T*)scratch(ctx, name, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+struct TileLists {
+    int32_t *start = nullptr, *end = nullptr, *list = nullptr;
+};
+
+TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_t* ay, const int32_t* ax,
+                      const int32_t* Rs, int Rconst, int ny, int nx, int nty, int ntx) {
+    cudaStream_t st = ctx->stream;
+    std::string t(tag);
+    int32_t* cnt = S<int32_t>(ctx, (t + "_cnt").c_str(), n_act + 1);
+    int32_t* offs = S<int32_t>(ctx, (t + "_offs").c_str(), n_act + 1);
+    k_tile_count<<<nblk(n_act), 256, 0, st>>>(n_act, ay, ax, Rs, Rconst, ny, nx, cnt);
+    check(cudaGetLastError(), "k_tile_count");
+    check(cudaMemsetAsync(cnt + n_act, 0, sizeof(int32_t), st), "memset");
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, cnt, offs, (int)(n_act + 1), st);
+    void* dtmp = scratch(ctx, (t + "_scan_tmp").c_str(), tmp);
+    cub::DeviceScan::ExclusiveSum(dtmp, tmp, cnt, offs, (int)(n_act + 1), st);
+    int32_t npairs = 0;
+    check(cudaMemcpyAsync(&npairs, offs + n_act, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h npairs");
+    check(cudaStreamSynchronize(st), "sync");
+    uint32_t* k0 = S<uint32_t>(ctx, (t + "_k0").c_str(), npairs);
+    uint32_t* k1 = S<uint32_t>(ctx, (t + "_k1").c_str(), npairs);
+    int32_t* v0 = S<int32_t>(ctx, (t + "_v0").c_str(), npairs);
+    TileLists tl;
+    tl.list = S<int32_t>(ctx, (t + "_list").c_str(), npairs);
+    const int64_t ntiles = (int64_t)nty * ntx;
+    tl.start = S<int32_t>(ctx, (t + "_start").c_str(), ntiles);
+    tl.end = S<int32_t>(ctx, (t + "_end").c_str(), ntiles);
+    check(cudaMemsetAsync(tl.start, 0, sizeof(int32_t) * ntiles, st), "memset");
+    check(cudaMemsetAsync(tl.end, 0, sizeof(int32_t) * ntiles, st), "memset");
+    if (npairs > 0) {
+        k_tile_emit<<<nblk(n_act), 256, 0, st>>>(n_act, ay, ax, Rs, Rconst, ny, nx, nty, offs, k0, v0);
+        check(cudaGetLastError(), "k_tile_emit");
+        int end_bit = 1;
+        while ((1LL << end_bit) < ntiles) ++end_bit;
+        tmp = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, v0, tl.list, npairs, 0, end_bit, st);
+        dtmp = scratch(ctx, (t + "_sort_tmp").c_str(), tmp);
+        cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, tl.list, npairs, 0, end_bit, st);
+        k_tile_bounds<<<nblk(npairs), 256, 0, st>>>(npairs, k1, tl.start, tl.end);
+        check(cudaGetLastError(), "k_tile_bounds");
+    }
+    return tl;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// driver
+// ---------------------------------------------------------------------------
+int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
+                         int32_t eltype, int64_t ny64, int64_t nx64, const void* d_inv_var, const void* d_background,
+                         int64_t n_stars, const double* d_y0, const double* d_x0, const double* d_flux0,
+                         cpb_sim_result* out) {
+    cudaStream_t st = ctx->stream;
+    const double NaN = std::numeric_limits<double>::quiet_NaN();
+    // argument checks in the reference's order (:984-997)
+    if (!(P->max_iter > 0)) throw ArgError{"max_iter must be positive"};
+    if (!(P->inner_iterations > 0)) throw ArgError{"inner_iterations must be positive"};
+    if (!(P->linear_tol > 0)) throw ArgError{"linear_tol must be positive"};
+    if (!(P->max_trials > 0)) throw ArgError{"max_trials must be positive"};
+    if (!P->model_rad_auto && !(P->model_rad > 0)) throw ArgError{"model_rad must be :auto or a positive real"};
+    const double model_rad_max = P->model_rad_max < 0 ? 10 * P->fit_rad : P->model_rad_max;
+    if (!(model_rad_max >= P->fit_rad)) throw ArgError{"model_rad_max must be >= fit_rad"};
+    if (!(P->model_rad_nsigma > 0)) throw ArgError{"model_rad_nsigma must be positive"};
+    if (P->solver != CPB_SOLVER_LSQR && P->solver != CPB_SOLVER_LSMR) throw ArgError{"solver must be :lsqr or :lsmr"};
+    if (P->solver == CPB_SOLVER_LSMR) throw ArgError{"solver :lsmr is not supported by the B200 path; use :lsqr"};
+    if (P->damping == CPB_DAMP_LEVENBERG)
+        throw ArgError{
+            "LevenbergDamping is not supported by fit_all_stars_simultaneous: it conflicts with the "
+            "column-equilibrated x_tol scaling. Use MarquardtDamping."};
+    if (!(P->fit_rad > 0)) throw ArgError{"fit_rad must be positive"};
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
+    if (ny64 <= 0 || nx64 <= 0 || ny64 * nx64 >= (1LL << 31)) throw ArgError{"image size out of range"};
+    if (P->precision != CPB_PREC_FP64) throw ArgError{"only the FP64 precision form is built for the simultaneous fit"};
+    const int ny = (int)ny64, nx = (int)nx64;
+    const int64_t npix = ny64 * nx64;
+    const bool reweighted =
+        P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && d_inv_var == nullptr);
+    out->n_active = 0;
+    out->n_union = 0;
+    out->n_trials = 0;
+    out->n_lsqr_iters = 0;
+    out->model_px_evals = 0;
+    out->lsqr_px_macs = 0;
+    out->device_seconds = 0;
+    auto nan_diag = [&](int64_t i) {
+        if (out->qfit) out->qfit[i] = NaN;
+        if (out->qfit_expected) out->qfit_expected[i] = NaN;
+        if (out->qfit_z) out->qfit_z[i] = NaN;
+        if (out->crowding) out->crowding[i] = NaN;
+    };
+    if (n_stars == 0) {
+        out->n_passes = 0;
+        out->n_failed = 0;
+        if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
+        return 0;
+    }
+    // free set (:1015-1051)
+    FitConst fc{};
+    fc.p = 0;
+    if (P->free_mask & CPB_FREE_Y) fc.gc[fc.p++] = 1;
+    if (P->free_mask & CPB_FREE_X) fc.gc[fc.p++] = 2;
+    if (P->free_mask & CPB_FREE_FLUX) fc.gc[fc.p++] = 3;
+    if (P->free_mask & ~(CPB_FREE_Y | CPB_FREE_X | CPB_FREE_FLUX))
+        throw ArgError{
+            "fit_all_stars_simultaneous fits only (y, x, flux) per star. Fix `bkg` (subtract the background first "
+            "and pass `fixed = (; bkg = zero(eltype(image)))`), and fix all shape parameters."};
+    if (fc.p == 0) throw ArgError{"all model parameters are fixed; nothing to fit"};
+    const int p = fc.p;
+    fc.ky = fc.kx = -1;
+    for (int k = 0; k < p; ++k) {
+        if (fc.gc[k] == 1) fc.ky = k;
+        if (fc.gc[k] == 2) fc.kx = k;
+    }
+    for (int k = p; k < 3; ++k) fc.gc[k] = 3;
+    fc.fixed_y = P->fixed_y;
+    fc.fixed_x = P->fixed_x;
+    fc.fixed_flux = P->fixed_flux;
+    fc.fixed_bkg = P->fixed_bkg;
+    fc.R = (int)std::ceil(P->fit_rad);
+    fc.S = 2 * fc.R + 1;
+    fc.S2 = fc.S * fc.S;
+    fc.VS = ((p * fc.S2 + 15) / 16) * 16;
+    fc.ny = ny;
+    fc.nx = nx;
+    fc.nty = (ny + TY - 1) / TY;
+    fc.ntx = (nx + TX - 1) / TX;
+    const int64_t ntiles = (int64_t)fc.nty * fc.ntx;
+    DevPsf dp = psf->dev;
+    dp.fwhm = P->fixed_fwhm;
+
+    check(cudaEventRecord(ctx->ev0, st), "event");
+    // device-resident scalars and reducers
+    Scalars* sc = S<Scalars>(ctx, "scalars", 1);
+    check(cudaMemsetAsync(sc, 0, sizeof(Scalars), st), "memset");
+    const int64_t max_blocks = std::max<int64_t>(ntiles, nblk(std::max<int64_t>(n_stars * 3, npix)) + 1);
+    Reducer red{S<double>(ctx, "red_partials", max_blocks), S<unsigned>(ctx, "red_counter", 1)};
+    check(cudaMemsetAsync(red.counter, 0, sizeof(unsigned), st), "memset");
+    Scalars* h_sc = (Scalars*)ctx->pinned;
+
+    // ---- data and weights (:1056-1084)
+    double* data = S<double>(ctx, "data", npix);
+    double* data_work = S<double>(ctx, "data_work", npix);
+    double* w = S<double>(ctx, "w", npix);
+    double* sw = S<double>(ctx, "sw", npix);
+    unsigned* flags = S<unsigned>(ctx, "flags", 4);
+    check(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned), st), "memset");
+    if (eltype == CPB_F64)
+        k_prepare<double><<<nblk(npix), 256, 0, st>>>((const double*)d_image, (const double*)d_inv_var,
+                                                      (const double*)d_background, npix, data, data_work, w, sw,
+                                                      flags);
+    else
+        k_prepare<float><<<nblk(npix), 256, 0, st>>>((const float*)d_image, (const float*)d_inv_var,
+                                                     (const float*)d_background, npix, data, data_work, w, sw, flags);
+    check(cudaGetLastError(), "k_prepare");
+
+    // ---- _build_stamps! (:245-323)
+    int32_t* ay_c = S<int32_t>(ctx, "ay_c", n_stars);
+    int32_t* ax_c = S<int32_t>(ctx, "ax_c", n_stars);
+    uint8_t* ok = S<uint8_t>(ctx, "ok", n_stars);
+    uint64_t* key = S<uint64_t>(ctx, "key", n_stars);
+    k_anchor<<<nblk(n_stars), 256, 0, st>>>(n_stars, d_y0, d_x0, d_flux0, fc.R, ny, nx, w, ay_c, ax_c, ok, key,
+                                            flags + 1);
+    check(cudaGetLastError(), "k_anchor");
+    // compact active stars in catalogue order, then stable radix sort by Morton key
+    int32_t* iota = S<int32_t>(ctx, "iota", n_stars);
+    int32_t* sel = S<int32_t>(ctx, "sel", n_stars);
+    uint64_t* selkey = S<uint64_t>(ctx, "selkey", n_stars);
+    uint64_t* selkey2 = S<uint64_t>(ctx, "selkey2", n_stars);
+    int32_t* act = S<int32_t>(ctx, "act", n_stars);
+    int* d_nsel = S<int>(ctx, "nsel", 1);
+    {
+        std::vector<int32_t> h_iota(n_stars);
+        for (int64_t i = 0; i < n_stars; ++i) h_iota[i] = (int32_t)i;
+        check(cudaMemcpyAsync(iota, h_iota.data(), sizeof(int32_t) * n_stars, cudaMemcpyHostToDevice, st), "h2d");
+        size_t tmp = 0;
+        cub::DeviceSelect::Flagged(nullptr, tmp, iota, ok, sel, d_nsel, (int)n_stars, st);
+        void* dtmp = scratch(ctx, "sel_tmp", tmp);
+        cub::DeviceSelect::Flagged(dtmp, tmp, iota, ok, sel, d_nsel, (int)n_stars, st);
+        tmp = 0;
+        cub::DeviceSelect::Flagged(nullptr, tmp, key, ok, selkey, d_nsel, (int)n_stars, st);
+        dtmp = scratch(ctx, "sel_tmp2", tmp);
+        cub::DeviceSelect::Flagged(dtmp, tmp, key, ok, selkey, d_nsel, (int)n_stars, st);
+        check(cudaGetLastError(), "select");
+    }
+    int h_nsel = 0;
+    unsigned h_flags[4];
+    check(cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    if (!d_inv_var && h_flags[0] > 0)
+        throw ArgError{
+            "the image contains non-finite values but `inv_var` was not provided; pass `inv_var` to mask them or "
+            "clean the image first"};
+    const int64_t n_act = h_nsel;
+    const int n_failed = (int)(n_stars - n_act);
+    out->n_active = n_act;
+    if (n_act == 0) {  // _empty_simultaneous_result (:1433-1445)
+        std::vector<double> y(n_stars), x(n_stars), f(n_stars);
+        check(cudaMemcpy(y.data(), d_y0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
+        check(cudaMemcpy(x.data(), d_x0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
+        check(cudaMemcpy(f.data(), d_flux0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
+        for (int64_t i = 0; i < n_stars; ++i) {
+            out->y[i] = y[i];
+            out->x[i] = x[i];
+            out->flux[i] = f[i];
+            out->bkg[i] = 0.0;
+            out->y_err[i] = (P->free_mask & CPB_FREE_Y) ? NaN : 0.0;
+            out->x_err[i] = (P->free_mask & CPB_FREE_X) ? NaN : 0.0;
+            out->flux_err[i] = (P->free_mask & CPB_FREE_FLUX) ? NaN : 0.0;
+            out->bkg_err[i] = 0.0;
+            out->converged[i] = 0;
+            out->valid[i] = 0;
+            if (out->chisq) out->chisq[i] = 0.0;
+            nan_diag(i);
+            out->n_iter[i] = 0;
+        }
+        out->n_passes = 0;
+        out->n_failed = (int32_t)n_stars;
+        if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
+        return 0;
+    }
+    if (h_flags[1] > 0)
+        throw ArgError{"InexactError: a star's integer anchor is negative (Morton key of a negative coordinate)"};
+    {
+        size_t tmp = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, selkey, selkey2, sel, act, (int)n_act, 0, 64, st);
+        void* dtmp = scratch(ctx, "sort_tmp", tmp);
+        cub::DeviceRadixSort::SortPairs(dtmp, tmp, selkey, selkey2, sel, act, (int)n_act, 0, 64, st);
+        check(cudaGetLastError(), "sort");
+    }
+    const int64_t n = (int64_t)p * n_act;
+    int32_t* ay = S<int32_t>(ctx, "ay", n_act);
+    int32_t* ax = S<int32_t>(ctx, "ax", n_act);
+    double* theta = S<double>(ctx, "theta", n);
+    k_gather_active<<<nblk(n_act), 256, 0, st>>>(n_act, act, ay_c, ax_c, d_y0, d_x0, d_flux0, p,
+                                                 make_int3(fc.gc[0], fc.gc[1], fc.gc[2]), ay, ax, theta);
+    check(cudaGetLastError(), "k_gather_active");
+
+    // ---- union of stamp pixels (:329-335)
+    uint8_t* umask = S<uint8_t>(ctx, "umask", npix);
+    check(cudaMemsetAsync(umask, 0, npix, st), "memset");
+    int32_t* dbg_pix = out->dbg_pixels ? S<int32_t>(ctx, "dbg_pix", (int64_t)fc.S2 * n_act) : nullptr;
+    k_union<<<(unsigned)n_act, 256, 0, st>>>(n_act, ay, ax, fc.R, ny, nx, w, umask, dbg_pix);
+    check(cudaGetLastError(), "k_union");
+    unsigned long long* ucnt = S<unsigned long long>(ctx, "ucnt", 1);
+    check(cudaMemsetAsync(ucnt, 0, sizeof(unsigned long long), st), "memset");
+    k_count_u8<<<nblk(npix), 256, 0, st>>>(umask, npix, ucnt);
+    unsigned long long h_ucnt = 0;
+    check(cudaMemcpyAsync(&h_ucnt, ucnt, sizeof(h_ucnt), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    out->n_union = (int64_t)h_ucnt;
+
+    // ---- model radii (:1111-1124); scalar model_rad only on the device path
+    if (P->model_rad_auto && !d_inv_var)
+        throw ArgError{
+            "model_rad=:auto requires inv_var (it needs a noise scale); pass inv_var or an explicit scalar model_rad"};
+    if (P->model_rad_auto) throw ArgError{"model_rad=:auto is not supported by the B200 path; pass a scalar model_rad"};
+    int model_R;
+    {
+        const int R_cap = (int)std::ceil(std::max(P->model_rad, P->fit_rad));
+        model_R = std::min(std::max((int)std::ceil(P->model_rad), fc.R), R_cap);
+    }
+    const double dof = (double)std::max<int64_t>((int64_t)h_ucnt - n, 1);
+
+    // ---- tile lists (fit box for J v; model box for renders)
+    TileLists tfit = build_tiles(ctx, "tfit", n_act, ay, ax, nullptr, fc.R, ny, nx, fc.nty, fc.ntx);
+    TileLists tmod = model_R == fc.R ? tfit
+                                     : build_tiles(ctx, "tmod", n_act, ay, ax, nullptr, model_R, ny, nx, fc.nty, fc.ntx);
+
+    // ---- working buffers (:1129-1166)
+    double* V = S<double>(ctx, "V", (int64_t)fc.VS * n_act);
+    double* cn = S<double>(ctx, "colnorm", n);
+    double* D = S<double>(ctx, "D", n);
+    double* bsc = S<double>(ctx, "b_scaled", n);
+    double* delta = S<double>(ctx, "delta", n);
+    double* dsc = S<double>(ctx, "delta_scaled", n);
+    double* xl = S<double>(ctx, "lsqr_x", n);
+    double* vt = S<double>(ctx, "lsqr_v", n);
+    double* wl = S<double>(ctx, "lsqr_w", n);
+    double* wt_resid = S<double>(ctx, "wt_resid", npix);
+    double* u = S<double>(ctx, "lsqr_u", npix);
+    StarCoef* coef = S<StarCoef>(ctx, "coef", n_act);
+    StarCoef* coefc = S<StarCoef>(ctx, "coef_cand", n_act);
+    uint8_t* live = S<uint8_t>(ctx, "live", n_act);
+    uint8_t* newf = S<uint8_t>(ctx, "newf", n_act);
+    uint8_t* conv = S<uint8_t>(ctx, "conv", n_act);
+    int32_t* frozen_at = S<int32_t>(ctx, "frozen_at", n_act);
+    int32_t* live_list = S<int32_t>(ctx, "live_list", n_act);
+    int32_t* iota_act = S<int32_t>(ctx, "iota_act", n_act);
+    int* d_nlive = S<int>(ctx, "nlive", 1);
+    check(cudaMemsetAsync(live, 1, n_act, st), "memset");
+    check(cudaMemsetAsync(conv, 0, n_act, st), "memset");
+    check(cudaMemsetAsync(frozen_at, 0, sizeof(int32_t) * n_act, st), "memset");
+    check(cudaMemsetAsync(cn, 0, sizeof(double) * n, st), "memset");
+    check(cudaMemsetAsync(V, 0, sizeof(double) * (int64_t)fc.VS * n_act, st), "memset");
+    check(cudaMemcpyAsync(iota_act, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
+    int64_t n_live = n_act;
+    check(cudaMemcpyAsync(live_list, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
+    size_t live_tmp_bytes = 0;
+    cub::DeviceSelect::Flagged(nullptr, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
+    void* live_tmp = scratch(ctx, "live_tmp", live_tmp_bytes);
+
+    const int fill_blocks = (int)std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16);
+    auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
+        if (nlist <= 0) return;
+        unsigned gb = (unsigned)std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16);
+        if (fc.S2 <= 256 * 2)
+            k_fill<256, 2><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+        else if (fc.S2 <= 256 * 4)
+            k_fill<256, 4><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+        else if (fc.S2 <= 256 * 8)
+            k_fill<256, 8><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+        else
+            throw ArgError{"fit_rad too large for the B200 stamp kernel (ceil(fit_rad) must be <= 22)"};
+        check(cudaGetLastError(), "k_fill");
+    };
+    (void)fill_blocks;
+    auto launch_render = [&](int mode, const uint8_t* incl, const StarCoef* cf, double* outp, const double* ref,
+                             double* result) {
+        switch (mode) {
+            case MODE_CUR:
+                k_render<MODE_CUR><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
+                                                                    nullptr, model_R, incl, cf, umask, w, sw, ref,
+                                                                    outp, red, result);
+                break;
+            case MODE_CAND:
+                k_render<MODE_CAND><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
+                                                                     nullptr, model_R, incl, cf, umask, w, sw, ref,
+                                                                     outp, red, result);
+                break;
+            case MODE_FREEZE:
+                k_render<MODE_FREEZE><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay,
+                                                                       ax, nullptr, model_R, incl, cf, umask, w, sw,
+                                                                       ref, outp, red, result);
+                break;
+            default:
+                k_render<MODE_FINAL><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
+                                                                      nullptr, model_R, incl, cf, umask, w, sw, ref,
+                                                                      outp, red, result);
+        }
+        check(cudaGetLastError(), "k_render");
+    };
+    auto update_live_list = [&]() {
+        cub::DeviceSelect::Flagged(live_tmp, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
+        int h = 0;
+        check(cudaMemcpyAsync(&h, d_nlive, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaStreamSynchronize(st), "sync");
+        n_live = h;
+    };
+    const unsigned jt_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
+    auto read_scalars = [&]() {
+        check(cudaMemcpyAsync(h_sc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaStreamSynchronize(st), "sync");
+    };
+    double evals = 0.0, macs = 0.0;
+
+    // ---- initial fill and cost (:1171-1178)
+    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+    launch_fill(live_list, n_live, nullptr);
+    launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
+    check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
+    evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
+    bool fresh = true;  // V / wt_resid / cost are at the current theta and live set
+    double lam = P->lambda_init;
+    int n_run = 0;
+    int64_t n_trials = 0, n_lsqr = 0;
+
+    // ---- outer loop (:1186-1284)
+    for (int iter = 1; iter <= P->max_iter; ++iter) {
+        if (!fresh) {
+            k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+            launch_fill(live_list, n_live, nullptr);
+            launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
+            evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
+        }
+        fresh = false;
+        // b_scaled = J' wt_resid (frozen stars stay 0)
+        check(cudaMemsetAsync(bsc, 0, sizeof(double) * n, st), "memset");
+        k_JT<false><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
+        check(cudaGetLastError(), "k_JT");
+        macs += (double)n_live * fc.S2;
+        k_gnorm<<<nblk(n), 256, 0, st>>>(n, cn, bsc, dof, sc, red);
+        check(cudaGetLastError(), "k_gnorm");
+        read_scalars();
+        const double cost = h_sc->cost;
+        if (h_sc->gnorm <= P->g_tol) {
+            k_freeze_all<<<nblk(n_act), 256, 0, st>>>(n_act, iter - 1, live, frozen_at, conv);
+            n_run = iter - 1;
+            break;
+        }
+        bool accepted = false, f_conv = false;
+        for (int trial = 1; trial <= P->max_trials; ++trial) {
+            ++n_trials;
+            // LSQR init (Krylov lsqr: beta1 u1 = b, alpha1 v1 = A'u1)
+            Scalars init{};
+            init.cost = cost;
+            init.beta1 = std::sqrt(cost);
+            init.beta = init.beta1;
+            init.inv_beta = init.beta1 != 0 ? 1.0 / init.beta1 : 0.0;
+            init.lambda = std::sqrt(lam);
+            init.atol = P->linear_tol;
+            init.btol = P->linear_tol;
+            init.itmax = P->inner_iterations;
+            init.c2 = -1.0;
+            init.stopped = init.beta1 == 0 ? 1 : 0;
+            init.status = init.beta1 == 0 ? 4 : 0;
+            *h_sc = init;
+            check(cudaMemcpyAsync(sc, h_sc, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
+            if (init.beta1 == 0) {
+                check(cudaMemsetAsync(xl, 0, sizeof(double) * n, st), "memset");
+            } else {
+                k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red);
+                k_lsqr_w0<<<nblk(n), 256, 0, st>>>(n, vt, wl, sc, red);
+                for (int it = 0; it < P->inner_iterations; ++it) {
+                    k_Jv<<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, ay, ax, live, V, vt,
+                                                         it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, sc, red);
+                    k_JT<true><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
+                    k_lsqr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, sc, red);
+                }
+                check(cudaGetLastError(), "lsqr");
+            }
+            k_step<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->max_step, xl, cn, delta, dsc);
+            k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
+            launch_render(MODE_CAND, live, coefc, nullptr, data_work, &sc->cost_cand);
+            evals += (double)n_live * (2 * model_R + 1) * (2 * model_R + 1);
+            read_scalars();
+            n_lsqr += h_sc->iter;
+            macs += 2.0 * h_sc->iter * n_live * fc.S2;
+            const double cost_cand = h_sc->cost_cand;
+            const double dcost = cost - cost_cand;
+            f_conv = (cost_cand < cost) && (dcost / cost <= P->f_tol);
+            if (cost_cand < cost) {
+                accepted = true;
+                lam = std::max(lam / P->lambda_down, P->lambda_min);
+                // cost := cost_cand is re-derived by the next residual pass
+                Scalars s2 = *h_sc;
+                s2.cost = cost_cand;
+                s2.n_new_frozen = 0;
+                *h_sc = s2;
+                check(cudaMemcpyAsync(sc, h_sc, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
+                // C_r of the freeze test uses the cost at the start of this iteration
+                Scalars* scf = S<Scalars>(ctx, "scalars_freeze", 1);
+                Scalars s3 = s2;
+                s3.cost = cost;
+                check(cudaMemcpyAsync(scf, &s3, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
+                k_accept_freeze<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->x_tol, P->g_tol, dof, iter, theta, delta,
+                                                            dsc, cn, D, bsc, live, newf, frozen_at, conv, scf);
+                check(cudaGetLastError(), "k_accept_freeze");
+                int h_new = 0;
+                check(cudaMemcpyAsync(&h_new, &scf->n_new_frozen, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaStreamSynchronize(st), "sync");
+                if (f_conv) {
+                    // f_tol freezes everything without subtraction (:1259-1264); the
+                    // per-star tests above are not part of that path, undo nothing:
+                    // stars they froze are frozen at `iter` either way.
+                    h_new = 0;
+                }
+                if (h_new > 0) {
+                    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+                    launch_render(MODE_FREEZE, newf, coef, data_work, nullptr, nullptr);
+                    evals += (double)h_new * (2 * model_R + 1) * (2 * model_R + 1);
+                    update_live_list();
+                }
+                break;
+            } else {
+                lam = std::min(lam * P->lambda_up, P->lambda_max);
+            }
+        }
+        n_run = iter;
+        if (f_conv) {
+            k_freeze_all<<<nblk(n_act), 256, 0, st>>>(n_act, iter, live, frozen_at, conv);
+            break;
+        }
+        if (accepted && n_live == 0) break;
+    }
+
+    // ---- errors at the final theta, every active star (:1302-1329)
+    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+    double* gram = S<double>(ctx, "gram", (int64_t)n_act * 6);
+    launch_fill(nullptr, n_act, gram);
+    double* err = S<double>(ctx, "err", n);
+    read_scalars();  // final cost
+    k_errors<<<nblk(n_act), 256, 0, st>>>(n_act, p, gram, reweighted, dof, sc, err);
+    check(cudaGetLastError(), "k_errors");
+    // ---- final render against the original data (:1344-1356) and diagnostics
+    double* resid = S<double>(ctx, "resid", npix);
+    launch_render(MODE_FINAL, nullptr, coef, resid, data, nullptr);
+    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 5);
+    if (eltype == CPB_F64)
+        k_diag<double><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
+                                                         (const double*)d_image, (const double*)d_background,
+                                                         (const double*)d_inv_var, diag);
+    else
+        k_diag<float><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid, (const float*)d_image,
+                                                        (const float*)d_background, (const float*)d_inv_var, diag);
+    check(cudaGetLastError(), "k_diag");
+    check(cudaEventRecord(ctx->ev1, st), "event");
+
+    // ---- download and assemble (:1289-1300, :1331-1337, :1404-1430)
+    std::vector<double> h_theta(n), h_err(n), h_diag(n_act * 5);
+    std::vector<int32_t> h_act(n_act), h_frozen(n_act);
+    std::vector<uint8_t> h_live(n_act), h_conv(n_act);
+    std::vector<double> y0(n_stars), x0(n_stars), f0(n_stars);
+    check(cudaMemcpyAsync(h_theta.data(), theta, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_err.data(), err, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_diag.data(), diag, sizeof(double) * n_act * 5, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_frozen.data(), frozen_at, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_live.data(), live, n_act, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_conv.data(), conv, n_act, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(y0.data(), d_y0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(x0.data(), d_x0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(f0.data(), d_flux0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+    if (out->residual)
+        check(cudaMemcpyAsync(out->residual, resid, sizeof(double) * npix, cudaMemcpyDeviceToHost, st), "d2h");
+    if (out->dbg_pixels)
+        check(cudaMemcpyAsync(out->dbg_pixels, dbg_pix, sizeof(int32_t) * fc.S2 * n_act, cudaMemcpyDeviceToHost, st),
+              "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    out->device_seconds = ms * 1e-3;
+
+    std::vector<double> oy(y0), ox(x0), of(f0);
+    std::vector<double> ey(n_stars, NaN), ex(n_stars, NaN), ef(n_stars, NaN);
+    std::vector<uint8_t> valid(n_stars, 0);
+    for (int64_t j = 0; j < n_act; ++j) {
+        int64_t i = h_act[j];
+        valid[i] = 1;
+        for (int k = 0; k < p; ++k) {
+            double v = h_theta[j * p + k], e = h_err[j * p + k];
+            if (fc.gc[k] == 1) {
+                oy[i] = v;
+                ey[i] = e;
+            } else if (fc.gc[k] == 2) {
+                ox[i] = v;
+                ex[i] = e;
+            } else {
+                of[i] = v;
+                ef[i] = e;
+            }
+        }
+    }
+    for (int64_t i = 0; i < n_stars; ++i) {
+        if (!(P->free_mask & CPB_FREE_Y)) {
+            oy[i] = P->fixed_y;
+            ey[i] = 0.0;
+        }
+        if (!(P->free_mask & CPB_FREE_X)) {
+            ox[i] = P->fixed_x;
+            ex[i] = 0.0;
+        }
+        if (!(P->free_mask & CPB_FREE_FLUX)) {
+            of[i] = P->fixed_flux;
+            ef[i] = 0.0;
+        }
+        if (valid[i] && !(std::isfinite(oy[i]) && std::isfinite(ox[i]) && std::isfinite(of[i]) && of[i] > 0))
+            valid[i] = 0;
+        out->y[i] = oy[i];
+        out->x[i] = ox[i];
+        out->flux[i] = of[i];
+        out->bkg[i] = P->fixed_bkg;
+        out->y_err[i] = ey[i];
+        out->x_err[i] = ex[i];
+        out->flux_err[i] = ef[i];
+        out->bkg_err[i] = 0.0;
+        out->valid[i] = valid[i];
+        out->converged[i] = 0;
+        out->n_iter[i] = 0;
+        if (out->chisq) out->chisq[i] = 0.0;
+        nan_diag(i);
+    }
+    for (int64_t j = 0; j < n_act; ++j) {
+        int64_t i = h_act[j];
+        out->converged[i] = h_conv[j];
+        out->n_iter[i] = h_live[j] ? n_run : h_frozen[j];
+        if (out->dbg_active) out->dbg_active[j] = h_act[j];
+        if (out->dbg_model_R) out->dbg_model_R[j] = model_R;
+        if (!valid[i]) continue;
+        const double* dg = &h_diag[j * 5];
+        if (out->chisq) out->chisq[i] = dg[0];
+        if (out->qfit) out->qfit[i] = dg[1];
+        if (out->qfit_expected) out->qfit_expected[i] = dg[2];
+        if (out->qfit_z) out->qfit_z[i] = dg[3];
+        if (out->crowding) out->crowding[i] = dg[4];
+    }
+    out->n_passes = n_run;
+    out->n_failed = n_failed;
+    out->n_trials = n_trials;
+    out->n_lsqr_iters = n_lsqr;
+    out->model_px_evals = evals;
+    out->lsqr_px_macs = macs;
+    return 0;
+}
+
+}  // namespace cpb

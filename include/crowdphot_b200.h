@@ -1,0 +1,268 @@
+/*
+ * crowdphot_b200.h -- C ABI of the B200 crowded-field PSF-fitting library.
+ *
+ * The library replaces two Julia entry points of CrowdPhot.jl:
+ *
+ *   CrowdPhot.fit_all_stars_simultaneous(image, psf, sources, fit_rad; kws...)
+ *       src/photometry/psf_photometry_simultaneous.jl:953-1431
+ *   CrowdPhot.PSF.fit_star(model, image, inds; kws...)
+ *       src/psf/psf_fitting.jl:229-308 (generic), :314-451 (CircularGaussianPSF),
+ *       :1086-1173 (ImagePSF), :1177-1210 (GriddedPSFModel{T,<:ImagePSF})
+ *
+ * Conventions (all entry points):
+ *   - Every image-shaped array is column-major (Julia layout): element (y, x),
+ *     1-based, lives at offset (y-1) + (x-1)*ny.
+ *   - Inputs and outputs are caller-owned host memory unless an entry point
+ *     says "device".  Device state is owned by the context handle.
+ *   - Return value 0 = success; negative = error (see CPB_ERR_*).  The text
+ *     of the last error is available from cpb_last_error().  Argument errors
+ *     carry the reference's ArgumentError message text.
+ *   - Per-star failures are not errors: they are reported in valid[] /
+ *     n_failed exactly as the reference does.
+ *   - One call at a time per context (an internal mutex serialises callers).
+ */
+#ifndef CROWDPHOT_B200_H
+#define CROWDPHOT_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define CPB_API __attribute__((visibility("default")))
+#else
+#define CPB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CPB_OK 0
+#define CPB_ERR_ARGUMENT (-1)  /* reference ArgumentError */
+#define CPB_ERR_CUDA (-2)      /* CUDA runtime / launch error */
+#define CPB_ERR_OOM (-3)       /* device memory exhausted or admission refused */
+#define CPB_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
+#define CPB_ERR_INTERNAL (-5)
+#define CPB_ERR_NO_DEVICE (-6) /* no CUDA device / library built without GPU */
+
+/* ---- element types ----------------------------------------------------- */
+#define CPB_F32 1
+#define CPB_F64 2
+
+/* ---- PSF kinds (the supported AbstractPSFModel subtypes) --------------- */
+#define CPB_PSF_GRIDDED_IMAGE 1     /* GriddedPSFModel{T,<:ImagePSF{T}}  src/psf/gridded_psf.jl:51-62 */
+#define CPB_PSF_IMAGE 2             /* ImagePSF{T}                        src/psf/empirical_models.jl:76-85 */
+#define CPB_PSF_CIRCULAR_GAUSSIAN 3 /* CircularGaussianPSF{T}             src/psf/parametric_models.jl:62-115 */
+
+/*
+ * PSF descriptor.  For CPB_PSF_GRIDDED_IMAGE every node is an ImagePSF;
+ * for CPB_PSF_IMAGE n_nodes == 1 (grid_y/grid_x ignored); for
+ * CPB_PSF_CIRCULAR_GAUSSIAN n_nodes == 0 and only `fwhm` is read.
+ * Node k's tabulated data is node_data[k], column-major node_ny[k] x node_nx[k]
+ * (ImagePSF.data), node_os[2k], node_os[2k+1] = ImagePSF.oversampling[1] (x
+ * factor), oversampling[2] (y factor); node_origin[2k], node_origin[2k+1] =
+ * ImagePSF.origin.y, origin.x; node_fill_value[k] = ImagePSF.fill_value;
+ * grid_y[k], grid_x[k] = GriddedPSFModel node positions.
+ */
+typedef struct cpb_psf_desc {
+    int32_t kind;
+    int32_t n_nodes;
+    int32_t eltype; /* element type of node_data */
+    int32_t reserved;
+    const void* const* node_data;
+    const int64_t* node_ny;
+    const int64_t* node_nx;
+    const int64_t* node_os;
+    const double* node_origin;
+    const double* node_fill_value;
+    const double* grid_y;
+    const double* grid_x;
+    double fwhm;
+} cpb_psf_desc;
+
+/* free-parameter bits (order of the reference's getproperties) */
+#define CPB_FREE_Y 1
+#define CPB_FREE_X 2
+#define CPB_FREE_FLUX 4
+#define CPB_FREE_BKG 8  /* fit_star only */
+#define CPB_FREE_FWHM 16 /* fit_star with CircularGaussianPSF only */
+
+/* arithmetic of the device path */
+#define CPB_PREC_FP64 0  /* plain form: every step in FP64 */
+#define CPB_PREC_MIXED 1 /* FP32 stamps/render/residual/J products; FP64 solver scalars */
+
+/* covariance estimator (levenberg_marquardt.jl:366-388) */
+#define CPB_COV_AUTO 0          /* KnownWeights iff inv_var given */
+#define CPB_COV_KNOWN_WEIGHTS 1
+#define CPB_COV_REWEIGHTED 2
+
+/* damping (levenberg_marquardt.jl:64-99) */
+#define CPB_DAMP_MARQUARDT 0
+#define CPB_DAMP_LEVENBERG 1
+#define CPB_DAMP_NONE 2
+
+/* inner Krylov solver of the simultaneous fit */
+#define CPB_SOLVER_LSQR 0
+#define CPB_SOLVER_LSMR 1 /* accepted by the reference; rejected here */
+
+/*
+ * Keyword arguments of fit_all_stars_simultaneous
+ * (psf_photometry_simultaneous.jl:953-981).  Non-free y/x/flux take the
+ * matching fixed_* value (the reference's `fixed` NamedTuple); bkg is always
+ * fixed (contract :1019-1031); fixed_fwhm is the Gaussian's fixed FWHM.
+ * model_rad_max < 0 means the default 10*fit_rad.
+ */
+typedef struct cpb_sim_params {
+    double fit_rad;
+    int32_t free_mask;
+    int32_t inner_iterations; /* 10 */
+    double fixed_y, fixed_x, fixed_flux, fixed_bkg, fixed_fwhm;
+    double linear_tol;        /* 1e-6 */
+    int32_t model_rad_auto;   /* 1 = :auto */
+    int32_t max_trials;       /* 8 */
+    double model_rad;         /* used when model_rad_auto == 0 */
+    double model_rad_max;     /* 10*fit_rad */
+    double model_rad_nsigma;  /* 1 */
+    double max_step;          /* 0.25 */
+    int32_t max_iter;         /* 40 */
+    int32_t covariance;       /* CPB_COV_* */
+    double x_tol, f_tol, g_tol;                          /* 1e-5, 1e-4, 1e-4 */
+    double lambda_init, lambda_up, lambda_down;          /* 1e-4, 10, 10 */
+    double lambda_min, lambda_max;                       /* 1e-12, 1e12 */
+    int32_t precision;        /* CPB_PREC_* */
+    int32_t solver;           /* CPB_SOLVER_* */
+    int32_t damping;          /* CPB_DAMP_* */
+    int32_t reserved;
+} cpb_sim_params;
+
+/*
+ * Result of a simultaneous fit (MultiPassPhotResult,
+ * psf_photometry_single.jl:99-122).  All arrays are caller-allocated with n
+ * entries (catalogue order); NULL skips an optional output.  residual is
+ * ny*nx column-major.  The dbg_* exports give the integer structures the
+ * reference builds once per fit (active order, stamp pixel indices, model
+ * radii) for bit-exact comparison; n_active and n_union are always written.
+ */
+typedef struct cpb_sim_result {
+    double *y, *x, *flux, *bkg;
+    double *y_err, *x_err, *flux_err, *bkg_err;
+    uint8_t *converged, *valid;
+    double* chisq;            /* optional */
+    double *qfit, *qfit_expected, *qfit_z, *crowding; /* optional diagnostics */
+    int32_t* n_iter;
+    double* residual;         /* optional, ny*nx */
+    int32_t* dbg_active;      /* optional, n: catalogue index (0-based) per active slot */
+    int32_t* dbg_pixels;      /* optional, S2*n: 1-based flat pixel per stamp entry, 0 = unusable */
+    int32_t* dbg_model_R;     /* optional, n: per active slot */
+    int32_t n_passes;
+    int32_t n_failed;
+    int64_t n_active;
+    int64_t n_union;
+    /* work counters */
+    int64_t n_trials;         /* damping trials run */
+    int64_t n_lsqr_iters;     /* LSQR iterations run (summed over trials) */
+    double model_px_evals;    /* stamp fills + renders, star-pixel evaluations */
+    double lsqr_px_macs;      /* star-pixel products in J and J^T */
+    double device_seconds;    /* device-timed fit, excluding host<->device copies */
+} cpb_sim_result;
+
+/*
+ * Keyword arguments of fit_star / lm_irls (psf_fitting.jl:229-250,
+ * levenberg_marquardt.jl:431-449).  IRLS (reweight) is not supported.
+ */
+typedef struct cpb_lm_params {
+    int32_t free_mask;        /* CPB_FREE_* bits */
+    int32_t max_iter;         /* 200 */
+    double fixed_y, fixed_x, fixed_flux, fixed_bkg, fixed_fwhm;
+    double x_tol, f_tol, g_tol;                  /* 1e-8, 1e-4, 1e-4 */
+    double lambda_init, lambda_up, lambda_down;  /* 1e-4, 10, 10 */
+    double lambda_min, lambda_max;               /* 1e-12, 1e12 */
+    double min_diagonal;      /* MarquardtDamping.min_diagonal, 1e-6 */
+    int32_t damping;          /* CPB_DAMP_* */
+    int32_t covariance;       /* CPB_COV_* */
+    int32_t precision;        /* CPB_PREC_* */
+    int32_t reserved;
+} cpb_lm_params;
+
+/*
+ * Per-cutout result of the batched LM fit (LMResult, levenberg_marquardt.jl:28-41).
+ * np = number of model parameters (4 for image/gridded: y,x,flux,bkg; 5 for
+ * CircularGaussianPSF: y,x,fwhm,flux,bkg); nf = number of free ones.
+ * params: n*np (fitted model parameters, fixed ones included);
+ * cov: n*nf*nf column-major (optional).  status[c] is 0, or CPB_ERR_ARGUMENT
+ * when cutout c fails the reference's input checks (too few valid pixels).
+ */
+typedef struct cpb_lm_result {
+    double* params;
+    double* cov;              /* optional */
+    double *cost, *cost_init, *chisq, *lambda_final;
+    uint8_t *converged, *x_converged, *f_converged, *g_converged;
+    int32_t* iterations;
+    int32_t* status;
+    double device_seconds;
+} cpb_lm_result;
+
+typedef struct cpb_ctx cpb_ctx;
+typedef struct cpb_psf cpb_psf;
+
+/* ---- context ------------------------------------------------------------ */
+/* Creates a context on CUDA device `device`. */
+CPB_API int cpb_ctx_create(int device, cpb_ctx** out);
+CPB_API int cpb_ctx_destroy(cpb_ctx* ctx);
+/* Text of the last error on this context ("" if none); valid until the next call. */
+CPB_API const char* cpb_last_error(const cpb_ctx* ctx);
+/* Library version string. */
+CPB_API const char* cpb_version(void);
+
+/* ---- PSF ---------------------------------------------------------------- */
+/*
+ * Validates and uploads a PSF once (GriddedPSFModel constructor checks,
+ * gridded_psf.jl:64-135; ImagePSF checks, empirical_models.jl:91-140).
+ * The node grid (ygrid, xgrid, index_grid) is derived here.
+ */
+CPB_API int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* desc, cpb_psf** out);
+CPB_API int cpb_psf_free(cpb_ctx* ctx, cpb_psf* psf);
+
+/* ---- simultaneous fit (fit_all_stars_simultaneous) ---------------------- */
+/*
+ * image: ny*nx of `eltype`; inv_var (nullable) and background (nullable):
+ * same shape and eltype.  The fitted data are image - background.  y0/x0/flux0:
+ * the catalogue (sources.y, sources.x, sources.flux), n entries.
+ * Replaces psf_photometry_simultaneous.jl:953-1431.
+ */
+CPB_API int cpb_fit_simultaneous(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                         const void* image, int32_t eltype, int64_t ny, int64_t nx,
+                         const void* inv_var, const void* background,
+                         int64_t n, const double* y0, const double* x0, const double* flux0,
+                         cpb_sim_result* out);
+
+/*
+ * Same fit with image / inv_var / background / catalogue already resident in
+ * device memory ("device" pointers).  Outputs are still host arrays.
+ */
+CPB_API int cpb_fit_simultaneous_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                                const void* d_image, int32_t eltype, int64_t ny, int64_t nx,
+                                const void* d_inv_var, const void* d_background,
+                                int64_t n, const double* d_y0, const double* d_x0,
+                                const double* d_flux0, cpb_sim_result* out);
+
+/* ---- batched per-star LM (fit_star) ------------------------------------- */
+/*
+ * n_cutouts independent fit_star calls.  Cutout c is the column-major block
+ * pixels[offsets[c] .. offsets[c] + ny[c]*nx[c]) holding image[inds] with
+ * inds = (y_origin[c] : y_origin[c]+ny[c]-1, x_origin[c] : x_origin[c]+nx[c]-1)
+ * (1-based image coordinates, which are the coordinates the model is evaluated
+ * at).  inv_var (nullable) shares the layout.  init: n_cutouts*np initial
+ * model parameters.  Replaces psf_fitting.jl:229-308, :314-451, :1086-1210.
+ */
+CPB_API int cpb_fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params,
+                     int64_t n_cutouts, const int64_t* offsets, const int32_t* ny,
+                     const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,
+                     const void* pixels, int32_t eltype, const void* inv_var,
+                     const double* init, cpb_lm_result* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CROWDPHOT_B200_H */
