@@ -1,0 +1,317 @@
+#!/usr/bin/env python
+"""Benchmark: fitted stars/s of the simultaneous PSF fit on the 2048^2 crowded field.
+
+Workload (one "step" = one fit_all_stars_simultaneous call over one field):
+  2048 x 2048 Float32 image, 50,000 stars (uniform positions, power-law
+  fluxes dN/dF ~ F^-1.5 on [1e1, 1e6]), Moffat beta=3 FWHM 2.8 ePSF tabulated
+  101 x 101 at 4x oversampling (single-node GriddedPSFModel{ImagePSF}),
+  25 x 25 fit boxes (fit_rad = model_rad = 12), background 50-200 counts,
+  Poisson + Gaussian read noise 5, inverse-variance weights, initial guesses
+  perturbed by N(0, 0.3 px) and x U(0.9, 1.1) in flux; fixed = (bkg = 0).
+  Synthetic, seeded; the reference publishes no dataset for this path.
+
+value: fitted (valid and converged) stars per second with inputs resident in
+HBM, device-timed (CUDA events on the library's stream), whole job over all
+GPUs.  e2e: the same through the public API with host buffers (host->device
+copies and the result readback inside the timed region).  Multi-GPU runs are
+independent replicas (one field per GPU, no collective on the data path).
+
+--impl reference times the CPU restatement of the reference algorithm (the
+oracle; the Julia reference cannot run on the box) on bounded samples of the
+same field across all host cores.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [ROOT, os.path.join(ROOT, "crowdphot.jl_b200")]
+
+import numpy as np  # noqa: E402
+
+METRIC = "fitted stars/s on 1 B200 (served+mixed vs plain, flux err<=1e-5); p50/p99 ms"
+NY = NX = 2048
+N_STARS = 50_000
+FIT_RAD = 12
+SEED = 1002
+SAMPLE = 512  # CPU sample side (same star density)
+
+
+def workload_config(ny=NY, nx=NX, n=N_STARS):
+    return {"workload": f"crowded field {ny}x{nx} Float32, {n} stars, Moffat ePSF 101x101 os4, 25x25 boxes",
+            "form": "plain (FP64 device arithmetic)", "image": [ny, nx], "n_stars": n, "fit_rad": FIT_RAD,
+            "model_rad": FIT_RAD, "psf": "GriddedPSFModel{ImagePSF} single node", "seed": SEED,
+            "l2": "intermediate stamp arrays exceed L2 (375-750 MB); a 256 MiB buffer is written between steps"}
+
+
+def make_field(ny, nx, n, seed):
+    from crowdphot_b200.simulate import crowded_field, moffat_epsf
+    psf = moffat_epsf()
+    img, bkg, iv, truth, init = crowded_field(ny, nx, n, seed=seed, psf=psf, dtype=np.float32)
+    return psf, img, bkg, iv, truth, init
+
+
+def fit_kwargs():
+    return dict(fixed={"bkg": 0.0}, model_rad=FIT_RAD)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        mx = [float(r[2]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the oracle on bounded samples (cpu_baseline and the reference arm)
+# ---------------------------------------------------------------------------
+def _cpu_sample_fit(seed):
+    from oracle import orc_fit_simultaneous
+    n = int(round(N_STARS * SAMPLE * SAMPLE / (NY * NX)))
+    psf, img, bkg, iv, truth, init = make_field(SAMPLE, SAMPLE, n, seed)
+    t = time.perf_counter()
+    r = orc_fit_simultaneous(img, psf, init, FIT_RAD, inv_var=iv, background=bkg, residual=False, **fit_kwargs())
+    dt = time.perf_counter() - t
+    return int((r.valid & r.converged).sum()), dt, n
+
+
+def cpu_baseline_single():
+    fitted, dt, n = _cpu_sample_fit(SEED + 1)
+    return {"value": fitted / dt, "unit": "stars/s", "cores": 1, "kind": "port",
+            "sample": f"{SAMPLE}x{SAMPLE} crop at the same star density ({n} stars), one fit, FP64 oracle, "
+                      f"{dt:.1f} s"}
+
+
+def run_reference(args):
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    times = []
+    total_fitted = 0
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            res = pool.map(_cpu_sample_fit, [SEED + 100 + step * cores + k for k in range(cores)])
+            dt = time.perf_counter() - t
+            if step >= args.warmup:
+                times.append(dt)
+                total_fitted += sum(r[0] for r in res)
+    total = sum(times)
+    value = total_fitted / total
+    n = int(round(N_STARS * SAMPLE * SAMPLE / (NY * NX)))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "stars/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(workload_config(), sample=f"{cores} x {SAMPLE}x{SAMPLE} samples per step"),
+            "cpu_baseline": {"value": value, "unit": "stars/s", "cores": cores, "kind": "port",
+                             "sample": f"each step: {cores} independent {SAMPLE}x{SAMPLE} fields at the workload's "
+                                       f"star density ({n} stars each), one process per core, FP64 oracle "
+                                       "(single-threaded restatement of the reference fitter)"},
+            "e2e": {"value": value, "unit": "stars/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args):
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    import crowdphot_b200 as cpb
+    from crowdphot_b200 import _abi
+    from crowdphot_b200.photometry import SimOutputs, sim_params
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    ny, nx, n = args.ny, args.nx, args.n_stars
+    psf, img, bkg, iv, truth, init = make_field(ny, nx, n, SEED + rank)
+    ctx = cpb.get_context(local)
+    hp = ctx.psf_handle(psf)
+    P = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD)
+
+    # device-resident inputs (column-major images = torch (nx, ny) contiguous)
+    t_img = torch.from_numpy(np.ascontiguousarray(img.T)).to(dev)
+    t_iv = torch.from_numpy(np.ascontiguousarray(iv.T)).to(dev)
+    t_bkg = torch.from_numpy(np.ascontiguousarray(bkg.T)).to(dev)
+    t_y = torch.from_numpy(np.asarray(init["y"], np.float64)).to(dev)
+    t_x = torch.from_numpy(np.asarray(init["x"], np.float64)).to(dev)
+    t_f = torch.from_numpy(np.asarray(init["flux"], np.float64)).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > 126 MB L2
+    R = FIT_RAD
+    S2 = (2 * R + 1) ** 2
+    outs = SimOutputs(n, ny, nx, S2, residual=False)
+    vp = lambda t: C.c_void_p(t.data_ptr())
+
+    def step_resident():
+        rc = ctx.lib.cpb_fit_simultaneous_device(ctx.handle, hp, C.byref(P), vp(t_img), _abi.CPB_F32, ny, nx,
+                                                 vp(t_iv), vp(t_bkg), n, vp(t_y), vp(t_x), vp(t_f), C.byref(outs.c))
+        ctx.raise_for(rc, "cpb_fit_simultaneous_device")
+        fitted = int((outs.valid[:n].astype(bool) & outs.converged[:n].astype(bool)).sum())
+        return fitted, float(outs.c.device_seconds)
+
+    for _ in range(args.warmup):
+        step_resident()
+        flush.fill_(1.0)
+    ctx.kernel_stats(reset=True)
+    barrier()
+    clocks = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    fitted_total, dev_times = 0, []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        f, s = step_resident()
+        fitted_total += f
+        dev_times.append(s)
+    barrier()
+    clk = clocks.stop() if clocks else None
+    _, launches = ctx.kernel_stats(reset=True)
+    total_s = float(sum(dev_times))
+    agg = torch.tensor([total_s, float(fitted_total), float(launches)], dtype=torch.float64, device=dev)
+    if world > 1:
+        mx = agg.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = agg.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        total_s, fitted_all, launches_all = float(mx[0]), float(sm[1]), int(sm[2])
+    else:
+        fitted_all, launches_all = float(fitted_total), launches
+    value = fitted_all / total_s
+
+    # profiling pass (not timed): per-kernel event timing and algorithmic bytes
+    ctx.set_profiling(True)
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    f_prof, s_prof = step_resident()
+    ctx.set_profiling(False)
+    kst, _ = ctx.kernel_stats(reset=True)
+    top = max(kst.items(), key=lambda kv: kv[1]["seconds"])
+    peak, peak_kind = peaks()
+    ach = top[1]["bytes"] / top[1]["seconds"] / 1e9
+    roof = {"kernel": top[0], "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_source": peak_kind, "traffic": None,
+            "launches": top[1]["launches"], "share_of_step": top[1]["seconds"] / max(s_prof, 1e-12)}
+    kernels = {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
+                   "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst.items())}
+
+    # end to end through the public API with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a.T)).pin_memory().numpy().T
+    h_img, h_iv, h_bkg = pin(img), pin(iv), pin(bkg)
+    e_times, e_fitted = [], 0
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        r = cpb.fit_all_stars_simultaneous(h_img, psf, init, FIT_RAD, inv_var=h_iv, background=h_bkg, ctx=ctx,
+                                           residual=True, **fit_kwargs())
+        ev1.record()
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e_times.append(ev0.elapsed_time(ev1) * 1e-3)
+            e_fitted += int((r.valid & r.converged).sum())
+    et = torch.tensor([sum(e_times), float(e_fitted)], dtype=torch.float64, device=dev)
+    if world > 1:
+        mx = et.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        sm = et.clone()
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+        e_value = float(sm[1]) / float(mx[0])
+    else:
+        e_value = e_fitted / sum(e_times)
+    h2d = 3 * img.nbytes + 3 * 8 * n
+    d2h = n * (12 * 8 + 2 + 4) + ny * nx * 8
+
+    if rank == 0:
+        ms = sorted(1e3 * t for t in dev_times)
+        line = {"metric": METRIC, "value": value, "unit": "stars/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": dict(workload_config(ny, nx, n), parallelism=f"replicas x{world}"),
+                "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99)),
+                "fitted_per_step": fitted_all / args.steps / world,
+                "model_px_evals_per_s": float(outs.c.model_px_evals) / s_prof,
+                "roofline": roof, "kernels": kernels, "gpu_launches": launches_all, "clocks": clk,
+                "e2e": {"value": e_value, "unit": "stars/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_baseline_single()
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--ny", type=int, default=NY)
+    ap.add_argument("--nx", type=int, default=NX)
+    ap.add_argument("--n-stars", type=int, default=N_STARS)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -162,12 +162,19 @@ class LMResultC(C.Structure):
     ]
 
 
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int64), ("seconds", C.c_double), ("bytes", C.c_double)]
+
+
 # Every entry point declared in include/crowdphot_b200.h: name -> (restype, argtypes)
 PROTOTYPES = {
     "cpb_ctx_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "cpb_ctx_destroy": (C.c_int, [C.c_void_p]),
     "cpb_last_error": (C.c_char_p, [C.c_void_p]),
     "cpb_version": (C.c_char_p, []),
+    "cpb_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "cpb_ctx_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int),
+                                       C.POINTER(C.c_int64), C.c_int]),
     "cpb_psf_upload": (C.c_int, [C.c_void_p, C.POINTER(PsfDesc), C.POINTER(C.c_void_p)]),
     "cpb_psf_free": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cpb_fit_simultaneous": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_void_p, C.c_int32,

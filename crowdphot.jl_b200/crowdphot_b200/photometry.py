@@ -76,6 +76,21 @@ class Context:
             raise MemoryError(f"{what}: {msg}")
         raise CudaError(f"{what} failed ({rc}): {msg}")
 
+    def set_profiling(self, enable: bool):
+        self.raise_for(self.lib.cpb_ctx_set_profiling(self.handle, int(bool(enable))), "cpb_ctx_set_profiling")
+
+    def kernel_stats(self, reset: bool = True):
+        """Per-kernel launch counts, event-timed seconds and algorithmic bytes, plus
+        the total launch count since the last reset."""
+        buf = (_abi.KernelStat * 64)()
+        n = C.c_int()
+        launches = C.c_int64()
+        rc = self.lib.cpb_ctx_kernel_stats(self.handle, buf, 64, C.byref(n), C.byref(launches), int(reset))
+        self.raise_for(rc, "cpb_ctx_kernel_stats")
+        stats = {buf[i].name.decode(): dict(launches=int(buf[i].launches), seconds=float(buf[i].seconds),
+                                            bytes=float(buf[i].bytes)) for i in range(min(n.value, 64))}
+        return stats, int(launches.value)
+
     def psf_handle(self, psf, fwhm_override=None):
         key = id(psf)
         hit = self._psfs.get(key)

@@ -37,6 +37,49 @@ void* scratch(cpb_ctx* ctx, const char* name, size_t bytes) {
     return p;
 }
 
+static cudaEvent_t pool_event(cpb_ctx* ctx) {
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    check(cudaEventCreate(&e), "cudaEventCreate");
+    return e;
+}
+
+KernelScope::KernelScope(cpb_ctx* c, const char* n, double by) : ctx(c), name(n), bytes(by) {
+    ctx->launches += 1;
+    if (ctx->profile) {
+        a = pool_event(ctx);
+        b = pool_event(ctx);
+        cudaEventRecord(a, ctx->stream);
+    }
+}
+
+KernelScope::~KernelScope() {
+    if (a) {
+        cudaEventRecord(b, ctx->stream);
+        ctx->pending.push_back({name, a, b, bytes});
+    }
+}
+
+void resolve_kernel_events(cpb_ctx* ctx) {
+    if (ctx->pending.empty()) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& p : ctx->pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, p.a, p.b);
+        auto& k = ctx->kstats[p.name];
+        k.launches += 1;
+        k.seconds += ms * 1e-3;
+        k.bytes += p.bytes;
+        ctx->event_pool.push_back(p.a);
+        ctx->event_pool.push_back(p.b);
+    }
+    ctx->pending.clear();
+}
+
 template <typename F>
 int guarded(cpb_ctx* ctx, F&& f) {
     if (!ctx) return CPB_ERR_ARGUMENT;
@@ -101,6 +144,11 @@ int cpb_ctx_destroy(cpb_ctx* ctx) {
             if (kv.second.p) cudaFree(kv.second.p);
         ctx->bufs.clear();
         if (ctx->pinned) cudaFreeHost(ctx->pinned);
+        for (auto e : ctx->event_pool) cudaEventDestroy(e);
+        for (auto& p : ctx->pending) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -110,6 +158,38 @@ int cpb_ctx_destroy(cpb_ctx* ctx) {
 }
 
 const char* cpb_last_error(const cpb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int cpb_ctx_set_profiling(cpb_ctx* ctx, int enable) {
+    return guarded(ctx, [&]() -> int {
+        resolve_kernel_events(ctx);
+        ctx->profile = enable != 0;
+        return CPB_OK;
+    });
+}
+
+int cpb_ctx_kernel_stats(cpb_ctx* ctx, cpb_kernel_stat* out, int max_out, int* n_out, int64_t* launches, int reset) {
+    return guarded(ctx, [&]() -> int {
+        resolve_kernel_events(ctx);
+        int k = 0;
+        for (auto& kv : ctx->kstats) {
+            if (out && k < max_out) {
+                std::memset(&out[k], 0, sizeof(cpb_kernel_stat));
+                std::strncpy(out[k].name, kv.first.c_str(), sizeof(out[k].name) - 1);
+                out[k].launches = kv.second.launches;
+                out[k].seconds = kv.second.seconds;
+                out[k].bytes = kv.second.bytes;
+            }
+            ++k;
+        }
+        if (n_out) *n_out = k;
+        if (launches) *launches = ctx->launches;
+        if (reset) {
+            ctx->kstats.clear();
+            ctx->launches = 0;
+        }
+        return CPB_OK;
+    });
+}
 
 int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
     return guarded(ctx, [&]() -> int {

@@ -282,12 +282,41 @@ struct cpb_ctx {
     std::map<std::string, Buf> bufs;  // grow-only scratch arena, reused across calls
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void* pinned = nullptr;  // small pinned staging for scalar readbacks
+    // kernel instrumentation: launch counter (always on) and, when profiling is
+    // enabled, CUDA-event timing of every launch on this context's stream
+    int64_t launches = 0;
+    bool profile = false;
+    struct KStat {
+        int64_t launches = 0;
+        double seconds = 0, bytes = 0;
+    };
+    std::map<std::string, KStat> kstats;
+    struct Pending {
+        std::string name;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
 };
 
 namespace cpb {
 
 // Scratch arena: returns a device buffer of at least `bytes` under `name`.
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
+
+// Brackets one kernel launch: counts it and, when profiling, records CUDA
+// events on the context stream with the launch's algorithmic bytes.
+struct KernelScope {
+    cpb_ctx* ctx;
+    const char* name;
+    double bytes;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelScope(cpb_ctx* c, const char* n, double by);
+    ~KernelScope();
+};
+// Resolves pending event pairs into ctx->kstats (after a stream sync).
+void resolve_kernel_events(cpb_ctx* ctx);
 
 struct CudaError {
     cudaError_t e;

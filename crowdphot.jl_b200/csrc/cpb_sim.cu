@@ -1232,6 +1232,10 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
         if (nlist <= 0) return;
         unsigned gb = (unsigned)std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16);
+        KernelScope ks_(ctx, gram ? "k_fill_gram" : "k_fill",
+                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * 8 + p * 8) +
+                                         std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1) + fc.S2) * 16 +
+                                         sizeof(StarCoef)));
         if (fc.S2 <= 256 * 2)
             k_fill<256, 2><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
         else if (fc.S2 <= 256 * 4)
@@ -1245,6 +1249,10 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     (void)fill_blocks;
     auto launch_render = [&](int mode, const uint8_t* incl, const StarCoef* cf, double* outp, const double* ref,
                              double* result) {
+        const double px_bytes = mode == MODE_CUR ? 25.0 : (mode == MODE_CAND ? 17.0 : 16.0);
+        KernelScope ks_(ctx, mode == MODE_CUR ? "k_render_resid" : (mode == MODE_CAND ? "k_render_cost" :
+                                                   (mode == MODE_FREEZE ? "k_render_freeze" : "k_render_final")),
+                        (double)npix * px_bytes + (double)n_live * sizeof(StarCoef));
         switch (mode) {
             case MODE_CUR:
                 k_render<MODE_CUR><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
@@ -1283,7 +1291,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     double evals = 0.0, macs = 0.0;
 
     // ---- initial fill and cost (:1171-1178)
-    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
     launch_fill(live_list, n_live, nullptr);
     launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
     check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
@@ -1296,7 +1304,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     // ---- outer loop (:1186-1284)
     for (int iter = 1; iter <= P->max_iter; ++iter) {
         if (!fresh) {
-            k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+            KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
             launch_fill(live_list, n_live, nullptr);
             launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
             evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
@@ -1304,10 +1312,16 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
         fresh = false;
         // b_scaled = J' wt_resid (frozen stars stay 0)
         check(cudaMemsetAsync(bsc, 0, sizeof(double) * n, st), "memset");
-        k_JT<false><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
+        {
+            KernelScope ks_(ctx, "k_JT", (double)n_live * ((double)p * fc.S2 * 8 + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
+            k_JT<false><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
+        }
         check(cudaGetLastError(), "k_JT");
         macs += (double)n_live * fc.S2;
-        k_gnorm<<<nblk(n), 256, 0, st>>>(n, cn, bsc, dof, sc, red);
+        {
+            KernelScope ks_(ctx, "k_gnorm", (double)n * 8 * 2);
+            k_gnorm<<<nblk(n), 256, 0, st>>>(n, cn, bsc, dof, sc, red);
+        }
         check(cudaGetLastError(), "k_gnorm");
         read_scalars();
         const double cost = h_sc->cost;
@@ -1337,18 +1351,36 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
             if (init.beta1 == 0) {
                 check(cudaMemsetAsync(xl, 0, sizeof(double) * n, st), "memset");
             } else {
-                k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red);
-                k_lsqr_w0<<<nblk(n), 256, 0, st>>>(n, vt, wl, sc, red);
+                {
+                    KernelScope ks_(ctx, "k_lsqr_v0", (double)n * 8 * 3);
+                    k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red);
+                }
+                {
+                    KernelScope ks_(ctx, "k_lsqr_w0", (double)n * 8 * 2);
+                    k_lsqr_w0<<<nblk(n), 256, 0, st>>>(n, vt, wl, sc, red);
+                }
                 for (int it = 0; it < P->inner_iterations; ++it) {
-                    k_Jv<<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, ay, ax, live, V, vt,
+                    {
+                        KernelScope ks_(ctx, "k_Jv", (double)n_live * ((double)p * fc.S2 * 8 + p * 8) + 2.0 * npix * 8);
+                        k_Jv<<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, ay, ax, live, V, vt,
                                                          it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, sc, red);
-                    k_JT<true><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
-                    k_lsqr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, sc, red);
+                    }
+                    {
+                        KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * 8 + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
+                        k_JT<true><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
+                    }
+                    {
+                        KernelScope ks_(ctx, "k_lsqr_update", (double)n * 8 * 5);
+                        k_lsqr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, sc, red);
+                    }
                 }
                 check(cudaGetLastError(), "lsqr");
             }
-            k_step<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->max_step, xl, cn, delta, dsc);
-            k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
+            {
+                KernelScope ks_(ctx, "k_step", (double)n * 8 * 4);
+                k_step<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->max_step, xl, cn, delta, dsc);
+            }
+            KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
             launch_render(MODE_CAND, live, coefc, nullptr, data_work, &sc->cost_cand);
             evals += (double)n_live * (2 * model_R + 1) * (2 * model_R + 1);
             read_scalars();
@@ -1371,8 +1403,11 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                 Scalars s3 = s2;
                 s3.cost = cost;
                 check(cudaMemcpyAsync(scf, &s3, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
-                k_accept_freeze<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->x_tol, P->g_tol, dof, iter, theta, delta,
+                {
+                    KernelScope ks_(ctx, "k_accept_freeze", (double)n * 8 * 7);
+                    k_accept_freeze<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->x_tol, P->g_tol, dof, iter, theta, delta,
                                                             dsc, cn, D, bsc, live, newf, frozen_at, conv, scf);
+                }
                 check(cudaGetLastError(), "k_accept_freeze");
                 int h_new = 0;
                 check(cudaMemcpyAsync(&h_new, &scf->n_new_frozen, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
@@ -1384,7 +1419,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                     h_new = 0;
                 }
                 if (h_new > 0) {
-                    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+                    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
                     launch_render(MODE_FREEZE, newf, coef, data_work, nullptr, nullptr);
                     evals += (double)h_new * (2 * model_R + 1) * (2 * model_R + 1);
                     update_live_list();
@@ -1403,7 +1438,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     }
 
     // ---- errors at the final theta, every active star (:1302-1329)
-    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
     double* gram = S<double>(ctx, "gram", (int64_t)n_act * 6);
     launch_fill(nullptr, n_act, gram);
     double* err = S<double>(ctx, "err", n);

@@ -214,6 +214,25 @@ CPB_API const char* cpb_last_error(const cpb_ctx* ctx);
 /* Library version string. */
 CPB_API const char* cpb_version(void);
 
+/*
+ * Instrumentation (no counterpart in the reference).  Every kernel launch of a
+ * context is counted; with profiling enabled each launch is also bracketed by
+ * CUDA events on the context stream and credited with its algorithmic bytes
+ * (each distinct array element it must move, counted once).  Profiling adds
+ * two event records per launch; leave it off for timed runs.
+ */
+typedef struct cpb_kernel_stat {
+    char name[32];
+    int64_t launches;
+    double seconds;  /* summed event-timed duration */
+    double bytes;    /* summed algorithmic bytes */
+} cpb_kernel_stat;
+CPB_API int cpb_ctx_set_profiling(cpb_ctx* ctx, int enable);
+/* Writes up to max_out per-kernel records, the number available to *n_out and
+ * the total launch count to *launches; reset != 0 clears the counters. */
+CPB_API int cpb_ctx_kernel_stats(cpb_ctx* ctx, cpb_kernel_stat* out, int max_out, int* n_out, int64_t* launches,
+                                 int reset);
+
 /* ---- PSF ---------------------------------------------------------------- */
 /*
  * Validates and uploads a PSF once (GriddedPSFModel constructor checks,
