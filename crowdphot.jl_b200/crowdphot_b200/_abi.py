@@ -183,6 +183,10 @@ PROTOTYPES = {
     "cpb_fit_simultaneous_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_void_p, C.c_int32,
                                               C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                               C.c_void_p, C.c_void_p, C.POINTER(SimResult)]),
+    "cpb_fit_simultaneous_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_void_p,
+                                                      C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                                      C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                      C.POINTER(SimResult)]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
 }

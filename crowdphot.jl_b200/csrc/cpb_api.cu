@@ -16,6 +16,7 @@
 namespace cpb {
 
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes) {
+    if (ctx->arena) return arena_carve(ctx->arena, name, bytes);
     auto& b = ctx->bufs[name];
     if (b.bytes >= bytes && b.p) return b.p;
     if (b.p) {

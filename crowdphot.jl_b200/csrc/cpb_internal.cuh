@@ -298,12 +298,23 @@ struct cpb_ctx {
     };
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> event_pool;
+    // When set (only inside cpb_fit_simultaneous_device_noalloc), scratch()
+    // carves buffers from this caller-independent static region instead of
+    // allocating; see cpb_noalloc.cu.
+    struct Arena {
+        char* base = nullptr;
+        size_t cap = 0, used = 0;
+        std::map<std::string, std::pair<size_t, size_t>> slots;  // name -> (offset, bytes)
+    };
+    Arena* arena = nullptr;
 };
 
 namespace cpb {
 
 // Scratch arena: returns a device buffer of at least `bytes` under `name`.
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
+// Carves `bytes` for `name` from a fixed region (no allocation); throws when it is full.
+void* arena_carve(cpb_ctx::Arena* a, const char* name, size_t bytes);
 
 // Brackets one kernel launch: counts it and, when profiling, records CUDA
 // events on the context stream with the launch's algorithmic bytes.

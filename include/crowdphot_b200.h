@@ -265,6 +265,27 @@ CPB_API int cpb_fit_simultaneous_device(cpb_ctx* ctx, const cpb_psf* psf, const 
                                 int64_t n, const double* d_y0, const double* d_x0,
                                 const double* d_flux0, cpb_sim_result* out);
 
+/*
+ * No-allocation form of cpb_fit_simultaneous_device.  It has no counterpart in
+ * the reference: it exists for callers that cannot allocate device memory
+ * while they fit -- code inside a CUDA stream capture, hosts whose device
+ * memory belongs to another allocator's pool, latency-critical loops.  It
+ * allocates nothing: all scratch comes from one static 64 MiB device region
+ * the library holds on each GPU that uses it until the process exits.  Fields
+ * whose scratch would exceed that region (roughly beyond 512 x 512 pixels with
+ * a few thousand 25 x 25 stamps) are rejected with CPB_ERR_ARGUMENT and a
+ * message naming the size.  The first call on a device looks up the region's
+ * address (cudaGetSymbolAddress); make that call before any stream capture.
+ * All calls share the region and find the previous call's contents in it
+ * (the fit clears what must start at zero); calls whose GPU work overlaps
+ * race on it, so serialise them.  The context must already exist.
+ */
+CPB_API int cpb_fit_simultaneous_device_noalloc(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                                                const void* d_image, int32_t eltype, int64_t ny, int64_t nx,
+                                                const void* d_inv_var, const void* d_background, int64_t n,
+                                                const double* d_y0, const double* d_x0, const double* d_flux0,
+                                                cpb_sim_result* out);
+
 /* ---- batched per-star LM (fit_star) ------------------------------------- */
 /*
  * n_cutouts independent fit_star calls.  Cutout c is the column-major block
