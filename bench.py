@@ -221,6 +221,14 @@ def run_gpu(args):
     clk = clocks.stop() if clocks else None
     _, launches = ctx.kernel_stats(reset=True)
     total_s = float(sum(dev_times))
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": fitted_total / total_s, "unit": "stars/s",
+                              "ms_per_step": 1e3 * total_s / args.steps, "gpu_launches": launches,
+                              "config": workload_config(ny, nx, n)}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
     agg = torch.tensor([total_s, float(fitted_total), float(launches)], dtype=torch.float64, device=dev)
     if world > 1:
         mx = agg.clone()
@@ -304,6 +312,8 @@ def main():
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--n-stars", type=int, default=N_STARS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--quick", action="store_true",
+                    help="only the warm-up and timed resident steps (for profiler captures); prints a short line")
     args = ap.parse_args()
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:

@@ -274,6 +274,28 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
             }
             std::vector<float> h32(h64.size());
             for (size_t q = 0; q < h64.size(); ++q) h32[q] = (float)h64[q];
+            // polyphase copies (DevNode): samples regrouped by oversampling phase
+            std::vector<double> pp;
+            for (int k = 0; k < nn; ++k) {
+                DevNode& nd = nodes[k];
+                nd.isy = (int32_t)d->node_os[2 * k + 1];
+                nd.isx = (int32_t)d->node_os[2 * k];
+                nd.PY = (nd.ny + nd.isy - 1) / nd.isy;
+                nd.PX = (nd.nx + nd.isx - 1) / nd.isx;
+                nd.poff = (int64_t)pp.size();
+                const int64_t plane = (int64_t)nd.PY * nd.PX;
+                pp.resize(pp.size() + (size_t)(plane * nd.isy * nd.isx + 3) / 4 * 4, 0.0);
+                for (int64_t kk = 0; kk < nd.nx; ++kk)
+                    for (int64_t ii = 0; ii < nd.ny; ++ii)
+                        pp[nd.poff + ((ii % nd.isy) + (kk % nd.isx) * nd.isy) * plane + ii / nd.isy + (kk / nd.isx) * nd.PY] =
+                            h64[nd.off + ii + kk * nd.ny];
+            }
+            std::vector<float> pp32(pp.size());
+            for (size_t q = 0; q < pp.size(); ++q) pp32[q] = (float)pp[q];
+            check(cudaMalloc(&ps->d_pp64, sizeof(double) * std::max<size_t>(pp.size(), 1)), "cudaMalloc");
+            check(cudaMalloc(&ps->d_pp32, sizeof(float) * std::max<size_t>(pp.size(), 1)), "cudaMalloc");
+            check(cudaMemcpy(ps->d_pp64, pp.data(), sizeof(double) * pp.size(), cudaMemcpyHostToDevice), "h2d");
+            check(cudaMemcpy(ps->d_pp32, pp32.data(), sizeof(float) * pp32.size(), cudaMemcpyHostToDevice), "h2d");
             check(cudaMalloc(&ps->d_data64, sizeof(double) * h64.size()), "cudaMalloc");
             check(cudaMalloc(&ps->d_data32, sizeof(float) * h32.size()), "cudaMalloc");
             check(cudaMalloc(&ps->d_nodes, sizeof(DevNode) * nn), "cudaMalloc");
@@ -291,6 +313,8 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
             dp.gnx = (int32_t)xg.size();
             dp.data64 = ps->d_data64;
             dp.data32 = ps->d_data32;
+            dp.pp64 = ps->d_pp64;
+            dp.pp32 = ps->d_pp32;
             dp.nodes = ps->d_nodes;
             dp.ygrid = ps->d_ygrid;
             dp.xgrid = ps->d_xgrid;
@@ -302,6 +326,8 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
         } catch (...) {
             cudaFree(ps->d_data64);
             cudaFree(ps->d_data32);
+            cudaFree(ps->d_pp64);
+            cudaFree(ps->d_pp32);
             cudaFree(ps->d_nodes);
             cudaFree(ps->d_ygrid);
             cudaFree(ps->d_xgrid);
@@ -320,6 +346,8 @@ int cpb_psf_free(cpb_ctx* ctx, cpb_psf* ps) {
         cudaStreamSynchronize(ctx->stream);
         cudaFree(ps->d_data64);
         cudaFree(ps->d_data32);
+        cudaFree(ps->d_pp64);
+        cudaFree(ps->d_pp32);
         cudaFree(ps->d_nodes);
         cudaFree(ps->d_ygrid);
         cudaFree(ps->d_xgrid);

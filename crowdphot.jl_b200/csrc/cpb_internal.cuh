@@ -28,6 +28,12 @@ struct DevNode {
     double oy, ox;      // origin.y, origin.x
     double sx, sy;      // oversampling x, y
     double fill;
+    // polyphase copy: sample (i, k) (0-based) lives at
+    // poff + ((i % isy) + (k % isx) * isy) * PY * PX + (i / isy) + (k / isx) * PY,
+    // so the samples one stencil tap needs at consecutive stamp rows are adjacent.
+    int64_t poff;
+    int32_t PY, PX;     // ceil(ny / isy), ceil(nx / isx)
+    int32_t isy, isx;   // integer oversampling (the reference's oversampling is a pair of Ints)
 };
 
 constexpr int kMaxNodes = 64;
@@ -39,6 +45,8 @@ struct DevPsf {
     double fwhm;        // CircularGaussianPSF FWHM (the fixed value of the fit)
     const double* data64;
     const float* data32;
+    const double* pp64;       // polyphase copies of the node data (see DevNode)
+    const float* pp32;
     const DevNode* nodes;     // n_nodes
     const double* ygrid;      // gny
     const double* xgrid;      // gnx
@@ -260,6 +268,8 @@ struct cpb_psf {
     cpb::DevPsf dev;
     double* d_data64 = nullptr;
     float* d_data32 = nullptr;
+    double* d_pp64 = nullptr;
+    float* d_pp32 = nullptr;
     cpb::DevNode* d_nodes = nullptr;
     double* d_ygrid = nullptr;
     double* d_xgrid = nullptr;

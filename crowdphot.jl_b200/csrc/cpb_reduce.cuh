@@ -60,10 +60,18 @@ __device__ __forceinline__ bool grid_reduce(double v, Reducer red, double* sh, d
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
+    // L2 reads (ld.global.cg: L1 is not coherent across blocks), eight in flight per thread
     double acc = 0.0;
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += NT) {
-        double pv = ((volatile double*)red.partials)[i];
-        acc = IS_MAX ? nan_max(acc, pv) : acc + pv;
+    const unsigned G = gridDim.x;
+    for (unsigned i0 = threadIdx.x; i0 < G; i0 += 8 * NT) {
+        double pv[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const unsigned i = i0 + k * NT;
+            pv[k] = i < G ? __ldcg(red.partials + i) : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc = IS_MAX ? nan_max(acc, pv[k]) : acc + pv[k];
     }
     double tot = IS_MAX ? block_max<NT>(acc, sh) : block_sum<NT>(acc, sh);
     __shared__ double tot_sh;

@@ -29,9 +29,10 @@
 namespace cpb {
 namespace {
 
-constexpr int TY = 32;   // tile rows (y, contiguous in memory)
-constexpr int TX = 8;    // tile columns
-constexpr int NT = 256;  // threads of the tile kernels (one pixel each)
+constexpr int TY = 32;   // region rows (y, contiguous in memory)
+constexpr int SW = 8;    // columns of one warp's strip
+constexpr int NT = 128;  // threads of the region kernels (4 warps)
+constexpr int TX = SW * (NT / 32);  // region columns
 constexpr double kEps64 = 2.220446049250313e-16;
 
 enum RenderMode { MODE_CUR = 0, MODE_CAND = 1, MODE_FREEZE = 2, MODE_FINAL = 3 };
@@ -203,6 +204,14 @@ __global__ void k_tile_bounds(int64_t npairs, const uint32_t* keys, int32_t* sta
     if (i == npairs - 1 || keys[i + 1] != k) end[k] = (int32_t)(i + 1);
 }
 
+__global__ void k_tile_pack(int64_t npairs, const int32_t* sorted_j, const int32_t* ay, const int32_t* ax,
+                            int4* packed) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= npairs) return;
+    const int j = sorted_j[i];
+    packed[i] = make_int4(j, ay[j], ax[j], 0);
+}
+
 // ---------------------------------------------------------------------------
 // per-iteration kernels
 // ---------------------------------------------------------------------------
@@ -212,6 +221,7 @@ struct FitConst {
     int ky, kx;    // index of y / x in the free list, -1 if fixed
     double fixed_y, fixed_x, fixed_flux, fixed_bkg;
     int R, S, S2, VS;
+    int q32, r32;  // 32 / S and 32 % S: advancing a stamp index by one warp
     int ny, nx;
     int nty, ntx;
 };
@@ -237,138 +247,574 @@ __global__ void k_coef(int64_t n_act, FitConst fc, DevPsf P, const double* theta
     coef[j] = c;
 }
 
-// _fill_stamps! (:342-399, :437-543) for the stars in `list`: one block per
-// star; raw = sqrt(w) * gradient, colnorm = max(||raw||, eps), V = raw / colnorm.
-// When `gram` is non-null it instead accumulates the unscaled p x p Gram
-// block sum(raw raw') per star for the error estimate (:1305-1318).
-template <int NTF, int MAXE>
-__global__ void __launch_bounds__(NTF) k_fill(const int32_t* __restrict__ list, int64_t nlist, FitConst fc, DevPsf P,
+// ---- separable cubic-convolution tables --------------------------------
+// The cubic convolution of empirical_models.jl:185-196 (Keys, a = -1/2) is
+// linear in the four samples: p(t) = sum_c w_c(t) f_c, p'(t) = sum_c d_c(t) f_c.
+// Tabulating these weights once per stamp row and column turns each pixel's
+// bicubic value and both derivatives into 16 sample loads and 44 FMAs.
+__device__ __forceinline__ void keys_weights(double t, double w[4], double d[4]) {
+    const double t2 = t * t, t3 = t2 * t;
+    w[0] = -0.5 * t + t2 - 0.5 * t3;
+    w[1] = 1.0 - 2.5 * t2 + 1.5 * t3;
+    w[2] = 0.5 * t + 2.0 * t2 - 1.5 * t3;
+    w[3] = -0.5 * t2 + 0.5 * t3;
+    d[0] = -0.5 + 2.0 * t - 1.5 * t2;
+    d[1] = -5.0 * t + 4.5 * t2;
+    d[2] = 0.5 + 4.0 * t - 4.5 * t2;
+    d[3] = -t + 1.5 * t2;
+}
+
+// One axis of one node at one stamp row or column: clamped sample offsets
+// (times the axis stride), weights, derivative weights, and the in-bounds
+// half of bicubic_interpolate's `_inbound` test.
+struct AxisTab {
+    double w[4], d[4];
+    int off[4];
+    int inb;
+    int pad;
+};
+
+// Offsets address the node's polyphase copy (DevNode): an axis with integer
+// oversampling s maps the 0-based sample index i to (i % s) * phase_stride +
+// (i / s) * elem_stride, so the row and column parts add to the element offset.
+__device__ __forceinline__ void axis_tab(double coord, int n, int s, int phase_stride, int elem_stride,
+                                         AxisTab& t) {
+    const bool inb = isfinite(coord) && coord >= 1.0 && coord <= (double)n;
+    const double c = inb ? coord : 1.0;
+    const int l = clampi((int)floor(c), 1, n - 1);
+    const double f = c - (double)l;
+    const int i0 = clampi(l - 1, 1, n) - 1, i1 = l - 1, i2 = l, i3 = clampi(l + 2, 1, n) - 1;
+    t.off[0] = (i0 % s) * phase_stride + (i0 / s) * elem_stride;
+    t.off[1] = (i1 % s) * phase_stride + (i1 / s) * elem_stride;
+    t.off[2] = (i2 % s) * phase_stride + (i2 / s) * elem_stride;
+    t.off[3] = (i3 % s) * phase_stride + (i3 / s) * elem_stride;
+    keys_weights(f, t.w, t.d);
+    t.inb = inb;
+}
+__device__ __forceinline__ void axis_tab_x(const DevNode& nd, double u, AxisTab& t) {
+    axis_tab(u, nd.nx, nd.isx, nd.isy * nd.PY * nd.PX, nd.PY, t);
+}
+__device__ __forceinline__ void axis_tab_y(const DevNode& nd, double v, AxisTab& t) {
+    axis_tab(v, nd.ny, nd.isy, nd.PY * nd.PX, 1, t);
+}
+
+// Bicubic value (and d/dv, d/du when GRAD) of one node from its tables.
+template <bool GRAD>
+__device__ __forceinline__ void tab_bicubic(const double* __restrict__ base, const AxisTab& tx, const AxisTab& ty,
+                                            double fill, double& pv, double& pdv, double& pdu) {
+    if (!(tx.inb && ty.inb)) {
+        pv = fill;
+        pdv = 0.0;
+        pdu = 0.0;
+        return;
+    }
+    double rv[4], rd[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const double* row = base + ty.off[r];
+        const double a = __ldg(row + tx.off[0]), b = __ldg(row + tx.off[1]), c = __ldg(row + tx.off[2]),
+                     e = __ldg(row + tx.off[3]);
+        rv[r] = tx.w[0] * a + tx.w[1] * b + tx.w[2] * c + tx.w[3] * e;
+        if (GRAD) rd[r] = tx.d[0] * a + tx.d[1] * b + tx.d[2] * c + tx.d[3] * e;
+    }
+    pv = ty.w[0] * rv[0] + ty.w[1] * rv[1] + ty.w[2] * rv[2] + ty.w[3] * rv[3];
+    if (GRAD) {
+        pdv = ty.d[0] * rv[0] + ty.d[1] * rv[1] + ty.d[2] * rv[2] + ty.d[3] * rv[3];
+        pdu = ty.w[0] * rd[0] + ty.w[1] * rd[1] + ty.w[2] * rd[2] + ty.w[3] * rd[3];
+    }
+}
+
+// Star-parallel stamp evaluation, one block per star of `list` (grid-stride).
+// GRAD (with gram == nullptr): _fill_stamps! (:342-399, :437-543) -- raw =
+//   sqrt(w) * gradient over the fit box, colnorm = max(||raw||, eps),
+//   V = raw * (1 / colnorm); masked and off-image entries are exactly 0.
+// GRAD with gram: the unscaled p x p Gram block sum(raw raw') of the error
+//   estimate (:1305-1318), nothing else written.
+// M != nullptr: the model value flux * s + bkg of every box pixel (the
+//   per-star term of _render_model!, :545-577 / :605-673), box half-width Rb.
+template <int NTF, int MAXE, bool GRAD>
+__global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, int64_t nlist, FitConst fc, DevPsf P,
                                               const StarCoef* __restrict__ coef, const int32_t* __restrict__ ay,
                                               const int32_t* __restrict__ ax, const double* __restrict__ w,
                                               const double* __restrict__ sw, double* __restrict__ V,
-                                              double* __restrict__ colnorm, double* __restrict__ gram) {
+                                              double* __restrict__ colnorm, double* __restrict__ gram,
+                                              double* __restrict__ M, int Rb, int MS) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    AxisTab* tabs = (AxisTab*)smem_raw;  // [corner][axis][Sb]
     __shared__ double sh[32];
-    __shared__ double cn_sh[3];
-    const double* base = P.data64;
+    __shared__ double cn_sh[6];
+    __shared__ StarCoef c;
+    const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
+    const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    const int p = fc.p;
+    const int g0 = fc.gc[0] - 1, g1 = fc.gc[1] - 1, g2 = fc.gc[2] - 1;
     for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int j = list ? list[li] : (int)li;
-        const StarCoef c = coef[j];
+        if (threadIdx.x == 0) c = coef[j];
+        __syncthreads();
         const int a_y = ay[j], a_x = ax[j];
+        if (!gauss) {
+            for (int e = threadIdx.x; e < 8 * Sb; e += NTF) {
+                const int k = e / (2 * Sb), rem = e % (2 * Sb), axis = rem / Sb, idx = rem % Sb;
+                if (c.idx[k] < 0) continue;
+                const DevNode nd = P.nodes[c.idx[k]];
+                if (axis == 0)
+                    axis_tab_x(nd, nd.sx * ((double)(a_x - Rb + idx) - c.x) + nd.ox, tabs[(2 * k) * Sb + idx]);
+                else
+                    axis_tab_y(nd, nd.sy * ((double)(a_y - Rb + idx) - c.y) + nd.oy, tabs[(2 * k + 1) * Sb + idx]);
+            }
+            __syncthreads();
+        }
         double raw[MAXE][3];
         double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int e = 0; e < MAXE; ++e) {
             const int m = threadIdx.x + e * NTF;
             raw[e][0] = raw[e][1] = raw[e][2] = 0.0;
-            if (m >= fc.S2) continue;
-            const int gy = a_y + (m % fc.S) - fc.R, gx = a_x + (m / fc.S) - fc.R;
+            if (m >= S2b) continue;
+            const int row = m % Sb, col = m / Sb;
+            const int gy = a_y - Rb + row, gx = a_x - Rb + col;
+            double s = 0.0, dY = 0.0, dX = 0.0, g[3];
+            if (gauss) {
+                const double val = gauss_eval<double, GRAD>(P.fwhm, c, (double)gy, (double)gx, g[0], g[1], g[2]);
+                if (M) M[(int64_t)j * MS + m] = val;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (c.idx[k] < 0) continue;
+                    const DevNode nd = P.nodes[c.idx[k]];
+                    double pv, pdv, pdu;
+                    tab_bicubic<GRAD>(P.pp64 + nd.poff, tabs[(2 * k) * Sb + col], tabs[(2 * k + 1) * Sb + row],
+                                      nd.fill, pv, pdv, pdu);
+                    s += c.w[k] * pv;
+                    if (GRAD) {
+                        dY += c.dwdy[k] * pv - c.w[k] * nd.sy * pdv;
+                        dX += c.dwdx[k] * pv - c.w[k] * nd.sx * pdu;
+                    }
+                }
+                if (M) M[(int64_t)j * MS + m] = c.flux * s + c.bkg;
+                g[0] = c.flux * dY;
+                g[1] = c.flux * dX;
+                g[2] = s;
+            }
+            if (!GRAD) continue;
             if (gy < 1 || gy > fc.ny || gx < 1 || gx > fc.nx) continue;
             const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
             if (!(w[q] > 0)) continue;
-            double g[3];
-            model_grad<double, double>(P, base, c, (double)gy, (double)gx, g);
-            const double s = sw[q];
-            for (int k = 0; k < fc.p; ++k) raw[e][k] = s * g[fc.gc[k] - 1];
-            if (gram) {
-                int t = 0;
-                for (int k = 0; k < fc.p; ++k)
-                    for (int l = k; l < fc.p; ++l) acc[t++] += raw[e][k] * raw[e][l];
+            const double sq = sw[q];
+            const double ga = g0 == 0 ? g[0] : (g0 == 1 ? g[1] : g[2]);
+            const double gb = g1 == 0 ? g[0] : (g1 == 1 ? g[1] : g[2]);
+            const double gc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
+            raw[e][0] = sq * ga;
+            raw[e][1] = p > 1 ? sq * gb : 0.0;
+            raw[e][2] = p > 2 ? sq * gc : 0.0;
+            if (gram) {  // packed upper triangle (0,0) (0,1) (0,2) (1,1) (1,2) (2,2) for p = 3
+                if (p == 1) {
+                    acc[0] += raw[e][0] * raw[e][0];
+                } else if (p == 2) {
+                    acc[0] += raw[e][0] * raw[e][0];
+                    acc[1] += raw[e][0] * raw[e][1];
+                    acc[2] += raw[e][1] * raw[e][1];
+                } else {
+                    acc[0] += raw[e][0] * raw[e][0];
+                    acc[1] += raw[e][0] * raw[e][1];
+                    acc[2] += raw[e][0] * raw[e][2];
+                    acc[3] += raw[e][1] * raw[e][1];
+                    acc[4] += raw[e][1] * raw[e][2];
+                    acc[5] += raw[e][2] * raw[e][2];
+                }
             } else {
-                for (int k = 0; k < fc.p; ++k) acc[k] += raw[e][k] * raw[e][k];
+                acc[0] += raw[e][0] * raw[e][0];
+                acc[1] += raw[e][1] * raw[e][1];
+                acc[2] += raw[e][2] * raw[e][2];
             }
         }
-        const int nacc = gram ? fc.p * (fc.p + 1) / 2 : fc.p;
-        for (int t = 0; t < nacc; ++t) {
-            double tot = block_sum<NTF>(acc[t], sh);
-            if (threadIdx.x == 0) {
-                if (gram) gram[(int64_t)j * 6 + t] = tot;
-                else cn_sh[t] = tot;
-            }
-        }
-        __syncthreads();
-        if (!gram) {
-            double inv[3];
-            for (int k = 0; k < fc.p; ++k) {
-                double cn = sqrt(cn_sh[k]);
-                cn = cn < kEps64 ? kEps64 : cn;
-                inv[k] = 1.0 / cn;
-                if (threadIdx.x == 0) colnorm[(int64_t)j * fc.p + k] = cn;
-            }
-            double* Vj = V + (int64_t)j * fc.VS;
+        if (GRAD) {
+            const int nacc = gram ? p * (p + 1) / 2 : p;
 #pragma unroll
-            for (int e = 0; e < MAXE; ++e) {
-                const int m = threadIdx.x + e * NTF;
-                if (m >= fc.S2) continue;
-                for (int k = 0; k < fc.p; ++k) Vj[m * fc.p + k] = raw[e][k] * inv[k];
+            for (int t = 0; t < 6; ++t) {
+                if (t >= nacc) break;
+                double tot = block_sum<NTF>(acc[t], sh);
+                if (threadIdx.x == 0) {
+                    if (gram) gram[(int64_t)j * 6 + t] = tot;
+                    else cn_sh[t] = tot;
+                }
+            }
+            __syncthreads();
+            if (!gram) {
+                double inv[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    double cn = sqrt(k < p ? cn_sh[k] : 1.0);
+                    cn = cn < kEps64 ? kEps64 : cn;
+                    inv[k] = 1.0 / cn;
+                    if (threadIdx.x == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
+                }
+                double* Vj = V + (int64_t)j * fc.VS;
+#pragma unroll
+                for (int e = 0; e < MAXE; ++e) {
+                    const int m = threadIdx.x + e * NTF;
+                    if (m >= S2b) continue;
+                    Vj[m * p] = raw[e][0] * inv[0];
+                    if (p > 1) Vj[m * p + 1] = raw[e][1] * inv[1];
+                    if (p > 2) Vj[m * p + 2] = raw[e][2] * inv[2];
+                }
             }
         }
         __syncthreads();
     }
 }
 
-// Model gather over one 32x8 tile: each pixel sums flux*s + bkg over the
-// stars of the tile list that cover it (mode selects the stars and the
-// epilogue).  Replaces the scatter of _render_model! (:545-577, :605-673),
-// _residual_cost! (:675-684), _cost! (:686-693) and _freeze_star! (:739-754).
-template <int MODE>
-__global__ void __launch_bounds__(NT) k_render(FitConst fc, DevPsf P, const int32_t* __restrict__ tstart,
-                                               const int32_t* __restrict__ tend, const int32_t* __restrict__ tlist,
-                                               const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                               const int32_t* __restrict__ Rs, int Rconst,
-                                               const uint8_t* __restrict__ incl, const StarCoef* __restrict__ coef,
-                                               const uint8_t* __restrict__ umask, const double* __restrict__ w,
-                                               const double* __restrict__ sw, const double* __restrict__ data_ref,
-                                               double* __restrict__ out, Reducer red, double* result) {
+// Warp-per-star stamp evaluation for single-node ePSFs and the Gaussian (the
+// common case): no block barriers, each warp keeps its star's row / column
+// tables in its own slice of shared memory, and GRAD runs two passes
+// (colnorm, then the scaled stamp) instead of caching the raw values.
+// Same outputs as k_eval.
+template <bool GRAD>
+__global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+                                                   DevPsf P, const StarCoef* __restrict__ coef,
+                                                   const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
+                                                   const double* __restrict__ w, const double* __restrict__ sw,
+                                                   double* __restrict__ V, double* __restrict__ colnorm,
+                                                   double* __restrict__ gram, double* __restrict__ M, int Rb, int MS) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
+    const int q32 = 32 / Sb, r32 = 32 % Sb;
+    AxisTab* tcol = (AxisTab*)smem_raw + wid * 2 * Sb;
+    AxisTab* trow = tcol + Sb;
+    const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    DevNode nd{};
+    if (!gauss) nd = P.nodes[0];
+    const double* base = gauss ? nullptr : P.pp64 + nd.poff;
+    const int p = fc.p;
+    const int g0 = fc.gc[0] - 1, g1 = fc.gc[1] - 1, g2 = fc.gc[2] - 1;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
+    for (int64_t li = warp; li < nlist; li += nwarps) {
+        const int j = list ? list[li] : (int)li;
+        const StarCoef& cg = coef[j];
+        const double cy = cg.y, cx = cg.x, flux = cg.flux, bkg = cg.bkg;
+        const double w0 = cg.w[0], dwy = cg.dwdy[0], dwx = cg.dwdx[0];
+        const int oy = ay[j] - Rb, ox = ax[j] - Rb;
+        if (!gauss) {
+            for (int idx = lane; idx < 2 * Sb; idx += 32) {
+                if (idx < Sb) axis_tab_x(nd, nd.sx * ((double)(ox + idx) - cx) + nd.ox, tcol[idx]);
+                else axis_tab_y(nd, nd.sy * ((double)(oy + idx - Sb) - cy) + nd.oy, trow[idx - Sb]);
+            }
+            __syncwarp();
+        }
+        StarCoef gc_;
+        if (gauss) {
+            gc_.y = cy;
+            gc_.x = cx;
+            gc_.flux = flux;
+            gc_.bkg = bkg;
+        }
+        // value (and gradient) at stamp entry (row, col)
+        auto eval_px = [&](int row, int col, double& val, double& ga, double& gb, double& gcc) {
+            const double py = (double)(oy + row), px = (double)(ox + col);
+            double g[3];
+            if (gauss) {
+                val = gauss_eval<double, GRAD>(P.fwhm, gc_, py, px, g[0], g[1], g[2]);
+            } else {
+                double pv, pdv = 0.0, pdu = 0.0;
+                tab_bicubic<GRAD>(base, tcol[col], trow[row], nd.fill, pv, pdv, pdu);
+                const double s = w0 * pv;
+                val = flux * s + bkg;
+                if (GRAD) {
+                    g[0] = flux * (dwy * pv - w0 * nd.sy * pdv);
+                    g[1] = flux * (dwx * pv - w0 * nd.sx * pdu);
+                    g[2] = s;
+                }
+            }
+            if (GRAD) {
+                ga = g0 == 0 ? g[0] : (g0 == 1 ? g[1] : g[2]);
+                gb = g1 == 0 ? g[0] : (g1 == 1 ? g[1] : g[2]);
+                gcc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
+            }
+        };
+        if (!GRAD) {
+            int row = lane % Sb, col = lane / Sb;
+            for (int m = lane; m < S2b; m += 32) {
+                double val, a, b, c;
+                eval_px(row, col, val, a, b, c);
+                M[(int64_t)j * MS + m] = val;
+                row += r32;
+                col += q32;
+                if (row >= Sb) {
+                    row -= Sb;
+                    col += 1;
+                }
+            }
+        } else {
+            double acc[6] = {0, 0, 0, 0, 0, 0};
+            int row = lane % Sb, col = lane / Sb;
+            for (int m = lane; m < S2b; m += 32) {
+                const int gy = oy + row, gx = ox + col;
+                if (gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx) {
+                    const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
+                    if (w[q] > 0) {
+                        double val, a, b, c;
+                        eval_px(row, col, val, a, b, c);
+                        const double sq = sw[q];
+                        const double r0 = sq * a, r1 = p > 1 ? sq * b : 0.0, r2 = p > 2 ? sq * c : 0.0;
+                        if (gram) {
+                            acc[0] += r0 * r0;
+                            acc[1] += r0 * r1;
+                            acc[2] += r0 * r2;
+                            acc[3] += r1 * r1;
+                            acc[4] += r1 * r2;
+                            acc[5] += r2 * r2;
+                        } else {
+                            acc[0] += r0 * r0;
+                            acc[1] += r1 * r1;
+                            acc[2] += r2 * r2;
+                        }
+                    }
+                }
+                row += r32;
+                col += q32;
+                if (row >= Sb) {
+                    row -= Sb;
+                    col += 1;
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 6; ++t) acc[t] = warp_sum(acc[t]);
+            if (gram) {
+                if (lane == 0) {
+                    double* gj = gram + (int64_t)j * 6;
+                    if (p == 1) gj[0] = acc[0];
+                    else if (p == 2) {
+                        gj[0] = acc[0];
+                        gj[1] = acc[1];
+                        gj[2] = acc[3];
+                    } else {
+                        for (int t = 0; t < 6; ++t) gj[t] = acc[t];
+                    }
+                }
+            } else {
+                double inv[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    double cn = sqrt(k < p ? acc[k] : 1.0);
+                    cn = cn < kEps64 ? kEps64 : cn;
+                    inv[k] = 1.0 / cn;
+                    if (lane == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
+                }
+                double* Vj = V + (int64_t)j * fc.VS;
+                row = lane % Sb;
+                col = lane / Sb;
+                for (int m = lane; m < S2b; m += 32) {
+                    const int gy = oy + row, gx = ox + col;
+                    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+                    const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
+                    const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
+                    const bool use = onimg && w[q] > 0;
+                    if (use || M) {
+                        double val, a, b, c;
+                        eval_px(row, col, val, a, b, c);
+                        if (M) M[(int64_t)j * MS + m] = val;
+                        if (use) {
+                            const double sq = sw[q];
+                            r0 = sq * a;
+                            r1 = sq * b;
+                            r2 = sq * c;
+                        }
+                    }
+                    Vj[m * p] = r0 * inv[0];
+                    if (p > 1) Vj[m * p + 1] = r1 * inv[1];
+                    if (p > 2) Vj[m * p + 2] = r2 * inv[2];
+                    row += r32;
+                    col += q32;
+                    if (row >= Sb) {
+                        row -= Sb;
+                        col += 1;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Per-region pixel gather over the region's star list (stars in Morton
+// order), the deterministic replacement of the reference's scatter-adds.
+// A block owns a TY x TX pixel region; warp w owns the SW-column strip
+// starting at column w*SW and accumulates it in shared memory.  For each star
+// whose box meets its strip the warp streams the star's stamp entries for
+// those (at most SW) columns -- a contiguous run of the star's block -- and
+// adds them to the strip, one star after another (no atomics, fixed order).
+//   KIND_JV: sum_k V[j, m, k] * v[j, k] / alpha  (apply_J!, :95-137)
+//   KIND_M : sum M[j, m]                         (_render_model!)
+// Epilogues (MODE): LSQR u update + beta (Krylov lsqr step 1); weighted
+// residual + cost (_residual_cost!, :675-684); candidate cost (_cost!,
+// :686-693); freeze subtraction (_freeze_star!, :739-754); final residual.
+constexpr int KIND_JV = 0, KIND_M = 1;
+constexpr int MODE_LSQR = 4;
+
+template <int KIND, int MODE>
+__global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
+                                               const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
+                                               const uint8_t* __restrict__ incl, const double* __restrict__ src,
+                                               int Rb, int64_t stride, const double* __restrict__ vt,
+                                               const double* u_src, double u_sign,
+                                               double* out, const uint8_t* __restrict__ umask,
+                                               const double* __restrict__ w, const double* __restrict__ sw,
+                                               const double* __restrict__ data_ref, Scalars* sc, Reducer red,
+                                               double* result) {
+    __shared__ double s_acc[NT / 32][TY * SW];
+    __shared__ int s_j[NT];
+    __shared__ int s_ay[NT];
+    __shared__ int s_ax[NT];
+    __shared__ double s_v[3][NT];
+    __shared__ int s_wcnt[NT / 32];
     __shared__ double sh[32];
-    const int tile = blockIdx.x;
-    const int ty = tile % fc.nty, tx = tile / fc.nty;
-    const int gy = ty * TY + (threadIdx.x & 31) + 1;
-    const int gx = tx * TX + (threadIdx.x >> 5) + 1;
-    const bool inside = gy <= fc.ny && gx <= fc.nx;
-    const double* base = P.data64;
-    double model = 0.0;
-    const int s0 = tstart[tile], s1 = tend[tile];
-    for (int li = s0; li < s1; ++li) {
-        const int j = tlist[li];
-        if (incl && !incl[j]) continue;
-        const int Rj = Rs ? Rs[j] : Rconst;
-        const int dxo = gx - ax[j];
-        if (dxo < -Rj || dxo > Rj) continue;  // warp-uniform: one column per warp
-        const int dyo = gy - ay[j];
-        if (dyo < -Rj || dyo > Rj || !inside) continue;
-        model += model_value<double, double>(P, base, coef[j], (double)gy, (double)gx);
+    double inv_alpha = 1.0, alpha = 0.0, uscale = 1.0;
+    if (KIND == KIND_JV) {
+        if (sc->stopped) return;  // uniform across the grid
+        inv_alpha = sc->inv_alpha;
+        alpha = sc->alpha;
+        uscale = u_sign * sc->inv_beta;
+    }
+    const int p = KIND == KIND_JV ? fc.p : 1;
+    const int Sb = 2 * Rb + 1;
+    const int reg = blockIdx.x;
+    const int ry = reg % fc.nty, rx = reg / fc.nty;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int y0 = ry * TY + 1, xs0 = rx * TX + wid * SW + 1;
+    const int yend = min(y0 + TY - 1, fc.ny), xend = min(xs0 + SW - 1, fc.nx);
+    double* acc = s_acc[wid];
+    for (int t = lane; t < TY * SW; t += 32) acc[t] = 0.0;
+    const int s0 = tstart[reg], s1 = tend[reg];
+    for (int c0 = s0; c0 < s1; c0 += NT) {
+        const int li = c0 + threadIdx.x;
+        int4 ent = make_int4(-1, 0, 0, 0);
+        bool keep = false;
+        if (li < s1) {
+            ent = tlist[li];
+            keep = incl ? incl[ent.x] != 0 : true;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_wcnt[wid] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+#pragma unroll
+        for (int q = 0; q < NT / 32; ++q) {
+            total += s_wcnt[q];
+            if (q < wid) before += s_wcnt[q];
+        }
+        if (keep) {
+            const int pos = before + __popc(bal & ((1u << lane) - 1u));
+            s_j[pos] = ent.x;
+            s_ay[pos] = ent.y;
+            s_ax[pos] = ent.z;
+            if (KIND == KIND_JV)
+                for (int k = 0; k < fc.p; ++k) s_v[k][pos] = vt[(int64_t)ent.x * fc.p + k] * inv_alpha;
+        }
+        __syncthreads();
+        if (xs0 <= fc.nx) {
+            for (int e = 0; e < total; ++e) {
+                const int ax_ = s_ax[e], ay_ = s_ay[e];
+                const int c_lo = max(ax_ - Rb, xs0), c_hi = min(ax_ + Rb, xend);
+                const int r_lo = max(ay_ - Rb, y0), r_hi = min(ay_ + Rb, yend);
+                if (c_lo > c_hi || r_lo > r_hi) continue;  // warp-uniform
+                const int nrows = r_hi - r_lo + 1;
+                const int tot = nrows * (c_hi - c_lo + 1);
+                const float inv_nrows = 1.0f / (float)nrows;
+                const double* base = src + (int64_t)s_j[e] * stride;
+                const int m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
+                const int a0 = (r_lo - y0) + (c_lo - xs0) * TY;
+                double wv0 = 1.0, wv1 = 0.0, wv2 = 0.0;
+                if (KIND == KIND_JV) {
+                    wv0 = s_v[0][e];
+                    if (p > 1) wv1 = s_v[1][e];
+                    if (p > 2) wv2 = s_v[2][e];
+                }
+                for (int t0 = 0; t0 < tot; t0 += 128) {
+                    double val[4];
+                    int dst[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int t = t0 + lane + 32 * q;
+                        dst[q] = -1;
+                        val[q] = 0.0;
+                        if (t < tot) {
+                            const int cc = (int)(((float)t + 0.5f) * inv_nrows);
+                            const int rr = t - cc * nrows;
+                            const double* ptr = base + (int64_t)(m0 + rr + cc * Sb) * p;
+                            if (KIND == KIND_JV) {
+                                double v = __ldg(ptr) * wv0;
+                                if (p > 1) v += __ldg(ptr + 1) * wv1;
+                                if (p > 2) v += __ldg(ptr + 2) * wv2;
+                                val[q] = v;
+                            } else {
+                                val[q] = __ldg(ptr);
+                            }
+                            dst[q] = a0 + rr + cc * TY;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        if (dst[q] >= 0) acc[dst[q]] += val[q];
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
     }
     double part = 0.0;
-    if (inside) {
+    for (int t = lane; t < TY * SW; t += 32) {
+        const int gy = y0 + (t % TY), gx = xs0 + t / TY;
+        if (gy > fc.ny || gx > fc.nx) continue;
         const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
-        if (MODE == MODE_CUR) {
+        const double a = acc[t];
+        if (MODE == MODE_LSQR) {
+            const double un = a - alpha * (u_src[q] * uscale);
+            out[q] = un;
+            part += un * un;
+        } else if (MODE == MODE_CUR) {
             double wr = 0.0;
             if (umask[q]) {
-                wr = sw[q] * (model - data_ref[q]);
-                part = wr * wr;
+                wr = sw[q] * (a - data_ref[q]);
+                part += wr * wr;
             }
             out[q] = wr;  // wt_resid (zero outside U)
         } else if (MODE == MODE_CAND) {
             if (umask[q]) {
-                double r = model - data_ref[q];
-                part = w[q] * r * r;
+                const double r = a - data_ref[q];
+                part += w[q] * r * r;
             }
         } else if (MODE == MODE_FREEZE) {
-            out[q] -= model;  // data_work
+            out[q] -= a;  // data_work
         } else {
-            out[q] = data_ref[q] - model;  // residual against the original data
+            out[q] = data_ref[q] - a;  // residual against the original data
         }
     }
-    if (MODE == MODE_CUR || MODE == MODE_CAND) grid_reduce<NT>(part, red, sh, result);
+    if (MODE == MODE_LSQR) {
+        double tot;
+        if (grid_reduce<NT>(part, red, sh, &tot) && threadIdx.x == 0) {
+            const double beta = sqrt(tot);
+            sc->beta = beta;
+            if (beta != 0.0) {
+                sc->inv_beta = 1.0 / beta;
+                sc->Anorm2 = sc->Anorm2 + alpha * alpha + beta * beta;
+                if (sc->lambda > 0) sc->Anorm2 += sc->lambda * sc->lambda;
+            }
+        }
+    } else if (MODE == MODE_CUR || MODE == MODE_CAND) {
+        grid_reduce<NT>(part, red, sh, result);
+    }
 }
 
 // J^T u for the stars of `list` (apply_JT!, :55-85): one warp per star,
-// coalesced reads of the star's V block, gathers of u.  Writes z[j*p+k] =
-// scale * sum_m V[j,m,k] u[pix(m)] (u already scaled when uscale != 1).
-// LSQR form (lsqr != 0): v_new = z - beta * v_old * inv_alpha_old, and the
-// grid reduction of ||v_new||^2 gives alpha (Krylov lsqr step 2).
+// coalesced reads of the star's stamp block, gathers of u; stamp indices
+// advance incrementally and four entries per lane are in flight at once.
+// Writes z[j*p+k] = sum_m V[j,m,k] u[pix(m)] * uscale.  LSQR form: v_new =
+// z - beta * v_old / alpha_old and alpha = ||v_new|| (Krylov lsqr step 2).
 template <bool LSQR>
-__global__ void __launch_bounds__(256) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+__global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                             const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
                                             const double* __restrict__ V, const double* __restrict__ u,
                                             double* __restrict__ z, Scalars* sc, Reducer red) {
@@ -383,98 +829,67 @@ __global__ void __launch_bounds__(256) k_JT(const int32_t* __restrict__ list, in
         beta = sc->beta;
         inv_alpha = sc->inv_alpha;
     }
+    const int p = fc.p, S = fc.S, S2 = fc.S2, R = fc.R;
     double part = 0.0;
     for (int64_t li = warp; li < nlist; li += nwarps) {
         const int j = list[li];
-        const int a_y = ay[j], a_x = ax[j];
+        const int a_y = ay[j] - R, a_x = ax[j] - R;
         const double* Vj = V + (int64_t)j * fc.VS;
         double acc0 = 0, acc1 = 0, acc2 = 0;
-        for (int m = lane; m < fc.S2; m += 32) {
-            const int gy = a_y + (m % fc.S) - fc.R, gx = a_x + (m / fc.S) - fc.R;
-            if (gy < 1 || gy > fc.ny || gx < 1 || gx > fc.nx) continue;
-            const double uv = LSQR ? u[(gy - 1) + (int64_t)(gx - 1) * fc.ny] * uscale
-                                   : u[(gy - 1) + (int64_t)(gx - 1) * fc.ny];
-            const double* vm = Vj + m * fc.p;
-            acc0 += vm[0] * uv;
-            if (fc.p > 1) acc1 += vm[1] * uv;
-            if (fc.p > 2) acc2 += vm[2] * uv;
+        int r = lane % S, c = lane / S;
+        for (int m0 = 0; m0 < S2; m0 += 128) {
+            double uv[4], v0[4], v1[4], v2[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int m = m0 + lane + 32 * q;
+                const int gy = a_y + r, gx = a_x + c;
+                const bool ok = m < S2 && gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
+                uv[q] = 0.0;
+                v0[q] = v1[q] = v2[q] = 0.0;
+                if (ok) {
+                    uv[q] = __ldg(u + (gy - 1) + (int64_t)(gx - 1) * fc.ny);
+                    const double* vm = Vj + m * p;
+                    v0[q] = __ldg(vm);
+                    if (p > 1) v1[q] = __ldg(vm + 1);
+                    if (p > 2) v2[q] = __ldg(vm + 2);
+                }
+                r += fc.r32;
+                c += fc.q32;
+                if (r >= S) {
+                    r -= S;
+                    c += 1;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double uq = LSQR ? uv[q] * uscale : uv[q];
+                acc0 += v0[q] * uq;
+                acc1 += v1[q] * uq;
+                acc2 += v2[q] * uq;
+            }
         }
         acc0 = warp_sum(acc0);
         acc1 = warp_sum(acc1);
         acc2 = warp_sum(acc2);
         if (lane == 0) {
-            double a[3] = {acc0, acc1, acc2};
-            for (int k = 0; k < fc.p; ++k) {
-                double val = a[k];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                if (k >= p) break;
+                double val = k == 0 ? acc0 : (k == 1 ? acc1 : acc2);
                 if (LSQR) {
-                    val = val - beta * (z[(int64_t)j * fc.p + k] * inv_alpha);
+                    val = val - beta * (z[(int64_t)j * p + k] * inv_alpha);
                     part += val * val;
                 }
-                z[(int64_t)j * fc.p + k] = val;
+                z[(int64_t)j * p + k] = val;
             }
         }
     }
     if (LSQR) {
         double tot;
         if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) {
-            double alpha = sqrt(tot);
+            const double alpha = sqrt(tot);
             sc->alpha = alpha;
             sc->inv_alpha = alpha != 0.0 ? 1.0 / alpha : 0.0;
-        }
-    }
-}
-
-// J v gather (apply_J!, :95-137) fused with the LSQR update
-// u_new = J v - alpha u (Krylov lsqr step 1) and beta = ||u_new||.
-__global__ void __launch_bounds__(NT) k_Jv(FitConst fc, const int32_t* __restrict__ tstart,
-                                           const int32_t* __restrict__ tend, const int32_t* __restrict__ tlist,
-                                           const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                           const uint8_t* __restrict__ live, const double* __restrict__ V,
-                                           const double* __restrict__ vt, const double* __restrict__ u_src,
-                                           double u_src_scale_sign, double* __restrict__ u_dst, Scalars* sc,
-                                           Reducer red) {
-    __shared__ double sh[32];
-    if (sc->stopped) return;
-    const double inv_alpha = sc->inv_alpha, alpha = sc->alpha;
-    // first iteration reads mrhs = -wt_resid with 1/beta1; later ones u_dst with 1/beta
-    const double uscale = u_src_scale_sign * sc->inv_beta;
-    const int tile = blockIdx.x;
-    const int ty = tile % fc.nty, tx = tile / fc.nty;
-    const int gy = ty * TY + (threadIdx.x & 31) + 1;
-    const int gx = tx * TX + (threadIdx.x >> 5) + 1;
-    const bool inside = gy <= fc.ny && gx <= fc.nx;
-    double acc = 0.0;
-    const int s0 = tstart[tile], s1 = tend[tile];
-    for (int li = s0; li < s1; ++li) {
-        const int j = tlist[li];
-        if (!live[j]) continue;
-        const int dxo = gx - ax[j];
-        if (dxo < -fc.R || dxo > fc.R) continue;
-        const int dyo = gy - ay[j];
-        if (dyo < -fc.R || dyo > fc.R || !inside) continue;
-        const int m = (dyo + fc.R) + (dxo + fc.R) * fc.S;
-        const double* vm = V + (int64_t)j * fc.VS + m * fc.p;
-        const double* vj = vt + (int64_t)j * fc.p;
-        double s = vm[0] * (vj[0] * inv_alpha);
-        if (fc.p > 1) s += vm[1] * (vj[1] * inv_alpha);
-        if (fc.p > 2) s += vm[2] * (vj[2] * inv_alpha);
-        acc += s;
-    }
-    double part = 0.0;
-    if (inside) {
-        const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
-        const double un = acc - alpha * (u_src[q] * uscale);
-        u_dst[q] = un;
-        part = un * un;
-    }
-    double tot;
-    if (grid_reduce<NT>(part, red, sh, &tot) && threadIdx.x == 0) {
-        double beta = sqrt(tot);
-        sc->beta = beta;
-        if (beta != 0.0) {
-            sc->inv_beta = 1.0 / beta;
-            sc->Anorm2 = sc->Anorm2 + alpha * alpha + beta * beta;
-            if (sc->lambda > 0) sc->Anorm2 += sc->lambda * sc->lambda;
         }
     }
 }
@@ -725,11 +1140,6 @@ __global__ void k_freeze_all(int64_t n_act, int iter, uint8_t* live, int32_t* fr
     conv[j] = 1;
 }
 
-__global__ void k_zero_nonlive(int64_t n_act, int p, const uint8_t* live, double* v) {
-    int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (j >= n_act || live[j]) return;
-    for (int k = 0; k < p; ++k) v[j * p + k] = 0.0;
-}
 
 // Per-star p x p covariance from the Gram block (:1305-1329,
 // levenberg_marquardt.jl:366-388): ridge 1e-12 tr, Cholesky inverse,
@@ -925,7 +1335,8 @@ T* S(cpb_ctx* ctx, const char* name, size_t count) {
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
 
 struct TileLists {
-    int32_t *start = nullptr, *end = nullptr, *list = nullptr;
+    int32_t *start = nullptr, *end = nullptr;
+    int4* list = nullptr;  // (star, anchor y, anchor x, 0) per (tile, star) pair
 };
 
 TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_t* ay, const int32_t* ax,
@@ -948,7 +1359,8 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
     uint32_t* k1 = S<uint32_t>(ctx, (t + "_k1").c_str(), npairs);
     int32_t* v0 = S<int32_t>(ctx, (t + "_v0").c_str(), npairs);
     TileLists tl;
-    tl.list = S<int32_t>(ctx, (t + "_list").c_str(), npairs);
+    int32_t* sorted_j = S<int32_t>(ctx, (t + "_sorted").c_str(), npairs);
+    tl.list = S<int4>(ctx, (t + "_list").c_str(), npairs);
     const int64_t ntiles = (int64_t)nty * ntx;
     tl.start = S<int32_t>(ctx, (t + "_start").c_str(), ntiles);
     tl.end = S<int32_t>(ctx, (t + "_end").c_str(), ntiles);
@@ -960,11 +1372,13 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
         int end_bit = 1;
         while ((1LL << end_bit) < ntiles) ++end_bit;
         tmp = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, v0, tl.list, npairs, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, v0, sorted_j, npairs, 0, end_bit, st);
         dtmp = scratch(ctx, (t + "_sort_tmp").c_str(), tmp);
-        cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, tl.list, npairs, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, sorted_j, npairs, 0, end_bit, st);
         k_tile_bounds<<<nblk(npairs), 256, 0, st>>>(npairs, k1, tl.start, tl.end);
         check(cudaGetLastError(), "k_tile_bounds");
+        k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_j, ay, ax, tl.list);
+        check(cudaGetLastError(), "k_tile_pack");
     }
     return tl;
 }
@@ -1048,6 +1462,8 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     fc.S = 2 * fc.R + 1;
     fc.S2 = fc.S * fc.S;
     fc.VS = ((p * fc.S2 + 15) / 16) * 16;
+    fc.q32 = 32 / fc.S;
+    fc.r32 = 32 % fc.S;
     fc.ny = ny;
     fc.nx = nx;
     fc.nty = (ny + TY - 1) / TY;
@@ -1229,52 +1645,84 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     void* live_tmp = scratch(ctx, "live_tmp", live_tmp_bytes);
 
     const int fill_blocks = (int)std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16);
+    // per-star model values of the render box (one block of MS per star)
+    const int Sm = 2 * model_R + 1;
+    const int MS = ((Sm * Sm + 15) / 16) * 16;
+    double* Mbuf = S<double>(ctx, "model_stamps", (int64_t)MS * n_act);
+    int32_t* evlist = S<int32_t>(ctx, "eval_list", n_act);
+    const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab);
+    bool m_fresh = false;  // Mbuf holds the current-theta model of the live stars (written by the fill)
+    const bool warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
+    if (warp_eval && 8 * 2 * std::max(fc.S, Sm) * sizeof(AxisTab) > 48 * 1024)
+        throw ArgError{"fit or model radius too large for the B200 stamp kernels"};
+    auto eval_grid = [&](int64_t nlist) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16)); };
     auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
         if (nlist <= 0) return;
-        unsigned gb = (unsigned)std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16);
-        KernelScope ks_(ctx, gram ? "k_fill_gram" : "k_fill",
-                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * 8 + p * 8) +
-                                         std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1) + fc.S2) * 16 +
+        const bool writeM = !gram && model_R == fc.R;
+        KernelScope ks_(ctx, gram ? "k_eval_gram" : "k_eval_fill",
+                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * 8 + p * 8) + (writeM ? fc.S2 * 8.0 : 0.0) +
+                                         std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1)) * 16 +
                                          sizeof(StarCoef)));
-        if (fc.S2 <= 256 * 2)
-            k_fill<256, 2><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+        const size_t smem = tab_bytes * fc.S;
+        double* Mo = writeM ? Mbuf : nullptr;
+        if (warp_eval) {
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<true><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+        } else if (fc.S2 <= 256 * 2)
+            k_eval<256, 2, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else if (fc.S2 <= 256 * 4)
-            k_fill<256, 4><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+            k_eval<256, 4, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else if (fc.S2 <= 256 * 8)
-            k_fill<256, 8><<<gb, 256, 0, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram);
+            k_eval<256, 8, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else
             throw ArgError{"fit_rad too large for the B200 stamp kernel (ceil(fit_rad) must be <= 22)"};
-        check(cudaGetLastError(), "k_fill");
+        check(cudaGetLastError(), "k_eval_fill");
+        m_fresh = writeM;
     };
     (void)fill_blocks;
-    auto launch_render = [&](int mode, const uint8_t* incl, const StarCoef* cf, double* outp, const double* ref,
-                             double* result) {
+    // model values at `cf` for the stars of `list` into Mbuf (value-only stamp evaluation)
+    auto launch_eval_model = [&](const int32_t* list, int64_t nlist, const StarCoef* cf) {
+        if (nlist <= 0) return;
+        KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * 8 + sizeof(StarCoef)));
+        const size_t smem = tab_bytes * Sm;
+        const unsigned gb = eval_grid(nlist);
+        if (warp_eval) {
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<false><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab), st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+        } else if (Sm * Sm <= 256)
+            k_eval<256, 1, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+        else if (Sm * Sm <= 512)
+            k_eval<256, 2, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+        else if (Sm * Sm <= 1024)
+            k_eval<256, 4, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+        else if (Sm * Sm <= 2048)
+            k_eval<256, 8, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+        else
+            throw ArgError{"model_rad too large for the B200 render kernel (ceil(model_rad) must be <= 22)"};
+        check(cudaGetLastError(), "k_eval_model");
+    };
+    auto launch_render = [&](int mode, const uint8_t* incl, const int32_t* list, int64_t nlist, const StarCoef* cf,
+                             double* outp, const double* ref, double* result) {
+        if (!(mode == MODE_CUR && m_fresh)) launch_eval_model(list, nlist, cf);
+        m_fresh = false;
         const double px_bytes = mode == MODE_CUR ? 25.0 : (mode == MODE_CAND ? 17.0 : 16.0);
-        KernelScope ks_(ctx, mode == MODE_CUR ? "k_render_resid" : (mode == MODE_CAND ? "k_render_cost" :
-                                                   (mode == MODE_FREEZE ? "k_render_freeze" : "k_render_final")),
-                        (double)npix * px_bytes + (double)n_live * sizeof(StarCoef));
+        KernelScope ks_(ctx, mode == MODE_CUR ? "k_gather_resid" : (mode == MODE_CAND ? "k_gather_cost" :
+                                                   (mode == MODE_FREEZE ? "k_gather_freeze" : "k_gather_final")),
+                        (double)npix * px_bytes + (double)nlist * Sm * Sm * 8);
         switch (mode) {
             case MODE_CUR:
-                k_render<MODE_CUR><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
-                                                                    nullptr, model_R, incl, cf, umask, w, sw, ref,
-                                                                    outp, red, result);
+                k_gather<KIND_M, MODE_CUR><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_CAND:
-                k_render<MODE_CAND><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
-                                                                     nullptr, model_R, incl, cf, umask, w, sw, ref,
-                                                                     outp, red, result);
+                k_gather<KIND_M, MODE_CAND><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_FREEZE:
-                k_render<MODE_FREEZE><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay,
-                                                                       ax, nullptr, model_R, incl, cf, umask, w, sw,
-                                                                       ref, outp, red, result);
+                k_gather<KIND_M, MODE_FREEZE><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             default:
-                k_render<MODE_FINAL><<<(unsigned)ntiles, NT, 0, st>>>(fc, dp, tmod.start, tmod.end, tmod.list, ay, ax,
-                                                                      nullptr, model_R, incl, cf, umask, w, sw, ref,
-                                                                      outp, red, result);
+                k_gather<KIND_M, MODE_FINAL><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
         }
-        check(cudaGetLastError(), "k_render");
+        check(cudaGetLastError(), "k_gather");
     };
     auto update_live_list = [&]() {
         cub::DeviceSelect::Flagged(live_tmp, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
@@ -1293,7 +1741,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     // ---- initial fill and cost (:1171-1178)
     KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
     launch_fill(live_list, n_live, nullptr);
-    launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
+    launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
     check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
     evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
     bool fresh = true;  // V / wt_resid / cost are at the current theta and live set
@@ -1306,7 +1754,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
         if (!fresh) {
             KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
             launch_fill(live_list, n_live, nullptr);
-            launch_render(MODE_CUR, live, coef, wt_resid, data_work, &sc->cost);
+            launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
             evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
         }
         fresh = false;
@@ -1361,9 +1809,8 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                 }
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
-                        KernelScope ks_(ctx, "k_Jv", (double)n_live * ((double)p * fc.S2 * 8 + p * 8) + 2.0 * npix * 8);
-                        k_Jv<<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, ay, ax, live, V, vt,
-                                                         it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, sc, red);
+                        KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * 8 + p * 8) + 2.0 * npix * 8);
+                        k_gather<KIND_JV, MODE_LSQR><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
                     }
                     {
                         KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * 8 + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
@@ -1381,7 +1828,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                 k_step<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->max_step, xl, cn, delta, dsc);
             }
             KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
-            launch_render(MODE_CAND, live, coefc, nullptr, data_work, &sc->cost_cand);
+            launch_render(MODE_CAND, live, live_list, n_live, coefc, nullptr, data_work, &sc->cost_cand);
             evals += (double)n_live * (2 * model_R + 1) * (2 * model_R + 1);
             read_scalars();
             n_lsqr += h_sc->iter;
@@ -1420,7 +1867,13 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                 }
                 if (h_new > 0) {
                     KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
-                    launch_render(MODE_FREEZE, newf, coef, data_work, nullptr, nullptr);
+                    {
+                        size_t tb = 0;
+                        cub::DeviceSelect::Flagged(nullptr, tb, iota_act, newf, evlist, d_nlive, (int)n_act, st);
+                        void* tmpb = scratch(ctx, "newf_tmp", tb);
+                        cub::DeviceSelect::Flagged(tmpb, tb, iota_act, newf, evlist, d_nlive, (int)n_act, st);
+                    }
+                    launch_render(MODE_FREEZE, newf, evlist, h_new, coef, data_work, nullptr, nullptr);
                     evals += (double)h_new * (2 * model_R + 1) * (2 * model_R + 1);
                     update_live_list();
                 }
@@ -1447,7 +1900,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     check(cudaGetLastError(), "k_errors");
     // ---- final render against the original data (:1344-1356) and diagnostics
     double* resid = S<double>(ctx, "resid", npix);
-    launch_render(MODE_FINAL, nullptr, coef, resid, data, nullptr);
+    launch_render(MODE_FINAL, nullptr, nullptr, n_act, coef, resid, data, nullptr);
     double* diag = S<double>(ctx, "diag", (int64_t)n_act * 5);
     if (eltype == CPB_F64)
         k_diag<double><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
