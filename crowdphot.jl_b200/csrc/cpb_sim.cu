@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "cpb_internal.cuh"
@@ -252,6 +253,9 @@ __global__ void k_coef(int64_t n_act, FitConst fc, DevPsf P, const double* theta
 // linear in the four samples: p(t) = sum_c w_c(t) f_c, p'(t) = sum_c d_c(t) f_c.
 // Tabulating these weights once per stamp row and column turns each pixel's
 // bicubic value and both derivatives into 16 sample loads and 44 FMAs.
+// T is the arithmetic / storage type of the stamps (double for the plain
+// form, float for the mixed-precision form); positions and weights are
+// always derived in double and rounded once.
 __device__ __forceinline__ void keys_weights(double t, double w[4], double d[4]) {
     const double t2 = t * t, t3 = t2 * t;
     w[0] = -0.5 * t + t2 - 0.5 * t3;
@@ -267,8 +271,9 @@ __device__ __forceinline__ void keys_weights(double t, double w[4], double d[4])
 // One axis of one node at one stamp row or column: clamped sample offsets
 // (times the axis stride), weights, derivative weights, and the in-bounds
 // half of bicubic_interpolate's `_inbound` test.
+template <typename T>
 struct AxisTab {
-    double w[4], d[4];
+    T w[4], d[4];
     int off[4];
     int inb;
     int pad;
@@ -277,8 +282,9 @@ struct AxisTab {
 // Offsets address the node's polyphase copy (DevNode): an axis with integer
 // oversampling s maps the 0-based sample index i to (i % s) * phase_stride +
 // (i / s) * elem_stride, so the row and column parts add to the element offset.
+template <typename T>
 __device__ __forceinline__ void axis_tab(double coord, int n, int s, int phase_stride, int elem_stride,
-                                         AxisTab& t) {
+                                         AxisTab<T>& t) {
     const bool inb = isfinite(coord) && coord >= 1.0 && coord <= (double)n;
     const double c = inb ? coord : 1.0;
     const int l = clampi((int)floor(c), 1, n - 1);
@@ -288,32 +294,47 @@ __device__ __forceinline__ void axis_tab(double coord, int n, int s, int phase_s
     t.off[1] = (i1 % s) * phase_stride + (i1 / s) * elem_stride;
     t.off[2] = (i2 % s) * phase_stride + (i2 / s) * elem_stride;
     t.off[3] = (i3 % s) * phase_stride + (i3 / s) * elem_stride;
-    keys_weights(f, t.w, t.d);
+    double w[4], d[4];
+    keys_weights(f, w, d);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        t.w[k] = (T)w[k];
+        t.d[k] = (T)d[k];
+    }
     t.inb = inb;
 }
-__device__ __forceinline__ void axis_tab_x(const DevNode& nd, double u, AxisTab& t) {
+template <typename T>
+__device__ __forceinline__ void axis_tab_x(const DevNode& nd, double u, AxisTab<T>& t) {
     axis_tab(u, nd.nx, nd.isx, nd.isy * nd.PY * nd.PX, nd.PY, t);
 }
-__device__ __forceinline__ void axis_tab_y(const DevNode& nd, double v, AxisTab& t) {
+template <typename T>
+__device__ __forceinline__ void axis_tab_y(const DevNode& nd, double v, AxisTab<T>& t) {
     axis_tab(v, nd.ny, nd.isy, nd.PY * nd.PX, 1, t);
 }
 
+template <typename T>
+__device__ __forceinline__ const T* pp_data(const DevPsf& P);
+template <>
+__device__ __forceinline__ const double* pp_data<double>(const DevPsf& P) { return P.pp64; }
+template <>
+__device__ __forceinline__ const float* pp_data<float>(const DevPsf& P) { return P.pp32; }
+
 // Bicubic value (and d/dv, d/du when GRAD) of one node from its tables.
-template <bool GRAD>
-__device__ __forceinline__ void tab_bicubic(const double* __restrict__ base, const AxisTab& tx, const AxisTab& ty,
-                                            double fill, double& pv, double& pdv, double& pdu) {
+template <bool GRAD, typename T>
+__device__ __forceinline__ void tab_bicubic(const T* __restrict__ base, const AxisTab<T>& tx, const AxisTab<T>& ty,
+                                            T fill, T& pv, T& pdv, T& pdu) {
     if (!(tx.inb && ty.inb)) {
         pv = fill;
-        pdv = 0.0;
-        pdu = 0.0;
+        pdv = 0;
+        pdu = 0;
         return;
     }
-    double rv[4], rd[4];
+    T rv[4], rd[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const double* row = base + ty.off[r];
-        const double a = __ldg(row + tx.off[0]), b = __ldg(row + tx.off[1]), c = __ldg(row + tx.off[2]),
-                     e = __ldg(row + tx.off[3]);
+        const T* row = base + ty.off[r];
+        const T a = __ldg(row + tx.off[0]), b = __ldg(row + tx.off[1]), c = __ldg(row + tx.off[2]),
+                e = __ldg(row + tx.off[3]);
         rv[r] = tx.w[0] * a + tx.w[1] * b + tx.w[2] * c + tx.w[3] * e;
         if (GRAD) rd[r] = tx.d[0] * a + tx.d[1] * b + tx.d[2] * c + tx.d[3] * e;
     }
@@ -324,7 +345,8 @@ __device__ __forceinline__ void tab_bicubic(const double* __restrict__ base, con
     }
 }
 
-// Star-parallel stamp evaluation, one block per star of `list` (grid-stride).
+// Star-parallel stamp evaluation, one block per star of `list` (grid-stride);
+// the general path (any number of ePSF nodes).
 // GRAD (with gram == nullptr): _fill_stamps! (:342-399, :437-543) -- raw =
 //   sqrt(w) * gradient over the fit box, colnorm = max(||raw||, eps),
 //   V = raw * (1 / colnorm); masked and off-image entries are exactly 0.
@@ -332,15 +354,16 @@ __device__ __forceinline__ void tab_bicubic(const double* __restrict__ base, con
 //   estimate (:1305-1318), nothing else written.
 // M != nullptr: the model value flux * s + bkg of every box pixel (the
 //   per-star term of _render_model!, :545-577 / :605-673), box half-width Rb.
-template <int NTF, int MAXE, bool GRAD>
+// Sums of squares and Gram entries accumulate in double for either T.
+template <int NTF, int MAXE, bool GRAD, typename T>
 __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, int64_t nlist, FitConst fc, DevPsf P,
                                               const StarCoef* __restrict__ coef, const int32_t* __restrict__ ay,
                                               const int32_t* __restrict__ ax, const double* __restrict__ w,
-                                              const double* __restrict__ sw, double* __restrict__ V,
+                                              const double* __restrict__ sw, T* __restrict__ V,
                                               double* __restrict__ colnorm, double* __restrict__ gram,
-                                              double* __restrict__ M, int Rb, int MS) {
+                                              T* __restrict__ M, int Rb, int MS) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    AxisTab* tabs = (AxisTab*)smem_raw;  // [corner][axis][Sb]
+    AxisTab<T>* tabs = (AxisTab<T>*)smem_raw;  // [corner][axis][Sb]
     __shared__ double sh[32];
     __shared__ double cn_sh[6];
     __shared__ StarCoef c;
@@ -348,6 +371,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
     const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     const int p = fc.p;
     const int g0 = fc.gc[0] - 1, g1 = fc.gc[1] - 1, g2 = fc.gc[2] - 1;
+    const T* data = pp_data<T>(P);
     for (int64_t li = blockIdx.x; li < nlist; li += gridDim.x) {
         const int j = list ? list[li] : (int)li;
         if (threadIdx.x == 0) c = coef[j];
@@ -365,68 +389,69 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             }
             __syncthreads();
         }
-        double raw[MAXE][3];
+        T raw[MAXE][3];
         double acc[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int e = 0; e < MAXE; ++e) {
             const int m = threadIdx.x + e * NTF;
-            raw[e][0] = raw[e][1] = raw[e][2] = 0.0;
+            raw[e][0] = raw[e][1] = raw[e][2] = 0;
             if (m >= S2b) continue;
             const int row = m % Sb, col = m / Sb;
             const int gy = a_y - Rb + row, gx = a_x - Rb + col;
-            double s = 0.0, dY = 0.0, dX = 0.0, g[3];
+            T s = 0, dY = 0, dX = 0, g[3];
             if (gauss) {
-                const double val = gauss_eval<double, GRAD>(P.fwhm, c, (double)gy, (double)gx, g[0], g[1], g[2]);
+                const T val = gauss_eval<T, GRAD>((T)P.fwhm, c, (T)gy, (T)gx, g[0], g[1], g[2]);
                 if (M) M[(int64_t)j * MS + m] = val;
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (c.idx[k] < 0) continue;
                     const DevNode nd = P.nodes[c.idx[k]];
-                    double pv, pdv, pdu;
-                    tab_bicubic<GRAD>(P.pp64 + nd.poff, tabs[(2 * k) * Sb + col], tabs[(2 * k + 1) * Sb + row],
-                                      nd.fill, pv, pdv, pdu);
-                    s += c.w[k] * pv;
+                    T pv, pdv, pdu;
+                    tab_bicubic<GRAD, T>(data + nd.poff, tabs[(2 * k) * Sb + col], tabs[(2 * k + 1) * Sb + row],
+                                         (T)nd.fill, pv, pdv, pdu);
+                    s += (T)c.w[k] * pv;
                     if (GRAD) {
-                        dY += c.dwdy[k] * pv - c.w[k] * nd.sy * pdv;
-                        dX += c.dwdx[k] * pv - c.w[k] * nd.sx * pdu;
+                        dY += (T)c.dwdy[k] * pv - (T)c.w[k] * (T)nd.sy * pdv;
+                        dX += (T)c.dwdx[k] * pv - (T)c.w[k] * (T)nd.sx * pdu;
                     }
                 }
-                if (M) M[(int64_t)j * MS + m] = c.flux * s + c.bkg;
-                g[0] = c.flux * dY;
-                g[1] = c.flux * dX;
+                if (M) M[(int64_t)j * MS + m] = (T)c.flux * s + (T)c.bkg;
+                g[0] = (T)c.flux * dY;
+                g[1] = (T)c.flux * dX;
                 g[2] = s;
             }
             if (!GRAD) continue;
             if (gy < 1 || gy > fc.ny || gx < 1 || gx > fc.nx) continue;
             const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
             if (!(w[q] > 0)) continue;
-            const double sq = sw[q];
-            const double ga = g0 == 0 ? g[0] : (g0 == 1 ? g[1] : g[2]);
-            const double gb = g1 == 0 ? g[0] : (g1 == 1 ? g[1] : g[2]);
-            const double gc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
+            const T sq = (T)sw[q];
+            const T ga = g0 == 0 ? g[0] : (g0 == 1 ? g[1] : g[2]);
+            const T gb = g1 == 0 ? g[0] : (g1 == 1 ? g[1] : g[2]);
+            const T gc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
             raw[e][0] = sq * ga;
-            raw[e][1] = p > 1 ? sq * gb : 0.0;
-            raw[e][2] = p > 2 ? sq * gc : 0.0;
+            raw[e][1] = p > 1 ? sq * gb : (T)0;
+            raw[e][2] = p > 2 ? sq * gc : (T)0;
+            const double r0 = raw[e][0], r1 = raw[e][1], r2 = raw[e][2];
             if (gram) {  // packed upper triangle (0,0) (0,1) (0,2) (1,1) (1,2) (2,2) for p = 3
                 if (p == 1) {
-                    acc[0] += raw[e][0] * raw[e][0];
+                    acc[0] += r0 * r0;
                 } else if (p == 2) {
-                    acc[0] += raw[e][0] * raw[e][0];
-                    acc[1] += raw[e][0] * raw[e][1];
-                    acc[2] += raw[e][1] * raw[e][1];
+                    acc[0] += r0 * r0;
+                    acc[1] += r0 * r1;
+                    acc[2] += r1 * r1;
                 } else {
-                    acc[0] += raw[e][0] * raw[e][0];
-                    acc[1] += raw[e][0] * raw[e][1];
-                    acc[2] += raw[e][0] * raw[e][2];
-                    acc[3] += raw[e][1] * raw[e][1];
-                    acc[4] += raw[e][1] * raw[e][2];
-                    acc[5] += raw[e][2] * raw[e][2];
+                    acc[0] += r0 * r0;
+                    acc[1] += r0 * r1;
+                    acc[2] += r0 * r2;
+                    acc[3] += r1 * r1;
+                    acc[4] += r1 * r2;
+                    acc[5] += r2 * r2;
                 }
             } else {
-                acc[0] += raw[e][0] * raw[e][0];
-                acc[1] += raw[e][1] * raw[e][1];
-                acc[2] += raw[e][2] * raw[e][2];
+                acc[0] += r0 * r0;
+                acc[1] += r1 * r1;
+                acc[2] += r2 * r2;
             }
         }
         if (GRAD) {
@@ -442,15 +467,15 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             }
             __syncthreads();
             if (!gram) {
-                double inv[3];
+                T inv[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     double cn = sqrt(k < p ? cn_sh[k] : 1.0);
                     cn = cn < kEps64 ? kEps64 : cn;
-                    inv[k] = 1.0 / cn;
+                    inv[k] = (T)(1.0 / cn);
                     if (threadIdx.x == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
                 }
-                double* Vj = V + (int64_t)j * fc.VS;
+                T* Vj = V + (int64_t)j * fc.VS;
 #pragma unroll
                 for (int e = 0; e < MAXE; ++e) {
                     const int m = threadIdx.x + e * NTF;
@@ -470,23 +495,24 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
 // tables in its own slice of shared memory, and GRAD runs two passes
 // (colnorm, then the scaled stamp) instead of caching the raw values.
 // Same outputs as k_eval.
-template <bool GRAD>
+template <bool GRAD, typename T>
 __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
-                                                   DevPsf P, const StarCoef* __restrict__ coef,
-                                                   const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                                   const double* __restrict__ w, const double* __restrict__ sw,
-                                                   double* __restrict__ V, double* __restrict__ colnorm,
-                                                   double* __restrict__ gram, double* __restrict__ M, int Rb, int MS) {
+                                                      DevPsf P, const StarCoef* __restrict__ coef,
+                                                      const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
+                                                      const double* __restrict__ w, const double* __restrict__ sw,
+                                                      T* __restrict__ V, double* __restrict__ colnorm,
+                                                      double* __restrict__ gram, T* __restrict__ M, int Rb, int MS) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
     const int q32 = 32 / Sb, r32 = 32 % Sb;
-    AxisTab* tcol = (AxisTab*)smem_raw + wid * 2 * Sb;
-    AxisTab* trow = tcol + Sb;
+    AxisTab<T>* tcol = (AxisTab<T>*)smem_raw + wid * 2 * Sb;
+    AxisTab<T>* trow = tcol + Sb;
     const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     DevNode nd{};
     if (!gauss) nd = P.nodes[0];
-    const double* base = gauss ? nullptr : P.pp64 + nd.poff;
+    const T* base = gauss ? nullptr : pp_data<T>(P) + nd.poff;
+    const T nfill = (T)nd.fill, nsy = (T)nd.sy, nsx = (T)nd.sx;
     const int p = fc.p;
     const int g0 = fc.gc[0] - 1, g1 = fc.gc[1] - 1, g2 = fc.gc[2] - 1;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -494,8 +520,9 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
     for (int64_t li = warp; li < nlist; li += nwarps) {
         const int j = list ? list[li] : (int)li;
         const StarCoef& cg = coef[j];
-        const double cy = cg.y, cx = cg.x, flux = cg.flux, bkg = cg.bkg;
-        const double w0 = cg.w[0], dwy = cg.dwdy[0], dwx = cg.dwdx[0];
+        const double cy = cg.y, cx = cg.x;
+        const T flux = (T)cg.flux, bkg = (T)cg.bkg;
+        const T w0 = (T)cg.w[0], dwy = (T)cg.dwdy[0], dwx = (T)cg.dwdx[0];
         const int oy = ay[j] - Rb, ox = ax[j] - Rb;
         if (!gauss) {
             for (int idx = lane; idx < 2 * Sb; idx += 32) {
@@ -508,23 +535,22 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         if (gauss) {
             gc_.y = cy;
             gc_.x = cx;
-            gc_.flux = flux;
-            gc_.bkg = bkg;
+            gc_.flux = cg.flux;
+            gc_.bkg = cg.bkg;
         }
         // value (and gradient) at stamp entry (row, col)
-        auto eval_px = [&](int row, int col, double& val, double& ga, double& gb, double& gcc) {
-            const double py = (double)(oy + row), px = (double)(ox + col);
-            double g[3];
+        auto eval_px = [&](int row, int col, T& val, T& ga, T& gb, T& gcc) {
+            T g[3];
             if (gauss) {
-                val = gauss_eval<double, GRAD>(P.fwhm, gc_, py, px, g[0], g[1], g[2]);
+                val = gauss_eval<T, GRAD>((T)P.fwhm, gc_, (T)(oy + row), (T)(ox + col), g[0], g[1], g[2]);
             } else {
-                double pv, pdv = 0.0, pdu = 0.0;
-                tab_bicubic<GRAD>(base, tcol[col], trow[row], nd.fill, pv, pdv, pdu);
-                const double s = w0 * pv;
+                T pv, pdv = 0, pdu = 0;
+                tab_bicubic<GRAD, T>(base, tcol[col], trow[row], nfill, pv, pdv, pdu);
+                const T s = w0 * pv;
                 val = flux * s + bkg;
                 if (GRAD) {
-                    g[0] = flux * (dwy * pv - w0 * nd.sy * pdv);
-                    g[1] = flux * (dwx * pv - w0 * nd.sx * pdu);
+                    g[0] = flux * (dwy * pv - w0 * nsy * pdv);
+                    g[1] = flux * (dwx * pv - w0 * nsx * pdu);
                     g[2] = s;
                 }
             }
@@ -537,7 +563,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         if (!GRAD) {
             int row = lane % Sb, col = lane / Sb;
             for (int m = lane; m < S2b; m += 32) {
-                double val, a, b, c;
+                T val, a, b, c;
                 eval_px(row, col, val, a, b, c);
                 M[(int64_t)j * MS + m] = val;
                 row += r32;
@@ -555,10 +581,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 if (gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx) {
                     const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
                     if (w[q] > 0) {
-                        double val, a, b, c;
+                        T val, a, b, c;
                         eval_px(row, col, val, a, b, c);
-                        const double sq = sw[q];
-                        const double r0 = sq * a, r1 = p > 1 ? sq * b : 0.0, r2 = p > 2 ? sq * c : 0.0;
+                        const T sq = (T)sw[q];
+                        const double r0 = sq * a, r1 = p > 1 ? (double)(sq * b) : 0.0,
+                                     r2 = p > 2 ? (double)(sq * c) : 0.0;
                         if (gram) {
                             acc[0] += r0 * r0;
                             acc[1] += r0 * r1;
@@ -595,29 +622,29 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     }
                 }
             } else {
-                double inv[3];
+                T inv[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     double cn = sqrt(k < p ? acc[k] : 1.0);
                     cn = cn < kEps64 ? kEps64 : cn;
-                    inv[k] = 1.0 / cn;
+                    inv[k] = (T)(1.0 / cn);
                     if (lane == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
                 }
-                double* Vj = V + (int64_t)j * fc.VS;
+                T* Vj = V + (int64_t)j * fc.VS;
                 row = lane % Sb;
                 col = lane / Sb;
                 for (int m = lane; m < S2b; m += 32) {
                     const int gy = oy + row, gx = ox + col;
-                    double r0 = 0.0, r1 = 0.0, r2 = 0.0;
+                    T r0 = 0, r1 = 0, r2 = 0;
                     const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
                     const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
                     const bool use = onimg && w[q] > 0;
                     if (use || M) {
-                        double val, a, b, c;
+                        T val, a, b, c;
                         eval_px(row, col, val, a, b, c);
                         if (M) M[(int64_t)j * MS + m] = val;
                         if (use) {
-                            const double sq = sw[q];
+                            const T sq = (T)sw[q];
                             r0 = sq * a;
                             r1 = sq * b;
                             r2 = sq * c;
@@ -654,10 +681,10 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 constexpr int KIND_JV = 0, KIND_M = 1;
 constexpr int MODE_LSQR = 4;
 
-template <int KIND, int MODE>
+template <int KIND, int MODE, typename TS>
 __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
-                                               const uint8_t* __restrict__ incl, const double* __restrict__ src,
+                                               const uint8_t* __restrict__ incl, const TS* __restrict__ src,
                                                int Rb, int64_t stride, const double* __restrict__ vt,
                                                const double* u_src, double u_sign,
                                                double* out, const uint8_t* __restrict__ umask,
@@ -723,7 +750,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                 const int nrows = r_hi - r_lo + 1;
                 const int tot = nrows * (c_hi - c_lo + 1);
                 const float inv_nrows = 1.0f / (float)nrows;
-                const double* base = src + (int64_t)s_j[e] * stride;
+                const TS* base = src + (int64_t)s_j[e] * stride;
                 const int m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
                 const int a0 = (r_lo - y0) + (c_lo - xs0) * TY;
                 double wv0 = 1.0, wv1 = 0.0, wv2 = 0.0;
@@ -743,14 +770,14 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                         if (t < tot) {
                             const int cc = (int)(((float)t + 0.5f) * inv_nrows);
                             const int rr = t - cc * nrows;
-                            const double* ptr = base + (int64_t)(m0 + rr + cc * Sb) * p;
+                            const TS* ptr = base + (int64_t)(m0 + rr + cc * Sb) * p;
                             if (KIND == KIND_JV) {
-                                double v = __ldg(ptr) * wv0;
-                                if (p > 1) v += __ldg(ptr + 1) * wv1;
-                                if (p > 2) v += __ldg(ptr + 2) * wv2;
+                                double v = (double)__ldg(ptr) * wv0;
+                                if (p > 1) v += (double)__ldg(ptr + 1) * wv1;
+                                if (p > 2) v += (double)__ldg(ptr + 2) * wv2;
                                 val[q] = v;
                             } else {
-                                val[q] = __ldg(ptr);
+                                val[q] = (double)__ldg(ptr);
                             }
                             dst[q] = a0 + rr + cc * TY;
                         }
@@ -813,10 +840,10 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
 // advance incrementally and four entries per lane are in flight at once.
 // Writes z[j*p+k] = sum_m V[j,m,k] u[pix(m)] * uscale.  LSQR form: v_new =
 // z - beta * v_old / alpha_old and alpha = ||v_new|| (Krylov lsqr step 2).
-template <bool LSQR>
+template <bool LSQR, typename TS>
 __global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                             const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                            const double* __restrict__ V, const double* __restrict__ u,
+                                            const TS* __restrict__ V, const double* __restrict__ u,
                                             double* __restrict__ z, Scalars* sc, Reducer red) {
     __shared__ double sh[32];
     const int lane = threadIdx.x & 31;
@@ -834,7 +861,7 @@ __global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list,
     for (int64_t li = warp; li < nlist; li += nwarps) {
         const int j = list[li];
         const int a_y = ay[j] - R, a_x = ax[j] - R;
-        const double* Vj = V + (int64_t)j * fc.VS;
+        const TS* Vj = V + (int64_t)j * fc.VS;
         double acc0 = 0, acc1 = 0, acc2 = 0;
         int r = lane % S, c = lane / S;
         for (int m0 = 0; m0 < S2; m0 += 128) {
@@ -848,10 +875,10 @@ __global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list,
                 v0[q] = v1[q] = v2[q] = 0.0;
                 if (ok) {
                     uv[q] = __ldg(u + (gy - 1) + (int64_t)(gx - 1) * fc.ny);
-                    const double* vm = Vj + m * p;
-                    v0[q] = __ldg(vm);
-                    if (p > 1) v1[q] = __ldg(vm + 1);
-                    if (p > 2) v2[q] = __ldg(vm + 2);
+                    const TS* vm = Vj + m * p;
+                    v0[q] = (double)__ldg(vm);
+                    if (p > 1) v1[q] = (double)__ldg(vm + 1);
+                    if (p > 2) v2[q] = (double)__ldg(vm + 2);
                 }
                 r += fc.r32;
                 c += fc.q32;
@@ -1388,7 +1415,8 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
 // ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
-int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
+template <typename TS>
+int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
                          int32_t eltype, int64_t ny64, int64_t nx64, const void* d_inv_var, const void* d_background,
                          int64_t n_stars, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out) {
@@ -1412,7 +1440,6 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     if (!(P->fit_rad > 0)) throw ArgError{"fit_rad must be positive"};
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
     if (ny64 <= 0 || nx64 <= 0 || ny64 * nx64 >= (1LL << 31)) throw ArgError{"image size out of range"};
-    if (P->precision != CPB_PREC_FP64) throw ArgError{"only the FP64 precision form is built for the simultaneous fit"};
     const int ny = (int)ny64, nx = (int)nx64;
     const int64_t npix = ny64 * nx64;
     const bool reweighted =
@@ -1612,7 +1639,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                                      : build_tiles(ctx, "tmod", n_act, ay, ax, nullptr, model_R, ny, nx, fc.nty, fc.ntx);
 
     // ---- working buffers (:1129-1166)
-    double* V = S<double>(ctx, "V", (int64_t)fc.VS * n_act);
+    TS* V = S<TS>(ctx, "V", (int64_t)fc.VS * n_act);
     double* cn = S<double>(ctx, "colnorm", n);
     double* D = S<double>(ctx, "D", n);
     double* bsc = S<double>(ctx, "b_scaled", n);
@@ -1636,7 +1663,7 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     check(cudaMemsetAsync(conv, 0, n_act, st), "memset");
     check(cudaMemsetAsync(frozen_at, 0, sizeof(int32_t) * n_act, st), "memset");
     check(cudaMemsetAsync(cn, 0, sizeof(double) * n, st), "memset");
-    check(cudaMemsetAsync(V, 0, sizeof(double) * (int64_t)fc.VS * n_act, st), "memset");
+    check(cudaMemsetAsync(V, 0, sizeof(TS) * (int64_t)fc.VS * n_act, st), "memset");
     check(cudaMemcpyAsync(iota_act, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
     int64_t n_live = n_act;
     check(cudaMemcpyAsync(live_list, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
@@ -1648,32 +1675,33 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     // per-star model values of the render box (one block of MS per star)
     const int Sm = 2 * model_R + 1;
     const int MS = ((Sm * Sm + 15) / 16) * 16;
-    double* Mbuf = S<double>(ctx, "model_stamps", (int64_t)MS * n_act);
+    TS* Mbuf = S<TS>(ctx, "model_stamps", (int64_t)MS * n_act);
+    constexpr double bts = sizeof(TS);  // bytes per stored stamp / model value
     int32_t* evlist = S<int32_t>(ctx, "eval_list", n_act);
-    const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab);
+    const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
     bool m_fresh = false;  // Mbuf holds the current-theta model of the live stars (written by the fill)
     const bool warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
-    if (warp_eval && 8 * 2 * std::max(fc.S, Sm) * sizeof(AxisTab) > 48 * 1024)
+    if (warp_eval && 8 * 2 * std::max(fc.S, Sm) * sizeof(AxisTab<double>) > 48 * 1024)
         throw ArgError{"fit or model radius too large for the B200 stamp kernels"};
     auto eval_grid = [&](int64_t nlist) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16)); };
     auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
         if (nlist <= 0) return;
         const bool writeM = !gram && model_R == fc.R;
         KernelScope ks_(ctx, gram ? "k_eval_gram" : "k_eval_fill",
-                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * 8 + p * 8) + (writeM ? fc.S2 * 8.0 : 0.0) +
+                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * bts + p * 8) + (writeM ? fc.S2 * bts : 0.0) +
                                          std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1)) * 16 +
                                          sizeof(StarCoef)));
         const size_t smem = tab_bytes * fc.S;
-        double* Mo = writeM ? Mbuf : nullptr;
+        TS* Mo = writeM ? Mbuf : nullptr;
         if (warp_eval) {
             const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval_warp<true, TS><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         } else if (fc.S2 <= 256 * 2)
-            k_eval<256, 2, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 2, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else if (fc.S2 <= 256 * 4)
-            k_eval<256, 4, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 4, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else if (fc.S2 <= 256 * 8)
-            k_eval<256, 8, true><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 8, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
         else
             throw ArgError{"fit_rad too large for the B200 stamp kernel (ceil(fit_rad) must be <= 22)"};
         check(cudaGetLastError(), "k_eval_fill");
@@ -1683,20 +1711,20 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     // model values at `cf` for the stars of `list` into Mbuf (value-only stamp evaluation)
     auto launch_eval_model = [&](const int32_t* list, int64_t nlist, const StarCoef* cf) {
         if (nlist <= 0) return;
-        KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * 8 + sizeof(StarCoef)));
+        KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * bts + sizeof(StarCoef)));
         const size_t smem = tab_bytes * Sm;
         const unsigned gb = eval_grid(nlist);
         if (warp_eval) {
             const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<false><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab), st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval_warp<false, TS><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
         } else if (Sm * Sm <= 256)
-            k_eval<256, 1, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 1, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
         else if (Sm * Sm <= 512)
-            k_eval<256, 2, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 2, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
         else if (Sm * Sm <= 1024)
-            k_eval<256, 4, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 4, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
         else if (Sm * Sm <= 2048)
-            k_eval<256, 8, false><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 8, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
         else
             throw ArgError{"model_rad too large for the B200 render kernel (ceil(model_rad) must be <= 22)"};
         check(cudaGetLastError(), "k_eval_model");
@@ -1708,19 +1736,19 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
         const double px_bytes = mode == MODE_CUR ? 25.0 : (mode == MODE_CAND ? 17.0 : 16.0);
         KernelScope ks_(ctx, mode == MODE_CUR ? "k_gather_resid" : (mode == MODE_CAND ? "k_gather_cost" :
                                                    (mode == MODE_FREEZE ? "k_gather_freeze" : "k_gather_final")),
-                        (double)npix * px_bytes + (double)nlist * Sm * Sm * 8);
+                        (double)npix * px_bytes + (double)nlist * Sm * Sm * bts);
         switch (mode) {
             case MODE_CUR:
-                k_gather<KIND_M, MODE_CUR><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_CAND:
-                k_gather<KIND_M, MODE_CAND><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_FREEZE:
-                k_gather<KIND_M, MODE_FREEZE><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             default:
-                k_gather<KIND_M, MODE_FINAL><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
         }
         check(cudaGetLastError(), "k_gather");
     };
@@ -1761,8 +1789,8 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
         // b_scaled = J' wt_resid (frozen stars stay 0)
         check(cudaMemsetAsync(bsc, 0, sizeof(double) * n, st), "memset");
         {
-            KernelScope ks_(ctx, "k_JT", (double)n_live * ((double)p * fc.S2 * 8 + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
-            k_JT<false><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
+            KernelScope ks_(ctx, "k_JT", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
+            k_JT<false, TS><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
         }
         check(cudaGetLastError(), "k_JT");
         macs += (double)n_live * fc.S2;
@@ -1809,12 +1837,12 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                 }
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
-                        KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * 8 + p * 8) + 2.0 * npix * 8);
-                        k_gather<KIND_JV, MODE_LSQR><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
+                        KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * 8);
+                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
                     }
                     {
-                        KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * 8 + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
-                        k_JT<true><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
+                        KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
+                        k_JT<true, TS><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
                     }
                     {
                         KernelScope ks_(ctx, "k_lsqr_update", (double)n * 8 * 5);
@@ -1893,14 +1921,56 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     // ---- errors at the final theta, every active star (:1302-1329)
     KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
     double* gram = S<double>(ctx, "gram", (int64_t)n_act * 6);
-    launch_fill(nullptr, n_act, gram);
+    // the final pass (errors, residual, diagnostics) is FP64 for either precision form
+    {
+        KernelScope ks_(ctx, "k_eval_gram", (double)n_act * (48.0 + sizeof(StarCoef)));
+        if (warp_eval) {
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<true, double><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<double>), st>>>(
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+        } else if (fc.S2 <= 256 * 2) {
+            k_eval<256, 2, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+        } else if (fc.S2 <= 256 * 4) {
+            k_eval<256, 4, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+        } else {
+            k_eval<256, 8, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+        }
+        check(cudaGetLastError(), "k_eval_gram");
+    }
     double* err = S<double>(ctx, "err", n);
     read_scalars();  // final cost
     k_errors<<<nblk(n_act), 256, 0, st>>>(n_act, p, gram, reweighted, dof, sc, err);
     check(cudaGetLastError(), "k_errors");
     // ---- final render against the original data (:1344-1356) and diagnostics
     double* resid = S<double>(ctx, "resid", npix);
-    launch_render(MODE_FINAL, nullptr, nullptr, n_act, coef, resid, data, nullptr);
+    {
+        double* M64 = std::is_same<TS, double>::value ? (double*)Mbuf : S<double>(ctx, "model_stamps64", (int64_t)MS * n_act);
+        {
+            KernelScope ks_(ctx, "k_eval_model", (double)n_act * ((double)Sm * Sm * 8 + sizeof(StarCoef)));
+            if (warp_eval) {
+                const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
+                k_eval_warp<false, double><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab<double>), st>>>(
+                    nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+            } else {
+                const size_t sm_ = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * Sm;
+                if (Sm * Sm <= 256)
+                    k_eval<256, 1, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                else if (Sm * Sm <= 512)
+                    k_eval<256, 2, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                else if (Sm * Sm <= 1024)
+                    k_eval<256, 4, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                else
+                    k_eval<256, 8, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+            }
+            check(cudaGetLastError(), "k_eval_model");
+        }
+        KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
+        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
+        check(cudaGetLastError(), "k_gather_final");
+    }
     double* diag = S<double>(ctx, "diag", (int64_t)n_act * 5);
     if (eltype == CPB_F64)
         k_diag<double><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
@@ -2007,6 +2077,18 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     out->model_px_evals = evals;
     out->lsqr_px_macs = macs;
     return 0;
+}
+
+int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
+                         int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var, const void* d_background,
+                         int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
+                         cpb_sim_result* out) {
+    if (P->precision == CPB_PREC_MIXED)
+        return fit_sim_impl<float>(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0,
+                                   d_flux0, out);
+    if (P->precision != CPB_PREC_FP64) throw ArgError{"precision must be CPB_PREC_FP64 or CPB_PREC_MIXED"};
+    return fit_sim_impl<double>(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0,
+                                d_flux0, out);
 }
 
 }  // namespace cpb
