@@ -189,6 +189,9 @@ PROTOTYPES = {
                                                       C.POINTER(SimResult)]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
+    "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                          C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(LMResultC)]),
 }
 
 PACKAGE_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))

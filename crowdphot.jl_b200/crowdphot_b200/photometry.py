@@ -502,6 +502,64 @@ def fit_star_batch(model, cutouts, *, inv_vars=None, origins, inits=None, fixed=
     return out
 
 
+def _lm_outputs(n, np_, nf):
+    return dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), cost=np.zeros(n), cost_init=np.zeros(n),
+                chisq=np.zeros(n), lambda_final=np.zeros(n), converged=np.zeros(n, np.uint8),
+                x_converged=np.zeros(n, np.uint8), f_converged=np.zeros(n, np.uint8),
+                g_converged=np.zeros(n, np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
+
+
+def _lm_result_struct(out, ptr):
+    """LMResultC pointing at the arrays of `out` through ptr(array) (host or device addresses)."""
+    r = _abi.LMResultC()
+    for f in ("params", "cov", "cost", "cost_init", "chisq", "lambda_final"):
+        setattr(r, f, C.cast(C.c_void_p(ptr(out[f])), _abi._dp) if out.get(f) is not None else None)
+    for f in ("converged", "x_converged", "f_converged", "g_converged"):
+        setattr(r, f, C.cast(C.c_void_p(ptr(out[f])), _abi._u8p) if out.get(f) is not None else None)
+    r.iterations = C.cast(C.c_void_p(ptr(out["iterations"])), _abi._i32p)
+    r.status = C.cast(C.c_void_p(ptr(out["status"])), _abi._i32p)
+    return r
+
+
+def fit_star_packed(model, pixels, offsets, ny, nx, y_origin, x_origin, init, *, inv_var=None, fixed=None,
+                    ctx: Context | None = None, **kw):
+    """Many fit_star calls over cutouts packed in one buffer (the C-ABI layout):
+    cutout c is pixels[offsets[c] : offsets[c] + ny[c]*nx[c]], column-major,
+    whose first pixel is image pixel (y_origin[c], x_origin[c]) (1-based);
+    inv_var (optional) shares the layout; init is (n, np) model parameters.
+    float32 pixels are fitted as float32 input, float64 as float64.
+    Returns a dict of per-cutout arrays like fit_star_batch."""
+    fixed = dict(fixed or {})
+    ctx = ctx or get_context()
+    P = lm_params(model, fixed, **kw)
+    n = len(offsets)
+    np_ = len(_props(model))
+    nf = bin(P.free_mask).count("1")
+    pix = np.ascontiguousarray(pixels)
+    dt = np.float32 if pix.dtype == np.float32 else np.float64
+    pix = pix.astype(dt, copy=False)
+    iv = None if inv_var is None else np.ascontiguousarray(inv_var, dtype=dt)
+    if iv is not None and iv.shape != pix.shape:
+        raise ArgumentError("`inv_var` must be the same size as `image`")
+    offs = np.ascontiguousarray(offsets, dtype=np.int64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    nyv, nxv, y1, x1 = i32(ny), i32(nx), i32(y_origin), i32(x_origin)
+    init = np.ascontiguousarray(init, dtype=np.float64).reshape(n, np_)
+    out = _lm_outputs(n, np_, nf)
+    r = _lm_result_struct(out, lambda a: a.ctypes.data)
+    et = _abi.CPB_F32 if dt == np.float32 else _abi.CPB_F64
+    rc = ctx.lib.cpb_fit_lm_batch(ctx.handle, ctx.psf_handle(model), C.byref(P), n, offs.ctypes.data_as(_abi._i64p),
+                                  nyv.ctypes.data_as(_abi._i32p), nxv.ctypes.data_as(_abi._i32p),
+                                  y1.ctypes.data_as(_abi._i32p), x1.ctypes.data_as(_abi._i32p),
+                                  pix.ctypes.data_as(C.c_void_p), et,
+                                  None if iv is None else iv.ctypes.data_as(C.c_void_p),
+                                  init.ctypes.data_as(_abi._dp), C.byref(r))
+    ctx.raise_for(rc, "cpb_fit_lm_batch")
+    out["device_seconds"] = float(r.device_seconds)
+    out["names"] = _props(model)
+    return out
+
+
 def fit_star(model, image, inds=None, *, fixed=None, inv_var=None, ctx: Context | None = None, **kw):
     """CrowdPhot.PSF.fit_star on the B200 (psf_fitting.jl:229-308) -> (best_model, LMResult).
 

@@ -227,3 +227,77 @@ def crowded_field(ny, nx, n, *, seed, psf=None, flux=(1e1, 1e6), flux_distributi
                 x=src["x"] + rng.normal(0, init_sigma, src["x"].size),
                 flux=src["flux"] * rng.uniform(init_flux[0], init_flux[1], src["flux"].size))
     return img.astype(dtype), bkg.astype(dtype), inv_var.astype(dtype), src, init
+
+
+def _catmull_rom(t):
+    """The four stencil weights of the clamped cubic in _cubic_rows, as functions of the fraction t."""
+    t2, t3 = t * t, t * t * t
+    return np.stack([(-t3 + 2 * t2 - t) / 2, (3 * t3 - 5 * t2 + 2) / 2, (-3 * t3 + 4 * t2 + t) / 2, (t3 - t2) / 2],
+                    axis=-1)
+
+
+def _axis_stencil(Yc, first, side, os_, origin, n):
+    """Per-cutout stencil of one axis for pixels first..first+side-1 of a star at Yc: the
+    grid fraction is the same on every pixel (the oversampling is an integer), so one weight
+    vector serves the whole axis.  Returns (indices (k, side, 4), in-grid mask (k, side), weights (k, 4))."""
+    v = os_ * (first[:, None] + np.arange(side)[None, :] - Yc[:, None]) + origin
+    inb = (v >= 1) & (v <= n)
+    lv = np.floor(np.where(inb, v, 1.0)).astype(np.int64)
+    t = v[:, 0] - np.floor(v[:, 0])
+    idx = np.clip(np.stack([lv - 1, lv, lv + 1, lv + 2], axis=-1), 1, n) - 1
+    return idx, inb, _catmull_rom(t)
+
+
+def render_cutouts(node: ImagePSF, Yc, Xc, flux, y1, x1, side):
+    """flux * ePSF over square cutouts of one side (k, side, side), separably: rows are
+    contracted first over the grid's columns, then the column stencil is applied."""
+    d = np.asarray(node.data, dtype=np.float64)
+    ny, nx = d.shape
+    sx, sy = node.oversampling
+    iy, my, wy = _axis_stencil(Yc, y1, side, sy, node.origin["y"], ny)
+    ix, mx, wx = _axis_stencil(Xc, x1, side, sx, node.origin["x"], nx)
+    rows = np.einsum("kr,kirc->kic", wy, d[iy])                     # (k, side, nx)
+    k = np.arange(len(Yc))[:, None, None, None]
+    g = rows[k, np.arange(side)[None, :, None, None], ix[:, None, :, :]]  # (k, side_i, side_j, 4)
+    val = np.einsum("kc,kijc->kij", wx, g)
+    val = np.where(my[:, :, None] & mx[:, None, :], val, node.fill_value)
+    return flux[:, None, None] * val
+
+
+def lm_cutouts(n, *, seed, psf=None, smin=9, smax=41, snr=(5.0, 1000.0), bkg=100.0, read_noise=5.0, gain=1.0,
+               dtype=np.float32, init_sigma=0.3, init_flux=(0.9, 1.1)):
+    """Isolated-star cutouts of uneven size for batched fit_star: side ~ U{smin..smax},
+    star at the cutout centre + U(-0.5, 0.5) px, flux from an SNR drawn log-uniform
+    in `snr` via flux_for_snr (bkg 100, read noise 5, gain 1), Poisson + Gaussian
+    noise, background subtracted, inverse-variance weights.  Cutouts are returned
+    concatenated (column-major each) with offsets, sizes and 1-based origins."""
+    rng = np.random.default_rng(seed)
+    psf = psf if psf is not None else moffat_epsf()
+    node = psf.psfs[0] if isinstance(psf, GriddedPSFModel) else psf
+    sides = rng.integers(smin, smax + 1, n)
+    y1 = rng.integers(1, 4000, n)
+    x1 = rng.integers(1, 4000, n)
+    yc = y1 + (sides - 1) / 2 + rng.uniform(-0.5, 0.5, n)
+    xc = x1 + (sides - 1) / 2 + rng.uniform(-0.5, 0.5, n)
+    s = np.exp(rng.uniform(np.log(snr[0]), np.log(snr[1]), n))
+    flux = flux_for_snr(node, s, background=bkg, read_noise=read_noise, gain=gain)
+    sizes = sides.astype(np.int64) ** 2
+    offsets = np.zeros(n, np.int64)
+    offsets[1:] = np.cumsum(sizes)[:-1]
+    pix = np.empty(int(sizes.sum()), dtype=dtype)
+    iv = np.empty_like(pix)
+    for side in np.unique(sides):
+        idx = np.nonzero(sides == side)[0]
+        model = render_cutouts(node, yc[idx], xc[idx], flux[idx], y1[idx], x1[idx], int(side))
+        img = rng.poisson(np.maximum(model + bkg, 0) * gain) / gain + read_noise * rng.standard_normal(model.shape)
+        var = bkg + model + read_noise ** 2
+        # column-major per cutout: (k, i, j) -> transpose to (k, j, i) then flatten
+        flat_img = np.ascontiguousarray(np.transpose(img - bkg, (0, 2, 1))).reshape(len(idx), -1)
+        flat_iv = np.ascontiguousarray(np.transpose(1.0 / var, (0, 2, 1))).reshape(len(idx), -1)
+        at = offsets[idx, None] + np.arange(side * side)[None, :]
+        pix[at] = flat_img
+        iv[at] = flat_iv
+    init = np.stack([yc + rng.normal(0, init_sigma, n), xc + rng.normal(0, init_sigma, n),
+                     flux * rng.uniform(init_flux[0], init_flux[1], n), np.zeros(n)], axis=1)
+    return dict(pix=pix, inv_var=iv, offsets=offsets, ny=sides.astype(np.int32), nx=sides.astype(np.int32),
+                y1=y1.astype(np.int32), x1=x1.astype(np.int32), init=init, truth=np.stack([yc, xc, flux], 1))

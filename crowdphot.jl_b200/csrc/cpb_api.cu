@@ -411,4 +411,18 @@ int cpb_fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* para
     });
 }
 
+int cpb_fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, int64_t n_cutouts,
+                            const int64_t* d_offsets, const int32_t* d_ny, const int32_t* d_nx,
+                            const int32_t* d_y_origin, const int32_t* d_x_origin, const void* d_pixels,
+                            int32_t eltype, const void* d_inv_var, const double* d_init, int64_t total_pixels,
+                            cpb_lm_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || (n_cutouts > 0 && (!d_offsets || !d_ny || !d_nx || !d_y_origin ||
+                                                          !d_x_origin || !d_pixels || !d_init || !out->status)))
+            throw ArgError{"null argument"};
+        return fit_lm_batch_device(ctx, psf, params, n_cutouts, d_offsets, d_ny, d_nx, d_y_origin, d_x_origin,
+                                   d_pixels, eltype, d_inv_var, d_init, total_pixels, out);
+    });
+}
+
 }  // extern "C"

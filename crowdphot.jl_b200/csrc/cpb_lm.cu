@@ -217,11 +217,12 @@ __device__ void lm_cov(const double* A0, int n, double* cov) {
     }
 }
 
+// Per-cutout outputs, device pointers; every one but status may be null.
 struct LMOut {
     double* params;   // n x np
     double* cov;      // n x nf x nf
-    double* scal;     // n x 4: cost, cost_init, chisq, lambda
-    uint8_t* flags;   // n x 4: converged, x, f, g
+    double *cost, *cost_init, *chisq, *lambda_final;
+    uint8_t *converged, *x_converged, *f_converged, *g_converged;
     int32_t* iters;
     int32_t* status;
 };
@@ -241,6 +242,10 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
         const TI* pix = pixels + offs[c];
         const TI* iv = ivs ? ivs + offs[c] : nullptr;
         const int64_t nobs = (int64_t)ny * nx;
+        if (ny <= 0 || nx <= 0) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
         // _prepare_fit_star_inputs checks (psf_fitting.jl:61-90) and lm_irls dof (:461-467)
         int bad = 0;
         if (iv) {
@@ -333,21 +338,23 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
         }
         if (lane == 0) {
             const double dof = (double)(nobs - nf);
-            double cov[25];
-            lm_cov(A, nf, cov);
-            const double f = L.reweighted ? cost / dof : 1.0;
-            if (out.cov)
+            if (out.cov) {
+                double cov[25];
+                lm_cov(A, nf, cov);
+                const double f = L.reweighted ? cost / dof : 1.0;
                 for (int k = 0; k < nf * nf; ++k) out.cov[c * nf * nf + k] = cov[k] * f;
-            for (int q = 0; q < np; ++q) out.params[c * np + q] = fv[q];
-            out.scal[c * 4 + 0] = cost;
-            out.scal[c * 4 + 1] = cost_init;
-            out.scal[c * 4 + 2] = cost / dof;
-            out.scal[c * 4 + 3] = lam;
-            out.flags[c * 4 + 0] = conv;
-            out.flags[c * 4 + 1] = xconv;
-            out.flags[c * 4 + 2] = fconv;
-            out.flags[c * 4 + 3] = gconv;
-            out.iters[c] = iter;
+            }
+            if (out.params)
+                for (int q = 0; q < np; ++q) out.params[c * np + q] = fv[q];
+            if (out.cost) out.cost[c] = cost;
+            if (out.cost_init) out.cost_init[c] = cost_init;
+            if (out.chisq) out.chisq[c] = cost / dof;
+            if (out.lambda_final) out.lambda_final[c] = lam;
+            if (out.converged) out.converged[c] = conv;
+            if (out.x_converged) out.x_converged[c] = xconv;
+            if (out.f_converged) out.f_converged[c] = fconv;
+            if (out.g_converged) out.g_converged[c] = gconv;
+            if (out.iters) out.iters[c] = iter;
             out.status[c] = 0;
         }
     }
@@ -357,12 +364,10 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
 
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
 
-int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
-                 const int32_t* ny, const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,
-                 const void* pixels, int32_t eltype, const void* inv_var, const double* init, cpb_lm_result* out) {
-    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
+namespace {
+
+LMConst lm_const(const cpb_psf* psf, const cpb_lm_params* P, bool have_iv) {
     if (P->precision != CPB_PREC_FP64) throw ArgError{"only the FP64 precision form is built for fit_star"};
-    if (n_cut <= 0) return 0;
     LMConst L{};
     L.gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     L.np = L.gauss ? 5 : 4;
@@ -378,7 +383,7 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     if (L.nf == 0) throw ArgError{"all model parameters are fixed; nothing to fit"};
     L.damping = P->damping;
     L.max_iter = P->max_iter;
-    L.reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && inv_var == nullptr);
+    L.reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && !have_iv);
     L.x_tol = P->x_tol;
     L.f_tol = P->f_tol;
     L.g_tol = P->g_tol;
@@ -388,10 +393,42 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     L.lambda_min = P->lambda_min;
     L.lambda_max = P->lambda_max;
     L.min_diagonal = P->min_diagonal;
+    return L;
+}
+
+// One launch of k_lm over device-resident cutouts; `pix_elems` (the cutout
+// pixels in total, for the instrumentation's byte count) may be 0.
+void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut, const int64_t* d_off,
+               const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1, const int32_t* d_x1, const void* d_pix,
+               int32_t eltype, const void* d_iv, const double* d_init, const LMOut& o, int64_t pix_elems) {
+    const size_t esz = eltype == CPB_F64 ? 8 : 4;
+    const double bytes = (double)pix_elems * esz * (d_iv ? 2 : 1) + (double)n_cut * (8 + 16 + 8 * L.np) +
+                         (double)n_cut * (8 * L.np + (o.cov ? 8 * L.nf * L.nf : 0) + 4 * 8 + 4 + 4 + 4);
+    const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
+    cudaStream_t st = ctx->stream;
+    KernelScope ks_(ctx, "k_lm", bytes);
+    if (eltype == CPB_F64)
+        k_lm<double><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
+                                             (const double*)d_pix, (const double*)d_iv, d_init, o);
+    else
+        k_lm<float><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1, (const float*)d_pix,
+                                            (const float*)d_iv, d_init, o);
+    check(cudaGetLastError(), "k_lm");
+}
+
+}  // namespace
+
+int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
+                 const int32_t* ny, const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,
+                 const void* pixels, int32_t eltype, const void* inv_var, const double* init, cpb_lm_result* out) {
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
+    const LMConst L = lm_const(psf, P, inv_var != nullptr);
+    if (n_cut <= 0) return 0;
     cudaStream_t st = ctx->stream;
     int64_t total = 0;
     for (int64_t c = 0; c < n_cut; ++c) {
         if (ny[c] <= 0 || nx[c] <= 0) throw ArgError{"cutout dimensions must be positive"};
+        if (offsets[c] < 0) throw ArgError{"cutout offsets must be non-negative"};
         total = std::max<int64_t>(total, offsets[c] + (int64_t)ny[c] * nx[c]);
     }
     const size_t esz = eltype == CPB_F64 ? 8 : 4;
@@ -409,45 +446,62 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     const void* d_pix = up("lm_pix", pixels, esz * total);
     const void* d_iv = inv_var ? up("lm_iv", inv_var, esz * total) : nullptr;
     const double* d_init = (const double*)up("lm_init", init, sizeof(double) * n_cut * L.np);
+    // device outputs: one block, carved in the order of the host fields
+    const size_t nd = (size_t)n_cut * (L.np + (out->cov ? L.nf * L.nf : 0) + 4);
+    double* dd = (double*)scratch(ctx, "lm_out_f64", sizeof(double) * nd);
+    uint8_t* du = (uint8_t*)scratch(ctx, "lm_out_u8", (size_t)n_cut * 4);
+    int32_t* di = (int32_t*)scratch(ctx, "lm_out_i32", sizeof(int32_t) * n_cut * 2);
     LMOut o;
-    o.params = (double*)scratch(ctx, "lm_params", sizeof(double) * n_cut * L.np);
-    o.cov = out->cov ? (double*)scratch(ctx, "lm_cov", sizeof(double) * n_cut * L.nf * L.nf) : nullptr;
-    o.scal = (double*)scratch(ctx, "lm_scal", sizeof(double) * n_cut * 4);
-    o.flags = (uint8_t*)scratch(ctx, "lm_flags", n_cut * 4);
-    o.iters = (int32_t*)scratch(ctx, "lm_iters", sizeof(int32_t) * n_cut);
-    o.status = (int32_t*)scratch(ctx, "lm_status", sizeof(int32_t) * n_cut);
-    const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
-    if (eltype == CPB_F64)
-        k_lm<double><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
-                                             (const double*)d_pix, (const double*)d_iv, d_init, o);
-    else
-        k_lm<float><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1, (const float*)d_pix,
-                                            (const float*)d_iv, d_init, o);
-    check(cudaGetLastError(), "k_lm");
+    o.params = dd;
+    o.cov = out->cov ? dd + n_cut * L.np : nullptr;
+    double* sc = dd + n_cut * L.np + (out->cov ? n_cut * L.nf * L.nf : 0);
+    o.cost = sc;
+    o.cost_init = sc + n_cut;
+    o.chisq = sc + 2 * n_cut;
+    o.lambda_final = sc + 3 * n_cut;
+    o.converged = du;
+    o.x_converged = du + n_cut;
+    o.f_converged = du + 2 * n_cut;
+    o.g_converged = du + 3 * n_cut;
+    o.iters = di;
+    o.status = di + n_cut;
+    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total);
     check(cudaEventRecord(ctx->ev1, st), "event");
-    std::vector<double> scal(n_cut * 4);
-    std::vector<uint8_t> flags(n_cut * 4);
-    check(cudaMemcpyAsync(out->params, o.params, sizeof(double) * n_cut * L.np, cudaMemcpyDeviceToHost, st), "d2h");
-    if (out->cov)
-        check(cudaMemcpyAsync(out->cov, o.cov, sizeof(double) * n_cut * L.nf * L.nf, cudaMemcpyDeviceToHost, st), "d2h");
-    check(cudaMemcpyAsync(scal.data(), o.scal, sizeof(double) * n_cut * 4, cudaMemcpyDeviceToHost, st), "d2h");
-    check(cudaMemcpyAsync(flags.data(), o.flags, n_cut * 4, cudaMemcpyDeviceToHost, st), "d2h");
-    check(cudaMemcpyAsync(out->iterations, o.iters, sizeof(int32_t) * n_cut, cudaMemcpyDeviceToHost, st), "d2h");
-    check(cudaMemcpyAsync(out->status, o.status, sizeof(int32_t) * n_cut, cudaMemcpyDeviceToHost, st), "d2h");
+    auto down = [&](void* h, const void* d, size_t bytes) {
+        if (h) check(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st), "d2h");
+    };
+    down(out->params, o.params, sizeof(double) * n_cut * L.np);
+    down(out->cov, o.cov, sizeof(double) * n_cut * L.nf * L.nf);
+    double* hs[4] = {out->cost, out->cost_init, out->chisq, out->lambda_final};
+    for (int k = 0; k < 4; ++k) down(hs[k], sc + k * n_cut, sizeof(double) * n_cut);
+    uint8_t* hf[4] = {out->converged, out->x_converged, out->f_converged, out->g_converged};
+    for (int k = 0; k < 4; ++k) down(hf[k], du + k * n_cut, (size_t)n_cut);
+    down(out->iterations, o.iters, sizeof(int32_t) * n_cut);
+    down(out->status, o.status, sizeof(int32_t) * n_cut);
     check(cudaStreamSynchronize(st), "sync");
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     out->device_seconds = ms * 1e-3;
-    for (int64_t c = 0; c < n_cut; ++c) {
-        if (out->cost) out->cost[c] = scal[c * 4 + 0];
-        if (out->cost_init) out->cost_init[c] = scal[c * 4 + 1];
-        if (out->chisq) out->chisq[c] = scal[c * 4 + 2];
-        if (out->lambda_final) out->lambda_final[c] = scal[c * 4 + 3];
-        if (out->converged) out->converged[c] = flags[c * 4 + 0];
-        if (out->x_converged) out->x_converged[c] = flags[c * 4 + 1];
-        if (out->f_converged) out->f_converged[c] = flags[c * 4 + 2];
-        if (out->g_converged) out->g_converged[c] = flags[c * 4 + 3];
-    }
+    return 0;
+}
+
+int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,
+                        const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1,
+                        const int32_t* d_x1, const void* d_pix, int32_t eltype, const void* d_iv,
+                        const double* d_init, int64_t total_pixels, cpb_lm_result* out) {
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
+    const LMConst L = lm_const(psf, P, d_iv != nullptr);
+    if (n_cut <= 0) return 0;
+    LMOut o{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
+            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+    cudaStream_t st = ctx->stream;
+    check(cudaEventRecord(ctx->ev0, st), "event");
+    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels);
+    check(cudaEventRecord(ctx->ev1, st), "event");
+    check(cudaStreamSynchronize(st), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    out->device_seconds = ms * 1e-3;
     return 0;
 }
 

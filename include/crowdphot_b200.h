@@ -301,6 +301,23 @@ CPB_API int cpb_fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_para
                      const void* pixels, int32_t eltype, const void* inv_var,
                      const double* init, cpb_lm_result* out);
 
+/*
+ * cpb_fit_lm_batch on device-resident cutouts (no counterpart in the
+ * reference, whose fit_star takes host arrays; this serves callers whose
+ * cutouts already sit on the GPU, and the throughput measurement).  Every
+ * array argument and every pointer in `out` is a device pointer on the
+ * context's device; out->status is required, the other outputs may be null.
+ * total_pixels = the pixel elements the cutouts span (used only to credit the
+ * instrumentation's byte count; 0 is allowed).  Cutout dimensions are checked
+ * on the device: a cutout with ny or nx <= 0 gets status CPB_ERR_ARGUMENT.
+ * Returns when the fits are done; out->device_seconds is their GPU time.
+ */
+CPB_API int cpb_fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params,
+                                    int64_t n_cutouts, const int64_t* d_offsets, const int32_t* d_ny,
+                                    const int32_t* d_nx, const int32_t* d_y_origin, const int32_t* d_x_origin,
+                                    const void* d_pixels, int32_t eltype, const void* d_inv_var,
+                                    const double* d_init, int64_t total_pixels, cpb_lm_result* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,10 @@ def load():
         lib.orc_model_radii_auto_gaussian.restype = C.c_int
         lib.orc_model_radii_auto_gaussian.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int64, _dp,
                                                       C.c_int64, _dp, _i32p]
+        lib.orc_fit_star_batch.restype = C.c_int
+        lib.orc_fit_star_batch.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_int64, _i64p,
+                                           _i32p, _i32p, _i32p, _i32p, _dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp,
+                                           _dp, _u8p, _i32p, _i32p, C.c_int]
         _lib = lib
     return _lib
 
@@ -260,3 +264,41 @@ def orc_model_radii_auto_gaussian(fwhm, nsigma, R_fit, R_cap, w, flux):
     if rc != 0:
         raise ArgumentError("no positive weights")
     return out
+
+
+def orc_fit_star_packed(model, pix, offsets, ny, nx, y1, x1, init, *, inv_var=None, fixed=None, threads=0, **kw):
+    """The oracle's fit_star over many packed cutouts (same layout as
+    crowdphot_b200.fit_star_packed), spread over `threads` host threads
+    (0 = all).  Returns (dict of per-cutout arrays, threads used)."""
+    lib = load()
+    fixed = dict(fixed or {})
+    P = lm_params(model, fixed, **kw)
+    n = len(offsets)
+    names = _props(model)
+    np_ = len(names)
+    nf = bin(_free_mask(model, fixed)).count("1")
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    pix, init = f64(pix), f64(init)
+    iv = None if inv_var is None else f64(inv_var)
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    ny, nx, y1, x1 = i32(ny), i32(nx), i32(y1), i32(x1)
+    out = dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), scal=np.zeros((n, 4)),
+               flags=np.zeros((n, 4), np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
+    desc, keep = psf_descriptor(model)
+    used = lib.orc_fit_star_batch(C.byref(desc), C.byref(P), n, offsets.ctypes.data_as(_i64p),
+                                  ny.ctypes.data_as(_i32p), nx.ctypes.data_as(_i32p), y1.ctypes.data_as(_i32p),
+                                  x1.ctypes.data_as(_i32p), pix.ctypes.data_as(_dp),
+                                  None if iv is None else iv.ctypes.data_as(_dp), init.ctypes.data_as(_dp), np_, nf,
+                                  out["params"].ctypes.data_as(_dp), out["cov"].ctypes.data_as(_dp),
+                                  out["scal"].ctypes.data_as(_dp), out["flags"].ctypes.data_as(_u8p),
+                                  out["iterations"].ctypes.data_as(_i32p), out["status"].ctypes.data_as(_i32p),
+                                  int(threads))
+    del keep
+    if used < 0:
+        raise ArgumentError("invalid PSF descriptor")
+    sc, fl = out.pop("scal"), out.pop("flags")
+    out.update(cost=sc[:, 0].copy(), cost_init=sc[:, 1].copy(), chisq=sc[:, 2].copy(), lambda_final=sc[:, 3].copy(),
+               converged=fl[:, 0].copy(), x_converged=fl[:, 1].copy(), f_converged=fl[:, 2].copy(),
+               g_converged=fl[:, 3].copy(), names=names)
+    return out, used

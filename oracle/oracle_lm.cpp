@@ -14,6 +14,8 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "oracle_psf.hpp"
@@ -145,6 +147,11 @@ bool chol_solve(const double* A, int n, const double* b, double* x) {
     return true;
 }
 
+int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const double* inv_var, int32_t ny, int32_t nx,
+            int32_t y1, int32_t x1, const double* init, double* out_params, double* cov_out, double* cost_out,
+            double* cost_init_out, double* chisq_out, double* lambda_out, uint8_t* flags_out, int32_t* iters_out,
+            char* errbuf, int errlen);
+
 }  // namespace
 
 extern "C" {
@@ -155,15 +162,61 @@ int orc_fit_star(const cpb_psf_desc* desc, const cpb_lm_params* P, const double*
                  int32_t ny, int32_t nx, int32_t y1, int32_t x1, const double* init, double* out_params,
                  double* cov_out, double* cost_out, double* cost_init_out, double* chisq_out, double* lambda_out,
                  uint8_t* flags_out /* converged, x, f, g */, int32_t* iters_out, char* errbuf, int errlen) {
+    Psf psf;
+    {
+        std::string e = load_psf(desc, psf);
+        if (!e.empty()) {
+            if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", e.c_str());
+            return CPB_ERR_ARGUMENT;
+        }
+    }
+    return fit_one(psf, P, pix, inv_var, ny, nx, y1, x1, init, out_params, cov_out, cost_out, cost_init_out,
+                   chisq_out, lambda_out, flags_out, iters_out, errbuf, errlen);
+}
+
+// n_cut fit_star calls on one loaded PSF, cutout c at pix[offsets[c]..] (column-major
+// ny[c] x nx[c]); the cutouts are independent, so they are spread over `threads`
+// host threads (<= 0: all hardware threads).  Per-cutout outputs as orc_fit_star's, packed:
+// params n*np, cov n*nf*nf (nullable), scal n*4 (cost, cost_init, chisq, lambda),
+// flags n*4, iters n, status n (0 or CPB_ERR_ARGUMENT).  Returns the threads used.
+int orc_fit_star_batch(const cpb_psf_desc* desc, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
+                       const int32_t* ny, const int32_t* nx, const int32_t* y1, const int32_t* x1, const double* pix,
+                       const double* inv_var, const double* init, int np, int nf, double* params, double* cov,
+                       double* scal, uint8_t* flags, int32_t* iters, int32_t* status, int threads) {
+    Psf psf;
+    if (!load_psf(desc, psf).empty()) return -1;
+    const int used = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<int64_t> next{0};
+    auto work = [&]() {
+        for (;;) {
+            const int64_t c0 = next.fetch_add(16);
+            if (c0 >= n_cut) return;
+            for (int64_t c = c0; c < std::min(n_cut, c0 + 16); ++c)
+                status[c] = fit_one(psf, P, pix + offsets[c], inv_var ? inv_var + offsets[c] : nullptr, ny[c], nx[c],
+                                    y1[c], x1[c], init + c * np, params + c * np, cov ? cov + c * nf * nf : nullptr,
+                                    &scal[c * 4], &scal[c * 4 + 1], &scal[c * 4 + 2], &scal[c * 4 + 3], flags + c * 4,
+                                    iters + c, nullptr, 0);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < used; ++t) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    return used;
+}
+
+}  // extern "C"
+
+namespace {
+
+int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const double* inv_var, int32_t ny, int32_t nx,
+            int32_t y1, int32_t x1, const double* init, double* out_params, double* cov_out, double* cost_out,
+            double* cost_init_out, double* chisq_out, double* lambda_out, uint8_t* flags_out, int32_t* iters_out,
+            char* errbuf, int errlen) {
     auto fail = [&](const std::string& m) {
         if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
         return CPB_ERR_ARGUMENT;
     };
-    Psf psf;
-    {
-        std::string e = load_psf(desc, psf);
-        if (!e.empty()) return fail(e);
-    }
     const bool gauss = psf.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     const int np = gauss ? 5 : 4;
     // free set in getproperties order
@@ -293,4 +346,4 @@ int orc_fit_star(const cpb_psf_desc* desc, const cpb_lm_params* P, const double*
     return 0;
 }
 
-}  // extern "C"
+}  // namespace

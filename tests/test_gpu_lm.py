@@ -93,3 +93,43 @@ def test_fit_star_errors():
         cpb.fit_star(m, img, inv_var=np.zeros_like(img))
     with pytest.raises(ArgumentError, match="all model parameters are fixed"):
         cpb.fit_star(m, img, fixed=dict(y=1, x=1, fwhm=1, flux=1, bkg=1))
+
+
+def test_packed_cutouts_host_and_device_entries_match_oracle():
+    """The C4 cutout workload (isolated stars, sides 9..41, SNR 5..1000, float32
+    pixels): host-buffer entry, device-buffer entry and the oracle agree cutout by cutout."""
+    import torch
+    from crowdphot_b200 import _abi
+    from crowdphot_b200.photometry import _lm_outputs, _lm_result_struct, lm_params
+    from crowdphot_b200.simulate import lm_cutouts
+    from oracle.ffi import orc_fit_star_packed
+    psf = moffat_epsf()
+    d = lm_cutouts(3000, seed=41)
+    args = (d["pix"], d["offsets"], d["ny"], d["nx"], d["y1"], d["x1"], d["init"])
+    fixed = {"bkg": 0.0}
+    host = cpb.fit_star_packed(psf, *args, inv_var=d["inv_var"], fixed=fixed)
+    ref, _ = orc_fit_star_packed(psf, *args, inv_var=d["inv_var"], fixed=fixed, threads=0)
+    assert np.all(host["status"] == 0) and np.all(ref["status"] == 0)
+    assert np.array_equal(host["iterations"], ref["iterations"])
+    assert np.array_equal(host["converged"], ref["converged"])
+    assert np.max(np.abs(host["params"][:, :2] - ref["params"][:, :2])) < 1e-7
+    assert np.max(np.abs(host["params"][:, 2] / ref["params"][:, 2] - 1)) < 1e-9
+    np.testing.assert_allclose(host["cov"], ref["cov"], rtol=1e-6, atol=1e-12)
+    np.testing.assert_allclose(host["cost"], ref["cost"], rtol=1e-9)
+
+    ctx = cpb.get_context(0)
+    dev = torch.device("cuda", 0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    dpix, div, doff = t(d["pix"]), t(d["inv_var"]), t(d["offsets"])
+    dny, dnx, dy1, dx1, dinit = t(d["ny"]), t(d["nx"]), t(d["y1"]), t(d["x1"]), t(d["init"])
+    outs = {k: torch.from_numpy(v).to(dev) for k, v in _lm_outputs(len(d["ny"]), 4, 3).items()}
+    r = _lm_result_struct(outs, lambda a: a.data_ptr())
+    P = lm_params(psf, fixed)
+    vp = lambda a: a.data_ptr()
+    rc = ctx.lib.cpb_fit_lm_batch_device(ctx.handle, ctx.psf_handle(psf), P, len(d["ny"]), vp(doff), vp(dny),
+                                         vp(dnx), vp(dy1), vp(dx1), vp(dpix), _abi.CPB_F32, vp(div), vp(dinit),
+                                         d["pix"].size, r)
+    assert rc == 0, ctx.error()
+    assert r.device_seconds > 0
+    for k in ("params", "cov", "cost", "chisq", "iterations", "converged", "status"):
+        assert np.array_equal(outs[k].cpu().numpy(), host[k]), k
