@@ -453,6 +453,14 @@ def run_gpu_lm(args):
     barrier()
     clk = clocks.stop() if clocks else None
     _, launches = ctx.kernel_stats(reset=True)
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": fitted / sum(times), "unit": "stars/s",
+                              "ms_per_step": 1e3 * sum(times) / args.steps, "gpu_launches": launches,
+                              "config": lm_config(n)}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
     agg = torch.tensor([sum(times), float(fitted), float(launches)], dtype=torch.float64, device=dev)
     if world > 1:
         mx, sm = agg.clone(), agg.clone()

@@ -360,6 +360,426 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fast form: compile-time parameter counts (every small matrix in registers),
+// single-node image PSFs read through the polyphase copy (the 16 stencil taps
+// of the 32 lanes' pixels -- consecutive cutout rows -- are adjacent doubles),
+// and a device work queue over the cutouts.  Arithmetic per pixel is the same
+// as corner_eval's (psf_fitting.jl:1233-1321 restated), so results match the
+// general kernel's to the last bit where the stencil is interior.
+// ---------------------------------------------------------------------------
+template <int NF>
+__device__ __forceinline__ bool chol_solve_t(const double* A, const double* b, double* x) {
+    double U[NF * NF];
+#pragma unroll
+    for (int j = 0; j < NF; ++j)
+#pragma unroll
+        for (int i = 0; i <= j; ++i) {
+            double s = A[i + j * NF];
+#pragma unroll
+            for (int k = 0; k < i; ++k) s -= U[k + i * NF] * U[k + j * NF];
+            if (i == j) {
+                if (!(s > 0)) return false;
+                U[j + j * NF] = sqrt(s);
+            } else {
+                U[i + j * NF] = s / U[i + i * NF];
+            }
+        }
+    double y[NF];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) {
+        double s = b[i];
+#pragma unroll
+        for (int k = 0; k < i; ++k) s -= U[k + i * NF] * y[k];
+        y[i] = s / U[i + i * NF];
+    }
+#pragma unroll
+    for (int i = NF - 1; i >= 0; --i) {
+        double s = y[i];
+#pragma unroll
+        for (int k = i + 1; k < NF; ++k) s -= U[i + k * NF] * x[k];
+        x[i] = s / U[i + i * NF];
+    }
+    return true;
+}
+
+// v[idx] for a register array v and a runtime index, without local memory.
+template <int N>
+__device__ __forceinline__ double pick(const double* v, int idx) {
+    double r = 0;
+#pragma unroll
+    for (int q = 0; q < N; ++q) r = (q == idx) ? v[q] : r;
+    return r;
+}
+
+// Stencil row / column taps of one axis in the polyphase copy: with the 0-based
+// sample index i0 of the first tap, the four taps i0..i0+3 live at
+// (i % is) * pstride + (i / is) * qstride.
+__device__ __forceinline__ void pp_taps(int i0, int is, float inv_is, int pstride, int qstride, int* t) {
+    int q = __float2int_rz(__int2float_rn(i0) * inv_is);
+    int r = i0 - q * is;
+    if (r < 0) {
+        r += is;
+        --q;
+    } else if (r >= is) {
+        r -= is;
+        ++q;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        t[k] = r * pstride + q * qstride;
+        if (++r == is) {
+            r = 0;
+            ++q;
+        }
+    }
+}
+
+struct PPNode {
+    const double* pp;   // this node's polyphase block
+    const double* dat;  // this node's column-major data (edge stencils)
+    DevNode nd;
+    int plane;          // PY * PX
+    float inv_isy, inv_isx;
+};
+
+// Single-node image profile and its derivatives in the detector frame:
+// s, dsdY = -sy * dp/dv, dsdX = -sx * dp/du (grid_profile with weights (1, 0, 0, 0)).
+__device__ __forceinline__ void pp_profile(const PPNode& N, double Y, double X, double py, double px, double& s,
+                                           double& dY, double& dX) {
+    const DevNode& nd = N.nd;
+    const double u = nd.sx * (px - X) + nd.ox;
+    const double v = nd.sy * (py - Y) + nd.oy;
+    const int nyd = nd.ny, nxd = nd.nx;
+    const bool inb = isfinite(u) && isfinite(v) && u >= 1.0 && u <= (double)nxd && v >= 1.0 && v <= (double)nyd;
+    if (!inb) {
+        s = nd.fill;
+        dY = 0.0;
+        dX = 0.0;
+        return;
+    }
+    const int lx = clampi((int)floor(u), 1, nxd - 1);
+    const int ly = clampi((int)floor(v), 1, nyd - 1);
+    if (lx < 2 || ly < 2 || lx + 2 > nxd || ly + 2 > nyd) {  // clamped stencil: the general evaluator
+        double pv, pdv, pdu;
+        corner_eval<double, double, true>(N.dat, nd, Y, X, py, px, pv, pdv, pdu);
+        s = pv;
+        dY = 0.0 * pv - 1.0 * nd.sy * pdv;
+        dX = 0.0 * pv - 1.0 * nd.sx * pdu;
+        return;
+    }
+    const double du = u - (double)lx, dv = v - (double)ly;
+    int ry[4], cx[4];
+    pp_taps(ly - 2, nd.isy, N.inv_isy, N.plane, 1, ry);
+    pp_taps(lx - 2, nd.isx, N.inv_isx, nd.isy * N.plane, nd.PY, cx);
+    double row[4], drow[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const double a = __ldg(N.pp + ry[r] + cx[0]), b = __ldg(N.pp + ry[r] + cx[1]);
+        const double c = __ldg(N.pp + ry[r] + cx[2]), e = __ldg(N.pp + ry[r] + cx[3]);
+        const double k1 = (c - a) / 2;
+        const double k4 = c - b - k1;
+        const double k2 = 3 * k4 - (e - b) / 2 + k1;
+        const double k3 = k4 - k2;
+        row[r] = du * (du * (du * k3 + k2) + k1) + b;
+        drow[r] = du * (3 * du * k3 + 2 * k2) + k1;
+    }
+    const double v1 = (row[2] - row[0]) / 2;
+    const double v4 = row[2] - row[1] - v1;
+    const double v2 = 3 * v4 - (row[3] - row[1]) / 2 + v1;
+    const double v3 = v4 - v2;
+    const double pv = dv * (dv * (dv * v3 + v2) + v1) + row[1];
+    const double pdv = dv * (3 * dv * v3 + 2 * v2) + v1;
+    const double u1 = (drow[2] - drow[0]) / 2;
+    const double u4 = drow[2] - drow[1] - u1;
+    const double u2 = 3 * u4 - (drow[3] - drow[1]) / 2 + u1;
+    const double u3 = u4 - u2;
+    const double pdu = dv * (dv * (dv * u3 + u2) + u1) + drow[1];
+    s = pv;
+    dY = 0.0 * pv - 1.0 * nd.sy * pdv;
+    dX = 0.0 * pv - 1.0 * nd.sx * pdu;
+}
+
+// Normal equations of one cutout at the full parameter vector fv, projected onto
+// the free set (A: NF x NF column-major, b: NF); every lane returns the same cost.
+template <typename TI, int NP, int NF>
+__device__ double lm_accum_t(const PPNode& N, const LMConst& L, const TI* __restrict__ pix,
+                             const TI* __restrict__ iv, int ny, int nx, int y1, int x1, int q32, int r32,
+                             const double* fv, double* A, double* b) {
+    constexpr int NT = NP * (NP + 1) / 2;
+    const int lane = threadIdx.x & 31;
+    double Af[NT], bf[NP], cost = 0;
+#pragma unroll
+    for (int q = 0; q < NT; ++q) Af[q] = 0;
+#pragma unroll
+    for (int q = 0; q < NP; ++q) bf[q] = 0;
+    const int npx = ny * nx;
+    int i = lane % ny, j = lane / ny;
+    for (int e = lane; e < npx; e += 32) {
+        double gv[NP], mval;
+        const double py = (double)(y1 + i), px = (double)(x1 + j);
+        if (NP == 5) {  // CircularGaussianPSF (parametric_models.jl:79-115)
+            const double gp = -2.772588722239781;
+            const double Y = fv[0], X = fv[1], fwhm = fv[2], flux = fv[3], bkg = fv[4];
+            const double f2 = fwhm * fwhm;
+            const double norm = -(3.141592653589793 * f2 / gp);
+            const double amp = flux / norm, gf2 = gp / f2;
+            const double dx = px - X, dy = py - Y;
+            const double sq = (dx * dx + dy * dy) / f2;
+            const double g = exp(gp * sq);
+            const double Ag = amp * g;
+            mval = amp * g + bkg;
+            gv[0] = -2 * Ag * gf2 * dy;
+            gv[1] = -2 * Ag * gf2 * dx;
+            gv[2] = -2 * Ag * (1 + gp * sq) / fwhm;
+            gv[3] = g / norm;
+            gv[NP - 1] = 1.0;
+        } else {
+            double s, dY, dX;
+            pp_profile(N, fv[0], fv[1], py, px, s, dY, dX);
+            const double flux = fv[2];
+            mval = flux * s + fv[3];
+            gv[0] = flux * dY;
+            gv[1] = flux * dX;
+            gv[2] = s;
+            gv[NP - 1] = 1.0;
+        }
+        const double r = mval - (double)pix[e];
+        double w = 1.0;
+        if (iv) {
+            const double vv = (double)iv[e];
+            w = (isfinite(vv) && vv > 0) ? vv : 0.0;
+        }
+        const double wr = w * r;
+        cost = wr * r + cost;
+        int t = 0;
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            bf[q] = wr * gv[q] + bf[q];
+#pragma unroll
+            for (int pq = 0; pq <= q; ++pq) {
+                Af[t] = (w * gv[pq]) * gv[q] + Af[t];
+                ++t;
+            }
+        }
+        i += r32;
+        j += q32;
+        if (i >= ny) {
+            i -= ny;
+            ++j;
+        }
+    }
+    // project onto the free set, then reduce only what the solve needs
+    double Ap[NF * (NF + 1) / 2], bp[NF];
+    {
+        int t = 0;
+#pragma unroll
+        for (int jq = 0; jq < NF; ++jq) {
+            bp[jq] = pick<NP>(bf, L.fidx[jq]);
+#pragma unroll
+            for (int iq = 0; iq <= jq; ++iq) {
+                const int a = L.fidx[iq], c = L.fidx[jq];
+                const int lo = min(a, c), hi = max(a, c);
+                Ap[t++] = pick<NT>(Af, hi * (hi + 1) / 2 + lo);
+            }
+        }
+    }
+    cost = warp_sum(cost);
+#pragma unroll
+    for (int q = 0; q < NF; ++q) b[q] = warp_sum(bp[q]);
+    {
+        int t = 0;
+#pragma unroll
+        for (int jq = 0; jq < NF; ++jq)
+#pragma unroll
+            for (int iq = 0; iq <= jq; ++iq) {
+                const double s = warp_sum(Ap[t++]);
+                A[iq + jq * NF] = s;
+                A[jq + iq * NF] = s;
+            }
+    }
+    return cost;
+}
+
+// covariance! (levenberg_marquardt.jl:366-388) for compile-time NF; the pinv
+// fallback is the general one.
+template <int NF>
+__device__ void lm_cov_t(const double* A, double* cov) {
+    double e[NF], x[NF];
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < NF; ++c) {
+#pragma unroll
+        for (int i = 0; i < NF; ++i) e[i] = (i == c) ? 1.0 : 0.0;
+        ok = ok && chol_solve_t<NF>(A, e, x);
+#pragma unroll
+        for (int i = 0; i < NF; ++i) cov[i + c * NF] = x[i];
+    }
+    if (!ok) lm_cov(A, NF, cov);
+}
+
+template <typename TI, int NP, int NF>
+__global__ void __launch_bounds__(64) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
+                                              const int64_t* __restrict__ offs, const int32_t* __restrict__ cny,
+                                              const int32_t* __restrict__ cnx, const int32_t* __restrict__ cy1,
+                                              const int32_t* __restrict__ cx1, const TI* __restrict__ pixels,
+                                              const TI* __restrict__ ivs, const double* __restrict__ init, LMOut out,
+                                              unsigned long long* __restrict__ queue) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long cc = 0;
+        if (lane == 0) cc = atomicAdd(queue, 1ull);
+        cc = __shfl_sync(0xffffffffu, cc, 0);
+        if (cc >= (unsigned long long)n_cut) return;
+        const int64_t c = (int64_t)cc;
+        const int ny = cny[c], nx = cnx[c], y1 = cy1[c], x1 = cx1[c];
+        const int64_t nobs = (int64_t)ny * nx;
+        if (ny <= 0 || nx <= 0) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
+        const TI* pix = pixels + offs[c];
+        const TI* iv = ivs ? ivs + offs[c] : nullptr;
+        // _prepare_fit_star_inputs checks (psf_fitting.jl:61-90) and lm_irls dof (:461-467)
+        bool bad = !(nobs - NF > 0);
+        if (iv) {
+            int nvalid = 0;
+            for (int64_t e = lane; e < nobs; e += 32) {
+                const double v = (double)iv[e];
+                nvalid += (isfinite(v) && v > 0) ? 1 : 0;
+            }
+            nvalid = warp_sum(nvalid);
+            bad = bad || !(nvalid > NF);
+        }
+        if (bad) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
+        const int q32 = 32 / ny, r32 = 32 % ny;
+        double fv[NP], x[NF], xc[NF], A[NF * NF], b[NF], Ac[NF * NF], bc[NF], Ad[NF * NF], d[NF], D[NF];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            bool fr = false;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) fr |= (L.fidx[k] == q);
+            fv[q] = fr ? init[c * NP + q] : L.fixv[q];
+        }
+#pragma unroll
+        for (int k = 0; k < NF; ++k) x[k] = pick<NP>(fv, L.fidx[k]);
+        double cost = lm_accum_t<TI, NP, NF>(N, L, pix, iv, ny, nx, y1, x1, q32, r32, fv, A, b);
+        const double cost_init = cost;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) D[k] = sqrt(fmax(A[k + k * NF], 1.0e-6));
+        double lam = L.lambda_init;
+        bool xconv = false, fconv = false, gconv = false, conv = false;
+        int iter = 0;
+        while (iter < L.max_iter) {
+            ++iter;
+            double gcos = 0;
+#pragma unroll
+            for (int k = 0; k < NF; ++k)
+                gcos = nan_max(gcos, fabs(b[k]) / (sqrt(A[k + k * NF] * cost) + 2.220446049250313e-16));
+            if (gcos <= L.g_tol) {
+                gconv = conv = true;
+                break;
+            }
+#pragma unroll
+            for (int k = 0; k < NF * NF; ++k) Ad[k] = A[k];
+            if (L.damping == CPB_DAMP_MARQUARDT) {
+#pragma unroll
+                for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam * fmax(Ad[k + k * NF], L.min_diagonal);
+            } else if (L.damping == CPB_DAMP_LEVENBERG) {
+#pragma unroll
+                for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam;
+            }
+            if (!chol_solve_t<NF>(Ad, b, d)) {
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+                continue;
+            }
+#pragma unroll
+            for (int k = 0; k < NF; ++k) d[k] = -d[k];
+            double db = 0, dAd = 0;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) db += d[k] * b[k];
+#pragma unroll
+            for (int k = 0; k < NF; ++k)
+#pragma unroll
+                for (int r = 0; r < NF; ++r) dAd += d[k] * A[k + r * NF] * d[r];
+            const double prered = -2 * db - dAd;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) xc[k] = x[k] + d[k];
+            double fc[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                double vq = fv[q];
+#pragma unroll
+                for (int k = 0; k < NF; ++k) vq = (L.fidx[k] == q) ? xc[k] : vq;
+                fc[q] = vq;
+            }
+            const double cost_c = lm_accum_t<TI, NP, NF>(N, L, pix, iv, ny, nx, y1, x1, q32, r32, fc, Ac, bc);
+            const bool accepted = cost_c < cost;
+            const double dcost = cost - cost_c;
+            const double ratio = prered > 0 ? dcost / prered : 0.0;
+            fconv = fabs(dcost) <= L.f_tol * (fabs(cost) + L.f_tol) && prered <= L.f_tol * (fabs(cost) + L.f_tol) &&
+                    0.5 * ratio <= 1;
+            double nd = 0, nxv = 0;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) {
+                nd += (D[k] * d[k]) * (D[k] * d[k]);
+                nxv += (D[k] * x[k]) * (D[k] * x[k]);
+            }
+            xconv = sqrt(nd) <= L.x_tol * (sqrt(nxv) + L.x_tol) && (accepted || fconv);
+            if (accepted) {
+                cost = cost_c;
+                lam = fmax(lam / L.lambda_down, L.lambda_min);
+#pragma unroll
+                for (int k = 0; k < NF; ++k) x[k] = xc[k];
+#pragma unroll
+                for (int k = 0; k < NF * NF; ++k) A[k] = Ac[k];
+#pragma unroll
+                for (int k = 0; k < NF; ++k) b[k] = bc[k];
+#pragma unroll
+                for (int q = 0; q < NP; ++q) fv[q] = fc[q];
+#pragma unroll
+                for (int k = 0; k < NF; ++k) D[k] = fmax(D[k], sqrt(A[k + k * NF]));
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+            } else {
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+            }
+        }
+        if (lane == 0) {
+            const double dof = (double)(nobs - NF);
+            if (out.cov) {
+                double cov[NF * NF];
+                lm_cov_t<NF>(A, cov);
+                const double f = L.reweighted ? cost / dof : 1.0;
+#pragma unroll
+                for (int k = 0; k < NF * NF; ++k) out.cov[c * NF * NF + k] = cov[k] * f;
+            }
+            if (out.params)
+#pragma unroll
+                for (int q = 0; q < NP; ++q) out.params[c * NP + q] = fv[q];
+            if (out.cost) out.cost[c] = cost;
+            if (out.cost_init) out.cost_init[c] = cost_init;
+            if (out.chisq) out.chisq[c] = cost / dof;
+            if (out.lambda_final) out.lambda_final[c] = lam;
+            if (out.converged) out.converged[c] = conv;
+            if (out.x_converged) out.x_converged[c] = xconv;
+            if (out.f_converged) out.f_converged[c] = fconv;
+            if (out.g_converged) out.g_converged[c] = gconv;
+            if (out.iters) out.iters[c] = iter;
+            out.status[c] = 0;
+        }
+    }
+}
+
 }  // namespace
 
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes);
@@ -404,8 +824,55 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
     const size_t esz = eltype == CPB_F64 ? 8 : 4;
     const double bytes = (double)pix_elems * esz * (d_iv ? 2 : 1) + (double)n_cut * (8 + 16 + 8 * L.np) +
                          (double)n_cut * (8 * L.np + (o.cov ? 8 * L.nf * L.nf : 0) + 4 * 8 + 4 + 4 + 4);
-    const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
     cudaStream_t st = ctx->stream;
+    const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    if (gauss || psf->dev.n_nodes == 1) {
+        // fast form: compile-time parameter counts, polyphase taps, work queue
+        PPNode N{};
+        if (!gauss) {
+            N.nd = psf->h_nodes[0];
+            N.pp = psf->dev.pp64 + N.nd.poff;
+            N.dat = psf->dev.data64 + N.nd.off;
+            N.plane = N.nd.PY * N.nd.PX;
+            N.inv_isy = 1.0f / (float)N.nd.isy;
+            N.inv_isx = 1.0f / (float)N.nd.isx;
+        }
+        auto* queue = (unsigned long long*)scratch(ctx, "lm_queue", sizeof(unsigned long long));
+        check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st), "memset");
+        // 64-thread blocks: registers (150-250 a thread) rather than blocks bound residency,
+        // and small blocks let every SM fill to its register limit
+        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 63) / 64, (int64_t)ctx->n_sm * 16);
+        KernelScope ks_(ctx, "k_lm", bytes);
+#define CPB_LM_LAUNCH(TI, NP, NF)                                                                               \
+    k_lm_t<TI, NP, NF><<<blocks, 64, 0, st>>>(n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix,     \
+                                               (const TI*)d_iv, d_init, o, queue)
+#define CPB_LM_NF(TI, NP)                          \
+    switch (L.nf) {                                \
+        case 1: CPB_LM_LAUNCH(TI, NP, 1); break;   \
+        case 2: CPB_LM_LAUNCH(TI, NP, 2); break;   \
+        case 3: CPB_LM_LAUNCH(TI, NP, 3); break;   \
+        case 4: CPB_LM_LAUNCH(TI, NP, 4); break;   \
+        default: CPB_LM_LAUNCH(TI, NP, NP); break; \
+    }
+        if (eltype == CPB_F64) {
+            if (gauss) {
+                CPB_LM_NF(double, 5)
+            } else {
+                CPB_LM_NF(double, 4)
+            }
+        } else {
+            if (gauss) {
+                CPB_LM_NF(float, 5)
+            } else {
+                CPB_LM_NF(float, 4)
+            }
+        }
+#undef CPB_LM_NF
+#undef CPB_LM_LAUNCH
+        check(cudaGetLastError(), "k_lm");
+        return;
+    }
+    const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
     KernelScope ks_(ctx, "k_lm", bytes);
     if (eltype == CPB_F64)
         k_lm<double><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
