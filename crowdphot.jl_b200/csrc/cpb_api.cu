@@ -290,6 +290,24 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
                         pp[nd.poff + ((ii % nd.isy) + (kk % nd.isx) * nd.isy) * plane + ii / nd.isy + (kk / nd.isx) * nd.PY] =
                             h64[nd.off + ii + kk * nd.ny];
             }
+            std::vector<double> lpp;
+            for (int k = 0; k < nn; ++k) {
+                DevNode& nd = nodes[k];
+                nd.LPY = (nd.ny + 2 + nd.isy - 1) / nd.isy;
+                nd.LPX = (nd.nx + 2 + nd.isx - 1) / nd.isx;
+                nd.lpoff = (int64_t)lpp.size();
+                const int64_t plane = (int64_t)nd.LPY * nd.LPX;
+                lpp.resize(lpp.size() + (size_t)(plane * nd.isy * nd.isx + 3) / 4 * 4, 0.0);
+                for (int64_t kk = 0; kk < nd.nx + 2; ++kk)
+                    for (int64_t ii = 0; ii < nd.ny + 2; ++ii) {
+                        const int64_t si = std::min<int64_t>(std::max<int64_t>(ii - 1, 0), nd.ny - 1);
+                        const int64_t sk = std::min<int64_t>(std::max<int64_t>(kk - 1, 0), nd.nx - 1);
+                        lpp[nd.lpoff + ((ii % nd.isy) + (kk % nd.isx) * nd.isy) * plane + ii / nd.isy +
+                            (kk / nd.isx) * nd.LPY] = h64[nd.off + si + sk * nd.ny];
+                    }
+            }
+            check(cudaMalloc(&ps->d_lpp64, sizeof(double) * std::max<size_t>(lpp.size(), 1)), "cudaMalloc");
+            check(cudaMemcpy(ps->d_lpp64, lpp.data(), sizeof(double) * lpp.size(), cudaMemcpyHostToDevice), "h2d");
             std::vector<float> pp32(pp.size());
             for (size_t q = 0; q < pp.size(); ++q) pp32[q] = (float)pp[q];
             check(cudaMalloc(&ps->d_pp64, sizeof(double) * std::max<size_t>(pp.size(), 1)), "cudaMalloc");
@@ -315,6 +333,7 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
             dp.data32 = ps->d_data32;
             dp.pp64 = ps->d_pp64;
             dp.pp32 = ps->d_pp32;
+            dp.lpp64 = ps->d_lpp64;
             dp.nodes = ps->d_nodes;
             dp.ygrid = ps->d_ygrid;
             dp.xgrid = ps->d_xgrid;
@@ -328,6 +347,7 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
             cudaFree(ps->d_data32);
             cudaFree(ps->d_pp64);
             cudaFree(ps->d_pp32);
+            cudaFree(ps->d_lpp64);
             cudaFree(ps->d_nodes);
             cudaFree(ps->d_ygrid);
             cudaFree(ps->d_xgrid);
@@ -348,6 +368,7 @@ int cpb_psf_free(cpb_ctx* ctx, cpb_psf* ps) {
         cudaFree(ps->d_data32);
         cudaFree(ps->d_pp64);
         cudaFree(ps->d_pp32);
+        cudaFree(ps->d_lpp64);
         cudaFree(ps->d_nodes);
         cudaFree(ps->d_ygrid);
         cudaFree(ps->d_xgrid);

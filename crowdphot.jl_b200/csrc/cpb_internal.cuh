@@ -34,6 +34,13 @@ struct DevNode {
     int64_t poff;
     int32_t PY, PX;     // ceil(ny / isy), ceil(nx / isx)
     int32_t isy, isx;   // integer oversampling (the reference's oversampling is a pair of Ints)
+    // edge-padded polyphase copy (fit_star): the node with one replicated sample
+    // on every side, so that a clamped stencil (empirical_models.jl:270-285) reads
+    // the same values as an interior one; padded sample (i + 1, k + 1) lives at
+    // lpoff + (((i + 1) % isy) + ((k + 1) % isx) * isy) * LPY * LPX
+    //       + (i + 1) / isy + ((k + 1) / isx) * LPY.
+    int64_t lpoff;
+    int32_t LPY, LPX;   // ceil((ny + 2) / isy), ceil((nx + 2) / isx)
 };
 
 constexpr int kMaxNodes = 64;
@@ -47,6 +54,7 @@ struct DevPsf {
     const float* data32;
     const double* pp64;       // polyphase copies of the node data (see DevNode)
     const float* pp32;
+    const double* lpp64;      // edge-padded polyphase copies (see DevNode)
     const DevNode* nodes;     // n_nodes
     const double* ygrid;      // gny
     const double* xgrid;      // gnx
@@ -270,6 +278,7 @@ struct cpb_psf {
     float* d_data32 = nullptr;
     double* d_pp64 = nullptr;
     float* d_pp32 = nullptr;
+    double* d_lpp64 = nullptr;
     cpb::DevNode* d_nodes = nullptr;
     double* d_ygrid = nullptr;
     double* d_xgrid = nullptr;

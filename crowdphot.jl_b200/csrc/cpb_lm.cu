@@ -362,11 +362,12 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
 
 // ---------------------------------------------------------------------------
 // Fast form: compile-time parameter counts (every small matrix in registers),
-// single-node image PSFs read through the polyphase copy (the 16 stencil taps
-// of the 32 lanes' pixels -- consecutive cutout rows -- are adjacent doubles),
-// and a device work queue over the cutouts.  Arithmetic per pixel is the same
-// as corner_eval's (psf_fitting.jl:1233-1321 restated), so results match the
-// general kernel's to the last bit where the stencil is interior.
+// single-node image PSFs read through the edge-padded polyphase copy (the 16
+// stencil taps of the 32 lanes' pixels -- consecutive cutout rows -- are
+// adjacent doubles, staged in shared memory), only the cutout rectangle that
+// can reach the ePSF grid evaluated in full, and a device work queue over the
+// cutouts.  Arithmetic per pixel is corner_eval's (psf_fitting.jl:1233-1321
+// restated); only the order of the per-lane sums differs.
 // ---------------------------------------------------------------------------
 template <int NF>
 __device__ __forceinline__ bool chol_solve_t(const double* A, const double* b, double* x) {
@@ -436,47 +437,62 @@ __device__ __forceinline__ void pp_taps(int i0, int is, float inv_is, int pstrid
 }
 
 struct PPNode {
-    const double* pp;   // this node's polyphase block
-    const double* dat;  // this node's column-major data (edge stencils)
+    const double* pp;   // this node's edge-padded polyphase block (DevNode::lpoff)
     DevNode nd;
-    int plane;          // PY * PX
+    int plane;          // LPY * LPX
     float inv_isy, inv_isx;
+};
+
+// Stencil offsets of the previous pixel a lane evaluated (ly = lx = 0: none).
+struct TapCursor {
+    int ly, lx;
+    int ry[4], cx[4];
 };
 
 // Single-node image profile and its derivatives in the detector frame:
 // s, dsdY = -sy * dp/dv, dsdX = -sx * dp/du (grid_profile with weights (1, 0, 0, 0)).
-__device__ __forceinline__ void pp_profile(const PPNode& N, double Y, double X, double py, double px, double& s,
-                                           double& dY, double& dX) {
+// pp: the node's edge-padded polyphase samples (shared or global memory), so the
+// clamped stencils at the grid's border need no special case.  (di, dj): how far
+// the cutout row / column moved since the lane's previous pixel; when the
+// stencil origin moved by whole oversampling periods the cached tap offsets are
+// advanced instead of recomputed.
+__device__ __forceinline__ void pp_profile(const PPNode& N, const double* pp, TapCursor& T, int di, int dj, double Y,
+                                           double X, double py, double px, double& s, double& dY, double& dX) {
     const DevNode& nd = N.nd;
     const double u = nd.sx * (px - X) + nd.ox;
     const double v = nd.sy * (py - Y) + nd.oy;
     const int nyd = nd.ny, nxd = nd.nx;
-    const bool inb = isfinite(u) && isfinite(v) && u >= 1.0 && u <= (double)nxd && v >= 1.0 && v <= (double)nyd;
+    // NaN and infinite u, v fail these range tests, as isfinite would
+    const bool inb = u >= 1.0 && u <= (double)nxd && v >= 1.0 && v <= (double)nyd;
     if (!inb) {
         s = nd.fill;
         dY = 0.0;
         dX = 0.0;
+        T.ly = T.lx = 0;
         return;
     }
     const int lx = clampi((int)floor(u), 1, nxd - 1);
     const int ly = clampi((int)floor(v), 1, nyd - 1);
-    if (lx < 2 || ly < 2 || lx + 2 > nxd || ly + 2 > nyd) {  // clamped stencil: the general evaluator
-        double pv, pdv, pdu;
-        corner_eval<double, double, true>(N.dat, nd, Y, X, py, px, pv, pdv, pdu);
-        s = pv;
-        dY = 0.0 * pv - 1.0 * nd.sy * pdv;
-        dX = 0.0 * pv - 1.0 * nd.sx * pdu;
-        return;
-    }
     const double du = u - (double)lx, dv = v - (double)ly;
-    int ry[4], cx[4];
-    pp_taps(ly - 2, nd.isy, N.inv_isy, N.plane, 1, ry);
-    pp_taps(lx - 2, nd.isx, N.inv_isx, nd.isy * N.plane, nd.PY, cx);
+    if (T.ly != 0 && ly == T.ly + nd.isy * di) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) T.ry[k] += di;
+    } else {
+        pp_taps(ly - 1, nd.isy, N.inv_isy, N.plane, 1, T.ry);  // padded index of sample ly - 2
+    }
+    if (T.lx != 0 && lx == T.lx + nd.isx * dj) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) T.cx[k] += dj * nd.LPY;
+    } else {
+        pp_taps(lx - 1, nd.isx, N.inv_isx, nd.isy * N.plane, nd.LPY, T.cx);
+    }
+    T.ly = ly;
+    T.lx = lx;
     double row[4], drow[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const double a = __ldg(N.pp + ry[r] + cx[0]), b = __ldg(N.pp + ry[r] + cx[1]);
-        const double c = __ldg(N.pp + ry[r] + cx[2]), e = __ldg(N.pp + ry[r] + cx[3]);
+        const double* q = pp + T.ry[r];
+        const double a = q[T.cx[0]], b = q[T.cx[1]], c = q[T.cx[2]], e = q[T.cx[3]];
         const double k1 = (c - a) / 2;
         const double k4 = c - b - k1;
         const double k2 = 3 * k4 - (e - b) / 2 + k1;
@@ -496,14 +512,14 @@ __device__ __forceinline__ void pp_profile(const PPNode& N, double Y, double X, 
     const double u3 = u4 - u2;
     const double pdu = dv * (dv * (dv * u3 + u2) + u1) + drow[1];
     s = pv;
-    dY = 0.0 * pv - 1.0 * nd.sy * pdv;
-    dX = 0.0 * pv - 1.0 * nd.sx * pdu;
+    dY = -(nd.sy * pdv);
+    dX = -(nd.sx * pdu);
 }
 
 // Normal equations of one cutout at the full parameter vector fv, projected onto
 // the free set (A: NF x NF column-major, b: NF); every lane returns the same cost.
 template <typename TI, int NP, int NF>
-__device__ double lm_accum_t(const PPNode& N, const LMConst& L, const TI* __restrict__ pix,
+__device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L, const TI* __restrict__ pix,
                              const TI* __restrict__ iv, int ny, int nx, int y1, int x1, int q32, int r32,
                              const double* fv, double* A, double* b) {
     constexpr int NT = NP * (NP + 1) / 2;
@@ -514,36 +530,8 @@ __device__ double lm_accum_t(const PPNode& N, const LMConst& L, const TI* __rest
 #pragma unroll
     for (int q = 0; q < NP; ++q) bf[q] = 0;
     const int npx = ny * nx;
-    int i = lane % ny, j = lane / ny;
-    for (int e = lane; e < npx; e += 32) {
-        double gv[NP], mval;
-        const double py = (double)(y1 + i), px = (double)(x1 + j);
-        if (NP == 5) {  // CircularGaussianPSF (parametric_models.jl:79-115)
-            const double gp = -2.772588722239781;
-            const double Y = fv[0], X = fv[1], fwhm = fv[2], flux = fv[3], bkg = fv[4];
-            const double f2 = fwhm * fwhm;
-            const double norm = -(3.141592653589793 * f2 / gp);
-            const double amp = flux / norm, gf2 = gp / f2;
-            const double dx = px - X, dy = py - Y;
-            const double sq = (dx * dx + dy * dy) / f2;
-            const double g = exp(gp * sq);
-            const double Ag = amp * g;
-            mval = amp * g + bkg;
-            gv[0] = -2 * Ag * gf2 * dy;
-            gv[1] = -2 * Ag * gf2 * dx;
-            gv[2] = -2 * Ag * (1 + gp * sq) / fwhm;
-            gv[3] = g / norm;
-            gv[NP - 1] = 1.0;
-        } else {
-            double s, dY, dX;
-            pp_profile(N, fv[0], fv[1], py, px, s, dY, dX);
-            const double flux = fv[2];
-            mval = flux * s + fv[3];
-            gv[0] = flux * dY;
-            gv[1] = flux * dX;
-            gv[2] = s;
-            gv[NP - 1] = 1.0;
-        }
+    // one pixel's contribution: cost, b and the upper triangle of A
+    auto acc = [&](int e, double mval, const double* gv) {
         const double r = mval - (double)pix[e];
         double w = 1.0;
         if (iv) {
@@ -562,11 +550,89 @@ __device__ double lm_accum_t(const PPNode& N, const LMConst& L, const TI* __rest
                 ++t;
             }
         }
-        i += r32;
-        j += q32;
-        if (i >= ny) {
-            i -= ny;
-            ++j;
+    };
+    if (NP == 5) {  // CircularGaussianPSF (parametric_models.jl:79-115)
+        const double gp = -2.772588722239781;
+        const double Y = fv[0], X = fv[1], fwhm = fv[2], flux = fv[3], bkg = fv[NP - 1];
+        const double f2 = fwhm * fwhm;
+        const double norm = -(3.141592653589793 * f2 / gp);
+        const double amp = flux / norm, gf2 = gp / f2;
+        int i = lane % ny, j = lane / ny;
+        for (int e = lane; e < npx; e += 32) {
+            const double py = (double)(y1 + i), px = (double)(x1 + j);
+            const double dx = px - X, dy = py - Y;
+            const double sq = (dx * dx + dy * dy) / f2;
+            const double g = exp(gp * sq);
+            const double Ag = amp * g;
+            double gv[NP];
+            gv[0] = -2 * Ag * gf2 * dy;
+            gv[1] = -2 * Ag * gf2 * dx;
+            gv[2] = -2 * Ag * (1 + gp * sq) / fwhm;
+            gv[3] = g / norm;
+            gv[NP - 1] = 1.0;
+            acc(e, amp * g + bkg, gv);
+            i += r32;
+            j += q32;
+            if (i >= ny) {
+                i -= ny;
+                ++j;
+            }
+        }
+    } else {
+        const DevNode& nd = N.nd;
+        const double Y = fv[0], X = fv[1], flux = fv[2], bkg = fv[3];
+        // Cutout pixels outside [ilo, ihi] x [jlo, jhi] are at least one pixel
+        // (>= one grid sample) beyond the grid, so their profile is the fill
+        // value with zero derivatives; the rectangle is evaluated in full.
+        int ilo = 0, ihi = ny - 1, jlo = 0, jhi = nx - 1;
+        if (isfinite(Y) && isfinite(X)) {
+            const double ya = Y - (double)y1 + (1.0 - nd.oy) / nd.sy;
+            const double yb = Y - (double)y1 + ((double)nd.ny - nd.oy) / nd.sy;
+            const double xa = X - (double)x1 + (1.0 - nd.ox) / nd.sx;
+            const double xb = X - (double)x1 + ((double)nd.nx - nd.ox) / nd.sx;
+            ilo = (int)fmin(fmax(0.0, floor(ya) - 1.0), (double)ny);
+            ihi = (int)fmax(fmin((double)(ny - 1), ceil(yb) + 1.0), -1.0);
+            jlo = (int)fmin(fmax(0.0, floor(xa) - 1.0), (double)nx);
+            jhi = (int)fmax(fmin((double)(nx - 1), ceil(xb) + 1.0), -1.0);
+        }
+        const int ni = ihi - ilo + 1, nj = jhi - jlo + 1;
+        if (ni > 0 && nj > 0) {
+            const int nr = ni * nj, rq = 32 / ni, rr = 32 % ni;
+            int ii = lane % ni, jj = lane / ni, di = 0, dj = 0;
+            TapCursor T;
+            T.ly = T.lx = 0;
+            for (int k = lane; k < nr; k += 32) {
+                const int i = ilo + ii, j = jlo + jj;
+                double s, dY, dX;
+                pp_profile(N, pp, T, di, dj, Y, X, (double)(y1 + i), (double)(x1 + j), s, dY, dX);
+                const double gv[NP] = {flux * dY, flux * dX, s, 1.0};
+                acc(i + j * ny, flux * s + bkg, gv);
+                ii += rr;
+                jj += rq;
+                di = rr;
+                dj = rq;
+                if (ii >= ni) {
+                    ii -= ni;
+                    ++jj;
+                    di -= ni;
+                    ++dj;
+                }
+            }
+        }
+        if (ni < ny || nj < nx) {
+            const double s = nd.fill, dY = 0.0, dX = 0.0;
+            const double gv[NP] = {flux * dY, flux * dX, s, 1.0};
+            const double mval = flux * s + bkg;
+            int i = lane % ny, j = lane / ny;
+            for (int e = lane; e < npx; e += 32) {
+                if (!(i >= ilo && i <= ihi && j >= jlo && j <= jhi)) acc(e, mval, gv);
+                i += r32;
+                j += q32;
+                if (i >= ny) {
+                    i -= ny;
+                    ++j;
+                }
+            }
         }
     }
     // project onto the free set, then reduce only what the solve needs
@@ -618,14 +684,196 @@ __device__ void lm_cov_t(const double* A, double* cov) {
     if (!ok) lm_cov(A, NF, cov);
 }
 
-template <typename TI, int NP, int NF>
-__global__ void __launch_bounds__(64) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
-                                              const int64_t* __restrict__ offs, const int32_t* __restrict__ cny,
-                                              const int32_t* __restrict__ cnx, const int32_t* __restrict__ cy1,
-                                              const int32_t* __restrict__ cx1, const TI* __restrict__ pixels,
-                                              const TI* __restrict__ ivs, const double* __restrict__ init, LMOut out,
-                                              unsigned long long* __restrict__ queue) {
+// LM bookkeeping of one cutout, kept in shared memory between normal-equation
+// passes so that none of it occupies registers during the pixel loop.
+template <int NP, int NF>
+struct LMState {
+    double fv[NP], fc[NP];       // accepted / candidate full parameter vectors
+    double x[NF], xc[NF], d[NF], D[NF], b[NF], A[NF * NF];
+    double cost, cost_init, lam, prered;
+    int iter, phase;             // phase 0: the initial pass is pending
+    int conv, xconv, fconv, gconv;
+};
+
+// Consumes one normal-equation pass (cost_c, Ac, bc at S.fc) and prepares the
+// next candidate; returns true when the fit is over.  Every lane computes the
+// same values; lane 0 stores them.  lm_irls, levenberg_marquardt.jl:478-680.
+template <int NP, int NF>
+__device__ __forceinline__ bool lm_step(LMState<NP, NF>& S, const LMConst& L, double cost_c, const double* Ac,
+                                        const double* bc, int lane) {
+    double fv[NP], x[NF], A[NF * NF], b[NF], D[NF];
+    double cost, lam = S.lam;
+    int iter = S.iter;
+    int conv = S.conv, xconv = S.xconv, fconv = S.fconv, gconv = S.gconv;
+    bool done = false;
+    if (S.phase == 0) {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) fv[q] = S.fc[q];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) x[k] = pick<NP>(fv, L.fidx[k]);
+#pragma unroll
+        for (int k = 0; k < NF * NF; ++k) A[k] = Ac[k];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) b[k] = bc[k];
+        cost = cost_c;
+        if (lane == 0) S.cost_init = cost_c;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) D[k] = sqrt(fmax(A[k + k * NF], 1.0e-6));
+    } else {
+        cost = S.cost;
+        double d[NF], xc[NF];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            x[k] = S.x[k];
+            d[k] = S.d[k];
+            xc[k] = S.xc[k];
+            D[k] = S.D[k];
+            b[k] = S.b[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NF * NF; ++k) A[k] = S.A[k];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) fv[q] = S.fv[q];
+        const double prered = S.prered;
+        const bool accepted = cost_c < cost;
+        const double dcost = cost - cost_c;
+        const double ratio = prered > 0 ? dcost / prered : 0.0;
+        fconv = fabs(dcost) <= L.f_tol * (fabs(cost) + L.f_tol) && prered <= L.f_tol * (fabs(cost) + L.f_tol) &&
+                0.5 * ratio <= 1;
+        double nd = 0, nxv = 0;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            nd += (D[k] * d[k]) * (D[k] * d[k]);
+            nxv += (D[k] * x[k]) * (D[k] * x[k]);
+        }
+        xconv = sqrt(nd) <= L.x_tol * (sqrt(nxv) + L.x_tol) && (accepted || fconv);
+        if (accepted) {
+            cost = cost_c;
+            lam = fmax(lam / L.lambda_down, L.lambda_min);
+#pragma unroll
+            for (int k = 0; k < NF; ++k) x[k] = xc[k];
+#pragma unroll
+            for (int k = 0; k < NF * NF; ++k) A[k] = Ac[k];
+#pragma unroll
+            for (int k = 0; k < NF; ++k) b[k] = bc[k];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) fv[q] = S.fc[q];
+#pragma unroll
+            for (int k = 0; k < NF; ++k) D[k] = fmax(D[k], sqrt(A[k + k * NF]));
+            if (xconv || fconv) conv = 1, done = true;
+        } else {
+            if (xconv || fconv) conv = 1, done = true;
+            else lam = fmin(lam * L.lambda_up, L.lambda_max);
+        }
+    }
+    // next candidate (the head of the lm_irls loop)
+    double d[NF], xc[NF], fc[NP], prered = 0;
+    while (!done) {
+        if (iter >= L.max_iter) {
+            done = true;
+            break;
+        }
+        ++iter;
+        double gcos = 0;
+#pragma unroll
+        for (int k = 0; k < NF; ++k)
+            gcos = nan_max(gcos, fabs(b[k]) / (sqrt(A[k + k * NF] * cost) + 2.220446049250313e-16));
+        if (gcos <= L.g_tol) {
+            gconv = conv = 1;
+            done = true;
+            break;
+        }
+        double Ad[NF * NF];
+#pragma unroll
+        for (int k = 0; k < NF * NF; ++k) Ad[k] = A[k];
+        if (L.damping == CPB_DAMP_MARQUARDT) {
+#pragma unroll
+            for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam * fmax(Ad[k + k * NF], L.min_diagonal);
+        } else if (L.damping == CPB_DAMP_LEVENBERG) {
+#pragma unroll
+            for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam;
+        }
+        if (!chol_solve_t<NF>(Ad, b, d)) {
+            lam = fmin(lam * L.lambda_up, L.lambda_max);
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < NF; ++k) d[k] = -d[k];
+        double db = 0, dAd = 0;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) db += d[k] * b[k];
+#pragma unroll
+        for (int k = 0; k < NF; ++k)
+#pragma unroll
+            for (int r = 0; r < NF; ++r) dAd += d[k] * A[k + r * NF] * d[r];
+        prered = -2 * db - dAd;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) xc[k] = x[k] + d[k];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            double vq = fv[q];
+#pragma unroll
+            for (int k = 0; k < NF; ++k) vq = (L.fidx[k] == q) ? xc[k] : vq;
+            fc[q] = vq;
+        }
+        break;
+    }
+    __syncwarp();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) S.fv[q] = fv[q];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            S.x[k] = x[k];
+            S.D[k] = D[k];
+            S.b[k] = b[k];
+        }
+#pragma unroll
+        for (int k = 0; k < NF * NF; ++k) S.A[k] = A[k];
+        if (!done) {
+#pragma unroll
+            for (int k = 0; k < NF; ++k) {
+                S.d[k] = d[k];
+                S.xc[k] = xc[k];
+            }
+#pragma unroll
+            for (int q = 0; q < NP; ++q) S.fc[q] = fc[q];
+            S.prered = prered;
+        }
+        S.cost = cost;
+        S.lam = lam;
+        S.iter = iter;
+        S.phase = 1;
+        S.conv = conv;
+        S.xconv = xconv;
+        S.fconv = fconv;
+        S.gconv = gconv;
+    }
+    __syncwarp();
+    return done;
+}
+
+constexpr int kLMThreads = 256;
+
+template <typename TI, int NP, int NF, bool SMEM>
+__global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
+                                             const int64_t* __restrict__ offs, const int32_t* __restrict__ cny,
+                                             const int32_t* __restrict__ cnx, const int32_t* __restrict__ cy1,
+                                             const int32_t* __restrict__ cx1, const TI* __restrict__ pixels,
+                                             const TI* __restrict__ ivs, const double* __restrict__ init, LMOut out,
+                                             unsigned long long* __restrict__ queue) {
+    __shared__ LMState<NP, NF> states[kLMThreads / 32];
+    extern __shared__ double node_smem[];
+    LMState<NP, NF>& S = states[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    // the node's polyphase samples, staged once per (persistent) block
+    const double* pp = N.pp;
+    if (SMEM && NP == 4) {
+        const int nel = N.plane * N.nd.isy * N.nd.isx;
+        for (int k = threadIdx.x; k < nel; k += blockDim.x) node_smem[k] = N.pp[k];
+        __syncthreads();
+        pp = node_smem;
+    }
     for (;;) {
         unsigned long long cc = 0;
         if (lane == 0) cc = atomicAdd(queue, 1ull);
@@ -656,127 +904,53 @@ __global__ void __launch_bounds__(64) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
             continue;
         }
         const int q32 = 32 / ny, r32 = 32 % ny;
-        double fv[NP], x[NF], xc[NF], A[NF * NF], b[NF], Ac[NF * NF], bc[NF], Ad[NF * NF], d[NF], D[NF];
-#pragma unroll
-        for (int q = 0; q < NP; ++q) {
-            bool fr = false;
-#pragma unroll
-            for (int k = 0; k < NF; ++k) fr |= (L.fidx[k] == q);
-            fv[q] = fr ? init[c * NP + q] : L.fixv[q];
-        }
-#pragma unroll
-        for (int k = 0; k < NF; ++k) x[k] = pick<NP>(fv, L.fidx[k]);
-        double cost = lm_accum_t<TI, NP, NF>(N, L, pix, iv, ny, nx, y1, x1, q32, r32, fv, A, b);
-        const double cost_init = cost;
-#pragma unroll
-        for (int k = 0; k < NF; ++k) D[k] = sqrt(fmax(A[k + k * NF], 1.0e-6));
-        double lam = L.lambda_init;
-        bool xconv = false, fconv = false, gconv = false, conv = false;
-        int iter = 0;
-        while (iter < L.max_iter) {
-            ++iter;
-            double gcos = 0;
-#pragma unroll
-            for (int k = 0; k < NF; ++k)
-                gcos = nan_max(gcos, fabs(b[k]) / (sqrt(A[k + k * NF] * cost) + 2.220446049250313e-16));
-            if (gcos <= L.g_tol) {
-                gconv = conv = true;
-                break;
-            }
-#pragma unroll
-            for (int k = 0; k < NF * NF; ++k) Ad[k] = A[k];
-            if (L.damping == CPB_DAMP_MARQUARDT) {
-#pragma unroll
-                for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam * fmax(Ad[k + k * NF], L.min_diagonal);
-            } else if (L.damping == CPB_DAMP_LEVENBERG) {
-#pragma unroll
-                for (int k = 0; k < NF; ++k) Ad[k + k * NF] += lam;
-            }
-            if (!chol_solve_t<NF>(Ad, b, d)) {
-                lam = fmin(lam * L.lambda_up, L.lambda_max);
-                continue;
-            }
-#pragma unroll
-            for (int k = 0; k < NF; ++k) d[k] = -d[k];
-            double db = 0, dAd = 0;
-#pragma unroll
-            for (int k = 0; k < NF; ++k) db += d[k] * b[k];
-#pragma unroll
-            for (int k = 0; k < NF; ++k)
-#pragma unroll
-                for (int r = 0; r < NF; ++r) dAd += d[k] * A[k + r * NF] * d[r];
-            const double prered = -2 * db - dAd;
-#pragma unroll
-            for (int k = 0; k < NF; ++k) xc[k] = x[k] + d[k];
-            double fc[NP];
+        __syncwarp();
+        if (lane == 0) {
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
-                double vq = fv[q];
+                bool fr = false;
 #pragma unroll
-                for (int k = 0; k < NF; ++k) vq = (L.fidx[k] == q) ? xc[k] : vq;
-                fc[q] = vq;
+                for (int k = 0; k < NF; ++k) fr |= (L.fidx[k] == q);
+                S.fc[q] = fr ? init[c * NP + q] : L.fixv[q];
             }
-            const double cost_c = lm_accum_t<TI, NP, NF>(N, L, pix, iv, ny, nx, y1, x1, q32, r32, fc, Ac, bc);
-            const bool accepted = cost_c < cost;
-            const double dcost = cost - cost_c;
-            const double ratio = prered > 0 ? dcost / prered : 0.0;
-            fconv = fabs(dcost) <= L.f_tol * (fabs(cost) + L.f_tol) && prered <= L.f_tol * (fabs(cost) + L.f_tol) &&
-                    0.5 * ratio <= 1;
-            double nd = 0, nxv = 0;
+            S.iter = 0;
+            S.phase = 0;
+            S.lam = L.lambda_init;
+            S.conv = S.xconv = S.fconv = S.gconv = 0;
+        }
+        __syncwarp();
+        for (;;) {
+            double fc[NP], Ac[NF * NF], bc[NF];
 #pragma unroll
-            for (int k = 0; k < NF; ++k) {
-                nd += (D[k] * d[k]) * (D[k] * d[k]);
-                nxv += (D[k] * x[k]) * (D[k] * x[k]);
-            }
-            xconv = sqrt(nd) <= L.x_tol * (sqrt(nxv) + L.x_tol) && (accepted || fconv);
-            if (accepted) {
-                cost = cost_c;
-                lam = fmax(lam / L.lambda_down, L.lambda_min);
-#pragma unroll
-                for (int k = 0; k < NF; ++k) x[k] = xc[k];
-#pragma unroll
-                for (int k = 0; k < NF * NF; ++k) A[k] = Ac[k];
-#pragma unroll
-                for (int k = 0; k < NF; ++k) b[k] = bc[k];
-#pragma unroll
-                for (int q = 0; q < NP; ++q) fv[q] = fc[q];
-#pragma unroll
-                for (int k = 0; k < NF; ++k) D[k] = fmax(D[k], sqrt(A[k + k * NF]));
-                if (xconv || fconv) {
-                    conv = true;
-                    break;
-                }
-            } else {
-                if (xconv || fconv) {
-                    conv = true;
-                    break;
-                }
-                lam = fmin(lam * L.lambda_up, L.lambda_max);
-            }
+            for (int q = 0; q < NP; ++q) fc[q] = S.fc[q];
+            const double cost_c = lm_accum_t<TI, NP, NF>(N, pp, L, pix, iv, ny, nx, y1, x1, q32, r32, fc, Ac, bc);
+            if (lm_step<NP, NF>(S, L, cost_c, Ac, bc, lane)) break;
         }
         if (lane == 0) {
             const double dof = (double)(nobs - NF);
+            const double cost = S.cost;
             if (out.cov) {
                 double cov[NF * NF];
-                lm_cov_t<NF>(A, cov);
+                lm_cov_t<NF>(S.A, cov);
                 const double f = L.reweighted ? cost / dof : 1.0;
 #pragma unroll
                 for (int k = 0; k < NF * NF; ++k) out.cov[c * NF * NF + k] = cov[k] * f;
             }
             if (out.params)
 #pragma unroll
-                for (int q = 0; q < NP; ++q) out.params[c * NP + q] = fv[q];
+                for (int q = 0; q < NP; ++q) out.params[c * NP + q] = S.fv[q];
             if (out.cost) out.cost[c] = cost;
-            if (out.cost_init) out.cost_init[c] = cost_init;
+            if (out.cost_init) out.cost_init[c] = S.cost_init;
             if (out.chisq) out.chisq[c] = cost / dof;
-            if (out.lambda_final) out.lambda_final[c] = lam;
-            if (out.converged) out.converged[c] = conv;
-            if (out.x_converged) out.x_converged[c] = xconv;
-            if (out.f_converged) out.f_converged[c] = fconv;
-            if (out.g_converged) out.g_converged[c] = gconv;
-            if (out.iters) out.iters[c] = iter;
+            if (out.lambda_final) out.lambda_final[c] = S.lam;
+            if (out.converged) out.converged[c] = S.conv;
+            if (out.x_converged) out.x_converged[c] = S.xconv;
+            if (out.f_converged) out.f_converged[c] = S.fconv;
+            if (out.g_converged) out.g_converged[c] = S.gconv;
+            if (out.iters) out.iters[c] = S.iter;
             out.status[c] = 0;
         }
+        __syncwarp();
     }
 }
 
@@ -831,21 +1005,33 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
         PPNode N{};
         if (!gauss) {
             N.nd = psf->h_nodes[0];
-            N.pp = psf->dev.pp64 + N.nd.poff;
-            N.dat = psf->dev.data64 + N.nd.off;
-            N.plane = N.nd.PY * N.nd.PX;
+            N.pp = psf->dev.lpp64 + N.nd.lpoff;
+            N.plane = N.nd.LPY * N.nd.LPX;
             N.inv_isy = 1.0f / (float)N.nd.isy;
             N.inv_isx = 1.0f / (float)N.nd.isx;
         }
         auto* queue = (unsigned long long*)scratch(ctx, "lm_queue", sizeof(unsigned long long));
         check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st), "memset");
-        // 64-thread blocks: registers (150-250 a thread) rather than blocks bound residency,
-        // and small blocks let every SM fill to its register limit
-        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 63) / 64, (int64_t)ctx->n_sm * 16);
+        // two persistent 256-thread blocks an SM (128 registers a thread); the
+        // node's samples go to shared memory when two copies fit an SM
+        const size_t node_bytes = gauss ? 0 : sizeof(double) * (size_t)N.plane * N.nd.isy * N.nd.isx;
+        const bool smem = !gauss && node_bytes <= 100 * 1024;
+        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + kLMThreads - 1) / kLMThreads,
+                                                            (int64_t)ctx->n_sm * 2);
         KernelScope ks_(ctx, "k_lm", bytes);
-#define CPB_LM_LAUNCH(TI, NP, NF)                                                                               \
-    k_lm_t<TI, NP, NF><<<blocks, 64, 0, st>>>(n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix,     \
-                                               (const TI*)d_iv, d_init, o, queue)
+#define CPB_LM_LAUNCH(TI, NP, NF)                                                                                  \
+    do {                                                                                                          \
+        if (smem) {                                                                                               \
+            check(cudaFuncSetAttribute(k_lm_t<TI, NP, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                       (int)node_bytes),                                                         \
+                  "smem attribute");                                                                             \
+            k_lm_t<TI, NP, NF, true><<<blocks, kLMThreads, node_bytes, st>>>(                                     \
+                n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix, (const TI*)d_iv, d_init, o, queue); \
+        } else {                                                                                                  \
+            k_lm_t<TI, NP, NF, false><<<blocks, kLMThreads, 0, st>>>(                                             \
+                n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix, (const TI*)d_iv, d_init, o, queue); \
+        }                                                                                                         \
+    } while (0)
 #define CPB_LM_NF(TI, NP)                          \
     switch (L.nf) {                                \
         case 1: CPB_LM_LAUNCH(TI, NP, 1); break;   \
