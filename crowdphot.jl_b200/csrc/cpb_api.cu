@@ -125,11 +125,17 @@ int cpb_ctx_create(int device, cpb_ctx** out) {
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
-        cudaMallocHost(&ctx->pinned, 4096) != cudaSuccess) {
+        cudaMallocHost(&ctx->pinned, 4096) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
         delete ctx;
         return CPB_ERR_CUDA;
     }
+    for (int k = 0; k < cpb_ctx::kCopyEvents; ++k)
+        if (cudaEventCreateWithFlags(&ctx->copy_ev[k], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return CPB_ERR_CUDA;
+        }
     cudaDeviceGetAttribute(&ctx->n_sm, cudaDevAttrMultiProcessorCount, device);
     *out = ctx;
     return CPB_OK;
@@ -152,6 +158,10 @@ int cpb_ctx_destroy(cpb_ctx* ctx) {
         }
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+        for (auto e : ctx->copy_ev)
+            if (e) cudaEventDestroy(e);
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
     }
     delete ctx;

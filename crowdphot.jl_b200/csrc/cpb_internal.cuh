@@ -300,6 +300,10 @@ struct cpb_ctx {
     };
     std::map<std::string, Buf> bufs;  // grow-only scratch arena, reused across calls
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // second stream for uploads that overlap kernels, with its hand-off events
+    cudaStream_t copy_stream = nullptr;
+    static constexpr int kCopyEvents = 16;
+    cudaEvent_t copy_ev[kCopyEvents] = {};
     void* pinned = nullptr;  // small pinned staging for scalar readbacks
     // kernel instrumentation: launch counter (always on) and, when profiling is
     // enabled, CUDA-event timing of every launch on this context's stream

@@ -1096,9 +1096,9 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     const int32_t* d_nx = (const int32_t*)up("lm_nx", nx, sizeof(int32_t) * n_cut);
     const int32_t* d_y1 = (const int32_t*)up("lm_y1", y_origin, sizeof(int32_t) * n_cut);
     const int32_t* d_x1 = (const int32_t*)up("lm_x1", x_origin, sizeof(int32_t) * n_cut);
-    const void* d_pix = up("lm_pix", pixels, esz * total);
-    const void* d_iv = inv_var ? up("lm_iv", inv_var, esz * total) : nullptr;
     const double* d_init = (const double*)up("lm_init", init, sizeof(double) * n_cut * L.np);
+    char* d_pix = (char*)scratch(ctx, "lm_pix", std::max<size_t>(esz * total, 8));
+    char* d_iv = inv_var ? (char*)scratch(ctx, "lm_iv", std::max<size_t>(esz * total, 8)) : nullptr;
     // device outputs: one block, carved in the order of the host fields
     const size_t nd = (size_t)n_cut * (L.np + (out->cov ? L.nf * L.nf : 0) + 4);
     double* dd = (double*)scratch(ctx, "lm_out_f64", sizeof(double) * nd);
@@ -1118,7 +1118,44 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     o.g_converged = du + 3 * n_cut;
     o.iters = di;
     o.status = di + n_cut;
-    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total);
+    // Pixels and weights: when the cutouts are packed in order they go up in
+    // chunks on the copy stream, and chunk k is fitted while chunk k + 1 is in
+    // flight; otherwise in one piece.
+    bool ordered = true;
+    for (int64_t c = 1; c < n_cut && ordered; ++c)
+        ordered = offsets[c] >= offsets[c - 1] + (int64_t)ny[c - 1] * nx[c - 1];
+    const int64_t bytes_all = (int64_t)esz * total * (inv_var ? 2 : 1);
+    const int K = ordered ? (int)std::min<int64_t>({(int64_t)8, n_cut, std::max<int64_t>(1, bytes_all >> 25)}) : 1;
+    for (int k = 0; k < K; ++k) {
+        const int64_t c0 = n_cut * k / K, c1 = n_cut * (k + 1) / K;
+        if (c1 <= c0) continue;
+        const int64_t e0 = K == 1 ? 0 : offsets[c0];
+        const int64_t e1 = K == 1 ? total : offsets[c1 - 1] + (int64_t)ny[c1 - 1] * nx[c1 - 1];
+        cudaStream_t cs = ctx->copy_stream;
+        check(cudaMemcpyAsync(d_pix + esz * e0, (const char*)pixels + esz * e0, esz * (e1 - e0),
+                              cudaMemcpyHostToDevice, cs), "h2d pixels");
+        if (inv_var)
+            check(cudaMemcpyAsync(d_iv + esz * e0, (const char*)inv_var + esz * e0, esz * (e1 - e0),
+                                  cudaMemcpyHostToDevice, cs), "h2d inv_var");
+        cudaEvent_t ev = ctx->copy_ev[k % cpb_ctx::kCopyEvents];
+        check(cudaEventRecord(ev, cs), "event");
+        check(cudaStreamWaitEvent(st, ev, 0), "wait");
+        LMOut ok = o;
+        ok.params += c0 * L.np;
+        if (ok.cov) ok.cov += c0 * L.nf * L.nf;
+        ok.cost += c0;
+        ok.cost_init += c0;
+        ok.chisq += c0;
+        ok.lambda_final += c0;
+        ok.converged += c0;
+        ok.x_converged += c0;
+        ok.f_converged += c0;
+        ok.g_converged += c0;
+        ok.iters += c0;
+        ok.status += c0;
+        launch_lm(ctx, psf, L, c1 - c0, d_off + c0, d_ny + c0, d_nx + c0, d_y1 + c0, d_x1 + c0, d_pix, eltype,
+                  d_iv, d_init + c0 * L.np, ok, e1 - e0);
+    }
     check(cudaEventRecord(ctx->ev1, st), "event");
     auto down = [&](void* h, const void* d, size_t bytes) {
         if (h) check(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st), "d2h");

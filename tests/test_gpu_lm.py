@@ -97,14 +97,16 @@ def test_fit_star_errors():
 
 def test_packed_cutouts_host_and_device_entries_match_oracle():
     """The C4 cutout workload (isolated stars, sides 9..41, SNR 5..1000, float32
-    pixels): host-buffer entry, device-buffer entry and the oracle agree cutout by cutout."""
+    pixels): host-buffer entry, device-buffer entry and the oracle agree cutout by cutout.
+    12,000 cutouts are 69 MB of pixels and weights, so the host entry uploads them
+    in two chunks that overlap the fits."""
     import torch
     from crowdphot_b200 import _abi
     from crowdphot_b200.photometry import _lm_outputs, _lm_result_struct, lm_params
     from crowdphot_b200.simulate import lm_cutouts
     from oracle.ffi import orc_fit_star_packed
     psf = moffat_epsf()
-    d = lm_cutouts(3000, seed=41)
+    d = lm_cutouts(12000, seed=41)
     args = (d["pix"], d["offsets"], d["ny"], d["nx"], d["y1"], d["x1"], d["init"])
     fixed = {"bkg": 0.0}
     host = cpb.fit_star_packed(psf, *args, inv_var=d["inv_var"], fixed=fixed)
