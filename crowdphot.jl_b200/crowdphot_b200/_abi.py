@@ -125,6 +125,25 @@ class SimResult(C.Structure):
     ]
 
 
+class GroupResult(C.Structure):
+    _fields_ = [
+        ("y", _dp), ("x", _dp), ("flux", _dp),
+        ("y_err", _dp), ("x_err", _dp), ("flux_err", _dp),
+        ("converged", _u8p), ("valid", _u8p),
+        ("n_iter", _i32p),
+        ("chisq", _dp),
+        ("qfit", _dp), ("qfit_expected", _dp), ("qfit_z", _dp), ("crowding", _dp),
+        ("residual", _dp),
+        ("n_passes", _i32p), ("n_failed", _i32p), ("status", _i32p),
+        ("error_kind", _i32p),
+        ("n_active", _i32p), ("n_union", _i32p),
+        ("n_trials", _i32p), ("n_lsqr_iters", _i32p),
+        ("n_kernel_groups", C.c_int64),
+        ("n_routed_groups", C.c_int64),
+        ("device_seconds", C.c_double),
+    ]
+
+
 class LMParams(C.Structure):
     _fields_ = [
         ("free_mask", C.c_int32),
@@ -187,6 +206,13 @@ PROTOTYPES = {
                                                       C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                                       C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                                       C.POINTER(SimResult)]),
+    "cpb_fit_simultaneous_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_int64, _i64p,
+                                             _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, _i64p,
+                                             _dp, _dp, _dp, C.POINTER(GroupResult)]),
+    "cpb_fit_simultaneous_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(SimParams), C.c_int64,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_int64, C.POINTER(GroupResult)]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
     "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,

@@ -406,6 +406,144 @@ def fit_all_stars_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_
     return outs.result(ny, nx, S2)
 
 
+_GROUP_ERRORS = {
+    1: "the image contains non-finite values but `inv_var` was not provided; pass `inv_var` to mask them or clean "
+       "the image first",
+    2: "InexactError: a star's integer anchor is negative (Morton key of a negative coordinate)",
+}
+
+
+def group_outputs(n_stars, n_groups, total_pixels=0, residual=False):
+    """Caller-owned output arrays of one cpb_group_result (numpy, host)."""
+    ns, G = max(n_stars, 1), max(n_groups, 1)
+    o = {k: np.zeros(ns) for k in ("y", "x", "flux", "y_err", "x_err", "flux_err", "chisq", "qfit",
+                                   "qfit_expected", "qfit_z", "crowding")}
+    o.update(converged=np.zeros(ns, np.uint8), valid=np.zeros(ns, np.uint8), n_iter=np.zeros(ns, np.int32))
+    o.update({k: np.zeros(G, np.int32) for k in ("n_passes", "n_failed", "status", "error_kind", "n_active",
+                                                 "n_union", "n_trials", "n_lsqr_iters")})
+    if residual:
+        o["residual"] = np.zeros(max(total_pixels, 1))
+    return o
+
+
+def group_result_struct(o, ptr):
+    """cpb_group_result over the arrays of `o`; ptr(array) gives its address (host or device)."""
+    r = _abi.GroupResult()
+    for name, _ in _abi.GroupResult._fields_:
+        if name in o:
+            setattr(r, name, C.cast(C.c_void_p(ptr(o[name])), dict(_abi.GroupResult._fields_)[name]))
+    return r
+
+
+def fit_groups_packed(psf, pixels, offsets, ny, nx, star_offsets, y0, x0, flux0, fit_rad, *, inv_var=None,
+                      background=None, fixed=None, ctx: Context | None = None, residual=False, **kw):
+    """Many independent fit_all_stars_simultaneous calls in one batch, packed form.
+
+    Group g's image is the column-major block pixels[offsets[g] : offsets[g] + ny[g]*nx[g]] (inv_var and
+    background share the layout); its catalogue is y0/x0/flux0[star_offsets[g] : star_offsets[g+1]] in the
+    group's own 1-based coordinates.  Returns the per-star and per-group output arrays of cpb_group_result
+    plus the batch counters.  Keyword arguments are those of fit_all_stars_simultaneous."""
+    fixed = dict(fixed or {})
+    ctx = ctx or get_context()
+    pix = np.ascontiguousarray(pixels)
+    dt = np.float32 if pix.dtype == np.float32 else np.float64
+    pix = np.ascontiguousarray(pix, dtype=dt)
+    iv = None if inv_var is None else np.ascontiguousarray(inv_var, dtype=dt)
+    bk = None if background is None else np.ascontiguousarray(background, dtype=dt)
+    et = _abi.CPB_F32 if dt == np.float32 else _abi.CPB_F64
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    nyv = np.ascontiguousarray(ny, dtype=np.int32)
+    nxv = np.ascontiguousarray(nx, dtype=np.int32)
+    so = np.ascontiguousarray(star_offsets, dtype=np.int64)
+    G = off.size
+    if nyv.size != G or nxv.size != G or so.size != G + 1:
+        raise ArgumentError("offsets, ny, nx must have one entry per group and star_offsets one more")
+    ys, xs, fs = (np.ascontiguousarray(a, dtype=np.float64) for a in (y0, x0, flux0))
+    if not (ys.size == xs.size == fs.size == (so[-1] if G else 0)):
+        raise ArgumentError("catalogue lengths must equal star_offsets[end]")
+    P = sim_params(psf, fit_rad, fixed, inv_var_given=iv is not None, **kw)
+    o = group_outputs(int(ys.size), G, int(pix.size), residual=residual)
+    r = group_result_struct(o, lambda a: a.ctypes.data)
+    hp = ctx.psf_handle(psf)
+    vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    rc = ctx.lib.cpb_fit_simultaneous_batch(ctx.handle, hp, C.byref(P), G, off.ctypes.data_as(_abi._i64p),
+                                            nyv.ctypes.data_as(_abi._i32p), nxv.ctypes.data_as(_abi._i32p), vp(pix),
+                                            et, vp(iv), vp(bk), so.ctypes.data_as(_abi._i64p),
+                                            ys.ctypes.data_as(_abi._dp), xs.ctypes.data_as(_abi._dp),
+                                            fs.ctypes.data_as(_abi._dp), C.byref(r))
+    ctx.raise_for(rc, "cpb_fit_simultaneous_batch")
+    ns = int(ys.size)
+    res = {k: (v[:ns] if v.size >= ns and k not in ("n_passes", "n_failed", "status", "error_kind", "n_active",
+                                                     "n_union", "n_trials", "n_lsqr_iters", "residual") else v)
+           for k, v in o.items()}
+    for k in ("n_passes", "n_failed", "status", "error_kind", "n_active", "n_union", "n_trials", "n_lsqr_iters"):
+        res[k] = o[k][:G]
+    res.update(n_kernel_groups=int(r.n_kernel_groups), n_routed_groups=int(r.n_routed_groups),
+               device_seconds=float(r.device_seconds))
+    return res
+
+
+def fit_all_stars_simultaneous_batch(images, psf, sources_list, fit_rad, *, inv_vars=None, backgrounds=None,
+                                     fixed=None, ctx: Context | None = None, residual=True,
+                                     **kw) -> list[MultiPassPhotResult]:
+    """fit_all_stars_simultaneous on each (image, sources) pair, all in one batch
+    (psf_photometry_simultaneous.jl:953-1431 per group).  A group that fails the
+    reference's data checks raises its ArgumentError, as the single call would."""
+    G = len(images)
+    if len(sources_list) != G:
+        raise ArgumentError("one catalogue per image is required")
+    arrs = [_image_arrays(im, None if inv_vars is None else inv_vars[g],
+                          None if backgrounds is None else backgrounds[g]) for g, im in enumerate(images)]
+    ets = {a[3] for a in arrs}
+    if len(ets) > 1:
+        raise ArgumentError("all images of a batch must share one element type")
+    if inv_vars is not None and any(a[1] is None for a in arrs):
+        raise ArgumentError("inv_vars must give one array per image")
+    cats = [_catalog(s) for s in sources_list]
+    sizes = np.array([a[0].size for a in arrs], np.int64)
+    offs = np.zeros(G, np.int64)
+    offs[1:] = np.cumsum(sizes)[:-1]
+    flat = lambda k: np.concatenate([a[k].ravel(order="F") for a in arrs]) if G else np.zeros(0)
+    pix = flat(0)
+    iv = flat(1) if inv_vars is not None else None
+    bk = flat(2) if backgrounds is not None else None
+    so = np.zeros(G + 1, np.int64)
+    so[1:] = np.cumsum([c[0].size for c in cats])
+    cat = lambda k: np.concatenate([c[k] for c in cats]) if G else np.zeros(0)
+    out = fit_groups_packed(psf, pix, offs, [a[0].shape[0] for a in arrs], [a[0].shape[1] for a in arrs], so,
+                            cat(0), cat(1), cat(2), fit_rad, inv_var=iv, background=bk, fixed=fixed, ctx=ctx,
+                            residual=residual, **kw)
+    fixed = dict(fixed or {})
+    results = []
+    for g in range(G):
+        if out["status"][g] != 0:
+            raise ArgumentError(_GROUP_ERRORS.get(int(out["error_kind"][g]), "invalid group input"))
+        s0, s1 = so[g], so[g + 1]
+        n = int(s1 - s0)
+        sl = slice(s0, s1)
+        ny_, nx_ = arrs[g][0].shape
+        nan = np.full(n, np.nan)
+        valid = out["valid"][sl].astype(bool)
+        msgs = [] if out["n_active"][g] == n else [
+            f"star {i + 1}: excluded before the solve (no usable pixels or non-finite initial parameters)"
+            for i in range(n) if not valid[i]]
+        resid = (out["residual"][offs[g]:offs[g] + sizes[g]].reshape((ny_, nx_), order="F").copy()
+                 if residual else np.zeros((ny_, nx_)))
+        results.append(MultiPassPhotResult(
+            y=out["y"][sl].copy(), x=out["x"][sl].copy(), y_err=out["y_err"][sl].copy(),
+            x_err=out["x_err"][sl].copy(), flux=out["flux"][sl].copy(), flux_err=out["flux_err"][sl].copy(),
+            bkg=np.full(n, float(fixed.get("bkg", 0.0))), bkg_err=np.zeros(n),
+            converged=out["converged"][sl].astype(bool), valid=valid, chisq=out["chisq"][sl].copy(),
+            qfit=out["qfit"][sl].copy(), qfit_expected=out["qfit_expected"][sl].copy(),
+            qfit_z=out["qfit_z"][sl].copy(), crowding=out["crowding"][sl].copy(), spread_model=nan.copy(),
+            spread_model_err=nan.copy(), n_iter=out["n_iter"][sl].astype(np.int64),
+            n_passes=int(out["n_passes"][g]), n_failed=int(out["n_failed"][g]), failure_msgs=msgs, residual=resid,
+            stats=dict(n_active=int(out["n_active"][g]), n_union=int(out["n_union"][g]),
+                       n_trials=int(out["n_trials"][g]), n_lsqr_iters=int(out["n_lsqr_iters"][g]),
+                       batch_device_seconds=out["device_seconds"])))
+    return results
+
+
 def lm_params(model, fixed, *, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
               lambda_max=1.0e12, damping="marquardt", max_iter=200, x_tol=1.0e-8, f_tol=1.0e-4, g_tol=1.0e-4,
               covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64"):

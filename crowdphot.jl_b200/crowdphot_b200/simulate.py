@@ -301,3 +301,53 @@ def lm_cutouts(n, *, seed, psf=None, smin=9, smax=41, snr=(5.0, 1000.0), bkg=100
                      flux * rng.uniform(init_flux[0], init_flux[1], n), np.zeros(n)], axis=1)
     return dict(pix=pix, inv_var=iv, offsets=offsets, ny=sides.astype(np.int32), nx=sides.astype(np.int32),
                 y1=y1.astype(np.int32), x1=x1.astype(np.int32), init=init, truth=np.stack([yc, xc, flux], 1))
+
+
+def lm_groups(n, *, seed, psf=None, kmin=2, kmax=12, snr=(5.0, 1000.0), bkg=100.0, read_noise=5.0, gain=1.0,
+              dtype=np.float32, init_sigma=0.3, init_flux=(0.9, 1.1), chunk=8192):
+    """Blended groups for the batched simultaneous fit: group g holds k ~ U{kmin..kmax}
+    stars placed uniformly in a (8k + 17)^2 cutout, fluxes from an SNR drawn log-uniform
+    in `snr` via flux_for_snr (bkg 100, read noise 5, gain 1), Poisson + Gaussian noise,
+    background subtracted, inverse-variance weights, perturbed initial guesses.  Groups
+    are packed like lm_cutouts (column-major each, offsets, sides) with star offsets
+    into the concatenated catalogue (coordinates local to each group, 1-based)."""
+    rng = np.random.default_rng(seed)
+    psf = psf if psf is not None else moffat_epsf()
+    node = psf.psfs[0] if isinstance(psf, GriddedPSFModel) else psf
+    k = rng.integers(kmin, kmax + 1, n)
+    side = (8 * k + 17).astype(np.int64)
+    sizes = side * side
+    offsets = np.zeros(n, np.int64)
+    offsets[1:] = np.cumsum(sizes)[:-1]
+    star_off = np.zeros(n + 1, np.int64)
+    star_off[1:] = np.cumsum(k)
+    ns = int(star_off[-1])
+    grp = np.repeat(np.arange(n), k)
+    sg = side[grp].astype(np.float64)
+    ys = rng.uniform(1.0, sg)
+    xs = rng.uniform(1.0, sg)
+    s = np.exp(rng.uniform(np.log(snr[0]), np.log(snr[1]), ns))
+    flux = flux_for_snr(node, s, background=bkg, read_noise=read_noise, gain=gain)
+    model = np.zeros(int(sizes.sum()), np.float64)
+    H = 13
+    box = 2 * H + 1
+    for c0 in range(0, ns, chunk):
+        sl = slice(c0, min(c0 + chunk, ns))
+        cy = np.round(ys[sl]).astype(np.int64)
+        cx = np.round(xs[sl]).astype(np.int64)
+        val = render_cutouts(node, ys[sl], xs[sl], flux[sl], cy - H, cx - H, box)  # (m, box, box)
+        gy = (cy - H)[:, None, None] + np.arange(box)[None, :, None]
+        gx = (cx - H)[:, None, None] + np.arange(box)[None, None, :]
+        gy, gx = np.broadcast_arrays(gy, gx)
+        sd = side[grp[sl]][:, None, None]
+        keep = (gy >= 1) & (gy <= sd) & (gx >= 1) & (gx <= sd)
+        flat = offsets[grp[sl]][:, None, None] + (gy - 1) + (gx - 1) * sd
+        np.add.at(model, flat[keep], val[keep])
+    img = rng.poisson(np.maximum(model + bkg, 0) * gain) / gain + read_noise * rng.standard_normal(model.size)
+    pix = (img - bkg).astype(dtype)
+    iv = (1.0 / (bkg + model + read_noise ** 2)).astype(dtype)
+    init_y = ys + rng.normal(0, init_sigma, ns)
+    init_x = xs + rng.normal(0, init_sigma, ns)
+    init_f = flux * rng.uniform(init_flux[0], init_flux[1], ns)
+    return dict(pix=pix, inv_var=iv, offsets=offsets, ny=side.astype(np.int32), nx=side.astype(np.int32),
+                star_offsets=star_off, y=init_y, x=init_x, flux=init_f, truth=np.stack([ys, xs, flux], 1))

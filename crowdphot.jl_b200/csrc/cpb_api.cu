@@ -428,6 +428,132 @@ int cpb_fit_simultaneous(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
     });
 }
 
+int cpb_fit_simultaneous_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                                      int64_t n_groups, const int64_t* d_pix_offsets, const int32_t* d_ny,
+                                      const int32_t* d_nx, const void* d_pixels, int32_t eltype,
+                                      const void* d_inv_var, const void* d_background,
+                                      const int64_t* d_star_offsets, const double* d_y0, const double* d_x0,
+                                      const double* d_flux0, int64_t total_pixels, cpb_group_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || (n_groups > 0 && (!d_pix_offsets || !d_ny || !d_nx || !d_pixels ||
+                                                         !d_star_offsets || !d_y0 || !d_x0 || !d_flux0)))
+            throw ArgError{"null argument"};
+        return fit_groups_dev(ctx, psf, params, n_groups, d_pix_offsets, d_ny, d_nx, d_pixels, eltype, d_inv_var,
+                              d_background, d_star_offsets, d_y0, d_x0, d_flux0, total_pixels, out, nullptr,
+                              nullptr, nullptr, nullptr);
+    });
+}
+
+int cpb_fit_simultaneous_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params, int64_t n_groups,
+                               const int64_t* pix_offsets, const int32_t* ny, const int32_t* nx, const void* pixels,
+                               int32_t eltype, const void* inv_var, const void* background,
+                               const int64_t* star_offsets, const double* y0, const double* x0, const double* flux0,
+                               cpb_group_result* out) {
+    return guarded(ctx, [&]() -> int {
+        if (!psf || !params || !out || n_groups < 0 || (n_groups > 0 && (!pix_offsets || !ny || !nx || !pixels ||
+                                                                          !star_offsets || !y0 || !x0 || !flux0)))
+            throw ArgError{"null argument"};
+        if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
+        if (!out->y || !out->x || !out->flux || !out->y_err || !out->x_err || !out->flux_err || !out->converged ||
+            !out->valid || !out->n_iter || !out->n_passes || !out->n_failed || !out->status)
+            throw ArgError{"null output array"};
+        const int64_t G = n_groups;
+        if (G == 0) {
+            out->n_kernel_groups = out->n_routed_groups = 0;
+            out->device_seconds = 0;
+            return CPB_OK;
+        }
+        int64_t npx = 0;
+        for (int64_t g = 0; g < G; ++g) {
+            if (ny[g] <= 0 || nx[g] <= 0) throw ArgError{"group image size out of range"};
+            if (pix_offsets[g] < 0) throw ArgError{"pixel offsets must be non-negative"};
+            npx = std::max<int64_t>(npx, pix_offsets[g] + (int64_t)ny[g] * nx[g]);
+        }
+        if (star_offsets[0] != 0) throw ArgError{"star_offsets[0] must be 0"};
+        for (int64_t g = 0; g < G; ++g)
+            if (star_offsets[g + 1] < star_offsets[g]) throw ArgError{"star_offsets must be non-decreasing"};
+        const int64_t ns = star_offsets[G];
+        const size_t esz = eltype == CPB_F64 ? 8 : 4;
+        cudaStream_t st = ctx->stream;
+        auto up = [&](const char* name, const void* src, size_t bytes) -> void* {
+            void* d = scratch(ctx, name, std::max<size_t>(bytes, 8));
+            if (src && bytes) check(cudaMemcpyAsync(d, src, bytes, cudaMemcpyHostToDevice, st), "h2d batch input");
+            return d;
+        };
+        const void* d_pix = up("gb_pix", pixels, esz * npx);
+        const void* d_iv = inv_var ? up("gb_iv", inv_var, esz * npx) : nullptr;
+        const void* d_bk = background ? up("gb_bkg", background, esz * npx) : nullptr;
+        const int64_t* d_off = (const int64_t*)up("gb_off", pix_offsets, 8 * G);
+        const int32_t* d_ny = (const int32_t*)up("gb_ny", ny, 4 * G);
+        const int32_t* d_nx = (const int32_t*)up("gb_nx", nx, 4 * G);
+        const int64_t* d_so = (const int64_t*)up("gb_soff", star_offsets, 8 * (G + 1));
+        const double* d_y = (const double*)up("gb_y0", y0, 8 * ns);
+        const double* d_x = (const double*)up("gb_x0", x0, 8 * ns);
+        const double* d_f = (const double*)up("gb_f0", flux0, 8 * ns);
+        // device outputs
+        cpb_group_result d = *out;
+        auto dout = [&](const char* name, void* host, size_t bytes) -> void* {
+            return host ? scratch(ctx, name, std::max<size_t>(bytes, 8)) : nullptr;
+        };
+        d.y = (double*)dout("gb_o_y", out->y, 8 * ns);
+        d.x = (double*)dout("gb_o_x", out->x, 8 * ns);
+        d.flux = (double*)dout("gb_o_f", out->flux, 8 * ns);
+        d.y_err = (double*)dout("gb_o_ey", out->y_err, 8 * ns);
+        d.x_err = (double*)dout("gb_o_ex", out->x_err, 8 * ns);
+        d.flux_err = (double*)dout("gb_o_ef", out->flux_err, 8 * ns);
+        d.converged = (uint8_t*)dout("gb_o_cv", out->converged, ns);
+        d.valid = (uint8_t*)dout("gb_o_va", out->valid, ns);
+        d.n_iter = (int32_t*)dout("gb_o_it", out->n_iter, 4 * ns);
+        d.chisq = (double*)dout("gb_o_chi", out->chisq, 8 * ns);
+        d.qfit = (double*)dout("gb_o_q1", out->qfit, 8 * ns);
+        d.qfit_expected = (double*)dout("gb_o_q2", out->qfit_expected, 8 * ns);
+        d.qfit_z = (double*)dout("gb_o_q3", out->qfit_z, 8 * ns);
+        d.crowding = (double*)dout("gb_o_cr", out->crowding, 8 * ns);
+        d.residual = (double*)dout("gb_o_res", out->residual, 8 * npx);
+        d.n_passes = (int32_t*)dout("gb_o_np", out->n_passes, 4 * G);
+        d.n_failed = (int32_t*)dout("gb_o_nf", out->n_failed, 4 * G);
+        d.status = (int32_t*)dout("gb_o_st", out->status, 4 * G);
+        d.error_kind = (int32_t*)dout("gb_o_ek", out->error_kind, 4 * G);
+        d.n_active = (int32_t*)dout("gb_o_na", out->n_active, 4 * G);
+        d.n_union = (int32_t*)dout("gb_o_nu", out->n_union, 4 * G);
+        d.n_trials = (int32_t*)dout("gb_o_nt", out->n_trials, 4 * G);
+        d.n_lsqr_iters = (int32_t*)dout("gb_o_nl", out->n_lsqr_iters, 4 * G);
+        fit_groups_dev(ctx, psf, params, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bk, d_so, d_y, d_x, d_f, npx, &d,
+                       pix_offsets, ny, nx, star_offsets);
+        auto down = [&](void* host, const void* dev, size_t bytes) {
+            if (host && bytes) check(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st), "d2h batch output");
+        };
+        down(out->y, d.y, 8 * ns);
+        down(out->x, d.x, 8 * ns);
+        down(out->flux, d.flux, 8 * ns);
+        down(out->y_err, d.y_err, 8 * ns);
+        down(out->x_err, d.x_err, 8 * ns);
+        down(out->flux_err, d.flux_err, 8 * ns);
+        down(out->converged, d.converged, ns);
+        down(out->valid, d.valid, ns);
+        down(out->n_iter, d.n_iter, 4 * ns);
+        down(out->chisq, d.chisq, 8 * ns);
+        down(out->qfit, d.qfit, 8 * ns);
+        down(out->qfit_expected, d.qfit_expected, 8 * ns);
+        down(out->qfit_z, d.qfit_z, 8 * ns);
+        down(out->crowding, d.crowding, 8 * ns);
+        down(out->residual, d.residual, 8 * npx);
+        down(out->n_passes, d.n_passes, 4 * G);
+        down(out->n_failed, d.n_failed, 4 * G);
+        down(out->status, d.status, 4 * G);
+        down(out->error_kind, d.error_kind, 4 * G);
+        down(out->n_active, d.n_active, 4 * G);
+        down(out->n_union, d.n_union, 4 * G);
+        down(out->n_trials, d.n_trials, 4 * G);
+        down(out->n_lsqr_iters, d.n_lsqr_iters, 4 * G);
+        check(cudaStreamSynchronize(st), "sync");
+        out->n_kernel_groups = d.n_kernel_groups;
+        out->n_routed_groups = d.n_routed_groups;
+        out->device_seconds = d.device_seconds;
+        return CPB_OK;
+    });
+}
+
 int cpb_fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, int64_t n_cutouts,
                      const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,
                      const int32_t* x_origin, const void* pixels, int32_t eltype, const void* inv_var,

@@ -374,6 +374,14 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                          int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out);
 
+// Batched simultaneous fits of small groups (cpb_groups.cu).  Device inputs and
+// outputs; the h_*_opt arrays (nullable) are host copies of the group metadata.
+int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
+                   const int32_t* d_ny, const int32_t* d_nx, const void* d_pix, int32_t eltype, const void* d_iv,
+                   const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
+                   const double* d_f0, int64_t total_pixels, cpb_group_result* out, const int64_t* h_off_opt,
+                   const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt);
+
 // Batched LM driver (cpb_lm.cu).  Host inputs.
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cutouts,
                  const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,

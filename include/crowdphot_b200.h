@@ -286,6 +286,72 @@ CPB_API int cpb_fit_simultaneous_device_noalloc(cpb_ctx* ctx, const cpb_psf* psf
                                                 const double* d_y0, const double* d_x0, const double* d_flux0,
                                                 cpb_sim_result* out);
 
+/* ---- many small simultaneous fits (star groups) ------------------------- */
+/*
+ * Results of a batch of independent fit_all_stars_simultaneous calls, one
+ * per group (a small field holding a blend of stars).  Per-star arrays have
+ * one entry per catalogue star, groups concatenated in order (group g's stars
+ * at star_offsets[g] .. star_offsets[g+1]); they mean what the same-named
+ * cpb_sim_result fields mean.  Per-group arrays have n_groups entries.
+ * status[g] is 0, or CPB_ERR_ARGUMENT when group g fails one of the
+ * reference's data checks (error_kind[g] = 1: the image holds non-finite
+ * values but no inv_var was given; 2: a star's integer anchor is negative);
+ * the per-star outputs of such a group hold its catalogue with NaN errors
+ * and valid = 0.  residual (optional) is packed like the pixels.  NULL skips
+ * an optional output.
+ */
+typedef struct cpb_group_result {
+    double *y, *x, *flux;
+    double *y_err, *x_err, *flux_err;
+    uint8_t *converged, *valid;
+    int32_t* n_iter;
+    double* chisq;                                     /* optional */
+    double *qfit, *qfit_expected, *qfit_z, *crowding;  /* optional */
+    double* residual;                                  /* optional, packed like the pixels */
+    int32_t *n_passes, *n_failed, *status;
+    int32_t* error_kind;                               /* optional */
+    int32_t *n_active, *n_union;                       /* optional */
+    int32_t *n_trials, *n_lsqr_iters;                  /* optional */
+    int64_t n_kernel_groups;  /* groups fitted by the one-block-per-group kernel */
+    int64_t n_routed_groups;  /* groups too large for it, fitted by the full-field path */
+    double device_seconds;
+} cpb_group_result;
+
+/*
+ * n_groups independent fit_all_stars_simultaneous calls sharing one PSF and
+ * one set of keyword arguments (psf_photometry_simultaneous.jl:953-1431,
+ * applied to each group).  Group g's image is the column-major block
+ * pixels[pix_offsets[g] .. pix_offsets[g] + ny[g]*nx[g]); inv_var and
+ * background (nullable) share the layout; its catalogue is y0/x0/flux0
+ * [star_offsets[g] .. star_offsets[g+1]) in the group's own 1-based pixel
+ * coordinates (star_offsets has n_groups + 1 entries).  Results equal those of
+ * cpb_fit_simultaneous on each group alone, within the parity tolerances
+ * (the batch sums its reductions in a different order).  Groups of at most
+ * 64 stars whose working set fits in shared memory are fitted by a
+ * persistent kernel, one thread block per group, from a device work queue;
+ * larger groups go through the full-field path.  precision must be
+ * CPB_PREC_FP64.  Host arrays.
+ */
+CPB_API int cpb_fit_simultaneous_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                                       int64_t n_groups, const int64_t* pix_offsets, const int32_t* ny,
+                                       const int32_t* nx, const void* pixels, int32_t eltype, const void* inv_var,
+                                       const void* background, const int64_t* star_offsets, const double* y0,
+                                       const double* x0, const double* flux0, cpb_group_result* out);
+
+/*
+ * cpb_fit_simultaneous_batch on device-resident groups (no counterpart in the
+ * reference): every array argument and every pointer in `out` is a device
+ * pointer on the context's device.  total_pixels = the pixel elements the
+ * groups span (sizes the residual; 0 is allowed when out->residual is NULL).
+ */
+CPB_API int cpb_fit_simultaneous_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
+                                              int64_t n_groups, const int64_t* d_pix_offsets, const int32_t* d_ny,
+                                              const int32_t* d_nx, const void* d_pixels, int32_t eltype,
+                                              const void* d_inv_var, const void* d_background,
+                                              const int64_t* d_star_offsets, const double* d_y0,
+                                              const double* d_x0, const double* d_flux0, int64_t total_pixels,
+                                              cpb_group_result* out);
+
 /* ---- batched per-star LM (fit_star) ------------------------------------- */
 /*
  * n_cutouts independent fit_star calls.  Cutout c is the column-major block
