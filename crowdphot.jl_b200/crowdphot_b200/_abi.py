@@ -144,6 +144,15 @@ class GroupResult(C.Structure):
     ]
 
 
+class TuneInfo(C.Structure):
+    _fields_ = [
+        ("lm_blocks_per_sm", C.c_int32), ("lm_node_in_smem", C.c_int32),
+        ("grp_threads", C.c_int32), ("grp_blocks_per_sm", C.c_int32),
+        ("from_cache", C.c_int32), ("n_timed", C.c_int32),
+        ("lm_ms", C.c_double), ("grp_ms", C.c_double),
+    ]
+
+
 class LMParams(C.Structure):
     _fields_ = [
         ("free_mask", C.c_int32),
@@ -213,6 +222,16 @@ PROTOTYPES = {
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                     C.c_void_p, C.c_int64, C.POINTER(GroupResult)]),
+    "cpb_batch_graph_create": (C.c_int, [C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64,
+                                         C.c_void_p,
+                                         C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_int64, C.c_void_p,
+                                         C.c_int32, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(TuneInfo)]),
+    "cpb_batch_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    "cpb_batch_graph_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
     "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,

@@ -544,6 +544,74 @@ def fit_all_stars_simultaneous_batch(images, psf, sources_list, fit_rad, *, inv_
     return results
 
 
+class BatchGraph:
+    """One captured CUDA graph that fits a batch of fit_star cutouts and a batch of
+    star groups concurrently (cpb_batch_graph_*).  Inputs and outputs are torch
+    tensors on the context's device, bound at construction: refill the inputs in
+    place and call launch() again.  `lm` holds the fit_star half
+    (offsets, ny, nx, y1, x1, pix, inv_var, init and the _lm_outputs tensors under
+    `out`), `groups` the group half (offsets, ny, nx, pix, inv_var, background,
+    star_offsets, y, x, flux and the group_outputs tensors under `out`); either
+    may be None.  autotune: 0 defaults, 1 tuned shapes (cached in cache_path),
+    2 re-tune."""
+
+    def __init__(self, psf, *, lm=None, lm_fixed=None, groups=None, fit_rad=None, group_kw=None,
+                 autotune=1, cache_path=None, ctx: Context | None = None):
+        self.ctx = ctx or get_context()
+        self._keep = []
+        hp = self.ctx.psf_handle(psf)
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        lm_args = [None, 0] + [None] * 6 + [0, None, None, 0, None]
+        if lm is not None:
+            P = lm_params(psf, dict(lm_fixed or {}))
+            r = _lm_result_struct(lm["out"], lambda a: a.data_ptr())
+            self._keep += [P, r]
+            et = _abi.CPB_F32 if str(lm["pix"].dtype) == "torch.float32" else _abi.CPB_F64
+            lm_args = [C.byref(P), int(lm["ny"].numel()), ptr(lm["offsets"]), ptr(lm["ny"]), ptr(lm["nx"]),
+                       ptr(lm["y1"]), ptr(lm["x1"]), ptr(lm["pix"]), et, ptr(lm.get("inv_var")), ptr(lm["init"]),
+                       int(lm["pix"].numel()), C.byref(r)]
+        g_args = [None, 0] + [None] * 4 + [0] + [None] * 6 + [0, None]
+        if groups is not None:
+            kw = dict(group_kw or {})
+            fixed = dict(kw.pop("fixed", {}) or {})
+            SP = sim_params(psf, fit_rad, fixed, inv_var_given=groups.get("inv_var") is not None, **kw)
+            gr = group_result_struct(groups["out"], lambda a: a.data_ptr())
+            self._keep += [SP, gr]
+            et = _abi.CPB_F32 if str(groups["pix"].dtype) == "torch.float32" else _abi.CPB_F64
+            g_args = [C.byref(SP), int(groups["ny"].numel()), ptr(groups["offsets"]), ptr(groups["ny"]),
+                      ptr(groups["nx"]), ptr(groups["pix"]), et, ptr(groups.get("inv_var")),
+                      ptr(groups.get("background")), ptr(groups["star_offsets"]), ptr(groups["y"]), ptr(groups["x"]),
+                      ptr(groups["flux"]), int(groups["pix"].numel()), C.byref(gr)]
+        self.handle = C.c_void_p()
+        self.info = _abi.TuneInfo()
+        rc = self.ctx.lib.cpb_batch_graph_create(self.ctx.handle, hp, *lm_args, *g_args, int(autotune),
+                                                 None if cache_path is None else str(cache_path).encode(),
+                                                 C.byref(self.handle), C.byref(self.info))
+        self.ctx.raise_for(rc, "cpb_batch_graph_create")
+        self.lm, self.groups = lm, groups
+
+    def launch(self) -> float:
+        """Replays the graph; returns its device time in seconds."""
+        t = C.c_double()
+        rc = self.ctx.lib.cpb_batch_graph_launch(self.ctx.handle, self.handle, C.byref(t))
+        self.ctx.raise_for(rc, "cpb_batch_graph_launch")
+        return float(t.value)
+
+    def tune_info(self) -> dict:
+        return {k: getattr(self.info, k) for k, _ in _abi.TuneInfo._fields_}
+
+    def close(self):
+        if self.handle:
+            self.ctx.lib.cpb_batch_graph_destroy(self.ctx.handle, self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def lm_params(model, fixed, *, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
               lambda_max=1.0e12, damping="marquardt", max_iter=200, x_tol=1.0e-8, f_tol=1.0e-4, g_tol=1.0e-4,
               covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64"):

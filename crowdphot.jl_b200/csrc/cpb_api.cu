@@ -81,29 +81,6 @@ void resolve_kernel_events(cpb_ctx* ctx) {
     ctx->pending.clear();
 }
 
-template <typename F>
-int guarded(cpb_ctx* ctx, F&& f) {
-    if (!ctx) return CPB_ERR_ARGUMENT;
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->err.clear();
-    try {
-        check(cudaSetDevice(ctx->device), "cudaSetDevice");
-        return f();
-    } catch (const ArgError& e) {
-        ctx->err = e.msg;
-        return CPB_ERR_ARGUMENT;
-    } catch (const OomError& e) {
-        ctx->err = e.msg;
-        return CPB_ERR_OOM;
-    } catch (const CudaError& e) {
-        ctx->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);
-        return CPB_ERR_CUDA;
-    } catch (const std::exception& e) {
-        ctx->err = e.what();
-        return CPB_ERR_INTERNAL;
-    }
-}
-
 }  // namespace cpb
 
 using namespace cpb;

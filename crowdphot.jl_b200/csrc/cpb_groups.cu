@@ -29,8 +29,10 @@
 // until the batch is done.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
+#include <string>
 #include <vector>
 
 #include "cpb_internal.cuh"
@@ -1151,13 +1153,33 @@ struct GroupPlan {
     size_t smem = 0;
 };
 
-}  // namespace
+// Everything a launch needs, derived once from the arguments.
+struct GroupSetup {
+    GroupConst C{};
+    DevPsf dp{};
+    GroupPlan plan;
+    GroupIn gin{};
+    GroupOut go{};
+    std::vector<int64_t> h_off, h_soff;
+    std::vector<int32_t> h_ny, h_nx;
+    int64_t total_pixels = 0;
+    int32_t eltype = CPB_F64;
+};
 
-int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
-                   const int32_t* d_ny, const int32_t* d_nx, const void* d_pix, int32_t eltype, const void* d_iv,
-                   const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
-                   const double* d_f0, int64_t total_pixels, cpb_group_result* out, const int64_t* h_off_opt,
-                   const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt) {
+constexpr size_t kStaticSmem = 8 * 1024;  // the kernel's static shared arrays, rounded up
+
+template <typename MaskT>
+size_t layout_bytes(int nmax, int S2, int umax, int keyn) {
+    return make_layout<MaskT>(nmax, S2, umax, keyn).total;
+}
+
+// Argument checks (the reference's, :984-1051), constants, group metadata on
+// the host and the shared-memory plan: which groups one block can hold.
+void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
+                  const int32_t* d_ny, const int32_t* d_nx, const void* d_pix, int32_t eltype, const void* d_iv,
+                  const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
+                  const double* d_f0, int64_t total_pixels, const cpb_group_result* out, const int64_t* h_off_opt,
+                  const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt, GroupSetup& su) {
     cudaStream_t st = ctx->stream;
     // argument checks in the reference's order (:984-997), shared by every group
     if (!(P->max_iter > 0)) throw ArgError{"max_iter must be positive"};
@@ -1186,7 +1208,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
     if (!out->y || !out->x || !out->flux || !out->y_err || !out->x_err || !out->flux_err || !out->converged ||
         !out->valid || !out->n_iter || !out->n_passes || !out->n_failed || !out->status)
         throw ArgError{"null output array"};
-    GroupConst C{};
+    GroupConst& C = su.C;
     C.p = 0;
     if (P->free_mask & CPB_FREE_Y) C.gc[C.p++] = 1;
     if (P->free_mask & CPB_FREE_X) C.gc[C.p++] = 2;
@@ -1229,16 +1251,26 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
     C.eltype = eltype;
     C.reweighted = (P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && d_iv == nullptr)) ? 1 : 0;
     C.fit_rad = P->fit_rad;
-    DevPsf dp = psf->dev;
-    dp.fwhm = P->fixed_fwhm;
+    su.dp = psf->dev;
+    su.dp.fwhm = P->fixed_fwhm;
 
-    out->n_kernel_groups = 0;
-    out->n_routed_groups = 0;
-    out->device_seconds = 0;
-    if (G == 0) return 0;
+    su.total_pixels = total_pixels;
+    su.eltype = eltype;
+    su.gin = GroupIn{d_off, d_ny, d_nx, d_pix, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0};
+    su.go = GroupOut{out->y, out->x, out->flux, out->y_err, out->x_err, out->flux_err, out->converged, out->valid,
+                     out->n_iter, out->chisq, out->qfit, out->qfit_expected, out->qfit_z, out->crowding,
+                     out->residual, out->n_passes, out->n_failed, out->status, out->error_kind, out->n_active,
+                     out->n_union, out->n_trials, out->n_lsqr_iters};
+    if (G == 0) return;
     // group sizes on the host (plan the shared-memory layout, route oversized groups)
-    std::vector<int64_t> h_off(G), h_soff(G + 1);
-    std::vector<int32_t> h_ny(G), h_nx(G);
+    std::vector<int64_t>& h_off = su.h_off;
+    std::vector<int64_t>& h_soff = su.h_soff;
+    std::vector<int32_t>& h_ny = su.h_ny;
+    std::vector<int32_t>& h_nx = su.h_nx;
+    h_off.resize(G);
+    h_soff.resize(G + 1);
+    h_ny.resize(G);
+    h_nx.resize(G);
     if (h_off_opt) {
         std::memcpy(h_off.data(), h_off_opt, sizeof(int64_t) * G);
         std::memcpy(h_soff.data(), h_soff_opt, sizeof(int64_t) * (G + 1));
@@ -1260,8 +1292,8 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
     }
     int smem_optin = 0;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
-    const size_t static_smem = 8 * 1024;  // the kernel's static shared arrays, rounded up
-    GroupPlan plan;
+    const size_t static_smem = kStaticSmem;
+    GroupPlan& plan = su.plan;
     // a group runs in the kernel when it has <= 64 stars and its own layout fits
     for (int64_t g = 0; g < G; ++g) {
         const int ng = (int)(h_soff[g + 1] - h_soff[g]);
@@ -1317,11 +1349,77 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
     C.umax = plan.umax;
     C.keyn = plan.keyn;
 
-    GroupIn gin{d_off, d_ny, d_nx, d_pix, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0};
-    GroupOut go{out->y, out->x, out->flux, out->y_err, out->x_err, out->flux_err, out->converged, out->valid,
-                out->n_iter, out->chisq, out->qfit, out->qfit_expected, out->qfit_z, out->crowding, out->residual,
-                out->n_passes, out->n_failed, out->status, out->error_kind, out->n_active, out->n_union,
-                out->n_trials, out->n_lsqr_iters};
+}
+
+template <int NT, typename MaskT>
+void* group_kernel() {
+    return (void*)k_groups<NT, MaskT>;
+}
+
+void* group_kernel_for(int threads, bool wide) {
+    if (threads == 128) return wide ? group_kernel<128, uint64_t>() : group_kernel<128, uint32_t>();
+    return wide ? group_kernel<256, uint64_t>() : group_kernel<256, uint32_t>();
+}
+
+// Resident blocks per SM of the group kernel at this plan and block size.
+int group_occupancy(const GroupSetup& su, int threads) {
+    void* kfn = group_kernel_for(threads, su.plan.wide_mask);
+    check(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su.plan.smem), "smem attr");
+    int per_sm = 0;
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, su.plan.smem), "occupancy");
+    return std::max(per_sm, 1);
+}
+
+// One launch of the group kernel over the planned groups: resets the work
+// queue and starts min(groups, SMs x blocks_per_sm) persistent blocks.
+// threads: 128 or 256; blocks_per_sm <= 0 means the occupancy limit.
+void launch_groups(cpb_ctx* ctx, cudaStream_t st, const GroupSetup& su, const int32_t* d_list, int* d_queue,
+                   int threads, int blocks_per_sm) {
+    const int64_t nk = (int64_t)su.plan.kernel_groups.size();
+    if (nk <= 0) return;
+    threads = threads == 128 ? 128 : 256;
+    const int occ = group_occupancy(su, threads);
+    const int per_sm = blocks_per_sm <= 0 ? occ : std::min(blocks_per_sm, occ);
+    const int64_t grid = std::min<int64_t>(nk, (int64_t)ctx->n_sm * per_sm);
+    check(cudaMemsetAsync(d_queue, 0, sizeof(int), st), "memset");
+    KernelScope ks_(ctx, "k_groups",
+                    (double)su.total_pixels * (su.eltype == CPB_F64 ? 8 : 4) * (su.gin.iv ? 2 : 1));
+    const bool wide = su.plan.wide_mask;
+    const size_t smem = su.plan.smem;
+    if (threads == 128) {
+        if (wide)
+            k_groups<128, uint64_t><<<(unsigned)grid, 128, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
+        else
+            k_groups<128, uint32_t><<<(unsigned)grid, 128, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
+    } else {
+        if (wide)
+            k_groups<256, uint64_t><<<(unsigned)grid, 256, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
+        else
+            k_groups<256, uint32_t><<<(unsigned)grid, 256, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
+    }
+    check(cudaGetLastError(), "k_groups");
+}
+
+}  // namespace
+
+int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
+                   const int32_t* d_ny, const int32_t* d_nx, const void* d_pix, int32_t eltype, const void* d_iv,
+                   const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
+                   const double* d_f0, int64_t total_pixels, cpb_group_result* out, const int64_t* h_off_opt,
+                   const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt) {
+    cudaStream_t st = ctx->stream;
+    GroupSetup su;
+    setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,
+                 total_pixels, out, h_off_opt, h_ny_opt, h_nx_opt, h_soff_opt, su);
+    out->n_kernel_groups = 0;
+    out->n_routed_groups = 0;
+    out->device_seconds = 0;
+    if (G == 0) return 0;
+    const GroupPlan& plan = su.plan;
+    const std::vector<int64_t>& h_off = su.h_off;
+    const std::vector<int64_t>& h_soff = su.h_soff;
+    const std::vector<int32_t>& h_ny = su.h_ny;
+    const std::vector<int32_t>& h_nx = su.h_nx;
     check(cudaEventRecord(ctx->ev0, st), "event");
     const int64_t nk = (int64_t)plan.kernel_groups.size();
     if (nk > 0) {
@@ -1329,20 +1427,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         int* d_queue = (int*)scratch(ctx, "grp_queue", sizeof(int));
         check(cudaMemcpyAsync(d_list, plan.kernel_groups.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st),
               "h2d");
-        check(cudaMemsetAsync(d_queue, 0, sizeof(int), st), "memset");
-        constexpr int NT = 256;
-        auto kfn = plan.wide_mask ? (void*)k_groups<NT, uint64_t> : (void*)k_groups<NT, uint32_t>;
-        check(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem), "smem attr");
-        int per_sm = 0;
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, NT, plan.smem), "occupancy");
-        per_sm = std::max(per_sm, 1);
-        const int64_t grid = std::min<int64_t>(nk, (int64_t)ctx->n_sm * per_sm);
-        KernelScope ks_(ctx, "k_groups", (double)total_pixels * (eltype == CPB_F64 ? 8 : 4) * (d_iv ? 2 : 1));
-        if (plan.wide_mask)
-            k_groups<NT, uint64_t><<<(unsigned)grid, NT, plan.smem, st>>>(C, dp, gin, go, d_list, (int)nk, d_queue);
-        else
-            k_groups<NT, uint32_t><<<(unsigned)grid, NT, plan.smem, st>>>(C, dp, gin, go, d_list, (int)nk, d_queue);
-        check(cudaGetLastError(), "k_groups");
+        launch_groups(ctx, st, su, d_list, d_queue, 256, 0);
     }
     check(cudaEventRecord(ctx->ev1, st), "event");
     check(cudaStreamSynchronize(st), "sync");
@@ -1448,6 +1533,78 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         out->device_seconds += r.device_seconds;
     }
     return 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// A bound batch over fixed device buffers (CUDA-graph capture and tuning)
+// ---------------------------------------------------------------------------
+struct GroupBatch {
+    GroupSetup su;
+    int32_t* d_list = nullptr;  // owned
+    int* d_queue = nullptr;     // owned
+};
+
+GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G,
+                               const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const void* d_pix,
+                               int32_t eltype, const void* d_iv, const void* d_bkg, const int64_t* d_soff,
+                               const double* d_y0, const double* d_x0, const double* d_f0, int64_t total_pixels,
+                               const cpb_group_result* out) {
+    if (G > 0 && (!d_off || !d_ny || !d_nx || !d_pix || !d_soff || !d_y0 || !d_x0 || !d_f0 || !out))
+        throw ArgError{"null argument"};
+    auto* b = new GroupBatch();
+    try {
+        if (G > 0)
+            setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,
+                         total_pixels, out, nullptr, nullptr, nullptr, nullptr, b->su);
+        if (!b->su.plan.routed_groups.empty())
+            throw ArgError{"group " + std::to_string(b->su.plan.routed_groups[0]) +
+                           " is too large for one thread block (more than 64 stars, or a working set beyond shared "
+                           "memory); fit it with cpb_fit_simultaneous_batch instead of a captured batch"};
+        const int64_t nk = (int64_t)b->su.plan.kernel_groups.size();
+        if (cudaMalloc(&b->d_list, sizeof(int32_t) * std::max<int64_t>(nk, 1)) != cudaSuccess ||
+            cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            throw OomError{"device memory exhausted allocating the group work queue"};
+        }
+        if (nk > 0)
+            check(cudaMemcpy(b->d_list, b->su.plan.kernel_groups.data(), sizeof(int32_t) * nk,
+                             cudaMemcpyHostToDevice), "h2d");
+    } catch (...) {
+        cudaFree(b->d_list);
+        cudaFree(b->d_queue);
+        delete b;
+        throw;
+    }
+    return b;
+}
+
+void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int threads, int blocks_per_sm) {
+    launch_groups(ctx, st, b->su, b->d_list, b->d_queue, threads, blocks_per_sm);
+}
+
+int group_batch_occupancy(GroupBatch* b, int threads) {
+    if (b->su.plan.kernel_groups.empty()) return 1;
+    return group_occupancy(b->su, threads);
+}
+
+int64_t group_batch_size(const GroupBatch* b) { return (int64_t)b->su.plan.kernel_groups.size(); }
+
+// Tuning signature: what the best launch shape depends on.
+std::string group_batch_signature(const GroupBatch* b) {
+    const GroupSetup& su = b->su;
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "groups psf%d nodes%d el%d p%d S2_%d mR%d nmax%d umax%d wide%d G2^%d",
+                  su.dp.kind, su.dp.n_nodes, su.eltype, su.C.p, su.C.S2, su.C.mR, su.plan.nmax, su.plan.umax,
+                  su.plan.wide_mask ? 1 : 0, (int)std::log2((double)std::max<size_t>(su.plan.kernel_groups.size(), 1)));
+    return buf;
+}
+
+void group_batch_destroy(GroupBatch* b) {
+    if (!b) return;
+    cudaFree(b->d_list);
+    cudaFree(b->d_queue);
+    delete b;
 }
 
 }  // namespace cpb

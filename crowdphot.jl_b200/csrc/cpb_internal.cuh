@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <exception>
 #include <map>
 #include <mutex>
 #include <string>
@@ -368,6 +369,32 @@ struct OomError {
     std::string msg;
 };
 
+// Runs one C-ABI entry point's body under the context's lock, translating
+// exceptions into CPB_* status codes and cpb_last_error() text.
+template <typename F>
+int guarded(cpb_ctx* ctx, F&& f) {
+    if (!ctx) return CPB_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->err.clear();
+    try {
+        check(cudaSetDevice(ctx->device), "cudaSetDevice");
+        return f();
+    } catch (const ArgError& e) {
+        ctx->err = e.msg;
+        return CPB_ERR_ARGUMENT;
+    } catch (const OomError& e) {
+        ctx->err = e.msg;
+        return CPB_ERR_OOM;
+    } catch (const CudaError& e) {
+        ctx->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);
+        return CPB_ERR_CUDA;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return CPB_ERR_INTERNAL;
+    }
+}
+
+
 // Simultaneous fit driver (cpb_sim.cu).  Inputs are device pointers.
 int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
                          int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var, const void* d_background,
@@ -381,6 +408,32 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
                    const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
                    const double* d_f0, int64_t total_pixels, cpb_group_result* out, const int64_t* h_off_opt,
                    const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt);
+
+// Bound batches over fixed device buffers (cpb_lm.cu, cpb_groups.cu): one
+// launch each, no host synchronisation and no allocation, so that a CUDA graph
+// can capture them; the *_signature strings key the launch-shape tuner.
+struct LMBatch;
+LMBatch* lm_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,
+                         const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1,
+                         const int32_t* d_x1, const void* d_pix, int32_t eltype, const void* d_iv,
+                         const double* d_init, int64_t total_pixels, const cpb_lm_result* out);
+void lm_batch_enqueue(cpb_ctx* ctx, LMBatch* b, cudaStream_t st, int blocks_per_sm, int smem_node);
+bool lm_batch_smem_possible(const LMBatch* b);
+int64_t lm_batch_size(const LMBatch* b);
+std::string lm_batch_signature(const LMBatch* b);
+void lm_batch_destroy(LMBatch* b);
+
+struct GroupBatch;
+GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G,
+                               const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const void* d_pix,
+                               int32_t eltype, const void* d_iv, const void* d_bkg, const int64_t* d_soff,
+                               const double* d_y0, const double* d_x0, const double* d_f0, int64_t total_pixels,
+                               const cpb_group_result* out);
+void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int threads, int blocks_per_sm);
+int group_batch_occupancy(GroupBatch* b, int threads);
+int64_t group_batch_size(const GroupBatch* b);
+std::string group_batch_signature(const GroupBatch* b);
+void group_batch_destroy(GroupBatch* b);
 
 // Batched LM driver (cpb_lm.cu).  Host inputs.
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cutouts,

@@ -12,6 +12,8 @@
 // Cholesky / accept-reject logic, so there is no divergence and no shared
 // state between cutouts.  Warps are persistent over a cutout queue.
 #include <algorithm>
+#include <cstdio>
+#include <string>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -992,13 +994,25 @@ LMConst lm_const(const cpb_psf* psf, const cpb_lm_params* P, bool have_iv) {
 
 // One launch of k_lm over device-resident cutouts; `pix_elems` (the cutout
 // pixels in total, for the instrumentation's byte count) may be 0.
+// Launch configuration: persistent blocks per SM (1 or 2; 0 = 2) and whether the
+// node's samples may be staged in shared memory (-1 = when they fit).  `queue`
+// (nullable) is the work-queue counter to use instead of the context's scratch
+// one; `st` (nullable) the stream instead of the context's.
+struct LMConfig {
+    int blocks_per_sm = 0;
+    int smem_node = -1;
+    unsigned long long* queue = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
 void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut, const int64_t* d_off,
                const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1, const int32_t* d_x1, const void* d_pix,
-               int32_t eltype, const void* d_iv, const double* d_init, const LMOut& o, int64_t pix_elems) {
+               int32_t eltype, const void* d_iv, const double* d_init, const LMOut& o, int64_t pix_elems,
+               const LMConfig& cfg = LMConfig()) {
     const size_t esz = eltype == CPB_F64 ? 8 : 4;
     const double bytes = (double)pix_elems * esz * (d_iv ? 2 : 1) + (double)n_cut * (8 + 16 + 8 * L.np) +
                          (double)n_cut * (8 * L.np + (o.cov ? 8 * L.nf * L.nf : 0) + 4 * 8 + 4 + 4 + 4);
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = cfg.stream ? cfg.stream : ctx->stream;
     const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     if (gauss || psf->dev.n_nodes == 1) {
         // fast form: compile-time parameter counts, polyphase taps, work queue
@@ -1010,14 +1024,16 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
             N.inv_isy = 1.0f / (float)N.nd.isy;
             N.inv_isx = 1.0f / (float)N.nd.isx;
         }
-        auto* queue = (unsigned long long*)scratch(ctx, "lm_queue", sizeof(unsigned long long));
+        auto* queue = cfg.queue ? cfg.queue
+                                : (unsigned long long*)scratch(ctx, "lm_queue", sizeof(unsigned long long));
         check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st), "memset");
         // two persistent 256-thread blocks an SM (128 registers a thread); the
         // node's samples go to shared memory when two copies fit an SM
         const size_t node_bytes = gauss ? 0 : sizeof(double) * (size_t)N.plane * N.nd.isy * N.nd.isx;
-        const bool smem = !gauss && node_bytes <= 100 * 1024;
+        const bool smem = !gauss && node_bytes <= 100 * 1024 && cfg.smem_node != 0;
+        const int per_sm = cfg.blocks_per_sm == 1 ? 1 : 2;
         const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + kLMThreads - 1) / kLMThreads,
-                                                            (int64_t)ctx->n_sm * 2);
+                                                            (int64_t)ctx->n_sm * per_sm);
         KernelScope ks_(ctx, "k_lm", bytes);
 #define CPB_LM_LAUNCH(TI, NP, NF)                                                                                  \
     do {                                                                                                          \
@@ -1070,6 +1086,92 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// A bound batch over fixed device buffers (CUDA-graph capture and tuning)
+// ---------------------------------------------------------------------------
+struct LMBatch {
+    const cpb_psf* psf;
+    LMConst L;
+    int64_t n_cut;
+    const int64_t* off;
+    const int32_t *ny, *nx, *y1, *x1;
+    const void* pix;
+    int32_t eltype;
+    const void* iv;
+    const double* init;
+    LMOut o;
+    int64_t pix_elems;
+    unsigned long long* queue = nullptr;  // owned
+};
+
+LMBatch* lm_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,
+                         const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1,
+                         const int32_t* d_x1, const void* d_pix, int32_t eltype, const void* d_iv,
+                         const double* d_init, int64_t total_pixels, const cpb_lm_result* out) {
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
+    if (n_cut > 0 && (!d_off || !d_ny || !d_nx || !d_y1 || !d_x1 || !d_pix || !d_init || !out || !out->status))
+        throw ArgError{"null argument"};
+    auto* b = new LMBatch();
+    b->psf = psf;
+    b->L = lm_const(psf, P, d_iv != nullptr);
+    b->n_cut = n_cut;
+    b->off = d_off;
+    b->ny = d_ny;
+    b->nx = d_nx;
+    b->y1 = d_y1;
+    b->x1 = d_x1;
+    b->pix = d_pix;
+    b->eltype = eltype;
+    b->iv = d_iv;
+    b->init = d_init;
+    if (out)
+        b->o = LMOut{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
+                     out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+    b->pix_elems = total_pixels;
+    if (cudaMalloc(&b->queue, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        delete b;
+        throw OomError{"device memory exhausted allocating the fit_star work queue"};
+    }
+    return b;
+}
+
+void lm_batch_enqueue(cpb_ctx* ctx, LMBatch* b, cudaStream_t st, int blocks_per_sm, int smem_node) {
+    if (b->n_cut <= 0) return;
+    LMConfig cfg;
+    cfg.blocks_per_sm = blocks_per_sm;
+    cfg.smem_node = smem_node;
+    cfg.queue = b->queue;
+    cfg.stream = st;
+    launch_lm(ctx, b->psf, b->L, b->n_cut, b->off, b->ny, b->nx, b->y1, b->x1, b->pix, b->eltype, b->iv, b->init,
+              b->o, b->pix_elems, cfg);
+}
+
+bool lm_batch_smem_possible(const LMBatch* b) {
+    const cpb_psf* psf = b->psf;
+    if (psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN || psf->dev.n_nodes != 1) return false;
+    const DevNode& nd = psf->h_nodes[0];
+    return sizeof(double) * (size_t)nd.LPY * nd.LPX * nd.isy * nd.isx <= 100 * 1024;
+}
+
+int64_t lm_batch_size(const LMBatch* b) { return b->n_cut; }
+
+// Tuning signature: what the best launch shape depends on.
+std::string lm_batch_signature(const LMBatch* b) {
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "fit_star psf%d nodes%d el%d np%d nf%d iv%d n2^%d px/cut%lld", b->psf->dev.kind,
+                  b->psf->dev.n_nodes, b->eltype, b->L.np, b->L.nf, b->iv ? 1 : 0,
+                  (int)std::log2((double)std::max<int64_t>(b->n_cut, 1)),
+                  (long long)(b->pix_elems / std::max<int64_t>(b->n_cut, 1) / 64 * 64));
+    return buf;
+}
+
+void lm_batch_destroy(LMBatch* b) {
+    if (!b) return;
+    cudaFree(b->queue);
+    delete b;
+}
 
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
                  const int32_t* ny, const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,

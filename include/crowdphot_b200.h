@@ -384,6 +384,63 @@ CPB_API int cpb_fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_
                                     const void* d_pixels, int32_t eltype, const void* d_inv_var,
                                     const double* d_init, int64_t total_pixels, cpb_lm_result* out);
 
+/* ---- one captured launch for a mixed batch (fit_star cutouts + groups) -- */
+/*
+ * No counterpart in the reference (whose fits run one call at a time on the
+ * CPU).  A batch graph binds a batch of fit_star cutouts
+ * (cpb_fit_lm_batch_device's arguments) and a batch of star groups
+ * (cpb_fit_simultaneous_batch_device's arguments) to fixed device buffers and
+ * captures both persistent kernels, each with its work-queue reset, in one
+ * CUDA graph whose two branches run concurrently.  Every replay fits the
+ * current contents of the bound input buffers into the bound output buffers:
+ * refill the inputs in place (same sizes) and launch again.  Either half may
+ * be empty (n_cutouts = 0 or n_groups = 0, other arguments of that half then
+ * ignored).  Groups too large for one thread block are refused
+ * (CPB_ERR_ARGUMENT): fit them with cpb_fit_simultaneous_batch.
+ *
+ * Launch shapes.  autotune = 0 uses the default shapes; 1 looks the batch's
+ * signature up in the tuning cache at cache_path (NULL: the file named by the
+ * CPB_TUNE_CACHE environment variable, else no file) and, when absent, times
+ * every candidate shape on the bound batch itself (each candidate runs the
+ * real fits once; outputs are overwritten), keeps the fastest and records it;
+ * 2 re-tunes even when cached.  The shapes are: persistent blocks per SM (1
+ * or 2) and whether the ePSF node is staged in shared memory for the fit_star
+ * kernel; threads per block (128 or 256) and resident blocks per SM for the
+ * group kernel.  `info` (nullable) reports the choice.
+ */
+typedef struct cpb_tune_info {
+    int32_t lm_blocks_per_sm;
+    int32_t lm_node_in_smem;
+    int32_t grp_threads;
+    int32_t grp_blocks_per_sm;
+    int32_t from_cache;   /* 1 when both choices came from the cache */
+    int32_t n_timed;      /* candidate launches timed by this call */
+    double lm_ms, grp_ms; /* device time of the chosen shapes (0 when not timed) */
+} cpb_tune_info;
+
+typedef struct cpb_batch_graph cpb_batch_graph;
+
+CPB_API int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf,
+                                   /* fit_star half */
+                                   const cpb_lm_params* lm_params, int64_t n_cutouts, const int64_t* d_offsets,
+                                   const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y_origin,
+                                   const int32_t* d_x_origin, const void* d_pixels, int32_t lm_eltype,
+                                   const void* d_inv_var, const double* d_init, int64_t lm_total_pixels,
+                                   const cpb_lm_result* d_lm_out,
+                                   /* group half */
+                                   const cpb_sim_params* sim_params, int64_t n_groups, const int64_t* d_pix_offsets,
+                                   const int32_t* d_gny, const int32_t* d_gnx, const void* d_gpixels,
+                                   int32_t g_eltype, const void* d_ginv_var, const void* d_gbackground,
+                                   const int64_t* d_star_offsets, const double* d_y0, const double* d_x0,
+                                   const double* d_flux0, int64_t g_total_pixels, const cpb_group_result* d_g_out,
+                                   /* launch shapes */
+                                   int32_t autotune, const char* cache_path, cpb_batch_graph** out,
+                                   cpb_tune_info* info);
+/* Replays the graph on the context's stream and waits for it; *device_seconds
+ * (nullable) receives its GPU time. */
+CPB_API int cpb_batch_graph_launch(cpb_ctx* ctx, cpb_batch_graph* graph, double* device_seconds);
+CPB_API int cpb_batch_graph_destroy(cpb_ctx* ctx, cpb_batch_graph* graph);
+
 #ifdef __cplusplus
 }
 #endif
