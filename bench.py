@@ -785,6 +785,119 @@ def run_gpu_c4(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# Served request stream (--workload serve): Poisson arrivals of fields of
+# mixed sizes into the continuous-batching server
+# ---------------------------------------------------------------------------
+SERVE_SIDES = (256, 512, 1024, 2048, 4096)
+SERVE_RATE = 200.0
+SERVE_METRIC = "fitted stars/s on 1 B200, served request stream (continuous batching, mixed precision); p50/p99 ms"
+
+
+def serve_requests(n, seed=5000):
+    """Arrival times (Poisson, mean SERVE_RATE / s) and per-request (side, density, seed)."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / SERVE_RATE, n))
+    out = []
+    for i in range(n):
+        r = np.random.default_rng(seed + i)
+        out.append((int(r.choice(SERVE_SIDES)), float(r.uniform(0.002, 0.02)), seed + i))
+    return arrivals - arrivals[0], out
+
+
+def serve_config(n, specs):
+    stars = sum(int(round(d * s * s)) for s, d, _ in specs)
+    return {"workload": f"{n} requests, Poisson arrivals at {SERVE_RATE:.0f}/s, sides uniform in {list(SERVE_SIDES)}, "
+                        f"density U[0.002, 0.02] px^-2 ({stars} stars in all), crowded-field PSF / noise model, "
+                        "fit_rad = model_rad = 12",
+            "n_requests": n, "seeds": "5000 + i", "sides": [s for s, _, _ in specs], "n_stars_total": stars,
+            "l2": "fields up to 4096^2 (stamp arrays up to 4 GB) exceed L2; requests run back to back"}
+
+
+def _run_stream(sv, psf, reqs, arrivals, precision):
+    """Submits the requests at their arrival times; returns (results, infos, makespan)."""
+    handles = []
+    t0 = time.perf_counter()
+    for (img, bkg, iv, init), at in zip(reqs, arrivals):
+        dt = t0 + at - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        handles.append(sv.submit(img, psf, init, FIT_RAD, inv_var=iv, background=bkg, precision=precision,
+                                 **fit_kwargs()))
+    results = [h.result(timeout=3600) for h in handles]
+    infos = [h.poll() for h in handles]
+    makespan = time.perf_counter() - t0
+    return results, infos, makespan
+
+
+def run_gpu_serve(args):
+    import torch
+
+    import crowdphot_b200 as cpb
+    from crowdphot_b200.simulate import moffat_epsf, served_field
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    psf = moffat_epsf()
+    arrivals, specs = serve_requests(args.n_requests, 5000 + 1000 * rank)
+    reqs = []
+    for side, dens, sd in specs:
+        img, bkg, iv, truth, init = served_field(side, dens, seed=sd, psf=psf)
+        reqs.append((img, bkg, iv, init))
+    # warm-up: one small request per form (contexts, PSF upload, kernels loaded)
+    warm = reqs[int(np.argmin([s for s, _, _ in specs]))]
+    clocks, clk = None, None
+    out = {}
+    for form, slots, prec in (("plain", 1, "fp64"), ("served_mixed", args.max_inflight, "mixed")):
+        with cpb.Server(device=local, max_inflight=slots) as sv:
+            for _ in range(max(args.warmup, 1)):
+                sv.submit(warm[0], psf, warm[3], FIT_RAD, inv_var=warm[2], background=warm[1], precision=prec,
+                          **fit_kwargs()).result(timeout=600)
+            if form == "served_mixed" and rank == 0:
+                clocks = ClockSampler(torch.cuda.current_device())
+            res, infos, makespan = _run_stream(sv, psf, reqs, arrivals, prec)
+            if form == "served_mixed" and clocks is not None:
+                clk = clocks.stop()
+        fitted = sum(int((r.valid & r.converged).sum()) for r in res)
+        lat = np.array([i["latency_seconds"] for i in infos]) * 1e3
+        out[form] = dict(results=res, value=fitted / makespan, fitted=fitted, makespan_s=makespan,
+                         p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                         device_seconds=float(sum(i["device_seconds"] for i in infos)),
+                         slots_used=len({i["slot"] for i in infos}))
+    # accuracy of the served mixed form against the plain FP64 form, per output
+    dfl, dpos = [], []
+    for a, b in zip(out["served_mixed"]["results"], out["plain"]["results"]):
+        ok = a.valid & a.converged & b.valid & b.converged & (a.n_iter == b.n_iter)
+        dfl.append(np.abs(a.flux[ok] / b.flux[ok] - 1))
+        dpos.append(np.maximum(np.abs(a.y[ok] - b.y[ok]), np.abs(a.x[ok] - b.x[ok])))
+    dfl, dpos = np.concatenate(dfl), np.concatenate(dpos)
+    acc = {"compared_stars": int(dfl.size),
+           "flux_rel_dev_vs_fp64": {"median": float(np.median(dfl)), "p99": float(np.percentile(dfl, 99)),
+                                    "frac_within_1e-5": float(np.mean(dfl <= 1e-5))},
+           "pos_dev_px_vs_fp64": {"median": float(np.median(dpos)), "p99": float(np.percentile(dpos, 99)),
+                                  "frac_within_1e-4": float(np.mean(dpos <= 1e-4))}}
+    sm, pl = out["served_mixed"], out["plain"]
+    h2d = sum(r[0].nbytes * 3 + 24 * r[3]["y"].size for r in reqs)
+    d2h = sum(r[3]["y"].size * (12 * 8 + 2 + 4) for r in reqs)
+    if rank == 0:
+        line = {"metric": SERVE_METRIC, "value": sm["value"], "unit": "stars/s", "n_gpus": 1,
+                "steps": args.n_requests, "warmup": max(args.warmup, 1),
+                "ms_per_step": 1e3 * sm["makespan_s"] / args.n_requests, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
+                "config": dict(serve_config(args.n_requests, specs), max_inflight=args.max_inflight),
+                "p50_ms": sm["p50_ms"], "p99_ms": sm["p99_ms"],
+                "forms": {k: {kk: vv for kk, vv in v.items() if kk != "results"} for k, v in out.items()},
+                "speedup_vs_plain": sm["value"] / pl["value"], "accuracy": acc, "clocks": clk,
+                "gpu_launches": None,
+                "e2e": {"value": sm["value"], "unit": "stars/s", "h2d_bytes_per_step": h2d // args.n_requests,
+                        "d2h_bytes_per_step": d2h // args.n_requests,
+                        "timer": "host wall clock from the first arrival to the last result: every request is "
+                                 "submitted with host buffers and its results read back"},
+                "note": "a step is one request; value is the served stream's fitted stars over its makespan"}
+        print(json.dumps(line))
+
+
 def C_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -799,17 +912,21 @@ def main():
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--n-stars", type=int, default=N_STARS)
-    ap.add_argument("--workload", choices=["crowded-field", "lm-cutouts", "c4"], default="crowded-field",
+    ap.add_argument("--workload", choices=["crowded-field", "lm-cutouts", "c4", "serve"], default="crowded-field",
                     help="crowded-field: the simultaneous fit (headline); lm-cutouts: batched fit_star; "
-                         "c4: fit_star cutouts + blended groups in one CUDA-graph launch")
+                         "c4: fit_star cutouts + blended groups in one CUDA-graph launch; "
+                         "serve: a Poisson request stream through the continuous-batching server")
     ap.add_argument("--n-groups", type=int, default=C4_GROUPS)
+    ap.add_argument("--n-requests", type=int, default=24)
+    ap.add_argument("--max-inflight", type=int, default=4)
     ap.add_argument("--n-cutouts", type=int, default=LM_CUTOUTS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the warm-up and timed resident steps (for profiler captures); prints a short line")
     args = ap.parse_args()
-    ref = {"crowded-field": run_reference, "lm-cutouts": run_reference_lm, "c4": run_reference_c4}
-    gpu = {"crowded-field": run_gpu, "lm-cutouts": run_gpu_lm, "c4": run_gpu_c4}
+    ref = {"crowded-field": run_reference, "lm-cutouts": run_reference_lm, "c4": run_reference_c4,
+           "serve": run_reference}
+    gpu = {"crowded-field": run_gpu, "lm-cutouts": run_gpu_lm, "c4": run_gpu_c4, "serve": run_gpu_serve}
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return

@@ -11,14 +11,14 @@ CircularMoffatPSF (evaluation only, to tabulate empirical PSFs).
 """
 from .psf import (AbstractPSFModel, ArgumentError, CircularGaussianPSF, CircularMoffatPSF, GriddedPSFModel,
                   ImagePSF, replace_params)
-from .photometry import (BatchGraph, Context, CudaError, LMResult, MultiPassPhotResult, fit_all_stars_simultaneous,
+from .photometry import (BatchGraph, Context, CudaError, Request, Server, LMResult, MultiPassPhotResult, fit_all_stars_simultaneous,
                          fit_all_stars_simultaneous_batch, fit_groups_packed, fit_star, fit_star_batch,
                          fit_star_packed, get_context, lm_params, psf_descriptor, sim_params)
 from ._abi import LIB_PATH, load_library
 
 __all__ = [
     "AbstractPSFModel", "ArgumentError", "CircularGaussianPSF", "CircularMoffatPSF", "GriddedPSFModel", "ImagePSF",
-    "replace_params", "BatchGraph", "Context", "CudaError", "LMResult", "MultiPassPhotResult", "fit_all_stars_simultaneous",
+    "replace_params", "BatchGraph", "Context", "Request", "Server", "CudaError", "LMResult", "MultiPassPhotResult", "fit_all_stars_simultaneous",
     "fit_all_stars_simultaneous_batch", "fit_groups_packed",
     "fit_star", "fit_star_batch", "fit_star_packed", "get_context", "lm_params", "psf_descriptor", "sim_params", "LIB_PATH",
     "load_library",

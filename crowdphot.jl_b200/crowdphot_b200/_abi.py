@@ -153,6 +153,24 @@ class TuneInfo(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("max_inflight", C.c_int32), ("hbm_reserve_bytes", C.c_int64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [
+        ("state", C.c_int32), ("status", C.c_int32), ("slot", C.c_int32), ("reserved", C.c_int32),
+        ("est_bytes", C.c_int64),
+        ("queued_seconds", C.c_double), ("run_seconds", C.c_double), ("latency_seconds", C.c_double),
+        ("device_seconds", C.c_double),
+        ("start_time", C.c_double), ("end_time", C.c_double),
+        ("error", C.c_char * 256),
+    ]
+
+
+CPB_REQ_QUEUED, CPB_REQ_RUNNING, CPB_REQ_DONE, CPB_REQ_FAILED, CPB_REQ_CANCELLED = 0, 1, 2, 3, 4
+
+
 class LMParams(C.Structure):
     _fields_ = [
         ("free_mask", C.c_int32),
@@ -232,6 +250,16 @@ PROTOTYPES = {
                                          C.c_int32, C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(TuneInfo)]),
     "cpb_batch_graph_launch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
     "cpb_batch_graph_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "cpb_server_create": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]),
+    "cpb_server_add_psf": (C.c_int, [C.c_void_p, C.POINTER(PsfDesc), C.POINTER(C.c_int32)]),
+    "cpb_server_submit": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(SimParams), C.c_void_p, C.c_int32, C.c_int64,
+                                    C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, _dp, _dp, _dp,
+                                    C.POINTER(SimResult), C.POINTER(C.c_int64)]),
+    "cpb_server_poll": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(RequestInfo)]),
+    "cpb_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+    "cpb_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+    "cpb_server_destroy": (C.c_int, [C.c_void_p]),
+    "cpb_server_last_error": (C.c_char_p, [C.c_void_p]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
     "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,

@@ -612,6 +612,120 @@ class BatchGraph:
             pass
 
 
+class Request:
+    """A submitted fit (Server.submit): poll() / wait() / result() / cancel()."""
+
+    _STATES = {0: "queued", 1: "running", 2: "done", 3: "failed", 4: "cancelled"}
+
+    def __init__(self, server, rid, keep, outs, shape):
+        self.server, self.id, self._keep, self._outs, self._shape = server, rid, keep, outs, shape
+
+    def _info(self, info):
+        d = {k: getattr(info, k) for k, _ in _abi.RequestInfo._fields_ if k not in ("error", "reserved")}
+        d["state"] = self._STATES.get(info.state, str(info.state))
+        d["error"] = info.error.decode(errors="replace")
+        return d
+
+    def poll(self) -> dict:
+        info = _abi.RequestInfo()
+        self.server._check(self.server.lib.cpb_server_poll(self.server.handle, self.id, C.byref(info)), "poll")
+        return self._info(info)
+
+    def wait(self, timeout=None) -> dict:
+        info = _abi.RequestInfo()
+        rc = self.server.lib.cpb_server_wait(self.server.handle, self.id, -1.0 if timeout is None else float(timeout),
+                                             C.byref(info))
+        if rc == _abi.CPB_ERR_TIMEOUT:
+            raise TimeoutError(f"request {self.id} still {self._STATES.get(info.state)} after {timeout} s")
+        self.server._check(rc, "wait")
+        return self._info(info)
+
+    def result(self, timeout=None) -> MultiPassPhotResult:
+        info = self.wait(timeout)
+        if info["state"] == "cancelled":
+            raise RuntimeError(f"request {self.id} was cancelled")
+        if info["status"] != 0:
+            if info["status"] == _abi.CPB_ERR_ARGUMENT:
+                raise ArgumentError(info["error"])
+            raise CudaError(f"request {self.id} failed ({info['status']}): {info['error']}")
+        ny, nx, S2 = self._shape
+        res = self._outs.result(ny, nx, S2)
+        res.stats = dict(res.stats or {}, serving=info)
+        return res
+
+    def cancel(self) -> bool:
+        return self.server.lib.cpb_server_cancel(self.server.handle, self.id) == 0
+
+
+class Server:
+    """Continuous batching of fit_all_stars_simultaneous requests on one GPU
+    (cpb_server_*): up to `max_inflight` fits run at once on their own streams,
+    admitted as slots and device memory free up; PSFs stay resident."""
+
+    def __init__(self, device: int = 0, max_inflight: int = 4, hbm_reserve_bytes: int = -1):
+        self.lib = _abi.load_library()
+        cfg = _abi.ServerConfig(device, max_inflight, hbm_reserve_bytes)
+        self.handle = C.c_void_p()
+        rc = self.lib.cpb_server_create(C.byref(cfg), C.byref(self.handle))
+        if rc != 0:
+            raise CudaError(f"cpb_server_create failed ({rc})")
+        self._psfs = {}
+
+    def _check(self, rc, what):
+        if rc == 0:
+            return
+        msg = (self.lib.cpb_server_last_error(self.handle) or b"").decode()
+        if rc == _abi.CPB_ERR_ARGUMENT:
+            raise ArgumentError(msg or what)
+        raise CudaError(f"cpb_server_{what} failed ({rc}): {msg}")
+
+    def psf_id(self, psf) -> int:
+        key = id(psf)
+        if key not in self._psfs:
+            desc, keep = psf_descriptor(psf)
+            pid = C.c_int32()
+            self._check(self.lib.cpb_server_add_psf(self.handle, C.byref(desc), C.byref(pid)), "add_psf")
+            del keep
+            self._psfs[key] = (int(pid.value), psf)
+        return self._psfs[key][0]
+
+    def submit(self, image, psf, sources, fit_rad, *, fixed=None, inv_var=None, background=None, residual=False,
+               **kw) -> Request:
+        """Queues fit_all_stars_simultaneous(image, psf, sources, fit_rad; kw...) and returns at once."""
+        fixed = dict(fixed or {})
+        imgf, ivf, bkf, et = _image_arrays(image, inv_var, background)
+        y0, x0, f0 = _catalog(sources)
+        P = sim_params(psf, fit_rad, fixed, inv_var_given=ivf is not None, **kw)
+        ny, nx = imgf.shape
+        R = int(np.ceil(fit_rad)) if fit_rad > 0 else 0
+        S2 = (2 * R + 1) ** 2
+        outs = SimOutputs(y0.size, ny, nx, S2, residual=residual)
+        pid = self.psf_id(psf)
+        rid = C.c_int64()
+        vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        self._check(self.lib.cpb_server_submit(self.handle, pid, C.byref(P), vp(imgf), et, ny, nx, vp(ivf), vp(bkf),
+                                               y0.size, y0.ctypes.data_as(_abi._dp), x0.ctypes.data_as(_abi._dp),
+                                               f0.ctypes.data_as(_abi._dp), C.byref(outs.c), C.byref(rid)), "submit")
+        return Request(self, int(rid.value), (imgf, ivf, bkf, y0, x0, f0, P), outs, (ny, nx, S2))
+
+    def close(self):
+        if self.handle:
+            self.lib.cpb_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def lm_params(model, fixed, *, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
               lambda_max=1.0e12, damping="marquardt", max_iter=200, x_tol=1.0e-8, f_tol=1.0e-4, g_tol=1.0e-4,
               covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64"):

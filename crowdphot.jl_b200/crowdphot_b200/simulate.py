@@ -351,3 +351,38 @@ def lm_groups(n, *, seed, psf=None, kmin=2, kmax=12, snr=(5.0, 1000.0), bkg=100.
     init_f = flux * rng.uniform(init_flux[0], init_flux[1], ns)
     return dict(pix=pix, inv_var=iv, offsets=offsets, ny=side.astype(np.int32), nx=side.astype(np.int32),
                 star_offsets=star_off, y=init_y, x=init_x, flux=init_f, truth=np.stack([ys, xs, flux], 1))
+
+
+def served_field(side, density, *, seed, psf=None, flux=(1e1, 1e6), flux_power=1.5, read_noise=5.0, gain=1.0,
+                 bkg_lo=50.0, bkg_span=150.0, dtype=np.float32, init_sigma=0.3, init_flux=(0.9, 1.1), chunk=16384):
+    """One field of a served request stream: side x side pixels, density * side^2
+    stars placed uniformly, power-law fluxes, the crowded-field background and
+    noise model, rendered per star over a +-13 px box with the separable ePSF
+    stencil (single-node image PSFs).  Returns (image, background, inv_var, truth, init)."""
+    rng = np.random.default_rng(seed)
+    psf = psf if psf is not None else moffat_epsf()
+    node = psf.psfs[0] if isinstance(psf, GriddedPSFModel) else psf
+    n = int(round(density * side * side))
+    src = simulate_sources((side, side), n, rng=rng, flux=flux, flux_distribution="powerlaw", flux_power=flux_power)
+    ys, xs, fs = (np.asarray(src[k], np.float64) for k in ("y", "x", "flux"))
+    model = np.zeros(side * side, np.float64)
+    H = 13
+    box = 2 * H + 1
+    for c0 in range(0, n, chunk):
+        sl = slice(c0, min(c0 + chunk, n))
+        cy = np.round(ys[sl]).astype(np.int64)
+        cx = np.round(xs[sl]).astype(np.int64)
+        val = render_cutouts(node, ys[sl], xs[sl], fs[sl], cy - H, cx - H, box)
+        gy = (cy - H)[:, None, None] + np.arange(box)[None, :, None]
+        gx = (cx - H)[:, None, None] + np.arange(box)[None, None, :]
+        gy, gx = np.broadcast_arrays(gy, gx)
+        keep = (gy >= 1) & (gy <= side) & (gx >= 1) & (gx <= side)
+        np.add.at(model, ((gy - 1) * side + (gx - 1))[keep], val[keep])  # row-major (y, x)
+    model = model.reshape(side, side)
+    u = (np.arange(1, side + 1) - 1) / max(side - 1, 1)
+    bkg = bkg_lo + bkg_span * (0.6 * u[None, :] + 0.4 * (u ** 2)[:, None])
+    img = rng.poisson(np.maximum(bkg + model, 0) * gain) / gain + read_noise * rng.standard_normal(model.shape)
+    inv_var = 1.0 / (bkg + model + read_noise ** 2)
+    init = dict(y=ys + rng.normal(0, init_sigma, n), x=xs + rng.normal(0, init_sigma, n),
+                flux=fs * rng.uniform(init_flux[0], init_flux[1], n))
+    return img.astype(dtype), bkg.astype(dtype), inv_var.astype(dtype), src, init

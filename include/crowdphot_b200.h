@@ -441,6 +441,76 @@ CPB_API int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf,
 CPB_API int cpb_batch_graph_launch(cpb_ctx* ctx, cpb_batch_graph* graph, double* device_seconds);
 CPB_API int cpb_batch_graph_destroy(cpb_ctx* ctx, cpb_batch_graph* graph);
 
+/* ---- serving: continuous batching of fit requests ------------------------ */
+/*
+ * No counterpart in the reference.  A server keeps PSFs resident on one GPU
+ * and runs fit_all_stars_simultaneous requests (fields of any size) as they
+ * arrive: up to max_inflight requests run at once, each on its own stream with
+ * its own device working memory (kept between requests and reused), so their
+ * kernels overlap on the GPU.  A queued request is admitted as soon as a slot
+ * is free and its estimated device memory fits the budget (free device memory
+ * at creation minus hbm_reserve_bytes, less what running requests and idle
+ * slots hold; idle slots give their memory back when an admission needs it).
+ * Queued requests are admitted first-fit in arrival order, so a large request
+ * does not hold back smaller ones that fit.  A request whose estimate exceeds
+ * the whole budget fails with CPB_ERR_OOM.  Each result is the one
+ * cpb_fit_simultaneous gives for the same request alone (the fits are
+ * deterministic and requests share no state).
+ *
+ * The host buffers a request names (inputs and cpb_sim_result arrays) must
+ * stay valid and untouched until the request is done, failed or cancelled.
+ * Calls are thread-safe.
+ */
+typedef struct cpb_server cpb_server;
+
+typedef struct cpb_server_config {
+    int32_t device;
+    int32_t max_inflight;       /* concurrent requests; <= 0 means 4 */
+    int64_t hbm_reserve_bytes;  /* device memory admission leaves free; < 0 means 2 GiB */
+} cpb_server_config;
+
+#define CPB_REQ_QUEUED 0
+#define CPB_REQ_RUNNING 1
+#define CPB_REQ_DONE 2
+#define CPB_REQ_FAILED 3
+#define CPB_REQ_CANCELLED 4
+
+typedef struct cpb_request_info {
+    int32_t state;            /* CPB_REQ_* */
+    int32_t status;           /* the fit's return code once done / failed */
+    int32_t slot;             /* slot that ran it, -1 if none */
+    int32_t reserved;
+    int64_t est_bytes;        /* admission estimate of its device memory */
+    double queued_seconds;    /* submit -> start */
+    double run_seconds;       /* start -> done (host clock) */
+    double latency_seconds;   /* submit -> done */
+    double device_seconds;    /* the fit's device time */
+    double start_time;        /* start and end, seconds since the server was created */
+    double end_time;
+    char error[256];          /* cpb_last_error text when failed */
+} cpb_request_info;
+
+CPB_API int cpb_server_create(const cpb_server_config* config, cpb_server** out);
+/* Uploads a PSF once (as cpb_psf_upload); *psf_id names it in submits. */
+CPB_API int cpb_server_add_psf(cpb_server* server, const cpb_psf_desc* desc, int32_t* psf_id);
+/* Queues one fit_all_stars_simultaneous request (cpb_fit_simultaneous's
+ * arguments; host buffers).  Returns at once with *request_id. */
+CPB_API int cpb_server_submit(cpb_server* server, int32_t psf_id, const cpb_sim_params* params, const void* image,
+                              int32_t eltype, int64_t ny, int64_t nx, const void* inv_var, const void* background,
+                              int64_t n, const double* y0, const double* x0, const double* flux0,
+                              cpb_sim_result* out, int64_t* request_id);
+CPB_API int cpb_server_poll(cpb_server* server, int64_t request_id, cpb_request_info* info);
+/* Waits until the request is done, failed or cancelled, or timeout_seconds
+ * pass (< 0: no limit); returns CPB_ERR_TIMEOUT on timeout. */
+CPB_API int cpb_server_wait(cpb_server* server, int64_t request_id, double timeout_seconds, cpb_request_info* info);
+/* Cancels a queued request (a running one finishes); CPB_ERR_ARGUMENT if it
+ * is no longer queued. */
+CPB_API int cpb_server_cancel(cpb_server* server, int64_t request_id);
+/* Cancels queued requests, waits for running ones, frees everything. */
+CPB_API int cpb_server_destroy(cpb_server* server);
+/* Text of the server's last call error ("" if none). */
+CPB_API const char* cpb_server_last_error(const cpb_server* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,8 +41,9 @@ def test_struct_layouts_match_c():
 #include <stddef.h>
 #include "crowdphot_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(cpb_psf_desc), sizeof(cpb_sim_params), sizeof(cpb_sim_result),
-         sizeof(cpb_lm_params), sizeof(cpb_lm_result), sizeof(cpb_group_result));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cpb_psf_desc), sizeof(cpb_sim_params),
+         sizeof(cpb_sim_result), sizeof(cpb_lm_params), sizeof(cpb_lm_result), sizeof(cpb_group_result),
+         sizeof(cpb_tune_info), sizeof(cpb_server_config), sizeof(cpb_request_info));
   printf("%zu %zu %zu %zu %zu %zu\n", offsetof(cpb_sim_params, precision), offsetof(cpb_sim_result, n_passes),
          offsetof(cpb_sim_result, device_seconds), offsetof(cpb_lm_params, min_diagonal),
          offsetof(cpb_group_result, n_lsqr_iters), offsetof(cpb_group_result, device_seconds));
@@ -58,7 +59,8 @@ int main(void) {
     sizes = [int(v) for v in out[0].split()]
     offs = [int(v) for v in out[1].split()]
     assert sizes == [C.sizeof(_abi.PsfDesc), C.sizeof(_abi.SimParams), C.sizeof(_abi.SimResult),
-                     C.sizeof(_abi.LMParams), C.sizeof(_abi.LMResultC), C.sizeof(_abi.GroupResult)]
+                     C.sizeof(_abi.LMParams), C.sizeof(_abi.LMResultC), C.sizeof(_abi.GroupResult),
+                     C.sizeof(_abi.TuneInfo), C.sizeof(_abi.ServerConfig), C.sizeof(_abi.RequestInfo)]
     assert offs == [_abi.SimParams.precision.offset, _abi.SimResult.n_passes.offset,
                     _abi.SimResult.device_seconds.offset, _abi.LMParams.min_diagonal.offset,
                     _abi.GroupResult.n_lsqr_iters.offset, _abi.GroupResult.device_seconds.offset]
