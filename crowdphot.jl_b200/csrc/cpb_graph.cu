@@ -7,8 +7,9 @@
 // ends.  A replay is one cudaGraphLaunch; nothing is read back in between.
 //
 // Tuner: candidates are timed with CUDA events on the bound batch itself, one
-// kernel at a time, after one untimed run of the default shape; the fastest
-// shape per kernel is kept.  Choices are cached in a text file, one line per
+// launch at a time, after one untimed run of the default shape; the fastest
+// shape is kept -- for the fit_star kernel, blocks per SM and the node in
+// shared memory or not; for each bucket of similar-size groups, the block size.  Choices are cached in a text file, one line per
 // (device, kernel signature): "<device>|<signature>\t<a> <b> <ms>".
 #include <algorithm>
 #include <cmath>
@@ -122,8 +123,8 @@ int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params
             cpb_tune_info& ti = g->info;
             ti.lm_blocks_per_sm = 2;
             ti.lm_node_in_smem = g->lm && lm_batch_smem_possible(g->lm) ? 1 : 0;
-            ti.grp_threads = 256;
-            ti.grp_blocks_per_sm = g->grp ? group_batch_occupancy(g->grp, 256) : 0;
+            ti.grp_threads = 0;
+            ti.grp_blocks_per_sm = 0;
             ti.from_cache = 0;
             ti.n_timed = 0;
             if (autotune) {
@@ -167,38 +168,41 @@ int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params
                     }
                 }
                 if (g->grp) {
-                    ++halves;
-                    const std::string key = dev + "|" + group_batch_signature(g->grp);
-                    auto it = cache.find(key);
-                    int a = 0, b = 0;
-                    double ms = 0;
-                    if (it != cache.end() && std::sscanf(it->second.c_str(), "%d %d %lf", &a, &b, &ms) == 3 &&
-                        (a == 128 || a == 256) && b >= 1 && b <= group_batch_occupancy(g->grp, a)) {
-                        ti.grp_threads = a;
-                        ti.grp_blocks_per_sm = b;
-                        ti.grp_ms = ms;
-                        ++cached;
-                    } else {
-                        group_batch_enqueue(ctx, g->grp, ctx->stream, ti.grp_threads, ti.grp_blocks_per_sm);  // warm
+                    // one block size per bucket of similar group sizes
+                    const int nb = group_batch_buckets(g->grp);
+                    double total_ms = 0;
+                    for (int k = 0; k < nb; ++k) {
+                        ++halves;
+                        const std::string key = dev + "|" + group_batch_signature(g->grp, k);
+                        auto it = cache.find(key);
+                        int a = 0, b = 0;
+                        double ms = 0;
+                        if (it != cache.end() && std::sscanf(it->second.c_str(), "%d %d %lf", &a, &b, &ms) >= 2 &&
+                            (a == 64 || a == 128 || a == 256)) {
+                            group_batch_set_threads(g->grp, k, a);
+                            total_ms += ms;
+                            ++cached;
+                            continue;
+                        }
+                        group_batch_enqueue(ctx, g->grp, ctx->stream, k, 0);  // warm
                         double best = 1e300;
-                        for (int nt : {256, 128}) {
-                            const int occ = std::min(group_batch_occupancy(g->grp, nt), 4);
-                            for (int bps = occ; bps >= 1; --bps) {
-                                const double t =
-                                    time_ms(ctx, [&] { group_batch_enqueue(ctx, g->grp, ctx->stream, nt, bps); });
-                                ++ti.n_timed;
-                                if (t < best) {
-                                    best = t;
-                                    ti.grp_threads = nt;
-                                    ti.grp_blocks_per_sm = bps;
-                                }
+                        int best_nt = group_batch_threads(g->grp, k);
+                        for (int nt : {64, 128, 256}) {
+                            const double t = time_ms(ctx, [&] { group_batch_enqueue(ctx, g->grp, ctx->stream, k, nt); });
+                            ++ti.n_timed;
+                            if (t < best) {
+                                best = t;
+                                best_nt = nt;
                             }
                         }
-                        ti.grp_ms = best;
+                        group_batch_set_threads(g->grp, k, best_nt);
+                        total_ms += best;
                         char v[64];
-                        std::snprintf(v, sizeof(v), "%d %d %.4f", ti.grp_threads, ti.grp_blocks_per_sm, best);
+                        std::snprintf(v, sizeof(v), "%d %d %.4f", best_nt,
+                                      group_batch_occupancy(g->grp, k, best_nt), best);
                         write_cache(path, key, v);
                     }
+                    ti.grp_ms = total_ms;
                 }
                 ti.from_cache = (halves > 0 && cached == halves) ? 1 : 0;
                 ctx->profile = prof;
@@ -211,7 +215,14 @@ int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params
             check(cudaEventCreate(&g->t1), "event");
             // attribute calls happen here, outside the capture
             if (g->lm) lm_batch_enqueue(ctx, g->lm, ctx->stream, ti.lm_blocks_per_sm, ti.lm_node_in_smem);
-            if (g->grp) group_batch_enqueue(ctx, g->grp, ctx->stream, ti.grp_threads, ti.grp_blocks_per_sm);
+            if (g->grp) {
+                group_batch_enqueue(ctx, g->grp, ctx->stream, -1, 0);
+                const int nb = group_batch_buckets(g->grp);
+                if (nb > 0) {  // buckets are ordered by group size: report the largest groups' launch
+                    ti.grp_threads = group_batch_threads(g->grp, nb - 1);
+                    ti.grp_blocks_per_sm = group_batch_occupancy(g->grp, nb - 1, ti.grp_threads);
+                }
+            }
             check(cudaStreamSynchronize(ctx->stream), "sync");
             ctx->profile = false;
             const int64_t l0 = ctx->launches;
@@ -220,7 +231,7 @@ int cpb_batch_graph_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params
                 check(cudaEventRecord(g->fork, ctx->stream), "fork");
                 check(cudaStreamWaitEvent(g->side, g->fork, 0), "fork wait");
                 if (g->lm) lm_batch_enqueue(ctx, g->lm, ctx->stream, ti.lm_blocks_per_sm, ti.lm_node_in_smem);
-                if (g->grp) group_batch_enqueue(ctx, g->grp, g->side, ti.grp_threads, ti.grp_blocks_per_sm);
+                if (g->grp) group_batch_enqueue(ctx, g->grp, g->side, -1, 0);
                 check(cudaEventRecord(g->join, g->side), "join");
                 check(cudaStreamWaitEvent(ctx->stream, g->join, 0), "join wait");
             } catch (...) {

@@ -210,6 +210,13 @@ struct GView {
     }
 };
 
+__device__ __forceinline__ double psf_value(const DevPsf& P, const StarCoef& c, int gy, int gx) {
+    return model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
+}
+__device__ __forceinline__ void psf_grad(const DevPsf& P, const StarCoef& c, int gy, int gx, double* g) {
+    model_grad<double, double>(P, P.data64, c, (double)gy, (double)gx, g);
+}
+
 template <int NT, typename MaskT>
 struct GroupFit {
     const GroupConst& C;
@@ -244,9 +251,7 @@ struct GroupFit {
         }
         grid_corners_dw(P, c.y, c.x, c);
     }
-    __device__ double mval(const StarCoef& c, int gy, int gx) const {
-        return model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
-    }
+    __device__ double mval(const StarCoef& c, int gy, int gx) const { return psf_value(P, c, gy, gx); }
     __device__ void uxy(int u, int& gy, int& gx) const {
         const int q = ip(L.upix)[u];
         gy = q % G.ny + 1;
@@ -286,7 +291,7 @@ struct GroupFit {
                 if (u == kNoU) continue;
                 const int gy = ay + (m % S) - R, gx = ax + (m / S) - R;
                 double g[3];
-                model_grad<double, double>(P, P.data64, c, (double)gy, (double)gx, g);
+                psf_grad(P, c, gy, gx, g);
                 const double swv = sqrt(w[u]);
                 double r[3] = {0, 0, 0};
                 for (int k = 0; k < p; ++k) r[k] = swv * g[C.gc[k] - 1];
@@ -1146,11 +1151,28 @@ inline int next_pow2(int v) {
     return p;
 }
 
-struct GroupPlan {
-    std::vector<int32_t> kernel_groups, routed_groups;
-    int nmax = 0, umax = 0, keyn = 0;
-    bool wide_mask = false;
+// Groups are launched in buckets of star count, each launch with a
+// shared-memory layout sized for its largest group.  Measured on the B200 with
+// the blended-group workload (2-12 stars), one launch over all groups (20,000
+// groups: 56 ms) beats four launches by size class (65 ms): the class
+// launches run one after another and each fills the GPU less.  So groups up to
+// 32 stars share one bucket; larger ones (up to 64) get a second.
+constexpr int kBucketEdges[] = {32, 64};
+constexpr int kNumBuckets = sizeof(kBucketEdges) / sizeof(int);
+
+struct Bucket {
+    std::vector<int32_t> groups;
+    int nmax = 1, umax = 1, keyn = 2;
+    bool wide = false;
     size_t smem = 0;
+    GroupConst C{};
+    int threads = 256;  // default block size
+};
+
+struct GroupPlan {
+    std::vector<Bucket> buckets;  // non-empty buckets only
+    std::vector<int32_t> routed_groups;
+    int64_t n_kernel = 0;
 };
 
 // Everything a launch needs, derived once from the arguments.
@@ -1290,65 +1312,56 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
         if (out->residual && h_off[g] + (int64_t)h_ny[g] * h_nx[g] > total_pixels)
             throw ArgError{"total_pixels is smaller than the pixels the groups span"};
     }
-    int smem_optin = 0;
+    int smem_optin = 0, smem_sm = 0;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
-    const size_t static_smem = kStaticSmem;
+    check(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device), "attr");
+    const size_t cap = (size_t)smem_optin - kStaticSmem;
     GroupPlan& plan = su.plan;
+    auto need_of = [&](int ng, int um, int kn) {
+        return ng > 32 ? layout_bytes<uint64_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn)
+                       : layout_bytes<uint32_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn);
+    };
     // a group runs in the kernel when it has <= 64 stars and its own layout fits
+    std::vector<Bucket> bk(kNumBuckets);
     for (int64_t g = 0; g < G; ++g) {
         const int ng = (int)(h_soff[g + 1] - h_soff[g]);
         const int um = (int)std::min<int64_t>((int64_t)ng * C.S2, (int64_t)h_ny[g] * h_nx[g]);
         const int kn = next_pow2(std::max(ng * C.S2, 2));
-        const size_t need = make_layout<uint64_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn).total;
-        if (ng <= kMaxGroupStars && need + static_smem <= (size_t)smem_optin) {
-            plan.kernel_groups.push_back((int32_t)g);
-            plan.nmax = std::max(plan.nmax, ng);
-            plan.umax = std::max(plan.umax, um);
-            plan.keyn = std::max(plan.keyn, kn);
-        } else {
+        if (ng > kMaxGroupStars || need_of(ng, um, kn) > cap) {
             plan.routed_groups.push_back((int32_t)g);
+            continue;
         }
-    }
-    plan.nmax = std::max(plan.nmax, 1);
-    plan.umax = std::max(plan.umax, 1);
-    plan.keyn = std::max(plan.keyn, 2);
-    plan.wide_mask = plan.nmax > 32;
-    plan.smem = plan.wide_mask ? make_layout<uint64_t>(plan.nmax, C.S2, plan.umax, plan.keyn).total
-                               : make_layout<uint32_t>(plan.nmax, C.S2, plan.umax, plan.keyn).total;
-    if (plan.smem + static_smem > (size_t)smem_optin) {
-        // the batch-wide maximum does not fit: route the largest groups until it does
-        std::vector<int32_t> keep;
-        for (int32_t g : plan.kernel_groups) plan.routed_groups.push_back(g);
-        plan.kernel_groups.clear();
-        std::sort(plan.routed_groups.begin(), plan.routed_groups.end());
-        plan.nmax = plan.umax = 1;
-        plan.keyn = 2;
-        std::vector<int32_t> still;
-        for (int32_t g : plan.routed_groups) {
-            const int ng = (int)(h_soff[g + 1] - h_soff[g]);
-            const int um = (int)std::min<int64_t>((int64_t)ng * C.S2, (int64_t)h_ny[g] * h_nx[g]);
-            const int kn = next_pow2(std::max(ng * C.S2, 2));
-            const int nm2 = std::max(plan.nmax, ng), um2 = std::max(plan.umax, um), kn2 = std::max(plan.keyn, kn);
-            const size_t need = nm2 > 32 ? make_layout<uint64_t>(nm2, C.S2, um2, kn2).total
-                                         : make_layout<uint32_t>(nm2, C.S2, um2, kn2).total;
-            if (ng <= kMaxGroupStars && need + static_smem <= (size_t)smem_optin / 2) {
-                plan.kernel_groups.push_back(g);
-                plan.nmax = nm2;
-                plan.umax = um2;
-                plan.keyn = kn2;
-            } else {
-                still.push_back(g);
-            }
+        int b = 0;
+        while (kBucketEdges[b] < ng) ++b;
+        Bucket& B = bk[b];
+        // the bucket's layout must still fit with this group's sizes folded in
+        const int nm2 = std::max(B.nmax, ng), um2 = std::max(B.umax, um), kn2 = std::max(B.keyn, kn);
+        if (need_of(nm2, um2, kn2) > cap) {
+            plan.routed_groups.push_back((int32_t)g);
+            continue;
         }
-        plan.routed_groups = still;
-        plan.wide_mask = plan.nmax > 32;
-        plan.smem = plan.wide_mask ? make_layout<uint64_t>(plan.nmax, C.S2, plan.umax, plan.keyn).total
-                                   : make_layout<uint32_t>(plan.nmax, C.S2, plan.umax, plan.keyn).total;
+        B.groups.push_back((int32_t)g);
+        B.nmax = nm2;
+        B.umax = um2;
+        B.keyn = kn2;
     }
-    C.nmax = plan.nmax;
-    C.umax = plan.umax;
-    C.keyn = plan.keyn;
-
+    std::sort(plan.routed_groups.begin(), plan.routed_groups.end());
+    for (Bucket& B : bk) {
+        if (B.groups.empty()) continue;
+        B.wide = B.nmax > 32;
+        B.smem = need_of(B.nmax, B.umax, B.keyn);
+        B.C = C;
+        B.C.nmax = B.nmax;
+        B.C.umax = B.umax;
+        B.C.keyn = B.keyn;
+        // default block size: about 512 threads an SM (the kernel's register budget
+        // allows 512 threads of 128 registers), in as many blocks as shared memory holds
+        const int by_smem = std::max(1, (int)((size_t)smem_sm / (B.smem + kStaticSmem + 1024)));
+        const int blocks = std::min(by_smem, 8);
+        B.threads = blocks >= 8 ? 64 : (blocks >= 4 ? 128 : 256);
+        plan.n_kernel += (int64_t)B.groups.size();
+        plan.buckets.push_back(std::move(B));
+    }
 }
 
 template <int NT, typename MaskT>
@@ -1357,46 +1370,53 @@ void* group_kernel() {
 }
 
 void* group_kernel_for(int threads, bool wide) {
+    if (threads == 64) return wide ? group_kernel<64, uint64_t>() : group_kernel<64, uint32_t>();
     if (threads == 128) return wide ? group_kernel<128, uint64_t>() : group_kernel<128, uint32_t>();
     return wide ? group_kernel<256, uint64_t>() : group_kernel<256, uint32_t>();
 }
 
-// Resident blocks per SM of the group kernel at this plan and block size.
-int group_occupancy(const GroupSetup& su, int threads) {
-    void* kfn = group_kernel_for(threads, su.plan.wide_mask);
-    check(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su.plan.smem), "smem attr");
+inline int valid_threads(int t) { return t == 64 ? 64 : (t == 128 ? 128 : 256); }
+
+// Resident blocks per SM of the group kernel for this bucket and block size.
+int group_occupancy(const Bucket& B, int threads) {
+    threads = valid_threads(threads);
+    void* kfn = group_kernel_for(threads, B.wide);
+    check(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)B.smem), "smem attr");
     int per_sm = 0;
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, su.plan.smem), "occupancy");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, threads, B.smem), "occupancy");
     return std::max(per_sm, 1);
 }
 
-// One launch of the group kernel over the planned groups: resets the work
+// One launch of the group kernel over one bucket's groups: resets the work
 // queue and starts min(groups, SMs x blocks_per_sm) persistent blocks.
-// threads: 128 or 256; blocks_per_sm <= 0 means the occupancy limit.
-void launch_groups(cpb_ctx* ctx, cudaStream_t st, const GroupSetup& su, const int32_t* d_list, int* d_queue,
-                   int threads, int blocks_per_sm) {
-    const int64_t nk = (int64_t)su.plan.kernel_groups.size();
+// threads: 64, 128 or 256 (<= 0: the bucket's default); blocks_per_sm <= 0
+// means the occupancy limit.
+void launch_bucket(cpb_ctx* ctx, cudaStream_t st, const GroupSetup& su, const Bucket& B, const int32_t* d_list,
+                   int* d_queue, int threads, int blocks_per_sm) {
+    const int64_t nk = (int64_t)B.groups.size();
     if (nk <= 0) return;
-    threads = threads == 128 ? 128 : 256;
-    const int occ = group_occupancy(su, threads);
+    threads = valid_threads(threads <= 0 ? B.threads : threads);
+    const int occ = group_occupancy(B, threads);
     const int per_sm = blocks_per_sm <= 0 ? occ : std::min(blocks_per_sm, occ);
     const int64_t grid = std::min<int64_t>(nk, (int64_t)ctx->n_sm * per_sm);
     check(cudaMemsetAsync(d_queue, 0, sizeof(int), st), "memset");
     KernelScope ks_(ctx, "k_groups",
-                    (double)su.total_pixels * (su.eltype == CPB_F64 ? 8 : 4) * (su.gin.iv ? 2 : 1));
-    const bool wide = su.plan.wide_mask;
-    const size_t smem = su.plan.smem;
-    if (threads == 128) {
-        if (wide)
-            k_groups<128, uint64_t><<<(unsigned)grid, 128, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
-        else
-            k_groups<128, uint32_t><<<(unsigned)grid, 128, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
-    } else {
-        if (wide)
-            k_groups<256, uint64_t><<<(unsigned)grid, 256, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
-        else
-            k_groups<256, uint32_t><<<(unsigned)grid, 256, smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk, d_queue);
-    }
+                    (double)su.total_pixels * (su.eltype == CPB_F64 ? 8 : 4) * (su.gin.iv ? 2 : 1) * nk /
+                        std::max<int64_t>(su.plan.n_kernel, 1));
+    const size_t smem = B.smem;
+#define CPB_GROUPS_LAUNCH(NTV)                                                                                      \
+    do {                                                                                                            \
+        if (B.wide)                                                                                                 \
+            k_groups<NTV, uint64_t><<<(unsigned)grid, NTV, smem, st>>>(B.C, su.dp, su.gin, su.go, d_list, (int)nk, \
+                                                                       d_queue);                                   \
+        else                                                                                                        \
+            k_groups<NTV, uint32_t><<<(unsigned)grid, NTV, smem, st>>>(B.C, su.dp, su.gin, su.go, d_list, (int)nk, \
+                                                                       d_queue);                                   \
+    } while (0)
+    if (threads == 64) CPB_GROUPS_LAUNCH(64);
+    else if (threads == 128) CPB_GROUPS_LAUNCH(128);
+    else CPB_GROUPS_LAUNCH(256);
+#undef CPB_GROUPS_LAUNCH
     check(cudaGetLastError(), "k_groups");
 }
 
@@ -1421,13 +1441,19 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
     const std::vector<int32_t>& h_ny = su.h_ny;
     const std::vector<int32_t>& h_nx = su.h_nx;
     check(cudaEventRecord(ctx->ev0, st), "event");
-    const int64_t nk = (int64_t)plan.kernel_groups.size();
+    const int64_t nk = plan.n_kernel;
     if (nk > 0) {
+        // every bucket's group list back to back, one queue counter per bucket
+        std::vector<int32_t> lists;
+        for (const Bucket& B : plan.buckets) lists.insert(lists.end(), B.groups.begin(), B.groups.end());
         int32_t* d_list = (int32_t*)scratch(ctx, "grp_list", sizeof(int32_t) * nk);
-        int* d_queue = (int*)scratch(ctx, "grp_queue", sizeof(int));
-        check(cudaMemcpyAsync(d_list, plan.kernel_groups.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st),
-              "h2d");
-        launch_groups(ctx, st, su, d_list, d_queue, 256, 0);
+        int* d_queue = (int*)scratch(ctx, "grp_queue", sizeof(int) * plan.buckets.size());
+        check(cudaMemcpyAsync(d_list, lists.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st), "h2d");
+        int64_t at = 0;
+        for (size_t b = 0; b < plan.buckets.size(); ++b) {
+            launch_bucket(ctx, st, su, plan.buckets[b], d_list + at, d_queue + b, 0, 0);
+            at += (int64_t)plan.buckets[b].groups.size();
+        }
     }
     check(cudaEventRecord(ctx->ev1, st), "event");
     check(cudaStreamSynchronize(st), "sync");
@@ -1541,8 +1567,10 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
 // ---------------------------------------------------------------------------
 struct GroupBatch {
     GroupSetup su;
-    int32_t* d_list = nullptr;  // owned
-    int* d_queue = nullptr;     // owned
+    int32_t* d_list = nullptr;  // owned: every bucket's groups back to back
+    int* d_queue = nullptr;     // owned: one counter per bucket
+    std::vector<int64_t> at;    // first list entry of each bucket
+    std::vector<int> threads;   // chosen block size per bucket
 };
 
 GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G,
@@ -1557,19 +1585,25 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
         if (G > 0)
             setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,
                          total_pixels, out, nullptr, nullptr, nullptr, nullptr, b->su);
-        if (!b->su.plan.routed_groups.empty())
-            throw ArgError{"group " + std::to_string(b->su.plan.routed_groups[0]) +
+        const GroupPlan& plan = b->su.plan;
+        if (!plan.routed_groups.empty())
+            throw ArgError{"group " + std::to_string(plan.routed_groups[0]) +
                            " is too large for one thread block (more than 64 stars, or a working set beyond shared "
                            "memory); fit it with cpb_fit_simultaneous_batch instead of a captured batch"};
-        const int64_t nk = (int64_t)b->su.plan.kernel_groups.size();
-        if (cudaMalloc(&b->d_list, sizeof(int32_t) * std::max<int64_t>(nk, 1)) != cudaSuccess ||
-            cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess) {
-            cudaGetLastError();
-            throw OomError{"device memory exhausted allocating the group work queue"};
+        std::vector<int32_t> lists;
+        for (const Bucket& B : plan.buckets) {
+            b->at.push_back((int64_t)lists.size());
+            b->threads.push_back(B.threads);
+            lists.insert(lists.end(), B.groups.begin(), B.groups.end());
         }
-        if (nk > 0)
-            check(cudaMemcpy(b->d_list, b->su.plan.kernel_groups.data(), sizeof(int32_t) * nk,
-                             cudaMemcpyHostToDevice), "h2d");
+        if (cudaMalloc(&b->d_list, sizeof(int32_t) * std::max<size_t>(lists.size(), 1)) != cudaSuccess ||
+            cudaMalloc(&b->d_queue, sizeof(int) * std::max<size_t>(plan.buckets.size(), 1)) != cudaSuccess) {
+            cudaGetLastError();
+            throw OomError{"device memory exhausted allocating the group work queues"};
+        }
+        if (!lists.empty())
+            check(cudaMemcpy(b->d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice),
+                  "h2d");
     } catch (...) {
         cudaFree(b->d_list);
         cudaFree(b->d_queue);
@@ -1579,24 +1613,33 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
     return b;
 }
 
-void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int threads, int blocks_per_sm) {
-    launch_groups(ctx, st, b->su, b->d_list, b->d_queue, threads, blocks_per_sm);
+int group_batch_buckets(const GroupBatch* b) { return (int)b->su.plan.buckets.size(); }
+
+// bucket < 0: every bucket, each with its chosen block size; threads <= 0: the chosen one.
+void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int bucket, int threads) {
+    const auto& bks = b->su.plan.buckets;
+    for (int k = 0; k < (int)bks.size(); ++k) {
+        if (bucket >= 0 && k != bucket) continue;
+        launch_bucket(ctx, st, b->su, bks[k], b->d_list + b->at[k], b->d_queue + k,
+                      threads > 0 ? threads : b->threads[k], 0);
+    }
 }
 
-int group_batch_occupancy(GroupBatch* b, int threads) {
-    if (b->su.plan.kernel_groups.empty()) return 1;
-    return group_occupancy(b->su, threads);
+void group_batch_set_threads(GroupBatch* b, int bucket, int threads) { b->threads[bucket] = valid_threads(threads); }
+int group_batch_threads(const GroupBatch* b, int bucket) { return b->threads[bucket]; }
+int group_batch_occupancy(GroupBatch* b, int bucket, int threads) {
+    return group_occupancy(b->su.plan.buckets[bucket], threads);
 }
+int64_t group_batch_size(const GroupBatch* b) { return b->su.plan.n_kernel; }
 
-int64_t group_batch_size(const GroupBatch* b) { return (int64_t)b->su.plan.kernel_groups.size(); }
-
-// Tuning signature: what the best launch shape depends on.
-std::string group_batch_signature(const GroupBatch* b) {
+// Tuning signature of one bucket: what its best block size depends on.
+std::string group_batch_signature(const GroupBatch* b, int bucket) {
     const GroupSetup& su = b->su;
+    const Bucket& B = su.plan.buckets[bucket];
     char buf[256];
-    std::snprintf(buf, sizeof(buf), "groups psf%d nodes%d el%d p%d S2_%d mR%d nmax%d umax%d wide%d G2^%d",
-                  su.dp.kind, su.dp.n_nodes, su.eltype, su.C.p, su.C.S2, su.C.mR, su.plan.nmax, su.plan.umax,
-                  su.plan.wide_mask ? 1 : 0, (int)std::log2((double)std::max<size_t>(su.plan.kernel_groups.size(), 1)));
+    std::snprintf(buf, sizeof(buf), "groups psf%d nodes%d el%d p%d S2_%d mR%d nmax%d umax%d G2^%d", su.dp.kind,
+                  su.dp.n_nodes, su.eltype, su.C.p, su.C.S2, su.C.mR, B.nmax, B.umax,
+                  (int)std::log2((double)std::max<size_t>(B.groups.size(), 1)));
     return buf;
 }
 

@@ -429,10 +429,14 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
                                int32_t eltype, const void* d_iv, const void* d_bkg, const int64_t* d_soff,
                                const double* d_y0, const double* d_x0, const double* d_f0, int64_t total_pixels,
                                const cpb_group_result* out);
-void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int threads, int blocks_per_sm);
-int group_batch_occupancy(GroupBatch* b, int threads);
+// Groups are launched in buckets of similar star count (one launch each).
+int group_batch_buckets(const GroupBatch* b);
+void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int bucket, int threads);
+void group_batch_set_threads(GroupBatch* b, int bucket, int threads);
+int group_batch_threads(const GroupBatch* b, int bucket);
+int group_batch_occupancy(GroupBatch* b, int bucket, int threads);
 int64_t group_batch_size(const GroupBatch* b);
-std::string group_batch_signature(const GroupBatch* b);
+std::string group_batch_signature(const GroupBatch* b, int bucket);
 void group_batch_destroy(GroupBatch* b);
 
 // Batched LM driver (cpb_lm.cu).  Host inputs.

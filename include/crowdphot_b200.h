@@ -405,8 +405,11 @@ CPB_API int cpb_fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_
  * real fits once; outputs are overwritten), keeps the fastest and records it;
  * 2 re-tunes even when cached.  The shapes are: persistent blocks per SM (1
  * or 2) and whether the ePSF node is staged in shared memory for the fit_star
- * kernel; threads per block (128 or 256) and resident blocks per SM for the
- * group kernel.  `info` (nullable) reports the choice.
+ * kernel; threads per block (64, 128 or 256) for each launch of the group
+ * kernel (groups are launched in buckets of similar star count, each with a
+ * shared-memory layout sized for its largest group).  `info` (nullable)
+ * reports the choice; its grp_* fields describe the launch of the largest
+ * groups.
  */
 typedef struct cpb_tune_info {
     int32_t lm_blocks_per_sm;

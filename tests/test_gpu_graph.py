@@ -75,7 +75,7 @@ def test_graph_matches_direct_entries_and_replays_new_inputs(tmp_path):
                        cache_path=cache)
     info = g.tune_info()
     assert info["n_timed"] >= 3 and info["from_cache"] == 0
-    assert info["grp_threads"] in (128, 256) and info["lm_blocks_per_sm"] in (1, 2)
+    assert info["grp_threads"] in (64, 128, 256) and info["lm_blocks_per_sm"] in (1, 2)
     t = g.launch()
     assert t > 0
     check_against_direct(psf, dl, tl, dg, tg)
