@@ -652,8 +652,8 @@ def run_gpu_c4(args):
     gr.update(y=t(dg["y"]), x=t(dg["x"]), flux=t(dg["flux"]))
     gr["out"] = {k: torch.from_numpy(v).to(dev) for k, v in group_outputs(ns, n_grp).items()}
     cache = os.path.join(_tf.gettempdir(), f"cpb_tune_{os.getuid()}.txt")
-    graph = cpb.BatchGraph(psf, lm=lm, lm_fixed={"bkg": 0.0}, groups=gr, fit_rad=5, group_kw=C4_GKW, autotune=1,
-                           cache_path=cache, ctx=ctx)
+    graph = cpb.BatchGraph(psf, lm=lm, lm_fixed={"bkg": 0.0}, groups=gr, fit_rad=5, group_kw=C4_GKW,
+                           autotune=0 if args.quick else 1, cache_path=cache, ctx=ctx)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def fitted_now():
@@ -683,6 +683,15 @@ def run_gpu_c4(args):
     barrier()
     clk = clocks.stop() if clocks else None
     _, launches = ctx.kernel_stats(reset=True)
+    if args.quick:
+        if rank == 0:
+            print(json.dumps({"quick": True, "value": (f_lm + f_g) / sum(times), "unit": "stars/s",
+                              "ms_per_step": 1e3 * sum(times) / args.steps, "gpu_launches": launches,
+                              "config": c4_config(n_cut, n_grp, ns)}))
+        graph.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
     agg = torch.tensor([sum(times), float(f_lm + f_g), float(launches)], dtype=torch.float64, device=dev)
     if world > 1:
         mx, sm = agg.clone(), agg.clone()

@@ -12,9 +12,9 @@ Differences from the Julia API, all deliberate:
   * the device computes in FP64 and results are returned as float64 arrays
     (Float32 cannot hold 1e-4 px at 2048 px);
   * ``background`` (image-shaped, optional) is subtracted on the device;
-  * ``solver=:lsmr``, ``model_rad=:auto``, IRLS ``reweight`` and PSF types
-    other than CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF}
-    raise ArgumentError -- there is no CPU fallback;
+  * ``solver=:lsmr``, IRLS ``reweight`` and PSF types other than
+    CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF} raise
+    ArgumentError -- there is no CPU fallback;
   * ``spread_model`` / ``spread_model_err`` are NaN.
 """
 from __future__ import annotations

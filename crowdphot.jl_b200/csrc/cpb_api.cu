@@ -327,6 +327,10 @@ int cpb_psf_upload(cpb_ctx* ctx, const cpb_psf_desc* d, cpb_psf** out) {
             dp.index_grid = ps->d_index_grid;
             dp.total_elems = (int64_t)h64.size();
             ps->h_nodes = nodes;
+            ps->h_data64 = h64;
+            ps->h_ygrid = yg;
+            ps->h_xgrid = xg;
+            ps->h_index_grid = ig;
             ps->smem_bytes64 = (int64_t)h64.size() * 8;
             ps->smem_bytes32 = (int64_t)h64.size() * 4;
         } catch (...) {

@@ -287,6 +287,13 @@ struct cpb_psf {
     std::vector<cpb::DevNode> h_nodes;
     int64_t smem_bytes64 = 0;  // padded bytes of all nodes in FP64
     int64_t smem_bytes32 = 0;
+    // host copies for the host-side curve of growth (model_rad = :auto)
+    std::vector<double> h_data64;
+    std::vector<double> h_ygrid, h_xgrid;
+    std::vector<int32_t> h_index_grid;
+    // unit-PSF annular surface brightness per (R_cap, fwhm), computed once
+    std::mutex cog_mu;
+    std::map<std::pair<int, double>, std::vector<double>> cog_sb;
 };
 
 struct cpb_ctx {
@@ -400,6 +407,12 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                          int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var, const void* d_background,
                          int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out);
+
+// model_rad = :auto (psf_photometry_simultaneous.jl:192-243), host side
+// (cpb_radii.cu): per-star model radii from the unit PSF's curve of growth and
+// the background noise of the weight sample.
+void model_radii_auto(const cpb_psf* psf, double fwhm, double nsigma, int R_fit, int R_cap,
+                      std::vector<double>& w_sample, const std::vector<double>& flux, std::vector<int32_t>& out);
 
 // Batched simultaneous fits of small groups (cpb_groups.cu).  Device inputs and
 // outputs; the h_*_opt arrays (nullable) are host copies of the group metadata.

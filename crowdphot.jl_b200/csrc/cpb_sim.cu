@@ -207,11 +207,11 @@ __global__ void k_tile_bounds(int64_t npairs, const uint32_t* keys, int32_t* sta
 }
 
 __global__ void k_tile_pack(int64_t npairs, const int32_t* sorted_j, const int32_t* ay, const int32_t* ax,
-                            int4* packed) {
+                            const int32_t* Rs, int Rconst, int4* packed) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= npairs) return;
     const int j = sorted_j[i];
-    packed[i] = make_int4(j, ay[j], ax[j], 0);
+    packed[i] = make_int4(j, ay[j], ax[j], Rs ? Rs[j] : Rconst);  // .w: the star's box radius
 }
 
 // ---------------------------------------------------------------------------
@@ -362,13 +362,13 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                                               const int32_t* __restrict__ ax, const double* __restrict__ w,
                                               const double* __restrict__ sw, T* __restrict__ V,
                                               double* __restrict__ colnorm, double* __restrict__ gram,
-                                              T* __restrict__ M, int Rb, int MS) {
+                                              T* __restrict__ M, int Rmax, int MS, const int32_t* __restrict__ Rs,
+                                              const int64_t* __restrict__ moff) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     AxisTab<T>* tabs = (AxisTab<T>*)smem_raw;  // [corner][axis][Sb]
     __shared__ double sh[32];
     __shared__ double cn_sh[6];
     __shared__ StarCoef c;
-    const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
     const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     const int p = fc.p;
     const int g0 = fc.gc[0] - 1, g1 = fc.gc[1] - 1, g2 = fc.gc[2] - 1;
@@ -377,6 +377,8 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
         const int j = list ? list[li] : (int)li;
         if (threadIdx.x == 0) c = coef[j];
         __syncthreads();
+        const int Rb = Rs ? Rs[j] : Rmax;  // this star's box radius (<= Rmax, which sized the tables)
+        const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
         const int a_y = ay[j], a_x = ax[j];
         if (!gauss) {
             for (int e = threadIdx.x; e < 8 * Sb; e += NTF) {
@@ -402,7 +404,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             T s = 0, dY = 0, dX = 0, g[3];
             if (gauss) {
                 const T val = gauss_eval<T, GRAD>((T)P.fwhm, c, (T)gy, (T)gx, g[0], g[1], g[2]);
-                if (M) M[(int64_t)j * MS + m] = val;
+                if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -417,7 +419,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                         dX += (T)c.dwdx[k] * pv - (T)c.w[k] * (T)nd.sx * pdu;
                     }
                 }
-                if (M) M[(int64_t)j * MS + m] = (T)c.flux * s + (T)c.bkg;
+                if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = (T)c.flux * s + (T)c.bkg;
                 g[0] = (T)c.flux * dY;
                 g[1] = (T)c.flux * dX;
                 g[2] = s;
@@ -502,13 +504,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                                                       const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
                                                       const double* __restrict__ w, const double* __restrict__ sw,
                                                       T* __restrict__ V, double* __restrict__ colnorm,
-                                                      double* __restrict__ gram, T* __restrict__ M, int Rb, int MS) {
+                                                      double* __restrict__ gram, T* __restrict__ M, int Rmax, int MS,
+                                                      const int32_t* __restrict__ Rs, const int64_t* __restrict__ moff) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
-    const int q32 = 32 / Sb, r32 = 32 % Sb;
-    AxisTab<T>* tcol = (AxisTab<T>*)smem_raw + wid * 2 * Sb;
-    AxisTab<T>* trow = tcol + Sb;
+    AxisTab<T>* tcol = (AxisTab<T>*)smem_raw + wid * 2 * (2 * Rmax + 1);
     const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     DevNode nd{};
     if (!gauss) nd = P.nodes[0];
@@ -524,6 +524,10 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const double cy = cg.y, cx = cg.x;
         const T flux = (T)cg.flux, bkg = (T)cg.bkg;
         const T w0 = (T)cg.w[0], dwy = (T)cg.dwdy[0], dwx = (T)cg.dwdx[0];
+        const int Rb = Rs ? Rs[j] : Rmax;  // this star's box radius
+        const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
+        const int q32 = 32 / Sb, r32 = 32 % Sb;
+        AxisTab<T>* trow = tcol + Sb;
         const int oy = ay[j] - Rb, ox = ax[j] - Rb;
         if (!gauss) {
             for (int idx = lane; idx < 2 * Sb; idx += 32) {
@@ -566,7 +570,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             for (int m = lane; m < S2b; m += 32) {
                 T val, a, b, c;
                 eval_px(row, col, val, a, b, c);
-                M[(int64_t)j * MS + m] = val;
+                M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
                 row += r32;
                 col += q32;
                 if (row >= Sb) {
@@ -643,7 +647,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     if (use || M) {
                         T val, a, b, c;
                         eval_px(row, col, val, a, b, c);
-                        if (M) M[(int64_t)j * MS + m] = val;
+                        if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
                         if (use) {
                             const T sq = (T)sw[q];
                             r0 = sq * a;
@@ -686,7 +690,8 @@ template <int KIND, int MODE, typename TS>
 __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
-                                               int Rb, int64_t stride, const double* __restrict__ vt,
+                                               int Rbox, int64_t stride, const int64_t* __restrict__ soff,
+                                               const double* __restrict__ vt,
                                                const double* u_src, double u_sign,
                                                double* out, const uint8_t* __restrict__ umask,
                                                const double* __restrict__ w, const double* __restrict__ sw,
@@ -696,6 +701,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
     __shared__ int s_j[NT];
     __shared__ int s_ay[NT];
     __shared__ int s_ax[NT];
+    __shared__ int s_rb[NT];
     __shared__ double s_v[3][NT];
     __shared__ int s_wcnt[NT / 32];
     __shared__ double sh[32];
@@ -707,7 +713,6 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         uscale = u_sign * sc->inv_beta;
     }
     const int p = KIND == KIND_JV ? fc.p : 1;
-    const int Sb = 2 * Rb + 1;
     const int reg = blockIdx.x;
     const int ry = reg % fc.nty, rx = reg / fc.nty;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -738,6 +743,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             s_j[pos] = ent.x;
             s_ay[pos] = ent.y;
             s_ax[pos] = ent.z;
+            s_rb[pos] = ent.w;
             if (KIND == KIND_JV)
                 for (int k = 0; k < fc.p; ++k) s_v[k][pos] = vt[(int64_t)ent.x * fc.p + k] * inv_alpha;
         }
@@ -745,13 +751,16 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         if (xs0 <= fc.nx) {
             for (int e = 0; e < total; ++e) {
                 const int ax_ = s_ax[e], ay_ = s_ay[e];
+                // model renders: each star's own model radius; J v: the fit box
+                const int Rb = KIND == KIND_M ? s_rb[e] : Rbox;
+                const int Sb = 2 * Rb + 1;
                 const int c_lo = max(ax_ - Rb, xs0), c_hi = min(ax_ + Rb, xend);
                 const int r_lo = max(ay_ - Rb, y0), r_hi = min(ay_ + Rb, yend);
                 if (c_lo > c_hi || r_lo > r_hi) continue;  // warp-uniform
                 const int nrows = r_hi - r_lo + 1;
                 const int tot = nrows * (c_hi - c_lo + 1);
                 const float inv_nrows = 1.0f / (float)nrows;
-                const TS* base = src + (int64_t)s_j[e] * stride;
+                const TS* base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride);
                 const int m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
                 const int a0 = (r_lo - y0) + (c_lo - xs0) * TY;
                 double wv0 = 1.0, wv1 = 0.0, wv2 = 0.0;
@@ -1260,7 +1269,7 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t
 
 struct TileLists {
     int32_t *start = nullptr, *end = nullptr;
-    int4* list = nullptr;  // (star, anchor y, anchor x, 0) per (tile, star) pair
+    int4* list = nullptr;  // (star, anchor y, anchor x, box radius) per (tile, star) pair
 };
 
 TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_t* ay, const int32_t* ax,
@@ -1301,7 +1310,7 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
         cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, sorted_j, npairs, 0, end_bit, st);
         k_tile_bounds<<<nblk(npairs), 256, 0, st>>>(npairs, k1, tl.start, tl.end);
         check(cudaGetLastError(), "k_tile_bounds");
-        k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_j, ay, ax, tl.list);
+        k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_j, ay, ax, Rs, Rconst, tl.list);
         check(cudaGetLastError(), "k_tile_pack");
     }
     return tl;
@@ -1518,22 +1527,47 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     check(cudaStreamSynchronize(st), "sync");
     out->n_union = (int64_t)h_ucnt;
 
-    // ---- model radii (:1111-1124); scalar model_rad only on the device path
+    // ---- model radii (:1111-1124)
     if (P->model_rad_auto && !d_inv_var)
         throw ArgError{
             "model_rad=:auto requires inv_var (it needs a noise scale); pass inv_var or an explicit scalar model_rad"};
-    if (P->model_rad_auto) throw ArgError{"model_rad=:auto is not supported by the B200 path; pass a scalar model_rad"};
-    int model_R;
-    {
+    int model_R;                  // the largest model radius (sizes the model stamps)
+    int32_t* d_modelR = nullptr;  // per active slot when model_rad = :auto
+    std::vector<int32_t> h_modelR;
+    double model_box_sum = 0;     // sum over active stars of (2 R_j + 1)^2
+    if (P->model_rad_auto) {
+        const int R_cap = (int)std::ceil(model_rad_max);
+        // the noise sample w[1 : step : end] and the active stars' catalogue fluxes
+        const int64_t step = std::max<int64_t>(1, npix / 65536);
+        const int64_t nsamp = (npix + step - 1) / step;
+        std::vector<double> wsamp(nsamp), f0(n_stars);
+        std::vector<int32_t> h_act_order(n_act);
+        check(cudaMemcpy2DAsync(wsamp.data(), sizeof(double), w, step * sizeof(double), sizeof(double), nsamp,
+                                cudaMemcpyDeviceToHost, st), "d2h weight sample");
+        check(cudaMemcpyAsync(f0.data(), d_flux0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaMemcpyAsync(h_act_order.data(), act, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaStreamSynchronize(st), "sync");
+        std::vector<double> fl(n_act);
+        for (int64_t j = 0; j < n_act; ++j) fl[j] = f0[h_act_order[j]];
+        model_radii_auto(psf, P->fixed_fwhm, P->model_rad_nsigma, fc.R, R_cap, wsamp, fl, h_modelR);
+        model_R = *std::max_element(h_modelR.begin(), h_modelR.end());
+        d_modelR = S<int32_t>(ctx, "model_R", n_act);
+        check(cudaMemcpyAsync(d_modelR, h_modelR.data(), sizeof(int32_t) * n_act, cudaMemcpyHostToDevice, st),
+              "h2d model radii");
+        for (int32_t r : h_modelR) model_box_sum += (double)(2 * r + 1) * (2 * r + 1);
+    } else {
         const int R_cap = (int)std::ceil(std::max(P->model_rad, P->fit_rad));
         model_R = std::min(std::max((int)std::ceil(P->model_rad), fc.R), R_cap);
+        model_box_sum = (double)n_act * (2 * model_R + 1) * (2 * model_R + 1);
     }
+    const double mean_box = model_box_sum / (double)n_act;  // per-star render work (instrumentation)
     const double dof = (double)std::max<int64_t>((int64_t)h_ucnt - n, 1);
 
     // ---- tile lists (fit box for J v; model box for renders)
     TileLists tfit = build_tiles(ctx, "tfit", n_act, ay, ax, nullptr, fc.R, ny, nx, fc.nty, fc.ntx);
-    TileLists tmod = model_R == fc.R ? tfit
-                                     : build_tiles(ctx, "tmod", n_act, ay, ax, nullptr, model_R, ny, nx, fc.nty, fc.ntx);
+    TileLists tmod = (model_R == fc.R && !d_modelR)
+                         ? tfit
+                         : build_tiles(ctx, "tmod", n_act, ay, ax, d_modelR, model_R, ny, nx, fc.nty, fc.ntx);
 
     // ---- working buffers (:1129-1166)
     TS* V = S<TS>(ctx, "V", (int64_t)fc.VS * n_act);
@@ -1569,21 +1603,47 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     void* live_tmp = scratch(ctx, "live_tmp", live_tmp_bytes);
 
     const int fill_blocks = (int)std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16);
-    // per-star model values of the render box (one block of MS per star)
+    // per-star model values of the render box: one block of MS per star, or with
+    // per-star radii (:auto) each star's own (2 R_j + 1)^2 block at moff[j]
     const int Sm = 2 * model_R + 1;
     const int MS = ((Sm * Sm + 15) / 16) * 16;
-    TS* Mbuf = S<TS>(ctx, "model_stamps", (int64_t)MS * n_act);
+    int64_t* d_moff = nullptr;
+    int64_t mtotal = (int64_t)MS * n_act;
+    if (d_modelR) {
+        std::vector<int64_t> h_moff(n_act);
+        mtotal = 0;
+        for (int64_t j = 0; j < n_act; ++j) {
+            h_moff[j] = mtotal;
+            const int64_t sj = 2 * (int64_t)h_modelR[j] + 1;
+            mtotal += (sj * sj + 15) / 16 * 16;
+        }
+        d_moff = S<int64_t>(ctx, "model_off", n_act);
+        check(cudaMemcpyAsync(d_moff, h_moff.data(), sizeof(int64_t) * n_act, cudaMemcpyHostToDevice, st), "h2d");
+    }
+    TS* Mbuf = S<TS>(ctx, "model_stamps", mtotal);
     constexpr double bts = sizeof(TS);  // bytes per stored stamp / model value
     int32_t* evlist = S<int32_t>(ctx, "eval_list", n_act);
     const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
     bool m_fresh = false;  // Mbuf holds the current-theta model of the live stars (written by the fill)
     const bool warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
-    if (warp_eval && 8 * 2 * std::max(fc.S, Sm) * sizeof(AxisTab<double>) > 48 * 1024)
-        throw ArgError{"fit or model radius too large for the B200 stamp kernels"};
+    if (warp_eval && 8 * 2 * fc.S * sizeof(AxisTab<double>) > 48 * 1024)
+        throw ArgError{"fit radius too large for the B200 stamp kernels"};
+    // model-value launches of the warp kernel: as many warps a block as their
+    // row / column tables fit in shared memory (large :auto model boxes use fewer)
+    int smem_optin = 0;
+    check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
+    auto model_warp_shape = [&](size_t tab_size, unsigned& threads, size_t& smem) {
+        int warps = 8;
+        while (warps > 1 && (size_t)warps * 2 * Sm * tab_size > (size_t)smem_optin) warps /= 2;
+        if ((size_t)warps * 2 * Sm * tab_size > (size_t)smem_optin)
+            throw ArgError{"model radius too large for the B200 render kernel"};
+        threads = 32u * warps;
+        smem = (size_t)warps * 2 * Sm * tab_size;
+    };
     auto eval_grid = [&](int64_t nlist) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16)); };
     auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
         if (nlist <= 0) return;
-        const bool writeM = !gram && model_R == fc.R;
+        const bool writeM = !gram && model_R == fc.R && !d_modelR;
         KernelScope ks_(ctx, gram ? "k_eval_gram" : "k_eval_fill",
                         (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * bts + p * 8) + (writeM ? fc.S2 * bts : 0.0) +
                                          std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1)) * 16 +
@@ -1592,13 +1652,13 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         TS* Mo = writeM ? Mbuf : nullptr;
         if (warp_eval) {
             const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, TS><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval_warp<true, TS><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
         } else if (fc.S2 <= 256 * 2)
-            k_eval<256, 2, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 2, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
         else if (fc.S2 <= 256 * 4)
-            k_eval<256, 4, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 4, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
         else if (fc.S2 <= 256 * 8)
-            k_eval<256, 8, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS);
+            k_eval<256, 8, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
         else
             throw ArgError{"fit_rad too large for the B200 stamp kernel (ceil(fit_rad) must be <= 22)"};
         check(cudaGetLastError(), "k_eval_fill");
@@ -1612,16 +1672,23 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         const size_t smem = tab_bytes * Sm;
         const unsigned gb = eval_grid(nlist);
         if (warp_eval) {
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<false, TS><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            unsigned thr;
+            size_t sm_bytes;
+            model_warp_shape(sizeof(AxisTab<TS>), thr, sm_bytes);
+            if (sm_bytes > 48 * 1024)
+                check(cudaFuncSetAttribute(k_eval_warp<false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm_bytes), "smem attr");
+            const int wpb = (int)(thr / 32);
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
         } else if (Sm * Sm <= 256)
-            k_eval<256, 1, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 1, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
         else if (Sm * Sm <= 512)
-            k_eval<256, 2, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 2, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
         else if (Sm * Sm <= 1024)
-            k_eval<256, 4, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 4, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
         else if (Sm * Sm <= 2048)
-            k_eval<256, 8, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS);
+            k_eval<256, 8, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
         else
             throw ArgError{"model_rad too large for the B200 render kernel (ceil(model_rad) must be <= 22)"};
         check(cudaGetLastError(), "k_eval_model");
@@ -1636,16 +1703,16 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                         (double)npix * px_bytes + (double)nlist * Sm * Sm * bts);
         switch (mode) {
             case MODE_CUR:
-                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_CAND:
-                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_FREEZE:
-                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             default:
-                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
         }
         check(cudaGetLastError(), "k_gather");
     };
@@ -1668,7 +1735,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     launch_fill(live_list, n_live, nullptr);
     launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
     check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
-    evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
+    evals += (double)n_live * (fc.S2 + mean_box);
     bool fresh = true;  // V / wt_resid / cost are at the current theta and live set
     double lam = P->lambda_init;
     int n_run = 0;
@@ -1680,7 +1747,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
             KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
             launch_fill(live_list, n_live, nullptr);
             launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
-            evals += (double)n_live * (fc.S2 + (2 * model_R + 1) * (2 * model_R + 1));
+            evals += (double)n_live * (fc.S2 + mean_box);
         }
         fresh = false;
         // b_scaled = J' wt_resid (frozen stars stay 0)
@@ -1735,7 +1802,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
                         KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * 8);
-                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
+                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, nullptr, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
                     }
                     {
                         KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
@@ -1754,7 +1821,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
             }
             KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
             launch_render(MODE_CAND, live, live_list, n_live, coefc, nullptr, data_work, &sc->cost_cand);
-            evals += (double)n_live * (2 * model_R + 1) * (2 * model_R + 1);
+            evals += (double)n_live * mean_box;
             read_scalars();
             n_lsqr += h_sc->iter;
             macs += 2.0 * h_sc->iter * n_live * fc.S2;
@@ -1799,7 +1866,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                         cub::DeviceSelect::Flagged(tmpb, tb, iota_act, newf, evlist, d_nlive, (int)n_act, st);
                     }
                     launch_render(MODE_FREEZE, newf, evlist, h_new, coef, data_work, nullptr, nullptr);
-                    evals += (double)h_new * (2 * model_R + 1) * (2 * model_R + 1);
+                    evals += (double)h_new * mean_box;
                     update_live_list();
                 }
                 break;
@@ -1824,16 +1891,16 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         if (warp_eval) {
             const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
             k_eval_warp<true, double><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<double>), st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
         } else if (fc.S2 <= 256 * 2) {
             k_eval<256, 2, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
         } else if (fc.S2 <= 256 * 4) {
             k_eval<256, 4, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
         } else {
             k_eval<256, 8, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS);
+                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
         }
         check(cudaGetLastError(), "k_eval_gram");
     }
@@ -1844,28 +1911,35 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     // ---- final render against the original data (:1344-1356) and diagnostics
     double* resid = S<double>(ctx, "resid", npix);
     {
-        double* M64 = std::is_same<TS, double>::value ? (double*)Mbuf : S<double>(ctx, "model_stamps64", (int64_t)MS * n_act);
+        double* M64 = std::is_same<TS, double>::value ? (double*)Mbuf : S<double>(ctx, "model_stamps64", mtotal);
         {
             KernelScope ks_(ctx, "k_eval_model", (double)n_act * ((double)Sm * Sm * 8 + sizeof(StarCoef)));
             if (warp_eval) {
-                const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
-                k_eval_warp<false, double><<<gbw, 256, 8 * 2 * Sm * sizeof(AxisTab<double>), st>>>(
-                    nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                unsigned thr;
+                size_t sm_bytes;
+                model_warp_shape(sizeof(AxisTab<double>), thr, sm_bytes);
+                if (sm_bytes > 48 * 1024)
+                    check(cudaFuncSetAttribute(k_eval_warp<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)sm_bytes), "smem attr");
+                const int wpb = (int)(thr / 32);
+                const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+                k_eval_warp<false, double><<<gbw, thr, sm_bytes, st>>>(
+                    nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
             } else {
                 const size_t sm_ = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * Sm;
                 if (Sm * Sm <= 256)
-                    k_eval<256, 1, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                    k_eval<256, 1, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
                 else if (Sm * Sm <= 512)
-                    k_eval<256, 2, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                    k_eval<256, 2, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
                 else if (Sm * Sm <= 1024)
-                    k_eval<256, 4, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                    k_eval<256, 4, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
                 else
-                    k_eval<256, 8, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS);
+                    k_eval<256, 8, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
             }
             check(cudaGetLastError(), "k_eval_model");
         }
         KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
-        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
+        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
     double* diag = S<double>(ctx, "diag", (int64_t)n_act * 5);
@@ -1958,7 +2032,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         out->converged[i] = h_conv[j];
         out->n_iter[i] = h_live[j] ? n_run : h_frozen[j];
         if (out->dbg_active) out->dbg_active[j] = h_act[j];
-        if (out->dbg_model_R) out->dbg_model_R[j] = model_R;
+        if (out->dbg_model_R) out->dbg_model_R[j] = d_modelR ? h_modelR[j] : model_R;
         if (!valid[i]) continue;
         const double* dg = &h_diag[j * 5];
         if (out->chisq) out->chisq[i] = dg[0];

@@ -118,7 +118,7 @@ typedef struct cpb_sim_params {
     int32_t inner_iterations; /* 10 */
     double fixed_y, fixed_x, fixed_flux, fixed_bkg, fixed_fwhm;
     double linear_tol;        /* 1e-6 */
-    int32_t model_rad_auto;   /* 1 = :auto */
+    int32_t model_rad_auto;   /* 1 = :auto: per-star radii from the unit PSF's curve of growth (needs inv_var) */
     int32_t max_trials;       /* 8 */
     double model_rad;         /* used when model_rad_auto == 0 */
     double model_rad_max;     /* 10*fit_rad */

@@ -64,6 +64,15 @@ def load():
         lib.orc_model_radii_auto_gaussian.restype = C.c_int
         lib.orc_model_radii_auto_gaussian.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int64, _dp,
                                                       C.c_int64, _dp, _i32p]
+        lib.orc_exact_overlap.restype = C.c_double
+        lib.orc_exact_overlap.argtypes = [C.c_double, C.c_double, C.c_double]
+        lib.orc_aperture_weight.restype = C.c_double
+        lib.orc_aperture_weight.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int64]
+        lib.orc_unit_curve_of_growth.restype = C.c_int
+        lib.orc_unit_curve_of_growth.argtypes = [C.POINTER(_abi.PsfDesc), C.c_double, C.c_int, _dp]
+        lib.orc_model_radii_auto.restype = C.c_int
+        lib.orc_model_radii_auto.argtypes = [C.POINTER(_abi.PsfDesc), C.c_double, C.c_double, C.c_int, C.c_int,
+                                             C.c_int64, _dp, C.c_int64, _dp, _i32p]
         lib.orc_fit_star_batch.restype = C.c_int
         lib.orc_fit_star_batch.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_int64, _i64p,
                                            _i32p, _i32p, _i32p, _i32p, _dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp,
@@ -253,6 +262,42 @@ def orc_fill_stamps(psf, fixed, R, ny, nx, pixels, anchor_y, anchor_x, theta, w,
     del keep
     if rc != 0:
         raise ArgumentError("bad psf")
+
+
+def orc_exact_overlap(dx, dy, r):
+    """Exact area of the unit pixel centred at (dx, dy) inside a circle of radius r at the origin."""
+    return float(load().orc_exact_overlap(float(dx), float(dy), float(r)))
+
+
+def orc_aperture_weight(yc, xc, r, i, j):
+    """aperture_weight(CircularAperture(yc, xc, r), i, j, ExactOverlap())."""
+    return float(load().orc_aperture_weight(float(yc), float(xc), float(r), int(i), int(j)))
+
+
+def orc_unit_curve_of_growth(psf, R_cap, fwhm=None):
+    lib = load()
+    desc, keep = psf_descriptor(psf)
+    out = np.zeros(R_cap)
+    rc = lib.orc_unit_curve_of_growth(C.byref(desc), float(getattr(psf, "fwhm", 0.0) if fwhm is None else fwhm),
+                                      int(R_cap), out.ctypes.data_as(_dp))
+    del keep
+    if rc != 0:
+        raise ArgumentError("bad psf")
+    return out
+
+
+def orc_model_radii_auto(psf, nsigma, R_fit, R_cap, w, flux, fwhm=None):
+    lib = load()
+    desc, keep = psf_descriptor(psf)
+    ww, ff = _f64(w), _f64(flux)
+    out = np.zeros(ff.size, np.int32)
+    rc = lib.orc_model_radii_auto(C.byref(desc), float(getattr(psf, "fwhm", 0.0) if fwhm is None else fwhm),
+                                  float(nsigma), int(R_fit), int(R_cap), ww.size, ww.ctypes.data_as(_dp), ff.size,
+                                  ff.ctypes.data_as(_dp), out.ctypes.data_as(_i32p))
+    del keep
+    if rc != 0:
+        raise ArgumentError("no positive weights")
+    return out
 
 
 def orc_model_radii_auto_gaussian(fwhm, nsigma, R_fit, R_cap, w, flux):

@@ -9,10 +9,10 @@
 //     of raising Julia's InexactError from round(Int, NaN);
 //   * a negative Morton anchor raises CPB_ERR_ARGUMENT (Julia raises
 //     InexactError from UInt64(negative)) -- same outcome: the call fails;
-//   * solver = :lsmr and model_rad = :auto are rejected with ArgumentError
-//     text (the GPU path implements LSQR with a scalar model_rad; :auto is
-//     restated by orc_model_radii_auto for the CircularGaussianPSF analytic
-//     curve of growth only);
+//   * solver = :lsmr is rejected with ArgumentError text (the GPU path
+//     implements LSQR); model_rad = :auto follows _model_radii with the unit
+//     PSF's curve of growth (analytic for the Gaussian, exact-overlap apertures
+//     otherwise), in FP64 whatever the image eltype;
 //   * spread_model / spread_model_err are not computed (NaN).
 #include <algorithm>
 #include <cmath>
@@ -458,6 +458,142 @@ void orc_bicubic(const double* data, int64_t ny, int64_t nx, int64_t n, const do
     for (int64_t i = 0; i < n; ++i) bicubic(data, ny, nx, y[i], x[i], fill, out[3 * i], out[3 * i + 1], out[3 * i + 2]);
 }
 
+// Exact pixel / circle overlap (apertures.jl:196-290, the photutils algorithm):
+// area of the rectangle [x0, x1] x [y0, y1] inside the circle of radius r at
+// the origin, by splitting the rectangle at the axes into first-quadrant pieces.
+static double tri_area(double ax, double ay, double bx, double by, double cx, double cy) {
+    return std::fabs(ax * (by - cy) + bx * (cy - ay) + cx * (ay - by)) / 2;
+}
+static double seg_area(double ax, double ay, double bx, double by, double r) {
+    double chord = std::sqrt((bx - ax) * (bx - ax) + (by - ay) * (by - ay));
+    double th = 2 * std::asin(chord / (2 * r));
+    return r * r * (th - std::sin(th)) / 2;
+}
+static double quad_overlap(double x0, double y0, double x1, double y1, double r) {  // 0 <= x0, 0 <= y0
+    double r2 = r * r;
+    if (x0 * x0 + y0 * y0 > r2) return 0.0;
+    if (x1 * x1 + y1 * y1 < r2) return (x1 - x0) * (y1 - y0);
+    bool c1 = std::sqrt(x1 * x1 + y0 * y0) < r, c2 = std::sqrt(x0 * x0 + y1 * y1) < r;
+    if (c1 && c2) {
+        double px = std::sqrt(r2 - y1 * y1), qy = std::sqrt(r2 - x1 * x1);
+        return (x1 - x0) * (y1 - y0) - tri_area(px, y1, x1, qy, x1, y1) + seg_area(px, y1, x1, qy, r);
+    }
+    if (c1) {
+        double py = std::sqrt(r2 - x0 * x0), qy = std::sqrt(r2 - x1 * x1);
+        return seg_area(x0, py, x1, qy, r) + tri_area(x0, py, x0, y0, x1, y0) + tri_area(x0, py, x1, y0, x1, qy);
+    }
+    if (c2) {
+        double px = std::sqrt(r2 - y0 * y0), qx = std::sqrt(r2 - y1 * y1);
+        return seg_area(px, y0, qx, y1, r) + tri_area(px, y0, x0, y0, x0, y1) + tri_area(px, y0, x0, y1, qx, y1);
+    }
+    double px = std::sqrt(r2 - y0 * y0), qy = std::sqrt(r2 - x0 * x0);
+    return seg_area(px, y0, x0, qy, r) + tri_area(px, y0, x0, qy, x0, y0);
+}
+static double rect_overlap(double x0, double y0, double x1, double y1, double r) {
+    if (r <= 0) return 0.0;
+    if (x0 >= 0) {
+        if (y0 >= 0) return quad_overlap(x0, y0, x1, y1, r);
+        if (y1 <= 0) return quad_overlap(-y1, x0, -y0, x1, r);
+        return rect_overlap(x0, y0, x1, 0, r) + rect_overlap(x0, 0, x1, y1, r);
+    }
+    if (x1 <= 0) {
+        if (y0 >= 0) return quad_overlap(-x1, y0, -x0, y1, r);
+        if (y1 <= 0) return quad_overlap(-x1, -y1, -x0, -y0, r);
+        return rect_overlap(x0, y0, x1, 0, r) + rect_overlap(x0, 0, x1, y1, r);
+    }
+    if (y0 >= 0 || y1 <= 0) return rect_overlap(x0, y0, 0, y1, r) + rect_overlap(0, y0, x1, y1, r);
+    return rect_overlap(x0, y0, 0, 0, r) + rect_overlap(0, y0, x1, 0, r) + rect_overlap(x0, 0, 0, y1, r) +
+           rect_overlap(0, 0, x1, y1, r);
+}
+// aperture_weight(CircularAperture(yc, xc, r), i, j, ExactOverlap()) (apertures.jl:93-103, 160-166).
+static double exact_weight(double yc, double xc, double r, int64_t i, int64_t j) {
+    double dy = (double)i - yc, dx = (double)j - xc, d2 = dx * dx + dy * dy, h = std::sqrt(2.0) / 2;
+    if (d2 > (r + h) * (r + h)) return 0.0;
+    if (r > h && d2 < (r - h) * (r - h)) return 1.0;
+    return rect_overlap(dx - 0.5, dy - 0.5, dx + 0.5, dy + 0.5, r);
+}
+
+extern "C" {
+double orc_exact_overlap(double dx, double dy, double r) { return rect_overlap(dx - 0.5, dy - 0.5, dx + 0.5, dy + 0.5, r); }
+double orc_aperture_weight(double yc, double xc, double r, int64_t i, int64_t j) { return exact_weight(yc, xc, r, i, j); }
+}
+
+// curve_of_growth (curve_of_growth.jl:143-173) of the unit model
+// (y = x = 0, flux = 1, bkg = 0) at radii 1..R_cap; the Gaussian uses its
+// analytic overload (:180-195).
+static void unit_curve_of_growth(const Psf& psf, int R_cap, std::vector<double>& cog) {
+    cog.assign(R_cap, 0.0);
+    if (psf.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        for (int r = 1; r <= R_cap; ++r)
+            cog[r - 1] = 1.0 * (1.0 - std::exp(gauss_pre() * ((double)r * (double)r) / (psf.fwhm * psf.fwhm)));
+        return;
+    }
+    StarP unit{0.0, 0.0, 1.0, 0.0, psf.fwhm};
+    for (int r = 1; r <= R_cap; ++r) {
+        // bounding_axes (apertures.jl:52-66) of a circle of integer radius at the origin: -r..r
+        double tot = 0;
+        for (int64_t j = -r; j <= r; ++j)
+            for (int64_t i = -r; i <= r; ++i) {
+                double w = exact_weight(0.0, 0.0, (double)r, i, j);
+                if (!(w > 0)) continue;
+                tot += w * evaluate(psf, unit, (double)i, (double)j);
+            }
+        cog[r - 1] = tot;
+    }
+}
+
+// _model_radii, :auto branch (:209-243), any supported PSF.
+static int model_radii_auto(const Psf& psf, double nsigma, int R_fit, int R_cap, int64_t nw, const double* w,
+                            int64_t n, const double* flux, int32_t* out) {
+    int64_t step = std::max<int64_t>(1, nw / 65536);
+    std::vector<double> ws;
+    for (int64_t i = 0; i < nw; i += step)
+        if (w[i] > 0 && std::isfinite(w[i])) ws.push_back(w[i]);
+    if (ws.empty()) return CPB_ERR_ARGUMENT;
+    std::sort(ws.begin(), ws.end());
+    double h = (double)(ws.size() - 1) * 0.84;  // quantile, type 7
+    size_t lo = (size_t)std::floor(h);
+    size_t hi = std::min(lo + 1, ws.size() - 1);
+    double wval = ws[lo] + (h - (double)lo) * (ws[hi] - ws[lo]);
+    double sigma_bg = wval > 0 ? std::sqrt(1.0 / wval) : 1.0;
+    std::vector<double> cog, sb(R_cap);
+    unit_curve_of_growth(psf, R_cap, cog);
+    double prev = 0;
+    for (int r = 1; r <= R_cap; ++r) {
+        double ee = cog[r - 1] / cog[R_cap - 1];
+        sb[r - 1] = std::max((ee - prev) / (M_PI * (double)(r * r - (r - 1) * (r - 1))), 0.0);
+        prev = ee;
+    }
+    double thr = nsigma * sigma_bg;
+    for (int64_t j = 0; j < n; ++j) {
+        double Fj = std::max(flux[j], 0.0);
+        int r = R_fit;
+        while (r < R_cap && Fj * sb[r - 1] > thr) ++r;
+        out[j] = r;
+    }
+    return 0;
+}
+
+extern "C" {
+// The unit model's curve of growth at radii 1..R_cap (tests).
+int orc_unit_curve_of_growth(const cpb_psf_desc* desc, double fwhm, int R_cap, double* out) {
+    Psf psf;
+    if (!load_psf(desc, psf).empty()) return CPB_ERR_ARGUMENT;
+    psf.fwhm = fwhm;
+    std::vector<double> cog;
+    unit_curve_of_growth(psf, R_cap, cog);
+    std::copy(cog.begin(), cog.end(), out);
+    return 0;
+}
+int orc_model_radii_auto(const cpb_psf_desc* desc, double fwhm, double nsigma, int R_fit, int R_cap, int64_t nw,
+                         const double* w, int64_t n, const double* flux, int32_t* out) {
+    Psf psf;
+    if (!load_psf(desc, psf).empty()) return CPB_ERR_ARGUMENT;
+    psf.fwhm = fwhm;
+    return model_radii_auto(psf, nsigma, R_fit, R_cap, nw, w, n, flux, out);
+}
+}
+
 // _model_radii, :auto branch (:209-243) for CircularGaussianPSF, whose curve
 // of growth is analytic (curve_of_growth.jl:180-195).  w: inverse-weight vector.
 int orc_model_radii_auto_gaussian(double fwhm, double nsigma, int R_fit, int R_cap, int64_t nw, const double* w,
@@ -702,13 +838,11 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
     const int R_fit = R;
     if (P->model_rad_auto) {
         const int R_cap = (int)std::ceil(model_rad_max);
-        if (psf.kind != CPB_PSF_CIRCULAR_GAUSSIAN) return fail("model_rad=:auto is supported for CircularGaussianPSF only");
         std::vector<double> fl(n_act);
         for (int64_t j = 0; j < n_act; ++j) fl[j] = flux0[active[j]];
         std::vector<int32_t> mr(n_act);
-        if (orc_model_radii_auto_gaussian(psf.fwhm, P->model_rad_nsigma, R_fit, R_cap, npix, w.data(), n_act,
-                                          fl.data(), mr.data()) != 0)
-            return fail("model_rad=:auto found no positive weights");
+        if (model_radii_auto(psf, P->model_rad_nsigma, R_fit, R_cap, npix, w.data(), n_act, fl.data(), mr.data()) != 0)
+            return fail("model_rad=:auto found no positive finite weights to estimate the noise");
         F.model_R.assign(mr.begin(), mr.end());
     } else {
         const int R_cap = (int)std::ceil(std::max(P->model_rad, P->fit_rad));

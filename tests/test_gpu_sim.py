@@ -212,3 +212,25 @@ def test_mixed_precision_isolated_noiseless_truth(kind):
     np.testing.assert_allclose(r.flux, src["flux"], rtol=2e-6)
     np.testing.assert_allclose(r.y, src["y"], atol=2e-5)
     np.testing.assert_allclose(r.x, src["x"], atol=2e-5)
+
+
+@pytest.mark.parametrize("case", ["gaussian", "epsf"])
+def test_model_rad_auto_radii_bit_exact_and_parity(case):
+    """model_rad = :auto (the reference's default): per-star model radii from the
+    unit PSF's curve of growth and the weight noise (_model_radii, :209-243) --
+    bit-exact against the oracle -- and the fit's parity gates with those radii."""
+    if case == "gaussian":
+        img, bkg, iv, psf, src, init = c1_field(seed=21, n=150, shape=(160, 160))
+        kw = dict(fixed={"fwhm": 2.5, "bkg": 0.0}, inv_var=iv, background=bkg, max_iter=20, debug=True)
+        R = 3
+    else:
+        psf = moffat_epsf()
+        img, bkg, iv, truth, init = crowded_field(256, 256, 780, seed=1012, psf=psf, dtype=np.float32)
+        kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, debug=True)
+        R = 8
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, R, model_rad="auto", **kw)
+    o = orc_fit_simultaneous(img, psf, init, R, model_rad="auto", **kw)
+    assert np.array_equal(g.debug["active"], o.debug["active"])
+    assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
+    assert len(np.unique(o.debug["model_R"])) > 1  # radii really vary with flux
+    assert_parity(g, o, min_same_frac=0.8)
