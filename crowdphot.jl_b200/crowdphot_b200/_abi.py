@@ -125,6 +125,20 @@ class SimResult(C.Structure):
     ]
 
 
+class MultipassResult(C.Structure):
+    _fields_ = [
+        ("params", _dp), ("errors", _dp),
+        ("converged", _u8p), ("valid", _u8p),
+        ("chisq", _dp),
+        ("qfit", _dp), ("qfit_expected", _dp), ("qfit_z", _dp), ("crowding", _dp),
+        ("n_iter", _i32p),
+        ("residual", _dp),
+        ("n_passes", C.c_int32), ("n_failed", C.c_int32),
+        ("n_levels", C.c_int64), ("n_fits", C.c_int64),
+        ("device_seconds", C.c_double),
+    ]
+
+
 class GroupResult(C.Structure):
     _fields_ = [
         ("y", _dp), ("x", _dp), ("flux", _dp),
@@ -260,6 +274,9 @@ PROTOTYPES = {
     "cpb_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
     "cpb_server_destroy": (C.c_int, [C.c_void_p]),
     "cpb_server_last_error": (C.c_char_p, [C.c_void_p]),
+    "cpb_fit_all_stars": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_double, C.c_int32, C.c_void_p,
+                                    C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, _dp,
+                                    C.POINTER(MultipassResult)]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
     "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,

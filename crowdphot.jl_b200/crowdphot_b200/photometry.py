@@ -880,6 +880,87 @@ def fit_star_packed(model, pixels, offsets, ny, nx, y_origin, x_origin, init, *,
     return out
 
 
+def params_matrix(psf, sources):
+    """_build_params_matrix (psf_photometry_single.jl:132-149): one row of model
+    parameters per star in getproperties order, from the catalogue where it has
+    the field and from the PSF's own value otherwise."""
+    names = _props(psf)
+    get = (lambda k: sources[k]) if isinstance(sources, dict) else (lambda k: getattr(sources, k))
+    has = (lambda k: k in sources) if isinstance(sources, dict) else (lambda k: hasattr(sources, k))
+    n = np.asarray(get("y")).size
+    cols = []
+    for k in names:
+        v = np.asarray(get(k), dtype=np.float64).ravel() if has(k) else np.full(n, float(getattr(psf, k)))
+        if v.size != n:
+            raise ArgumentError(f"source field `{k}` has {v.size} entries, expected {n}")
+        cols.append(v)
+    return np.ascontiguousarray(np.stack(cols, axis=1)) if n else np.zeros((0, len(names)))
+
+
+class MultipassOutputs:
+    """Caller-owned output arrays of one cpb_multipass_result."""
+
+    def __init__(self, n, np_, ny, nx, residual=True):
+        m = max(n, 1)
+        self.n, self.np_ = n, np_
+        self.params, self.errors = np.zeros((m, np_)), np.zeros((m, np_))
+        self.converged, self.valid = np.zeros(m, np.uint8), np.zeros(m, np.uint8)
+        self.chisq, self.qfit, self.qfit_expected, self.qfit_z, self.crowding = (np.zeros(m) for _ in range(5))
+        self.n_iter = np.zeros(m, np.int32)
+        self.residual = np.zeros((ny, nx), order="F") if residual else None
+        r = _abi.MultipassResult()
+        dp = lambda a: a.ctypes.data_as(_abi._dp)
+        r.params, r.errors = dp(self.params), dp(self.errors)
+        r.converged = self.converged.ctypes.data_as(_abi._u8p)
+        r.valid = self.valid.ctypes.data_as(_abi._u8p)
+        r.chisq, r.qfit, r.qfit_expected = dp(self.chisq), dp(self.qfit), dp(self.qfit_expected)
+        r.qfit_z, r.crowding = dp(self.qfit_z), dp(self.crowding)
+        r.n_iter = self.n_iter.ctypes.data_as(_abi._i32p)
+        if residual:
+            r.residual = dp(self.residual)
+        self.c = r
+
+    def result(self, psf, ny, nx) -> MultiPassPhotResult:
+        n, names = self.n, _props(psf)
+        col = lambda a, k: a[:n, names.index(k)].copy()
+        nan = np.full(n, np.nan)
+        r = self.c
+        return MultiPassPhotResult(
+            y=col(self.params, "y"), x=col(self.params, "x"), y_err=col(self.errors, "y"),
+            x_err=col(self.errors, "x"), flux=col(self.params, "flux"), flux_err=col(self.errors, "flux"),
+            bkg=col(self.params, "bkg"), bkg_err=col(self.errors, "bkg"),
+            converged=self.converged[:n].astype(bool), valid=self.valid[:n].astype(bool),
+            chisq=self.chisq[:n].copy(), qfit=self.qfit[:n].copy(), qfit_expected=self.qfit_expected[:n].copy(),
+            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(), spread_model=nan.copy(),
+            spread_model_err=nan.copy(), n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes),
+            n_failed=int(r.n_failed), failure_msgs=[],
+            residual=self.residual if self.residual is not None else np.zeros((ny, nx)),
+            stats=dict(n_levels=int(r.n_levels), n_fits=int(r.n_fits), device_seconds=float(r.device_seconds),
+                       params=self.params[:n].copy()))
+
+
+def fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_var=None, spread_model_fwhm=None,
+                  ctx: Context | None = None, residual=True, **kw) -> MultiPassPhotResult:
+    """CrowdPhot.fit_all_stars on the B200 (psf_photometry_single.jl:267-469): brightness-
+    ordered passes of fit_star against the running residual, each pass run as batches of
+    stars whose boxes are disjoint (the sequential result).  Keyword arguments other than
+    n_passes / fixed / inv_var go to fit_star (max_iter, x_tol, f_tol, g_tol, damping, ...).
+    spread_model is not computed (NaN)."""
+    fixed = dict(fixed or {})
+    ctx = ctx or get_context()
+    imgf, ivf, _, et = _image_arrays(image, inv_var, None)
+    init = params_matrix(psf, sources)
+    P = lm_params(psf, fixed, **kw)
+    ny, nx = imgf.shape
+    outs = MultipassOutputs(init.shape[0], init.shape[1], ny, nx, residual=residual)
+    vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    rc = ctx.lib.cpb_fit_all_stars(ctx.handle, ctx.psf_handle(psf), C.byref(P), float(fit_rad), int(n_passes),
+                                   vp(imgf), et, ny, nx, vp(ivf), init.shape[0], init.ctypes.data_as(_abi._dp),
+                                   C.byref(outs.c))
+    ctx.raise_for(rc, "cpb_fit_all_stars")
+    return outs.result(psf, ny, nx)
+
+
 def fit_star(model, image, inds=None, *, fixed=None, inv_var=None, ctx: Context | None = None, **kw):
     """CrowdPhot.PSF.fit_star on the B200 (psf_fitting.jl:229-308) -> (best_model, LMResult).
 

@@ -452,6 +452,11 @@ int64_t group_batch_size(const GroupBatch* b);
 std::string group_batch_signature(const GroupBatch* b, int bucket);
 void group_batch_destroy(GroupBatch* b);
 
+// fit_all_stars (cpb_multipass.cu): device image / weights, host catalogue and outputs.
+int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, double fit_rad, int n_passes,
+                      const void* d_img, int32_t eltype, int64_t ny, int64_t nx, const void* d_iv, int64_t n,
+                      const double* init, cpb_multipass_result* out);
+
 // Batched LM driver (cpb_lm.cu).  Host inputs.
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cutouts,
                  const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,

@@ -1,0 +1,451 @@
+// cpb_multipass.cu -- CrowdPhot.fit_all_stars (sequential multi-pass photometry).
+//
+// Restates src/photometry/psf_photometry_single.jl:267-469.  Each pass visits
+// the valid stars brightest first; a star is added back into the running
+// residual image (passes 2+), fitted with fit_star on its +-fit_rad box and
+// subtracted with its new model.  The only coupling between two stars of a
+// pass is the pixels their boxes share, and the boxes are fixed when the pass
+// starts (a star's box comes from its parameters before it is refitted), so
+// the visit order is replaced by batches: star s goes into batch
+// 1 + max{batch(t) : t earlier than s and box(t) meets box(s)}.  Stars of one
+// batch have pairwise disjoint boxes, every star they depend on is in an
+// earlier batch, and each pixel sees its adds and subtracts in the reference's
+// order -- so the result is the sequential one, while each batch is one
+// add-back launch, one cutout gather, one batched LM launch (the fit_star
+// kernel of cpb_lm.cu) and one subtract launch.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <unordered_map>
+#include <vector>
+
+#include "cpb_internal.cuh"
+
+namespace cpb {
+namespace {
+
+struct MPConst {
+    int np;           // model parameters per star (4 image PSFs, 5 Gaussian)
+    int gauss;
+    int ry, rx, rf, rb, rw;  // rows of y, x, flux, bkg, fwhm (-1: none)
+};
+
+// The star's model at pixel (i, j) from its parameter row.
+__device__ __forceinline__ double mp_model(const DevPsf& P, const MPConst& M, const double* pr, int i, int j) {
+    StarCoef c;
+    c.y = pr[M.ry];
+    c.x = pr[M.rx];
+    c.flux = pr[M.rf];
+    c.bkg = pr[M.rb];
+    if (M.gauss) {
+        DevPsf Pj = P;
+        Pj.fwhm = pr[M.rw];
+        double a, b, e;
+        return gauss_eval<double, false>(Pj.fwhm, c, (double)i, (double)j, a, b, e);
+    }
+    grid_corners_dw(P, c.y, c.x, c);
+    return model_value<double, double>(P, P.data64, c, (double)i, (double)j);
+}
+
+// add_star! / subtract_star! (PSF.jl:420-447) over each star's box: one warp a
+// star, lanes over the box pixels.  flags (nullable): stars with 0 are skipped.
+__global__ void k_mp_addsub(int nL, const int4* __restrict__ boxes, const double* __restrict__ params,
+                            const uint8_t* __restrict__ flags, double sign, DevPsf P, MPConst M, double* residual,
+                            int ny) {
+    const int lane = threadIdx.x & 31;
+    const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (s >= nL || (flags && !flags[s])) return;
+    const int4 b = boxes[s];  // y1, x1, box rows, box columns
+    const double* pr = params + (int64_t)s * M.np;
+    for (int e = lane; e < b.z * b.w; e += 32) {
+        const int i = b.x + e % b.z, j = b.y + e / b.z;
+        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
+        residual[q] = residual[q] + sign * mp_model(P, M, pr, i, j);
+    }
+}
+
+template <typename TI>
+__global__ void k_mp_cutouts(int nL, const int4* __restrict__ boxes, const int64_t* __restrict__ offs,
+                             const double* __restrict__ residual, const TI* __restrict__ iv, int ny,
+                             double* __restrict__ pix, double* __restrict__ ivc) {
+    const int lane = threadIdx.x & 31;
+    const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (s >= nL) return;
+    const int4 b = boxes[s];
+    const int64_t o = offs[s];
+    for (int e = lane; e < b.z * b.w; e += 32) {
+        const int i = b.x + e % b.z, j = b.y + e / b.z;
+        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
+        pix[o + e] = residual[q];
+        if (iv) ivc[o + e] = (double)iv[q];
+    }
+}
+
+// _star_diagnostics! (psf_photometry_diagnostics.jl:154-231) over the fitted
+// box: image is the original data, residual the star's fit residual (every
+// model subtracted, its own included), star_model its best-fit render.
+// out: qfit, qfit_expected, qfit_z, crowding per star (NaN where undefined).
+template <typename TI>
+__global__ void k_mp_diag(int nL, const int4* __restrict__ boxes, const double* __restrict__ params,
+                          const uint8_t* __restrict__ flags, const TI* __restrict__ img,
+                          const double* __restrict__ residual, const TI* __restrict__ iv, DevPsf P, MPConst M,
+                          int n_free, int ny, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (s >= nL) return;
+    const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+    double* o = out + (int64_t)s * 4;
+    const double* pr = params + (int64_t)s * M.np;
+    const double flux = pr[M.rf], bkg = pr[M.rb];
+    if (!flags[s] || !(flux > 0)) {
+        if (lane == 0) o[0] = o[1] = o[2] = o[3] = NaN;
+        return;
+    }
+    const int4 b = boxes[s];
+    const double inv_flux = 1.0 / flux;
+    double qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
+    int ngood = 0;
+    for (int e = lane; e < b.z * b.w; e += 32) {
+        const int i = b.x + e % b.z, j = b.y + e / b.z;
+        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
+        const double mv = mp_model(P, M, pr, i, j);
+        const double wp = iv ? (double)iv[q] : 1.0;
+        if (isfinite(wp) && wp > 0) {
+            const double r = residual[q];
+            qv += fabs(r);
+            const double Pp = (mv - bkg) * inv_flux;
+            const double wP = wp * Pp;
+            ncl += wP * (r + mv - bkg);
+            ndi += wP * ((double)img[q] - bkg);
+            den += wP * Pp;
+        }
+        if (iv) {
+            const double v = (double)iv[q];
+            if (isfinite(v) && v > 0) {
+                const double si = 1.0 / sqrt(v);
+                ss += si;
+                ss2 += si * si;
+                ngood += 1;
+            }
+        }
+    }
+    qv = warp_sum(qv);
+    ncl = warp_sum(ncl);
+    ndi = warp_sum(ndi);
+    den = warp_sum(den);
+    ss = warp_sum(ss);
+    ss2 = warp_sum(ss2);
+    ngood = warp_sum(ngood);
+    if (lane == 0) {
+        const double c2p = 0.7978845608028654;  // sqrt(2 / pi)
+        o[0] = qv * inv_flux;
+        o[3] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
+        o[1] = iv ? c2p * ss * inv_flux : NaN;
+        o[2] = NaN;
+        if (iv && ss2 > 0 && ngood > n_free) {
+            const double dfac = sqrt(1.0 - (double)n_free / (double)ngood);
+            o[2] = (qv - c2p * dfac * ss) / (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
+        }
+    }
+}
+
+template <typename TI>
+__global__ void k_mp_init(int64_t npix, const TI* __restrict__ img, double* __restrict__ residual) {
+    const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (q < npix) residual[q] = (double)img[q];
+}
+
+inline unsigned warps_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256); }
+
+}  // namespace
+
+int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, double fit_rad, int n_passes,
+                      const void* d_img, int32_t eltype, int64_t ny64, int64_t nx64, const void* d_iv, int64_t n,
+                      const double* init, cpb_multipass_result* out) {
+    if (!(n_passes > 0)) throw ArgError{"n_passes must be positive, got " + std::to_string(n_passes)};
+    if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
+    if (ny64 <= 0 || nx64 <= 0 || ny64 * nx64 >= (1LL << 31)) throw ArgError{"image size out of range"};
+    if (P->precision != CPB_PREC_FP64) throw ArgError{"only the FP64 precision form is built for fit_all_stars"};
+    if (!out->params || !out->errors || !out->converged || !out->valid || !out->chisq || !out->n_iter)
+        throw ArgError{"null output array"};
+    const int ny = (int)ny64, nx = (int)nx64;
+    const int64_t npix = ny64 * nx64;
+    cudaStream_t st = ctx->stream;
+    const DevPsf dp = psf->dev;
+    MPConst M{};
+    M.gauss = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 1 : 0;
+    M.np = M.gauss ? 5 : 4;
+    M.ry = 0;
+    M.rx = 1;
+    M.rw = M.gauss ? 2 : -1;
+    M.rf = M.gauss ? 3 : 2;
+    M.rb = M.gauss ? 4 : 3;
+    // free set in getproperties order (psf_fitting.jl:8-26)
+    const int bits_g[5] = {CPB_FREE_Y, CPB_FREE_X, CPB_FREE_FWHM, CPB_FREE_FLUX, CPB_FREE_BKG};
+    const int bits_i[4] = {CPB_FREE_Y, CPB_FREE_X, CPB_FREE_FLUX, CPB_FREE_BKG};
+    std::vector<int> free_idx;
+    for (int q = 0; q < M.np; ++q)
+        if (P->free_mask & (M.gauss ? bits_g[q] : bits_i[q])) free_idx.push_back(q);
+    if (free_idx.empty()) throw ArgError{"all model parameters are fixed; nothing to fit"};
+    const int nf = (int)free_idx.size();
+    const int np = M.np;
+    const double NaN = std::numeric_limits<double>::quiet_NaN();
+
+    out->n_passes = n_passes;
+    out->n_failed = 0;
+    out->n_levels = 0;
+    out->n_fits = 0;
+    out->device_seconds = 0;
+    // per-star state (host): parameters, errors, flags (:282-323)
+    std::vector<double> prm(init, init + n * np), err(n * np, NaN);
+    for (int64_t s = 0; s < n; ++s)
+        for (int q = 0; q < np; ++q)
+            if (std::find(free_idx.begin(), free_idx.end(), q) == free_idx.end()) err[s * np + q] = 0.0;
+    std::vector<uint8_t> valid(n, 1), conv(n, 0);
+    std::vector<double> chisq(n, 0.0), diag(n * 4, NaN);
+    std::vector<int32_t> niter(n, 0);
+    if (n == 0) {
+        if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
+        return 0;
+    }
+
+    double* resid = (double*)scratch(ctx, "mp_residual", sizeof(double) * npix);
+    check(cudaEventRecord(ctx->ev0, st), "event");
+    if (eltype == CPB_F64)
+        k_mp_init<double><<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(npix, (const double*)d_img, resid);
+    else
+        k_mp_init<float><<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(npix, (const float*)d_img, resid);
+    check(cudaGetLastError(), "k_mp_init");
+    double dev_s = 0;
+
+    // batch buffers, sized for all stars at once (a batch never exceeds n)
+    const int Rmax = (int)std::ceil(std::max(fit_rad, 0.0)) + 1;
+    const int64_t box_max = (int64_t)(2 * Rmax + 1) * (2 * Rmax + 1);
+    int4* d_box = (int4*)scratch(ctx, "mp_box", sizeof(int4) * n);
+    double* d_pin = (double*)scratch(ctx, "mp_pin", sizeof(double) * n * np);
+    double* d_psub = (double*)scratch(ctx, "mp_psub", sizeof(double) * n * np);
+    uint8_t* d_flag = (uint8_t*)scratch(ctx, "mp_flag", n);
+    int64_t* d_off = (int64_t*)scratch(ctx, "mp_off", sizeof(int64_t) * n);
+    int32_t* d_dims = (int32_t*)scratch(ctx, "mp_dims", sizeof(int32_t) * n * 4);  // ny, nx, y1, x1
+    double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * n * box_max);
+    double* d_civ = d_iv ? (double*)scratch(ctx, "mp_civ", sizeof(double) * n * box_max) : nullptr;
+    double* d_lmd = (double*)scratch(ctx, "mp_lm_f64", sizeof(double) * n * (np + nf * nf + 4));
+    uint8_t* d_lmu = (uint8_t*)scratch(ctx, "mp_lm_u8", (size_t)n * 4);
+    int32_t* d_lmi = (int32_t*)scratch(ctx, "mp_lm_i32", sizeof(int32_t) * n * 2);
+    double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 4);
+
+    // host staging of one batch
+    std::vector<int4> hbox;
+    std::vector<double> hpin, hpsub, hlm;
+    std::vector<uint8_t> hflag, hlmu;
+    std::vector<int64_t> hoff;
+    std::vector<int32_t> hdims, hlmi;
+    std::vector<double> hdiag;
+    const double FTfit = fit_rad;
+
+    for (int pass = 1; pass <= n_passes; ++pass) {
+        // brightest first, stable (sortperm(rev = true))
+        std::vector<int64_t> order(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int64_t a, int64_t b) { return prm[a * np + M.rf] > prm[b * np + M.rf]; });
+        // boxes at the pass start and the batch of every valid star
+        std::vector<int4> box(n);
+        std::vector<int> level(n, -1);
+        int nlev = 0;
+        {
+            const int cell = 2 * Rmax + 2;
+            const int gnx = nx / cell + 2;
+            std::unordered_map<int64_t, std::vector<int64_t>> grid;
+            for (int64_t s : order) {
+                if (!valid[s]) continue;
+                const double y = prm[s * np + M.ry], x = prm[s * np + M.rx];
+                if (!(std::isfinite(y) && std::isfinite(x))) {
+                    valid[s] = 0;
+                    continue;
+                }
+                int ylo = (int)std::max(std::floor(y - FTfit), 1.0), yhi = (int)std::min(std::ceil(y + FTfit), (double)ny);
+                int xlo = (int)std::max(std::floor(x - FTfit), 1.0), xhi = (int)std::min(std::ceil(x + FTfit), (double)nx);
+                const int64_t by = std::max(yhi - ylo + 1, 0), bx = std::max(xhi - xlo + 1, 0);
+                if (by * bx < 3) {  // :343-348
+                    valid[s] = 0;
+                    continue;
+                }
+                box[s] = make_int4(ylo, xlo, (int)by, (int)bx);
+                int lv = 0;
+                const int cy0 = (ylo - 1) / cell, cy1 = (yhi - 1) / cell, cx0 = (xlo - 1) / cell, cx1 = (xhi - 1) / cell;
+                for (int cx = cx0; cx <= cx1; ++cx)
+                    for (int cy = cy0; cy <= cy1; ++cy) {
+                        auto it = grid.find((int64_t)cy * gnx + cx);
+                        if (it == grid.end()) continue;
+                        for (int64_t t : it->second) {
+                            const int4& bt = box[t];
+                            if (bt.x <= yhi && ylo <= bt.x + bt.z - 1 && bt.y <= xhi && xlo <= bt.y + bt.w - 1)
+                                lv = std::max(lv, level[t] + 1);
+                        }
+                    }
+                level[s] = lv;
+                nlev = std::max(nlev, lv + 1);
+                for (int cx = cx0; cx <= cx1; ++cx)
+                    for (int cy = cy0; cy <= cy1; ++cy) grid[(int64_t)cy * gnx + cx].push_back(s);
+            }
+        }
+        std::vector<std::vector<int64_t>> batches(nlev);
+        for (int64_t s : order)
+            if (valid[s] && level[s] >= 0) batches[level[s]].push_back(s);
+        out->n_levels += nlev;
+
+        for (int L = 0; L < nlev; ++L) {
+            const std::vector<int64_t>& B = batches[L];
+            const int nL = (int)B.size();
+            if (nL == 0) continue;
+            hbox.resize(nL);
+            hpin.resize((size_t)nL * np);
+            hoff.resize(nL);
+            hdims.resize((size_t)nL * 4);
+            int64_t tot = 0;
+            for (int k = 0; k < nL; ++k) {
+                const int64_t s = B[k];
+                hbox[k] = box[s];
+                std::memcpy(&hpin[(size_t)k * np], &prm[s * np], sizeof(double) * np);
+                hoff[k] = tot;
+                tot += (int64_t)box[s].z * box[s].w;
+                hdims[k] = box[s].z;
+                hdims[nL + k] = box[s].w;
+                hdims[2 * nL + k] = box[s].x;
+                hdims[3 * nL + k] = box[s].y;
+            }
+            check(cudaMemcpyAsync(d_box, hbox.data(), sizeof(int4) * nL, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_pin, hpin.data(), sizeof(double) * nL * np, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_off, hoff.data(), sizeof(int64_t) * nL, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_dims, hdims.data(), sizeof(int32_t) * nL * 4, cudaMemcpyHostToDevice, st), "h2d");
+            // passes 2+: the star's previous model goes back in (:360-365)
+            if (pass > 1) {
+                KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
+                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_pin, nullptr, 1.0, dp, M, resid, ny);
+                check(cudaGetLastError(), "k_mp_addsub");
+            }
+            {
+                KernelScope ks_(ctx, "k_mp_cutouts", (double)tot * (d_iv ? 32 : 16));
+                if (eltype == CPB_F64)
+                    k_mp_cutouts<double><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_off, resid, (const double*)d_iv,
+                                                                       ny, d_cpix, d_civ);
+                else
+                    k_mp_cutouts<float><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_off, resid, (const float*)d_iv,
+                                                                      ny, d_cpix, d_civ);
+                check(cudaGetLastError(), "k_mp_cutouts");
+            }
+            // fit_star on every box of the batch (:367-371): the fit_star kernel
+            cpb_lm_result r{};
+            r.params = d_lmd;
+            r.cov = d_lmd + (size_t)nL * np;
+            double* sc = d_lmd + (size_t)nL * (np + nf * nf);
+            r.cost = sc;
+            r.cost_init = sc + nL;
+            r.chisq = sc + 2 * nL;
+            r.lambda_final = sc + 3 * nL;
+            r.converged = d_lmu;
+            r.x_converged = d_lmu + nL;
+            r.f_converged = d_lmu + 2 * nL;
+            r.g_converged = d_lmu + 3 * nL;
+            r.iterations = d_lmi;
+            r.status = d_lmi + nL;
+            fit_lm_batch_device(ctx, psf, P, nL, d_off, d_dims, d_dims + nL, d_dims + 2 * nL, d_dims + 3 * nL, d_cpix,
+                                CPB_F64, d_civ, d_pin, tot, &r);
+            dev_s += r.device_seconds;
+            out->n_fits += nL;
+            hlm.resize((size_t)nL * (np + nf * nf + 4));
+            hlmu.resize((size_t)nL * 4);
+            hlmi.resize((size_t)nL * 2);
+            check(cudaMemcpyAsync(hlm.data(), d_lmd, sizeof(double) * hlm.size(), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaMemcpyAsync(hlmu.data(), d_lmu, hlmu.size(), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaMemcpyAsync(hlmi.data(), d_lmi, sizeof(int32_t) * hlmi.size(), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaStreamSynchronize(st), "sync");
+            // bookkeeping (:373-390) and what to subtract: the new model, or on a
+            // failed fit of pass 2+ the previous one again (undoing the add-back)
+            hpsub.resize((size_t)nL * np);
+            hflag.assign(nL, 0);
+            const double* hcov = hlm.data() + (size_t)nL * np;
+            const double* hsc = hlm.data() + (size_t)nL * (np + nf * nf);
+            for (int k = 0; k < nL; ++k) {
+                const int64_t s = B[k];
+                if (hlmi[nL + k] != 0) {  // fit_star threw (:391-401)
+                    valid[s] = 0;
+                    out->n_failed += 1;
+                    if (pass > 1) {
+                        std::memcpy(&hpsub[(size_t)k * np], &prm[s * np], sizeof(double) * np);
+                        hflag[k] = 1;
+                    }
+                    continue;
+                }
+                std::memcpy(&prm[s * np], &hlm[(size_t)k * np], sizeof(double) * np);
+                for (int a = 0; a < nf; ++a) {
+                    const double cv = hcov[(size_t)k * nf * nf + a + a * nf];
+                    err[s * np + free_idx[a]] = std::sqrt(std::max(0.0, cv));
+                }
+                conv[s] = hlmu[k];
+                chisq[s] = hsc[2 * nL + k];
+                niter[s] += hlmi[k];
+                std::memcpy(&hpsub[(size_t)k * np], &hlm[(size_t)k * np], sizeof(double) * np);
+                hflag[k] = 2;  // fitted
+            }
+            std::vector<uint8_t> sub_on(nL);
+            for (int k = 0; k < nL; ++k) sub_on[k] = hflag[k] != 0;
+            check(cudaMemcpyAsync(d_psub, hpsub.data(), sizeof(double) * nL * np, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
+            {
+                KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
+                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, -1.0, dp, M, resid, ny);
+                check(cudaGetLastError(), "k_mp_addsub");
+            }
+            if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389)
+                for (int k = 0; k < nL; ++k) sub_on[k] = hflag[k] == 2;
+                check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
+                KernelScope ks_(ctx, "k_mp_diag", (double)tot * (d_iv ? 24 : 16));
+                if (eltype == CPB_F64)
+                    k_mp_diag<double><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, (const double*)d_img,
+                                                                    resid, (const double*)d_iv, dp, M, nf, ny, d_diag);
+                else
+                    k_mp_diag<float><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, (const float*)d_img,
+                                                                   resid, (const float*)d_iv, dp, M, nf, ny, d_diag);
+                check(cudaGetLastError(), "k_mp_diag");
+                hdiag.resize((size_t)nL * 4);
+                check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * nL * 4, cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaStreamSynchronize(st), "sync");
+                for (int k = 0; k < nL; ++k)
+                    if (hflag[k] == 2)
+                        for (int t = 0; t < 4; ++t) diag[B[k] * 4 + t] = hdiag[(size_t)k * 4 + t];
+            }
+        }
+        // between-pass validation (:404-412)
+        for (int64_t s = 0; s < n; ++s) {
+            const double y = prm[s * np + M.ry], x = prm[s * np + M.rx], f = prm[s * np + M.rf];
+            valid[s] = valid[s] && conv[s] && std::isfinite(y) && std::isfinite(x) && std::isfinite(f) && f > 0;
+        }
+    }
+    check(cudaEventRecord(ctx->ev1, st), "event");
+    if (out->residual)
+        check(cudaMemcpyAsync(out->residual, resid, sizeof(double) * npix, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    out->device_seconds = ms * 1e-3;
+    (void)dev_s;
+    std::memcpy(out->params, prm.data(), sizeof(double) * n * np);
+    std::memcpy(out->errors, err.data(), sizeof(double) * n * np);
+    for (int64_t s = 0; s < n; ++s) {
+        out->converged[s] = conv[s];
+        out->valid[s] = valid[s];
+        out->chisq[s] = chisq[s];
+        out->n_iter[s] = niter[s];
+        if (out->qfit) out->qfit[s] = diag[s * 4];
+        if (out->qfit_expected) out->qfit_expected[s] = diag[s * 4 + 1];
+        if (out->qfit_z) out->qfit_z[s] = diag[s * 4 + 2];
+        if (out->crowding) out->crowding[s] = diag[s * 4 + 3];
+    }
+    return 0;
+}
+
+}  // namespace cpb

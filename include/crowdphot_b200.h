@@ -286,6 +286,47 @@ CPB_API int cpb_fit_simultaneous_device_noalloc(cpb_ctx* ctx, const cpb_psf* psf
                                                 const double* d_y0, const double* d_x0, const double* d_flux0,
                                                 cpb_sim_result* out);
 
+/* ---- sequential multi-pass photometry (fit_all_stars) ------------------- */
+/*
+ * Result of fit_all_stars (MultiPassPhotResult, psf_photometry_single.jl:99-122)
+ * with the models' parameters in getproperties order (np per star: y, x, flux,
+ * bkg for image PSFs; y, x, fwhm, flux, bkg for CircularGaussianPSF).
+ * Arrays are caller-allocated host memory; NULL skips an optional one.
+ */
+typedef struct cpb_multipass_result {
+    double* params;            /* n*np fitted parameters (fixed ones as given) */
+    double* errors;            /* n*np (0 for fixed parameters, NaN before a star's first fit) */
+    uint8_t *converged, *valid;
+    double* chisq;
+    double *qfit, *qfit_expected, *qfit_z, *crowding; /* optional */
+    int32_t* n_iter;           /* LM iterations summed over the passes */
+    double* residual;          /* optional, ny*nx: the data with every valid star's model subtracted */
+    int32_t n_passes;
+    int32_t n_failed;          /* fits that failed the reference's input checks */
+    int64_t n_levels;          /* batches run (summed over the passes) */
+    int64_t n_fits;            /* fit_star calls run */
+    double device_seconds;
+} cpb_multipass_result;
+
+/*
+ * CrowdPhot.fit_all_stars (psf_photometry_single.jl:267-469): n_passes
+ * brightness-ordered passes; each valid star is added back (passes 2+),
+ * fitted with fit_star on its +-fit_rad box of the running residual image and
+ * subtracted again.  Two stars depend on each other only through pixels their
+ * boxes share, and each pass fixes every box at its start, so the pass is run
+ * as a sequence of batches: a star's batch is one more than the latest batch
+ * of any earlier (brighter) star whose box overlaps its own, and the stars of
+ * one batch -- pairwise disjoint -- are fitted together in one launch.  The
+ * result equals the one-star-at-a-time order of the reference.  image: ny*nx
+ * of eltype (background-subtracted); inv_var nullable; init: n*np initial
+ * parameters (the catalogue, with the PSF's own values for parameters the
+ * catalogue lacks).  LM keyword arguments as cpb_fit_lm_batch.  Host arrays.
+ * spread_model is not computed.
+ */
+CPB_API int cpb_fit_all_stars(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, double fit_rad,
+                              int32_t n_passes, const void* image, int32_t eltype, int64_t ny, int64_t nx,
+                              const void* inv_var, int64_t n, const double* init, cpb_multipass_result* out);
+
 /* ---- many small simultaneous fits (star groups) ------------------------- */
 /*
  * Results of a batch of independent fit_all_stars_simultaneous calls, one

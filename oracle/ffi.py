@@ -73,6 +73,10 @@ def load():
         lib.orc_model_radii_auto.restype = C.c_int
         lib.orc_model_radii_auto.argtypes = [C.POINTER(_abi.PsfDesc), C.c_double, C.c_double, C.c_int, C.c_int,
                                              C.c_int64, _dp, C.c_int64, _dp, _i32p]
+        lib.orc_fit_all_stars.restype = C.c_int
+        lib.orc_fit_all_stars.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_double, C.c_int,
+                                          C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, _dp,
+                                          C.POINTER(_abi.MultipassResult), C.c_char_p, C.c_int]
         lib.orc_fit_star_batch.restype = C.c_int
         lib.orc_fit_star_batch.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_int64, _i64p,
                                            _i32p, _i32p, _i32p, _i32p, _dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp,
@@ -347,3 +351,26 @@ def orc_fit_star_packed(model, pix, offsets, ny, nx, y1, x1, init, *, inv_var=No
                converged=fl[:, 0].copy(), x_converged=fl[:, 1].copy(), f_converged=fl[:, 2].copy(),
                g_converged=fl[:, 3].copy(), names=names)
     return out, used
+
+
+def orc_fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_var=None, residual=True, **kw):
+    """The oracle's fit_all_stars (same call shape as the product's)."""
+    from crowdphot_b200.photometry import MultipassOutputs, params_matrix
+    lib = load()
+    fixed = dict(fixed or {})
+    kw.pop("ctx", None)
+    kw.pop("spread_model_fwhm", None)
+    imgf, ivf, _, et = _image_arrays(image, inv_var, None)
+    init = params_matrix(psf, sources)
+    P = lm_params(psf, fixed, **kw)
+    ny, nx = imgf.shape
+    outs = MultipassOutputs(init.shape[0], init.shape[1], ny, nx, residual=residual)
+    desc, keep = psf_descriptor(psf)
+    err = C.create_string_buffer(1024)
+    vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+    rc = lib.orc_fit_all_stars(C.byref(desc), C.byref(P), float(fit_rad), int(n_passes), vp(imgf), et, ny, nx, vp(ivf),
+                               init.shape[0], init.ctypes.data_as(_dp), C.byref(outs.c), err, 1024)
+    del keep
+    if rc != 0:
+        raise ArgumentError(err.value.decode())
+    return outs.result(psf, ny, nx)

@@ -347,3 +347,14 @@ int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const dou
 }
 
 }  // namespace
+
+namespace orc {
+// fit_one for the other oracle files (fit_all_stars calls fit_star per star).
+int fit_star_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const double* inv_var, int32_t ny,
+                 int32_t nx, int32_t y1, int32_t x1, const double* init, double* out_params, double* cov_out,
+                 double* cost_out, double* cost_init_out, double* chisq_out, double* lambda_out, uint8_t* flags_out,
+                 int32_t* iters_out) {
+    return fit_one(psf, P, pix, inv_var, ny, nx, y1, x1, init, out_params, cov_out, cost_out, cost_init_out,
+                   chisq_out, lambda_out, flags_out, iters_out, nullptr, 0);
+}
+}  // namespace orc
