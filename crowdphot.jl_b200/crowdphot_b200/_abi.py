@@ -98,6 +98,7 @@ class SimParams(C.Structure):
         ("solver", C.c_int32),
         ("damping", C.c_int32),
         ("reserved", C.c_int32),
+        ("spread_model_fwhm", C.c_double),
     ]
 
 
@@ -122,6 +123,7 @@ class SimResult(C.Structure):
         ("model_px_evals", C.c_double),
         ("lsqr_px_macs", C.c_double),
         ("device_seconds", C.c_double),
+        ("spread_model", _dp), ("spread_model_err", _dp),
     ]
 
 
@@ -136,6 +138,7 @@ class MultipassResult(C.Structure):
         ("n_passes", C.c_int32), ("n_failed", C.c_int32),
         ("n_levels", C.c_int64), ("n_fits", C.c_int64),
         ("device_seconds", C.c_double),
+        ("spread_model", _dp), ("spread_model_err", _dp),
     ]
 
 
@@ -274,9 +277,11 @@ PROTOTYPES = {
     "cpb_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
     "cpb_server_destroy": (C.c_int, [C.c_void_p]),
     "cpb_server_last_error": (C.c_char_p, [C.c_void_p]),
-    "cpb_fit_all_stars": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_double, C.c_int32, C.c_void_p,
+    "cpb_fit_all_stars": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_double, C.c_int32,
+                                    C.c_double, C.c_void_p,
                                     C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, _dp,
                                     C.POINTER(MultipassResult)]),
+    "cpb_exp_disk_kernel": (C.c_int, [C.c_double, C.c_int32, _dp]),
     "cpb_fit_lm_batch": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, _i64p, _i32p, _i32p,
                                    _i32p, _i32p, C.c_void_p, C.c_int32, C.c_void_p, _dp, C.POINTER(LMResultC)]),
     "cpb_fit_lm_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LMParams), C.c_int64, C.c_void_p,

@@ -15,7 +15,9 @@ Differences from the Julia API, all deliberate:
   * ``solver=:lsmr``, IRLS ``reweight`` and PSF types other than
     CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF} raise
     ArgumentError -- there is no CPU fallback;
-  * ``spread_model`` / ``spread_model_err`` are NaN.
+  * the batched group entry points (``fit_all_stars_simultaneous_batch``,
+    ``fit_groups_packed``, ``BatchGraph``, ``Server``) leave ``spread_model`` /
+    ``spread_model_err`` NaN; the single-field entry points compute them.
 """
 from __future__ import annotations
 
@@ -272,9 +274,10 @@ def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_itera
                model_rad="auto", model_rad_max=None, model_rad_nsigma=1.0, max_step=0.25, max_trials=8, max_iter=40,
                x_tol=1.0e-5, f_tol=1.0e-4, g_tol=1.0e-4, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0,
                lambda_min=1.0e-12, lambda_max=1.0e12, damping="marquardt", covariance_estimator=None,
-               precision="fp64"):
+               precision="fp64", spread_model_fwhm=None):
     """Keyword arguments -> cpb_sim_params (shared by the device path and the oracle)."""
     P = _abi.SimParams()
+    P.spread_model_fwhm = spread_fwhm_arg(spread_model_fwhm)
     P.fit_rad = float(fit_rad)
     P.free_mask = _free_mask(psf, fixed)
     P.inner_iterations = int(inner_iterations)
@@ -309,6 +312,16 @@ def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_itera
     return P
 
 
+def spread_fwhm_arg(v):
+    """spread_model_fwhm keyword -> the C-ABI double: nothing (None) -> NaN, the
+    PSF-derived width; a non-finite or non-positive value -> 0, no spread_model
+    (the reference skips the reference disk when the width is not finite and > 0)."""
+    if v is None:
+        return float("nan")
+    v = float(v)
+    return v if np.isfinite(v) and v > 0 else 0.0
+
+
 class SimOutputs:
     """Caller-owned output arrays for one cpb_sim_result."""
 
@@ -318,6 +331,7 @@ class SimOutputs:
         self.y, self.x, self.flux, self.bkg = z(), z(), z(), z()
         self.y_err, self.x_err, self.flux_err, self.bkg_err = z(), z(), z(), z()
         self.chisq, self.qfit, self.qfit_expected, self.qfit_z, self.crowding = z(), z(), z(), z(), z()
+        self.spread_model, self.spread_model_err = z(), z()
         self.converged = np.zeros(max(n, 1), dtype=np.uint8)
         self.valid = np.zeros(max(n, 1), dtype=np.uint8)
         self.n_iter = np.zeros(max(n, 1), dtype=np.int32)
@@ -335,6 +349,7 @@ class SimOutputs:
         r.valid = self.valid.ctypes.data_as(_abi._u8p)
         r.chisq, r.qfit, r.qfit_expected = dp(self.chisq), dp(self.qfit), dp(self.qfit_expected)
         r.qfit_z, r.crowding = dp(self.qfit_z), dp(self.crowding)
+        r.spread_model, r.spread_model_err = dp(self.spread_model), dp(self.spread_model_err)
         r.n_iter = self.n_iter.ctypes.data_as(_abi._i32p)
         if residual:
             r.residual = dp(self.residual)
@@ -352,14 +367,14 @@ class SimOutputs:
                 for i in range(n) if not valid[i] and r.n_active < n]
         if r.n_active == n:
             msgs = []
-        nan = np.full(n, np.nan)
         res = MultiPassPhotResult(
             y=self.y[:n].copy(), x=self.x[:n].copy(), y_err=self.y_err[:n].copy(), x_err=self.x_err[:n].copy(),
             flux=self.flux[:n].copy(), flux_err=self.flux_err[:n].copy(), bkg=self.bkg[:n].copy(),
             bkg_err=self.bkg_err[:n].copy(), converged=self.converged[:n].astype(bool), valid=valid,
             chisq=self.chisq[:n].copy(), qfit=self.qfit[:n].copy(), qfit_expected=self.qfit_expected[:n].copy(),
-            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(), spread_model=nan.copy(),
-            spread_model_err=nan.copy(), n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes),
+            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(),
+            spread_model=self.spread_model[:n].copy(), spread_model_err=self.spread_model_err[:n].copy(),
+            n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes),
             n_failed=int(r.n_failed), failure_msgs=msgs,
             residual=self.residual if self.residual is not None else np.zeros((ny, nx)),
             stats=dict(n_active=int(r.n_active), n_union=int(r.n_union), n_trials=int(r.n_trials),
@@ -392,7 +407,7 @@ def fit_all_stars_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_
                    max_trials=max_trials, max_iter=max_iter, x_tol=x_tol, f_tol=f_tol, g_tol=g_tol,
                    lambda_init=lambda_init, lambda_up=lambda_up, lambda_down=lambda_down, lambda_min=lambda_min,
                    lambda_max=lambda_max, damping=damping, covariance_estimator=covariance_estimator,
-                   precision=precision)
+                   precision=precision, spread_model_fwhm=spread_model_fwhm)
     ny, nx = imgf.shape
     R = int(np.ceil(fit_rad)) if fit_rad > 0 else 0
     S2 = (2 * R + 1) ** 2
@@ -906,6 +921,7 @@ class MultipassOutputs:
         self.params, self.errors = np.zeros((m, np_)), np.zeros((m, np_))
         self.converged, self.valid = np.zeros(m, np.uint8), np.zeros(m, np.uint8)
         self.chisq, self.qfit, self.qfit_expected, self.qfit_z, self.crowding = (np.zeros(m) for _ in range(5))
+        self.spread_model, self.spread_model_err = np.zeros(m), np.zeros(m)
         self.n_iter = np.zeros(m, np.int32)
         self.residual = np.zeros((ny, nx), order="F") if residual else None
         r = _abi.MultipassResult()
@@ -915,6 +931,7 @@ class MultipassOutputs:
         r.valid = self.valid.ctypes.data_as(_abi._u8p)
         r.chisq, r.qfit, r.qfit_expected = dp(self.chisq), dp(self.qfit), dp(self.qfit_expected)
         r.qfit_z, r.crowding = dp(self.qfit_z), dp(self.crowding)
+        r.spread_model, r.spread_model_err = dp(self.spread_model), dp(self.spread_model_err)
         r.n_iter = self.n_iter.ctypes.data_as(_abi._i32p)
         if residual:
             r.residual = dp(self.residual)
@@ -923,7 +940,6 @@ class MultipassOutputs:
     def result(self, psf, ny, nx) -> MultiPassPhotResult:
         n, names = self.n, _props(psf)
         col = lambda a, k: a[:n, names.index(k)].copy()
-        nan = np.full(n, np.nan)
         r = self.c
         return MultiPassPhotResult(
             y=col(self.params, "y"), x=col(self.params, "x"), y_err=col(self.errors, "y"),
@@ -931,9 +947,10 @@ class MultipassOutputs:
             bkg=col(self.params, "bkg"), bkg_err=col(self.errors, "bkg"),
             converged=self.converged[:n].astype(bool), valid=self.valid[:n].astype(bool),
             chisq=self.chisq[:n].copy(), qfit=self.qfit[:n].copy(), qfit_expected=self.qfit_expected[:n].copy(),
-            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(), spread_model=nan.copy(),
-            spread_model_err=nan.copy(), n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes),
-            n_failed=int(r.n_failed), failure_msgs=[],
+            qfit_z=self.qfit_z[:n].copy(), crowding=self.crowding[:n].copy(),
+            spread_model=self.spread_model[:n].copy(), spread_model_err=self.spread_model_err[:n].copy(),
+            n_iter=self.n_iter[:n].astype(np.int64), n_passes=int(r.n_passes), n_failed=int(r.n_failed),
+            failure_msgs=[],
             residual=self.residual if self.residual is not None else np.zeros((ny, nx)),
             stats=dict(n_levels=int(r.n_levels), n_fits=int(r.n_fits), device_seconds=float(r.device_seconds),
                        params=self.params[:n].copy()))
@@ -944,8 +961,8 @@ def fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_v
     """CrowdPhot.fit_all_stars on the B200 (psf_photometry_single.jl:267-469): brightness-
     ordered passes of fit_star against the running residual, each pass run as batches of
     stars whose boxes are disjoint (the sequential result).  Keyword arguments other than
-    n_passes / fixed / inv_var go to fit_star (max_iter, x_tol, f_tol, g_tol, damping, ...).
-    spread_model is not computed (NaN)."""
+    n_passes / fixed / inv_var / spread_model_fwhm go to fit_star (max_iter, x_tol, f_tol,
+    g_tol, damping, ...)."""
     fixed = dict(fixed or {})
     ctx = ctx or get_context()
     imgf, ivf, _, et = _image_arrays(image, inv_var, None)
@@ -955,8 +972,8 @@ def fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_v
     outs = MultipassOutputs(init.shape[0], init.shape[1], ny, nx, residual=residual)
     vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
     rc = ctx.lib.cpb_fit_all_stars(ctx.handle, ctx.psf_handle(psf), C.byref(P), float(fit_rad), int(n_passes),
-                                   vp(imgf), et, ny, nx, vp(ivf), init.shape[0], init.ctypes.data_as(_abi._dp),
-                                   C.byref(outs.c))
+                                   spread_fwhm_arg(spread_model_fwhm), vp(imgf), et, ny, nx, vp(ivf), init.shape[0],
+                                   init.ctypes.data_as(_abi._dp), C.byref(outs.c))
     ctx.raise_for(rc, "cpb_fit_all_stars")
     return outs.result(psf, ny, nx)
 

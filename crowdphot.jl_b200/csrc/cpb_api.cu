@@ -536,8 +536,8 @@ int cpb_fit_simultaneous_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
 }
 
 int cpb_fit_all_stars(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, double fit_rad,
-                      int32_t n_passes, const void* image, int32_t eltype, int64_t ny, int64_t nx,
-                      const void* inv_var, int64_t n, const double* init, cpb_multipass_result* out) {
+                      int32_t n_passes, double spread_model_fwhm, const void* image, int32_t eltype, int64_t ny,
+                      int64_t nx, const void* inv_var, int64_t n, const double* init, cpb_multipass_result* out) {
     return guarded(ctx, [&]() -> int {
         if (!psf || !params || !out || !image || (n > 0 && !init)) throw ArgError{"null argument"};
         if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
@@ -547,7 +547,8 @@ int cpb_fit_all_stars(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* par
         void* d_iv = inv_var ? scratch(ctx, "mp_in_inv_var", bytes) : nullptr;
         check(cudaMemcpyAsync(d_img, image, bytes, cudaMemcpyHostToDevice, ctx->stream), "h2d image");
         if (d_iv) check(cudaMemcpyAsync(d_iv, inv_var, bytes, cudaMemcpyHostToDevice, ctx->stream), "h2d inv_var");
-        return fit_all_stars_dev(ctx, psf, params, fit_rad, n_passes, d_img, eltype, ny, nx, d_iv, n, init, out);
+        return fit_all_stars_dev(ctx, psf, params, fit_rad, n_passes, spread_model_fwhm, d_img, eltype, ny, nx, d_iv,
+                                 n, init, out);
     });
 }
 

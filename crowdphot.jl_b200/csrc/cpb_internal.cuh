@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <exception>
 #include <map>
 #include <mutex>
@@ -268,6 +269,36 @@ __device__ __forceinline__ T warp_max(T v) {
     return v;
 }
 
+// The spread_model reference convolution of a star's model stamp (correlate!
+// with a zero border, correlation.jl:122-141) at stamp pixel (r, c): ms is the
+// bh x bw stamp (column-major), K the (2 kh + 1)^2 kernel.
+__device__ __forceinline__ double spread_conv(const double* ms, int bh, int bw, int r, int c,
+                                              const double* __restrict__ K, int kh) {
+    const int n = 2 * kh + 1;
+    double g = 0.0;
+    for (int q = -kh; q <= kh; ++q) {
+        const int cc = c + q;
+        if (cc < 0 || cc >= bw) continue;
+        for (int p = -kh; p <= kh; ++p) {
+            const int rr = r + p;
+            if (rr < 0 || rr >= bh) continue;
+            g += K[(p + kh) + (q + kh) * n] * ms[rr + cc * bh];
+        }
+    }
+    return g;
+}
+
+// Warps per block of a diagnostics launch that keeps one boxmax-double model
+// stamp per warp in shared memory (8, fewer for large fit radii); boxes above
+// the 200 KB a single warp may take (fit_rad beyond ~80 px) leave spread_model
+// NaN (spread_fits_smem false, K not uploaded).
+inline bool spread_fits_smem(int boxmax) { return (size_t)boxmax * sizeof(double) <= 200 * 1024; }
+inline int diag_warps_per_block(const void* K, int boxmax) {
+    if (!K) return 8;
+    const size_t per = (size_t)boxmax * sizeof(double);
+    return (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / per));
+}
+
 }  // namespace cpb
 
 // ---------------------------------------------------------------------------
@@ -414,6 +445,11 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
 void model_radii_auto(const cpb_psf* psf, double fwhm, double nsigma, int R_fit, int R_cap,
                       std::vector<double>& w_sample, const std::vector<double>& flux, std::vector<int32_t>& out);
 
+// spread_model reference disk (cpb_spread.cu): the (2 half + 1)^2 kernel, false
+// when spread_model is off.
+bool spread_kernel(const cpb_psf* psf, double psf_fwhm, double param, double y1, double x1, double fit_rad,
+                   std::vector<double>& K, int& half);
+
 // Batched simultaneous fits of small groups (cpb_groups.cu).  Device inputs and
 // outputs; the h_*_opt arrays (nullable) are host copies of the group metadata.
 int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
@@ -454,8 +490,8 @@ void group_batch_destroy(GroupBatch* b);
 
 // fit_all_stars (cpb_multipass.cu): device image / weights, host catalogue and outputs.
 int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, double fit_rad, int n_passes,
-                      const void* d_img, int32_t eltype, int64_t ny, int64_t nx, const void* d_iv, int64_t n,
-                      const double* init, cpb_multipass_result* out);
+                      double spread_model_fwhm, const void* d_img, int32_t eltype, int64_t ny, int64_t nx,
+                      const void* d_iv, int64_t n, const double* init, cpb_multipass_result* out);
 
 // Batched LM driver (cpb_lm.cu).  Host inputs.
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cutouts,

@@ -85,41 +85,62 @@ __global__ void k_mp_cutouts(int nL, const int4* __restrict__ boxes, const int64
 
 // _star_diagnostics! (psf_photometry_diagnostics.jl:154-231) over the fitted
 // box: image is the original data, residual the star's fit residual (every
-// model subtracted, its own included), star_model its best-fit render.
-// out: qfit, qfit_expected, qfit_z, crowding per star (NaN where undefined).
+// model subtracted, its own included), star_model its best-fit render, kept in
+// the warp's shared-memory slice (boxmax doubles) for the spread_model
+// convolution (K null: spread_model off).  out: qfit, qfit_expected, qfit_z,
+// crowding, spread_model, spread_model_err per star (NaN where undefined).
 template <typename TI>
 __global__ void k_mp_diag(int nL, const int4* __restrict__ boxes, const double* __restrict__ params,
                           const uint8_t* __restrict__ flags, const TI* __restrict__ img,
                           const double* __restrict__ residual, const TI* __restrict__ iv, DevPsf P, MPConst M,
-                          int n_free, int ny, double* __restrict__ out) {
+                          int n_free, int ny, const double* __restrict__ K, int kh, int boxmax,
+                          double* __restrict__ out) {
+    extern __shared__ double ms_all[];
     const int lane = threadIdx.x & 31;
     const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (s >= nL) return;
+    double* ms = ms_all + (threadIdx.x >> 5) * boxmax;
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
-    double* o = out + (int64_t)s * 4;
+    double* o = out + (int64_t)s * 6;
     const double* pr = params + (int64_t)s * M.np;
     const double flux = pr[M.rf], bkg = pr[M.rb];
     if (!flags[s] || !(flux > 0)) {
-        if (lane == 0) o[0] = o[1] = o[2] = o[3] = NaN;
+        if (lane == 0) o[0] = o[1] = o[2] = o[3] = o[4] = o[5] = NaN;
         return;
     }
     const int4 b = boxes[s];
+    const int nb = b.z * b.w;
+    const bool spread = K != nullptr && nb <= boxmax;
+    if (spread) {
+        for (int e = lane; e < nb; e += 32) ms[e] = mp_model(P, M, pr, b.x + e % b.z, b.y + e / b.z);
+        __syncwarp();
+    }
     const double inv_flux = 1.0 / flux;
     double qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
+    double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
     int ngood = 0;
-    for (int e = lane; e < b.z * b.w; e += 32) {
+    for (int e = lane; e < nb; e += 32) {
         const int i = b.x + e % b.z, j = b.y + e / b.z;
         const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
-        const double mv = mp_model(P, M, pr, i, j);
+        const double mv = spread ? ms[e] : mp_model(P, M, pr, i, j);
         const double wp = iv ? (double)iv[q] : 1.0;
         if (isfinite(wp) && wp > 0) {
             const double r = residual[q];
             qv += fabs(r);
             const double Pp = (mv - bkg) * inv_flux;
             const double wP = wp * Pp;
-            ncl += wP * (r + mv - bkg);
+            const double p_i = r + mv - bkg;
+            ncl += wP * p_i;
             ndi += wP * ((double)img[q] - bkg);
             den += wP * Pp;
+            if (spread) {
+                const double g_i = (spread_conv(ms, b.z, b.w, e % b.z, e / b.z, K, kh) - bkg) * inv_flux;
+                Sp += wP * p_i;
+                Sq += wp * g_i * p_i;
+                Sp0 += wP * Pp;
+                Sq0 += wp * Pp * g_i;
+                SqG += wp * g_i * g_i;
+            }
         }
         if (iv) {
             const double v = (double)iv[q];
@@ -137,6 +158,11 @@ __global__ void k_mp_diag(int nL, const int4* __restrict__ boxes, const double* 
     den = warp_sum(den);
     ss = warp_sum(ss);
     ss2 = warp_sum(ss2);
+    Sp = warp_sum(Sp);
+    Sq = warp_sum(Sq);
+    Sp0 = warp_sum(Sp0);
+    Sq0 = warp_sum(Sq0);
+    SqG = warp_sum(SqG);
     ngood = warp_sum(ngood);
     if (lane == 0) {
         const double c2p = 0.7978845608028654;  // sqrt(2 / pi)
@@ -147,6 +173,11 @@ __global__ void k_mp_diag(int nL, const int4* __restrict__ boxes, const double* 
         if (iv && ss2 > 0 && ngood > n_free) {
             const double dfac = sqrt(1.0 - (double)n_free / (double)ngood);
             o[2] = (qv - c2p * dfac * ss) / (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
+        }
+        o[4] = o[5] = NaN;
+        if (spread && Sp > 0) {
+            o[4] = Sq / Sp - Sq0 / Sp0;
+            if (iv) o[5] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
         }
     }
 }
@@ -162,8 +193,8 @@ inline unsigned warps_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n
 }  // namespace
 
 int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, double fit_rad, int n_passes,
-                      const void* d_img, int32_t eltype, int64_t ny64, int64_t nx64, const void* d_iv, int64_t n,
-                      const double* init, cpb_multipass_result* out) {
+                      double spread_model_fwhm, const void* d_img, int32_t eltype, int64_t ny64, int64_t nx64,
+                      const void* d_iv, int64_t n, const double* init, cpb_multipass_result* out) {
     if (!(n_passes > 0)) throw ArgError{"n_passes must be positive, got " + std::to_string(n_passes)};
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
     if (ny64 <= 0 || nx64 <= 0 || ny64 * nx64 >= (1LL << 31)) throw ArgError{"image size out of range"};
@@ -204,7 +235,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         for (int q = 0; q < np; ++q)
             if (std::find(free_idx.begin(), free_idx.end(), q) == free_idx.end()) err[s * np + q] = 0.0;
     std::vector<uint8_t> valid(n, 1), conv(n, 0);
-    std::vector<double> chisq(n, 0.0), diag(n * 4, NaN);
+    std::vector<double> chisq(n, 0.0), diag(n * 6, NaN);
     std::vector<int32_t> niter(n, 0);
     if (n == 0) {
         if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
@@ -234,7 +265,26 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     double* d_lmd = (double*)scratch(ctx, "mp_lm_f64", sizeof(double) * n * (np + nf * nf + 4));
     uint8_t* d_lmu = (uint8_t*)scratch(ctx, "mp_lm_u8", (size_t)n * 4);
     int32_t* d_lmi = (int32_t*)scratch(ctx, "mp_lm_i32", sizeof(int32_t) * n * 2);
-    double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 4);
+    double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 6);
+    // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
+    std::vector<double> h_spread;
+    int kh = 0;
+    double* d_K = nullptr;
+    const int boxmax = (int)box_max;
+    if (spread_kernel(psf, psf->dev.fwhm, spread_model_fwhm, init[0], init[1], fit_rad, h_spread, kh) &&
+        spread_fits_smem(boxmax)) {
+        d_K = (double*)scratch(ctx, "mp_spread_K", sizeof(double) * h_spread.size());
+        check(cudaMemcpyAsync(d_K, h_spread.data(), sizeof(double) * h_spread.size(), cudaMemcpyHostToDevice, st),
+              "h2d");
+    }
+    const int dwpb = diag_warps_per_block(d_K, boxmax);
+    const size_t diag_smem = d_K ? (size_t)dwpb * boxmax * sizeof(double) : 0;
+    if (diag_smem > 48 * 1024) {
+        check(cudaFuncSetAttribute(k_mp_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+              "smem attr");
+        check(cudaFuncSetAttribute(k_mp_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+              "smem attr");
+    }
 
     // host staging of one batch
     std::vector<int4> hbox;
@@ -405,18 +455,20 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
                 KernelScope ks_(ctx, "k_mp_diag", (double)tot * (d_iv ? 24 : 16));
                 if (eltype == CPB_F64)
-                    k_mp_diag<double><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, (const double*)d_img,
-                                                                    resid, (const double*)d_iv, dp, M, nf, ny, d_diag);
+                    k_mp_diag<double><<<(unsigned)((nL + dwpb - 1) / dwpb), 32 * dwpb, diag_smem, st>>>(
+                        nL, d_box, d_psub, d_flag, (const double*)d_img, resid, (const double*)d_iv, dp, M, nf, ny, d_K,
+                        kh, boxmax, d_diag);
                 else
-                    k_mp_diag<float><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, (const float*)d_img,
-                                                                   resid, (const float*)d_iv, dp, M, nf, ny, d_diag);
+                    k_mp_diag<float><<<(unsigned)((nL + dwpb - 1) / dwpb), 32 * dwpb, diag_smem, st>>>(
+                        nL, d_box, d_psub, d_flag, (const float*)d_img, resid, (const float*)d_iv, dp, M, nf, ny, d_K,
+                        kh, boxmax, d_diag);
                 check(cudaGetLastError(), "k_mp_diag");
-                hdiag.resize((size_t)nL * 4);
-                check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * nL * 4, cudaMemcpyDeviceToHost, st), "d2h");
+                hdiag.resize((size_t)nL * 6);
+                check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * nL * 6, cudaMemcpyDeviceToHost, st), "d2h");
                 check(cudaStreamSynchronize(st), "sync");
                 for (int k = 0; k < nL; ++k)
                     if (hflag[k] == 2)
-                        for (int t = 0; t < 4; ++t) diag[B[k] * 4 + t] = hdiag[(size_t)k * 4 + t];
+                        for (int t = 0; t < 6; ++t) diag[B[k] * 6 + t] = hdiag[(size_t)k * 6 + t];
             }
         }
         // between-pass validation (:404-412)
@@ -440,10 +492,12 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         out->valid[s] = valid[s];
         out->chisq[s] = chisq[s];
         out->n_iter[s] = niter[s];
-        if (out->qfit) out->qfit[s] = diag[s * 4];
-        if (out->qfit_expected) out->qfit_expected[s] = diag[s * 4 + 1];
-        if (out->qfit_z) out->qfit_z[s] = diag[s * 4 + 2];
-        if (out->crowding) out->crowding[s] = diag[s * 4 + 3];
+        if (out->qfit) out->qfit[s] = diag[s * 6];
+        if (out->qfit_expected) out->qfit_expected[s] = diag[s * 6 + 1];
+        if (out->qfit_z) out->qfit_z[s] = diag[s * 6 + 2];
+        if (out->crowding) out->crowding[s] = diag[s * 6 + 3];
+        if (out->spread_model) out->spread_model[s] = diag[s * 6 + 4];
+        if (out->spread_model_err) out->spread_model_err[s] = diag[s * 6 + 5];
     }
     return 0;
 }

@@ -89,12 +89,12 @@ double aperture_weight(int i, int j, double r) {
     return overlap_single(dx - 0.5, dy - 0.5, dx + 0.5, dy + 0.5, r);
 }
 
-// bicubic_interpolate value of one node at detector pixel (py, px) for a star
-// at the origin (empirical_models.jl:185-292).
-double node_value(const cpb_psf* ps, const DevNode& nd, double py, double px) {
+// bicubic_interpolate value of one node at detector offset (dy, dx) = pixel
+// minus star centre (empirical_models.jl:185-292).
+double node_value(const cpb_psf* ps, const DevNode& nd, double dy, double dx) {
     const double* data = ps->h_data64.data() + nd.off;
-    const double u = nd.sx * px + nd.ox;
-    const double v = nd.sy * py + nd.oy;
+    const double u = nd.sx * dx + nd.ox;
+    const double v = nd.sy * dy + nd.oy;
     const int nyd = nd.ny, nxd = nd.nx;
     if (!(std::isfinite(u) && std::isfinite(v) && u >= 1 && u <= nxd && v >= 1 && v <= nyd)) return nd.fill;
     const int lx = std::min(std::max((int)std::floor(u), 1), nxd - 1);
@@ -115,31 +115,94 @@ double node_value(const cpb_psf* ps, const DevNode& nd, double py, double px) {
     return dv * (dv * (dv * v3 + v2) + v1) + row[1];
 }
 
-// The unit model (y = x = 0, flux = 1, bkg = 0) at pixel (i, j): the node blend
-// of GriddedPSFModel at the origin (_grid_corners_dw, gridded_psf.jl:176-208).
-double unit_value(const cpb_psf* ps, int i, int j) {
+// Node weights of GriddedPSFModel at (Y, X) (_grid_corners_dw, gridded_psf.jl:176-208,
+// weights only); single-node and ImagePSF models: node 0 with weight 1.
+int host_corners(const cpb_psf* ps, double Y, double X, int idx[4], double wts[4]) {
     const DevPsf& P = ps->dev;
-    if (P.n_nodes == 1 || P.kind != CPB_PSF_GRIDDED_IMAGE) return node_value(ps, ps->h_nodes[0], i, j);
+    if (P.n_nodes == 1 || P.kind != CPB_PSF_GRIDDED_IMAGE) {
+        idx[0] = 0;
+        wts[0] = 1.0;
+        return 1;
+    }
     const auto& yg = ps->h_ygrid;
     const auto& xg = ps->h_xgrid;
     const int gny = (int)yg.size(), gnx = (int)xg.size();
     int iy = 0, ix = 0;
-    for (int k = 0; k < gny; ++k) iy += yg[k] <= 0.0 ? 1 : 0;
-    for (int k = 0; k < gnx; ++k) ix += xg[k] <= 0.0 ? 1 : 0;
+    for (int k = 0; k < gny; ++k) iy += yg[k] <= Y ? 1 : 0;
+    for (int k = 0; k < gnx; ++k) ix += xg[k] <= X ? 1 : 0;
     iy = std::min(std::max(iy, 1), gny - 1);
     ix = std::min(std::max(ix, 1), gnx - 1);
     const double y0 = yg[iy - 1], y1 = yg[iy], x0 = xg[ix - 1], x1 = xg[ix];
-    const double Yc = std::min(std::max(0.0, y0), y1), Xc = std::min(std::max(0.0, x0), x1);
+    const double Yc = std::min(std::max(Y, y0), y1), Xc = std::min(std::max(X, x0), x1);
     const double inv = 1.0 / ((x1 - x0) * (y1 - y0));
-    const double wts[4] = {(x1 - Xc) * (y1 - Yc) * inv, (Xc - x0) * (y1 - Yc) * inv, (x1 - Xc) * (Yc - y0) * inv,
-                           (Xc - x0) * (Yc - y0) * inv};
-    const int idx[4] = {ps->h_index_grid[(iy - 1) + (ix - 1) * gny], ps->h_index_grid[(iy - 1) + ix * gny],
-                        ps->h_index_grid[iy + (ix - 1) * gny], ps->h_index_grid[iy + ix * gny]};
+    const double w4[4] = {(x1 - Xc) * (y1 - Yc) * inv, (Xc - x0) * (y1 - Yc) * inv, (x1 - Xc) * (Yc - y0) * inv,
+                          (Xc - x0) * (Yc - y0) * inv};
+    const int i4[4] = {ps->h_index_grid[(iy - 1) + (ix - 1) * gny], ps->h_index_grid[(iy - 1) + ix * gny],
+                       ps->h_index_grid[iy + (ix - 1) * gny], ps->h_index_grid[iy + ix * gny]};
+    int k = 0;
+    for (int q = 0; q < 4; ++q)
+        if (w4[q] != 0.0) {
+            idx[k] = i4[q];
+            wts[k] = w4[q];
+            ++k;
+        }
+    return k;
+}
+
+}  // namespace
+
+// The unit model (flux = 1, bkg = 0) centred at (Y, X), at pixel (i, j).
+double host_unit_value(const cpb_psf* ps, double fwhm, double Y, double X, int i, int j) {
+    if (ps->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        const double g = -4.0 * std::log(2.0);
+        const double r2 = ((double)i - Y) * ((double)i - Y) + ((double)j - X) * ((double)j - X);
+        const double norm = -(kPi * fwhm * fwhm / g);
+        return (1.0 / norm) * std::exp(g * r2 / (fwhm * fwhm));
+    }
+    int idx[4];
+    double wts[4];
+    const int nc = host_corners(ps, Y, X, idx, wts);
     double s = 0;
-    for (int k = 0; k < 4; ++k)
-        if (wts[k] != 0.0) s += wts[k] * node_value(ps, ps->h_nodes[idx[k]], i, j);
+    for (int k = 0; k < nc; ++k) s += wts[k] * node_value(ps, ps->h_nodes[idx[k]], (double)i - Y, (double)j - X);
     return s;
 }
+
+// PSF.extent of the model centred at (Y, X) (PSF.jl:285-296, empirical_models.jl:167-176,
+// gridded_psf.jl:281-300): (ymin, ymax, xmin, xmax).
+void host_extent(const cpb_psf* ps, double fwhm, double Y, double X, double e[4]) {
+    if (ps->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        const double a = 5.0 * fwhm / 2;  // fwhm_factor 5, no rotation
+        e[0] = Y - a;
+        e[1] = Y + a;
+        e[2] = X - a;
+        e[3] = X + a;
+        return;
+    }
+    int idx[4];
+    double wts[4];
+    const int nc = host_corners(ps, Y, X, idx, wts);
+    for (int k = 0; k < nc; ++k) {
+        const DevNode& nd = ps->h_nodes[idx[k]];
+        const double lo_y = Y - (nd.oy - 1.0) / nd.sy, hi_y = Y + ((double)nd.ny - nd.oy) / nd.sy;
+        const double lo_x = X - (nd.ox - 1.0) / nd.sx, hi_x = X + ((double)nd.nx - nd.ox) / nd.sx;
+        if (k == 0) {
+            e[0] = lo_y;
+            e[1] = hi_y;
+            e[2] = lo_x;
+            e[3] = hi_x;
+        } else {
+            e[0] = std::min(e[0], lo_y);
+            e[1] = std::max(e[1], hi_y);
+            e[2] = std::min(e[2], lo_x);
+            e[3] = std::max(e[3], hi_x);
+        }
+    }
+}
+
+namespace {
+
+// The unit model (y = x = 0, flux = 1, bkg = 0) at pixel (i, j).
+double unit_value(const cpb_psf* ps, int i, int j) { return host_unit_value(ps, 0.0, 0.0, 0.0, i, j); }
 
 // Annular mean surface brightness of the unit PSF for radii 1..R_cap
 // (_model_radii, :226-236), from its curve of growth.

@@ -392,12 +392,15 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             }
             __syncthreads();
         }
-        T raw[MAXE][3];
+        constexpr int RE = MAXE > 0 ? MAXE : 1;
+        T raw[RE][3];
         double acc[6] = {0, 0, 0, 0, 0, 0};
+        const int ne = MAXE > 0 ? MAXE : (S2b + NTF - 1) / NTF;  // MAXE 0: value-only, any box
 #pragma unroll
-        for (int e = 0; e < MAXE; ++e) {
+        for (int e = 0; e < ne; ++e) {
             const int m = threadIdx.x + e * NTF;
-            raw[e][0] = raw[e][1] = raw[e][2] = 0;
+            const int er = MAXE > 0 ? e : 0;
+            raw[er][0] = raw[er][1] = raw[er][2] = 0;
             if (m >= S2b) continue;
             const int row = m % Sb, col = m / Sb;
             const int gy = a_y - Rb + row, gx = a_x - Rb + col;
@@ -432,10 +435,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             const T ga = g0 == 0 ? g[0] : (g0 == 1 ? g[1] : g[2]);
             const T gb = g1 == 0 ? g[0] : (g1 == 1 ? g[1] : g[2]);
             const T gc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
-            raw[e][0] = sq * ga;
-            raw[e][1] = p > 1 ? sq * gb : (T)0;
-            raw[e][2] = p > 2 ? sq * gc : (T)0;
-            const double r0 = raw[e][0], r1 = raw[e][1], r2 = raw[e][2];
+            raw[er][0] = sq * ga;
+            raw[er][1] = p > 1 ? sq * gb : (T)0;
+            raw[er][2] = p > 2 ? sq * gc : (T)0;
+            const double r0 = raw[er][0], r1 = raw[er][1], r2 = raw[er][2];
             if (gram) {  // packed upper triangle (0,0) (0,1) (0,2) (1,1) (1,2) (2,2) for p = 3
                 if (p == 1) {
                     acc[0] += r0 * r0;
@@ -480,7 +483,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                 }
                 T* Vj = V + (int64_t)j * fc.VS;
 #pragma unroll
-                for (int e = 0; e < MAXE; ++e) {
+                for (int e = 0; e < RE; ++e) {
                     const int m = threadIdx.x + e * NTF;
                     if (m >= S2b) continue;
                     Vj[m * p] = raw[e][0] * inv[0];
@@ -1177,33 +1180,45 @@ __global__ void k_errors(int64_t n_act, int p, const double* gram, bool reweight
     for (int k = 0; k < p; ++k) err[j * p + k] = sqrt(fmax(0.0, inv[k + k * p] * f));
 }
 
-// chisq and the qfit / crowding diagnostics per active star (:1358-1397,
-// psf_photometry_diagnostics.jl:154-231); one warp per star.
+// chisq and the qfit / crowding / spread_model diagnostics per active star
+// (:1358-1397, psf_photometry_diagnostics.jl:154-231); one warp per star, the
+// star's model stamp over its box kept in the warp's slice of shared memory
+// (boxmax doubles) for the spread_model convolution (K null: spread_model off).
 template <typename TI>
 __global__ void k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad, const StarCoef* __restrict__ coef,
                        const double* __restrict__ resid, const TI* __restrict__ img, const TI* __restrict__ bkgimg,
-                       const TI* __restrict__ iv, double* out /* n_act x 5: chisq qfit qfit_exp qfit_z crowding */) {
+                       const TI* __restrict__ iv, const double* __restrict__ K, int kh, int boxmax,
+                       double* out /* n_act x 7: chisq qfit qfit_exp qfit_z crowding spread spread_err */) {
+    extern __shared__ double ms_all[];
     const int lane = threadIdx.x & 31;
     const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (j >= n_act) return;
+    double* ms = ms_all + (threadIdx.x >> 5) * boxmax;
     const StarCoef c = coef[j];
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
-    double* o = out + j * 5;
+    double* o = out + j * 7;
     const bool validp = isfinite(c.y) && isfinite(c.x) && isfinite(c.flux) && c.flux > 0;
     if (!validp) {
         if (lane == 0) {
             o[0] = 0.0;
-            o[1] = o[2] = o[3] = o[4] = NaN;
+            o[1] = o[2] = o[3] = o[4] = o[5] = o[6] = NaN;
         }
         return;
     }
     int ylo = max((int)floor(c.y - fit_rad), 1), yhi = min((int)ceil(c.y + fit_rad), fc.ny);
     int xlo = max((int)floor(c.x - fit_rad), 1), xhi = min((int)ceil(c.x + fit_rad), fc.nx);
     double num = 0, qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
+    double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
     int ng = 0, ngi = 0;
     const int h = yhi - ylo + 1, wd = xhi - xlo + 1;
     const double inv_flux = 1.0 / c.flux;
+    const bool spread = K != nullptr && h > 0 && wd > 0 && h * wd <= boxmax;
     if (h > 0 && wd > 0) {
+        if (spread) {
+            for (int e = lane; e < h * wd; e += 32)
+                ms[e] = model_value<double, double>(P, P.data64, c, (double)(ylo + e % h), (double)(xlo + e / h));
+            __syncwarp();
+        }
         for (int e = lane; e < h * wd; e += 32) {
             const int gy = ylo + e % h, gx = xlo + e / h;
             const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
@@ -1212,14 +1227,23 @@ __global__ void k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad, con
             if (isfinite(wp) && wp > 0) {
                 num += wp * (r * r);
                 ng += 1;
-                double mv = model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
+                const double mv = spread ? ms[e] : model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
                 qv += fabs(r);
-                double Pp = (mv - c.bkg) * inv_flux;
-                double wP = wp * Pp;
-                ncl += wP * (r + mv - c.bkg);
-                double im = (double)img[q] - (bkgimg ? (double)bkgimg[q] : 0.0);
+                const double Pp = (mv - c.bkg) * inv_flux;
+                const double wP = wp * Pp;
+                const double p_i = r + mv - c.bkg;
+                ncl += wP * p_i;
+                const double im = (double)img[q] - (bkgimg ? (double)bkgimg[q] : 0.0);
                 ndi += wP * (im - c.bkg);
                 den += wP * Pp;
+                if (spread) {
+                    const double g_i = (spread_conv(ms, h, wd, e % h, e / h, K, kh) - c.bkg) * inv_flux;
+                    Sp += wP * p_i;
+                    Sq += wp * g_i * p_i;
+                    Sp0 += wP * Pp;
+                    Sq0 += wp * Pp * g_i;
+                    SqG += wp * g_i * g_i;
+                }
                 if (iv) {
                     double si = 1.0 / sqrt(wp);
                     ss += si;
@@ -1236,12 +1260,22 @@ __global__ void k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad, con
     den = warp_sum(den);
     ss = warp_sum(ss);
     ss2 = warp_sum(ss2);
+    Sp = warp_sum(Sp);
+    Sq = warp_sum(Sq);
+    Sp0 = warp_sum(Sp0);
+    Sq0 = warp_sum(Sq0);
+    SqG = warp_sum(SqG);
     ng = warp_sum(ng);
     ngi = warp_sum(ngi);
     if (lane == 0) {
         o[0] = (ng - fc.p > 0) ? num / (double)(ng - fc.p) : 0.0;
         o[1] = qv * inv_flux;
         o[4] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
+        o[5] = o[6] = NaN;
+        if (spread && Sp > 0) {
+            o[5] = Sq / Sp - Sq0 / Sp0;
+            if (iv) o[6] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
+        }
         if (iv) {
             o[2] = sqrt(2.0 / 3.141592653589793) * ss * inv_flux;
             if (ss2 > 0 && ngi > fc.p) {
@@ -1266,6 +1300,34 @@ T* S(cpb_ctx* ctx, const char* name, size_t count) {
 }
 
 inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t>(1, (n + t - 1) / t); }
+
+// k_eval with the register cache its box needs: 256 threads for boxes up to
+// 2,048 pixels, 512 / 1,024 threads up to 4,096 / 8,192 (ceil(radius) <= 44);
+// the value-only form (no cache) takes any box.  smem: the axis tables.
+template <bool GRAD, typename T, typename... A>
+void launch_k_eval(int64_t S2, unsigned grid, size_t smem, cudaStream_t st, A... args) {
+    auto go = [&](auto kern, int threads) {
+        if (smem > 48 * 1024)
+            check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
+        kern<<<grid, threads, smem, st>>>(args...);
+    };
+    if (S2 <= 256)
+        go(k_eval<256, 1, GRAD, T>, 256);
+    else if (S2 <= 512)
+        go(k_eval<256, 2, GRAD, T>, 256);
+    else if (S2 <= 1024)
+        go(k_eval<256, 4, GRAD, T>, 256);
+    else if (S2 <= 2048)
+        go(k_eval<256, 8, GRAD, T>, 256);
+    else if (S2 <= 4096)
+        go(k_eval<512, 8, GRAD, T>, 512);
+    else if (S2 <= 8192)
+        go(k_eval<1024, 8, GRAD, T>, 1024);
+    else if constexpr (!GRAD)
+        go(k_eval<256, 0, false, T>, 256);
+    else
+        throw ArgError{"fit_rad too large for the B200 stamp kernel of a gridded PSF (ceil(fit_rad) must be <= 44)"};
+}
 
 struct TileLists {
     int32_t *start = nullptr, *end = nullptr;
@@ -1362,6 +1424,8 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         if (out->qfit_expected) out->qfit_expected[i] = NaN;
         if (out->qfit_z) out->qfit_z[i] = NaN;
         if (out->crowding) out->crowding[i] = NaN;
+        if (out->spread_model) out->spread_model[i] = NaN;
+        if (out->spread_model_err) out->spread_model_err[i] = NaN;
     };
     if (n_stars == 0) {
         out->n_passes = 0;
@@ -1463,6 +1527,12 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     unsigned h_flags[4];
     check(cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st), "d2h");
+    // the first catalogue star's position sizes the spread_model reference disk
+    double h_yx1[2] = {0, 0};
+    if (n_stars > 0) {
+        check(cudaMemcpyAsync(&h_yx1[0], d_y0, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaMemcpyAsync(&h_yx1[1], d_x0, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
+    }
     check(cudaStreamSynchronize(st), "sync");
     if (!d_inv_var && h_flags[0] > 0)
         throw ArgError{
@@ -1626,19 +1696,22 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
     bool m_fresh = false;  // Mbuf holds the current-theta model of the live stars (written by the fill)
     const bool warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
-    if (warp_eval && 8 * 2 * fc.S * sizeof(AxisTab<double>) > 48 * 1024)
-        throw ArgError{"fit radius too large for the B200 stamp kernels"};
     // model-value launches of the warp kernel: as many warps a block as their
     // row / column tables fit in shared memory (large :auto model boxes use fewer)
     int smem_optin = 0;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
-    auto model_warp_shape = [&](size_t tab_size, unsigned& threads, size_t& smem) {
+    // warps per block of a k_eval_warp launch whose per-warp axis tables (2 Sx
+    // entries) fit the opt-in shared memory
+    auto warp_shape = [&](int Sx, size_t tab_size, unsigned& threads, size_t& smem) {
         int warps = 8;
-        while (warps > 1 && (size_t)warps * 2 * Sm * tab_size > (size_t)smem_optin) warps /= 2;
-        if ((size_t)warps * 2 * Sm * tab_size > (size_t)smem_optin)
-            throw ArgError{"model radius too large for the B200 render kernel"};
+        while (warps > 1 && (size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin) warps /= 2;
+        if ((size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin)
+            throw ArgError{"radius too large for the B200 stamp kernels"};
         threads = 32u * warps;
-        smem = (size_t)warps * 2 * Sm * tab_size;
+        smem = (size_t)warps * 2 * Sx * tab_size;
+    };
+    auto model_warp_shape = [&](size_t tab_size, unsigned& threads, size_t& smem) {
+        warp_shape(Sm, tab_size, threads, smem);
     };
     auto eval_grid = [&](int64_t nlist) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16)); };
     auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
@@ -1651,16 +1724,19 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         const size_t smem = tab_bytes * fc.S;
         TS* Mo = writeM ? Mbuf : nullptr;
         if (warp_eval) {
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, TS><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<TS>), st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
-        } else if (fc.S2 <= 256 * 2)
-            k_eval<256, 2, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
-        else if (fc.S2 <= 256 * 4)
-            k_eval<256, 4, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
-        else if (fc.S2 <= 256 * 8)
-            k_eval<256, 8, true, TS><<<eval_grid(nlist), 256, smem, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
-        else
-            throw ArgError{"fit_rad too large for the B200 stamp kernel (ceil(fit_rad) must be <= 22)"};
+            unsigned thr;
+            size_t sm_bytes;
+            warp_shape(fc.S, sizeof(AxisTab<TS>), thr, sm_bytes);
+            if (sm_bytes > 48 * 1024)
+                check(cudaFuncSetAttribute(k_eval_warp<true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm_bytes), "smem attr");
+            const int wpb = (int)(thr / 32);
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
+        } else {
+            launch_k_eval<true, TS>(fc.S2, eval_grid(nlist), smem, st, list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn,
+                                    gram, Mo, fc.R, MS, (const int32_t*)nullptr, (const int64_t*)nullptr);
+        }
         check(cudaGetLastError(), "k_eval_fill");
         m_fresh = writeM;
     };
@@ -1681,16 +1757,11 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
             const int wpb = (int)(thr / 32);
             const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
             k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        } else if (Sm * Sm <= 256)
-            k_eval<256, 1, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        else if (Sm * Sm <= 512)
-            k_eval<256, 2, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        else if (Sm * Sm <= 1024)
-            k_eval<256, 4, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        else if (Sm * Sm <= 2048)
-            k_eval<256, 8, false, TS><<<gb, 256, smem, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        else
-            throw ArgError{"model_rad too large for the B200 render kernel (ceil(model_rad) must be <= 22)"};
+        } else {
+            launch_k_eval<false, TS>((int64_t)Sm * Sm, gb, smem, st, list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn,
+                                     (double*)nullptr, Mbuf, model_R, MS, (const int32_t*)d_modelR,
+                                     (const int64_t*)d_moff);
+        }
         check(cudaGetLastError(), "k_eval_model");
     };
     auto launch_render = [&](int mode, const uint8_t* incl, const int32_t* list, int64_t nlist, const StarCoef* cf,
@@ -1889,18 +1960,21 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     {
         KernelScope ks_(ctx, "k_eval_gram", (double)n_act * (48.0 + sizeof(StarCoef)));
         if (warp_eval) {
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, double><<<gbw, 256, 8 * 2 * fc.S * sizeof(AxisTab<double>), st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
-        } else if (fc.S2 <= 256 * 2) {
-            k_eval<256, 2, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
-        } else if (fc.S2 <= 256 * 4) {
-            k_eval<256, 4, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
+            unsigned thr;
+            size_t sm_bytes;
+            warp_shape(fc.S, sizeof(AxisTab<double>), thr, sm_bytes);
+            if (sm_bytes > 48 * 1024)
+                check(cudaFuncSetAttribute(k_eval_warp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)sm_bytes), "smem attr");
+            const int wpb = (int)(thr / 32);
+            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<true, double><<<gbw, thr, sm_bytes, st>>>(
                 nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
         } else {
-            k_eval<256, 8, true, double><<<eval_grid(n_act), 256, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
+            launch_k_eval<true, double>(fc.S2, eval_grid(n_act), (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S,
+                                        st, (const int32_t*)nullptr, n_act, fc, dp, coef, ay, ax, w, sw, (double*)nullptr,
+                                        cn, gram, (double*)nullptr, fc.R, MS, (const int32_t*)nullptr,
+                                        (const int64_t*)nullptr);
         }
         check(cudaGetLastError(), "k_eval_gram");
     }
@@ -1927,14 +2001,9 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                     nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
             } else {
                 const size_t sm_ = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * Sm;
-                if (Sm * Sm <= 256)
-                    k_eval<256, 1, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
-                else if (Sm * Sm <= 512)
-                    k_eval<256, 2, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
-                else if (Sm * Sm <= 1024)
-                    k_eval<256, 4, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
-                else
-                    k_eval<256, 8, false, double><<<eval_grid(n_act), 256, sm_, st>>>(nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
+                launch_k_eval<false, double>((int64_t)Sm * Sm, eval_grid(n_act), sm_, st, (const int32_t*)nullptr, n_act,
+                                             fc, dp, coef, ay, ax, w, sw, (double*)nullptr, cn, (double*)nullptr, M64,
+                                             model_R, MS, (const int32_t*)d_modelR, (const int64_t*)d_moff);
             }
             check(cudaGetLastError(), "k_eval_model");
         }
@@ -1942,25 +2011,49 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
-    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 5);
-    if (eltype == CPB_F64)
-        k_diag<double><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
-                                                         (const double*)d_image, (const double*)d_background,
-                                                         (const double*)d_inv_var, diag);
-    else
-        k_diag<float><<<nblk(n_act * 32), 256, 0, st>>>(n_act, fc, dp, P->fit_rad, coef, resid, (const float*)d_image,
-                                                        (const float*)d_background, (const float*)d_inv_var, diag);
+    // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
+    std::vector<double> h_spread;
+    int kh = 0;
+    double* d_K = nullptr;
+    {
+        if (spread_kernel(psf, psf->dev.fwhm, P->spread_model_fwhm, h_yx1[0], h_yx1[1], P->fit_rad, h_spread, kh) &&
+            spread_fits_smem((2 * (int)std::ceil(P->fit_rad) + 2) * (2 * (int)std::ceil(P->fit_rad) + 2))) {
+            d_K = S<double>(ctx, "spread_K", (int64_t)h_spread.size());
+            check(cudaMemcpyAsync(d_K, h_spread.data(), sizeof(double) * h_spread.size(), cudaMemcpyHostToDevice, st),
+                  "h2d");
+        }
+    }
+    const int boxmax = (2 * (int)std::ceil(P->fit_rad) + 2) * (2 * (int)std::ceil(P->fit_rad) + 2);
+    const int dwpb = diag_warps_per_block(d_K, boxmax);
+    const size_t diag_smem = d_K ? (size_t)dwpb * boxmax * sizeof(double) : 0;
+    const unsigned dgrid = (unsigned)std::max<int64_t>(1, (n_act + dwpb - 1) / dwpb);
+    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 7);
+    if (eltype == CPB_F64) {
+        if (diag_smem > 48 * 1024)
+            check(cudaFuncSetAttribute(k_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+                  "smem attr");
+        k_diag<double><<<dgrid, 32 * dwpb, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
+                                                           (const double*)d_image, (const double*)d_background,
+                                                           (const double*)d_inv_var, d_K, kh, boxmax, diag);
+    } else {
+        if (diag_smem > 48 * 1024)
+            check(cudaFuncSetAttribute(k_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+                  "smem attr");
+        k_diag<float><<<dgrid, 32 * dwpb, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
+                                                          (const float*)d_image, (const float*)d_background,
+                                                          (const float*)d_inv_var, d_K, kh, boxmax, diag);
+    }
     check(cudaGetLastError(), "k_diag");
     check(cudaEventRecord(ctx->ev1, st), "event");
 
     // ---- download and assemble (:1289-1300, :1331-1337, :1404-1430)
-    std::vector<double> h_theta(n), h_err(n), h_diag(n_act * 5);
+    std::vector<double> h_theta(n), h_err(n), h_diag(n_act * 7);
     std::vector<int32_t> h_act(n_act), h_frozen(n_act);
     std::vector<uint8_t> h_live(n_act), h_conv(n_act);
     std::vector<double> y0(n_stars), x0(n_stars), f0(n_stars);
     check(cudaMemcpyAsync(h_theta.data(), theta, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_err.data(), err, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
-    check(cudaMemcpyAsync(h_diag.data(), diag, sizeof(double) * n_act * 5, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(h_diag.data(), diag, sizeof(double) * n_act * 7, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_act.data(), act, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_frozen.data(), frozen_at, sizeof(int32_t) * n_act, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_live.data(), live, n_act, cudaMemcpyDeviceToHost, st), "d2h");
@@ -2034,7 +2127,9 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         if (out->dbg_active) out->dbg_active[j] = h_act[j];
         if (out->dbg_model_R) out->dbg_model_R[j] = d_modelR ? h_modelR[j] : model_R;
         if (!valid[i]) continue;
-        const double* dg = &h_diag[j * 5];
+        const double* dg = &h_diag[j * 7];
+        if (out->spread_model) out->spread_model[i] = dg[5];
+        if (out->spread_model_err) out->spread_model_err[i] = dg[6];
         if (out->chisq) out->chisq[i] = dg[0];
         if (out->qfit) out->qfit[i] = dg[1];
         if (out->qfit_expected) out->qfit_expected[i] = dg[2];

@@ -133,6 +133,9 @@ typedef struct cpb_sim_params {
     int32_t solver;           /* CPB_SOLVER_* */
     int32_t damping;          /* CPB_DAMP_* */
     int32_t reserved;
+    /* spread_model reference disk FWHM: NaN = from the PSF's effective area
+     * (the reference default, _spread_fwhm); <= 0 = skip spread_model */
+    double spread_model_fwhm;
 } cpb_sim_params;
 
 /*
@@ -164,6 +167,7 @@ typedef struct cpb_sim_result {
     double model_px_evals;    /* stamp fills + renders, star-pixel evaluations */
     double lsqr_px_macs;      /* star-pixel products in J and J^T */
     double device_seconds;    /* device-timed fit, excluding host<->device copies */
+    double *spread_model, *spread_model_err; /* optional, n */
 } cpb_sim_result;
 
 /*
@@ -306,6 +310,7 @@ typedef struct cpb_multipass_result {
     int64_t n_levels;          /* batches run (summed over the passes) */
     int64_t n_fits;            /* fit_star calls run */
     double device_seconds;
+    double *spread_model, *spread_model_err; /* optional */
 } cpb_multipass_result;
 
 /*
@@ -321,11 +326,22 @@ typedef struct cpb_multipass_result {
  * of eltype (background-subtracted); inv_var nullable; init: n*np initial
  * parameters (the catalogue, with the PSF's own values for parameters the
  * catalogue lacks).  LM keyword arguments as cpb_fit_lm_batch.  Host arrays.
- * spread_model is not computed.
+ * spread_model_fwhm: as cpb_sim_params.spread_model_fwhm.
  */
 CPB_API int cpb_fit_all_stars(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, double fit_rad,
-                              int32_t n_passes, const void* image, int32_t eltype, int64_t ny, int64_t nx,
-                              const void* inv_var, int64_t n, const double* init, cpb_multipass_result* out);
+                              int32_t n_passes, double spread_model_fwhm, const void* image, int32_t eltype,
+                              int64_t ny, int64_t nx, const void* inv_var, int64_t n, const double* init,
+                              cpb_multipass_result* out);
+
+/*
+ * The spread_model reference disk (_exp_disk_kernel_bandlimited,
+ * src/photometry/psf_photometry_diagnostics.jl:82-108): the circular
+ * exponential disk of FWHM fwhm (scale length fwhm/16, a 6-Gaussian mixture)
+ * band-limited to the pixel Nyquist frequency, (2 half + 1)^2 values
+ * column-major into K, normalised to sum 1.  The fits use it with
+ * half = ceil(fit_rad).  Host-only (no device work).
+ */
+CPB_API int cpb_exp_disk_kernel(double fwhm, int32_t half, double* K);
 
 /* ---- many small simultaneous fits (star groups) ------------------------- */
 /*

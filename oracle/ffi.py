@@ -19,7 +19,7 @@ if _PKG not in sys.path:
 
 from crowdphot_b200 import _abi  # noqa: E402  (struct layouts of the shared header)
 from crowdphot_b200.photometry import (LMResult, SimOutputs, _catalog, _free_mask, _image_arrays, _props,  # noqa: E402
-                                       lm_params, psf_descriptor, sim_params)
+                                       lm_params, psf_descriptor, sim_params, spread_fwhm_arg)
 from crowdphot_b200.psf import ArgumentError, replace_params  # noqa: E402
 
 LIB = os.path.join(_HERE, "liborc.so")
@@ -64,6 +64,10 @@ def load():
         lib.orc_model_radii_auto_gaussian.restype = C.c_int
         lib.orc_model_radii_auto_gaussian.argtypes = [C.c_double, C.c_double, C.c_int, C.c_int, C.c_int64, _dp,
                                                       C.c_int64, _dp, _i32p]
+        lib.orc_exp_disk_kernel.restype = C.c_int
+        lib.orc_exp_disk_kernel.argtypes = [C.c_double, C.c_int, _dp]
+        lib.orc_spread_fwhm.restype = C.c_double
+        lib.orc_spread_fwhm.argtypes = [C.POINTER(_abi.PsfDesc), C.c_double, C.c_double]
         lib.orc_exact_overlap.restype = C.c_double
         lib.orc_exact_overlap.argtypes = [C.c_double, C.c_double, C.c_double]
         lib.orc_aperture_weight.restype = C.c_double
@@ -75,7 +79,7 @@ def load():
                                              C.c_int64, _dp, C.c_int64, _dp, _i32p]
         lib.orc_fit_all_stars.restype = C.c_int
         lib.orc_fit_all_stars.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_double, C.c_int,
-                                          C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, _dp,
+                                          C.c_double, C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_int64, _dp,
                                           C.POINTER(_abi.MultipassResult), C.c_char_p, C.c_int]
         lib.orc_fit_star_batch.restype = C.c_int
         lib.orc_fit_star_batch.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_int64, _i64p,
@@ -94,7 +98,6 @@ def orc_fit_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_var=No
     """The oracle's fit_all_stars_simultaneous (same call shape as the product's)."""
     lib = load()
     fixed = dict(fixed or {})
-    kw.pop("spread_model_fwhm", None)
     kw.pop("show_trace", None)
     kw.pop("ctx", None)
     imgf, ivf, bkf, et = _image_arrays(image, inv_var, background)
@@ -268,6 +271,23 @@ def orc_fill_stamps(psf, fixed, R, ny, nx, pixels, anchor_y, anchor_x, theta, w,
         raise ArgumentError("bad psf")
 
 
+def orc_exp_disk_kernel(fwhm, half):
+    """The oracle's _exp_disk_kernel_bandlimited(fwhm; half) as a (2 half + 1)^2 matrix."""
+    n = 2 * int(half) + 1
+    K = np.zeros(n * n)
+    if load().orc_exp_disk_kernel(float(fwhm), int(half), K.ctypes.data_as(_dp)) != 0:
+        raise ArgumentError("invalid exp-disk kernel arguments")
+    return K.reshape((n, n), order="F")
+
+
+def orc_spread_fwhm(psf, y, x):
+    """The oracle's _spread_fwhm(psf, y, x)."""
+    desc, keep = psf_descriptor(psf)
+    v = float(load().orc_spread_fwhm(C.byref(desc), float(y), float(x)))
+    del keep
+    return v
+
+
 def orc_exact_overlap(dx, dy, r):
     """Exact area of the unit pixel centred at (dx, dy) inside a circle of radius r at the origin."""
     return float(load().orc_exact_overlap(float(dx), float(dy), float(r)))
@@ -353,13 +373,13 @@ def orc_fit_star_packed(model, pix, offsets, ny, nx, y1, x1, init, *, inv_var=No
     return out, used
 
 
-def orc_fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_var=None, residual=True, **kw):
+def orc_fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, inv_var=None, residual=True,
+                      spread_model_fwhm=None, **kw):
     """The oracle's fit_all_stars (same call shape as the product's)."""
     from crowdphot_b200.photometry import MultipassOutputs, params_matrix
     lib = load()
     fixed = dict(fixed or {})
     kw.pop("ctx", None)
-    kw.pop("spread_model_fwhm", None)
     imgf, ivf, _, et = _image_arrays(image, inv_var, None)
     init = params_matrix(psf, sources)
     P = lm_params(psf, fixed, **kw)
@@ -368,7 +388,8 @@ def orc_fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, i
     desc, keep = psf_descriptor(psf)
     err = C.create_string_buffer(1024)
     vp = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
-    rc = lib.orc_fit_all_stars(C.byref(desc), C.byref(P), float(fit_rad), int(n_passes), vp(imgf), et, ny, nx, vp(ivf),
+    rc = lib.orc_fit_all_stars(C.byref(desc), C.byref(P), float(fit_rad), int(n_passes),
+                               spread_fwhm_arg(spread_model_fwhm), vp(imgf), et, ny, nx, vp(ivf),
                                init.shape[0], init.ctypes.data_as(_dp), C.byref(outs.c), err, 1024)
     del keep
     if rc != 0:

@@ -4,8 +4,9 @@
 // (src/photometry/psf_photometry_single.jl:267-469): brightness-ordered passes,
 // one star at a time, each star added back (passes 2+), fitted with fit_star
 // on its +-fit_rad box of the running residual and subtracted again; per-star
-// diagnostics on the final pass (psf_photometry_diagnostics.jl:154-231).
-// spread_model is not computed (NaN).  Stars with non-finite positions are
+// diagnostics on the final pass (psf_photometry_diagnostics.jl:154-231), with
+// spread_model from the band-limited exponential-disk reference kernel
+// (oracle_spread.cpp; :322-326 of the reference).  Stars with non-finite positions are
 // marked invalid (Julia would raise InexactError from floor(Int, NaN)).
 #include <algorithm>
 #include <cmath>
@@ -40,7 +41,7 @@ StarP star_of(const double* pr, bool gauss) {
 }  // namespace
 
 extern "C" int orc_fit_all_stars(const cpb_psf_desc* desc, const cpb_lm_params* P, double fit_rad, int n_passes,
-                                 const void* image, int32_t eltype, int64_t ny, int64_t nx, const void* inv_var,
+                                 double spread_model_fwhm, const void* image, int32_t eltype, int64_t ny, int64_t nx, const void* inv_var,
                                  int64_t n, const double* init, cpb_multipass_result* out, char* errbuf, int errlen) {
     auto fail = [&](const std::string& m) {
         if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
@@ -70,7 +71,12 @@ extern "C" int orc_fit_all_stars(const cpb_psf_desc* desc, const cpb_lm_params* 
         for (int q = 0; q < np; ++q)
             if (std::find(free_idx.begin(), free_idx.end(), q) == free_idx.end()) err[s * np + q] = 0.0;
     std::vector<uint8_t> valid(n, 1), conv(n, 0);
-    std::vector<double> chisq(n, 0.0), diag(n * 4, NaN);
+    std::vector<double> chisq(n, 0.0), diag(n * 6, NaN);
+    // spread_model reference disk from the first catalogue star (:322-326)
+    std::vector<double> spread_K;
+    int spread_half = 0;
+    const bool have_spread =
+        n > 0 && spread_kernel(psf, spread_model_fwhm, init[0], init[1], fit_rad, spread_K, spread_half);
     std::vector<int32_t> niter(n, 0);
     std::vector<double> resid(npix), ivd(inv_var ? npix : 0);
     for (int64_t q = 0; q < npix; ++q) resid[q] = ld(image, eltype, q);
@@ -134,21 +140,40 @@ extern "C" int orc_fit_all_stars(const cpb_psf_desc* desc, const cpb_lm_params* 
             addsub(best.data(), ylo, yhi, xlo, xhi, -1.0);
             if (pass == n_passes) {  // _star_diagnostics!
                 StarP sp = star_of(best.data(), gauss);
-                double* d = &diag[s * 4];
+                double* d = &diag[s * 6];
                 if (sp.flux > 0) {
+                    std::vector<double> ms((size_t)by * bx), gs;
+                    for (int j = 0; j < bx; ++j)
+                        for (int i = 0; i < by; ++i)
+                            ms[i + (size_t)j * by] = evaluate(psf, sp, (double)(ylo + i), (double)(xlo + j));
+                    if (have_spread) {
+                        gs.resize(ms.size());
+                        correlate_zero(ms.data(), by, bx, spread_K, spread_half, gs.data());
+                    }
                     double inv_flux = 1.0 / sp.flux, qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
+                    double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
                     int64_t ng = 0;
                     for (int j = xlo; j <= xhi; ++j)
                         for (int i = ylo; i <= yhi; ++i) {
                             int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
-                            double mv = evaluate(psf, sp, (double)i, (double)j);
+                            const size_t e = (size_t)(i - ylo) + (size_t)(j - xlo) * by;
+                            double mv = ms[e];
                             double wp = inv_var ? ivd[q] : 1.0;
                             if (std::isfinite(wp) && wp > 0) {
                                 qv += std::fabs(resid[q]);
                                 double Pp = (mv - sp.bkg) * inv_flux, wP = wp * Pp;
-                                ncl += wP * (resid[q] + mv - sp.bkg);
+                                double p_i = resid[q] + mv - sp.bkg;
+                                ncl += wP * p_i;
                                 ndi += wP * (ld(image, eltype, q) - sp.bkg);
                                 den += wP * Pp;
+                                if (have_spread) {
+                                    double g_i = (gs[e] - sp.bkg) * inv_flux;
+                                    Sp += wP * p_i;
+                                    Sq += wp * g_i * p_i;
+                                    Sp0 += wP * Pp;
+                                    Sq0 += wp * Pp * g_i;
+                                    SqG += wp * g_i * g_i;
+                                }
                             }
                             if (inv_var && std::isfinite(ivd[q]) && ivd[q] > 0) {
                                 double si = 1.0 / std::sqrt(ivd[q]);
@@ -159,6 +184,11 @@ extern "C" int orc_fit_all_stars(const cpb_psf_desc* desc, const cpb_lm_params* 
                         }
                     d[0] = qv * inv_flux;
                     if (den > 0 && ncl > 0 && ndi > 0) d[3] = 2.5 * std::log10(ndi / ncl);
+                    if (have_spread && Sp > 0) {
+                        d[4] = Sq / Sp - Sq0 / Sp0;
+                        if (inv_var)
+                            d[5] = std::sqrt(std::max(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
+                    }
                     if (inv_var) {
                         d[1] = std::sqrt(2.0 / M_PI) * ss * inv_flux;
                         if (ss2 > 0 && ng > nf) {
@@ -182,10 +212,12 @@ extern "C" int orc_fit_all_stars(const cpb_psf_desc* desc, const cpb_lm_params* 
         out->valid[s] = valid[s];
         out->chisq[s] = chisq[s];
         out->n_iter[s] = niter[s];
-        if (out->qfit) out->qfit[s] = diag[s * 4];
-        if (out->qfit_expected) out->qfit_expected[s] = diag[s * 4 + 1];
-        if (out->qfit_z) out->qfit_z[s] = diag[s * 4 + 2];
-        if (out->crowding) out->crowding[s] = diag[s * 4 + 3];
+        if (out->qfit) out->qfit[s] = diag[s * 6];
+        if (out->qfit_expected) out->qfit_expected[s] = diag[s * 6 + 1];
+        if (out->qfit_z) out->qfit_z[s] = diag[s * 6 + 2];
+        if (out->crowding) out->crowding[s] = diag[s * 6 + 3];
+        if (out->spread_model) out->spread_model[s] = diag[s * 6 + 4];
+        if (out->spread_model_err) out->spread_model_err[s] = diag[s * 6 + 5];
     }
     if (out->residual) std::memcpy(out->residual, resid.data(), sizeof(double) * npix);
     out->n_passes = n_passes;

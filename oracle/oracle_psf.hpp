@@ -83,4 +83,14 @@ void grid_corners_dw(const Psf& psf, double Y, double X, Corner c[4]);
 double evaluate(const Psf& psf, const StarP& s, double py, double px);
 double evaluate_fg(const Psf& psf, const StarP& s, double py, double px, double g[3]);
 
+// spread_model pieces (oracle_spread.cpp): the band-limited exponential-disk
+// kernel, the PSF's Gaussian-equivalent FWHM at (Y, X), the kernel of one fit
+// (param NaN: the PSF-derived width; false: spread_model off) and the
+// zero-border correlation of an h x w column-major stamp.
+void exp_disk_kernel(double fwhm, int half, std::vector<double>& K);
+double spread_fwhm(const Psf& psf, double Y, double X);
+bool spread_kernel(const Psf& psf, double param, double y1, double x1, double fit_rad, std::vector<double>& K,
+                   int& half);
+void correlate_zero(const double* ms, int h, int w, const std::vector<double>& K, int half, double* g);
+
 }  // namespace orc

@@ -677,6 +677,8 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
         if (out->qfit_expected) out->qfit_expected[i] = kNaN;
         if (out->qfit_z) out->qfit_z[i] = kNaN;
         if (out->crowding) out->crowding[i] = kNaN;
+        if (out->spread_model) out->spread_model[i] = kNaN;
+        if (out->spread_model_err) out->spread_model_err[i] = kNaN;
     };
     if (n_stars == 0) {
         out->n_passes = 0;
@@ -1093,6 +1095,12 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
         if (out->chisq) out->chisq[i] = 0.0;
         put_nan_diag(i);
     }
+    // spread_model reference disk: one field-constant kernel sized from the
+    // catalogue's first star (:1361-1365)
+    std::vector<double> spread_K;
+    int spread_half = 0;
+    const bool have_spread =
+        spread_kernel(psf, P->spread_model_fwhm, y0[0], x0[0], P->fit_rad, spread_K, spread_half);
     // per-star diagnostics (:1382-1397 chisq; psf_photometry_diagnostics.jl:154-231)
     for (int64_t j = 0; j < n_act; ++j) {
         int64_t i = active[j];
@@ -1107,16 +1115,27 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
         xlo = std::max<int64_t>(xlo, 1);
         xhi = std::min<int64_t>(xhi, nx);
         if (ylo > yhi || xlo > xhi) continue;
-        // _star_diagnostics! (qfit, qfit_expected, qfit_z, crowding)
+        // _star_diagnostics! (qfit, qfit_expected, qfit_z, crowding, spread_model)
         double flux = s.flux, bkg = s.bkg;
         if (flux > 0) {
+            const int h = (int)(yhi - ylo + 1), w = (int)(xhi - xlo + 1);
+            std::vector<double> ms((size_t)h * w), gs;
+            for (int c = 0; c < w; ++c)
+                for (int r = 0; r < h; ++r) ms[r + (size_t)c * h] = evaluate(psf, s, (double)(ylo + r), (double)(xlo + c));
+            const bool do_spread = have_spread;
+            if (do_spread) {
+                gs.resize(ms.size());
+                correlate_zero(ms.data(), h, w, spread_K, spread_half, gs.data());
+            }
             double inv_flux = 1.0 / flux, qv = 0, num_clean = 0, num_dirty = 0, den = 0;
+            double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
             double sig_sum = 0, sig2_sum = 0;
             int64_t ngood = 0;
             for (int64_t gx = xlo; gx <= xhi; ++gx)
                 for (int64_t gy = ylo; gy <= yhi; ++gy) {
                     int64_t q = (gy - 1) + (gx - 1) * ny;
-                    double mv = evaluate(psf, s, (double)gy, (double)gx);
+                    const size_t e = (size_t)(gy - ylo) + (size_t)(gx - xlo) * h;
+                    double mv = ms[e];
                     double wp = inv_var ? load(inv_var, eltype, q) : 1.0;
                     if (std::isfinite(wp) && wp > 0) {
                         qv += std::fabs(resid[q]);
@@ -1127,6 +1146,14 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
                         double img = load(image, eltype, q) - (background ? load(background, eltype, q) : 0.0);
                         num_dirty += wP * (img - bkg);
                         den += wP * Pp;
+                        if (do_spread) {
+                            double g_i = (gs[e] - bkg) * inv_flux;
+                            Sp += wP * p_i;
+                            Sq += wp * g_i * p_i;
+                            Sp0 += wP * Pp;
+                            Sq0 += wp * Pp * g_i;
+                            SqG += wp * g_i * g_i;
+                        }
                     }
                     if (inv_var) {
                         double iv = load(inv_var, eltype, q);
@@ -1141,6 +1168,13 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
             if (out->qfit) out->qfit[i] = qv * inv_flux;
             if (out->crowding && den > 0 && num_clean > 0 && num_dirty > 0)
                 out->crowding[i] = 2.5 * std::log10(num_dirty / num_clean);
+            if (do_spread && Sp > 0) {
+                if (out->spread_model) out->spread_model[i] = Sq / Sp - Sq0 / Sp0;
+                if (inv_var && out->spread_model_err) {
+                    double v = Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0;
+                    out->spread_model_err[i] = std::sqrt(std::max(0.0, v)) / (Sp * Sp);
+                }
+            }
             if (inv_var) {
                 if (out->qfit_expected) out->qfit_expected[i] = std::sqrt(2.0 / M_PI) * sig_sum * inv_flux;
                 if (out->qfit_z && sig2_sum > 0 && ngood > p) {

@@ -26,8 +26,11 @@ def compare(g, o, rtol=1e-8):
         np.testing.assert_allclose(getattr(g, k)[ok], getattr(o, k)[ok], rtol=0, atol=1e-7)
     for k in ("flux", "bkg", "flux_err", "y_err", "chisq"):
         np.testing.assert_allclose(getattr(g, k)[ok], getattr(o, k)[ok], rtol=rtol, atol=1e-10)
-    for k in ("qfit", "qfit_expected", "qfit_z", "crowding"):
+    for k in ("qfit", "qfit_expected", "qfit_z", "crowding", "spread_model_err"):
         np.testing.assert_allclose(getattr(g, k)[ok], getattr(o, k)[ok], rtol=1e-6, atol=1e-10)
+    # spread_model is a difference of two ratios near 1 (about 0 for a point source)
+    np.testing.assert_allclose(g.spread_model[ok], o.spread_model[ok], rtol=1e-6, atol=1e-8)
+    assert np.array_equal(np.isnan(g.spread_model), np.isnan(o.spread_model))
 
 
 def test_crowded_epsf_three_passes():
@@ -61,3 +64,32 @@ def test_gaussian_noiseless_and_edge_cases():
     assert r.flux.size == 0
     with pytest.raises(ArgumentError, match="n_passes"):
         cpb.fit_all_stars(img, psf, src, 5, n_passes=0)
+
+
+def test_spread_model_known_answers_and_wide_boxes():
+    """The reference's spread_model expectations (test/photometry/psf_photometry_single.jl:
+    269-321) on the device, each against the oracle; a 30 px fit radius (model stamps
+    of 63 x 63 per warp, fewer warps per block) and the off switch."""
+    from test_oracle_spread import CAT, FW, KW, PSF, _img
+    iv = np.full((60, 60), 1 / 20.0)
+    sm = []
+    for w in (2.5, 3.0, 4.0, 6.0):
+        img = _img((60, 60), 30.4, 29.7, w, 5000.0)
+        g = cpb.fit_all_stars(img, PSF, CAT, 8, inv_var=iv, **KW)
+        compare(g, orc_fit_all_stars(img, PSF, CAT, 8, inv_var=iv, **KW))
+        sm.append(g.spread_model[0])
+    assert abs(sm[0]) < 3e-3 and all(s > 5e-4 for s in sm[1:]) and sm == sorted(sm)
+    img = _img((60, 60), 30.4, 29.7, 4.0, 5000.0)
+    g = cpb.fit_all_stars(img, PSF, CAT, 8, inv_var=iv, spread_model_fwhm=8.0, **KW)
+    compare(g, orc_fit_all_stars(img, PSF, CAT, 8, inv_var=iv, spread_model_fwhm=8.0, **KW))
+    assert g.spread_model[0] > sm[2]
+    g = cpb.fit_all_stars(img, PSF, CAT, 8, inv_var=iv, spread_model_fwhm=0.0, **KW)
+    assert np.isnan(g.spread_model[0]) and np.isnan(g.spread_model_err[0]) and np.isfinite(g.qfit[0])
+    g = cpb.fit_all_stars(img, PSF, CAT, 8, **KW)
+    assert np.isfinite(g.spread_model[0]) and np.isnan(g.spread_model_err[0])
+    big, src = field((160, 160), 4, 5, min_sep=40, border=35)
+    kw = dict(n_passes=2, max_iter=100, fixed={"bkg": 20.0}, inv_var=np.ones(big.shape))
+    g = cpb.fit_all_stars(big, CircularGaussianPSF(fwhm=2.0), src, 30, **kw)
+    o = orc_fit_all_stars(big, CircularGaussianPSF(fwhm=2.0), src, 30, **kw)
+    assert np.all(np.isfinite(g.spread_model[g.valid]))
+    compare(g, o)

@@ -137,6 +137,9 @@ def test_errors_chisq_qfit_match_oracle():
     np.testing.assert_allclose(g.y_err[same], o.y_err[same], rtol=1e-4)
     np.testing.assert_allclose(g.chisq[same], o.chisq[same], rtol=1e-3)
     np.testing.assert_allclose(g.qfit[same], o.qfit[same], rtol=1e-3)
+    assert np.isfinite(g.spread_model[same]).all()
+    np.testing.assert_allclose(g.spread_model[same], o.spread_model[same], rtol=0, atol=1e-4)
+    np.testing.assert_allclose(g.spread_model_err[same], o.spread_model_err[same], rtol=1e-3)
 
 
 def test_contract_errors_empty_and_failures_on_device():
@@ -234,3 +237,94 @@ def test_model_rad_auto_radii_bit_exact_and_parity(case):
     assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
     assert len(np.unique(o.debug["model_R"])) > 1  # radii really vary with flux
     assert_parity(g, o, min_same_frac=0.8)
+
+
+def test_spread_model_parity_and_sequential_agreement():
+    """spread_model on the device: the reference's simultaneous-vs-sequential test
+    (test/photometry/psf_photometry_simultaneous.jl:356-383), the ePSF path (the disk
+    width from the gridded PSF's effective area) against the oracle, a 30 px fit
+    radius and the off switch."""
+    from test_oracle_spread import FW, PSF
+    img = np.full((90, 90), 20.0)
+    pts = [(20.5, 20.5), (20.5, 68.5), (68.5, 20.5)]
+    for (yy, xx) in pts:
+        render_sources(img, PSF, np.array([yy]), np.array([xx]), np.array([4000.0]), model_radius=40)
+    render_sources(img, CircularGaussianPSF(fwhm=5.0), np.array([68.5]), np.array([68.5]), np.array([4000.0]),
+                   model_radius=40)
+    sub = img - 20.0
+    cat = dict(y=np.array([p[0] for p in pts] + [68.5]), x=np.array([p[1] for p in pts] + [68.5]),
+               flux=np.full(4, 4000.0))
+    iv = np.full(img.shape, 1 / 20.0)
+    fixed = {"fwhm": FW, "bkg": 0.0}
+    rseq = cpb.fit_all_stars(sub, PSF, cat, 7, fixed=fixed, n_passes=3, max_iter=100, inv_var=iv)
+    rsim = cpb.fit_all_stars_simultaneous(sub, PSF, cat, 7, fixed=fixed, max_iter=40, inv_var=iv)
+    osim = orc_fit_simultaneous(sub, PSF, cat, 7, fixed=fixed, max_iter=40, inv_var=iv)
+    np.testing.assert_allclose(rsim.spread_model, osim.spread_model, rtol=0, atol=1e-6)
+    np.testing.assert_allclose(rsim.spread_model_err, osim.spread_model_err, rtol=1e-5)
+    for i in range(3):
+        assert abs(rseq.spread_model[i]) < 3e-3 and abs(rsim.spread_model[i]) < 3e-3
+        assert abs(rseq.spread_model[i] - rsim.spread_model[i]) < 2e-3
+    assert rseq.spread_model[3] > 5e-3 and rsim.spread_model[3] > 5e-3
+    off = cpb.fit_all_stars_simultaneous(sub, PSF, cat, 7, fixed=fixed, max_iter=40, inv_var=iv, spread_model_fwhm=0)
+    assert np.isnan(off.spread_model).all() and np.isfinite(off.qfit).all()
+    # ePSF, float32, crowded; and a 30 px fit radius
+    psf = moffat_epsf()
+    img, bkg, iv, truth, init = crowded_field(128, 128, 200, seed=1009, psf=psf, dtype=np.float32)
+    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=12, max_iter=10)
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, 12, **kw)
+    o = orc_fit_simultaneous(img, psf, init, 12, **kw)
+    both, same, *_ = parity_report(g, o)
+    assert np.isfinite(g.spread_model[same]).all()
+    np.testing.assert_allclose(g.spread_model[same], o.spread_model[same], rtol=0, atol=1e-4)
+    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=30, max_iter=3)
+    sel = {k: np.asarray(v)[:12] for k, v in init.items()}
+    g = cpb.fit_all_stars_simultaneous(img, psf, sel, 30, **kw)
+    o = orc_fit_simultaneous(img, psf, sel, 30, **kw)
+    both, same, *_ = parity_report(g, o)
+    assert same.sum() > 0
+    np.testing.assert_allclose(g.spread_model[same], o.spread_model[same], rtol=0, atol=1e-4)
+
+
+def four_node_epsf():
+    """A 2 x 2 grid of Moffat ePSF nodes (FWHM 2.4 .. 3.2 px) over a 128^2 field: the
+    general (several-node) stamp path."""
+    nodes = [moffat_epsf(fwhm=f, size=121).psfs[0] for f in (2.4, 2.8, 2.8, 3.2)]
+    return cpb.GriddedPSFModel(nodes, [20.0, 20.0, 110.0, 110.0], [20.0, 110.0, 20.0, 110.0])
+
+
+def test_four_node_gridded_parity_and_large_radii():
+    """Multi-node GriddedPSFModel against the oracle: the block-per-star stamp kernels,
+    spread_model from the blended PSF's effective area; then a 26 px fit radius and a
+    50 px model radius (the 512-thread stamp kernel and the value-only render)."""
+    from oracle import orc_psf_eval
+    psf = four_node_epsf()
+    rng = np.random.default_rng(1013)
+    n, shape = 150, (128, 128)
+    src = simulate_sources(shape, n, rng=rng, flux=(3e2, 3e4), flux_distribution="loguniform")
+    model = np.zeros(shape)
+    for y, x, f in zip(src["y"], src["x"], src["flux"]):
+        ya, yb = max(int(y) - 15, 1), min(int(y) + 15, shape[0])
+        xa, xb = max(int(x) - 15, 1), min(int(x) + 15, shape[1])
+        yy, xx = np.meshgrid(np.arange(ya, yb + 1), np.arange(xa, xb + 1), indexing="ij")
+        v = orc_psf_eval(psf, y, x, f, 0.0, yy.ravel().astype(float), xx.ravel().astype(float), grad=False)
+        model[ya - 1:yb, xa - 1:xb] += v.reshape(yy.shape)
+    bkg = np.full(shape, 50.0)
+    img = add_noise(model + bkg, rng=rng, noise="poisson", gain=1.0)
+    iv = 1.0 / (bkg + model)
+    init = dict(y=src["y"] + rng.normal(0, 0.3, n), x=src["x"] + rng.normal(0, 0.3, n),
+                flux=src["flux"] * rng.uniform(0.9, 1.1, n))
+    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=12, max_iter=12, debug=True)
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, 8, **kw)
+    o = orc_fit_simultaneous(img, psf, init, 8, **kw)
+    assert np.array_equal(g.debug["active"], o.debug["active"])
+    assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
+    assert_parity(g, o, min_same_frac=0.8)
+    both, same, *_ = parity_report(g, o)
+    np.testing.assert_allclose(g.spread_model[same], o.spread_model[same], rtol=0, atol=1e-4)
+    sel = {k: np.asarray(v)[:10] for k, v in init.items()}
+    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=50, max_iter=10, debug=True)
+    g = cpb.fit_all_stars_simultaneous(img, psf, sel, 26, **kw)
+    o = orc_fit_simultaneous(img, psf, sel, 26, **kw)
+    assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
+    assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
+    assert_parity(g, o, min_same_frac=0.5)
