@@ -269,34 +269,133 @@ __device__ __forceinline__ T warp_max(T v) {
     return v;
 }
 
-// The spread_model reference convolution of a star's model stamp (correlate!
-// with a zero border, correlation.jl:122-141) at stamp pixel (r, c): ms is the
-// bh x bw stamp (column-major), K the (2 kh + 1)^2 kernel.
-__device__ __forceinline__ double spread_conv(const double* ms, int bh, int bw, int r, int c,
-                                              const double* __restrict__ K, int kh) {
-    const int n = 2 * kh + 1;
-    double g = 0.0;
-    for (int q = -kh; q <= kh; ++q) {
-        const int cc = c + q;
-        if (cc < 0 || cc >= bw) continue;
-        for (int p = -kh; p <= kh; ++p) {
-            const int rr = r + p;
-            if (rr < 0 || rr >= bh) continue;
-            g += K[(p + kh) + (q + kh) * n] * ms[rr + cc * bh];
+// The spread_model reference disk on the device.  The band-limited disk is a
+// sum of six separable Gaussian-mixture components, K = sum_c alpha_c I_c I_c',
+// with I_c zero beyond |m| = L_c (the reference's overflow cutoff), so the
+// zero-border correlation (correlate!(g, ms, K, :zero), correlation.jl:122-141)
+// is run as one x pass and one y pass per component -- sum_c 2 (2 L_c + 1)
+// multiply-adds a pixel instead of (2 kh + 1)^2.
+struct SpreadDev {
+    const double* I;  // 6 x (2 kh + 1), I_c(m) at c * (2 kh + 1) + m + kh
+    double alpha[6];  // a_c / (sum of the unnormalised kernel)
+    int L[6];         // support half-width of I_c (<= kh)
+    int kh;
+};
+
+// G = K correlated with the bh x bw column-major stamp M (zero border), by the
+// whole block (every thread calls it); T and G are block scratch of bh * bw
+// doubles each.  Ends with a barrier: G is complete on return.
+__device__ __forceinline__ void spread_stamp_block(const SpreadDev& D, const double* M, double* T, double* G, int bh,
+                                                   int bw) {
+    const int nb = bh * bw, n = 2 * D.kh + 1;
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) G[e] = 0.0;
+    for (int c = 0; c < 6; ++c) {
+        const int L = D.L[c];
+        const double* I = D.I + c * n + D.kh;
+        __syncthreads();
+        for (int e = threadIdx.x; e < nb; e += blockDim.x) {  // x pass
+            const int r = e % bh, col = e / bh;
+            const int q0 = max(-L, -col), q1 = min(L, bw - 1 - col);
+            double t = 0.0;
+            for (int q = q0; q <= q1; ++q) t += I[q] * M[r + (col + q) * bh];
+            T[e] = t;
         }
+        __syncthreads();
+        for (int e = threadIdx.x; e < nb; e += blockDim.x) {  // y pass
+            const int r = e % bh, col = e / bh;
+            const int p0 = max(-L, -r), p1 = min(L, bh - 1 - r);
+            double t = 0.0;
+            for (int p = p0; p <= p1; ++p) t += I[p] * T[r + p + col * bh];
+            G[e] += D.alpha[c] * t;
+        }
+    }
+    __syncthreads();
+}
+
+// Block-wide sums of K values in a fixed order (warp sums, then the warps in
+// index order); results valid in thread 0.  sh: K * (blockDim.x / 32) doubles.
+template <int K>
+__device__ __forceinline__ void block_sum_n(double (&v)[K], double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) sh[wid * K + k] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double t = 0.0;
+            for (int w2 = 0; w2 < nw; ++w2) t += sh[w2 * K + k];
+            v[k] = t;
+        }
+    }
+}
+
+// The x pass of all six components at once (each stamp value is loaded once
+// for every component whose support reaches it): T[c * ld + e] = sum_q
+// I_c(q) M[r, col + q] over the in-box columns, e = r + col * bh.  Is: the six
+// profiles in shared memory, 6 x (2 kh + 1).  The y pass and the weighting are
+// spread_ypass at each pixel.  No barrier inside.
+__device__ __forceinline__ void spread_xpass_all(const SpreadDev& D, const double* Is, const double* M, double* T,
+                                                 int ld, int bh, int bw) {
+    const int n = 2 * D.kh + 1, nb = bh * bw;
+    int Lmax = 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) Lmax = max(Lmax, D.L[c]);
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+        const int r = e % bh, col = e / bh;
+        const int q0 = max(-Lmax, -col), q1 = min(Lmax, bw - 1 - col);
+        double t[6] = {0, 0, 0, 0, 0, 0};
+        for (int q = q0; q <= q1; ++q) {
+            const double m = M[r + (col + q) * bh];
+            const int aq = q < 0 ? -q : q;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                if (aq <= D.L[c]) t[c] += Is[c * n + D.kh + q] * m;
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c) T[c * ld + e] = t[c];
+    }
+}
+
+// The disk-correlated stamp value at pixel e = r + col * bh from the x-pass
+// planes T (component c at T + c * ld): sum_c alpha_c sum_p I_c(p) T_c[r + p, col].
+__device__ __forceinline__ double spread_ypass(const SpreadDev& D, const double* Is, const double* T, int ld, int bh,
+                                               int e) {
+    const int n = 2 * D.kh + 1, r = e % bh;
+    double g = 0.0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const int L = D.L[c];
+        const int p0 = max(-L, -r), p1 = min(L, bh - 1 - r);
+        const double* I = Is + c * n + D.kh;
+        const double* Tc = T + c * ld + e;
+        double t = 0.0;
+        for (int p = p0; p <= p1; ++p) t += I[p] * Tc[p];
+        g += D.alpha[c] * t;
     }
     return g;
 }
 
-// Warps per block of a diagnostics launch that keeps one boxmax-double model
-// stamp per warp in shared memory (8, fewer for large fit radii); boxes above
-// the 200 KB a single warp may take (fit_rad beyond ~80 px) leave spread_model
-// NaN (spread_fits_smem false, K not uploaded).
-inline bool spread_fits_smem(int boxmax) { return (size_t)boxmax * sizeof(double) <= 200 * 1024; }
-inline int diag_warps_per_block(const void* K, int boxmax) {
-    if (!K) return 8;
-    const size_t per = (size_t)boxmax * sizeof(double);
-    return (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / per));
+// Threads of a diagnostics block (one block a star) and its shared memory when
+// spread_model is on.  Mode 1 (the usual): the model stamp, six x-pass planes
+// and the profiles, (7 boxmax + 6 (2 kh + 1)) doubles; mode 2 (large boxes):
+// the model stamp, one x-pass plane and the correlated stamp, one component at
+// a time, 3 boxmax doubles.  Boxes beyond both within 200 KB (fit_rad above
+// ~45 px) leave spread_model NaN (mode 0).
+constexpr int kDiagThreads = 256;
+inline size_t spread_smem_bytes(int mode, int boxmax, int kh) {
+    return mode == 1 ? ((size_t)7 * boxmax + 6 * (2 * (size_t)kh + 1)) * sizeof(double)
+                     : (mode == 2 ? (size_t)3 * boxmax * sizeof(double) : 0);
+}
+inline int spread_mode(int boxmax, int kh) {
+    if (spread_smem_bytes(1, boxmax, kh) <= 200 * 1024) return 1;
+    if (spread_smem_bytes(2, boxmax, kh) <= 200 * 1024) return 2;
+    return 0;
 }
 
 }  // namespace cpb
@@ -445,10 +544,17 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
 void model_radii_auto(const cpb_psf* psf, double fwhm, double nsigma, int R_fit, int R_cap,
                       std::vector<double>& w_sample, const std::vector<double>& flux, std::vector<int32_t>& out);
 
-// spread_model reference disk (cpb_spread.cu): the (2 half + 1)^2 kernel, false
+// spread_model reference disk (cpb_spread.cu): the separable components of
+// the band-limited exponential disk with support half = ceil(fit_rad); false
 // when spread_model is off.
+struct SpreadHost {
+    int kh = 0;
+    std::vector<double> I;  // 6 x (2 kh + 1)
+    double alpha[6] = {0, 0, 0, 0, 0, 0};
+    int L[6] = {0, 0, 0, 0, 0, 0};
+};
 bool spread_kernel(const cpb_psf* psf, double psf_fwhm, double param, double y1, double x1, double fit_rad,
-                   std::vector<double>& K, int& half);
+                   SpreadHost& out);
 
 // Batched simultaneous fits of small groups (cpb_groups.cu).  Device inputs and
 // outputs; the h_*_opt arrays (nullable) are host copies of the group metadata.

@@ -86,98 +86,104 @@ __global__ void k_mp_cutouts(int nL, const int4* __restrict__ boxes, const int64
 // _star_diagnostics! (psf_photometry_diagnostics.jl:154-231) over the fitted
 // box: image is the original data, residual the star's fit residual (every
 // model subtracted, its own included), star_model its best-fit render, kept in
-// the warp's shared-memory slice (boxmax doubles) for the spread_model
-// convolution (K null: spread_model off).  out: qfit, qfit_expected, qfit_z,
-// crowding, spread_model, spread_model_err per star (NaN where undefined).
+// shared memory with its disk-correlated copy for spread_model (D.I null:
+// spread_model off).  One block of kDiagThreads a star (grid-stride).  out:
+// qfit, qfit_expected, qfit_z, crowding, spread_model, spread_model_err per
+// star (NaN where undefined).
 template <typename TI>
-__global__ void k_mp_diag(int nL, const int4* __restrict__ boxes, const double* __restrict__ params,
-                          const uint8_t* __restrict__ flags, const TI* __restrict__ img,
-                          const double* __restrict__ residual, const TI* __restrict__ iv, DevPsf P, MPConst M,
-                          int n_free, int ny, const double* __restrict__ K, int kh, int boxmax,
-                          double* __restrict__ out) {
-    extern __shared__ double ms_all[];
-    const int lane = threadIdx.x & 31;
-    const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-    if (s >= nL) return;
-    double* ms = ms_all + (threadIdx.x >> 5) * boxmax;
+__global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4* __restrict__ boxes,
+                                                         const double* __restrict__ params,
+                                                         const uint8_t* __restrict__ flags,
+                                                         const TI* __restrict__ img,
+                                                         const double* __restrict__ residual,
+                                                         const TI* __restrict__ iv, DevPsf P, MPConst M, int n_free,
+                                                         int ny, SpreadDev D, int smode, int boxmax, double* __restrict__ out) {
+    extern __shared__ double stamp[];  // model stamp, x-pass scratch, disk-correlated stamp
+    __shared__ double red[12 * (kDiagThreads / 32)];
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
-    double* o = out + (int64_t)s * 6;
-    const double* pr = params + (int64_t)s * M.np;
-    const double flux = pr[M.rf], bkg = pr[M.rb];
-    if (!flags[s] || !(flux > 0)) {
-        if (lane == 0) o[0] = o[1] = o[2] = o[3] = o[4] = o[5] = NaN;
-        return;
-    }
-    const int4 b = boxes[s];
-    const int nb = b.z * b.w;
-    const bool spread = K != nullptr && nb <= boxmax;
-    if (spread) {
-        for (int e = lane; e < nb; e += 32) ms[e] = mp_model(P, M, pr, b.x + e % b.z, b.y + e / b.z);
-        __syncwarp();
-    }
-    const double inv_flux = 1.0 / flux;
-    double qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
-    double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
-    int ngood = 0;
-    for (int e = lane; e < nb; e += 32) {
-        const int i = b.x + e % b.z, j = b.y + e / b.z;
-        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
-        const double mv = spread ? ms[e] : mp_model(P, M, pr, i, j);
-        const double wp = iv ? (double)iv[q] : 1.0;
-        if (isfinite(wp) && wp > 0) {
-            const double r = residual[q];
-            qv += fabs(r);
-            const double Pp = (mv - bkg) * inv_flux;
-            const double wP = wp * Pp;
-            const double p_i = r + mv - bkg;
-            ncl += wP * p_i;
-            ndi += wP * ((double)img[q] - bkg);
-            den += wP * Pp;
-            if (spread) {
-                const double g_i = (spread_conv(ms, b.z, b.w, e % b.z, e / b.z, K, kh) - bkg) * inv_flux;
-                Sp += wP * p_i;
-                Sq += wp * g_i * p_i;
-                Sp0 += wP * Pp;
-                Sq0 += wp * Pp * g_i;
-                SqG += wp * g_i * g_i;
+    const int mode = D.I ? smode : 0;
+    double* Is = stamp + 7 * boxmax;  // mode 1: the six profiles
+    if (mode == 1)
+        for (int i = threadIdx.x; i < 6 * (2 * D.kh + 1); i += blockDim.x) Is[i] = D.I[i];
+    for (int s = blockIdx.x; s < nL; s += gridDim.x) {
+        __syncthreads();  // the previous star's stamps are no longer read
+        double* o = out + (int64_t)s * 6;
+        const double* pr = params + (int64_t)s * M.np;
+        const double flux = pr[M.rf], bkg = pr[M.rb];
+        if (!flags[s] || !(flux > 0)) {
+            if (threadIdx.x == 0) o[0] = o[1] = o[2] = o[3] = o[4] = o[5] = NaN;
+            continue;
+        }
+        const int4 b = boxes[s];
+        const int nb = b.z * b.w;
+        const bool spread = mode != 0 && nb <= boxmax;
+        double* G = stamp + 2 * boxmax;  // mode 2: the correlated stamp
+        if (spread) {
+            for (int e = threadIdx.x; e < nb; e += blockDim.x) stamp[e] = mp_model(P, M, pr, b.x + e % b.z, b.y + e / b.z);
+            __syncthreads();
+            if (mode == 1) {
+                spread_xpass_all(D, Is, stamp, stamp + boxmax, boxmax, b.z, b.w);
+                __syncthreads();
+            } else {
+                spread_stamp_block(D, stamp, stamp + boxmax, G, b.z, b.w);
             }
         }
-        if (iv) {
-            const double v = (double)iv[q];
-            if (isfinite(v) && v > 0) {
-                const double si = 1.0 / sqrt(v);
-                ss += si;
-                ss2 += si * si;
-                ngood += 1;
+        const double inv_flux = 1.0 / flux;
+        // qv ncl ndi den ss ss2 Sp Sq Sp0 Sq0 SqG ngood
+        double v[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+            const int i = b.x + e % b.z, j = b.y + e / b.z;
+            const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
+            const double wp = iv ? (double)iv[q] : 1.0;
+            if (isfinite(wp) && wp > 0) {
+                const double mv = spread ? stamp[e] : mp_model(P, M, pr, i, j);
+                const double r = residual[q];
+                v[0] += fabs(r);
+                const double Pp = (mv - bkg) * inv_flux;
+                const double wP = wp * Pp;
+                const double p_i = r + mv - bkg;
+                v[1] += wP * p_i;
+                v[2] += wP * ((double)img[q] - bkg);
+                v[3] += wP * Pp;
+                if (spread) {
+                    const double gm = mode == 1 ? spread_ypass(D, Is, stamp + boxmax, boxmax, b.z, e) : G[e];
+                    const double g_i = (gm - bkg) * inv_flux;
+                    v[6] += wP * p_i;
+                    v[7] += wp * g_i * p_i;
+                    v[8] += wP * Pp;
+                    v[9] += wp * Pp * g_i;
+                    v[10] += wp * g_i * g_i;
+                }
+            }
+            if (iv) {
+                const double vq = (double)iv[q];
+                if (isfinite(vq) && vq > 0) {
+                    const double si = 1.0 / sqrt(vq);
+                    v[4] += si;
+                    v[5] += si * si;
+                    v[11] += 1.0;
+                }
             }
         }
-    }
-    qv = warp_sum(qv);
-    ncl = warp_sum(ncl);
-    ndi = warp_sum(ndi);
-    den = warp_sum(den);
-    ss = warp_sum(ss);
-    ss2 = warp_sum(ss2);
-    Sp = warp_sum(Sp);
-    Sq = warp_sum(Sq);
-    Sp0 = warp_sum(Sp0);
-    Sq0 = warp_sum(Sq0);
-    SqG = warp_sum(SqG);
-    ngood = warp_sum(ngood);
-    if (lane == 0) {
-        const double c2p = 0.7978845608028654;  // sqrt(2 / pi)
-        o[0] = qv * inv_flux;
-        o[3] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
-        o[1] = iv ? c2p * ss * inv_flux : NaN;
-        o[2] = NaN;
-        if (iv && ss2 > 0 && ngood > n_free) {
-            const double dfac = sqrt(1.0 - (double)n_free / (double)ngood);
-            o[2] = (qv - c2p * dfac * ss) / (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
-        }
-        o[4] = o[5] = NaN;
-        if (spread && Sp > 0) {
-            o[4] = Sq / Sp - Sq0 / Sp0;
-            if (iv) o[5] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
+        block_sum_n<12>(v, red);
+        if (threadIdx.x == 0) {
+            const double qv = v[0], ncl = v[1], ndi = v[2], den = v[3], ss = v[4], ss2 = v[5];
+            const double Sp = v[6], Sq = v[7], Sp0 = v[8], Sq0 = v[9], SqG = v[10];
+            const int ngood = (int)v[11];
+            const double c2p = 0.7978845608028654;  // sqrt(2 / pi)
+            o[0] = qv * inv_flux;
+            o[3] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
+            o[1] = iv ? c2p * ss * inv_flux : NaN;
+            o[2] = NaN;
+            if (iv && ss2 > 0 && ngood > n_free) {
+                const double dfac = sqrt(1.0 - (double)n_free / (double)ngood);
+                o[2] = (qv - c2p * dfac * ss) / (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
+            }
+            o[4] = o[5] = NaN;
+            if (spread && Sp > 0) {
+                o[4] = Sq / Sp - Sq0 / Sp0;
+                if (iv) o[5] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
+            }
         }
     }
 }
@@ -267,18 +273,19 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     int32_t* d_lmi = (int32_t*)scratch(ctx, "mp_lm_i32", sizeof(int32_t) * n * 2);
     double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 6);
     // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
-    std::vector<double> h_spread;
-    int kh = 0;
-    double* d_K = nullptr;
+    SpreadHost sh;
+    SpreadDev sd{};
     const int boxmax = (int)box_max;
-    if (spread_kernel(psf, psf->dev.fwhm, spread_model_fwhm, init[0], init[1], fit_rad, h_spread, kh) &&
-        spread_fits_smem(boxmax)) {
-        d_K = (double*)scratch(ctx, "mp_spread_K", sizeof(double) * h_spread.size());
-        check(cudaMemcpyAsync(d_K, h_spread.data(), sizeof(double) * h_spread.size(), cudaMemcpyHostToDevice, st),
-              "h2d");
+    int smode = 0;
+    if (spread_kernel(psf, psf->dev.fwhm, spread_model_fwhm, init[0], init[1], fit_rad, sh) &&
+        (smode = spread_mode(boxmax, sh.kh)) != 0) {
+        double* d_I = (double*)scratch(ctx, "mp_spread_I", sizeof(double) * sh.I.size());
+        check(cudaMemcpyAsync(d_I, sh.I.data(), sizeof(double) * sh.I.size(), cudaMemcpyHostToDevice, st), "h2d");
+        sd.I = d_I;
+        sd.kh = sh.kh;
+        for (int c = 0; c < 6; ++c) sd.alpha[c] = sh.alpha[c], sd.L[c] = sh.L[c];
     }
-    const int dwpb = diag_warps_per_block(d_K, boxmax);
-    const size_t diag_smem = d_K ? (size_t)dwpb * boxmax * sizeof(double) : 0;
+    const size_t diag_smem = spread_smem_bytes(smode, boxmax, sd.kh);
     if (diag_smem > 48 * 1024) {
         check(cudaFuncSetAttribute(k_mp_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
               "smem attr");
@@ -455,13 +462,13 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
                 KernelScope ks_(ctx, "k_mp_diag", (double)tot * (d_iv ? 24 : 16));
                 if (eltype == CPB_F64)
-                    k_mp_diag<double><<<(unsigned)((nL + dwpb - 1) / dwpb), 32 * dwpb, diag_smem, st>>>(
-                        nL, d_box, d_psub, d_flag, (const double*)d_img, resid, (const double*)d_iv, dp, M, nf, ny, d_K,
-                        kh, boxmax, d_diag);
+                    k_mp_diag<double><<<(unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16), kDiagThreads, diag_smem, st>>>(
+                        nL, d_box, d_psub, d_flag, (const double*)d_img, resid, (const double*)d_iv, dp, M, nf, ny, sd,
+                        smode, boxmax, d_diag);
                 else
-                    k_mp_diag<float><<<(unsigned)((nL + dwpb - 1) / dwpb), 32 * dwpb, diag_smem, st>>>(
-                        nL, d_box, d_psub, d_flag, (const float*)d_img, resid, (const float*)d_iv, dp, M, nf, ny, d_K,
-                        kh, boxmax, d_diag);
+                    k_mp_diag<float><<<(unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16), kDiagThreads, diag_smem, st>>>(
+                        nL, d_box, d_psub, d_flag, (const float*)d_img, resid, (const float*)d_iv, dp, M, nf, ny, sd,
+                        smode, boxmax, d_diag);
                 check(cudaGetLastError(), "k_mp_diag");
                 hdiag.resize((size_t)nL * 6);
                 check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * nL * 6, cudaMemcpyDeviceToHost, st), "d2h");

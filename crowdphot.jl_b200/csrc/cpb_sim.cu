@@ -1181,112 +1181,117 @@ __global__ void k_errors(int64_t n_act, int p, const double* gram, bool reweight
 }
 
 // chisq and the qfit / crowding / spread_model diagnostics per active star
-// (:1358-1397, psf_photometry_diagnostics.jl:154-231); one warp per star, the
-// star's model stamp over its box kept in the warp's slice of shared memory
-// (boxmax doubles) for the spread_model convolution (K null: spread_model off).
+// (:1358-1397, psf_photometry_diagnostics.jl:154-231); one block of
+// kDiagThreads a star (grid-stride), the star's model stamp over its box and
+// its disk-correlated copy kept in shared memory (D.I null: spread_model off).
 template <typename TI>
-__global__ void k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad, const StarCoef* __restrict__ coef,
-                       const double* __restrict__ resid, const TI* __restrict__ img, const TI* __restrict__ bkgimg,
-                       const TI* __restrict__ iv, const double* __restrict__ K, int kh, int boxmax,
-                       double* out /* n_act x 7: chisq qfit qfit_exp qfit_z crowding spread spread_err */) {
-    extern __shared__ double ms_all[];
-    const int lane = threadIdx.x & 31;
-    const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (j >= n_act) return;
-    double* ms = ms_all + (threadIdx.x >> 5) * boxmax;
-    const StarCoef c = coef[j];
+__global__ void __launch_bounds__(kDiagThreads, 3) k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad,
+                                                      const StarCoef* __restrict__ coef,
+                                                      const double* __restrict__ resid, const TI* __restrict__ img,
+                                                      const TI* __restrict__ bkgimg, const TI* __restrict__ iv,
+                                                      SpreadDev D, int smode, int boxmax,
+                                                      double* out /* n_act x 7: chisq qfit qfit_exp qfit_z crowding
+                                                                     spread spread_err */) {
+    extern __shared__ double stamp[];  // model stamp, x-pass scratch, disk-correlated stamp
+    __shared__ double red[14 * (kDiagThreads / 32)];
+    __shared__ StarCoef c;
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
-    double* o = out + j * 7;
-    const bool validp = isfinite(c.y) && isfinite(c.x) && isfinite(c.flux) && c.flux > 0;
-    if (!validp) {
-        if (lane == 0) {
-            o[0] = 0.0;
-            o[1] = o[2] = o[3] = o[4] = o[5] = o[6] = NaN;
+    const int mode = D.I ? smode : 0;
+    double* Is = stamp + 7 * boxmax;  // mode 1: the six profiles
+    if (mode == 1)
+        for (int i = threadIdx.x; i < 6 * (2 * D.kh + 1); i += blockDim.x) Is[i] = D.I[i];
+    for (int64_t j = blockIdx.x; j < n_act; j += gridDim.x) {
+        __syncthreads();  // the previous star's c and stamps are no longer read
+        if (threadIdx.x == 0) c = coef[j];
+        __syncthreads();
+        double* o = out + j * 7;
+        const bool validp = isfinite(c.y) && isfinite(c.x) && isfinite(c.flux) && c.flux > 0;
+        if (!validp) {
+            if (threadIdx.x == 0) {
+                o[0] = 0.0;
+                o[1] = o[2] = o[3] = o[4] = o[5] = o[6] = NaN;
+            }
+            continue;
         }
-        return;
-    }
-    int ylo = max((int)floor(c.y - fit_rad), 1), yhi = min((int)ceil(c.y + fit_rad), fc.ny);
-    int xlo = max((int)floor(c.x - fit_rad), 1), xhi = min((int)ceil(c.x + fit_rad), fc.nx);
-    double num = 0, qv = 0, ncl = 0, ndi = 0, den = 0, ss = 0, ss2 = 0;
-    double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
-    int ng = 0, ngi = 0;
-    const int h = yhi - ylo + 1, wd = xhi - xlo + 1;
-    const double inv_flux = 1.0 / c.flux;
-    const bool spread = K != nullptr && h > 0 && wd > 0 && h * wd <= boxmax;
-    if (h > 0 && wd > 0) {
+        const int ylo = max((int)floor(c.y - fit_rad), 1), yhi = min((int)ceil(c.y + fit_rad), fc.ny);
+        const int xlo = max((int)floor(c.x - fit_rad), 1), xhi = min((int)ceil(c.x + fit_rad), fc.nx);
+        const int h = max(yhi - ylo + 1, 0), wd = max(xhi - xlo + 1, 0);
+        const int nb = h * wd;
+        const double inv_flux = 1.0 / c.flux;
+        const bool spread = mode != 0 && nb > 0 && nb <= boxmax;
+        double* G = stamp + 2 * boxmax;  // mode 2: the correlated stamp
         if (spread) {
-            for (int e = lane; e < h * wd; e += 32)
-                ms[e] = model_value<double, double>(P, P.data64, c, (double)(ylo + e % h), (double)(xlo + e / h));
-            __syncwarp();
+            for (int e = threadIdx.x; e < nb; e += blockDim.x)
+                stamp[e] = model_value<double, double>(P, P.data64, c, (double)(ylo + e % h), (double)(xlo + e / h));
+            __syncthreads();
+            if (mode == 1) {
+                spread_xpass_all(D, Is, stamp, stamp + boxmax, boxmax, h, wd);
+                __syncthreads();
+            } else {
+                spread_stamp_block(D, stamp, stamp + boxmax, G, h, wd);
+            }
         }
-        for (int e = lane; e < h * wd; e += 32) {
+        // num qv ncl ndi den ss ss2 Sp Sq Sp0 Sq0 SqG ng ngi
+        double v[14] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int e = threadIdx.x; e < nb; e += blockDim.x) {
             const int gy = ylo + e % h, gx = xlo + e / h;
             const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
             const double r = resid[q];
             const double wp = iv ? (double)iv[q] : 1.0;
             if (isfinite(wp) && wp > 0) {
-                num += wp * (r * r);
-                ng += 1;
-                const double mv = spread ? ms[e] : model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
-                qv += fabs(r);
+                v[0] += wp * (r * r);
+                v[12] += 1.0;
+                const double mv = spread ? stamp[e] : model_value<double, double>(P, P.data64, c, (double)gy, (double)gx);
+                v[1] += fabs(r);
                 const double Pp = (mv - c.bkg) * inv_flux;
                 const double wP = wp * Pp;
                 const double p_i = r + mv - c.bkg;
-                ncl += wP * p_i;
+                v[2] += wP * p_i;
                 const double im = (double)img[q] - (bkgimg ? (double)bkgimg[q] : 0.0);
-                ndi += wP * (im - c.bkg);
-                den += wP * Pp;
+                v[3] += wP * (im - c.bkg);
+                v[4] += wP * Pp;
                 if (spread) {
-                    const double g_i = (spread_conv(ms, h, wd, e % h, e / h, K, kh) - c.bkg) * inv_flux;
-                    Sp += wP * p_i;
-                    Sq += wp * g_i * p_i;
-                    Sp0 += wP * Pp;
-                    Sq0 += wp * Pp * g_i;
-                    SqG += wp * g_i * g_i;
+                    const double gm = mode == 1 ? spread_ypass(D, Is, stamp + boxmax, boxmax, h, e) : G[e];
+                    const double g_i = (gm - c.bkg) * inv_flux;
+                    v[7] += wP * p_i;
+                    v[8] += wp * g_i * p_i;
+                    v[9] += wP * Pp;
+                    v[10] += wp * Pp * g_i;
+                    v[11] += wp * g_i * g_i;
                 }
                 if (iv) {
-                    double si = 1.0 / sqrt(wp);
-                    ss += si;
-                    ss2 += si * si;
-                    ngi += 1;
+                    const double si = 1.0 / sqrt(wp);
+                    v[5] += si;
+                    v[6] += si * si;
+                    v[13] += 1.0;
                 }
             }
         }
-    }
-    num = warp_sum(num);
-    qv = warp_sum(qv);
-    ncl = warp_sum(ncl);
-    ndi = warp_sum(ndi);
-    den = warp_sum(den);
-    ss = warp_sum(ss);
-    ss2 = warp_sum(ss2);
-    Sp = warp_sum(Sp);
-    Sq = warp_sum(Sq);
-    Sp0 = warp_sum(Sp0);
-    Sq0 = warp_sum(Sq0);
-    SqG = warp_sum(SqG);
-    ng = warp_sum(ng);
-    ngi = warp_sum(ngi);
-    if (lane == 0) {
-        o[0] = (ng - fc.p > 0) ? num / (double)(ng - fc.p) : 0.0;
-        o[1] = qv * inv_flux;
-        o[4] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
-        o[5] = o[6] = NaN;
-        if (spread && Sp > 0) {
-            o[5] = Sq / Sp - Sq0 / Sp0;
-            if (iv) o[6] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
-        }
-        if (iv) {
-            o[2] = sqrt(2.0 / 3.141592653589793) * ss * inv_flux;
-            if (ss2 > 0 && ngi > fc.p) {
-                double dfac = sqrt(1.0 - (double)fc.p / (double)ngi);
-                o[3] = (qv - sqrt(2.0 / 3.141592653589793) * dfac * ss) /
-                       (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
-            } else {
-                o[3] = NaN;
+        block_sum_n<14>(v, red);
+        if (threadIdx.x == 0) {
+            const double num = v[0], qv = v[1], ncl = v[2], ndi = v[3], den = v[4], ss = v[5], ss2 = v[6];
+            const double Sp = v[7], Sq = v[8], Sp0 = v[9], Sq0 = v[10], SqG = v[11];
+            const int ng = (int)v[12], ngi = (int)v[13];
+            o[0] = (ng - fc.p > 0) ? num / (double)(ng - fc.p) : 0.0;
+            o[1] = qv * inv_flux;
+            o[4] = (den > 0 && ncl > 0 && ndi > 0) ? 2.5 * log10(ndi / ncl) : NaN;
+            o[5] = o[6] = NaN;
+            if (spread && Sp > 0) {
+                o[5] = Sq / Sp - Sq0 / Sp0;
+                if (iv) o[6] = sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp);
             }
-        } else {
-            o[2] = o[3] = NaN;
+            if (iv) {
+                o[2] = sqrt(2.0 / 3.141592653589793) * ss * inv_flux;
+                if (ss2 > 0 && ngi > fc.p) {
+                    double dfac = sqrt(1.0 - (double)fc.p / (double)ngi);
+                    o[3] = (qv - sqrt(2.0 / 3.141592653589793) * dfac * ss) /
+                           (sqrt((1.0 - 2.0 / 3.141592653589793) * ss2) * dfac);
+                } else {
+                    o[3] = NaN;
+                }
+            } else {
+                o[2] = o[3] = NaN;
+            }
         }
     }
 }
@@ -2012,38 +2017,41 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         check(cudaGetLastError(), "k_gather_final");
     }
     // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
-    std::vector<double> h_spread;
-    int kh = 0;
-    double* d_K = nullptr;
-    {
-        if (spread_kernel(psf, psf->dev.fwhm, P->spread_model_fwhm, h_yx1[0], h_yx1[1], P->fit_rad, h_spread, kh) &&
-            spread_fits_smem((2 * (int)std::ceil(P->fit_rad) + 2) * (2 * (int)std::ceil(P->fit_rad) + 2))) {
-            d_K = S<double>(ctx, "spread_K", (int64_t)h_spread.size());
-            check(cudaMemcpyAsync(d_K, h_spread.data(), sizeof(double) * h_spread.size(), cudaMemcpyHostToDevice, st),
-                  "h2d");
-        }
-    }
+    SpreadHost sh;
+    SpreadDev sd{};
     const int boxmax = (2 * (int)std::ceil(P->fit_rad) + 2) * (2 * (int)std::ceil(P->fit_rad) + 2);
-    const int dwpb = diag_warps_per_block(d_K, boxmax);
-    const size_t diag_smem = d_K ? (size_t)dwpb * boxmax * sizeof(double) : 0;
-    const unsigned dgrid = (unsigned)std::max<int64_t>(1, (n_act + dwpb - 1) / dwpb);
-    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 7);
-    if (eltype == CPB_F64) {
-        if (diag_smem > 48 * 1024)
-            check(cudaFuncSetAttribute(k_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
-                  "smem attr");
-        k_diag<double><<<dgrid, 32 * dwpb, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
-                                                           (const double*)d_image, (const double*)d_background,
-                                                           (const double*)d_inv_var, d_K, kh, boxmax, diag);
-    } else {
-        if (diag_smem > 48 * 1024)
-            check(cudaFuncSetAttribute(k_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
-                  "smem attr");
-        k_diag<float><<<dgrid, 32 * dwpb, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
-                                                          (const float*)d_image, (const float*)d_background,
-                                                          (const float*)d_inv_var, d_K, kh, boxmax, diag);
+    int smode = 0;
+    if (spread_kernel(psf, psf->dev.fwhm, P->spread_model_fwhm, h_yx1[0], h_yx1[1], P->fit_rad, sh) &&
+        (smode = spread_mode(boxmax, sh.kh)) != 0) {
+        double* d_I = S<double>(ctx, "spread_I", (int64_t)sh.I.size());
+        check(cudaMemcpyAsync(d_I, sh.I.data(), sizeof(double) * sh.I.size(), cudaMemcpyHostToDevice, st), "h2d");
+        sd.I = d_I;
+        sd.kh = sh.kh;
+        for (int c = 0; c < 6; ++c) sd.alpha[c] = sh.alpha[c], sd.L[c] = sh.L[c];
     }
-    check(cudaGetLastError(), "k_diag");
+    const size_t diag_smem = spread_smem_bytes(smode, boxmax, sd.kh);
+    const unsigned dgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
+    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 7);
+    {
+        KernelScope ks_(ctx, "k_diag",
+                        (double)n_act * boxmax * (8.0 + (d_inv_var ? 2.0 : 1.0) * (eltype == CPB_F64 ? 8 : 4)));
+        if (eltype == CPB_F64) {
+            if (diag_smem > 48 * 1024)
+                check(cudaFuncSetAttribute(k_diag<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+                      "smem attr");
+            k_diag<double><<<dgrid, kDiagThreads, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
+                                                               (const double*)d_image, (const double*)d_background,
+                                                               (const double*)d_inv_var, sd, smode, boxmax, diag);
+        } else {
+            if (diag_smem > 48 * 1024)
+                check(cudaFuncSetAttribute(k_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
+                      "smem attr");
+            k_diag<float><<<dgrid, kDiagThreads, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
+                                                              (const float*)d_image, (const float*)d_background,
+                                                              (const float*)d_inv_var, sd, smode, boxmax, diag);
+        }
+        check(cudaGetLastError(), "k_diag");
+    }
     check(cudaEventRecord(ctx->ev1, st), "event");
 
     // ---- download and assemble (:1289-1300, :1331-1337, :1404-1430)

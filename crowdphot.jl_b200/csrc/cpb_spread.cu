@@ -82,18 +82,25 @@ double spread_fwhm(const cpb_psf* psf, double fwhm, double Y, double X) {
     return std::sqrt(ea * 2 * std::log(2.0) / kPi);
 }
 
-// _exp_disk_kernel_bandlimited(fwhm; half): (2 half + 1)^2, column-major, sum 1.
-void exp_disk_kernel(double fwhm, int half, std::vector<double>& K) {
+// The six band-limited component profiles I_c(m), m = -half..half, of
+// _exp_disk_kernel_bandlimited(fwhm; half), their support half-widths and the
+// weights alpha_c = a_c / total that make sum_c alpha_c I_c I_c' the kernel
+// normalised to sum 1.
+void exp_disk_components(double fwhm, int half, SpreadHost& S) {
     const int n = 2 * half + 1;
     const double re = fwhm / 16 * 1.67834699;
     std::vector<double> gx, gw;
     gauss_legendre(32, gx, gw);
     const int panels = std::max(4, 2 * half);
     const double hw = 0.5 / panels;  // half-width of one panel on [-1/2, 1/2]
-    K.assign((size_t)n * n, 0.0);
-    std::vector<double> Iv(n);
+    S.kh = half;
+    S.I.assign((size_t)6 * n, 0.0);
+    double total = 0;
     for (int c = 0; c < 6; ++c) {
         const double a = 2 * kPi * kPi * re * re * kExpVar[c];
+        double* Iv = S.I.data() + (size_t)c * n;
+        S.L[c] = 0;
+        double sum = 0;
         for (int m = -half; m <= half; ++m) {
             double I = 0;
             if (!(kPi * kPi * (double)m * m / a > 690)) {
@@ -106,13 +113,25 @@ void exp_disk_kernel(double fwhm, int half, std::vector<double>& K) {
                 }
             }
             Iv[m + half] = I;
+            if (I != 0.0) S.L[c] = std::max(S.L[c], std::abs(m));
+            sum += I;
         }
-        for (int jj = 0; jj < n; ++jj)
-            for (int ii = 0; ii < n; ++ii) K[ii + (size_t)jj * n] += kExpAmp[c] * Iv[ii] * Iv[jj];
+        total += kExpAmp[c] * sum * sum;
     }
-    double tot = 0;
-    for (double v : K) tot += v;
-    for (double& v : K) v /= tot;
+    for (int c = 0; c < 6; ++c) S.alpha[c] = kExpAmp[c] / total;
+}
+
+// _exp_disk_kernel_bandlimited(fwhm; half): (2 half + 1)^2, column-major, sum 1.
+void exp_disk_kernel(double fwhm, int half, std::vector<double>& K) {
+    SpreadHost S;
+    exp_disk_components(fwhm, half, S);
+    const int n = 2 * half + 1;
+    K.assign((size_t)n * n, 0.0);
+    for (int c = 0; c < 6; ++c) {
+        const double* Iv = S.I.data() + (size_t)c * n;
+        for (int jj = 0; jj < n; ++jj)
+            for (int ii = 0; ii < n; ++ii) K[ii + (size_t)jj * n] += S.alpha[c] * Iv[ii] * Iv[jj];
+    }
 }
 
 // The spread_model kernel of one fit: the disk FWHM is `param` when given
@@ -120,11 +139,10 @@ void exp_disk_kernel(double fwhm, int half, std::vector<double>& K) {
 // does), the support half = ceil(fit_rad).  Returns false when spread_model
 // is off (a non-finite or non-positive disk FWHM).
 bool spread_kernel(const cpb_psf* psf, double psf_fwhm, double param, double y1, double x1, double fit_rad,
-                   std::vector<double>& K, int& half) {
+                   SpreadHost& out) {
     const double f = std::isnan(param) ? spread_fwhm(psf, psf_fwhm, y1, x1) : param;
     if (!(std::isfinite(f) && f > 0)) return false;
-    half = (int)std::ceil(fit_rad);
-    exp_disk_kernel(f, half, K);
+    exp_disk_components(f, (int)std::ceil(fit_rad), out);
     return true;
 }
 
