@@ -896,16 +896,21 @@ def fit_star_packed(model, pixels, offsets, ny, nx, y_origin, x_origin, init, *,
 
 
 def params_matrix(psf, sources):
-    """_build_params_matrix (psf_photometry_single.jl:132-149): one row of model
-    parameters per star in getproperties order, from the catalogue where it has
-    the field and from the PSF's own value otherwise."""
+    """_extract_source_catalog + _build_params_matrix (psf_photometry_single.jl:132-181):
+    one row of model parameters per star in getproperties order; y and x from the
+    catalogue, flux from it or 1, bkg from it or 0, every other parameter (the
+    Gaussian's fwhm) the PSF's own value."""
     names = _props(psf)
     get = (lambda k: sources[k]) if isinstance(sources, dict) else (lambda k: getattr(sources, k))
     has = (lambda k: k in sources) if isinstance(sources, dict) else (lambda k: hasattr(sources, k))
     n = np.asarray(get("y")).size
+    default = {"flux": 1.0, "bkg": 0.0}
     cols = []
     for k in names:
-        v = np.asarray(get(k), dtype=np.float64).ravel() if has(k) else np.full(n, float(getattr(psf, k)))
+        if k in ("y", "x") or (k in default and has(k)):
+            v = np.asarray(get(k), dtype=np.float64).ravel()
+        else:
+            v = np.full(n, default.get(k, float(getattr(psf, k, 0.0))))
         if v.size != n:
             raise ArgumentError(f"source field `{k}` has {v.size} entries, expected {n}")
         cols.append(v)
