@@ -518,14 +518,53 @@ __device__ __forceinline__ void pp_profile(const PPNode& N, const double* pp, Ta
     dX = -(nd.sx * pdu);
 }
 
+// A cutout is fitted by a team of WPC warps (1: one warp a cutout, the
+// throughput form for large batches; 4: a 128-thread team, the latency form for
+// batches too small to fill the GPU).  Teams synchronise on their own named
+// barrier (1 + team index; barrier 0 is __syncthreads).
+template <int WPC>
+__device__ __forceinline__ void team_sync() {
+    if (WPC == 1) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / (32 * WPC))), "r"(32 * WPC) : "memory");
+    }
+}
+
+// Sums of K per-thread values over the team, in a fixed order (warp sums, then
+// the team's warps in index order); every thread of the team receives them.
+// red: the team's K * WPC doubles of shared memory.
+template <int WPC, int K>
+__device__ __forceinline__ void team_sum(double (&v)[K], double* red) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (WPC == 1) return;
+    const int lane = threadIdx.x & 31, w = (threadIdx.x >> 5) % WPC;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[w * K + k] = v[k];
+    team_sync<WPC>();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        double t = red[k];
+#pragma unroll
+        for (int q = 1; q < WPC; ++q) t += red[q * K + k];
+        v[k] = t;
+    }
+}
+
 // Normal equations of one cutout at the full parameter vector fv, projected onto
-// the free set (A: NF x NF column-major, b: NF); every lane returns the same cost.
-template <typename TI, int NP, int NF>
+// the free set (A: NF x NF column-major, b: NF); every thread of the team returns
+// the same cost.  (qs, rs): the column / row step of a 32 * WPC pixel stride;
+// red: the team's reduction scratch (WPC * (1 + NF + NF (NF + 1) / 2) doubles).
+template <typename TI, int NP, int NF, int WPC>
 __device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L, const TI* __restrict__ pix,
-                             const TI* __restrict__ iv, int ny, int nx, int y1, int x1, int q32, int r32,
-                             const double* fv, double* A, double* b) {
+                             const TI* __restrict__ iv, int ny, int nx, int y1, int x1, int qs, int rs,
+                             const double* fv, double* A, double* b, double* red) {
     constexpr int NT = NP * (NP + 1) / 2;
-    const int lane = threadIdx.x & 31;
+    constexpr int TS = 32 * WPC;  // team size = pixel stride
+    const int lane = threadIdx.x % TS;
+    const int q32 = qs, r32 = rs;
     double Af[NT], bf[NP], cost = 0;
 #pragma unroll
     for (int q = 0; q < NT; ++q) Af[q] = 0;
@@ -560,7 +599,7 @@ __device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L
         const double norm = -(3.141592653589793 * f2 / gp);
         const double amp = flux / norm, gf2 = gp / f2;
         int i = lane % ny, j = lane / ny;
-        for (int e = lane; e < npx; e += 32) {
+        for (int e = lane; e < npx; e += TS) {
             const double py = (double)(y1 + i), px = (double)(x1 + j);
             const double dx = px - X, dy = py - Y;
             const double sq = (dx * dx + dy * dy) / f2;
@@ -599,11 +638,11 @@ __device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L
         }
         const int ni = ihi - ilo + 1, nj = jhi - jlo + 1;
         if (ni > 0 && nj > 0) {
-            const int nr = ni * nj, rq = 32 / ni, rr = 32 % ni;
+            const int nr = ni * nj, rq = TS / ni, rr = TS % ni;
             int ii = lane % ni, jj = lane / ni, di = 0, dj = 0;
             TapCursor T;
             T.ly = T.lx = 0;
-            for (int k = lane; k < nr; k += 32) {
+            for (int k = lane; k < nr; k += TS) {
                 const int i = ilo + ii, j = jlo + jj;
                 double s, dY, dX;
                 pp_profile(N, pp, T, di, dj, Y, X, (double)(y1 + i), (double)(x1 + j), s, dY, dX);
@@ -626,7 +665,7 @@ __device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L
             const double gv[NP] = {flux * dY, flux * dX, s, 1.0};
             const double mval = flux * s + bkg;
             int i = lane % ny, j = lane / ny;
-            for (int e = lane; e < npx; e += 32) {
+            for (int e = lane; e < npx; e += TS) {
                 if (!(i >= ilo && i <= ihi && j >= jlo && j <= jhi)) acc(e, mval, gv);
                 i += r32;
                 j += q32;
@@ -652,21 +691,28 @@ __device__ double lm_accum_t(const PPNode& N, const double* pp, const LMConst& L
             }
         }
     }
-    cost = warp_sum(cost);
+    constexpr int KR = 1 + NF + NF * (NF + 1) / 2;
+    double v[KR];
+    v[0] = cost;
 #pragma unroll
-    for (int q = 0; q < NF; ++q) b[q] = warp_sum(bp[q]);
+    for (int q = 0; q < NF; ++q) v[1 + q] = bp[q];
+#pragma unroll
+    for (int t = 0; t < NF * (NF + 1) / 2; ++t) v[1 + NF + t] = Ap[t];
+    team_sum<WPC, KR>(v, red);
+#pragma unroll
+    for (int q = 0; q < NF; ++q) b[q] = v[1 + q];
     {
         int t = 0;
 #pragma unroll
         for (int jq = 0; jq < NF; ++jq)
 #pragma unroll
             for (int iq = 0; iq <= jq; ++iq) {
-                const double s = warp_sum(Ap[t++]);
+                const double s = v[1 + NF + t++];
                 A[iq + jq * NF] = s;
                 A[jq + iq * NF] = s;
             }
     }
-    return cost;
+    return v[0];
 }
 
 // covariance! (levenberg_marquardt.jl:366-388) for compile-time NF; the pinv
@@ -698,9 +744,10 @@ struct LMState {
 };
 
 // Consumes one normal-equation pass (cost_c, Ac, bc at S.fc) and prepares the
-// next candidate; returns true when the fit is over.  Every lane computes the
-// same values; lane 0 stores them.  lm_irls, levenberg_marquardt.jl:478-680.
-template <int NP, int NF>
+// next candidate; returns true when the fit is over.  Every thread of the team
+// computes the same values; its first thread (lane 0) stores them.  lm_irls,
+// levenberg_marquardt.jl:478-680.
+template <int NP, int NF, int WPC>
 __device__ __forceinline__ bool lm_step(LMState<NP, NF>& S, const LMConst& L, double cost_c, const double* Ac,
                                         const double* bc, int lane) {
     double fv[NP], x[NF], A[NF * NF], b[NF], D[NF];
@@ -820,7 +867,7 @@ __device__ __forceinline__ bool lm_step(LMState<NP, NF>& S, const LMConst& L, do
         }
         break;
     }
-    __syncwarp();
+    team_sync<WPC>();
     if (lane == 0) {
 #pragma unroll
         for (int q = 0; q < NP; ++q) S.fv[q] = fv[q];
@@ -851,23 +898,29 @@ __device__ __forceinline__ bool lm_step(LMState<NP, NF>& S, const LMConst& L, do
         S.fconv = fconv;
         S.gconv = gconv;
     }
-    __syncwarp();
+    team_sync<WPC>();
     return done;
 }
 
 constexpr int kLMThreads = 256;
 
-template <typename TI, int NP, int NF, bool SMEM>
+template <typename TI, int NP, int NF, bool SMEM, int WPC>
 __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
                                              const int64_t* __restrict__ offs, const int32_t* __restrict__ cny,
                                              const int32_t* __restrict__ cnx, const int32_t* __restrict__ cy1,
                                              const int32_t* __restrict__ cx1, const TI* __restrict__ pixels,
                                              const TI* __restrict__ ivs, const double* __restrict__ init, LMOut out,
                                              unsigned long long* __restrict__ queue) {
-    __shared__ LMState<NP, NF> states[kLMThreads / 32];
+    constexpr int TS = 32 * WPC;
+    constexpr int KR = 1 + NF + NF * (NF + 1) / 2;
+    __shared__ LMState<NP, NF> states[kLMThreads / TS];
+    __shared__ double red_all[(kLMThreads / 32) * KR];
+    __shared__ unsigned long long cut_sh[kLMThreads / TS];
     extern __shared__ double node_smem[];
-    LMState<NP, NF>& S = states[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
+    const int team = threadIdx.x / TS;
+    LMState<NP, NF>& S = states[team];
+    double* red = red_all + team * WPC * KR;
+    const int lane = threadIdx.x % TS;  // index within the team (lane 0 stores the team's state)
     // the node's polyphase samples, staged once per (persistent) block
     const double* pp = N.pp;
     if (SMEM && NP == 4) {
@@ -878,14 +931,21 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
     }
     for (;;) {
         unsigned long long cc = 0;
-        if (lane == 0) cc = atomicAdd(queue, 1ull);
-        cc = __shfl_sync(0xffffffffu, cc, 0);
+        if (WPC == 1) {
+            if (lane == 0) cc = atomicAdd(queue, 1ull);
+            cc = __shfl_sync(0xffffffffu, cc, 0);
+        } else {
+            if (lane == 0) cut_sh[team] = atomicAdd(queue, 1ull);
+            team_sync<WPC>();
+            cc = cut_sh[team];
+        }
         if (cc >= (unsigned long long)n_cut) return;
         const int64_t c = (int64_t)cc;
         const int ny = cny[c], nx = cnx[c], y1 = cy1[c], x1 = cx1[c];
         const int64_t nobs = (int64_t)ny * nx;
         if (ny <= 0 || nx <= 0) {
             if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            team_sync<WPC>();
             continue;
         }
         const TI* pix = pixels + offs[c];
@@ -893,20 +953,22 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
         // _prepare_fit_star_inputs checks (psf_fitting.jl:61-90) and lm_irls dof (:461-467)
         bool bad = !(nobs - NF > 0);
         if (iv) {
-            int nvalid = 0;
-            for (int64_t e = lane; e < nobs; e += 32) {
+            double nv[1] = {0.0};
+            for (int64_t e = lane; e < nobs; e += TS) {
                 const double v = (double)iv[e];
-                nvalid += (isfinite(v) && v > 0) ? 1 : 0;
+                nv[0] += (isfinite(v) && v > 0) ? 1.0 : 0.0;
             }
-            nvalid = warp_sum(nvalid);
-            bad = bad || !(nvalid > NF);
+            team_sum<WPC, 1>(nv, red);
+            team_sync<WPC>();  // red is reused by the first normal-equation pass
+            bad = bad || !((int)nv[0] > NF);
         }
         if (bad) {
             if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            team_sync<WPC>();
             continue;
         }
-        const int q32 = 32 / ny, r32 = 32 % ny;
-        __syncwarp();
+        const int qs = TS / ny, rs = TS % ny;
+        team_sync<WPC>();
         if (lane == 0) {
 #pragma unroll
             for (int q = 0; q < NP; ++q) {
@@ -920,13 +982,14 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
             S.lam = L.lambda_init;
             S.conv = S.xconv = S.fconv = S.gconv = 0;
         }
-        __syncwarp();
+        team_sync<WPC>();
         for (;;) {
             double fc[NP], Ac[NF * NF], bc[NF];
 #pragma unroll
             for (int q = 0; q < NP; ++q) fc[q] = S.fc[q];
-            const double cost_c = lm_accum_t<TI, NP, NF>(N, pp, L, pix, iv, ny, nx, y1, x1, q32, r32, fc, Ac, bc);
-            if (lm_step<NP, NF>(S, L, cost_c, Ac, bc, lane)) break;
+            const double cost_c =
+                lm_accum_t<TI, NP, NF, WPC>(N, pp, L, pix, iv, ny, nx, y1, x1, qs, rs, fc, Ac, bc, red);
+            if (lm_step<NP, NF, WPC>(S, L, cost_c, Ac, bc, lane)) break;
         }
         if (lane == 0) {
             const double dof = (double)(nobs - NF);
@@ -952,7 +1015,7 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
             if (out.iters) out.iters[c] = S.iter;
             out.status[c] = 0;
         }
-        __syncwarp();
+        team_sync<WPC>();
     }
 }
 
@@ -1032,21 +1095,33 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
         const size_t node_bytes = gauss ? 0 : sizeof(double) * (size_t)N.plane * N.nd.isy * N.nd.isx;
         const bool smem = !gauss && node_bytes <= 100 * 1024 && cfg.smem_node != 0;
         const int per_sm = cfg.blocks_per_sm == 1 ? 1 : 2;
-        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + kLMThreads - 1) / kLMThreads,
+        // one warp a cutout while the batch fills the GPU's warps; a batch too
+        // small for that (the late batches of fit_all_stars) gets 128-thread
+        // teams, which cut each LM iteration's latency instead
+        const int64_t warps_total = (int64_t)ctx->n_sm * per_sm * (kLMThreads / 32);
+        const int wpc = n_cut * 4 <= warps_total ? 4 : 1;
+        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 * wpc + kLMThreads - 1) / kLMThreads,
                                                             (int64_t)ctx->n_sm * per_sm);
         KernelScope ks_(ctx, "k_lm", bytes);
-#define CPB_LM_LAUNCH(TI, NP, NF)                                                                                  \
+#define CPB_LM_LAUNCH_W(TI, NP, NF, W)                                                                             \
     do {                                                                                                          \
         if (smem) {                                                                                               \
-            check(cudaFuncSetAttribute(k_lm_t<TI, NP, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+            check(cudaFuncSetAttribute(k_lm_t<TI, NP, NF, true, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,  \
                                        (int)node_bytes),                                                         \
                   "smem attribute");                                                                             \
-            k_lm_t<TI, NP, NF, true><<<blocks, kLMThreads, node_bytes, st>>>(                                     \
+            k_lm_t<TI, NP, NF, true, W><<<blocks, kLMThreads, node_bytes, st>>>(                                  \
                 n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix, (const TI*)d_iv, d_init, o, queue); \
         } else {                                                                                                  \
-            k_lm_t<TI, NP, NF, false><<<blocks, kLMThreads, 0, st>>>(                                             \
+            k_lm_t<TI, NP, NF, false, W><<<blocks, kLMThreads, 0, st>>>(                                          \
                 n_cut, L, N, d_off, d_ny, d_nx, d_y1, d_x1, (const TI*)d_pix, (const TI*)d_iv, d_init, o, queue); \
         }                                                                                                         \
+    } while (0)
+#define CPB_LM_LAUNCH(TI, NP, NF)             \
+    do {                                      \
+        if (wpc == 4)                         \
+            CPB_LM_LAUNCH_W(TI, NP, NF, 4);   \
+        else                                  \
+            CPB_LM_LAUNCH_W(TI, NP, NF, 1);   \
     } while (0)
 #define CPB_LM_NF(TI, NP)                          \
     switch (L.nf) {                                \
@@ -1071,6 +1146,7 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
         }
 #undef CPB_LM_NF
 #undef CPB_LM_LAUNCH
+#undef CPB_LM_LAUNCH_W
         check(cudaGetLastError(), "k_lm");
         return;
     }
@@ -1275,6 +1351,17 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     out->device_seconds = ms * 1e-3;
     return 0;
+}
+
+void lm_enqueue_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* d_off,
+                       const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1, const int32_t* d_x1,
+                       const void* d_pix, int32_t eltype, const void* d_iv, const double* d_init, int64_t total_pixels,
+                       const cpb_lm_result* out) {
+    const LMConst L = lm_const(psf, P, d_iv != nullptr);
+    if (n_cut <= 0) return;
+    LMOut o{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
+            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels);
 }
 
 int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,

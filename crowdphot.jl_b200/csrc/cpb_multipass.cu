@@ -12,7 +12,9 @@
 // earlier batch, and each pixel sees its adds and subtracts in the reference's
 // order -- so the result is the sequential one, while each batch is one
 // add-back launch, one cutout gather, one batched LM launch (the fit_star
-// kernel of cpb_lm.cu) and one subtract launch.
+// kernel of cpb_lm.cu), one bookkeeping launch and one subtract launch.  The
+// per-star state lives on the device for the whole pass; the host plans a pass
+// (brightness order, boxes, batches) from the state read back once per pass.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -25,6 +27,10 @@
 
 namespace cpb {
 namespace {
+
+struct MPFree {
+    int idx[5];  // the free parameters' rows
+};
 
 struct MPConst {
     int np;           // model parameters per star (4 image PSFs, 5 Gaussian)
@@ -110,7 +116,7 @@ __global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4*
         double* o = out + (int64_t)s * 6;
         const double* pr = params + (int64_t)s * M.np;
         const double flux = pr[M.rf], bkg = pr[M.rb];
-        if (!flags[s] || !(flux > 0)) {
+        if (flags[s] != 2 || !(flux > 0)) {  // 2: fitted in this batch
             if (threadIdx.x == 0) o[0] = o[1] = o[2] = o[3] = o[4] = o[5] = NaN;
             continue;
         }
@@ -194,6 +200,43 @@ __global__ void k_mp_init(int64_t npix, const TI* __restrict__ img, double* __re
     if (q < npix) residual[q] = (double)img[q];
 }
 
+// Bookkeeping of one batch after its fit_star launch (:373-401), one thread a
+// star: on success the star's parameters, errors of the free parameters,
+// convergence, chi^2 and iteration count are updated and its new model is
+// queued for subtraction (flag 2); a fit that failed the input checks
+// invalidates the star and, on passes 2+, queues its previous model again to
+// undo the add-back (flag 1).  Positions index the batch; idx maps them to stars.
+__global__ void k_mp_book(int nL, const int32_t* __restrict__ idx, int pass, int np, int nf, MPFree F,
+                          const double* __restrict__ lm_params, const double* __restrict__ lm_cov,
+                          const double* __restrict__ lm_chisq, const uint8_t* __restrict__ lm_conv,
+                          const int32_t* __restrict__ lm_iters, const int32_t* __restrict__ lm_status,
+                          const double* __restrict__ pin, double* __restrict__ prm, double* __restrict__ err,
+                          uint8_t* __restrict__ conv, double* __restrict__ chisq, int32_t* __restrict__ niter,
+                          uint8_t* __restrict__ valid, int* __restrict__ n_failed, double* __restrict__ psub,
+                          uint8_t* __restrict__ flag) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nL) return;
+    const int64_t s = idx[k];
+    if (lm_status[k] != 0) {  // fit_star threw (:391-401)
+        valid[s] = 0;
+        atomicAdd(n_failed, 1);
+        for (int q = 0; q < np; ++q) psub[(int64_t)k * np + q] = pin[(int64_t)k * np + q];
+        flag[k] = pass > 1 ? 1 : 0;
+        return;
+    }
+    for (int q = 0; q < np; ++q) {
+        const double v = lm_params[(int64_t)k * np + q];
+        prm[s * np + q] = v;
+        psub[(int64_t)k * np + q] = v;
+    }
+    for (int a = 0; a < nf; ++a)
+        err[s * np + F.idx[a]] = sqrt(fmax(0.0, lm_cov[(int64_t)k * nf * nf + a + a * nf]));
+    conv[s] = lm_conv[k];
+    chisq[s] = lm_chisq[k];
+    niter[s] += lm_iters[k];
+    flag[k] = 2;
+}
+
 inline unsigned warps_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256); }
 
 }  // namespace
@@ -255,23 +298,39 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     else
         k_mp_init<float><<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(npix, (const float*)d_img, resid);
     check(cudaGetLastError(), "k_mp_init");
-    double dev_s = 0;
 
-    // batch buffers, sized for all stars at once (a batch never exceeds n)
+    // per-star state on the device (star order) and per-position buffers of a
+    // pass (level order; a pass never holds more than n positions)
     const int Rmax = (int)std::ceil(std::max(fit_rad, 0.0)) + 1;
     const int64_t box_max = (int64_t)(2 * Rmax + 1) * (2 * Rmax + 1);
+    double* d_prm = (double*)scratch(ctx, "mp_prm", sizeof(double) * n * np);
+    double* d_err = (double*)scratch(ctx, "mp_err", sizeof(double) * n * np);
+    double* d_chisq = (double*)scratch(ctx, "mp_chisq", sizeof(double) * n);
+    int32_t* d_niter = (int32_t*)scratch(ctx, "mp_niter", sizeof(int32_t) * n);
+    uint8_t* d_sflag = (uint8_t*)scratch(ctx, "mp_sflags", (size_t)n * 2);  // valid, converged
+    uint8_t* d_valid = d_sflag;
+    uint8_t* d_conv = d_sflag + n;
+    int* d_nfail = (int*)scratch(ctx, "mp_nfail", sizeof(int));
+    int32_t* d_idx = (int32_t*)scratch(ctx, "mp_idx", sizeof(int32_t) * n);
     int4* d_box = (int4*)scratch(ctx, "mp_box", sizeof(int4) * n);
     double* d_pin = (double*)scratch(ctx, "mp_pin", sizeof(double) * n * np);
     double* d_psub = (double*)scratch(ctx, "mp_psub", sizeof(double) * n * np);
     uint8_t* d_flag = (uint8_t*)scratch(ctx, "mp_flag", n);
     int64_t* d_off = (int64_t*)scratch(ctx, "mp_off", sizeof(int64_t) * n);
-    int32_t* d_dims = (int32_t*)scratch(ctx, "mp_dims", sizeof(int32_t) * n * 4);  // ny, nx, y1, x1
-    double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * n * box_max);
-    double* d_civ = d_iv ? (double*)scratch(ctx, "mp_civ", sizeof(double) * n * box_max) : nullptr;
+    int32_t* d_dims = (int32_t*)scratch(ctx, "mp_dims", sizeof(int32_t) * n * 4);  // ny, nx, y1, x1 planes
     double* d_lmd = (double*)scratch(ctx, "mp_lm_f64", sizeof(double) * n * (np + nf * nf + 4));
     uint8_t* d_lmu = (uint8_t*)scratch(ctx, "mp_lm_u8", (size_t)n * 4);
     int32_t* d_lmi = (int32_t*)scratch(ctx, "mp_lm_i32", sizeof(int32_t) * n * 2);
     double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 6);
+    // cutout pixels of one batch: the largest batch of a pass sizes them (grown on demand)
+    check(cudaMemcpyAsync(d_prm, prm.data(), sizeof(double) * n * np, cudaMemcpyHostToDevice, st), "h2d");
+    check(cudaMemcpyAsync(d_err, err.data(), sizeof(double) * n * np, cudaMemcpyHostToDevice, st), "h2d");
+    check(cudaMemsetAsync(d_chisq, 0, sizeof(double) * n, st), "memset");
+    check(cudaMemsetAsync(d_niter, 0, sizeof(int32_t) * n, st), "memset");
+    check(cudaMemsetAsync(d_conv, 0, (size_t)n, st), "memset");
+    check(cudaMemsetAsync(d_nfail, 0, sizeof(int), st), "memset");
+    MPFree F{};
+    for (int a = 0; a < nf; ++a) F.idx[a] = free_idx[a];
     // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
     SpreadHost sh;
     SpreadDev sd{};
@@ -293,12 +352,13 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
               "smem attr");
     }
 
-    // host staging of one batch
+    // host plan of one pass (level order)
+    std::vector<int32_t> hidx;
     std::vector<int4> hbox;
-    std::vector<double> hpin, hpsub, hlm;
-    std::vector<uint8_t> hflag, hlmu;
+    std::vector<double> hpin;
     std::vector<int64_t> hoff;
-    std::vector<int32_t> hdims, hlmi;
+    std::vector<int32_t> hdims;
+    std::vector<int64_t> lev_start, lev_pix;
     std::vector<double> hdiag;
     const double FTfit = fit_rad;
 
@@ -349,134 +409,136 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                     for (int cy = cy0; cy <= cy1; ++cy) grid[(int64_t)cy * gnx + cx].push_back(s);
             }
         }
-        std::vector<std::vector<int64_t>> batches(nlev);
+        // positions in level order (brightness order inside a level), each
+        // batch's cutouts packed from offset 0
+        std::vector<int64_t> cnt(nlev + 1, 0);
         for (int64_t s : order)
-            if (valid[s] && level[s] >= 0) batches[level[s]].push_back(s);
-        out->n_levels += nlev;
-
-        for (int L = 0; L < nlev; ++L) {
-            const std::vector<int64_t>& B = batches[L];
-            const int nL = (int)B.size();
-            if (nL == 0) continue;
-            hbox.resize(nL);
-            hpin.resize((size_t)nL * np);
-            hoff.resize(nL);
-            hdims.resize((size_t)nL * 4);
-            int64_t tot = 0;
-            for (int k = 0; k < nL; ++k) {
-                const int64_t s = B[k];
+            if (valid[s] && level[s] >= 0) cnt[level[s] + 1] += 1;
+        lev_start.assign(nlev + 1, 0);
+        for (int L = 0; L < nlev; ++L) lev_start[L + 1] = lev_start[L] + cnt[L + 1];
+        const int64_t npos = lev_start[nlev];
+        hidx.resize(npos);
+        hbox.resize(npos);
+        hpin.resize((size_t)npos * np);
+        hoff.resize(npos);
+        hdims.resize((size_t)npos * 4);
+        lev_pix.assign(nlev, 0);
+        {
+            std::vector<int64_t> fill(lev_start.begin(), lev_start.end() - 1);
+            for (int64_t s : order) {
+                if (!(valid[s] && level[s] >= 0)) continue;
+                const int L = level[s];
+                const int64_t k = fill[L]++;
+                hidx[k] = (int32_t)s;
                 hbox[k] = box[s];
                 std::memcpy(&hpin[(size_t)k * np], &prm[s * np], sizeof(double) * np);
-                hoff[k] = tot;
-                tot += (int64_t)box[s].z * box[s].w;
+                hoff[k] = lev_pix[L];
+                lev_pix[L] += (int64_t)box[s].z * box[s].w;
                 hdims[k] = box[s].z;
-                hdims[nL + k] = box[s].w;
-                hdims[2 * nL + k] = box[s].x;
-                hdims[3 * nL + k] = box[s].y;
+                hdims[npos + k] = box[s].w;
+                hdims[2 * npos + k] = box[s].x;
+                hdims[3 * npos + k] = box[s].y;
             }
-            check(cudaMemcpyAsync(d_box, hbox.data(), sizeof(int4) * nL, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_pin, hpin.data(), sizeof(double) * nL * np, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_off, hoff.data(), sizeof(int64_t) * nL, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_dims, hdims.data(), sizeof(int32_t) * nL * 4, cudaMemcpyHostToDevice, st), "h2d");
+        }
+        out->n_levels += nlev;
+        out->n_fits += npos;
+        const int64_t pix_max = lev_pix.empty() ? 1 : std::max<int64_t>(1, *std::max_element(lev_pix.begin(), lev_pix.end()));
+        double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * pix_max);
+        double* d_civ = d_iv ? (double*)scratch(ctx, "mp_civ", sizeof(double) * pix_max) : nullptr;
+        if (npos > 0) {
+            check(cudaMemcpyAsync(d_valid, valid.data(), (size_t)n, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_idx, hidx.data(), sizeof(int32_t) * npos, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_box, hbox.data(), sizeof(int4) * npos, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_pin, hpin.data(), sizeof(double) * npos * np, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_off, hoff.data(), sizeof(int64_t) * npos, cudaMemcpyHostToDevice, st), "h2d");
+            check(cudaMemcpyAsync(d_dims, hdims.data(), sizeof(int32_t) * npos * 4, cudaMemcpyHostToDevice, st),
+                  "h2d");
+        }
+        // fit_star results per position
+        double* lm_par = d_lmd;
+        double* lm_cov = d_lmd + (size_t)npos * np;
+        double* lm_sc = d_lmd + (size_t)npos * (np + nf * nf);  // cost, cost_init, chisq, lambda planes
+        for (int L = 0; L < nlev; ++L) {
+            const int64_t p0 = lev_start[L];
+            const int nL = (int)(lev_start[L + 1] - p0);
+            if (nL == 0) continue;
+            const int64_t tot = lev_pix[L];
+            const int4* bx = d_box + p0;
             // passes 2+: the star's previous model goes back in (:360-365)
             if (pass > 1) {
                 KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
-                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_pin, nullptr, 1.0, dp, M, resid, ny);
+                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_pin + p0 * np, nullptr, 1.0, dp, M, resid, ny);
                 check(cudaGetLastError(), "k_mp_addsub");
             }
             {
                 KernelScope ks_(ctx, "k_mp_cutouts", (double)tot * (d_iv ? 32 : 16));
                 if (eltype == CPB_F64)
-                    k_mp_cutouts<double><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_off, resid, (const double*)d_iv,
-                                                                       ny, d_cpix, d_civ);
+                    k_mp_cutouts<double><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_off + p0, resid,
+                                                                       (const double*)d_iv, ny, d_cpix, d_civ);
                 else
-                    k_mp_cutouts<float><<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_off, resid, (const float*)d_iv,
-                                                                      ny, d_cpix, d_civ);
+                    k_mp_cutouts<float><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_off + p0, resid,
+                                                                      (const float*)d_iv, ny, d_cpix, d_civ);
                 check(cudaGetLastError(), "k_mp_cutouts");
             }
             // fit_star on every box of the batch (:367-371): the fit_star kernel
             cpb_lm_result r{};
-            r.params = d_lmd;
-            r.cov = d_lmd + (size_t)nL * np;
-            double* sc = d_lmd + (size_t)nL * (np + nf * nf);
-            r.cost = sc;
-            r.cost_init = sc + nL;
-            r.chisq = sc + 2 * nL;
-            r.lambda_final = sc + 3 * nL;
-            r.converged = d_lmu;
-            r.x_converged = d_lmu + nL;
-            r.f_converged = d_lmu + 2 * nL;
-            r.g_converged = d_lmu + 3 * nL;
-            r.iterations = d_lmi;
-            r.status = d_lmi + nL;
-            fit_lm_batch_device(ctx, psf, P, nL, d_off, d_dims, d_dims + nL, d_dims + 2 * nL, d_dims + 3 * nL, d_cpix,
-                                CPB_F64, d_civ, d_pin, tot, &r);
-            dev_s += r.device_seconds;
-            out->n_fits += nL;
-            hlm.resize((size_t)nL * (np + nf * nf + 4));
-            hlmu.resize((size_t)nL * 4);
-            hlmi.resize((size_t)nL * 2);
-            check(cudaMemcpyAsync(hlm.data(), d_lmd, sizeof(double) * hlm.size(), cudaMemcpyDeviceToHost, st), "d2h");
-            check(cudaMemcpyAsync(hlmu.data(), d_lmu, hlmu.size(), cudaMemcpyDeviceToHost, st), "d2h");
-            check(cudaMemcpyAsync(hlmi.data(), d_lmi, sizeof(int32_t) * hlmi.size(), cudaMemcpyDeviceToHost, st), "d2h");
-            check(cudaStreamSynchronize(st), "sync");
-            // bookkeeping (:373-390) and what to subtract: the new model, or on a
-            // failed fit of pass 2+ the previous one again (undoing the add-back)
-            hpsub.resize((size_t)nL * np);
-            hflag.assign(nL, 0);
-            const double* hcov = hlm.data() + (size_t)nL * np;
-            const double* hsc = hlm.data() + (size_t)nL * (np + nf * nf);
-            for (int k = 0; k < nL; ++k) {
-                const int64_t s = B[k];
-                if (hlmi[nL + k] != 0) {  // fit_star threw (:391-401)
-                    valid[s] = 0;
-                    out->n_failed += 1;
-                    if (pass > 1) {
-                        std::memcpy(&hpsub[(size_t)k * np], &prm[s * np], sizeof(double) * np);
-                        hflag[k] = 1;
-                    }
-                    continue;
-                }
-                std::memcpy(&prm[s * np], &hlm[(size_t)k * np], sizeof(double) * np);
-                for (int a = 0; a < nf; ++a) {
-                    const double cv = hcov[(size_t)k * nf * nf + a + a * nf];
-                    err[s * np + free_idx[a]] = std::sqrt(std::max(0.0, cv));
-                }
-                conv[s] = hlmu[k];
-                chisq[s] = hsc[2 * nL + k];
-                niter[s] += hlmi[k];
-                std::memcpy(&hpsub[(size_t)k * np], &hlm[(size_t)k * np], sizeof(double) * np);
-                hflag[k] = 2;  // fitted
-            }
-            std::vector<uint8_t> sub_on(nL);
-            for (int k = 0; k < nL; ++k) sub_on[k] = hflag[k] != 0;
-            check(cudaMemcpyAsync(d_psub, hpsub.data(), sizeof(double) * nL * np, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
+            r.params = lm_par + p0 * np;
+            r.cov = lm_cov + p0 * nf * nf;
+            r.cost = lm_sc + p0;
+            r.cost_init = lm_sc + npos + p0;
+            r.chisq = lm_sc + 2 * npos + p0;
+            r.lambda_final = lm_sc + 3 * npos + p0;
+            r.converged = d_lmu + p0;
+            r.x_converged = d_lmu + npos + p0;
+            r.f_converged = d_lmu + 2 * npos + p0;
+            r.g_converged = d_lmu + 3 * npos + p0;
+            r.iterations = d_lmi + p0;
+            r.status = d_lmi + npos + p0;
+            lm_enqueue_device(ctx, psf, P, nL, d_off + p0, d_dims + p0, d_dims + npos + p0, d_dims + 2 * npos + p0,
+                              d_dims + 3 * npos + p0, d_cpix, CPB_F64, d_civ, d_pin + p0 * np, tot, &r);
+            // bookkeeping (:373-401) and what to subtract
+            k_mp_book<<<(unsigned)((nL + 127) / 128), 128, 0, st>>>(
+                nL, d_idx + p0, pass, np, nf, F, r.params, r.cov, r.chisq, r.converged, r.iterations, r.status,
+                d_pin + p0 * np, d_prm, d_err, d_conv, d_chisq, d_niter, d_valid, d_nfail, d_psub + p0 * np,
+                d_flag + p0);
+            check(cudaGetLastError(), "k_mp_book");
             {
                 KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
-                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, d_box, d_psub, d_flag, -1.0, dp, M, resid, ny);
+                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_psub + p0 * np, d_flag + p0, -1.0, dp, M, resid,
+                                                            ny);
                 check(cudaGetLastError(), "k_mp_addsub");
             }
             if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389)
-                for (int k = 0; k < nL; ++k) sub_on[k] = hflag[k] == 2;
-                check(cudaMemcpyAsync(d_flag, sub_on.data(), nL, cudaMemcpyHostToDevice, st), "h2d");
                 KernelScope ks_(ctx, "k_mp_diag", (double)tot * (d_iv ? 24 : 16));
+                const unsigned g = (unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16);
                 if (eltype == CPB_F64)
-                    k_mp_diag<double><<<(unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16), kDiagThreads, diag_smem, st>>>(
-                        nL, d_box, d_psub, d_flag, (const double*)d_img, resid, (const double*)d_iv, dp, M, nf, ny, sd,
-                        smode, boxmax, d_diag);
+                    k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
+                        nL, bx, d_psub + p0 * np, d_flag + p0, (const double*)d_img, resid, (const double*)d_iv, dp,
+                        M, nf, ny, sd, smode, boxmax, d_diag + p0 * 6);
                 else
-                    k_mp_diag<float><<<(unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16), kDiagThreads, diag_smem, st>>>(
-                        nL, d_box, d_psub, d_flag, (const float*)d_img, resid, (const float*)d_iv, dp, M, nf, ny, sd,
-                        smode, boxmax, d_diag);
+                    k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
+                        nL, bx, d_psub + p0 * np, d_flag + p0, (const float*)d_img, resid, (const float*)d_iv, dp,
+                        M, nf, ny, sd, smode, boxmax, d_diag + p0 * 6);
                 check(cudaGetLastError(), "k_mp_diag");
-                hdiag.resize((size_t)nL * 6);
-                check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * nL * 6, cudaMemcpyDeviceToHost, st), "d2h");
-                check(cudaStreamSynchronize(st), "sync");
-                for (int k = 0; k < nL; ++k)
-                    if (hflag[k] == 2)
-                        for (int t = 0; t < 6; ++t) diag[B[k] * 6 + t] = hdiag[(size_t)k * 6 + t];
             }
+        }
+        // the pass's state back on the host: parameters and flags for the next
+        // pass's plan; on the last pass also the diagnostics of every position
+        check(cudaMemcpyAsync(prm.data(), d_prm, sizeof(double) * n * np, cudaMemcpyDeviceToHost, st), "d2h");
+        std::vector<uint8_t> hflags((size_t)n * 2);
+        check(cudaMemcpyAsync(hflags.data(), d_sflag, (size_t)n * 2, cudaMemcpyDeviceToHost, st), "d2h");
+        if (pass == n_passes && npos > 0) {
+            hdiag.resize((size_t)npos * 6);
+            check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * npos * 6, cudaMemcpyDeviceToHost, st), "d2h");
+        }
+        check(cudaStreamSynchronize(st), "sync");
+        if (npos > 0)
+            for (int64_t s = 0; s < n; ++s) valid[s] = hflags[s];  // fit failures of this pass
+        for (int64_t s = 0; s < n; ++s) conv[s] = hflags[n + s];
+        if (pass == n_passes && npos > 0) {
+            // diagnostics of the fitted positions (k_mp_diag wrote NaN for the others)
+            for (int64_t k = 0; k < npos; ++k)
+                for (int t = 0; t < 6; ++t) diag[(int64_t)hidx[k] * 6 + t] = hdiag[(size_t)k * 6 + t];
         }
         // between-pass validation (:404-412)
         for (int64_t s = 0; s < n; ++s) {
@@ -485,13 +547,18 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         }
     }
     check(cudaEventRecord(ctx->ev1, st), "event");
+    int nfail = 0;
+    check(cudaMemcpyAsync(err.data(), d_err, sizeof(double) * n * np, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(chisq.data(), d_chisq, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(niter.data(), d_niter, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(&nfail, d_nfail, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
     if (out->residual)
         check(cudaMemcpyAsync(out->residual, resid, sizeof(double) * npix, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaStreamSynchronize(st), "sync");
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     out->device_seconds = ms * 1e-3;
-    (void)dev_s;
+    out->n_failed = nfail;
     std::memcpy(out->params, prm.data(), sizeof(double) * n * np);
     std::memcpy(out->errors, err.data(), sizeof(double) * n * np);
     for (int64_t s = 0; s < n; ++s) {
