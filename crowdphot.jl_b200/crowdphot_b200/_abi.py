@@ -43,6 +43,15 @@ CPB_DAMP_NONE = 2
 CPB_SOLVER_LSQR = 0
 CPB_SOLVER_LSMR = 1
 
+CPB_LOSS_NONE = 0
+CPB_LOSS_L2DIST = 1
+CPB_LOSS_HUBER = 2
+CPB_LOSS_TUKEY = 3
+CPB_SCALE_AUTO = 0
+CPB_SCALE_MAD = 1
+CPB_SCALE_FIXED = 2
+CPB_SCALE_MSCALE = 3
+
 _dp = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
 _i64p = C.POINTER(C.c_int64)
@@ -210,6 +219,15 @@ class LMParams(C.Structure):
         ("covariance", C.c_int32),
         ("precision", C.c_int32),
         ("reserved", C.c_int32),
+        ("reweight", C.c_int32),
+        ("scale_estimator", C.c_int32),
+        ("loss_param", C.c_double),
+        ("scale_value", C.c_double),
+        ("mscale_delta", C.c_double),
+        ("mscale_tol", C.c_double),
+        ("mscale_max_iter", C.c_int32),
+        ("reserved2", C.c_int32),
+        ("weight_reset_tol", C.c_double),
     ]
 
 
@@ -222,6 +240,7 @@ class LMResultC(C.Structure):
         ("iterations", _i32p),
         ("status", _i32p),
         ("device_seconds", C.c_double),
+        ("sigma_final", _dp),
     ]
 
 

@@ -12,9 +12,9 @@ Differences from the Julia API, all deliberate:
   * the device computes in FP64 and results are returned as float64 arrays
     (Float32 cannot hold 1e-4 px at 2048 px);
   * ``background`` (image-shaped, optional) is subtracted on the device;
-  * ``solver=:lsmr``, IRLS ``reweight`` and PSF types other than
-    CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF} raise
-    ArgumentError -- there is no CPU fallback;
+  * ``solver=:lsmr``, IRLS losses other than L2DistLoss / HuberLoss /
+    TukeyLoss and PSF types other than CircularGaussianPSF / ImagePSF /
+    GriddedPSFModel{ImagePSF} raise ArgumentError -- there is no CPU fallback;
   * the batched group entry points (``fit_all_stars_simultaneous_batch``,
     ``fit_groups_packed``, ``BatchGraph``, ``Server``) leave ``spread_model`` /
     ``spread_model_err`` NaN; the single-field entry points compute them.
@@ -743,8 +743,13 @@ class Server:
 
 def lm_params(model, fixed, *, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
               lambda_max=1.0e12, damping="marquardt", max_iter=200, x_tol=1.0e-8, f_tol=1.0e-4, g_tol=1.0e-4,
-              covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64"):
+              covariance_estimator=None, min_diagonal=1.0e-6, precision="fp64", reweight=None, scale_estimator=None,
+              weight_reset_tol=0.1, show_trace=False):
+    """fit_star / lm_irls keyword arguments -> cpb_lm_params (psf_fitting.jl:229-250,
+    levenberg_marquardt.jl:431-449); show_trace is accepted and ignored."""
+    from .robust import set_irls
     P = _abi.LMParams()
+    set_irls(P, reweight, scale_estimator, weight_reset_tol)
     P.free_mask = _free_mask(model, fixed)
     P.max_iter = int(max_iter)
     P.fixed_y = float(fixed.get("y", model.y))
@@ -776,12 +781,6 @@ def fit_star_batch(model, cutouts, *, inv_vars=None, origins, inits=None, fixed=
     Returns a dict of arrays (params, cov, cost, ..., status).
     """
     fixed = dict(fixed or {})
-    if kw.get("reweight") is not None:
-        raise ArgumentError("IRLS reweighting is not supported by the B200 path")
-    kw.pop("reweight", None)
-    kw.pop("scale_estimator", None)
-    kw.pop("weight_reset_tol", None)
-    kw.pop("show_trace", None)
     ctx = ctx or get_context()
     P = lm_params(model, fixed, **kw)
     n = len(cutouts)
@@ -810,19 +809,8 @@ def fit_star_batch(model, cutouts, *, inv_vars=None, origins, inits=None, fixed=
     init = np.ascontiguousarray(np.stack(inits) if inits is not None else np.tile(_model_vector(model), (n, 1)),
                                 dtype=np.float64)
     nf = bin(P.free_mask).count("1")
-    out = dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), cost=np.zeros(n), cost_init=np.zeros(n),
-               chisq=np.zeros(n), lambda_final=np.zeros(n), converged=np.zeros(n, np.uint8),
-               x_converged=np.zeros(n, np.uint8), f_converged=np.zeros(n, np.uint8),
-               g_converged=np.zeros(n, np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
-    r = _abi.LMResultC()
-    dp = lambda a: a.ctypes.data_as(_abi._dp)
-    u8 = lambda a: a.ctypes.data_as(_abi._u8p)
-    r.params, r.cov, r.cost, r.cost_init = dp(out["params"]), dp(out["cov"]), dp(out["cost"]), dp(out["cost_init"])
-    r.chisq, r.lambda_final = dp(out["chisq"]), dp(out["lambda_final"])
-    r.converged, r.x_converged = u8(out["converged"]), u8(out["x_converged"])
-    r.f_converged, r.g_converged = u8(out["f_converged"]), u8(out["g_converged"])
-    r.iterations = out["iterations"].ctypes.data_as(_abi._i32p)
-    r.status = out["status"].ctypes.data_as(_abi._i32p)
+    out = _lm_outputs(n, np_, nf)
+    r = _lm_result_struct(out, lambda a: a.ctypes.data)
     hp = ctx.psf_handle(model)
     et = _abi.CPB_F32 if dt == np.float32 else _abi.CPB_F64
     rc = ctx.lib.cpb_fit_lm_batch(ctx.handle, hp, C.byref(P), n, offs.ctypes.data_as(_abi._i64p),
@@ -841,13 +829,14 @@ def _lm_outputs(n, np_, nf):
     return dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), cost=np.zeros(n), cost_init=np.zeros(n),
                 chisq=np.zeros(n), lambda_final=np.zeros(n), converged=np.zeros(n, np.uint8),
                 x_converged=np.zeros(n, np.uint8), f_converged=np.zeros(n, np.uint8),
-                g_converged=np.zeros(n, np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
+                g_converged=np.zeros(n, np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32),
+                sigma_final=np.zeros(n))
 
 
 def _lm_result_struct(out, ptr):
     """LMResultC pointing at the arrays of `out` through ptr(array) (host or device addresses)."""
     r = _abi.LMResultC()
-    for f in ("params", "cov", "cost", "cost_init", "chisq", "lambda_final"):
+    for f in ("params", "cov", "cost", "cost_init", "chisq", "lambda_final", "sigma_final"):
         setattr(r, f, C.cast(C.c_void_p(ptr(out[f])), _abi._dp) if out.get(f) is not None else None)
     for f in ("converged", "x_converged", "f_converged", "g_converged"):
         setattr(r, f, C.cast(C.c_void_p(ptr(out[f])), _abi._u8p) if out.get(f) is not None else None)
@@ -1015,5 +1004,5 @@ def fit_star(model, image, inds=None, *, fixed=None, inv_var=None, ctx: Context 
                    converged=bool(out["converged"][0]), x_converged=bool(out["x_converged"][0]),
                    f_converged=bool(out["f_converged"][0]), g_converged=bool(out["g_converged"][0]),
                    iterations=int(out["iterations"][0]), lambda_final=float(out["lambda_final"][0]),
-                   sigma_final=float("nan"), cov=out["cov"][0].copy(), chisq=float(out["chisq"][0]))
+                   sigma_final=float(out["sigma_final"][0]), cov=out["cov"][0].copy(), chisq=float(out["chisq"][0]))
     return best, res

@@ -5,7 +5,8 @@
 //   _accum_circular_gaussian!               :354-451
 //   _accum_image_psf!                       :1115-1173
 //   _accum_gridded_imagepsf!                :1383-1517
-//   lm_irls (without IRLS), damp!, covariance!  src/levenberg_marquardt.jl:64-99, 361-680
+//   lm_irls, damp!, covariance!              src/levenberg_marquardt.jl:64-99, 361-680
+//   IRLS weights and scale estimators        :105-355 (k_lm_irls)
 // One warp owns one cutout for the whole fit: lanes stride over the cutout's
 // pixels, the normal equations are reduced with warp shuffles (every lane
 // ends with the same A, b, cost), and every lane runs the identical small
@@ -31,15 +32,22 @@ struct LMConst {
     int damping;
     int max_iter;
     int reweighted;
+    int irls;         // CPB_LOSS_* (0: plain LM)
+    int scale;        // CPB_SCALE_*
+    int mscale_max_iter;
+    double loss_param, scale_value, mscale_delta, mscale_tol, weight_reset_tol;
     double fixv[5];  // fixed value per model parameter
     double x_tol, f_tol, g_tol;
     double lambda_init, lambda_up, lambda_down, lambda_min, lambda_max, min_diagonal;
 };
 
 // Normal equations at the full parameter vector fv (projected onto the free set).
+// wv (nullable): per-pixel weights replacing the sanitised inv_var (IRLS);
+// res (nullable): receives every pixel's residual model - data.
 template <typename TI>
 __device__ double lm_accum(const DevPsf& P, const LMConst& L, const TI* __restrict__ pix, const TI* __restrict__ iv,
-                           int ny, int nx, int y1, int x1, const double* fv, double* A, double* b) {
+                           int ny, int nx, int y1, int x1, const double* fv, double* A, double* b,
+                           const double* wv = nullptr, double* res = nullptr) {
     const int lane = threadIdx.x & 31;
     double Af[15], bf[5], cost = 0;
 #pragma unroll
@@ -61,10 +69,13 @@ __device__ double lm_accum(const DevPsf& P, const LMConst& L, const TI* __restri
             const double Ag = amp * g;
             const double r = (amp * g + bkg) - (double)pix[e];
             double w = 1.0;
-            if (iv) {
+            if (wv) {
+                w = wv[e];
+            } else if (iv) {
                 double v = (double)iv[e];
                 w = (isfinite(v) && v > 0) ? v : 0.0;
             }
+            if (res) res[e] = r;
             const double wr = w * r;
             cost = wr * r + cost;
             const double gv[5] = {-2 * Ag * gf2 * dy, -2 * Ag * gf2 * dx, -2 * Ag * (1 + gp * sq) / fwhm, g / norm,
@@ -94,10 +105,13 @@ __device__ double lm_accum(const DevPsf& P, const LMConst& L, const TI* __restri
             grid_profile<double, double, true>(P, P.data64, c, (double)(y1 + i), (double)(x1 + j), s, dY, dX);
             const double r = (flux * s + bkg) - (double)pix[e];
             double w = 1.0;
-            if (iv) {
+            if (wv) {
+                w = wv[e];
+            } else if (iv) {
                 double v = (double)iv[e];
                 w = (isfinite(v) && v > 0) ? v : 0.0;
             }
+            if (res) res[e] = r;
             const double wr = w * r;
             cost = wr * r + cost;
             const double gv[4] = {flux * dY, flux * dX, s, 1.0};
@@ -227,6 +241,7 @@ struct LMOut {
     uint8_t *converged, *x_converged, *f_converged, *g_converged;
     int32_t* iters;
     int32_t* status;
+    double* sigma_final;  // IRLS scale estimate (NaN without IRLS)
 };
 
 template <typename TI>
@@ -357,8 +372,331 @@ __global__ void __launch_bounds__(256) k_lm(int64_t n_cut, LMConst L, DevPsf P, 
             if (out.f_converged) out.f_converged[c] = fconv;
             if (out.g_converged) out.g_converged[c] = gconv;
             if (out.iters) out.iters[c] = iter;
+            if (out.sigma_final) out.sigma_final[c] = __longlong_as_double(0x7ff8000000000000LL);
             out.status[c] = 0;
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// IRLS (lm_irls with reweight, levenberg_marquardt.jl:105-355, 611-645)
+// ---------------------------------------------------------------------------
+// Order-preserving 64-bit key of a double (negative values reversed).
+__device__ __forceinline__ unsigned long long dkey(double v) {
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
+    return (bits >> 63) ? ~bits : (bits | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+    const unsigned long long bits = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+    return __longlong_as_double((long long)bits);
+}
+
+// The k-th smallest (0-based) of val(0..n-1), exactly, by one warp: an 8-pass
+// radix select on the keys with a 256-bin histogram in the warp's shared memory.
+template <class F>
+__device__ double warp_kth(F val, int n, int k, unsigned* hist) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long prefix = 0, mask = 0;
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int t = lane; t < 256; t += 32) hist[t] = 0;
+        __syncwarp();
+        for (int e = lane; e < n; e += 32) {
+            const unsigned long long key = dkey(val(e));
+            if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255], 1u);
+        }
+        __syncwarp();
+        unsigned cnt[8], tot = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            cnt[q] = hist[lane * 8 + q];
+            tot += cnt[q];
+        }
+        unsigned incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const unsigned excl = incl - tot;
+        const unsigned ball = __ballot_sync(0xffffffffu, (unsigned)k >= excl && (unsigned)k < incl);
+        const int owner = ball ? __ffs(ball) - 1 : 31;
+        int bin = 0;
+        unsigned before = 0;
+        if (lane == owner) {
+            unsigned acc = excl;
+            bin = lane * 8 + 7;
+            before = acc;
+            for (int q = 0; q < 8; ++q) {
+                if ((unsigned)k < acc + cnt[q]) {
+                    bin = lane * 8 + q;
+                    before = acc;
+                    break;
+                }
+                acc += cnt[q];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        before = __shfl_sync(0xffffffffu, before, owner);
+        k -= (int)before;
+        prefix |= (unsigned long long)bin << shift;
+        mask |= 255ull << shift;
+        __syncwarp();
+    }
+    return dkey_inv(prefix);
+}
+
+// Statistics.median: the middle order statistic, or middle(a, b) = a/2 + b/2 of
+// the two; NaN when any value is NaN.
+template <class F>
+__device__ double warp_median(F val, int n, unsigned* hist) {
+    const int lane = threadIdx.x & 31;
+    bool nan = false;
+    for (int e = lane; e < n; e += 32) nan |= isnan(val(e));
+    if (__any_sync(0xffffffffu, nan)) return __longlong_as_double(0x7ff8000000000000LL);
+    if (n & 1) return warp_kth(val, n, (n - 1) / 2, hist);
+    const double a = warp_kth(val, n, n / 2 - 1, hist), b = warp_kth(val, n, n / 2, hist);
+    return a / 2 + b / 2;
+}
+
+// estimate_scale for MADScale / FixedScale / MScale over the n residuals r.
+__device__ double irls_scale(const LMConst& L, const double* r, int n, double fixed_sigma, unsigned* hist) {
+    if (L.scale == CPB_SCALE_FIXED || (L.scale == CPB_SCALE_AUTO && fixed_sigma == fixed_sigma))
+        return L.scale == CPB_SCALE_FIXED ? L.scale_value : fixed_sigma;
+    const double med = warp_median([&](int e) { return r[e]; }, n, hist);
+    const double mad = 1.4826 * warp_median([&](int e) { return fabs(r[e] - med); }, n, hist);
+    if (L.scale != CPB_SCALE_MSCALE) return mad;
+    const int lane = threadIdx.x & 31;
+    const double eps = 2.220446049250313e-16;
+    double sg = isnan(mad) ? mad : fmax(mad, eps);
+    for (int it = 0; it < L.mscale_max_iter; ++it) {
+        const double cap = 9 * (sg * sg);
+        double chi = 0;
+        for (int e = lane; e < n; e += 32) {
+            const double r2 = r[e] * r[e];
+            chi += r2 < cap ? r2 : cap;
+        }
+        chi = warp_sum(chi);
+        const double sn = sqrt(chi / (n * L.mscale_delta));
+        if (fabs(sn - sg) <= L.mscale_tol * fmax(sg, L.mscale_tol)) {
+            sg = sn;
+            break;
+        }
+        sg = sn;
+    }
+    return sg;
+}
+
+// weight(loss, r) = psi(r) / (r psi'(0)), 1 near r = 0.
+__device__ __forceinline__ double irls_weight(const LMConst& L, double r) {
+    if (fabs(r) < 2.220446049250313e-16 * 10) return 1.0;
+    const double c = L.loss_param;
+    if (L.irls == CPB_LOSS_L2DIST) return (2 * r) / (r * 2.0);
+    if (L.irls == CPB_LOSS_HUBER) {
+        const double psi = fabs(r) <= c ? r : c * (r > 0 ? 1.0 : -1.0);
+        const double psi0 = 0.0 <= c ? 1.0 : 0.0;
+        return psi / (r * psi0);
+    }
+    // TukeyLoss
+    double psi = 0.0;
+    if (fabs(r) <= c) {
+        const double rc2 = (r / c) * (r / c);
+        psi = r * ((1 - rc2) * (1 - rc2));
+    }
+    const double psi0 = 0.0 <= c ? 1.0 : 0.0;
+    return psi / (r * psi0);
+}
+
+// One warp a cutout, as k_lm, with lm_irls's reweighting: after an accepted,
+// unconverged step the scale is estimated from the residuals, every pixel's
+// weight becomes base * weight(r / sigma), the normal equations are rebuilt at
+// the accepted point and, when the weights moved by weight_reset_tol or more,
+// lambda and D restart.  wbuf / rbuf: per-pixel weights and residuals, laid
+// out like the cutouts.
+template <typename TI>
+__global__ void __launch_bounds__(256) k_lm_irls(int64_t n_cut, LMConst L, DevPsf P, const int64_t* __restrict__ offs,
+                                                 const int32_t* __restrict__ cny, const int32_t* __restrict__ cnx,
+                                                 const int32_t* __restrict__ cy1, const int32_t* __restrict__ cx1,
+                                                 const TI* __restrict__ pixels, const TI* __restrict__ ivs,
+                                                 const double* __restrict__ init, double* __restrict__ wbuf,
+                                                 double* __restrict__ rbuf, LMOut out) {
+    __shared__ unsigned hist_all[8][256];
+    unsigned* hist = hist_all[(threadIdx.x >> 5) & 7];
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int np = L.np, nf = L.nf;
+    const double eps = 2.220446049250313e-16;
+    for (int64_t c = warp; c < n_cut; c += nwarps) {
+        const int ny = cny[c], nx = cnx[c], y1 = cy1[c], x1 = cx1[c];
+        const TI* pix = pixels + offs[c];
+        const TI* iv = ivs ? ivs + offs[c] : nullptr;
+        double* wts = wbuf + offs[c];
+        double* res = rbuf + offs[c];
+        const int64_t nobs = (int64_t)ny * nx;
+        if (ny <= 0 || nx <= 0) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
+        int bad = 0;
+        double wsum = 0;
+        for (int64_t e = lane; e < nobs; e += 32) {
+            double w = 1.0;
+            if (iv) {
+                const double v = (double)iv[e];
+                w = (isfinite(v) && v > 0) ? v : 0.0;
+            }
+            wts[e] = w;
+            wsum += w;
+        }
+        if (iv) {
+            int nvalid = 0;
+            for (int64_t e = lane; e < nobs; e += 32) {
+                const double v = (double)iv[e];
+                nvalid += (isfinite(v) && v > 0) ? 1 : 0;
+            }
+            nvalid = warp_sum(nvalid);
+            if (!(nvalid > nf)) bad = 1;
+        }
+        if (!(nobs - nf > 0)) bad = 1;
+        if (bad) {
+            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+            continue;
+        }
+        // the default scale with weights: FixedScale(sqrt(inv(mean(base_weights))))
+        const double fixed_sigma = iv ? sqrt(1.0 / (warp_sum(wsum) / (double)nobs))
+                                      : __longlong_as_double(0x7ff8000000000000LL);
+        __syncwarp();
+        double fv[5], x[5], xc[5], A[25], b[5], Ac[25], bc[5], Ad[25], d[5], D[5];
+        for (int q = 0; q < np; ++q) fv[q] = init[c * np + q];
+        for (int q = 0; q < np; ++q) {
+            bool fr = false;
+            for (int k = 0; k < nf; ++k) fr |= (L.fidx[k] == q);
+            if (!fr) fv[q] = L.fixv[q];
+        }
+        for (int k = 0; k < nf; ++k) x[k] = fv[L.fidx[k]];
+        double cost = lm_accum<TI>(P, L, pix, iv, ny, nx, y1, x1, fv, A, b, wts, res);
+        const double cost_init = cost;
+        for (int k = 0; k < nf; ++k) D[k] = sqrt(fmax(A[k + k * nf], 1.0e-6));
+        double lam = L.lambda_init;
+        double sigma_final = __longlong_as_double(0x7ff8000000000000LL);
+        bool xconv = false, fconv = false, gconv = false, conv = false;
+        int iter = 0;
+        while (iter < L.max_iter) {
+            ++iter;
+            double gcos = 0;
+            for (int k = 0; k < nf; ++k)
+                gcos = nan_max(gcos, fabs(b[k]) / (sqrt(A[k + k * nf] * cost) + eps));
+            if (gcos <= L.g_tol) {
+                gconv = conv = true;
+                break;
+            }
+            for (int k = 0; k < nf * nf; ++k) Ad[k] = A[k];
+            if (L.damping == CPB_DAMP_MARQUARDT)
+                for (int k = 0; k < nf; ++k) Ad[k + k * nf] += lam * fmax(Ad[k + k * nf], L.min_diagonal);
+            else if (L.damping == CPB_DAMP_LEVENBERG)
+                for (int k = 0; k < nf; ++k) Ad[k + k * nf] += lam;
+            if (!lm_chol_solve(Ad, nf, b, d)) {
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+                continue;
+            }
+            for (int k = 0; k < nf; ++k) d[k] = -d[k];
+            double db = 0, dAd = 0;
+            for (int k = 0; k < nf; ++k) db += d[k] * b[k];
+            for (int k = 0; k < nf; ++k)
+                for (int r = 0; r < nf; ++r) dAd += d[k] * A[k + r * nf] * d[r];
+            const double prered = -2 * db - dAd;
+            for (int k = 0; k < nf; ++k) xc[k] = x[k] + d[k];
+            double fc[5];
+            for (int q = 0; q < np; ++q) fc[q] = fv[q];
+            for (int k = 0; k < nf; ++k) fc[L.fidx[k]] = xc[k];
+            const double cost_c = lm_accum<TI>(P, L, pix, iv, ny, nx, y1, x1, fc, Ac, bc, wts, res);
+            __syncwarp();
+            const bool accepted = cost_c < cost;
+            const double dcost = cost - cost_c;
+            const double ratio = prered > 0 ? dcost / prered : 0.0;
+            fconv = fabs(dcost) <= L.f_tol * (fabs(cost) + L.f_tol) && prered <= L.f_tol * (fabs(cost) + L.f_tol) &&
+                    0.5 * ratio <= 1;
+            double nd = 0, nxv = 0;
+            for (int k = 0; k < nf; ++k) {
+                nd += (D[k] * d[k]) * (D[k] * d[k]);
+                nxv += (D[k] * x[k]) * (D[k] * x[k]);
+            }
+            xconv = sqrt(nd) <= L.x_tol * (sqrt(nxv) + L.x_tol) && (accepted || fconv);
+            if (accepted) {
+                cost = cost_c;
+                lam = fmax(lam / L.lambda_down, L.lambda_min);
+                for (int k = 0; k < nf; ++k) x[k] = xc[k];
+                for (int k = 0; k < nf * nf; ++k) A[k] = Ac[k];
+                for (int k = 0; k < nf; ++k) b[k] = bc[k];
+                for (int q = 0; q < np; ++q) fv[q] = fc[q];
+                for (int k = 0; k < nf; ++k) D[k] = fmax(D[k], sqrt(A[k + k * nf]));
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+                // reweighting from the residuals at the accepted point (:611-645)
+                sigma_final = irls_scale(L, res, (int)nobs, fixed_sigma, hist);
+                if (sigma_final > eps) {
+                    double dw2 = 0, wo2 = 0, wn2 = 0;
+                    for (int64_t e = lane; e < nobs; e += 32) {
+                        const double old_w = wts[e];
+                        double base_w = 1.0;
+                        if (iv) {
+                            const double v = (double)iv[e];
+                            base_w = (isfinite(v) && v > 0) ? v : 0.0;
+                        }
+                        const double new_w = base_w * irls_weight(L, res[e] / sigma_final);
+                        const double dw = new_w - old_w;
+                        dw2 = fma(dw, dw, dw2);
+                        wo2 = fma(old_w, old_w, wo2);
+                        wn2 = fma(new_w, new_w, wn2);
+                        wts[e] = new_w;
+                    }
+                    dw2 = warp_sum(dw2);
+                    wo2 = warp_sum(wo2);
+                    wn2 = warp_sum(wn2);
+                    __syncwarp();
+                    cost = lm_accum<TI>(P, L, pix, iv, ny, nx, y1, x1, fv, A, b, wts, res);
+                    __syncwarp();
+                    const double wchange = sqrt(dw2) / fmax(fmax(sqrt(wo2), sqrt(wn2)), eps);
+                    if (wchange >= L.weight_reset_tol) {
+                        lam = L.lambda_init;
+                        for (int k = 0; k < nf; ++k) D[k] = sqrt(fmax(A[k + k * nf], 1.0e-6));
+                    }
+                }
+            } else {
+                if (xconv || fconv) {
+                    conv = true;
+                    break;
+                }
+                lam = fmin(lam * L.lambda_up, L.lambda_max);
+            }
+        }
+        if (lane == 0) {
+            const double dof = (double)(nobs - nf);
+            if (out.cov) {
+                double cov[25];
+                lm_cov(A, nf, cov);
+                const double f = L.reweighted ? cost / dof : 1.0;
+                for (int k = 0; k < nf * nf; ++k) out.cov[c * nf * nf + k] = cov[k] * f;
+            }
+            const double s2 = cost / dof;
+            const bool scaled = !iv && !isnan(sigma_final) && sigma_final > eps;
+            if (out.params)
+                for (int q = 0; q < np; ++q) out.params[c * np + q] = fv[q];
+            if (out.cost) out.cost[c] = cost;
+            if (out.cost_init) out.cost_init[c] = cost_init;
+            if (out.chisq) out.chisq[c] = scaled ? s2 / (sigma_final * sigma_final) : s2;
+            if (out.lambda_final) out.lambda_final[c] = lam;
+            if (out.converged) out.converged[c] = conv;
+            if (out.x_converged) out.x_converged[c] = xconv;
+            if (out.f_converged) out.f_converged[c] = fconv;
+            if (out.g_converged) out.g_converged[c] = gconv;
+            if (out.iters) out.iters[c] = iter;
+            if (out.sigma_final) out.sigma_final[c] = sigma_final;
+            out.status[c] = 0;
+        }
+        __syncwarp();
     }
 }
 
@@ -1013,6 +1351,7 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
             if (out.f_converged) out.f_converged[c] = S.fconv;
             if (out.g_converged) out.g_converged[c] = S.gconv;
             if (out.iters) out.iters[c] = S.iter;
+            if (out.sigma_final) out.sigma_final[c] = __longlong_as_double(0x7ff8000000000000LL);
             out.status[c] = 0;
         }
         team_sync<WPC>();
@@ -1042,7 +1381,22 @@ LMConst lm_const(const cpb_psf* psf, const cpb_lm_params* P, bool have_iv) {
     if (L.nf == 0) throw ArgError{"all model parameters are fixed; nothing to fit"};
     L.damping = P->damping;
     L.max_iter = P->max_iter;
-    L.reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && !have_iv);
+    if (!(P->weight_reset_tol >= 0) && P->reweight != CPB_LOSS_NONE)
+        throw ArgError{"`weight_reset_tol` must be non-negative"};
+    if (P->reweight < CPB_LOSS_NONE || P->reweight > CPB_LOSS_TUKEY) throw ArgError{"unknown IRLS loss"};
+    if (P->scale_estimator < CPB_SCALE_AUTO || P->scale_estimator > CPB_SCALE_MSCALE)
+        throw ArgError{"unknown IRLS scale estimator"};
+    L.irls = P->reweight;
+    L.scale = P->scale_estimator;
+    L.loss_param = P->loss_param;
+    L.scale_value = P->scale_value;
+    L.mscale_delta = P->mscale_delta;
+    L.mscale_tol = P->mscale_tol;
+    L.mscale_max_iter = P->mscale_max_iter;
+    L.weight_reset_tol = P->weight_reset_tol;
+    // covariance_estimator default (:647-653): known weights only without IRLS
+    L.reweighted = P->covariance == CPB_COV_REWEIGHTED ||
+                   (P->covariance == CPB_COV_AUTO && (!have_iv || P->reweight != CPB_LOSS_NONE));
     L.x_tol = P->x_tol;
     L.f_tol = P->f_tol;
     L.g_tol = P->g_tol;
@@ -1077,6 +1431,21 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
                          (double)n_cut * (8 * L.np + (o.cov ? 8 * L.nf * L.nf : 0) + 4 * 8 + 4 + 4 + 4);
     cudaStream_t st = cfg.stream ? cfg.stream : ctx->stream;
     const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    if (L.irls != CPB_LOSS_NONE) {
+        if (pix_elems <= 0) throw ArgError{"IRLS reweighting needs the cutouts' total pixel count"};
+        double* wbuf = (double*)scratch(ctx, "lm_irls_w", sizeof(double) * (size_t)pix_elems);
+        double* rbuf = (double*)scratch(ctx, "lm_irls_r", sizeof(double) * (size_t)pix_elems);
+        const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 + 255) / 256, (int64_t)ctx->n_sm * 16);
+        KernelScope ks_(ctx, "k_lm_irls", bytes);
+        if (eltype == CPB_F64)
+            k_lm_irls<double><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
+                                                      (const double*)d_pix, (const double*)d_iv, d_init, wbuf, rbuf, o);
+        else
+            k_lm_irls<float><<<blocks, 256, 0, st>>>(n_cut, L, psf->dev, d_off, d_ny, d_nx, d_y1, d_x1,
+                                                     (const float*)d_pix, (const float*)d_iv, d_init, wbuf, rbuf, o);
+        check(cudaGetLastError(), "k_lm_irls");
+        return;
+    }
     if (gauss || psf->dev.n_nodes == 1) {
         // fast form: compile-time parameter counts, polyphase taps, work queue
         PPNode N{};
@@ -1188,9 +1557,11 @@ LMBatch* lm_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* 
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
     if (n_cut > 0 && (!d_off || !d_ny || !d_nx || !d_y1 || !d_x1 || !d_pix || !d_init || !out || !out->status))
         throw ArgError{"null argument"};
+    const LMConst Lc = lm_const(psf, P, d_iv != nullptr);
+    if (Lc.irls != CPB_LOSS_NONE) throw ArgError{"IRLS reweighting is not supported in a bound fit_star batch"};
     auto* b = new LMBatch();
     b->psf = psf;
-    b->L = lm_const(psf, P, d_iv != nullptr);
+    b->L = Lc;
     b->n_cut = n_cut;
     b->off = d_off;
     b->ny = d_ny;
@@ -1203,7 +1574,7 @@ LMBatch* lm_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* 
     b->init = d_init;
     if (out)
         b->o = LMOut{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
-                     out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+                     out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status, out->sigma_final};
     b->pix_elems = total_pixels;
     if (cudaMalloc(&b->queue, sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();
@@ -1296,6 +1667,7 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     o.g_converged = du + 3 * n_cut;
     o.iters = di;
     o.status = di + n_cut;
+    o.sigma_final = out->sigma_final ? (double*)scratch(ctx, "lm_out_sigma", sizeof(double) * n_cut) : nullptr;
     // Pixels and weights: when the cutouts are packed in order they go up in
     // chunks on the copy stream, and chunk k is fitted while chunk k + 1 is in
     // flight; otherwise in one piece.
@@ -1303,7 +1675,10 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     for (int64_t c = 1; c < n_cut && ordered; ++c)
         ordered = offsets[c] >= offsets[c - 1] + (int64_t)ny[c - 1] * nx[c - 1];
     const int64_t bytes_all = (int64_t)esz * total * (inv_var ? 2 : 1);
-    const int K = ordered ? (int)std::min<int64_t>({(int64_t)8, n_cut, std::max<int64_t>(1, bytes_all >> 25)}) : 1;
+    // (IRLS keeps one launch: its weight / residual scratch is laid out like the whole batch)
+    const int K = ordered && L.irls == CPB_LOSS_NONE
+                      ? (int)std::min<int64_t>({(int64_t)8, n_cut, std::max<int64_t>(1, bytes_all >> 25)})
+                      : 1;
     for (int k = 0; k < K; ++k) {
         const int64_t c0 = n_cut * k / K, c1 = n_cut * (k + 1) / K;
         if (c1 <= c0) continue;
@@ -1331,6 +1706,7 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
         ok.g_converged += c0;
         ok.iters += c0;
         ok.status += c0;
+        if (ok.sigma_final) ok.sigma_final += c0;
         launch_lm(ctx, psf, L, c1 - c0, d_off + c0, d_ny + c0, d_nx + c0, d_y1 + c0, d_x1 + c0, d_pix, eltype,
                   d_iv, d_init + c0 * L.np, ok, e1 - e0);
     }
@@ -1346,6 +1722,7 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
     for (int k = 0; k < 4; ++k) down(hf[k], du + k * n_cut, (size_t)n_cut);
     down(out->iterations, o.iters, sizeof(int32_t) * n_cut);
     down(out->status, o.status, sizeof(int32_t) * n_cut);
+    down(out->sigma_final, o.sigma_final, sizeof(double) * n_cut);
     check(cudaStreamSynchronize(st), "sync");
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
@@ -1360,7 +1737,7 @@ void lm_enqueue_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P,
     const LMConst L = lm_const(psf, P, d_iv != nullptr);
     if (n_cut <= 0) return;
     LMOut o{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
-            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status, out->sigma_final};
     launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels);
 }
 
@@ -1372,7 +1749,7 @@ int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P
     const LMConst L = lm_const(psf, P, d_iv != nullptr);
     if (n_cut <= 0) return 0;
     LMOut o{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
-            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status};
+            out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status, out->sigma_final};
     cudaStream_t st = ctx->stream;
     check(cudaEventRecord(ctx->ev0, st), "event");
     launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels);

@@ -172,7 +172,7 @@ typedef struct cpb_sim_result {
 
 /*
  * Keyword arguments of fit_star / lm_irls (psf_fitting.jl:229-250,
- * levenberg_marquardt.jl:431-449).  IRLS (reweight) is not supported.
+ * levenberg_marquardt.jl:431-449), IRLS reweighting included (fields below).
  */
 typedef struct cpb_lm_params {
     int32_t free_mask;        /* CPB_FREE_* bits */
@@ -186,7 +186,31 @@ typedef struct cpb_lm_params {
     int32_t covariance;       /* CPB_COV_* */
     int32_t precision;        /* CPB_PREC_* */
     int32_t reserved;
+    /* IRLS reweighting: lm_irls's reweight / scale_estimator / weight_reset_tol
+     * (levenberg_marquardt.jl:105-355, 420-425, 611-645).  CPB_LOSS_NONE (the
+     * zero value) is the plain fit. */
+    int32_t reweight;         /* CPB_LOSS_* */
+    int32_t scale_estimator;  /* CPB_SCALE_* */
+    double loss_param;        /* HuberLoss d / TukeyLoss c */
+    double scale_value;       /* FixedScale sigma */
+    double mscale_delta, mscale_tol; /* MScale: 0.5, 1e-6 */
+    int32_t mscale_max_iter;  /* MScale: 30 */
+    int32_t reserved2;
+    double weight_reset_tol;  /* 0.1 */
 } cpb_lm_params;
+
+/* IRLS losses (LossFunctions.L2DistLoss, LossFunctions.HuberLoss(d),
+ * CrowdPhot.TukeyLoss(c)) and scale estimators (MADScale, FixedScale(sigma),
+ * MScale(delta, tol, max_iter)); CPB_SCALE_AUTO is the reference's default:
+ * FixedScale(sqrt(1 / mean(weights))) when inv_var is given, else MADScale. */
+#define CPB_LOSS_NONE 0
+#define CPB_LOSS_L2DIST 1
+#define CPB_LOSS_HUBER 2
+#define CPB_LOSS_TUKEY 3
+#define CPB_SCALE_AUTO 0
+#define CPB_SCALE_MAD 1
+#define CPB_SCALE_FIXED 2
+#define CPB_SCALE_MSCALE 3
 
 /*
  * Per-cutout result of the batched LM fit (LMResult, levenberg_marquardt.jl:28-41).
@@ -204,6 +228,7 @@ typedef struct cpb_lm_result {
     int32_t* iterations;
     int32_t* status;
     double device_seconds;
+    double* sigma_final;      /* optional: the last IRLS scale estimate (NaN without IRLS) */
 } cpb_lm_result;
 
 typedef struct cpb_ctx cpb_ctx;

@@ -40,7 +40,13 @@ def load():
         lib.orc_fit_star.restype = C.c_int
         lib.orc_fit_star.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), _dp, _dp, C.c_int32,
                                      C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _u8p, _i32p,
-                                     C.c_char_p, C.c_int]
+                                     C.c_char_p, C.c_int, _dp]
+        lib.orc_lm_irls_line.restype = C.c_int
+        lib.orc_lm_irls_line.argtypes = [_dp, _dp, C.c_int, C.POINTER(_abi.LMParams), _dp, _dp, _dp, _dp, _i32p]
+        lib.orc_estimate_scale.restype = C.c_double
+        lib.orc_estimate_scale.argtypes = [C.c_int, C.POINTER(_abi.LMParams), C.c_double, _dp, C.c_int64]
+        lib.orc_irls_weight.restype = C.c_double
+        lib.orc_irls_weight.argtypes = [C.c_int, C.c_double, C.c_double]
         lib.orc_apply_J.argtypes = [C.c_int, C.c_int, C.c_int64, C.c_int64, _dp, _i32p, _u8p, _dp, _dp]
         lib.orc_apply_JT.argtypes = [C.c_int, C.c_int, C.c_int64, _dp, _i32p, _u8p, _dp, _dp]
         lib.orc_lsqr_stamp.restype = C.c_int
@@ -84,7 +90,7 @@ def load():
         lib.orc_fit_star_batch.restype = C.c_int
         lib.orc_fit_star_batch.argtypes = [C.POINTER(_abi.PsfDesc), C.POINTER(_abi.LMParams), C.c_int64, _i64p,
                                            _i32p, _i32p, _i32p, _i32p, _dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp,
-                                           _dp, _u8p, _i32p, _i32p, C.c_int]
+                                           _dp, _u8p, _i32p, _i32p, C.c_int, _dp]
         _lib = lib
     return _lib
 
@@ -123,10 +129,7 @@ def orc_fit_star(model, image, inds=None, *, fixed=None, inv_var=None, **kw):
     """The oracle's fit_star -> (best_model, LMResult)."""
     lib = load()
     fixed = dict(fixed or {})
-    kw.pop("show_trace", None)
     kw.pop("ctx", None)
-    if kw.pop("reweight", None) is not None:
-        raise ArgumentError("IRLS reweighting is not restated")
     P = lm_params(model, fixed, **kw)
     img = np.asarray(image, dtype=np.float64)
     if inds is None:
@@ -146,13 +149,14 @@ def orc_fit_star(model, image, inds=None, *, fixed=None, inv_var=None, **kw):
     sc = [C.c_double() for _ in range(4)]
     flags = np.zeros(4, dtype=np.uint8)
     iters = C.c_int32()
+    sigma = C.c_double()
     desc, keep = psf_descriptor(model)
     err = C.create_string_buffer(1024)
     rc = lib.orc_fit_star(C.byref(desc), C.byref(P), cut.ctypes.data_as(_dp),
                           None if ivc is None else ivc.ctypes.data_as(_dp), cut.shape[0], cut.shape[1], ya, xa,
                           init.ctypes.data_as(_dp), outp.ctypes.data_as(_dp), cov.ctypes.data_as(_dp),
                           C.byref(sc[0]), C.byref(sc[1]), C.byref(sc[2]), C.byref(sc[3]),
-                          flags.ctypes.data_as(_u8p), C.byref(iters), err, 1024)
+                          flags.ctypes.data_as(_u8p), C.byref(iters), err, 1024, C.byref(sigma))
     del keep
     if rc != 0:
         raise ArgumentError(err.value.decode())
@@ -160,7 +164,7 @@ def orc_fit_star(model, image, inds=None, *, fixed=None, inv_var=None, **kw):
     free = [i for i, k in enumerate(names) if k not in fixed]
     res = LMResult(minimizer=outp[free].copy(), minimum=sc[0].value, cost_init=sc[1].value, converged=bool(flags[0]),
                    x_converged=bool(flags[1]), f_converged=bool(flags[2]), g_converged=bool(flags[3]),
-                   iterations=int(iters.value), lambda_final=sc[3].value, sigma_final=float("nan"),
+                   iterations=int(iters.value), lambda_final=sc[3].value, sigma_final=sigma.value,
                    cov=cov[:nf * nf].reshape(nf, nf, order="F").copy(), chisq=sc[2].value)
     return best, res
 
@@ -353,7 +357,8 @@ def orc_fit_star_packed(model, pix, offsets, ny, nx, y1, x1, init, *, inv_var=No
     offsets = np.ascontiguousarray(offsets, dtype=np.int64)
     ny, nx, y1, x1 = i32(ny), i32(nx), i32(y1), i32(x1)
     out = dict(params=np.zeros((n, np_)), cov=np.zeros((n, nf, nf)), scal=np.zeros((n, 4)),
-               flags=np.zeros((n, 4), np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32))
+               flags=np.zeros((n, 4), np.uint8), iterations=np.zeros(n, np.int32), status=np.zeros(n, np.int32),
+               sigma_final=np.zeros(n))
     desc, keep = psf_descriptor(model)
     used = lib.orc_fit_star_batch(C.byref(desc), C.byref(P), n, offsets.ctypes.data_as(_i64p),
                                   ny.ctypes.data_as(_i32p), nx.ctypes.data_as(_i32p), y1.ctypes.data_as(_i32p),
@@ -362,7 +367,7 @@ def orc_fit_star_packed(model, pix, offsets, ny, nx, y1, x1, init, *, inv_var=No
                                   out["params"].ctypes.data_as(_dp), out["cov"].ctypes.data_as(_dp),
                                   out["scal"].ctypes.data_as(_dp), out["flags"].ctypes.data_as(_u8p),
                                   out["iterations"].ctypes.data_as(_i32p), out["status"].ctypes.data_as(_i32p),
-                                  int(threads))
+                                  int(threads), out["sigma_final"].ctypes.data_as(_dp))
     del keep
     if used < 0:
         raise ArgumentError("invalid PSF descriptor")
@@ -395,3 +400,34 @@ def orc_fit_all_stars(image, psf, sources, fit_rad, *, n_passes=3, fixed=None, i
     if rc != 0:
         raise ArgumentError(err.value.decode())
     return outs.result(psf, ny, nx)
+
+
+def orc_lm_irls_line(xs, ys, x0=(0.0, 0.0), **kw):
+    """lm_irls on the reference's straight-line test problem -> (x, lambda_final, sigma_final, iterations).
+    Keyword arguments are lm_irls's (reweight, scale_estimator, weight_reset_tol, tolerances, ...)."""
+    from crowdphot_b200 import CircularGaussianPSF
+    lib = load()
+    P = lm_params(CircularGaussianPSF(fwhm=1.0), {}, **kw)
+    xs, ys, x0 = _f64(xs), _f64(ys), _f64(x0)
+    xo, lam, sig, it = np.zeros(2), C.c_double(), C.c_double(), C.c_int32()
+    rc = lib.orc_lm_irls_line(xs.ctypes.data_as(_dp), ys.ctypes.data_as(_dp), xs.size, C.byref(P),
+                              x0.ctypes.data_as(_dp), xo.ctypes.data_as(_dp), C.byref(lam), C.byref(sig), C.byref(it))
+    if rc != 0:
+        raise ArgumentError("degrees of freedom must be positive")
+    return xo, lam.value, sig.value, it.value
+
+
+def orc_estimate_scale(estimator, r):
+    """estimate_scale(estimator, r) for MADScale / FixedScale / MScale."""
+    from crowdphot_b200 import CircularGaussianPSF
+    P = lm_params(CircularGaussianPSF(fwhm=1.0), {}, reweight=None, scale_estimator=estimator)
+    rr = _f64(r)
+    return float(load().orc_estimate_scale(P.scale_estimator, C.byref(P), P.scale_value, rr.ctypes.data_as(_dp),
+                                           rr.size))
+
+
+def orc_irls_weight(loss, r):
+    """weight(loss, r) for L2DistLoss / HuberLoss / TukeyLoss."""
+    from crowdphot_b200 import CircularGaussianPSF
+    P = lm_params(CircularGaussianPSF(fwhm=1.0), {}, reweight=loss)
+    return float(load().orc_irls_weight(P.reweight, P.loss_param, float(r)))

@@ -1,12 +1,14 @@
 // oracle_lm.cpp -- TEST INFRASTRUCTURE ONLY (the oracle).
 //
 // FP64 restatement of CrowdPhot.PSF.fit_star for the three supported PSF kinds
-// and of the LM driver lm_irls without IRLS:
+// and of the LM driver lm_irls, IRLS reweighting included:
 //   _prepare_fit_star_inputs   src/psf/psf_fitting.jl:36-101
 //   fit_star(CircularGaussianPSF) + _accum_circular_gaussian!  :314-451
 //   fit_star(ImagePSF) + _accum_image_psf!                    :1086-1173
 //   fit_star(GriddedPSFModel{ImagePSF}) + _accum_gridded_imagepsf!  :1177-1517
 //   lm_irls, damp!, covariance!  src/levenberg_marquardt.jl:64-99, 361-680
+//   MADScale / FixedScale / MScale, TukeyLoss, weight  :105-355 (HuberLoss and
+//   L2DistLoss as LossFunctions.jl defines their derivatives)
 // Only tests/, smoke() and bench.py's CPU legs load it.
 #include <algorithm>
 #include <cmath>
@@ -41,7 +43,7 @@ struct Cutout {
 // the full parameter vector `full` (Gaussian: y,x,fwhm,flux,bkg; else y,x,flux,bkg),
 // then projects onto the free set (psf_fitting.jl:423-450, 1165-1172, 1500-1516).
 double accum(const Psf& psf, const Cutout& c, const std::vector<double>& wts, const double* full, const int* fidx,
-             int nf, double* A, double* b) {
+             int nf, double* A, double* b, double* res) {
     const bool gauss = psf.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     const int np = gauss ? 5 : 4;
     double Af[25] = {0}, bf[5] = {0}, cost = 0;
@@ -59,6 +61,7 @@ double accum(const Psf& psf, const Cutout& c, const std::vector<double>& wts, co
                 double g = std::exp(gp * sq);
                 double Ag = amp * g;
                 double r = (amp * g + bkg) - c.pix[i + j * c.ny];
+                res[i + j * c.ny] = r;
                 double w = wts[i + j * c.ny];
                 double wr = w * r;
                 cost = wr * r + cost;
@@ -98,6 +101,7 @@ double accum(const Psf& psf, const Cutout& c, const std::vector<double>& wts, co
                     }
                 }
                 double r = (flux * s + bkg) - c.pix[i + j * c.ny];
+                res[i + j * c.ny] = r;
                 double w = wts[i + j * c.ny];
                 double wr = w * r;
                 cost = wr * r + cost;
@@ -150,7 +154,197 @@ bool chol_solve(const double* A, int n, const double* b, double* x) {
 int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const double* inv_var, int32_t ny, int32_t nx,
             int32_t y1, int32_t x1, const double* init, double* out_params, double* cov_out, double* cost_out,
             double* cost_init_out, double* chisq_out, double* lambda_out, uint8_t* flags_out, int32_t* iters_out,
-            char* errbuf, int errlen);
+            char* errbuf, int errlen, double* sigma_out = nullptr);
+
+const double kNaN = std::numeric_limits<double>::quiet_NaN();
+
+// Statistics.median (NaN if any value is NaN; middle(a, b) = a/2 + b/2).
+double median_of(std::vector<double> v) {
+    for (double x : v)
+        if (std::isnan(x)) return kNaN;
+    std::sort(v.begin(), v.end());
+    const size_t n = v.size();
+    if (n == 0) return kNaN;
+    return (n & 1) ? v[(n - 1) / 2] : v[n / 2 - 1] / 2 + v[n / 2] / 2;
+}
+
+// estimate_scale (:137-140 MADScale, :159 FixedScale, :201-224 MScale)
+double estimate_scale(int kind, const cpb_lm_params* P, double fixed_sigma, const std::vector<double>& r) {
+    if (kind == CPB_SCALE_FIXED) return fixed_sigma;
+    const double med = median_of(r);
+    std::vector<double> dev(r.size());
+    for (size_t k = 0; k < r.size(); ++k) dev[k] = std::fabs(r[k] - med);
+    const double mad = 1.4826 * median_of(dev);
+    if (kind != CPB_SCALE_MSCALE) return mad;
+    double sg = std::isnan(mad) ? mad : std::max(mad, kEps);
+    const double n = (double)r.size();
+    for (int it = 0; it < P->mscale_max_iter; ++it) {
+        const double cap = 9 * (sg * sg);
+        double chi = 0;
+        for (double ri : r) {
+            const double r2 = ri * ri;
+            chi += r2 < cap ? r2 : cap;
+        }
+        const double sn = std::sqrt(chi / (n * P->mscale_delta));
+        if (std::fabs(sn - sg) <= P->mscale_tol * std::max(sg, P->mscale_tol)) {
+            sg = sn;
+            break;
+        }
+        sg = sn;
+    }
+    return sg;
+}
+
+// weight(loss, r) = psi(r) / (r psi'(0)) (:337-345) for L2DistLoss (psi = 2r),
+// HuberLoss(d) (psi = r inside d, d sign(r) beyond) and TukeyLoss(c) (:289-313).
+double irls_weight(int loss, double c, double r) {
+    if (std::fabs(r) < kEps * 10) return 1.0;
+    if (loss == CPB_LOSS_L2DIST) return (2 * r) / (r * 2.0);
+    if (loss == CPB_LOSS_HUBER) {
+        const double psi = std::fabs(r) <= c ? r : c * (r > 0 ? 1.0 : -1.0);
+        const double psi0 = 0.0 <= c ? 1.0 : 0.0;
+        return psi / (r * psi0);
+    }
+    double psi = 0.0;
+    if (std::fabs(r) <= c) {
+        const double rc2 = (r / c) * (r / c);
+        psi = r * ((1 - rc2) * (1 - rc2));
+    }
+    return psi / (r * 1.0);
+}
+
+struct LMRun {
+    std::vector<double> x, A;
+    double cost = 0, cost_init = 0, lam = 0, sigma_final = kNaN, chisq = 0;
+    bool conv = false, xconv = false, fconv = false, gconv = false;
+    int iter = 0;
+    bool reweighted = false;
+};
+
+// lm_irls (:431-680) on a generic problem: accum(x, w, A, b, res) fills the
+// normal equations, the residuals and returns the cost, w being the current
+// per-observation weights (nullptr: unit weights).  base: the fixed input
+// weights (nullptr: none).
+template <class Acc>
+LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std::vector<double>* base,
+                  const cpb_lm_params* P) {
+    LMRun R;
+    const bool do_irls = P->reweight != CPB_LOSS_NONE;
+    const int64_t dof = nobs - n;
+    double fixed_sigma = P->scale_value;
+    int scale_kind = P->scale_estimator;
+    if (scale_kind == CPB_SCALE_AUTO) {
+        if (base) {
+            double sm = 0;
+            for (double w : *base) sm += w;
+            fixed_sigma = std::sqrt(1.0 / (sm / (double)nobs));
+            scale_kind = CPB_SCALE_FIXED;
+        } else {
+            scale_kind = CPB_SCALE_MAD;
+        }
+    }
+    std::vector<double> weights;
+    const std::vector<double>* wp = base;
+    if (do_irls) {
+        weights = base ? *base : std::vector<double>(nobs, 1.0);
+        wp = &weights;
+    }
+    std::vector<double> res(nobs, 0.0);
+    std::vector<double> x(x0, x0 + n), xc(n), A(n * n), b(n), Ac(n * n), bc(n), Ad(n * n), d(n), D(n);
+    double cost = accum(x.data(), wp, A.data(), b.data(), res.data());
+    R.cost_init = cost;
+    const double d_floor = 1.0e-6;
+    for (int q = 0; q < n; ++q) D[q] = std::sqrt(std::max(A[q + q * n], d_floor));
+    double lam = P->lambda_init;
+    while (R.iter < P->max_iter) {
+        ++R.iter;
+        double gcos = 0;
+        for (int q = 0; q < n; ++q) gcos = std::max(gcos, std::fabs(b[q]) / (std::sqrt(A[q + q * n] * cost) + kEps));
+        if (gcos <= P->g_tol) {
+            R.gconv = R.conv = true;
+            break;
+        }
+        Ad = A;
+        if (P->damping == CPB_DAMP_MARQUARDT) {
+            for (int q = 0; q < n; ++q) Ad[q + q * n] += lam * std::max(Ad[q + q * n], P->min_diagonal);
+        } else if (P->damping == CPB_DAMP_LEVENBERG) {
+            for (int q = 0; q < n; ++q) Ad[q + q * n] += lam;
+        }
+        if (!chol_solve(Ad.data(), n, b.data(), d.data())) {
+            lam = std::min(lam * P->lambda_up, P->lambda_max);
+            continue;
+        }
+        for (int q = 0; q < n; ++q) d[q] *= -1;
+        double db = 0, dAd = 0;
+        for (int q = 0; q < n; ++q) db += d[q] * b[q];
+        for (int q = 0; q < n; ++q)
+            for (int r = 0; r < n; ++r) dAd += d[q] * A[q + r * n] * d[r];
+        const double prered = -2 * db - dAd;
+        for (int q = 0; q < n; ++q) xc[q] = x[q] + d[q];
+        const double cost_c = accum(xc.data(), wp, Ac.data(), bc.data(), res.data());
+        const bool accepted = cost_c < cost;
+        const double dcost = cost - cost_c;
+        const double ratio = prered > 0 ? dcost / prered : 0.0;
+        R.fconv = std::fabs(dcost) <= P->f_tol * (std::fabs(cost) + P->f_tol) &&
+                  prered <= P->f_tol * (std::fabs(cost) + P->f_tol) && 0.5 * ratio <= 1;
+        double nd = 0, nxv = 0;
+        for (int q = 0; q < n; ++q) {
+            nd += (D[q] * d[q]) * (D[q] * d[q]);
+            nxv += (D[q] * x[q]) * (D[q] * x[q]);
+        }
+        R.xconv = std::sqrt(nd) <= P->x_tol * (std::sqrt(nxv) + P->x_tol) && (accepted || R.fconv);
+        if (accepted) {
+            cost = cost_c;
+            lam = std::max(lam / P->lambda_down, P->lambda_min);
+            x = xc;
+            A = Ac;
+            b = bc;
+            for (int q = 0; q < n; ++q) D[q] = std::max(D[q], std::sqrt(A[q + q * n]));
+            if (R.xconv || R.fconv) {
+                R.conv = true;
+                break;
+            }
+            if (do_irls) {  // :611-645
+                R.sigma_final = estimate_scale(scale_kind, P, fixed_sigma, res);
+                if (R.sigma_final > kEps) {
+                    double dw2 = 0, wo2 = 0, wn2 = 0;
+                    for (int64_t k = 0; k < nobs; ++k) {
+                        const double old_w = weights[k];
+                        const double base_w = base ? (*base)[k] : 1.0;
+                        const double new_w = base_w * irls_weight(P->reweight, P->loss_param, res[k] / R.sigma_final);
+                        const double dw = new_w - old_w;
+                        dw2 = std::fma(dw, dw, dw2);
+                        wo2 = std::fma(old_w, old_w, wo2);
+                        wn2 = std::fma(new_w, new_w, wn2);
+                        weights[k] = new_w;
+                    }
+                    cost = accum(x.data(), wp, A.data(), b.data(), res.data());
+                    const double wchange = std::sqrt(dw2) / std::max({std::sqrt(wo2), std::sqrt(wn2), kEps});
+                    if (wchange >= P->weight_reset_tol) {
+                        lam = P->lambda_init;
+                        for (int q = 0; q < n; ++q) D[q] = std::sqrt(std::max(A[q + q * n], d_floor));
+                    }
+                }
+            }
+        } else {
+            if (R.xconv || R.fconv) {
+                R.conv = true;
+                break;
+            }
+            lam = std::min(lam * P->lambda_up, P->lambda_max);
+        }
+    }
+    R.reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && (!base || do_irls));
+    const double s2 = cost / (double)dof;
+    R.chisq = (!base && do_irls && !std::isnan(R.sigma_final) && R.sigma_final > kEps)
+                  ? s2 / (R.sigma_final * R.sigma_final)
+                  : s2;
+    R.x = x;
+    R.A = A;
+    R.cost = cost;
+    R.lam = lam;
+    return R;
+}
 
 }  // namespace
 
@@ -161,7 +355,8 @@ extern "C" {
 int orc_fit_star(const cpb_psf_desc* desc, const cpb_lm_params* P, const double* pix, const double* inv_var,
                  int32_t ny, int32_t nx, int32_t y1, int32_t x1, const double* init, double* out_params,
                  double* cov_out, double* cost_out, double* cost_init_out, double* chisq_out, double* lambda_out,
-                 uint8_t* flags_out /* converged, x, f, g */, int32_t* iters_out, char* errbuf, int errlen) {
+                 uint8_t* flags_out /* converged, x, f, g */, int32_t* iters_out, char* errbuf, int errlen,
+                 double* sigma_out /* nullable: LMResult.sigma_final */) {
     Psf psf;
     {
         std::string e = load_psf(desc, psf);
@@ -171,7 +366,7 @@ int orc_fit_star(const cpb_psf_desc* desc, const cpb_lm_params* P, const double*
         }
     }
     return fit_one(psf, P, pix, inv_var, ny, nx, y1, x1, init, out_params, cov_out, cost_out, cost_init_out,
-                   chisq_out, lambda_out, flags_out, iters_out, errbuf, errlen);
+                   chisq_out, lambda_out, flags_out, iters_out, errbuf, errlen, sigma_out);
 }
 
 // n_cut fit_star calls on one loaded PSF, cutout c at pix[offsets[c]..] (column-major
@@ -182,7 +377,8 @@ int orc_fit_star(const cpb_psf_desc* desc, const cpb_lm_params* P, const double*
 int orc_fit_star_batch(const cpb_psf_desc* desc, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
                        const int32_t* ny, const int32_t* nx, const int32_t* y1, const int32_t* x1, const double* pix,
                        const double* inv_var, const double* init, int np, int nf, double* params, double* cov,
-                       double* scal, uint8_t* flags, int32_t* iters, int32_t* status, int threads) {
+                       double* scal, uint8_t* flags, int32_t* iters, int32_t* status, int threads,
+                       double* sigma /* nullable, n */) {
     Psf psf;
     if (!load_psf(desc, psf).empty()) return -1;
     const int used = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
@@ -195,7 +391,7 @@ int orc_fit_star_batch(const cpb_psf_desc* desc, const cpb_lm_params* P, int64_t
                 status[c] = fit_one(psf, P, pix + offsets[c], inv_var ? inv_var + offsets[c] : nullptr, ny[c], nx[c],
                                     y1[c], x1[c], init + c * np, params + c * np, cov ? cov + c * nf * nf : nullptr,
                                     &scal[c * 4], &scal[c * 4 + 1], &scal[c * 4 + 2], &scal[c * 4 + 3], flags + c * 4,
-                                    iters + c, nullptr, 0);
+                                    iters + c, nullptr, 0, sigma ? sigma + c : nullptr);
         }
     };
     std::vector<std::thread> pool;
@@ -205,6 +401,49 @@ int orc_fit_star_batch(const cpb_psf_desc* desc, const cpb_lm_params* P, int64_t
     return used;
 }
 
+// lm_irls on the straight-line problem of the reference's weight-reset test
+// (test/psf/psf_fitting_tests.jl:176-233): y = x[0] * xs + x[1], unit base
+// weights absent.  Returns 0 and writes the minimiser, lambda_final,
+// sigma_final and the iteration count.
+int orc_lm_irls_line(const double* xs, const double* ys, int n, const cpb_lm_params* P, const double* x0,
+                     double* x_out, double* lambda_out, double* sigma_out, int32_t* iters_out) {
+    auto acc = [&](const double* x, const std::vector<double>* w, double* A, double* b, double* res) {
+        for (int k = 0; k < 4; ++k) A[k] = 0;
+        b[0] = b[1] = 0;
+        double cost = 0;
+        for (int k = 0; k < n; ++k) {
+            const double wk = w ? (*w)[k] : 1.0;
+            const double r = x[0] * xs[k] + x[1] - ys[k];
+            res[k] = r;
+            const double wr = wk * r;
+            cost = std::fma(wr, r, cost);
+            A[0] = std::fma(wk * xs[k], xs[k], A[0]);
+            A[1] = std::fma(wk, xs[k], A[1]);
+            A[2] = std::fma(wk * xs[k], 1.0, A[2]);
+            A[3] += wk;
+            b[0] = std::fma(wr, xs[k], b[0]);
+            b[1] += wr;
+        }
+        return cost;
+    };
+    if (n - 2 <= 0) return CPB_ERR_ARGUMENT;
+    LMRun R = lm_irls_run(acc, 2, n, x0, nullptr, P);
+    x_out[0] = R.x[0];
+    x_out[1] = R.x[1];
+    *lambda_out = R.lam;
+    *sigma_out = R.sigma_final;
+    *iters_out = R.iter;
+    return 0;
+}
+
+// estimate_scale(kind, r) for MADScale / FixedScale(sigma) / MScale(P's delta, tol, max_iter).
+double orc_estimate_scale(int kind, const cpb_lm_params* P, double sigma, const double* r, int64_t n) {
+    return estimate_scale(kind, P, sigma, std::vector<double>(r, r + n));
+}
+
+// weight(loss, r) for CPB_LOSS_L2DIST / _HUBER (d = c) / _TUKEY (c).
+double orc_irls_weight(int loss, double c, double r) { return irls_weight(loss, c, r); }
+
 }  // extern "C"
 
 namespace {
@@ -212,7 +451,7 @@ namespace {
 int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const double* inv_var, int32_t ny, int32_t nx,
             int32_t y1, int32_t x1, const double* init, double* out_params, double* cov_out, double* cost_out,
             double* cost_init_out, double* chisq_out, double* lambda_out, uint8_t* flags_out, int32_t* iters_out,
-            char* errbuf, int errlen) {
+            char* errbuf, int errlen, double* sigma_out) {
     auto fail = [&](const std::string& m) {
         if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
         return CPB_ERR_ARGUMENT;
@@ -226,6 +465,8 @@ int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const dou
     for (int q = 0; q < np; ++q)
         if (P->free_mask & (gauss ? bits_g[q] : bits_i[q])) fidx[nf++] = q;
     if (nf == 0) return fail("all model parameters are fixed; nothing to fit");
+    if (P->reweight != CPB_LOSS_NONE && !(P->weight_reset_tol >= 0))
+        return fail("`weight_reset_tol` must be non-negative");
     double full[5];
     for (int q = 0; q < np; ++q) full[q] = init[q];
     // fixed values override (model_from_vector merges `fixed`)
@@ -255,94 +496,35 @@ int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const dou
         return fail("degrees of freedom must be positive; too many free parameters (" + std::to_string(nf) +
                     ") for the number of observations (" + std::to_string(nobs) + ")");
     Cutout c{pix, inv_var, ny, nx, y1, x1};
-    double x[5], xc[5], A[25], b[5], Ac[25], bc[5], Ad[25], d[5], D[5];
-    for (int q = 0; q < nf; ++q) x[q] = full[fidx[q]];
+    double x0[5];
+    for (int q = 0; q < nf; ++q) x0[q] = full[fidx[q]];
     auto set_full = [&](const double* xv, double* fv) {
         for (int q = 0; q < np; ++q) fv[q] = full[q];
         for (int q = 0; q < nf; ++q) fv[fidx[q]] = xv[q];
     };
+    const std::vector<double> ones(nobs, 1.0);
+    auto acc = [&](const double* xv, const std::vector<double>* w, double* A, double* b, double* res) {
+        double fv[5];
+        set_full(xv, fv);
+        return accum(psf, c, w ? *w : ones, fv, fidx, nf, A, b, res);
+    };
+    LMRun R = lm_irls_run(acc, nf, nobs, x0, inv_var ? &wts : nullptr, P);
+    std::vector<double> cov;
+    covariance(R.A, nf, R.reweighted, R.cost, (double)dof, cov);
     double fv[5];
-    set_full(x, fv);
-    double cost = accum(psf, c, wts, fv, fidx, nf, A, b);
-    const double cost_init = cost;
-    const double d_floor = 1.0e-6;
-    for (int q = 0; q < nf; ++q) D[q] = std::sqrt(std::max(A[q + q * nf], d_floor));
-    double lam = P->lambda_init;
-    bool xconv = false, fconv = false, gconv = false, conv = false;
-    int iter = 0;
-    while (iter < P->max_iter) {
-        ++iter;
-        double gcos = 0;
-        for (int q = 0; q < nf; ++q) gcos = std::max(gcos, std::fabs(b[q]) / (std::sqrt(A[q + q * nf] * cost) + kEps));
-        if (gcos <= P->g_tol) {
-            gconv = true;
-            conv = true;
-            break;
-        }
-        std::memcpy(Ad, A, sizeof(double) * nf * nf);
-        if (P->damping == CPB_DAMP_MARQUARDT) {
-            for (int q = 0; q < nf; ++q) Ad[q + q * nf] += lam * std::max(Ad[q + q * nf], P->min_diagonal);
-        } else if (P->damping == CPB_DAMP_LEVENBERG) {
-            for (int q = 0; q < nf; ++q) Ad[q + q * nf] += lam;
-        }
-        if (!chol_solve(Ad, nf, b, d)) {
-            lam = std::min(lam * P->lambda_up, P->lambda_max);
-            continue;
-        }
-        for (int q = 0; q < nf; ++q) d[q] *= -1;
-        double db = 0, dAd = 0;
-        for (int q = 0; q < nf; ++q) db += d[q] * b[q];
-        for (int q = 0; q < nf; ++q)
-            for (int r = 0; r < nf; ++r) dAd += d[q] * A[q + r * nf] * d[r];
-        double prered = -2 * db - dAd;
-        for (int q = 0; q < nf; ++q) xc[q] = x[q] + d[q];
-        set_full(xc, fv);
-        double cost_c = accum(psf, c, wts, fv, fidx, nf, Ac, bc);
-        bool accepted = cost_c < cost;
-        double dcost = cost - cost_c;
-        double ratio = prered > 0 ? dcost / prered : 0.0;
-        fconv = std::fabs(dcost) <= P->f_tol * (std::fabs(cost) + P->f_tol) &&
-                prered <= P->f_tol * (std::fabs(cost) + P->f_tol) && 0.5 * ratio <= 1;
-        double nd = 0, nx_ = 0;
-        for (int q = 0; q < nf; ++q) {
-            nd += (D[q] * d[q]) * (D[q] * d[q]);
-            nx_ += (D[q] * x[q]) * (D[q] * x[q]);
-        }
-        xconv = std::sqrt(nd) <= P->x_tol * (std::sqrt(nx_) + P->x_tol) && (accepted || fconv);
-        if (accepted) {
-            cost = cost_c;
-            lam = std::max(lam / P->lambda_down, P->lambda_min);
-            std::memcpy(x, xc, sizeof(double) * nf);
-            std::memcpy(A, Ac, sizeof(double) * nf * nf);
-            std::memcpy(b, bc, sizeof(double) * nf);
-            for (int q = 0; q < nf; ++q) D[q] = std::max(D[q], std::sqrt(A[q + q * nf]));
-            if (xconv || fconv) {
-                conv = true;
-                break;
-            }
-        } else {
-            if (xconv || fconv) {
-                conv = true;
-                break;
-            }
-            lam = std::min(lam * P->lambda_up, P->lambda_max);
-        }
-    }
-    const bool reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && !inv_var);
-    std::vector<double> Av(A, A + nf * nf), cov;
-    covariance(Av, nf, reweighted, cost, (double)dof, cov);
-    set_full(x, fv);
+    set_full(R.x.data(), fv);
     for (int q = 0; q < np; ++q) out_params[q] = fv[q];
     if (cov_out) std::memcpy(cov_out, cov.data(), sizeof(double) * nf * nf);
-    *cost_out = cost;
-    *cost_init_out = cost_init;
-    *chisq_out = cost / (double)dof;
-    *lambda_out = lam;
-    flags_out[0] = conv;
-    flags_out[1] = xconv;
-    flags_out[2] = fconv;
-    flags_out[3] = gconv;
-    *iters_out = iter;
+    *cost_out = R.cost;
+    *cost_init_out = R.cost_init;
+    *chisq_out = R.chisq;
+    *lambda_out = R.lam;
+    flags_out[0] = R.conv;
+    flags_out[1] = R.xconv;
+    flags_out[2] = R.fconv;
+    flags_out[3] = R.gconv;
+    *iters_out = R.iter;
+    if (sigma_out) *sigma_out = R.sigma_final;
     return 0;
 }
 
