@@ -606,10 +606,13 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
                  const double* init, cpb_lm_result* out);
 // The fit_star launch of fit_lm_batch_device on the context's stream, with no
 // event, synchronisation or host read-back (callers chain further kernels).
+// team_warps: warps a cutout (0: chosen by the batch size; 1 or 4);
+// zeroed_queue (nullable): a work-queue counter already at zero.
 void lm_enqueue_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* d_off,
                        const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1, const int32_t* d_x1,
                        const void* d_pix, int32_t eltype, const void* d_iv, const double* d_init, int64_t total_pixels,
-                       const cpb_lm_result* out);
+                       const cpb_lm_result* out, int team_warps = 0,
+                       unsigned long long* zeroed_queue = nullptr);
 int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,
                         const int64_t* d_off, const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1,
                         const int32_t* d_x1, const void* d_pix, int32_t eltype, const void* d_iv,

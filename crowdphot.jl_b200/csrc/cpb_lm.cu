@@ -1418,6 +1418,8 @@ LMConst lm_const(const cpb_psf* psf, const cpb_lm_params* P, bool have_iv) {
 struct LMConfig {
     int blocks_per_sm = 0;
     int smem_node = -1;
+    int team_warps = 0;  // warps a cutout: 0 = by batch size (1 or 4), else 1 or 4
+    bool queue_zeroed = false;  // `queue` is already zero (no reset launch)
     unsigned long long* queue = nullptr;
     cudaStream_t stream = nullptr;
 };
@@ -1458,7 +1460,7 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
         }
         auto* queue = cfg.queue ? cfg.queue
                                 : (unsigned long long*)scratch(ctx, "lm_queue", sizeof(unsigned long long));
-        check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st), "memset");
+        if (!(cfg.queue && cfg.queue_zeroed)) check(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), st), "memset");
         // two persistent 256-thread blocks an SM (128 registers a thread); the
         // node's samples go to shared memory when two copies fit an SM
         const size_t node_bytes = gauss ? 0 : sizeof(double) * (size_t)N.plane * N.nd.isy * N.nd.isx;
@@ -1468,7 +1470,8 @@ void launch_lm(cpb_ctx* ctx, const cpb_psf* psf, const LMConst& L, int64_t n_cut
         // small for that (the late batches of fit_all_stars) gets 128-thread
         // teams, which cut each LM iteration's latency instead
         const int64_t warps_total = (int64_t)ctx->n_sm * per_sm * (kLMThreads / 32);
-        const int wpc = n_cut * 4 <= warps_total ? 4 : 1;
+        const int wpc = cfg.team_warps == 4 || cfg.team_warps == 1 ? cfg.team_warps
+                                                                  : (n_cut * 4 <= warps_total ? 4 : 1);
         const unsigned blocks = (unsigned)std::min<int64_t>((n_cut * 32 * wpc + kLMThreads - 1) / kLMThreads,
                                                             (int64_t)ctx->n_sm * per_sm);
         KernelScope ks_(ctx, "k_lm", bytes);
@@ -1733,12 +1736,16 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
 void lm_enqueue_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* d_off,
                        const int32_t* d_ny, const int32_t* d_nx, const int32_t* d_y1, const int32_t* d_x1,
                        const void* d_pix, int32_t eltype, const void* d_iv, const double* d_init, int64_t total_pixels,
-                       const cpb_lm_result* out) {
+                       const cpb_lm_result* out, int team_warps, unsigned long long* zeroed_queue) {
     const LMConst L = lm_const(psf, P, d_iv != nullptr);
     if (n_cut <= 0) return;
     LMOut o{out->params, out->cov, out->cost, out->cost_init, out->chisq, out->lambda_final, out->converged,
             out->x_converged, out->f_converged, out->g_converged, out->iterations, out->status, out->sigma_final};
-    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels);
+    LMConfig cfg;
+    cfg.team_warps = team_warps;
+    cfg.queue = zeroed_queue;
+    cfg.queue_zeroed = zeroed_queue != nullptr;
+    launch_lm(ctx, psf, L, n_cut, d_off, d_ny, d_nx, d_y1, d_x1, d_pix, eltype, d_iv, d_init, o, total_pixels, cfg);
 }
 
 int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut,

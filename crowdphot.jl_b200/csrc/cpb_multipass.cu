@@ -23,6 +23,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <cub/cub.cuh>
+
 #include "cpb_internal.cuh"
 
 namespace cpb {
@@ -55,36 +57,28 @@ __device__ __forceinline__ double mp_model(const DevPsf& P, const MPConst& M, co
     return model_value<double, double>(P, P.data64, c, (double)i, (double)j);
 }
 
-// add_star! / subtract_star! (PSF.jl:420-447) over each star's box: one warp a
-// star, lanes over the box pixels.  flags (nullable): stars with 0 are skipped.
-__global__ void k_mp_addsub(int nL, const int4* __restrict__ boxes, const double* __restrict__ params,
-                            const uint8_t* __restrict__ flags, double sign, DevPsf P, MPConst M, double* residual,
-                            int ny) {
-    const int lane = threadIdx.x & 31;
-    const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-    if (s >= nL || (flags && !flags[s])) return;
-    const int4 b = boxes[s];  // y1, x1, box rows, box columns
-    const double* pr = params + (int64_t)s * M.np;
-    for (int e = lane; e < b.z * b.w; e += 32) {
-        const int i = b.x + e % b.z, j = b.y + e / b.z;
-        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
-        residual[q] = residual[q] + sign * mp_model(P, M, pr, i, j);
-    }
-}
-
+// Passes 2+: add_star! (PSF.jl:420-428) of the star's previous model over its
+// box, then the fit_star cutout of the running residual (and of inv_var) at
+// offs[s] -- one warp a star, lanes over the box pixels.
 template <typename TI>
-__global__ void k_mp_cutouts(int nL, const int4* __restrict__ boxes, const int64_t* __restrict__ offs,
-                             const double* __restrict__ residual, const TI* __restrict__ iv, int ny,
-                             double* __restrict__ pix, double* __restrict__ ivc) {
+__global__ void k_mp_addcut(int nL, const int4* __restrict__ boxes, const double* __restrict__ params, int add,
+                            DevPsf P, MPConst M, double* residual, const TI* __restrict__ iv, int ny,
+                            const int64_t* __restrict__ offs, double* __restrict__ pix, double* __restrict__ ivc) {
     const int lane = threadIdx.x & 31;
     const int s = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (s >= nL) return;
-    const int4 b = boxes[s];
+    const int4 b = boxes[s];  // y1, x1, box rows, box columns
+    const double* pr = params + (int64_t)s * M.np;
     const int64_t o = offs[s];
     for (int e = lane; e < b.z * b.w; e += 32) {
         const int i = b.x + e % b.z, j = b.y + e / b.z;
         const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
-        pix[o + e] = residual[q];
+        double r = residual[q];
+        if (add) {
+            r = r + mp_model(P, M, pr, i, j);
+            residual[q] = r;
+        }
+        pix[o + e] = r;
         if (iv) ivc[o + e] = (double)iv[q];
     }
 }
@@ -103,7 +97,8 @@ __global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4*
                                                          const TI* __restrict__ img,
                                                          const double* __restrict__ residual,
                                                          const TI* __restrict__ iv, DevPsf P, MPConst M, int n_free,
-                                                         int ny, SpreadDev D, int smode, int boxmax, double* __restrict__ out) {
+                                                         int ny, SpreadDev D, int smode, int boxmax,
+                                                         const int32_t* __restrict__ idx, double* __restrict__ out) {
     extern __shared__ double stamp[];  // model stamp, x-pass scratch, disk-correlated stamp
     __shared__ double red[12 * (kDiagThreads / 32)];
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
@@ -113,7 +108,7 @@ __global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4*
         for (int i = threadIdx.x; i < 6 * (2 * D.kh + 1); i += blockDim.x) Is[i] = D.I[i];
     for (int s = blockIdx.x; s < nL; s += gridDim.x) {
         __syncthreads();  // the previous star's stamps are no longer read
-        double* o = out + (int64_t)s * 6;
+        double* o = out + (int64_t)idx[s] * 6;  // star order
         const double* pr = params + (int64_t)s * M.np;
         const double flux = pr[M.rf], bkg = pr[M.rb];
         if (flags[s] != 2 || !(flux > 0)) {  // 2: fitted in this batch
@@ -200,41 +195,213 @@ __global__ void k_mp_init(int64_t npix, const TI* __restrict__ img, double* __re
     if (q < npix) residual[q] = (double)img[q];
 }
 
-// Bookkeeping of one batch after its fit_star launch (:373-401), one thread a
-// star: on success the star's parameters, errors of the free parameters,
-// convergence, chi^2 and iteration count are updated and its new model is
-// queued for subtraction (flag 2); a fit that failed the input checks
-// invalidates the star and, on passes 2+, queues its previous model again to
-// undo the add-back (flag 1).  Positions index the batch; idx maps them to stars.
-__global__ void k_mp_book(int nL, const int32_t* __restrict__ idx, int pass, int np, int nf, MPFree F,
-                          const double* __restrict__ lm_params, const double* __restrict__ lm_cov,
-                          const double* __restrict__ lm_chisq, const uint8_t* __restrict__ lm_conv,
-                          const int32_t* __restrict__ lm_iters, const int32_t* __restrict__ lm_status,
-                          const double* __restrict__ pin, double* __restrict__ prm, double* __restrict__ err,
-                          uint8_t* __restrict__ conv, double* __restrict__ chisq, int32_t* __restrict__ niter,
-                          uint8_t* __restrict__ valid, int* __restrict__ n_failed, double* __restrict__ psub,
-                          uint8_t* __restrict__ flag) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+// Bookkeeping of one batch after its fit_star launch (:373-401) and the
+// subtraction that follows, one warp a star: on success the star's parameters,
+// errors of the free parameters, convergence, chi^2 and iteration count are
+// updated and its new model is subtracted (flag 2); a fit that failed the input
+// checks invalidates the star and, on passes 2+, subtracts its previous model
+// again to undo the add-back (flag 1).  Positions index the batch; idx maps
+// them to stars.  psub / flag keep the subtracted model for the diagnostics.
+__global__ void k_mp_booksub(int nL, const int32_t* __restrict__ idx, int pass, int nf, MPFree F,
+                             const double* __restrict__ lm_params, const double* __restrict__ lm_cov,
+                             const double* __restrict__ lm_chisq, const uint8_t* __restrict__ lm_conv,
+                             const int32_t* __restrict__ lm_iters, const int32_t* __restrict__ lm_status,
+                             const double* __restrict__ pin, const int4* __restrict__ boxes, DevPsf P, MPConst M,
+                             double* residual, int ny, double* __restrict__ prm, double* __restrict__ err,
+                             uint8_t* __restrict__ conv, double* __restrict__ chisq, int32_t* __restrict__ niter,
+                             uint8_t* __restrict__ valid, int* __restrict__ n_failed, double* __restrict__ psub,
+                             uint8_t* __restrict__ flag) {
+    const int lane = threadIdx.x & 31;
+    const int k = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (k >= nL) return;
+    const int np = M.np;
     const int64_t s = idx[k];
-    if (lm_status[k] != 0) {  // fit_star threw (:391-401)
+    const bool failed = lm_status[k] != 0;
+    const double* src = failed ? pin + (int64_t)k * np : lm_params + (int64_t)k * np;
+    double* ps = psub + (int64_t)k * np;
+    if (lane == 0) {
+        if (failed) {  // fit_star threw (:391-401)
+            valid[s] = 0;
+            atomicAdd(n_failed, 1);
+            flag[k] = pass > 1 ? 1 : 0;
+        } else {
+            for (int q = 0; q < np; ++q) prm[s * np + q] = src[q];
+            for (int a = 0; a < nf; ++a)
+                err[s * np + F.idx[a]] = sqrt(fmax(0.0, lm_cov[(int64_t)k * nf * nf + a + a * nf]));
+            conv[s] = lm_conv[k];
+            chisq[s] = lm_chisq[k];
+            niter[s] += lm_iters[k];
+            flag[k] = 2;
+        }
+        for (int q = 0; q < np; ++q) ps[q] = src[q];
+    }
+    if (failed && pass == 1) return;
+    // subtract_star! of the new (or, undoing the add-back, the previous) model
+    double pr[5];
+    for (int q = 0; q < np; ++q) pr[q] = src[q];
+    const int4 b = boxes[k];
+    for (int e = lane; e < b.z * b.w; e += 32) {
+        const int i = b.x + e % b.z, j = b.y + e / b.z;
+        const int64_t q = (i - 1) + (int64_t)(j - 1) * ny;
+        residual[q] = residual[q] - mp_model(P, M, pr, i, j);
+    }
+}
+
+// ---- the plan of a pass on the device ---------------------------------------
+// Order-preserving 64-bit key of a double (NaN above +inf, as isless orders it).
+__device__ __forceinline__ unsigned long long mp_dkey(double v) {
+    if (v != v) return 0xffffffffffffffffull;
+    const unsigned long long bits = (unsigned long long)__double_as_longlong(v);
+    return (bits >> 63) ? ~bits : (bits | 0x8000000000000000ull);
+}
+
+// Per star at the pass start: its +-fit_rad box clamped to the image (:343-348)
+// or invalidation (non-finite position, fewer than 3 box pixels), its grid cell
+// (cells at least one box wide, so overlapping boxes have their corners in
+// neighbouring cells), and the brightness key (flux descending; invalid last).
+__global__ void k_plan_box(int n, const double* __restrict__ prm, MPConst M, double fit_rad, int ny, int nx,
+                           int cell, int gny, uint8_t* __restrict__ valid, int4* __restrict__ box,
+                           int32_t* __restrict__ cellid, unsigned long long* __restrict__ fkey,
+                           int32_t* __restrict__ iota, int32_t* __restrict__ cell_count) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    iota[s] = s;
+    cellid[s] = -1;
+    fkey[s] = 0xffffffffffffffffull;
+    if (!valid[s]) return;
+    const double y = prm[(int64_t)s * M.np + M.ry], x = prm[(int64_t)s * M.np + M.rx];
+    if (!(isfinite(y) && isfinite(x))) {
         valid[s] = 0;
-        atomicAdd(n_failed, 1);
-        for (int q = 0; q < np; ++q) psub[(int64_t)k * np + q] = pin[(int64_t)k * np + q];
-        flag[k] = pass > 1 ? 1 : 0;
         return;
     }
-    for (int q = 0; q < np; ++q) {
-        const double v = lm_params[(int64_t)k * np + q];
-        prm[s * np + q] = v;
-        psub[(int64_t)k * np + q] = v;
+    const int ylo = (int)fmax(floor(y - fit_rad), 1.0), yhi = (int)fmin(ceil(y + fit_rad), (double)ny);
+    const int xlo = (int)fmax(floor(x - fit_rad), 1.0), xhi = (int)fmin(ceil(x + fit_rad), (double)nx);
+    const int by = max(yhi - ylo + 1, 0), bx = max(xhi - xlo + 1, 0);
+    if ((int64_t)by * bx < 3) {
+        valid[s] = 0;
+        return;
     }
-    for (int a = 0; a < nf; ++a)
-        err[s * np + F.idx[a]] = sqrt(fmax(0.0, lm_cov[(int64_t)k * nf * nf + a + a * nf]));
-    conv[s] = lm_conv[k];
-    chisq[s] = lm_chisq[k];
-    niter[s] += lm_iters[k];
-    flag[k] = 2;
+    box[s] = make_int4(ylo, xlo, by, bx);
+    const int c = ((xlo - 1) / cell) * gny + (ylo - 1) / cell;
+    cellid[s] = c;
+    atomicAdd(&cell_count[c], 1);
+    // ascending key = descending flux; the sort is stable, so ties keep the star order
+    fkey[s] = ~mp_dkey(prm[(int64_t)s * M.np + M.rf]);
+}
+
+__global__ void k_plan_rank(int n, const int32_t* __restrict__ order, int32_t* __restrict__ rank,
+                            int32_t* __restrict__ level) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    rank[order[k]] = k;
+    level[k] = 0;
+}
+
+__global__ void k_plan_cells(int n, const int32_t* __restrict__ cellid, const int32_t* __restrict__ cell_start,
+                             int32_t* __restrict__ cell_fill, int32_t* __restrict__ cell_list) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || cellid[s] < 0) return;
+    const int c = cellid[s];
+    cell_list[cell_start[c] + atomicAdd(&cell_fill[c], 1)] = s;
+}
+
+// One relaxation sweep of level(s) = 1 + max level of the brighter stars whose
+// boxes meet box(s) (0 if none).  Levels only grow towards the fixed point, so
+// sweeps may run in place; a sweep that changes nothing ends the iteration.
+__global__ void k_plan_relax(int n, const int4* __restrict__ box, const int32_t* __restrict__ cellid,
+                             const int32_t* __restrict__ rank, const int32_t* __restrict__ cell_start,
+                             const int32_t* __restrict__ cell_list, int gny, int gnx, int32_t* level,
+                             int* __restrict__ changed) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || cellid[s] < 0) return;
+    const int4 bs = box[s];
+    const int ylo = bs.x, yhi = bs.x + bs.z - 1, xlo = bs.y, xhi = bs.y + bs.w - 1;
+    const int rs = rank[s];
+    const int cx = cellid[s] / gny, cy = cellid[s] % gny;
+    int lv = 0;
+    for (int gx = max(cx - 1, 0); gx <= min(cx + 1, gnx - 1); ++gx)
+        for (int gy = max(cy - 1, 0); gy <= min(cy + 1, gny - 1); ++gy) {
+            const int c = gx * gny + gy;
+            for (int q = cell_start[c]; q < cell_start[c + 1]; ++q) {
+                const int t = cell_list[q];
+                if (rank[t] >= rs) continue;
+                const int4 bt = box[t];
+                if (bt.x <= yhi && ylo <= bt.x + bt.z - 1 && bt.y <= xhi && xlo <= bt.y + bt.w - 1)
+                    lv = max(lv, ((volatile const int32_t*)level)[t] + 1);
+            }
+        }
+    if (lv > level[s]) {
+        atomicMax(&level[s], lv);
+        *changed = 1;
+    }
+}
+
+__global__ void k_plan_poskey(int n, const int32_t* __restrict__ cellid, const int32_t* __restrict__ level,
+                              const int32_t* __restrict__ rank, unsigned long long* __restrict__ key) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    key[s] = cellid[s] < 0 ? 0xffffffffffffffffull
+                           : ((unsigned long long)(unsigned)level[s] << 32) | (unsigned long long)(unsigned)rank[s];
+}
+
+// Per position (level order): box, initial parameters, fit_star dims planes,
+// box size; level starts, and npos / nlev into meta.
+__global__ void k_plan_pos(int n, const int32_t* __restrict__ idx, const unsigned long long* __restrict__ skey,
+                           const int4* __restrict__ box_s, const double* __restrict__ prm, int np,
+                           const int32_t* __restrict__ level, int4* __restrict__ box, double* __restrict__ pin,
+                           int32_t* __restrict__ dims, int64_t* __restrict__ size, int32_t* __restrict__ lev_start,
+                           int32_t* __restrict__ meta) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const bool ok = skey[k] != 0xffffffffffffffffull;
+    const bool last = k == n - 1 || skey[k + 1] == 0xffffffffffffffffull;
+    if (!ok) {
+        size[k] = 0;
+        if (k == 0) meta[0] = meta[1] = 0;
+        return;
+    }
+    const int s = idx[k];
+    const int4 b = box_s[s];
+    box[k] = b;
+    for (int q = 0; q < np; ++q) pin[(int64_t)k * np + q] = prm[(int64_t)s * np + q];
+    dims[k] = b.z;
+    dims[n + k] = b.w;
+    dims[2 * n + k] = b.x;
+    dims[3 * n + k] = b.y;
+    size[k] = (int64_t)b.z * b.w;
+    const int L = level[s];
+    if (k == 0 || level[idx[k - 1]] != L) lev_start[L] = k;
+    if (last) {
+        meta[0] = k + 1;  // positions
+        meta[1] = L + 1;  // levels
+        lev_start[L + 1] = k + 1;
+    }
+}
+
+// Cutout offsets from each level's first pixel, and each level's pixel count.
+__global__ void k_plan_offsets(int npos, int nlev, const int32_t* __restrict__ idx,
+                               const int32_t* __restrict__ level, const int64_t* __restrict__ scan,
+                               const int32_t* __restrict__ lev_start, int64_t* __restrict__ off,
+                               int64_t* __restrict__ lev_pix) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < npos) off[k] = scan[k] - scan[lev_start[level[idx[k]]]];
+    if (k < nlev) lev_pix[k] = scan[lev_start[k + 1]] - scan[lev_start[k]];
+}
+
+// Between-pass validation (:404-412).
+__global__ void k_mp_validate(int n, const double* __restrict__ prm, MPConst M, const uint8_t* __restrict__ conv,
+                              uint8_t* __restrict__ valid) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const double y = prm[(int64_t)s * M.np + M.ry], x = prm[(int64_t)s * M.np + M.rx];
+    const double f = prm[(int64_t)s * M.np + M.rf];
+    valid[s] = valid[s] && conv[s] && isfinite(y) && isfinite(x) && isfinite(f) && f > 0;
+}
+
+template <typename T>
+__global__ void k_mp_fill(int64_t n, T v, T* __restrict__ a) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
 }
 
 inline unsigned warps_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256); }
@@ -303,32 +470,75 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     // pass (level order; a pass never holds more than n positions)
     const int Rmax = (int)std::ceil(std::max(fit_rad, 0.0)) + 1;
     const int64_t box_max = (int64_t)(2 * Rmax + 1) * (2 * Rmax + 1);
+    const int cell = 2 * Rmax + 2;  // >= every box side
+    const int gny = (ny - 1) / cell + 1, gnx = (nx - 1) / cell + 1;
+    const int ncell = gny * gnx;
+    auto I32 = [&](const char* name, size_t cnt) { return (int32_t*)scratch(ctx, name, sizeof(int32_t) * std::max<size_t>(cnt, 1)); };
+    auto U64 = [&](const char* name, size_t cnt) {
+        return (unsigned long long*)scratch(ctx, name, sizeof(unsigned long long) * std::max<size_t>(cnt, 1));
+    };
     double* d_prm = (double*)scratch(ctx, "mp_prm", sizeof(double) * n * np);
     double* d_err = (double*)scratch(ctx, "mp_err", sizeof(double) * n * np);
     double* d_chisq = (double*)scratch(ctx, "mp_chisq", sizeof(double) * n);
-    int32_t* d_niter = (int32_t*)scratch(ctx, "mp_niter", sizeof(int32_t) * n);
+    int32_t* d_niter = I32("mp_niter", n);
     uint8_t* d_sflag = (uint8_t*)scratch(ctx, "mp_sflags", (size_t)n * 2);  // valid, converged
     uint8_t* d_valid = d_sflag;
     uint8_t* d_conv = d_sflag + n;
-    int* d_nfail = (int*)scratch(ctx, "mp_nfail", sizeof(int));
-    int32_t* d_idx = (int32_t*)scratch(ctx, "mp_idx", sizeof(int32_t) * n);
+    int32_t* d_misc = I32("mp_misc", 4);  // failures, changed, positions, levels
+    int* d_nfail = d_misc;
+    int* d_changed = d_misc + 1;
+    int32_t* d_meta = d_misc + 2;
+    double* d_diagS = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 6);
+    // plan
+    int4* d_boxs = (int4*)scratch(ctx, "mp_box_star", sizeof(int4) * n);
+    int32_t* d_cellid = I32("mp_cellid", n);
+    unsigned long long* d_fkey = U64("mp_fkey", n);
+    unsigned long long* d_fkey2 = U64("mp_fkey2", n);
+    int32_t* d_iota = I32("mp_iota", n);
+    int32_t* d_order = I32("mp_order", n);
+    int32_t* d_rank = I32("mp_rank", n);
+    int32_t* d_level = I32("mp_level", n);
+    int32_t* d_ccount = I32("mp_cell_count", ncell + 1);
+    int32_t* d_cstart = I32("mp_cell_start", ncell + 1);
+    int32_t* d_cfill = I32("mp_cell_fill", ncell);
+    int32_t* d_clist = I32("mp_cell_list", n);
+    unsigned long long* d_pkey = U64("mp_pkey", n);
+    unsigned long long* d_pkey2 = U64("mp_pkey2", n);
+    int32_t* d_idx = I32("mp_idx", n);
+    int64_t* d_size = (int64_t*)scratch(ctx, "mp_size", sizeof(int64_t) * (n + 1));
+    int64_t* d_scan = (int64_t*)scratch(ctx, "mp_scan", sizeof(int64_t) * (n + 1));
+    int32_t* d_lstart = I32("mp_lev_start", n + 1);
+    int64_t* d_lpix = (int64_t*)scratch(ctx, "mp_lev_pix", sizeof(int64_t) * n);
+    unsigned long long* d_queues = U64("mp_queues", n);
+    // per position
     int4* d_box = (int4*)scratch(ctx, "mp_box", sizeof(int4) * n);
     double* d_pin = (double*)scratch(ctx, "mp_pin", sizeof(double) * n * np);
     double* d_psub = (double*)scratch(ctx, "mp_psub", sizeof(double) * n * np);
     uint8_t* d_flag = (uint8_t*)scratch(ctx, "mp_flag", n);
     int64_t* d_off = (int64_t*)scratch(ctx, "mp_off", sizeof(int64_t) * n);
-    int32_t* d_dims = (int32_t*)scratch(ctx, "mp_dims", sizeof(int32_t) * n * 4);  // ny, nx, y1, x1 planes
+    int32_t* d_dims = I32("mp_dims", (size_t)n * 4);  // ny, nx, y1, x1 planes
     double* d_lmd = (double*)scratch(ctx, "mp_lm_f64", sizeof(double) * n * (np + nf * nf + 4));
     uint8_t* d_lmu = (uint8_t*)scratch(ctx, "mp_lm_u8", (size_t)n * 4);
-    int32_t* d_lmi = (int32_t*)scratch(ctx, "mp_lm_i32", sizeof(int32_t) * n * 2);
-    double* d_diag = (double*)scratch(ctx, "mp_diag", sizeof(double) * n * 6);
-    // cutout pixels of one batch: the largest batch of a pass sizes them (grown on demand)
+    int32_t* d_lmi = I32("mp_lm_i32", (size_t)n * 2);
+    // CUB temporary storage (the largest of the sorts and scans)
+    size_t tmp_bytes = 0, t = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t, d_fkey, d_fkey2, d_iota, d_order, (int)n, 0, 64, st);
+    tmp_bytes = std::max(tmp_bytes, t);
+    cub::DeviceScan::ExclusiveSum(nullptr, t, d_ccount, d_cstart, ncell + 1, st);
+    tmp_bytes = std::max(tmp_bytes, t);
+    cub::DeviceScan::ExclusiveSum(nullptr, t, d_size, d_scan, (int)n + 1, st);
+    tmp_bytes = std::max(tmp_bytes, t);
+    void* d_tmp = scratch(ctx, "mp_cub_tmp", std::max<size_t>(tmp_bytes, 16));
+
     check(cudaMemcpyAsync(d_prm, prm.data(), sizeof(double) * n * np, cudaMemcpyHostToDevice, st), "h2d");
     check(cudaMemcpyAsync(d_err, err.data(), sizeof(double) * n * np, cudaMemcpyHostToDevice, st), "h2d");
     check(cudaMemsetAsync(d_chisq, 0, sizeof(double) * n, st), "memset");
     check(cudaMemsetAsync(d_niter, 0, sizeof(int32_t) * n, st), "memset");
+    check(cudaMemsetAsync(d_valid, 1, (size_t)n, st), "memset");
     check(cudaMemsetAsync(d_conv, 0, (size_t)n, st), "memset");
-    check(cudaMemsetAsync(d_nfail, 0, sizeof(int), st), "memset");
+    check(cudaMemsetAsync(d_misc, 0, sizeof(int32_t) * 4, st), "memset");
+    k_mp_fill<double><<<(unsigned)((n * 6 + 255) / 256), 256, 0, st>>>(n * 6, NaN, d_diagS);
+    check(cudaGetLastError(), "k_mp_fill");
     MPFree F{};
     for (int a = 0; a < nf; ++a) F.idx[a] = free_idx[a];
     // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
@@ -351,109 +561,67 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         check(cudaFuncSetAttribute(k_mp_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
               "smem attr");
     }
-
-    // host plan of one pass (level order)
-    std::vector<int32_t> hidx;
-    std::vector<int4> hbox;
-    std::vector<double> hpin;
-    std::vector<int64_t> hoff;
-    std::vector<int32_t> hdims;
-    std::vector<int64_t> lev_start, lev_pix;
-    std::vector<double> hdiag;
-    const double FTfit = fit_rad;
+    const unsigned gs = (unsigned)((n + 255) / 256);
+    std::vector<int32_t> lev_start;
+    std::vector<int64_t> lev_pix;
 
     for (int pass = 1; pass <= n_passes; ++pass) {
-        // brightest first, stable (sortperm(rev = true))
-        std::vector<int64_t> order(n);
-        std::iota(order.begin(), order.end(), 0);
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int64_t a, int64_t b) { return prm[a * np + M.rf] > prm[b * np + M.rf]; });
-        // boxes at the pass start and the batch of every valid star
-        std::vector<int4> box(n);
-        std::vector<int> level(n, -1);
-        int nlev = 0;
-        {
-            const int cell = 2 * Rmax + 2;
-            const int gnx = nx / cell + 2;
-            std::unordered_map<int64_t, std::vector<int64_t>> grid;
-            for (int64_t s : order) {
-                if (!valid[s]) continue;
-                const double y = prm[s * np + M.ry], x = prm[s * np + M.rx];
-                if (!(std::isfinite(y) && std::isfinite(x))) {
-                    valid[s] = 0;
-                    continue;
-                }
-                int ylo = (int)std::max(std::floor(y - FTfit), 1.0), yhi = (int)std::min(std::ceil(y + FTfit), (double)ny);
-                int xlo = (int)std::max(std::floor(x - FTfit), 1.0), xhi = (int)std::min(std::ceil(x + FTfit), (double)nx);
-                const int64_t by = std::max(yhi - ylo + 1, 0), bx = std::max(xhi - xlo + 1, 0);
-                if (by * bx < 3) {  // :343-348
-                    valid[s] = 0;
-                    continue;
-                }
-                box[s] = make_int4(ylo, xlo, (int)by, (int)bx);
-                int lv = 0;
-                const int cy0 = (ylo - 1) / cell, cy1 = (yhi - 1) / cell, cx0 = (xlo - 1) / cell, cx1 = (xhi - 1) / cell;
-                for (int cx = cx0; cx <= cx1; ++cx)
-                    for (int cy = cy0; cy <= cy1; ++cy) {
-                        auto it = grid.find((int64_t)cy * gnx + cx);
-                        if (it == grid.end()) continue;
-                        for (int64_t t : it->second) {
-                            const int4& bt = box[t];
-                            if (bt.x <= yhi && ylo <= bt.x + bt.z - 1 && bt.y <= xhi && xlo <= bt.y + bt.w - 1)
-                                lv = std::max(lv, level[t] + 1);
-                        }
-                    }
-                level[s] = lv;
-                nlev = std::max(nlev, lv + 1);
-                for (int cx = cx0; cx <= cx1; ++cx)
-                    for (int cy = cy0; cy <= cy1; ++cy) grid[(int64_t)cy * gnx + cx].push_back(s);
-            }
+        // ---- plan (:326-348): brightness order, boxes, and the batch (level)
+        // of every valid star, all on the device
+        check(cudaMemsetAsync(d_ccount, 0, sizeof(int32_t) * (ncell + 1), st), "memset");
+        check(cudaMemsetAsync(d_cfill, 0, sizeof(int32_t) * ncell, st), "memset");
+        k_plan_box<<<gs, 256, 0, st>>>((int)n, d_prm, M, fit_rad, ny, nx, cell, gny, d_valid, d_boxs, d_cellid, d_fkey,
+                                       d_iota, d_ccount);
+        check(cudaGetLastError(), "k_plan_box");
+        t = tmp_bytes;
+        check(cub::DeviceRadixSort::SortPairs(d_tmp, t, d_fkey, d_fkey2, d_iota, d_order, (int)n, 0, 64, st), "sort");
+        k_plan_rank<<<gs, 256, 0, st>>>((int)n, d_order, d_rank, d_level);
+        t = tmp_bytes;
+        check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_ccount, d_cstart, ncell + 1, st), "scan");
+        k_plan_cells<<<gs, 256, 0, st>>>((int)n, d_cellid, d_cstart, d_cfill, d_clist);
+        check(cudaGetLastError(), "k_plan_cells");
+        for (int64_t sweep = 0;; sweep += 2) {
+            if (sweep > n + 2) throw CudaError{cudaErrorUnknown, "fit_all_stars: the batch plan did not converge"};
+            int changed = 0;
+            check(cudaMemsetAsync(d_changed, 0, sizeof(int), st), "memset");
+            for (int k = 0; k < 2; ++k)
+                k_plan_relax<<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx,
+                                                 d_level, d_changed);
+            check(cudaGetLastError(), "k_plan_relax");
+            check(cudaMemcpyAsync(&changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaStreamSynchronize(st), "sync");
+            if (!changed) break;
         }
-        // positions in level order (brightness order inside a level), each
-        // batch's cutouts packed from offset 0
-        std::vector<int64_t> cnt(nlev + 1, 0);
-        for (int64_t s : order)
-            if (valid[s] && level[s] >= 0) cnt[level[s] + 1] += 1;
-        lev_start.assign(nlev + 1, 0);
-        for (int L = 0; L < nlev; ++L) lev_start[L + 1] = lev_start[L] + cnt[L + 1];
-        const int64_t npos = lev_start[nlev];
-        hidx.resize(npos);
-        hbox.resize(npos);
-        hpin.resize((size_t)npos * np);
-        hoff.resize(npos);
-        hdims.resize((size_t)npos * 4);
-        lev_pix.assign(nlev, 0);
-        {
-            std::vector<int64_t> fill(lev_start.begin(), lev_start.end() - 1);
-            for (int64_t s : order) {
-                if (!(valid[s] && level[s] >= 0)) continue;
-                const int L = level[s];
-                const int64_t k = fill[L]++;
-                hidx[k] = (int32_t)s;
-                hbox[k] = box[s];
-                std::memcpy(&hpin[(size_t)k * np], &prm[s * np], sizeof(double) * np);
-                hoff[k] = lev_pix[L];
-                lev_pix[L] += (int64_t)box[s].z * box[s].w;
-                hdims[k] = box[s].z;
-                hdims[npos + k] = box[s].w;
-                hdims[2 * npos + k] = box[s].x;
-                hdims[3 * npos + k] = box[s].y;
-            }
-        }
+        k_plan_poskey<<<gs, 256, 0, st>>>((int)n, d_cellid, d_level, d_rank, d_pkey);
+        t = tmp_bytes;
+        check(cub::DeviceRadixSort::SortPairs(d_tmp, t, d_pkey, d_pkey2, d_iota, d_idx, (int)n, 0, 64, st), "sort");
+        k_plan_pos<<<gs, 256, 0, st>>>((int)n, d_idx, d_pkey2, d_boxs, d_prm, np, d_level, d_box, d_pin, d_dims, d_size,
+                                       d_lstart, d_meta);
+        check(cudaGetLastError(), "k_plan_pos");
+        check(cudaMemsetAsync(d_size + n, 0, sizeof(int64_t), st), "memset");
+        t = tmp_bytes;
+        check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_size, d_scan, (int)n + 1, st), "scan");
+        int32_t meta[2] = {0, 0};
+        check(cudaMemcpyAsync(meta, d_meta, sizeof(meta), cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaStreamSynchronize(st), "sync");
+        const int npos = meta[0], nlev = meta[1];
         out->n_levels += nlev;
         out->n_fits += npos;
-        const int64_t pix_max = lev_pix.empty() ? 1 : std::max<int64_t>(1, *std::max_element(lev_pix.begin(), lev_pix.end()));
+        lev_start.assign(nlev + 1, 0);
+        lev_pix.assign(std::max(nlev, 1), 0);
+        if (npos > 0) {
+            k_plan_offsets<<<(unsigned)((std::max(npos, nlev) + 255) / 256), 256, 0, st>>>(npos, nlev, d_idx, d_level,
+                                                                                        d_scan, d_lstart, d_off, d_lpix);
+            check(cudaGetLastError(), "k_plan_offsets");
+            check(cudaMemcpyAsync(lev_start.data(), d_lstart, sizeof(int32_t) * (nlev + 1), cudaMemcpyDeviceToHost, st),
+                  "d2h");
+            check(cudaMemcpyAsync(lev_pix.data(), d_lpix, sizeof(int64_t) * nlev, cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaMemsetAsync(d_queues, 0, sizeof(unsigned long long) * nlev, st), "memset");
+            check(cudaStreamSynchronize(st), "sync");
+        }
+        const int64_t pix_max = std::max<int64_t>(1, *std::max_element(lev_pix.begin(), lev_pix.end()));
         double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * pix_max);
         double* d_civ = d_iv ? (double*)scratch(ctx, "mp_civ", sizeof(double) * pix_max) : nullptr;
-        if (npos > 0) {
-            check(cudaMemcpyAsync(d_valid, valid.data(), (size_t)n, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_idx, hidx.data(), sizeof(int32_t) * npos, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_box, hbox.data(), sizeof(int4) * npos, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_pin, hpin.data(), sizeof(double) * npos * np, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_off, hoff.data(), sizeof(int64_t) * npos, cudaMemcpyHostToDevice, st), "h2d");
-            check(cudaMemcpyAsync(d_dims, hdims.data(), sizeof(int32_t) * npos * 4, cudaMemcpyHostToDevice, st),
-                  "h2d");
-        }
         // fit_star results per position
         double* lm_par = d_lmd;
         double* lm_cov = d_lmd + (size_t)npos * np;
@@ -464,21 +632,17 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             if (nL == 0) continue;
             const int64_t tot = lev_pix[L];
             const int4* bx = d_box + p0;
-            // passes 2+: the star's previous model goes back in (:360-365)
-            if (pass > 1) {
-                KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
-                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_pin + p0 * np, nullptr, 1.0, dp, M, resid, ny);
-                check(cudaGetLastError(), "k_mp_addsub");
-            }
-            {
-                KernelScope ks_(ctx, "k_mp_cutouts", (double)tot * (d_iv ? 32 : 16));
+            {  // passes 2+: the star's previous model goes back in (:360-365); the cutouts
+                KernelScope ks_(ctx, "k_mp_addcut", (double)tot * (pass > 1 ? 32 : 16) + (d_iv ? tot * 16.0 : 0.0));
                 if (eltype == CPB_F64)
-                    k_mp_cutouts<double><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_off + p0, resid,
-                                                                       (const double*)d_iv, ny, d_cpix, d_civ);
+                    k_mp_addcut<double><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_pin + p0 * np, pass > 1, dp, M, resid,
+                                                                      (const double*)d_iv, ny, d_off + p0, d_cpix,
+                                                                      d_civ);
                 else
-                    k_mp_cutouts<float><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_off + p0, resid,
-                                                                      (const float*)d_iv, ny, d_cpix, d_civ);
-                check(cudaGetLastError(), "k_mp_cutouts");
+                    k_mp_addcut<float><<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_pin + p0 * np, pass > 1, dp, M, resid,
+                                                                     (const float*)d_iv, ny, d_off + p0, d_cpix,
+                                                                     d_civ);
+                check(cudaGetLastError(), "k_mp_addcut");
             }
             // fit_star on every box of the batch (:367-371): the fit_star kernel
             cpb_lm_result r{};
@@ -494,19 +658,15 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             r.g_converged = d_lmu + 3 * npos + p0;
             r.iterations = d_lmi + p0;
             r.status = d_lmi + npos + p0;
-            lm_enqueue_device(ctx, psf, P, nL, d_off + p0, d_dims + p0, d_dims + npos + p0, d_dims + 2 * npos + p0,
-                              d_dims + 3 * npos + p0, d_cpix, CPB_F64, d_civ, d_pin + p0 * np, tot, &r);
-            // bookkeeping (:373-401) and what to subtract
-            k_mp_book<<<(unsigned)((nL + 127) / 128), 128, 0, st>>>(
-                nL, d_idx + p0, pass, np, nf, F, r.params, r.cov, r.chisq, r.converged, r.iterations, r.status,
-                d_pin + p0 * np, d_prm, d_err, d_conv, d_chisq, d_niter, d_valid, d_nfail, d_psub + p0 * np,
-                d_flag + p0);
-            check(cudaGetLastError(), "k_mp_book");
-            {
-                KernelScope ks_(ctx, "k_mp_addsub", (double)tot * 16);
-                k_mp_addsub<<<warps_grid(nL), 256, 0, st>>>(nL, bx, d_psub + p0 * np, d_flag + p0, -1.0, dp, M, resid,
-                                                            ny);
-                check(cudaGetLastError(), "k_mp_addsub");
+            lm_enqueue_device(ctx, psf, P, nL, d_off + p0, d_dims + p0, d_dims + n + p0, d_dims + 2 * n + p0,
+                              d_dims + 3 * n + p0, d_cpix, CPB_F64, d_civ, d_pin + p0 * np, tot, &r, 4, d_queues + L);
+            {  // bookkeeping (:373-401) and the subtraction
+                KernelScope ks_(ctx, "k_mp_booksub", (double)tot * 16);
+                k_mp_booksub<<<warps_grid(nL), 256, 0, st>>>(
+                    nL, d_idx + p0, pass, nf, F, r.params, r.cov, r.chisq, r.converged, r.iterations, r.status,
+                    d_pin + p0 * np, bx, dp, M, resid, ny, d_prm, d_err, d_conv, d_chisq, d_niter, d_valid, d_nfail,
+                    d_psub + p0 * np, d_flag + p0);
+                check(cudaGetLastError(), "k_mp_booksub");
             }
             if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389)
                 KernelScope ks_(ctx, "k_mp_diag", (double)tot * (d_iv ? 24 : 16));
@@ -514,39 +674,23 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 if (eltype == CPB_F64)
                     k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
                         nL, bx, d_psub + p0 * np, d_flag + p0, (const double*)d_img, resid, (const double*)d_iv, dp,
-                        M, nf, ny, sd, smode, boxmax, d_diag + p0 * 6);
+                        M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
                 else
                     k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
                         nL, bx, d_psub + p0 * np, d_flag + p0, (const float*)d_img, resid, (const float*)d_iv, dp,
-                        M, nf, ny, sd, smode, boxmax, d_diag + p0 * 6);
+                        M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
                 check(cudaGetLastError(), "k_mp_diag");
             }
         }
-        // the pass's state back on the host: parameters and flags for the next
-        // pass's plan; on the last pass also the diagnostics of every position
-        check(cudaMemcpyAsync(prm.data(), d_prm, sizeof(double) * n * np, cudaMemcpyDeviceToHost, st), "d2h");
-        std::vector<uint8_t> hflags((size_t)n * 2);
-        check(cudaMemcpyAsync(hflags.data(), d_sflag, (size_t)n * 2, cudaMemcpyDeviceToHost, st), "d2h");
-        if (pass == n_passes && npos > 0) {
-            hdiag.resize((size_t)npos * 6);
-            check(cudaMemcpyAsync(hdiag.data(), d_diag, sizeof(double) * npos * 6, cudaMemcpyDeviceToHost, st), "d2h");
-        }
-        check(cudaStreamSynchronize(st), "sync");
-        if (npos > 0)
-            for (int64_t s = 0; s < n; ++s) valid[s] = hflags[s];  // fit failures of this pass
-        for (int64_t s = 0; s < n; ++s) conv[s] = hflags[n + s];
-        if (pass == n_passes && npos > 0) {
-            // diagnostics of the fitted positions (k_mp_diag wrote NaN for the others)
-            for (int64_t k = 0; k < npos; ++k)
-                for (int t = 0; t < 6; ++t) diag[(int64_t)hidx[k] * 6 + t] = hdiag[(size_t)k * 6 + t];
-        }
         // between-pass validation (:404-412)
-        for (int64_t s = 0; s < n; ++s) {
-            const double y = prm[s * np + M.ry], x = prm[s * np + M.rx], f = prm[s * np + M.rf];
-            valid[s] = valid[s] && conv[s] && std::isfinite(y) && std::isfinite(x) && std::isfinite(f) && f > 0;
-        }
+        k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
+        check(cudaGetLastError(), "k_mp_validate");
     }
     check(cudaEventRecord(ctx->ev1, st), "event");
+    check(cudaMemcpyAsync(prm.data(), d_prm, sizeof(double) * n * np, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(valid.data(), d_valid, (size_t)n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(conv.data(), d_conv, (size_t)n, cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaMemcpyAsync(diag.data(), d_diagS, sizeof(double) * n * 6, cudaMemcpyDeviceToHost, st), "d2h");
     int nfail = 0;
     check(cudaMemcpyAsync(err.data(), d_err, sizeof(double) * n * np, cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(chisq.data(), d_chisq, sizeof(double) * n, cudaMemcpyDeviceToHost, st), "d2h");
