@@ -269,6 +269,61 @@ __device__ __forceinline__ T warp_max(T v) {
     return v;
 }
 
+// fit_all_stars (cpb_multipass.cu): per-star parameter rows.
+struct MPFree {
+    int idx[5];  // the free parameters' rows
+};
+
+struct MPConst {
+    int np;           // model parameters per star (4 image PSFs, 5 Gaussian)
+    int gauss;
+    int ry, rx, rf, rb, rw;  // rows of y, x, flux, bkg, fwhm (-1: none)
+};
+
+// The star's model at pixel (i, j) from its parameter row.
+__device__ __forceinline__ double mp_model(const DevPsf& P, const MPConst& M, const double* pr, int i, int j) {
+    StarCoef c;
+    c.y = pr[M.ry];
+    c.x = pr[M.rx];
+    c.flux = pr[M.rf];
+    c.bkg = pr[M.rb];
+    if (M.gauss) {
+        DevPsf Pj = P;
+        Pj.fwhm = pr[M.rw];
+        double a, b, e;
+        return gauss_eval<double, false>(Pj.fwhm, c, (double)i, (double)j, a, b, e);
+    }
+    grid_corners_dw(P, c.y, c.x, c);
+    return model_value<double, double>(P, P.data64, c, (double)i, (double)j);
+}
+
+// One dependency-driven fit_all_stars pass (k_mp_dag, cpb_lm.cu).
+struct DagArgs {
+    int npos, pass, ny, box_max;
+    MPConst M;
+    MPFree F;
+    const int32_t* idx;         // position -> star
+    const int4* box;            // per position: y1, x1, rows, columns
+    const double* pin;          // per position: parameters at the pass start
+    const int32_t* succ_start;  // per position (npos + 1): stars that wait for it
+    const int32_t* succ_list;
+    int32_t* indeg;             // per position: unfinished stars it waits for
+    int32_t* queue;             // npos ready positions, -1 = not yet
+    int32_t* counters;          // head, tail, error
+    double* resid;
+    const void* iv;             // image inv_var (nullable), eltype of the image
+    double *cpix, *civ;         // per team: box_max doubles each
+    double *prm, *err;
+    uint8_t *conv, *valid;
+    double* chisq;
+    int32_t* niter;
+    int* n_failed;
+    double* psub;               // per position: the subtracted model
+    uint8_t* flag;              // per position: 2 fitted, 1 add-back undone, 0 none
+    double* snap;               // last pass: residual box after the subtraction (nullable)
+    const int64_t* snap_off;    // per position
+};
+
 // The spread_model reference disk on the device.  The band-limited disk is a
 // sum of six separable Gaussian-mixture components, K = sum_c alpha_c I_c I_c',
 // with I_c zero beyond |m| = L_c (the reference's overflow cutoff), so the
@@ -604,6 +659,14 @@ int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64
                  const int64_t* offsets, const int32_t* ny, const int32_t* nx, const int32_t* y_origin,
                  const int32_t* x_origin, const void* pixels, int32_t eltype, const void* inv_var,
                  const double* init, cpb_lm_result* out);
+// fit_all_stars pass as one dependency-driven launch (cpb_lm.cu): whether the
+// PSF / keywords allow it (single-node image PSFs and the Gaussian, no IRLS),
+// the number of 128-thread teams the launch runs (its per-team scratch), and
+// the launch itself (iv_eltype: element type of the image and inv_var).
+bool mp_dag_supported(const cpb_psf* psf, const cpb_lm_params* P);
+int mp_dag_teams(cpb_ctx* ctx);
+void mp_dag_launch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int32_t iv_eltype, const DagArgs& A);
+
 // The fit_star launch of fit_lm_batch_device on the context's stream, with no
 // event, synchronisation or host read-back (callers chain further kernels).
 // team_warps: warps a cutout (0: chosen by the batch size; 1 or 4);

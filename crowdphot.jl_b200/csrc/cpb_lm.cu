@@ -1242,6 +1242,56 @@ __device__ __forceinline__ bool lm_step(LMState<NP, NF>& S, const LMConst& L, do
 
 constexpr int kLMThreads = 256;
 
+// fit_star of one cutout by a team (pixels pix / weights iv, column-major
+// ny x nx whose first pixel is image pixel (y1, x1); init: the NP model
+// parameters, fixed ones replaced by L.fixv).  Returns 0 with the result in S,
+// or CPB_ERR_ARGUMENT when the inputs fail _prepare_fit_star_inputs's checks
+// (psf_fitting.jl:61-90) or lm_irls's dof test (:461-467).
+template <typename TI, int NP, int NF, int WPC>
+__device__ int lm_team_fit(const PPNode& N, const double* pp, const LMConst& L, const TI* __restrict__ pix,
+                           const TI* __restrict__ iv, int ny, int nx, int y1, int x1, const double* init,
+                           LMState<NP, NF>& S, double* red, int lane) {
+    constexpr int TS = 32 * WPC;
+    const int64_t nobs = (int64_t)ny * nx;
+    if (ny <= 0 || nx <= 0) return CPB_ERR_ARGUMENT;
+    bool bad = !(nobs - NF > 0);
+    if (iv) {
+        double nv[1] = {0.0};
+        for (int64_t e = lane; e < nobs; e += TS) {
+            const double v = (double)iv[e];
+            nv[0] += (isfinite(v) && v > 0) ? 1.0 : 0.0;
+        }
+        team_sum<WPC, 1>(nv, red);
+        team_sync<WPC>();  // red is reused by the first normal-equation pass
+        bad = bad || !((int)nv[0] > NF);
+    }
+    if (bad) return CPB_ERR_ARGUMENT;
+    const int qs = TS / ny, rs = TS % ny;
+    team_sync<WPC>();
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+            bool fr = false;
+#pragma unroll
+            for (int k = 0; k < NF; ++k) fr |= (L.fidx[k] == q);
+            S.fc[q] = fr ? init[q] : L.fixv[q];
+        }
+        S.iter = 0;
+        S.phase = 0;
+        S.lam = L.lambda_init;
+        S.conv = S.xconv = S.fconv = S.gconv = 0;
+    }
+    team_sync<WPC>();
+    for (;;) {
+        double fc[NP], Ac[NF * NF], bc[NF];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) fc[q] = S.fc[q];
+        const double cost_c = lm_accum_t<TI, NP, NF, WPC>(N, pp, L, pix, iv, ny, nx, y1, x1, qs, rs, fc, Ac, bc, red);
+        if (lm_step<NP, NF, WPC>(S, L, cost_c, Ac, bc, lane)) break;
+    }
+    return 0;
+}
+
 template <typename TI, int NP, int NF, bool SMEM, int WPC>
 __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L, PPNode N,
                                              const int64_t* __restrict__ offs, const int32_t* __restrict__ cny,
@@ -1279,58 +1329,17 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
         }
         if (cc >= (unsigned long long)n_cut) return;
         const int64_t c = (int64_t)cc;
-        const int ny = cny[c], nx = cnx[c], y1 = cy1[c], x1 = cx1[c];
-        const int64_t nobs = (int64_t)ny * nx;
-        if (ny <= 0 || nx <= 0) {
-            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
+        const int ny = cny[c], nx = cnx[c];
+        const int64_t o = (ny > 0 && nx > 0) ? offs[c] : 0;
+        const int st = lm_team_fit<TI, NP, NF, WPC>(N, pp, L, pixels + o, ivs ? ivs + o : nullptr, ny, nx, cy1[c],
+                                                    cx1[c], init + c * NP, S, red, lane);
+        if (st != 0) {
+            if (lane == 0) out.status[c] = st;
             team_sync<WPC>();
             continue;
         }
-        const TI* pix = pixels + offs[c];
-        const TI* iv = ivs ? ivs + offs[c] : nullptr;
-        // _prepare_fit_star_inputs checks (psf_fitting.jl:61-90) and lm_irls dof (:461-467)
-        bool bad = !(nobs - NF > 0);
-        if (iv) {
-            double nv[1] = {0.0};
-            for (int64_t e = lane; e < nobs; e += TS) {
-                const double v = (double)iv[e];
-                nv[0] += (isfinite(v) && v > 0) ? 1.0 : 0.0;
-            }
-            team_sum<WPC, 1>(nv, red);
-            team_sync<WPC>();  // red is reused by the first normal-equation pass
-            bad = bad || !((int)nv[0] > NF);
-        }
-        if (bad) {
-            if (lane == 0) out.status[c] = CPB_ERR_ARGUMENT;
-            team_sync<WPC>();
-            continue;
-        }
-        const int qs = TS / ny, rs = TS % ny;
-        team_sync<WPC>();
         if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < NP; ++q) {
-                bool fr = false;
-#pragma unroll
-                for (int k = 0; k < NF; ++k) fr |= (L.fidx[k] == q);
-                S.fc[q] = fr ? init[c * NP + q] : L.fixv[q];
-            }
-            S.iter = 0;
-            S.phase = 0;
-            S.lam = L.lambda_init;
-            S.conv = S.xconv = S.fconv = S.gconv = 0;
-        }
-        team_sync<WPC>();
-        for (;;) {
-            double fc[NP], Ac[NF * NF], bc[NF];
-#pragma unroll
-            for (int q = 0; q < NP; ++q) fc[q] = S.fc[q];
-            const double cost_c =
-                lm_accum_t<TI, NP, NF, WPC>(N, pp, L, pix, iv, ny, nx, y1, x1, qs, rs, fc, Ac, bc, red);
-            if (lm_step<NP, NF, WPC>(S, L, cost_c, Ac, bc, lane)) break;
-        }
-        if (lane == 0) {
-            const double dof = (double)(nobs - NF);
+            const double dof = (double)((int64_t)ny * nx - NF);
             const double cost = S.cost;
             if (out.cov) {
                 double cov[NF * NF];
@@ -1353,6 +1362,149 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
             if (out.iters) out.iters[c] = S.iter;
             if (out.sigma_final) out.sigma_final[c] = __longlong_as_double(0x7ff8000000000000LL);
             out.status[c] = 0;
+        }
+        team_sync<WPC>();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// fit_all_stars as one dependency-driven launch per pass
+// ---------------------------------------------------------------------------
+// A star may be fitted as soon as every brighter star whose box meets its own
+// has been subtracted; stars that are ready together have disjoint boxes.  One
+// persistent launch per pass walks that order: 128-thread teams take ready
+// stars from a device queue (position indices, filled in the order they become
+// ready), add the star's previous model back (passes 2+), copy its cutout, fit
+// it (lm_team_fit), update the star's state, subtract the new model, keep a
+// snapshot of its box for the diagnostics on the last pass, and release the
+// stars that waited for it.  Each pixel still sees its adds and subtracts in
+// brightness order, so the result is the one-star-at-a-time one, but a slow
+// fit only holds back the stars that overlap it.  The residual image is read
+// and written around L1 (ld/st.cg): other SMs change it between uses.
+constexpr long long kDagSpinLimit = 1ll << 26;  // ~64 M polls of >= 64 ns before a team gives up
+
+template <typename TIV, int NP, int NF, bool SMEM>
+__global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, DevPsf P, DagArgs A) {
+    constexpr int WPC = 4, TS = 128;
+    constexpr int KR = 1 + NF + NF * (NF + 1) / 2;
+    __shared__ LMState<NP, NF> states[kLMThreads / TS];
+    __shared__ double red_all[(kLMThreads / 32) * KR];
+    __shared__ int pos_sh[kLMThreads / TS];
+    extern __shared__ double node_smem[];
+    const int team = threadIdx.x / TS;
+    LMState<NP, NF>& S = states[team];
+    double* red = red_all + team * WPC * KR;
+    const int lane = threadIdx.x % TS;
+    const int gteam = blockIdx.x * (kLMThreads / TS) + team;
+    double* cpix = A.cpix + (int64_t)gteam * A.box_max;
+    double* civ = A.civ ? A.civ + (int64_t)gteam * A.box_max : nullptr;
+    const TIV* ivimg = (const TIV*)A.iv;
+    const double* pp = N.pp;
+    if (SMEM && NP == 4) {
+        const int nel = N.plane * N.nd.isy * N.nd.isx;
+        for (int k = threadIdx.x; k < nel; k += blockDim.x) node_smem[k] = N.pp[k];
+        __syncthreads();
+        pp = node_smem;
+    }
+    int* head = A.counters;
+    int* tail = A.counters + 1;
+    int* errf = A.counters + 2;
+    const int np = A.M.np;
+    for (;;) {
+        // claim the next queue slot and wait (bounded) until a ready star fills it
+        if (lane == 0) {
+            int k = -2;
+            const int h = atomicAdd(head, 1);
+            if (h < A.npos) {
+                for (long long it = 0;; ++it) {
+                    k = ((volatile int32_t*)A.queue)[h];
+                    if (k >= 0) break;
+                    if (it > kDagSpinLimit || ((volatile int*)errf)[0]) {
+                        atomicExch(errf, 1);
+                        k = -2;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+            pos_sh[team] = k;
+        }
+        team_sync<WPC>();
+        const int k = pos_sh[team];
+        if (k < 0) return;
+        const int4 b = A.box[k];
+        const int nb = b.z * b.w;
+        const double* pin = A.pin + (int64_t)k * np;
+        // passes 2+: the previous model back in (:360-365), and the cutout
+        for (int e = lane; e < nb; e += TS) {
+            const int i = b.x + e % b.z, j = b.y + e / b.z;
+            const int64_t q = (i - 1) + (int64_t)(j - 1) * A.ny;
+            double r = __ldcg(A.resid + q);
+            if (A.pass > 1) {
+                r = r + mp_model(P, A.M, pin, i, j);
+                __stcg(A.resid + q, r);
+            }
+            cpix[e] = r;
+            if (civ) civ[e] = (double)ivimg[q];
+        }
+        team_sync<WPC>();
+        const int st = lm_team_fit<double, NP, NF, WPC>(N, pp, L, cpix, civ, b.z, b.w, b.x, b.y, pin, S, red, lane);
+        // bookkeeping (:373-401)
+        const int64_t s = A.idx[k];
+        double* ps = A.psub + (int64_t)k * np;
+        if (lane == 0) {
+            if (st != 0) {
+                A.valid[s] = 0;
+                atomicAdd(A.n_failed, 1);
+                A.flag[k] = A.pass > 1 ? 1 : 0;
+                for (int q = 0; q < np; ++q) ps[q] = pin[q];
+            } else {
+                const double dof = (double)((int64_t)nb - NF);
+                double cov[NF * NF];
+                lm_cov_t<NF>(S.A, cov);
+                const double f = L.reweighted ? S.cost / dof : 1.0;
+                for (int q = 0; q < np; ++q) {
+                    A.prm[s * np + q] = S.fv[q];
+                    ps[q] = S.fv[q];
+                }
+                for (int a = 0; a < NF; ++a) A.err[s * np + A.F.idx[a]] = sqrt(fmax(0.0, cov[a + a * NF] * f));
+                A.conv[s] = S.conv;
+                A.chisq[s] = S.cost / dof;
+                A.niter[s] += S.iter;
+                A.flag[k] = 2;
+            }
+        }
+        team_sync<WPC>();
+        // subtract_star! of the new (or, undoing the add-back, the previous) model
+        if (!(st != 0 && A.pass == 1)) {
+            double pr[NP];
+#pragma unroll
+            for (int q = 0; q < NP; ++q) pr[q] = ps[q];
+            for (int e = lane; e < nb; e += TS) {
+                const int i = b.x + e % b.z, j = b.y + e / b.z;
+                const int64_t q = (i - 1) + (int64_t)(j - 1) * A.ny;
+                const double r = __ldcg(A.resid + q) - mp_model(P, A.M, pr, i, j);
+                __stcg(A.resid + q, r);
+                if (A.snap) A.snap[A.snap_off[k] + e] = r;
+            }
+        } else if (A.snap) {
+            for (int e = lane; e < nb; e += TS) {
+                const int i = b.x + e % b.z, j = b.y + e / b.z;
+                A.snap[A.snap_off[k] + e] = __ldcg(A.resid + (i - 1) + (int64_t)(j - 1) * A.ny);
+            }
+        }
+        __threadfence();
+        team_sync<WPC>();
+        // release the stars that waited for this one
+        if (lane == 0) {
+            for (int q = A.succ_start[k]; q < A.succ_start[k + 1]; ++q) {
+                const int u = A.succ_list[q];
+                if (atomicSub(&A.indeg[u], 1) == 1) {
+                    const int t = atomicAdd(tail, 1);
+                    atomicExch(&A.queue[t], u);
+                }
+            }
         }
         team_sync<WPC>();
     }
@@ -1766,6 +1918,67 @@ int fit_lm_batch_device(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     out->device_seconds = ms * 1e-3;
     return 0;
+}
+
+
+bool mp_dag_supported(const cpb_psf* psf, const cpb_lm_params* P) {
+    const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    return (gauss || psf->dev.n_nodes == 1) && P->reweight == CPB_LOSS_NONE && P->precision == CPB_PREC_FP64;
+}
+
+int mp_dag_teams(cpb_ctx* ctx) { return ctx->n_sm * 2 * (kLMThreads / 128); }
+
+void mp_dag_launch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int32_t iv_eltype, const DagArgs& A) {
+    const LMConst L = lm_const(psf, P, A.iv != nullptr);
+    cudaStream_t st = ctx->stream;
+    const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
+    PPNode N{};
+    if (!gauss) {
+        N.nd = psf->h_nodes[0];
+        N.pp = psf->dev.lpp64 + N.nd.lpoff;
+        N.plane = N.nd.LPY * N.nd.LPX;
+        N.inv_isy = 1.0f / (float)N.nd.isy;
+        N.inv_isx = 1.0f / (float)N.nd.isx;
+    }
+    const size_t node_bytes = gauss ? 0 : sizeof(double) * (size_t)N.plane * N.nd.isy * N.nd.isx;
+    const bool smem = !gauss && node_bytes <= 100 * 1024;
+    const unsigned blocks = (unsigned)(ctx->n_sm * 2);  // persistent: every team resident
+    KernelScope ks_(ctx, "k_mp_dag", 0.0);
+#define CPB_DAG(TIV, NP, NF)                                                                                    \
+    do {                                                                                                        \
+        if (smem) {                                                                                             \
+            check(cudaFuncSetAttribute(k_mp_dag<TIV, NP, NF, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                       (int)node_bytes),                                                       \
+                  "smem attribute");                                                                           \
+            k_mp_dag<TIV, NP, NF, true><<<blocks, kLMThreads, node_bytes, st>>>(L, N, psf->dev, A);             \
+        } else {                                                                                                \
+            k_mp_dag<TIV, NP, NF, false><<<blocks, kLMThreads, 0, st>>>(L, N, psf->dev, A);                     \
+        }                                                                                                       \
+    } while (0)
+#define CPB_DAG_NF(TIV, NP)                     \
+    switch (L.nf) {                             \
+        case 1: CPB_DAG(TIV, NP, 1); break;     \
+        case 2: CPB_DAG(TIV, NP, 2); break;     \
+        case 3: CPB_DAG(TIV, NP, 3); break;     \
+        case 4: CPB_DAG(TIV, NP, 4); break;     \
+        default: CPB_DAG(TIV, NP, NP); break;   \
+    }
+    if (iv_eltype == CPB_F64) {
+        if (gauss) {
+            CPB_DAG_NF(double, 5)
+        } else {
+            CPB_DAG_NF(double, 4)
+        }
+    } else {
+        if (gauss) {
+            CPB_DAG_NF(float, 5)
+        } else {
+            CPB_DAG_NF(float, 4)
+        }
+    }
+#undef CPB_DAG_NF
+#undef CPB_DAG
+    check(cudaGetLastError(), "k_mp_dag");
 }
 
 }  // namespace cpb

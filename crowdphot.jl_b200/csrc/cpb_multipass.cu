@@ -30,33 +30,6 @@
 namespace cpb {
 namespace {
 
-struct MPFree {
-    int idx[5];  // the free parameters' rows
-};
-
-struct MPConst {
-    int np;           // model parameters per star (4 image PSFs, 5 Gaussian)
-    int gauss;
-    int ry, rx, rf, rb, rw;  // rows of y, x, flux, bkg, fwhm (-1: none)
-};
-
-// The star's model at pixel (i, j) from its parameter row.
-__device__ __forceinline__ double mp_model(const DevPsf& P, const MPConst& M, const double* pr, int i, int j) {
-    StarCoef c;
-    c.y = pr[M.ry];
-    c.x = pr[M.rx];
-    c.flux = pr[M.rf];
-    c.bkg = pr[M.rb];
-    if (M.gauss) {
-        DevPsf Pj = P;
-        Pj.fwhm = pr[M.rw];
-        double a, b, e;
-        return gauss_eval<double, false>(Pj.fwhm, c, (double)i, (double)j, a, b, e);
-    }
-    grid_corners_dw(P, c.y, c.x, c);
-    return model_value<double, double>(P, P.data64, c, (double)i, (double)j);
-}
-
 // Passes 2+: add_star! (PSF.jl:420-428) of the star's previous model over its
 // box, then the fit_star cutout of the running residual (and of inv_var) at
 // offs[s] -- one warp a star, lanes over the box pixels.
@@ -89,13 +62,17 @@ __global__ void k_mp_addcut(int nL, const int4* __restrict__ boxes, const double
 // shared memory with its disk-correlated copy for spread_model (D.I null:
 // spread_model off).  One block of kDiagThreads a star (grid-stride).  out:
 // qfit, qfit_expected, qfit_z, crowding, spread_model, spread_model_err per
-// star (NaN where undefined).
+// star (NaN where undefined).  snap (nullable): the star's residual box saved
+// right after its subtraction (snap_off per position), used in place of the
+// residual image when the diagnostics run after the whole pass.
 template <typename TI>
 __global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4* __restrict__ boxes,
                                                          const double* __restrict__ params,
                                                          const uint8_t* __restrict__ flags,
                                                          const TI* __restrict__ img,
                                                          const double* __restrict__ residual,
+                                                         const double* __restrict__ snap,
+                                                         const int64_t* __restrict__ snap_off,
                                                          const TI* __restrict__ iv, DevPsf P, MPConst M, int n_free,
                                                          int ny, SpreadDev D, int smode, int boxmax,
                                                          const int32_t* __restrict__ idx, double* __restrict__ out) {
@@ -138,7 +115,7 @@ __global__ void __launch_bounds__(kDiagThreads, 3) k_mp_diag(int nL, const int4*
             const double wp = iv ? (double)iv[q] : 1.0;
             if (isfinite(wp) && wp > 0) {
                 const double mv = spread ? stamp[e] : mp_model(P, M, pr, i, j);
-                const double r = residual[q];
+                const double r = snap ? snap[snap_off[s] + e] : residual[q];
                 v[0] += fabs(r);
                 const double Pp = (mv - bkg) * inv_flux;
                 const double wP = wp * Pp;
@@ -350,7 +327,7 @@ __global__ void k_plan_pos(int n, const int32_t* __restrict__ idx, const unsigne
                            const int4* __restrict__ box_s, const double* __restrict__ prm, int np,
                            const int32_t* __restrict__ level, int4* __restrict__ box, double* __restrict__ pin,
                            int32_t* __restrict__ dims, int64_t* __restrict__ size, int32_t* __restrict__ lev_start,
-                           int32_t* __restrict__ meta) {
+                           int32_t* __restrict__ meta, int32_t* __restrict__ pos_of) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const bool ok = skey[k] != 0xffffffffffffffffull;
@@ -361,6 +338,7 @@ __global__ void k_plan_pos(int n, const int32_t* __restrict__ idx, const unsigne
         return;
     }
     const int s = idx[k];
+    pos_of[s] = k;
     const int4 b = box_s[s];
     box[k] = b;
     for (int q = 0; q < np; ++q) pin[(int64_t)k * np + q] = prm[(int64_t)s * np + q];
@@ -386,6 +364,53 @@ __global__ void k_plan_offsets(int npos, int nlev, const int32_t* __restrict__ i
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k < npos) off[k] = scan[k] - scan[lev_start[level[idx[k]]]];
     if (k < nlev) lev_pix[k] = scan[lev_start[k + 1]] - scan[lev_start[k]];
+}
+
+// The dependency lists of a pass for k_mp_dag: per position, how many brighter
+// overlapping stars it waits for (indeg) and how many dimmer ones wait for it
+// (nsucc); then the waiting positions themselves (succ_list from succ_start).
+template <bool FILL>
+__global__ void k_dag_edges(int n, const int4* __restrict__ box, const int32_t* __restrict__ cellid,
+                            const int32_t* __restrict__ rank, const int32_t* __restrict__ cell_start,
+                            const int32_t* __restrict__ cell_list, int gny, int gnx, const int32_t* __restrict__ pos_of,
+                            int32_t* __restrict__ indeg, int32_t* __restrict__ nsucc,
+                            const int32_t* __restrict__ succ_start, int32_t* __restrict__ succ_list) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || cellid[s] < 0) return;
+    const int4 bs = box[s];
+    const int ylo = bs.x, yhi = bs.x + bs.z - 1, xlo = bs.y, xhi = bs.y + bs.w - 1;
+    const int rs = rank[s];
+    const int cx = cellid[s] / gny, cy = cellid[s] % gny;
+    const int k = pos_of[s];
+    int np_ = 0, ns = 0;
+    for (int gx = max(cx - 1, 0); gx <= min(cx + 1, gnx - 1); ++gx)
+        for (int gy = max(cy - 1, 0); gy <= min(cy + 1, gny - 1); ++gy) {
+            const int c = gx * gny + gy;
+            for (int q = cell_start[c]; q < cell_start[c + 1]; ++q) {
+                const int t = cell_list[q];
+                if (t == s) continue;
+                const int4 bt = box[t];
+                if (!(bt.x <= yhi && ylo <= bt.x + bt.z - 1 && bt.y <= xhi && xlo <= bt.y + bt.w - 1)) continue;
+                if (rank[t] < rs) {
+                    ++np_;
+                } else {
+                    if (FILL) succ_list[succ_start[k] + ns] = pos_of[t];
+                    ++ns;
+                }
+            }
+        }
+    if (!FILL) {
+        indeg[k] = np_;
+        nsucc[k] = ns;
+    }
+}
+
+// The ready queue of a pass: every position that waits for nobody.
+__global__ void k_dag_queue(int npos, const int32_t* __restrict__ indeg, int32_t* __restrict__ queue,
+                            int32_t* __restrict__ counters) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npos || indeg[k] != 0) return;
+    queue[atomicAdd(&counters[1], 1)] = k;
 }
 
 // Between-pass validation (:404-412).
@@ -510,6 +535,21 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     int32_t* d_lstart = I32("mp_lev_start", n + 1);
     int64_t* d_lpix = (int64_t*)scratch(ctx, "mp_lev_pix", sizeof(int64_t) * n);
     unsigned long long* d_queues = U64("mp_queues", n);
+    int32_t* d_posof = I32("mp_pos_of", n);
+    // dependency-driven passes (k_mp_dag): edges, ready queue, per-team cutouts
+    const bool dag = mp_dag_supported(psf, P);
+    int32_t *d_indeg = nullptr, *d_nsucc = nullptr, *d_sstart = nullptr, *d_queue = nullptr, *d_dagc = nullptr;
+    double *d_tpix = nullptr, *d_tiv = nullptr;
+    if (dag) {
+        d_indeg = I32("mp_indeg", n);
+        d_nsucc = I32("mp_nsucc", n + 1);
+        d_sstart = I32("mp_succ_start", n + 1);
+        d_queue = I32("mp_queue", n);
+        d_dagc = I32("mp_dag_counters", 4);
+        const int teams = mp_dag_teams(ctx);
+        d_tpix = (double*)scratch(ctx, "mp_team_pix", sizeof(double) * teams * box_max);
+        if (d_iv) d_tiv = (double*)scratch(ctx, "mp_team_iv", sizeof(double) * teams * box_max);
+    }
     // per position
     int4* d_box = (int4*)scratch(ctx, "mp_box", sizeof(int4) * n);
     double* d_pin = (double*)scratch(ctx, "mp_pin", sizeof(double) * n * np);
@@ -527,6 +567,8 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     cub::DeviceScan::ExclusiveSum(nullptr, t, d_ccount, d_cstart, ncell + 1, st);
     tmp_bytes = std::max(tmp_bytes, t);
     cub::DeviceScan::ExclusiveSum(nullptr, t, d_size, d_scan, (int)n + 1, st);
+    tmp_bytes = std::max(tmp_bytes, t);
+    cub::DeviceScan::ExclusiveSum(nullptr, t, d_ccount, d_cstart, (int)n + 1, st);
     tmp_bytes = std::max(tmp_bytes, t);
     void* d_tmp = scratch(ctx, "mp_cub_tmp", std::max<size_t>(tmp_bytes, 16));
 
@@ -596,7 +638,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         t = tmp_bytes;
         check(cub::DeviceRadixSort::SortPairs(d_tmp, t, d_pkey, d_pkey2, d_iota, d_idx, (int)n, 0, 64, st), "sort");
         k_plan_pos<<<gs, 256, 0, st>>>((int)n, d_idx, d_pkey2, d_boxs, d_prm, np, d_level, d_box, d_pin, d_dims, d_size,
-                                       d_lstart, d_meta);
+                                       d_lstart, d_meta, d_posof);
         check(cudaGetLastError(), "k_plan_pos");
         check(cudaMemsetAsync(d_size + n, 0, sizeof(int64_t), st), "memset");
         t = tmp_bytes;
@@ -618,6 +660,84 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             check(cudaMemcpyAsync(lev_pix.data(), d_lpix, sizeof(int64_t) * nlev, cudaMemcpyDeviceToHost, st), "d2h");
             check(cudaMemsetAsync(d_queues, 0, sizeof(unsigned long long) * nlev, st), "memset");
             check(cudaStreamSynchronize(st), "sync");
+        }
+        if (dag && npos > 0) {
+            // dependency lists, the ready queue, and one launch for the whole pass
+            k_dag_edges<false><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
+                                                   d_indeg, d_nsucc, nullptr, nullptr);
+            check(cudaGetLastError(), "k_dag_edges");
+            check(cudaMemsetAsync(d_nsucc + npos, 0, sizeof(int32_t), st), "memset");
+            t = tmp_bytes;
+            check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_nsucc, d_sstart, npos + 1, st), "scan");
+            int32_t nedge = 0;
+            check(cudaMemcpyAsync(&nedge, d_sstart + npos, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaStreamSynchronize(st), "sync");
+            int32_t* d_slist = I32("mp_succ_list", (size_t)nedge);
+            k_dag_edges<true><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
+                                                  nullptr, nullptr, d_sstart, d_slist);
+            check(cudaGetLastError(), "k_dag_edges");
+            k_mp_fill<int32_t><<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, -1, d_queue);
+            check(cudaMemsetAsync(d_dagc, 0, sizeof(int32_t) * 4, st), "memset");
+            k_dag_queue<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, d_indeg, d_queue, d_dagc);
+            check(cudaGetLastError(), "k_dag_queue");
+            double* d_snap = nullptr;
+            if (pass == n_passes) {
+                int64_t tot_all = 0;
+                check(cudaMemcpyAsync(&tot_all, d_scan + npos, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaStreamSynchronize(st), "sync");
+                d_snap = (double*)scratch(ctx, "mp_snap", sizeof(double) * std::max<int64_t>(tot_all, 1));
+            }
+            DagArgs A{};
+            A.npos = npos;
+            A.pass = pass;
+            A.ny = ny;
+            A.box_max = boxmax;
+            A.M = M;
+            A.F = F;
+            A.idx = d_idx;
+            A.box = d_box;
+            A.pin = d_pin;
+            A.succ_start = d_sstart;
+            A.succ_list = d_slist;
+            A.indeg = d_indeg;
+            A.queue = d_queue;
+            A.counters = d_dagc;
+            A.resid = resid;
+            A.iv = d_iv;
+            A.cpix = d_tpix;
+            A.civ = d_tiv;
+            A.prm = d_prm;
+            A.err = d_err;
+            A.conv = d_conv;
+            A.valid = d_valid;
+            A.chisq = d_chisq;
+            A.niter = d_niter;
+            A.n_failed = d_nfail;
+            A.psub = d_psub;
+            A.flag = d_flag;
+            A.snap = d_snap;
+            A.snap_off = d_scan;
+            mp_dag_launch(ctx, psf, P, eltype, A);
+            if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389), from the snapshots
+                KernelScope ks_(ctx, "k_mp_diag", 0.0);
+                const unsigned g = (unsigned)std::min<int64_t>(npos, (int64_t)ctx->n_sm * 16);
+                if (eltype == CPB_F64)
+                    k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
+                        npos, d_box, d_psub, d_flag, (const double*)d_img, resid, d_snap, d_scan,
+                        (const double*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx, d_diagS);
+                else
+                    k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
+                        npos, d_box, d_psub, d_flag, (const float*)d_img, resid, d_snap, d_scan,
+                        (const float*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx, d_diagS);
+                check(cudaGetLastError(), "k_mp_diag");
+            }
+            int32_t dag_err = 0;
+            check(cudaMemcpyAsync(&dag_err, d_dagc + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaStreamSynchronize(st), "sync");
+            if (dag_err) throw CudaError{cudaErrorLaunchTimeout, "fit_all_stars: a pass stalled waiting for ready stars"};
+            k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
+            check(cudaGetLastError(), "k_mp_validate");
+            continue;
         }
         const int64_t pix_max = std::max<int64_t>(1, *std::max_element(lev_pix.begin(), lev_pix.end()));
         double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * pix_max);
@@ -673,12 +793,12 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 const unsigned g = (unsigned)std::min<int64_t>(nL, (int64_t)ctx->n_sm * 16);
                 if (eltype == CPB_F64)
                     k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
-                        nL, bx, d_psub + p0 * np, d_flag + p0, (const double*)d_img, resid, (const double*)d_iv, dp,
-                        M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
+                        nL, bx, d_psub + p0 * np, d_flag + p0, (const double*)d_img, resid, nullptr, nullptr,
+                        (const double*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
                 else
                     k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
-                        nL, bx, d_psub + p0 * np, d_flag + p0, (const float*)d_img, resid, (const float*)d_iv, dp,
-                        M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
+                        nL, bx, d_psub + p0 * np, d_flag + p0, (const float*)d_img, resid, nullptr, nullptr,
+                        (const float*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx + p0, d_diagS);
                 check(cudaGetLastError(), "k_mp_diag");
             }
         }

@@ -93,3 +93,30 @@ def test_spread_model_known_answers_and_wide_boxes():
     o = orc_fit_all_stars(big, CircularGaussianPSF(fwhm=2.0), src, 30, **kw)
     assert np.all(np.isfinite(g.spread_model[g.valid]))
     compare(g, o)
+
+
+def test_batch_level_path_irls_and_four_node_psf():
+    """The batch-by-batch path (fit_star launches per batch) serves what the
+    dependency-driven launch does not: IRLS reweighting and multi-node gridded
+    PSFs.  Both against the oracle."""
+    from crowdphot_b200 import HuberLoss
+    from test_gpu_sim import four_node_epsf
+    psf = CircularGaussianPSF(fwhm=2.0)
+    img, src = field((96, 96), 12, 6, min_sep=6)
+    kw = dict(n_passes=2, max_iter=100, fixed={"bkg": 20.0}, reweight=HuberLoss(1.0))
+    compare(cpb.fit_all_stars(img, psf, src, 5, **kw), orc_fit_all_stars(img, psf, src, 5, **kw))
+    g4 = four_node_epsf()
+    from oracle import orc_psf_eval
+    rng = np.random.default_rng(11)
+    ys, xs = rng.uniform(12, 118, 40), rng.uniform(12, 118, 40)
+    fl = rng.uniform(500, 5000, 40)
+    img = np.zeros((128, 128))
+    yy, xx = np.meshgrid(np.arange(1, 129), np.arange(1, 129), indexing="ij")
+    for y, x, f in zip(ys, xs, fl):
+        img += orc_psf_eval(g4, y, x, f, 0.0, yy.ravel().astype(float), xx.ravel().astype(float),
+                            grad=False).reshape(img.shape)
+    img += rng.normal(0, 1.0, img.shape)
+    iv = np.ones(img.shape)
+    cat = dict(y=ys + rng.normal(0, 0.2, 40), x=xs + rng.normal(0, 0.2, 40), flux=fl)
+    kw = dict(n_passes=2, max_iter=60, fixed={"bkg": 0.0}, inv_var=iv)
+    compare(cpb.fit_all_stars(img, g4, cat, 6, **kw), orc_fit_all_stars(img, g4, cat, 6, **kw))
