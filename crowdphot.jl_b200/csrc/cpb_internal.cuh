@@ -308,8 +308,9 @@ struct DagArgs {
     const int32_t* succ_start;  // per position (npos + 1): stars that wait for it
     const int32_t* succ_list;
     int32_t* indeg;             // per position: unfinished stars it waits for
+    int32_t* plevel;            // per position: longest chain of stars before it (0 at the start)
     int32_t* queue;             // npos ready positions, -1 = not yet
-    int32_t* counters;          // head, tail, error
+    int32_t* counters;          // head, tail, error, deepest level
     double* resid;
     const void* iv;             // image inv_var (nullable), eltype of the image
     double *cpix, *civ;         // per team: box_max doubles each

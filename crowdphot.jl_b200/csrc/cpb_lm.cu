@@ -1496,8 +1496,12 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, D
         }
         __threadfence();
         team_sync<WPC>();
-        // release the stars that waited for this one
+        // release the stars that waited for this one (their chain depth first)
         if (lane == 0) {
+            const int lv = ((volatile int32_t*)A.plevel)[k];
+            atomicMax(A.counters + 3, lv);
+            for (int q = A.succ_start[k]; q < A.succ_start[k + 1]; ++q) atomicMax(&A.plevel[A.succ_list[q]], lv + 1);
+            __threadfence();
             for (int q = A.succ_start[k]; q < A.succ_start[k + 1]; ++q) {
                 const int u = A.succ_list[q];
                 if (atomicSub(&A.indeg[u], 1) == 1) {

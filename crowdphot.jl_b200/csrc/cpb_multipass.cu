@@ -405,6 +405,30 @@ __global__ void k_dag_edges(int n, const int4* __restrict__ box, const int32_t* 
     }
 }
 
+// Positions of a dependency-driven pass in brightness order (order: stars by
+// rank, the invalid ones last): box, initial parameters and box size per
+// position, the star -> position map, and the number of positions into meta.
+__global__ void k_dag_pos(int n, const int32_t* __restrict__ order, const unsigned long long* __restrict__ skey,
+                          const int4* __restrict__ box_s, const double* __restrict__ prm, int np,
+                          int4* __restrict__ box, double* __restrict__ pin, int64_t* __restrict__ size,
+                          int32_t* __restrict__ pos_of, int32_t* __restrict__ meta) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const bool ok = skey[k] != 0xffffffffffffffffull;
+    if (!ok) {
+        size[k] = 0;
+        if (k == 0) meta[0] = 0;
+        return;
+    }
+    if (k == n - 1 || skey[k + 1] == 0xffffffffffffffffull) meta[0] = k + 1;
+    const int s = order[k];
+    pos_of[s] = k;
+    const int4 b = box_s[s];
+    box[k] = b;
+    for (int q = 0; q < np; ++q) pin[(int64_t)k * np + q] = prm[(int64_t)s * np + q];
+    size[k] = (int64_t)b.z * b.w;
+}
+
 // The ready queue of a pass: every position that waits for nobody.
 __global__ void k_dag_queue(int npos, const int32_t* __restrict__ indeg, int32_t* __restrict__ queue,
                             int32_t* __restrict__ counters) {
@@ -622,6 +646,99 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_ccount, d_cstart, ncell + 1, st), "scan");
         k_plan_cells<<<gs, 256, 0, st>>>((int)n, d_cellid, d_cstart, d_cfill, d_clist);
         check(cudaGetLastError(), "k_plan_cells");
+        if (dag) {
+            // positions in brightness order, the dependency lists, the ready
+            // queue, and one launch for the whole pass
+            k_dag_pos<<<gs, 256, 0, st>>>((int)n, d_order, d_fkey2, d_boxs, d_prm, np, d_box, d_pin, d_size, d_posof,
+                                          d_meta);
+            check(cudaGetLastError(), "k_dag_pos");
+            check(cudaMemsetAsync(d_size + n, 0, sizeof(int64_t), st), "memset");
+            t = tmp_bytes;
+            check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_size, d_scan, (int)n + 1, st), "scan");
+            k_dag_edges<false><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
+                                                   d_indeg, d_nsucc, nullptr, nullptr);
+            check(cudaGetLastError(), "k_dag_edges");
+            int32_t meta[2] = {0, 0};
+            check(cudaMemcpyAsync(meta, d_meta, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
+            check(cudaStreamSynchronize(st), "sync");
+            const int npos = meta[0];
+            out->n_fits += npos;
+            if (npos > 0) {
+                check(cudaMemsetAsync(d_nsucc + npos, 0, sizeof(int32_t), st), "memset");
+                t = tmp_bytes;
+                check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_nsucc, d_sstart, npos + 1, st), "scan");
+                int32_t nedge = 0;
+                int64_t tot_all = 0;
+                check(cudaMemcpyAsync(&nedge, d_sstart + npos, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaMemcpyAsync(&tot_all, d_scan + npos, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaStreamSynchronize(st), "sync");
+                int32_t* d_slist = I32("mp_succ_list", (size_t)nedge);
+                k_dag_edges<true><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx,
+                                                      d_posof, nullptr, nullptr, d_sstart, d_slist);
+                check(cudaGetLastError(), "k_dag_edges");
+                k_mp_fill<int32_t><<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, -1, d_queue);
+                check(cudaMemsetAsync(d_level, 0, sizeof(int32_t) * npos, st), "memset");
+                check(cudaMemsetAsync(d_dagc, 0, sizeof(int32_t) * 4, st), "memset");
+                k_dag_queue<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, d_indeg, d_queue, d_dagc);
+                check(cudaGetLastError(), "k_dag_queue");
+                double* d_snap = pass == n_passes
+                                     ? (double*)scratch(ctx, "mp_snap", sizeof(double) * std::max<int64_t>(tot_all, 1))
+                                     : nullptr;
+                DagArgs A{};
+                A.npos = npos;
+                A.pass = pass;
+                A.ny = ny;
+                A.box_max = boxmax;
+                A.M = M;
+                A.F = F;
+                A.idx = d_order;
+                A.box = d_box;
+                A.pin = d_pin;
+                A.succ_start = d_sstart;
+                A.succ_list = d_slist;
+                A.indeg = d_indeg;
+                A.plevel = d_level;
+                A.queue = d_queue;
+                A.counters = d_dagc;
+                A.resid = resid;
+                A.iv = d_iv;
+                A.cpix = d_tpix;
+                A.civ = d_tiv;
+                A.prm = d_prm;
+                A.err = d_err;
+                A.conv = d_conv;
+                A.valid = d_valid;
+                A.chisq = d_chisq;
+                A.niter = d_niter;
+                A.n_failed = d_nfail;
+                A.psub = d_psub;
+                A.flag = d_flag;
+                A.snap = d_snap;
+                A.snap_off = d_scan;
+                mp_dag_launch(ctx, psf, P, eltype, A);
+                if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389), from the snapshots
+                    KernelScope ks_(ctx, "k_mp_diag", (double)tot_all * (d_iv ? 24 : 16));
+                    const unsigned g = (unsigned)std::min<int64_t>(npos, (int64_t)ctx->n_sm * 16);
+                    if (eltype == CPB_F64)
+                        k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
+                            npos, d_box, d_psub, d_flag, (const double*)d_img, resid, d_snap, d_scan,
+                            (const double*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_order, d_diagS);
+                    else
+                        k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
+                            npos, d_box, d_psub, d_flag, (const float*)d_img, resid, d_snap, d_scan,
+                            (const float*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_order, d_diagS);
+                    check(cudaGetLastError(), "k_mp_diag");
+                }
+                int32_t dc[4] = {0, 0, 0, 0};
+                check(cudaMemcpyAsync(dc, d_dagc, sizeof(dc), cudaMemcpyDeviceToHost, st), "d2h");
+                check(cudaStreamSynchronize(st), "sync");
+                if (dc[2]) throw CudaError{cudaErrorLaunchTimeout, "fit_all_stars: a pass stalled waiting for ready stars"};
+                out->n_levels += dc[3] + 1;  // the longest chain of dependent fits
+            }
+            k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
+            check(cudaGetLastError(), "k_mp_validate");
+            continue;
+        }
         for (int64_t sweep = 0;; sweep += 2) {
             if (sweep > n + 2) throw CudaError{cudaErrorUnknown, "fit_all_stars: the batch plan did not converge"};
             int changed = 0;
@@ -660,84 +777,6 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             check(cudaMemcpyAsync(lev_pix.data(), d_lpix, sizeof(int64_t) * nlev, cudaMemcpyDeviceToHost, st), "d2h");
             check(cudaMemsetAsync(d_queues, 0, sizeof(unsigned long long) * nlev, st), "memset");
             check(cudaStreamSynchronize(st), "sync");
-        }
-        if (dag && npos > 0) {
-            // dependency lists, the ready queue, and one launch for the whole pass
-            k_dag_edges<false><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
-                                                   d_indeg, d_nsucc, nullptr, nullptr);
-            check(cudaGetLastError(), "k_dag_edges");
-            check(cudaMemsetAsync(d_nsucc + npos, 0, sizeof(int32_t), st), "memset");
-            t = tmp_bytes;
-            check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_nsucc, d_sstart, npos + 1, st), "scan");
-            int32_t nedge = 0;
-            check(cudaMemcpyAsync(&nedge, d_sstart + npos, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
-            check(cudaStreamSynchronize(st), "sync");
-            int32_t* d_slist = I32("mp_succ_list", (size_t)nedge);
-            k_dag_edges<true><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
-                                                  nullptr, nullptr, d_sstart, d_slist);
-            check(cudaGetLastError(), "k_dag_edges");
-            k_mp_fill<int32_t><<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, -1, d_queue);
-            check(cudaMemsetAsync(d_dagc, 0, sizeof(int32_t) * 4, st), "memset");
-            k_dag_queue<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, d_indeg, d_queue, d_dagc);
-            check(cudaGetLastError(), "k_dag_queue");
-            double* d_snap = nullptr;
-            if (pass == n_passes) {
-                int64_t tot_all = 0;
-                check(cudaMemcpyAsync(&tot_all, d_scan + npos, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "d2h");
-                check(cudaStreamSynchronize(st), "sync");
-                d_snap = (double*)scratch(ctx, "mp_snap", sizeof(double) * std::max<int64_t>(tot_all, 1));
-            }
-            DagArgs A{};
-            A.npos = npos;
-            A.pass = pass;
-            A.ny = ny;
-            A.box_max = boxmax;
-            A.M = M;
-            A.F = F;
-            A.idx = d_idx;
-            A.box = d_box;
-            A.pin = d_pin;
-            A.succ_start = d_sstart;
-            A.succ_list = d_slist;
-            A.indeg = d_indeg;
-            A.queue = d_queue;
-            A.counters = d_dagc;
-            A.resid = resid;
-            A.iv = d_iv;
-            A.cpix = d_tpix;
-            A.civ = d_tiv;
-            A.prm = d_prm;
-            A.err = d_err;
-            A.conv = d_conv;
-            A.valid = d_valid;
-            A.chisq = d_chisq;
-            A.niter = d_niter;
-            A.n_failed = d_nfail;
-            A.psub = d_psub;
-            A.flag = d_flag;
-            A.snap = d_snap;
-            A.snap_off = d_scan;
-            mp_dag_launch(ctx, psf, P, eltype, A);
-            if (pass == n_passes) {  // diagnostics of the fitted stars (:381-389), from the snapshots
-                KernelScope ks_(ctx, "k_mp_diag", 0.0);
-                const unsigned g = (unsigned)std::min<int64_t>(npos, (int64_t)ctx->n_sm * 16);
-                if (eltype == CPB_F64)
-                    k_mp_diag<double><<<g, kDiagThreads, diag_smem, st>>>(
-                        npos, d_box, d_psub, d_flag, (const double*)d_img, resid, d_snap, d_scan,
-                        (const double*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx, d_diagS);
-                else
-                    k_mp_diag<float><<<g, kDiagThreads, diag_smem, st>>>(
-                        npos, d_box, d_psub, d_flag, (const float*)d_img, resid, d_snap, d_scan,
-                        (const float*)d_iv, dp, M, nf, ny, sd, smode, boxmax, d_idx, d_diagS);
-                check(cudaGetLastError(), "k_mp_diag");
-            }
-            int32_t dag_err = 0;
-            check(cudaMemcpyAsync(&dag_err, d_dagc + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, st), "d2h");
-            check(cudaStreamSynchronize(st), "sync");
-            if (dag_err) throw CudaError{cudaErrorLaunchTimeout, "fit_all_stars: a pass stalled waiting for ready stars"};
-            k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
-            check(cudaGetLastError(), "k_mp_validate");
-            continue;
         }
         const int64_t pix_max = std::max<int64_t>(1, *std::max_element(lev_pix.begin(), lev_pix.end()));
         double* d_cpix = (double*)scratch(ctx, "mp_cpix", sizeof(double) * pix_max);
