@@ -1382,10 +1382,13 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
 // fit only holds back the stars that overlap it.  The residual image is read
 // and written around L1 (ld/st.cg): other SMs change it between uses.
 constexpr long long kDagSpinLimit = 1ll << 26;  // ~64 M polls of >= 64 ns before a team gives up
+// Warps of one team: 4 measured fastest on the 2048^2 field (k_mp_dag 34.6 ms for
+// three passes, against 58.2 ms with 1 and 41.0 ms with 8).
+constexpr int kDagWarps = 4;
 
 template <typename TIV, int NP, int NF, bool SMEM>
 __global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, DevPsf P, DagArgs A) {
-    constexpr int WPC = 4, TS = 128;
+    constexpr int WPC = kDagWarps, TS = 32 * kDagWarps;
     constexpr int KR = 1 + NF + NF * (NF + 1) / 2;
     __shared__ LMState<NP, NF> states[kLMThreads / TS];
     __shared__ double red_all[(kLMThreads / 32) * KR];
@@ -1930,7 +1933,7 @@ bool mp_dag_supported(const cpb_psf* psf, const cpb_lm_params* P) {
     return (gauss || psf->dev.n_nodes == 1) && P->reweight == CPB_LOSS_NONE && P->precision == CPB_PREC_FP64;
 }
 
-int mp_dag_teams(cpb_ctx* ctx) { return ctx->n_sm * 2 * (kLMThreads / 128); }
+int mp_dag_teams(cpb_ctx* ctx) { return ctx->n_sm * 2 * (kLMThreads / (32 * kDagWarps)); }
 
 void mp_dag_launch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int32_t iv_eltype, const DagArgs& A) {
     const LMConst L = lm_const(psf, P, A.iv != nullptr);
