@@ -561,6 +561,10 @@ struct ArgError {
 struct OomError {
     std::string msg;
 };
+// A bounded device-side wait gave up (CPB_ERR_TIMEOUT).
+struct WaitTimeout {
+    std::string msg;
+};
 
 // Runs one C-ABI entry point's body under the context's lock, translating
 // exceptions into CPB_* status codes and cpb_last_error() text.
@@ -578,6 +582,9 @@ int guarded(cpb_ctx* ctx, F&& f) {
     } catch (const OomError& e) {
         ctx->err = e.msg;
         return CPB_ERR_OOM;
+    } catch (const WaitTimeout& e) {
+        ctx->err = e.msg;
+        return CPB_ERR_TIMEOUT;
     } catch (const CudaError& e) {
         ctx->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);
         return CPB_ERR_CUDA;

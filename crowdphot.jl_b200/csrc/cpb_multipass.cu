@@ -732,7 +732,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 int32_t dc[4] = {0, 0, 0, 0};
                 check(cudaMemcpyAsync(dc, d_dagc, sizeof(dc), cudaMemcpyDeviceToHost, st), "d2h");
                 check(cudaStreamSynchronize(st), "sync");
-                if (dc[2]) throw CudaError{cudaErrorLaunchTimeout, "fit_all_stars: a pass stalled waiting for ready stars"};
+                if (dc[2]) throw WaitTimeout{"fit_all_stars: a pass stalled waiting for ready stars"};
                 out->n_levels += dc[3] + 1;  // the longest chain of dependent fits
             }
             k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);

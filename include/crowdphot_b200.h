@@ -332,7 +332,7 @@ typedef struct cpb_multipass_result {
     double* residual;          /* optional, ny*nx: the data with every valid star's model subtracted */
     int32_t n_passes;
     int32_t n_failed;          /* fits that failed the reference's input checks */
-    int64_t n_levels;          /* batches run (summed over the passes) */
+    int64_t n_levels;          /* longest chain of dependent fits, summed over the passes */
     int64_t n_fits;            /* fit_star calls run */
     double device_seconds;
     double *spread_model, *spread_model_err; /* optional */
@@ -343,14 +343,17 @@ typedef struct cpb_multipass_result {
  * brightness-ordered passes; each valid star is added back (passes 2+),
  * fitted with fit_star on its +-fit_rad box of the running residual image and
  * subtracted again.  Two stars depend on each other only through pixels their
- * boxes share, and each pass fixes every box at its start, so the pass is run
- * as a sequence of batches: a star's batch is one more than the latest batch
- * of any earlier (brighter) star whose box overlaps its own, and the stars of
- * one batch -- pairwise disjoint -- are fitted together in one launch.  The
- * result equals the one-star-at-a-time order of the reference.  image: ny*nx
- * of eltype (background-subtracted); inv_var nullable; init: n*np initial
- * parameters (the catalogue, with the PSF's own values for parameters the
- * catalogue lacks).  LM keyword arguments as cpb_fit_lm_batch.  Host arrays.
+ * boxes share, and each pass fixes every box at its start, so a star waits
+ * only for the brighter stars whose boxes meet its own; stars that are ready
+ * together have disjoint boxes and are fitted concurrently (one device launch
+ * per pass; IRLS and multi-node PSFs run the pass as batches of such stars).
+ * The result equals the one-star-at-a-time order of the reference.  image:
+ * ny*nx of eltype (background-subtracted); inv_var nullable; init: n*np
+ * initial parameters (_extract_source_catalog: y, x from the catalogue, flux
+ * from it or 1, bkg from it or 0, other parameters the PSF's own).  LM keyword
+ * arguments (IRLS included) as cpb_fit_lm_batch.  Host arrays.  A pass whose
+ * device queue stalls (a fault of the library, not of the data) returns
+ * CPB_ERR_TIMEOUT after a bounded wait of a few seconds.
  * spread_model_fwhm: as cpb_sim_params.spread_model_fwhm.
  */
 CPB_API int cpb_fit_all_stars(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* params, double fit_rad,
