@@ -455,6 +455,9 @@ __global__ void k_mp_fill(int64_t n, T v, T* __restrict__ a) {
 
 inline unsigned warps_grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n * 32 + 255) / 256); }
 
+// Counts a launch that has no KernelScope (the context's launch counter).
+inline void counted(cpb_ctx* ctx) { ctx->launches += 1; }
+
 }  // namespace
 
 int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, double fit_rad, int n_passes,
@@ -509,6 +512,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
 
     double* resid = (double*)scratch(ctx, "mp_residual", sizeof(double) * npix);
     check(cudaEventRecord(ctx->ev0, st), "event");
+    counted(ctx);
     if (eltype == CPB_F64)
         k_mp_init<double><<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(npix, (const double*)d_img, resid);
     else
@@ -603,6 +607,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     check(cudaMemsetAsync(d_valid, 1, (size_t)n, st), "memset");
     check(cudaMemsetAsync(d_conv, 0, (size_t)n, st), "memset");
     check(cudaMemsetAsync(d_misc, 0, sizeof(int32_t) * 4, st), "memset");
+    counted(ctx);
     k_mp_fill<double><<<(unsigned)((n * 6 + 255) / 256), 256, 0, st>>>(n * 6, NaN, d_diagS);
     check(cudaGetLastError(), "k_mp_fill");
     MPFree F{};
@@ -636,25 +641,30 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         // of every valid star, all on the device
         check(cudaMemsetAsync(d_ccount, 0, sizeof(int32_t) * (ncell + 1), st), "memset");
         check(cudaMemsetAsync(d_cfill, 0, sizeof(int32_t) * ncell, st), "memset");
+        counted(ctx);
         k_plan_box<<<gs, 256, 0, st>>>((int)n, d_prm, M, fit_rad, ny, nx, cell, gny, d_valid, d_boxs, d_cellid, d_fkey,
                                        d_iota, d_ccount);
         check(cudaGetLastError(), "k_plan_box");
         t = tmp_bytes;
         check(cub::DeviceRadixSort::SortPairs(d_tmp, t, d_fkey, d_fkey2, d_iota, d_order, (int)n, 0, 64, st), "sort");
+        counted(ctx);
         k_plan_rank<<<gs, 256, 0, st>>>((int)n, d_order, d_rank, d_level);
         t = tmp_bytes;
         check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_ccount, d_cstart, ncell + 1, st), "scan");
+        counted(ctx);
         k_plan_cells<<<gs, 256, 0, st>>>((int)n, d_cellid, d_cstart, d_cfill, d_clist);
         check(cudaGetLastError(), "k_plan_cells");
         if (dag) {
             // positions in brightness order, the dependency lists, the ready
             // queue, and one launch for the whole pass
+            counted(ctx);
             k_dag_pos<<<gs, 256, 0, st>>>((int)n, d_order, d_fkey2, d_boxs, d_prm, np, d_box, d_pin, d_size, d_posof,
                                           d_meta);
             check(cudaGetLastError(), "k_dag_pos");
             check(cudaMemsetAsync(d_size + n, 0, sizeof(int64_t), st), "memset");
             t = tmp_bytes;
             check(cub::DeviceScan::ExclusiveSum(d_tmp, t, d_size, d_scan, (int)n + 1, st), "scan");
+            counted(ctx);
             k_dag_edges<false><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx, d_posof,
                                                    d_indeg, d_nsucc, nullptr, nullptr);
             check(cudaGetLastError(), "k_dag_edges");
@@ -673,12 +683,15 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 check(cudaMemcpyAsync(&tot_all, d_scan + npos, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "d2h");
                 check(cudaStreamSynchronize(st), "sync");
                 int32_t* d_slist = I32("mp_succ_list", (size_t)nedge);
+                counted(ctx);
                 k_dag_edges<true><<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx,
                                                       d_posof, nullptr, nullptr, d_sstart, d_slist);
                 check(cudaGetLastError(), "k_dag_edges");
+                counted(ctx);
                 k_mp_fill<int32_t><<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, -1, d_queue);
                 check(cudaMemsetAsync(d_level, 0, sizeof(int32_t) * npos, st), "memset");
                 check(cudaMemsetAsync(d_dagc, 0, sizeof(int32_t) * 4, st), "memset");
+                counted(ctx);
                 k_dag_queue<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, d_indeg, d_queue, d_dagc);
                 check(cudaGetLastError(), "k_dag_queue");
                 double* d_snap = pass == n_passes
@@ -735,6 +748,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 if (dc[2]) throw WaitTimeout{"fit_all_stars: a pass stalled waiting for ready stars"};
                 out->n_levels += dc[3] + 1;  // the longest chain of dependent fits
             }
+            counted(ctx);
             k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
             check(cudaGetLastError(), "k_mp_validate");
             continue;
@@ -743,17 +757,21 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             if (sweep > n + 2) throw CudaError{cudaErrorUnknown, "fit_all_stars: the batch plan did not converge"};
             int changed = 0;
             check(cudaMemsetAsync(d_changed, 0, sizeof(int), st), "memset");
-            for (int k = 0; k < 2; ++k)
+            for (int k = 0; k < 2; ++k) {
+                counted(ctx);
                 k_plan_relax<<<gs, 256, 0, st>>>((int)n, d_boxs, d_cellid, d_rank, d_cstart, d_clist, gny, gnx,
                                                  d_level, d_changed);
+            }
             check(cudaGetLastError(), "k_plan_relax");
             check(cudaMemcpyAsync(&changed, d_changed, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
             check(cudaStreamSynchronize(st), "sync");
             if (!changed) break;
         }
+        counted(ctx);
         k_plan_poskey<<<gs, 256, 0, st>>>((int)n, d_cellid, d_level, d_rank, d_pkey);
         t = tmp_bytes;
         check(cub::DeviceRadixSort::SortPairs(d_tmp, t, d_pkey, d_pkey2, d_iota, d_idx, (int)n, 0, 64, st), "sort");
+        counted(ctx);
         k_plan_pos<<<gs, 256, 0, st>>>((int)n, d_idx, d_pkey2, d_boxs, d_prm, np, d_level, d_box, d_pin, d_dims, d_size,
                                        d_lstart, d_meta, d_posof);
         check(cudaGetLastError(), "k_plan_pos");
@@ -769,6 +787,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
         lev_start.assign(nlev + 1, 0);
         lev_pix.assign(std::max(nlev, 1), 0);
         if (npos > 0) {
+            counted(ctx);
             k_plan_offsets<<<(unsigned)((std::max(npos, nlev) + 255) / 256), 256, 0, st>>>(npos, nlev, d_idx, d_level,
                                                                                         d_scan, d_lstart, d_off, d_lpix);
             check(cudaGetLastError(), "k_plan_offsets");
@@ -842,6 +861,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
             }
         }
         // between-pass validation (:404-412)
+        counted(ctx);
         k_mp_validate<<<gs, 256, 0, st>>>((int)n, d_prm, M, d_conv, d_valid);
         check(cudaGetLastError(), "k_mp_validate");
     }
