@@ -72,6 +72,26 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def max_and_sum_over_ranks(values, device="cpu"):
+    """Whole-job aggregates of per-rank values: (max over the ranks, sum over the
+    ranks), each a list in the order of `values`.  Times take the max (the job ends
+    with its slowest replica), counts the sum.  A single process gets its own values
+    back twice."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    mx, sm = t.clone(), t.clone()
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
+def replica_seed(base, rank):
+    """The seed of one replica's synthetic input: every rank fits its own field."""
+    return base + rank
+
+
 class ClockSampler:
     """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
 
@@ -183,7 +203,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
 
     ny, nx, n = args.ny, args.nx, args.n_stars
-    psf, img, bkg, iv, truth, init = make_field(ny, nx, n, SEED + rank)
+    psf, img, bkg, iv, truth, init = make_field(ny, nx, n, replica_seed(SEED, rank))
     ctx = cpb.get_context(local)
     hp = ctx.psf_handle(psf)
     P = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD)
@@ -235,15 +255,8 @@ def run_gpu(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    agg = torch.tensor([total_s, float(fitted_total), float(launches)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx = agg.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = agg.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_s, fitted_all, launches_all = float(mx[0]), float(sm[1]), int(sm[2])
-    else:
-        fitted_all, launches_all = float(fitted_total), launches
+    mx, sm = max_and_sum_over_ranks([total_s, fitted_total, launches], dev)
+    total_s, fitted_all, launches_all = mx[0], sm[1], int(sm[2])
     value = fitted_all / total_s
 
     # mixed-precision form: same protocol, and its per-output deviation from the
@@ -262,15 +275,8 @@ def run_gpu(args):
         m_fitted += f
         m_times.append(s_)
     barrier()
-    mt = torch.tensor([float(sum(m_times)), float(m_fitted)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx_ = mt.clone()
-        dist.all_reduce(mx_, op=dist.ReduceOp.MAX)
-        sm_ = mt.clone()
-        dist.all_reduce(sm_, op=dist.ReduceOp.SUM)
-        m_value = float(sm_[1]) / float(mx_[0])
-    else:
-        m_value = m_fitted / sum(m_times)
+    mx_, sm_ = max_and_sum_over_ranks([sum(m_times), m_fitted], dev)
+    m_value = sm_[1] / mx_[0]
     ok = (outs.valid[:n] & outs.converged[:n] & outs_m.valid[:n] & outs_m.converged[:n] &
           (outs.n_iter[:n] == outs_m.n_iter[:n])).astype(bool)
     dfl = np.abs(outs_m.flux[:n][ok] / outs.flux[:n][ok] - 1)
@@ -321,15 +327,8 @@ def run_gpu(args):
         if i >= args.warmup:
             e_times.append(ev0.elapsed_time(ev1) * 1e-3)
             e_fitted += int((r.valid & r.converged).sum())
-    et = torch.tensor([sum(e_times), float(e_fitted)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx = et.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        sm = et.clone()
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        e_value = float(sm[1]) / float(mx[0])
-    else:
-        e_value = e_fitted / sum(e_times)
+    mx, sm = max_and_sum_over_ranks([sum(e_times), e_fitted], dev)
+    e_value = sm[1] / mx[0]
     h2d = 3 * img.nbytes + 3 * 8 * n
     d2h = n * (12 * 8 + 2 + 4) + ny * nx * 8
 
@@ -421,7 +420,7 @@ def run_gpu_lm(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    psf, d = _lm_packed(args.n_cutouts, LM_SEED + rank)
+    psf, d = _lm_packed(args.n_cutouts, replica_seed(LM_SEED, rank))
     n = len(d["ny"])
     ctx = cpb.get_context(local)
     hp = ctx.psf_handle(psf)
@@ -469,14 +468,8 @@ def run_gpu_lm(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    agg = torch.tensor([sum(times), float(fitted), float(launches)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx, sm = agg.clone(), agg.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_s, fitted_all, launches_all = float(mx[0]), float(sm[1]), int(sm[2])
-    else:
-        total_s, fitted_all, launches_all = sum(times), float(fitted), launches
+    mx, sm = max_and_sum_over_ranks([sum(times), fitted, launches], dev)
+    total_s, fitted_all, launches_all = mx[0], sm[1], int(sm[2])
     value = fitted_all / total_s
     iters = outs["iterations"].cpu().numpy()
 
@@ -510,14 +503,8 @@ def run_gpu_lm(args):
         if i >= args.warmup:
             e_times.append(dt)
             e_fitted += int(((out["status"] == 0) & (out["converged"] != 0)).sum())
-    et = torch.tensor([sum(e_times), float(e_fitted)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx, sm = et.clone(), et.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        e_value = float(sm[1]) / float(mx[0])
-    else:
-        e_value = e_fitted / sum(e_times)
+    mx, sm = max_and_sum_over_ranks([sum(e_times), e_fitted], dev)
+    e_value = sm[1] / mx[0]
     h2d = 2 * d["pix"].nbytes + n * (8 + 16 + 32)
     d2h = n * (8 * 4 + 8 * 9 + 8 * 4 + 4 + 8)
     if rank == 0:
@@ -648,8 +635,8 @@ def run_gpu_c4(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    psf, dl = _lm_packed(args.n_cutouts, LM_SEED + rank)
-    dg = lm_groups(args.n_groups, seed=C4_GROUP_SEED + rank, psf=psf)
+    psf, dl = _lm_packed(args.n_cutouts, replica_seed(LM_SEED, rank))
+    dg = lm_groups(args.n_groups, seed=replica_seed(C4_GROUP_SEED, rank), psf=psf)
     n_cut, n_grp = len(dl["ny"]), len(dg["ny"])
     ns = int(dg["star_offsets"][-1])
     ctx = cpb.get_context(local)
@@ -700,14 +687,8 @@ def run_gpu_c4(args):
         if world > 1:
             dist.destroy_process_group()
         return
-    agg = torch.tensor([sum(times), float(f_lm + f_g), float(launches)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx, sm = agg.clone(), agg.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_s, fitted_all, launches_all = float(mx[0]), float(sm[1]), int(sm[2])
-    else:
-        total_s, fitted_all, launches_all = sum(times), float(f_lm + f_g), launches
+    mx, sm = max_and_sum_over_ranks([sum(times), f_lm + f_g, launches], dev)
+    total_s, fitted_all, launches_all = mx[0], sm[1], int(sm[2])
     value = fitted_all / total_s
     info = graph.tune_info()
     # profiling pass (not timed): each kernel alone through the direct device entries
@@ -773,14 +754,8 @@ def run_gpu_c4(args):
                                                                    (h_out[12].numpy()[:ns] != 0)).sum())
     h2d = sum(h.numel() * h.element_size() for h in h_in.values())
     d2h = sum(h.numel() * h.element_size() for h in h_out)
-    et = torch.tensor([sum(e_times), float(e_fitted)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx, sm = et.clone(), et.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        e_value = float(sm[1]) / float(mx[0])
-    else:
-        e_value = e_fitted / sum(e_times)
+    mx, sm = max_and_sum_over_ranks([sum(e_times), e_fitted], dev)
+    e_value = sm[1] / mx[0]
     graph.close()
     if rank == 0:
         ms = sorted(1e3 * x for x in times)
@@ -991,7 +966,7 @@ def run_gpu_mp(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ny, nx, n = args.ny, args.nx, args.n_stars
-    psf, data, iv, init = _mp_field(ny, nx, n, SEED + rank)
+    psf, data, iv, init = _mp_field(ny, nx, n, replica_seed(SEED, rank))
     ctx = cpb.get_context(local)
     hp = ctx.psf_handle(psf)
     P = lm_params(psf, {"bkg": 0.0})
@@ -1032,14 +1007,8 @@ def run_gpu_mp(args):
     barrier()
     clk = clocks.stop() if clocks else None
     _, launches = ctx.kernel_stats(reset=True)
-    agg = torch.tensor([sum(times), float(fitted), float(launches), sum(walls)], dtype=torch.float64, device=dev)
-    if world > 1:
-        mx, sm = agg.clone(), agg.clone()
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        total_s, fitted_all, launches_all, wall_s = float(mx[0]), float(sm[1]), int(sm[2]), float(mx[3])
-    else:
-        total_s, fitted_all, launches_all, wall_s = sum(times), float(fitted), launches, sum(walls)
+    mx, sm = max_and_sum_over_ranks([sum(times), fitted, launches, sum(walls)], dev)
+    total_s, fitted_all, launches_all, wall_s = mx[0], sm[1], int(sm[2]), mx[3]
     value = fitted_all / total_s
     e_value = fitted_all / wall_s
     ctx.set_profiling(True)
