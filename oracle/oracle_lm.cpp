@@ -214,7 +214,7 @@ double irls_weight(int loss, double c, double r) {
 }
 
 struct LMRun {
-    std::vector<double> x, A;
+    double x[5], A[25];
     double cost = 0, cost_init = 0, lam = 0, sigma_final = kNaN, chisq = 0;
     bool conv = false, xconv = false, fconv = false, gconv = false;
     int iter = 0;
@@ -243,15 +243,20 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
             scale_kind = CPB_SCALE_MAD;
         }
     }
-    std::vector<double> weights;
+    // per-thread buffers (the batch entry fits many cutouts on each host thread)
+    thread_local std::vector<double> weights, res;
     const std::vector<double>* wp = base;
     if (do_irls) {
-        weights = base ? *base : std::vector<double>(nobs, 1.0);
+        if (base)
+            weights = *base;
+        else
+            weights.assign(nobs, 1.0);
         wp = &weights;
     }
-    std::vector<double> res(nobs, 0.0);
-    std::vector<double> x(x0, x0 + n), xc(n), A(n * n), b(n), Ac(n * n), bc(n), Ad(n * n), d(n), D(n);
-    double cost = accum(x.data(), wp, A.data(), b.data(), res.data());
+    res.resize(nobs);
+    double x[5], xc[5], A[25], b[5], Ac[25], bc[5], Ad[25], d[5], D[5];
+    std::copy(x0, x0 + n, x);
+    double cost = accum(x, wp, A, b, res.data());
     R.cost_init = cost;
     const double d_floor = 1.0e-6;
     for (int q = 0; q < n; ++q) D[q] = std::sqrt(std::max(A[q + q * n], d_floor));
@@ -264,13 +269,13 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
             R.gconv = R.conv = true;
             break;
         }
-        Ad = A;
+        std::copy(A, A + n * n, Ad);
         if (P->damping == CPB_DAMP_MARQUARDT) {
             for (int q = 0; q < n; ++q) Ad[q + q * n] += lam * std::max(Ad[q + q * n], P->min_diagonal);
         } else if (P->damping == CPB_DAMP_LEVENBERG) {
             for (int q = 0; q < n; ++q) Ad[q + q * n] += lam;
         }
-        if (!chol_solve(Ad.data(), n, b.data(), d.data())) {
+        if (!chol_solve(Ad, n, b, d)) {
             lam = std::min(lam * P->lambda_up, P->lambda_max);
             continue;
         }
@@ -281,7 +286,7 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
             for (int r = 0; r < n; ++r) dAd += d[q] * A[q + r * n] * d[r];
         const double prered = -2 * db - dAd;
         for (int q = 0; q < n; ++q) xc[q] = x[q] + d[q];
-        const double cost_c = accum(xc.data(), wp, Ac.data(), bc.data(), res.data());
+        const double cost_c = accum(xc, wp, Ac, bc, res.data());
         const bool accepted = cost_c < cost;
         const double dcost = cost - cost_c;
         const double ratio = prered > 0 ? dcost / prered : 0.0;
@@ -296,9 +301,9 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
         if (accepted) {
             cost = cost_c;
             lam = std::max(lam / P->lambda_down, P->lambda_min);
-            x = xc;
-            A = Ac;
-            b = bc;
+            std::copy(xc, xc + n, x);
+            std::copy(Ac, Ac + n * n, A);
+            std::copy(bc, bc + n, b);
             for (int q = 0; q < n; ++q) D[q] = std::max(D[q], std::sqrt(A[q + q * n]));
             if (R.xconv || R.fconv) {
                 R.conv = true;
@@ -318,7 +323,7 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
                         wn2 = std::fma(new_w, new_w, wn2);
                         weights[k] = new_w;
                     }
-                    cost = accum(x.data(), wp, A.data(), b.data(), res.data());
+                    cost = accum(x, wp, A, b, res.data());
                     const double wchange = std::sqrt(dw2) / std::max({std::sqrt(wo2), std::sqrt(wn2), kEps});
                     if (wchange >= P->weight_reset_tol) {
                         lam = P->lambda_init;
@@ -339,8 +344,8 @@ LMRun lm_irls_run(Acc&& accum, int n, int64_t nobs, const double* x0, const std:
     R.chisq = (!base && do_irls && !std::isnan(R.sigma_final) && R.sigma_final > kEps)
                   ? s2 / (R.sigma_final * R.sigma_final)
                   : s2;
-    R.x = x;
-    R.A = A;
+    std::copy(x, x + n, R.x);
+    std::copy(A, A + n * n, R.A);
     R.cost = cost;
     R.lam = lam;
     return R;
@@ -502,17 +507,16 @@ int fit_one(const Psf& psf, const cpb_lm_params* P, const double* pix, const dou
         for (int q = 0; q < np; ++q) fv[q] = full[q];
         for (int q = 0; q < nf; ++q) fv[fidx[q]] = xv[q];
     };
-    const std::vector<double> ones(nobs, 1.0);
     auto acc = [&](const double* xv, const std::vector<double>* w, double* A, double* b, double* res) {
         double fv[5];
         set_full(xv, fv);
-        return accum(psf, c, w ? *w : ones, fv, fidx, nf, A, b, res);
+        return accum(psf, c, w ? *w : wts, fv, fidx, nf, A, b, res);  // wts: all 1 without inv_var
     };
     LMRun R = lm_irls_run(acc, nf, nobs, x0, inv_var ? &wts : nullptr, P);
-    std::vector<double> cov;
-    covariance(R.A, nf, R.reweighted, R.cost, (double)dof, cov);
+    std::vector<double> cov, Av(R.A, R.A + nf * nf);
+    covariance(Av, nf, R.reweighted, R.cost, (double)dof, cov);
     double fv[5];
-    set_full(R.x.data(), fv);
+    set_full(R.x, fv);
     for (int q = 0; q < np; ++q) out_params[q] = fv[q];
     if (cov_out) std::memcpy(cov_out, cov.data(), sizeof(double) * nf * nf);
     *cost_out = R.cost;

@@ -4,7 +4,7 @@ diagnostic itself.
 The kernel (_exp_disk_kernel_bandlimited, src/photometry/psf_photometry_diagnostics.jl:82-108)
 is pinned against the reference's closed form, I(m; v) = exp(-pi^2 m^2 / a)
 sqrt(pi / a) Re erf(sqrt(a)/2 + i pi m / sqrt(a)), evaluated here with scipy's
-complex erf: both the oracle's restatement (composite Simpson) and the
+complex erf: both the oracle's restatement (Gauss-Legendre panels) and the
 product's host routine (composite Gauss-Legendre, cpb_exp_disk_kernel) must
 match it to rounding.  The diagnostic is pinned by the reference's own
 known-answer tests (test/photometry/psf_photometry_single.jl:269-321,
