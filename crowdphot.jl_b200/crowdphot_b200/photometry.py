@@ -16,8 +16,9 @@ Differences from the Julia API, all deliberate:
     TukeyLoss and PSF types other than CircularGaussianPSF / ImagePSF /
     GriddedPSFModel{ImagePSF} raise ArgumentError -- there is no CPU fallback;
   * the batched group entry points (``fit_all_stars_simultaneous_batch``,
-    ``fit_groups_packed``, ``BatchGraph``, ``Server``) leave ``spread_model`` /
-    ``spread_model_err`` NaN; the single-field entry points compute them.
+    ``fit_groups_packed``, ``BatchGraph``) leave ``spread_model`` /
+    ``spread_model_err`` NaN; the single-field entry points and ``Server``
+    compute them.
 """
 from __future__ import annotations
 
