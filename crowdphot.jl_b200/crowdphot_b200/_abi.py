@@ -167,6 +167,7 @@ class GroupResult(C.Structure):
         ("n_kernel_groups", C.c_int64),
         ("n_routed_groups", C.c_int64),
         ("device_seconds", C.c_double),
+        ("spread_model", _dp), ("spread_model_err", _dp),
     ]
 
 

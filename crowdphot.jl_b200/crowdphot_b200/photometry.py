@@ -15,10 +15,9 @@ Differences from the Julia API, all deliberate:
   * ``solver=:lsmr``, IRLS losses other than L2DistLoss / HuberLoss /
     TukeyLoss and PSF types other than CircularGaussianPSF / ImagePSF /
     GriddedPSFModel{ImagePSF} raise ArgumentError -- there is no CPU fallback;
-  * the batched group entry points (``fit_all_stars_simultaneous_batch``,
-    ``fit_groups_packed``, ``BatchGraph``) leave ``spread_model`` /
-    ``spread_model_err`` NaN; the single-field entry points and ``Server``
-    compute them.
+  * a simultaneous fit whose first catalogue star has a non-finite position
+    returns ``spread_model`` NaN where the reference's ``_spread_fwhm`` raises
+    an InexactError.
 """
 from __future__ import annotations
 
@@ -433,7 +432,7 @@ def group_outputs(n_stars, n_groups, total_pixels=0, residual=False):
     """Caller-owned output arrays of one cpb_group_result (numpy, host)."""
     ns, G = max(n_stars, 1), max(n_groups, 1)
     o = {k: np.zeros(ns) for k in ("y", "x", "flux", "y_err", "x_err", "flux_err", "chisq", "qfit",
-                                   "qfit_expected", "qfit_z", "crowding")}
+                                   "qfit_expected", "qfit_z", "crowding", "spread_model", "spread_model_err")}
     o.update(converged=np.zeros(ns, np.uint8), valid=np.zeros(ns, np.uint8), n_iter=np.zeros(ns, np.int32))
     o.update({k: np.zeros(G, np.int32) for k in ("n_passes", "n_failed", "status", "error_kind", "n_active",
                                                  "n_union", "n_trials", "n_lsqr_iters")})
@@ -538,7 +537,6 @@ def fit_all_stars_simultaneous_batch(images, psf, sources_list, fit_rad, *, inv_
         n = int(s1 - s0)
         sl = slice(s0, s1)
         ny_, nx_ = arrs[g][0].shape
-        nan = np.full(n, np.nan)
         valid = out["valid"][sl].astype(bool)
         msgs = [] if out["n_active"][g] == n else [
             f"star {i + 1}: excluded before the solve (no usable pixels or non-finite initial parameters)"
@@ -551,8 +549,9 @@ def fit_all_stars_simultaneous_batch(images, psf, sources_list, fit_rad, *, inv_
             bkg=np.full(n, float(fixed.get("bkg", 0.0))), bkg_err=np.zeros(n),
             converged=out["converged"][sl].astype(bool), valid=valid, chisq=out["chisq"][sl].copy(),
             qfit=out["qfit"][sl].copy(), qfit_expected=out["qfit_expected"][sl].copy(),
-            qfit_z=out["qfit_z"][sl].copy(), crowding=out["crowding"][sl].copy(), spread_model=nan.copy(),
-            spread_model_err=nan.copy(), n_iter=out["n_iter"][sl].astype(np.int64),
+            qfit_z=out["qfit_z"][sl].copy(), crowding=out["crowding"][sl].copy(),
+            spread_model=out["spread_model"][sl].copy(), spread_model_err=out["spread_model_err"][sl].copy(),
+            n_iter=out["n_iter"][sl].astype(np.int64),
             n_passes=int(out["n_passes"][g]), n_failed=int(out["n_failed"][g]), failure_msgs=msgs, residual=resid,
             stats=dict(n_active=int(out["n_active"][g]), n_union=int(out["n_union"][g]),
                        n_trials=int(out["n_trials"][g]), n_lsqr_iters=int(out["n_lsqr_iters"][g]),

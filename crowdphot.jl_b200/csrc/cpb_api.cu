@@ -490,6 +490,8 @@ int cpb_fit_simultaneous_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
         d.qfit_expected = (double*)dout("gb_o_q2", out->qfit_expected, 8 * ns);
         d.qfit_z = (double*)dout("gb_o_q3", out->qfit_z, 8 * ns);
         d.crowding = (double*)dout("gb_o_cr", out->crowding, 8 * ns);
+        d.spread_model = (double*)dout("gb_o_sm", out->spread_model, 8 * ns);
+        d.spread_model_err = (double*)dout("gb_o_sme", out->spread_model_err, 8 * ns);
         d.residual = (double*)dout("gb_o_res", out->residual, 8 * npx);
         d.n_passes = (int32_t*)dout("gb_o_np", out->n_passes, 4 * G);
         d.n_failed = (int32_t*)dout("gb_o_nf", out->n_failed, 4 * G);
@@ -518,6 +520,8 @@ int cpb_fit_simultaneous_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
         down(out->qfit_expected, d.qfit_expected, 8 * ns);
         down(out->qfit_z, d.qfit_z, 8 * ns);
         down(out->crowding, d.crowding, 8 * ns);
+        down(out->spread_model, d.spread_model, 8 * ns);
+        down(out->spread_model_err, d.spread_model_err, 8 * ns);
         down(out->residual, d.residual, 8 * npx);
         down(out->n_passes, d.n_passes, 4 * G);
         down(out->n_failed, d.n_failed, 4 * G);

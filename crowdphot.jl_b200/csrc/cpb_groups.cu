@@ -62,6 +62,12 @@ struct GroupConst {
     int eltype;
     int reweighted;
     double fit_rad;
+    // spread_model: on when requested and its disk width is NaN (derived per
+    // group) or finite and positive; the disk table length and the fit box
+    // capacity ((2 R + 2)^2 pixels)
+    int sp_on, sp_tab, sp_box;
+    double sp_param;     // spread_model_fwhm (NaN: _spread_fwhm of the group's first star)
+    double sp_psf_fwhm;  // the PSF object's own FWHM, which _spread_fwhm renders
 };
 
 struct GroupIn {
@@ -82,6 +88,9 @@ struct GroupOut {
     double *chisq, *qfit, *qfit_expected, *qfit_z, *crowding;
     double* residual;
     int32_t *n_passes, *n_failed, *status, *error_kind, *n_active, *n_union, *n_trials, *n_lsqr;
+    double *spread, *spread_err;
+    double* sp_rw;          // per star: residual and weight over its box, 2 sp_box doubles (spread_model)
+    const double* sp_rule;  // kSpreadRuleLen doubles (spread_rule)
 };
 
 // Byte offsets of the shared-memory layout (same computation on host and device).
@@ -625,6 +634,8 @@ __global__ void __launch_bounds__(NT) k_groups(GroupConst C, DevPsf P, GroupIn i
             if (O.qfit_expected) O.qfit_expected[o] = NaN;
             if (O.qfit_z) O.qfit_z[o] = NaN;
             if (O.crowding) O.crowding[o] = NaN;
+            if (O.spread) O.spread[o] = NaN;
+            if (O.spread_err) O.spread_err[o] = NaN;
         };
         auto fixed_fix = [&](int64_t o) {  // fixed parameters take the fixed values, error 0
             bool fy = false, fx = false, ff = false;
@@ -1071,7 +1082,9 @@ __global__ void __launch_bounds__(NT) k_groups(GroupConst C, DevPsf P, GroupIn i
             }
         }
         // ---- chisq and the qfit / crowding diagnostics (:1358-1397,
-        // psf_photometry_diagnostics.jl:154-231), one warp per valid star
+        // psf_photometry_diagnostics.jl:154-231), one warp per valid star; with
+        // spread_model on, each box pixel's residual and weight also go to the
+        // star's planes for k_group_spread
         for (int a = wid; a < n_act; a += NT / 32) {
             const StarCoef c = cf[a];
             const int64_t o = soff + act[a];
@@ -1082,6 +1095,7 @@ __global__ void __launch_bounds__(NT) k_groups(GroupConst C, DevPsf P, GroupIn i
             int ng_ = 0, ngi = 0;
             const int h = yhi - ylo + 1, wd = xhi - xlo + 1;
             const double inv_flux = 1.0 / c.flux;
+            double* rw = C.sp_on ? O.sp_rw + (size_t)o * 2 * C.sp_box : nullptr;
             if (h > 0 && wd > 0)
                 for (int e = lane; e < h * wd; e += 32) {
                     const int gy = ylo + e % h, gx = xlo + e / h;
@@ -1093,6 +1107,10 @@ __global__ void __launch_bounds__(NT) k_groups(GroupConst C, DevPsf P, GroupIn i
                     F.G.data_w(q, d, wsan);
                     const double r = d - acc;
                     const double wp = in.iv ? F.G.ld(in.iv, q) : 1.0;
+                    if (rw) {
+                        rw[e] = r;
+                        rw[C.sp_box + e] = (isfinite(wp) && wp > 0) ? wp : 0.0;
+                    }
                     if (isfinite(wp) && wp > 0) {
                         num += wp * (r * r);
                         ng_ += 1;
@@ -1142,6 +1160,115 @@ __global__ void __launch_bounds__(NT) k_groups(GroupConst C, DevPsf P, GroupIn i
     }
 }
 
+// spread_model of the kernel-fitted groups (_star_diagnostics!,
+// psf_photometry_diagnostics.jl:200-231, with the disk of
+// psf_photometry_simultaneous.jl:1361-1365), after k_groups: one block per group
+// (grid-stride over the group list), one warp per valid star.  The block builds
+// the group's disk into shared memory, its width from the first catalogue
+// star's final parameters; each warp renders its star's model stamp over the
+// fit box and correlates it with the disk one component at a time (x pass, then
+// the y pass added into the correlated stamp), all in its own 3 sp_box doubles
+// of shared memory, and sums against the residual and weight planes k_groups
+// saved for the star.  Kept out of k_groups so that the fit's register
+// allocation does not carry it.
+__global__ void __launch_bounds__(128) k_group_spread(GroupConst C, DevPsf P, GroupIn in, GroupOut O,
+                                                      const int32_t* __restrict__ glist, int nlist) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[2 * 4 + 1];
+    const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+    const int kh = C.R, box = C.sp_box, n = 2 * kh + 1;
+    const int nw = blockDim.x >> 5, lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double* tab = sm;
+    double* pan = tab + ((C.sp_tab + 1) & ~1);
+    double* M = pan + (7 + kh) * kSpreadGL + (size_t)wid * 3 * box;  // the warp's model stamp
+    double* T = M + box;                                             // one component's x pass
+    double* Gs = T + box;                                            // the disk-correlated stamp
+    DevPsf Ps = P;
+    Ps.fwhm = C.sp_psf_fwhm;  // _spread_fwhm renders the PSF object's own width
+    for (int li = blockIdx.x; li < nlist; li += gridDim.x) {
+        const int g = glist[li];
+        const int64_t soff = in.star_off[g];
+        const int ng = (int)(in.star_off[g + 1] - soff);
+        int any = 0;
+        for (int i = threadIdx.x; i < ng; i += blockDim.x) any |= O.valid[soff + i];
+        if (!__syncthreads_or(any)) continue;  // also: the previous group's disk is no longer read
+        spread_disk_block(Ps, C.sp_param, kh, O.y[soff], O.x[soff], O.sp_rule, tab, red, pan);
+        if (!spread_tab_on(tab)) continue;
+        const SpreadDev D = spread_dev(tab, kh);
+        const int ny = in.ny[g], nx = in.nx[g];
+        for (int i = wid; i < ng; i += nw) {
+            const int64_t o = soff + i;
+            if (!O.valid[o]) continue;
+            StarCoef c;
+            c.y = O.y[o];
+            c.x = O.x[o];
+            c.flux = O.flux[o];
+            c.bkg = C.fixed_bkg;
+            grid_corners_dw(P, c.y, c.x, c);
+            const int ylo = max((int)floor(c.y - C.fit_rad), 1), yhi = min((int)ceil(c.y + C.fit_rad), ny);
+            const int xlo = max((int)floor(c.x - C.fit_rad), 1), xhi = min((int)ceil(c.x + C.fit_rad), nx);
+            const int h = yhi - ylo + 1, wd = xhi - xlo + 1, nb = h * wd;
+            if (h <= 0 || wd <= 0 || nb > box) continue;
+            const double* Rr = O.sp_rw + (size_t)o * 2 * box;
+            const double* Wt = Rr + box;
+            __syncwarp();  // the warp's previous stamp is no longer read
+            for (int e = lane; e < nb; e += 32) {
+                M[e] = psf_value(P, c, ylo + e % h, xlo + e / h);
+                Gs[e] = 0.0;
+            }
+            for (int cc = 0; cc < 6; ++cc) {
+                const int L = D.L[cc];
+                const double* I = D.I + cc * n + kh;
+                __syncwarp();
+                for (int e = lane; e < nb; e += 32) {  // x pass
+                    const int r = e % h, col = e / h;
+                    const int q0 = max(-L, -col), q1 = min(L, wd - 1 - col);
+                    double t = 0.0;
+                    for (int q = q0; q <= q1; ++q) t += I[q] * M[r + (col + q) * h];
+                    T[e] = t;
+                }
+                __syncwarp();
+                for (int e = lane; e < nb; e += 32) {  // y pass
+                    const int r = e % h, col = e / h;
+                    const int p0 = max(-L, -r), p1 = min(L, h - 1 - r);
+                    double t = 0.0;
+                    for (int p = p0; p <= p1; ++p) t += I[p] * T[r + p + col * h];
+                    Gs[e] += D.alpha[cc] * t;
+                }
+            }
+            __syncwarp();
+            const double inv_flux = 1.0 / c.flux;
+            double Sp = 0, Sq = 0, Sp0 = 0, Sq0 = 0, SqG = 0;
+            for (int e = lane; e < nb; e += 32) {
+                const double wp = Wt[e];
+                if (wp > 0) {
+                    const double mv = M[e];
+                    const double Pp = (mv - c.bkg) * inv_flux;
+                    const double wP = wp * Pp;
+                    const double p_i = Rr[e] + mv - c.bkg;
+                    const double g_i = (Gs[e] - c.bkg) * inv_flux;
+                    Sp += wP * p_i;
+                    Sq += wp * g_i * p_i;
+                    Sp0 += wP * Pp;
+                    Sq0 += wp * Pp * g_i;
+                    SqG += wp * g_i * g_i;
+                }
+            }
+            Sp = warp_sum(Sp);
+            Sq = warp_sum(Sq);
+            Sp0 = warp_sum(Sp0);
+            Sq0 = warp_sum(Sq0);
+            SqG = warp_sum(SqG);
+            if (lane == 0 && Sp > 0) {
+                if (O.spread) O.spread[o] = Sq / Sp - Sq0 / Sp0;
+                if (O.spread_err)
+                    O.spread_err[o] =
+                        in.iv ? sqrt(fmax(0.0, Sp * Sp * SqG + Sq * Sq * Sp0 - 2 * Sq * Sp * Sq0)) / (Sp * Sp) : NaN;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -1186,6 +1313,9 @@ struct GroupSetup {
     std::vector<int32_t> h_ny, h_nx;
     int64_t total_pixels = 0;
     int32_t eltype = CPB_F64;
+    int sp_nw = 0;        // spread_model: warps a k_group_spread block (0: off)
+    size_t sp_smem = 0;   // its dynamic shared memory
+    int64_t n_stars = 0;  // catalogue length (sizes the residual / weight planes)
 };
 
 constexpr size_t kStaticSmem = 8 * 1024;  // the kernel's static shared arrays, rounded up
@@ -1273,6 +1403,14 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
     C.eltype = eltype;
     C.reweighted = (P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && d_iv == nullptr)) ? 1 : 0;
     C.fit_rad = P->fit_rad;
+    {
+        const double spp = P->spread_model_fwhm;
+        C.sp_on = (out->spread_model || out->spread_model_err) && (std::isnan(spp) || (std::isfinite(spp) && spp > 0));
+        C.sp_tab = spread_tab_len(C.R);
+        C.sp_box = (2 * C.R + 2) * (2 * C.R + 2);
+        C.sp_param = spp;
+        C.sp_psf_fwhm = psf->dev.fwhm;
+    }
     su.dp = psf->dev;
     su.dp.fwhm = P->fixed_fwhm;
 
@@ -1282,7 +1420,8 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
     su.go = GroupOut{out->y, out->x, out->flux, out->y_err, out->x_err, out->flux_err, out->converged, out->valid,
                      out->n_iter, out->chisq, out->qfit, out->qfit_expected, out->qfit_z, out->crowding,
                      out->residual, out->n_passes, out->n_failed, out->status, out->error_kind, out->n_active,
-                     out->n_union, out->n_trials, out->n_lsqr_iters};
+                     out->n_union, out->n_trials, out->n_lsqr_iters, out->spread_model, out->spread_model_err,
+                     nullptr, nullptr};
     if (G == 0) return;
     // group sizes on the host (plan the shared-memory layout, route oversized groups)
     std::vector<int64_t>& h_off = su.h_off;
@@ -1316,6 +1455,19 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
     check(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device), "attr");
     const size_t cap = (size_t)smem_optin - kStaticSmem;
+    su.n_stars = h_soff[G];
+    if (C.sp_on) {
+        // k_group_spread: the disk table and one panel of the quadrature, then
+        // 3 sp_box doubles a warp; up to 4 warps within 96 KB, else fewer; a fit
+        // box beyond shared memory even for one warp leaves spread_model NaN
+        const size_t fixed = ((size_t)((C.sp_tab + 1) & ~1) + (size_t)(7 + C.R) * kSpreadGL) * sizeof(double);
+        const size_t per_warp = (size_t)3 * C.sp_box * sizeof(double);
+        int nw = 4;
+        while (nw > 1 && fixed + nw * per_warp > 96 * 1024) --nw;
+        if (fixed + nw * per_warp > cap) C.sp_on = 0;
+        su.sp_nw = C.sp_on ? nw : 0;
+        su.sp_smem = fixed + nw * per_warp;
+    }
     GroupPlan& plan = su.plan;
     auto need_of = [&](int ng, int um, int kn) {
         return ng > 32 ? layout_bytes<uint64_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn)
@@ -1420,6 +1572,20 @@ void launch_bucket(cpb_ctx* ctx, cudaStream_t st, const GroupSetup& su, const Bu
     check(cudaGetLastError(), "k_groups");
 }
 
+// k_group_spread over the kernel-fitted groups (after their bucket launches).
+void launch_spread(cpb_ctx* ctx, cudaStream_t st, const GroupSetup& su, const int32_t* d_list, int64_t nk) {
+    if (!su.C.sp_on || nk <= 0) return;
+    const int threads = 32 * su.sp_nw;
+    check(cudaFuncSetAttribute(k_group_spread, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)su.sp_smem),
+          "smem attr");
+    int per_sm = 0;
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_group_spread, threads, su.sp_smem), "occupancy");
+    const int64_t grid = std::min<int64_t>(nk, (int64_t)ctx->n_sm * std::max(per_sm, 1));
+    KernelScope ks_(ctx, "k_group_spread", 0.0);
+    k_group_spread<<<(unsigned)grid, threads, su.sp_smem, st>>>(su.C, su.dp, su.gin, su.go, d_list, (int)nk);
+    check(cudaGetLastError(), "k_group_spread");
+}
+
 }  // namespace
 
 int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G, const int64_t* d_off,
@@ -1446,6 +1612,14 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         // every bucket's group list back to back, one queue counter per bucket
         std::vector<int32_t> lists;
         for (const Bucket& B : plan.buckets) lists.insert(lists.end(), B.groups.begin(), B.groups.end());
+        if (su.C.sp_on) {
+            double h_rule[kSpreadRuleLen];
+            spread_rule(h_rule);
+            auto* d_rule = (double*)scratch(ctx, "grp_sp_rule", sizeof(h_rule));
+            check(cudaMemcpyAsync(d_rule, h_rule, sizeof(h_rule), cudaMemcpyHostToDevice, st), "h2d");
+            su.go.sp_rule = d_rule;
+            su.go.sp_rw = (double*)scratch(ctx, "grp_sp_rw", sizeof(double) * 2 * su.C.sp_box * su.n_stars);
+        }
         int32_t* d_list = (int32_t*)scratch(ctx, "grp_list", sizeof(int32_t) * nk);
         int* d_queue = (int*)scratch(ctx, "grp_queue", sizeof(int) * plan.buckets.size());
         check(cudaMemcpyAsync(d_list, lists.data(), sizeof(int32_t) * nk, cudaMemcpyHostToDevice, st), "h2d");
@@ -1454,6 +1628,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
             launch_bucket(ctx, st, su, plan.buckets[b], d_list + at, d_queue + b, 0, 0);
             at += (int64_t)plan.buckets[b].groups.size();
         }
+        launch_spread(ctx, st, su, d_list, nk);
     }
     check(cudaEventRecord(ctx->ev1, st), "event");
     check(cudaStreamSynchronize(st), "sync");
@@ -1469,7 +1644,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         const size_t esz = eltype == CPB_F64 ? 8 : 4;
         const int64_t off = h_off[g];
         std::vector<double> y(ng), x(ng), f(ng), b(ng), ey(ng), ex(ng), ef(ng), eb(ng), chi(ng), q1(ng), q2(ng),
-            q3(ng), cr(ng);
+            q3(ng), cr(ng), sm(ng), sme(ng);
         std::vector<uint8_t> cv(ng), va(ng);
         std::vector<int32_t> it(ng);
         std::vector<double> res(out->residual ? (size_t)ny * nx : 0);
@@ -1489,6 +1664,8 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         r.qfit_expected = q2.data();
         r.qfit_z = q3.data();
         r.crowding = cr.data();
+        r.spread_model = sm.data();
+        r.spread_model_err = sme.data();
         r.n_iter = it.data();
         r.residual = out->residual ? res.data() : nullptr;
         int32_t status = 0, kind = 0;
@@ -1518,7 +1695,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
                 va[i] = 0;
                 it[i] = 0;
                 chi[i] = 0.0;
-                q1[i] = q2[i] = q3[i] = cr[i] = NaN;
+                q1[i] = q2[i] = q3[i] = cr[i] = sm[i] = sme[i] = NaN;
             }
             std::fill(res.begin(), res.end(), 0.0);
             r.n_passes = 0;
@@ -1545,6 +1722,8 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
         if (out->qfit_expected) up(out->qfit_expected + s0, q2.data(), 8 * ng);
         if (out->qfit_z) up(out->qfit_z + s0, q3.data(), 8 * ng);
         if (out->crowding) up(out->crowding + s0, cr.data(), 8 * ng);
+        if (out->spread_model) up(out->spread_model + s0, sm.data(), 8 * ng);
+        if (out->spread_model_err) up(out->spread_model_err + s0, sme.data(), 8 * ng);
         if (out->residual) up(out->residual + off, res.data(), 8 * res.size());
         const int32_t na = (int32_t)r.n_active, nu = (int32_t)r.n_union, ntr = (int32_t)r.n_trials,
                       nls = (int32_t)r.n_lsqr_iters;
@@ -1571,6 +1750,7 @@ struct GroupBatch {
     int* d_queue = nullptr;     // owned: one counter per bucket
     std::vector<int64_t> at;    // first list entry of each bucket
     std::vector<int> threads;   // chosen block size per bucket
+    double* sp_buf = nullptr;   // owned: spread_model rule and the stars' residual / weight planes
 };
 
 GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int64_t G,
@@ -1604,7 +1784,21 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
         if (!lists.empty())
             check(cudaMemcpy(b->d_list, lists.data(), sizeof(int32_t) * lists.size(), cudaMemcpyHostToDevice),
                   "h2d");
+        GroupSetup& su = b->su;
+        if (su.C.sp_on && !plan.buckets.empty()) {
+            const size_t n_rule = kSpreadRuleLen, n_rw = (size_t)2 * su.C.sp_box * su.n_stars;
+            if (cudaMalloc(&b->sp_buf, sizeof(double) * (n_rule + n_rw)) != cudaSuccess) {
+                cudaGetLastError();
+                throw OomError{"device memory exhausted allocating the spread_model planes"};
+            }
+            double h_rule[kSpreadRuleLen];
+            spread_rule(h_rule);
+            check(cudaMemcpy(b->sp_buf, h_rule, sizeof(h_rule), cudaMemcpyHostToDevice), "h2d");
+            su.go.sp_rule = b->sp_buf;
+            su.go.sp_rw = b->sp_buf + n_rule;
+        }
     } catch (...) {
+        cudaFree(b->sp_buf);
         cudaFree(b->d_list);
         cudaFree(b->d_queue);
         delete b;
@@ -1623,6 +1817,7 @@ void group_batch_enqueue(cpb_ctx* ctx, GroupBatch* b, cudaStream_t st, int bucke
         launch_bucket(ctx, st, b->su, bks[k], b->d_list + b->at[k], b->d_queue + k,
                       threads > 0 ? threads : b->threads[k], 0);
     }
+    if (bucket < 0) launch_spread(ctx, st, b->su, b->d_list, group_batch_size(b));
 }
 
 void group_batch_set_threads(GroupBatch* b, int bucket, int threads) { b->threads[bucket] = valid_threads(threads); }
@@ -1645,6 +1840,7 @@ std::string group_batch_signature(const GroupBatch* b, int bucket) {
 
 void group_batch_destroy(GroupBatch* b) {
     if (!b) return;
+    cudaFree(b->sp_buf);
     cudaFree(b->d_list);
     cudaFree(b->d_queue);
     delete b;

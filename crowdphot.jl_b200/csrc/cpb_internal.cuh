@@ -395,14 +395,19 @@ __device__ __forceinline__ void block_sum_n(double (&v)[K], double* sh) {
 // for every component whose support reaches it): T[c * ld + e] = sum_q
 // I_c(q) M[r, col + q] over the in-box columns, e = r + col * bh.  Is: the six
 // profiles in shared memory, 6 x (2 kh + 1).  The y pass and the weighting are
-// spread_ypass at each pixel.  No barrier inside.
+// spread_ypass at each pixel.  Pixels t0, t0 + ts, ... (the block by default,
+// a warp with t0 = lane, ts = 32).  No barrier inside.
 __device__ __forceinline__ void spread_xpass_all(const SpreadDev& D, const double* Is, const double* M, double* T,
-                                                 int ld, int bh, int bw) {
+                                                 int ld, int bh, int bw, int t0 = -1, int ts = 0) {
+    if (t0 < 0) {
+        t0 = threadIdx.x;
+        ts = blockDim.x;
+    }
     const int n = 2 * D.kh + 1, nb = bh * bw;
     int Lmax = 0;
 #pragma unroll
     for (int c = 0; c < 6; ++c) Lmax = max(Lmax, D.L[c]);
-    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+    for (int e = t0; e < nb; e += ts) {
         const int r = e % bh, col = e / bh;
         const int q0 = max(-Lmax, -col), q1 = min(Lmax, bw - 1 - col);
         double t[6] = {0, 0, 0, 0, 0, 0};
@@ -452,6 +457,169 @@ inline int spread_mode(int boxmax, int kh) {
     if (spread_smem_bytes(1, boxmax, kh) <= 200 * 1024) return 1;
     if (spread_smem_bytes(2, boxmax, kh) <= 200 * 1024) return 2;
     return 0;
+}
+
+// A spread_model disk built on the device, for fits whose disk width depends on
+// a fitted position (the simultaneous fit sizes it from the first catalogue
+// star's final parameters, psf_photometry_simultaneous.jl:1363-1365).  Table of
+// spread_tab_len(kh) doubles: [0] the disk FWHM (spread_model is off unless it
+// is finite and positive), [1..6] alpha_c, [7..12] L_c, then the six profiles
+// I_c(m), m = -kh..kh, as in SpreadDev.  The quadrature rule (spread_rule in
+// cpb_spread.cu, kSpreadRuleLen doubles): the 32 Gauss-Legendre nodes on
+// [-1, 1], their weights, the six mixture amplitudes and the six variances.
+constexpr int kSpreadHdr = 13;
+constexpr int kSpreadGL = 32;
+constexpr int kSpreadRuleLen = 2 * kSpreadGL + 12;
+__host__ __device__ inline int spread_tab_len(int kh) { return kSpreadHdr + 6 * (2 * kh + 1); }
+void spread_rule(double* out);  // host: fills kSpreadRuleLen doubles
+
+__device__ inline bool spread_tab_on(const double* tab) { return isfinite(tab[0]) && tab[0] > 0; }
+
+__device__ inline SpreadDev spread_dev(const double* tab, int kh) {
+    SpreadDev D;
+    D.I = tab + kSpreadHdr;
+    D.kh = kh;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        D.alpha[c] = tab[1 + c];
+        D.L[c] = (int)tab[7 + c];
+    }
+    return D;
+}
+
+// _spread_fwhm (psf_photometry_diagnostics.jl:113-125) by the whole block: the
+// unit render centred at (Y, X) over PSF.extent(Int, m), sqrt(ea 2 ln2 / pi)
+// with ea = (sum g)^2 / sum g^2.  P.fwhm is the PSF's own FWHM (Gaussian).
+// red: 2 (blockDim.x / 32) + 1 doubles of shared memory.  Every thread gets
+// the value; a non-finite position gives NaN.
+__device__ inline double spread_fwhm_block(const DevPsf& P, double Y, double X, double* red) {
+    if (!(isfinite(Y) && isfinite(X))) return __longlong_as_double(0x7ff8000000000000LL);
+    StarCoef c;
+    c.y = Y;
+    c.x = X;
+    c.flux = 1.0;
+    c.bkg = 0.0;
+    grid_corners_dw(P, Y, X, c);
+    double e0 = 0, e1 = 0, e2 = 0, e3 = 0;
+    if (P.kind == CPB_PSF_CIRCULAR_GAUSSIAN) {
+        const double a = 5.0 * P.fwhm / 2;  // fwhm_factor 5, no rotation
+        e0 = Y - a;
+        e1 = Y + a;
+        e2 = X - a;
+        e3 = X + a;
+    } else {
+        bool first = true;
+        for (int k = 0; k < 4; ++k) {
+            if (c.idx[k] < 0 || c.w[k] == 0.0) continue;
+            const DevNode nd = P.nodes[c.idx[k]];
+            const double lo_y = Y - (nd.oy - 1.0) / nd.sy, hi_y = Y + ((double)nd.ny - nd.oy) / nd.sy;
+            const double lo_x = X - (nd.ox - 1.0) / nd.sx, hi_x = X + ((double)nd.nx - nd.ox) / nd.sx;
+            e0 = first ? lo_y : fmin(e0, lo_y);
+            e1 = first ? hi_y : fmax(e1, hi_y);
+            e2 = first ? lo_x : fmin(e2, lo_x);
+            e3 = first ? hi_x : fmax(e3, hi_x);
+            first = false;
+        }
+    }
+    const int ylo = (int)floor(e0), yhi = (int)ceil(e1), xlo = (int)floor(e2), xhi = (int)ceil(e3);
+    const int h = max(yhi - ylo + 1, 0), w = max(xhi - xlo + 1, 0);
+    double v[2] = {0.0, 0.0};
+    for (int e = threadIdx.x; e < h * w; e += blockDim.x) {
+        const double g = model_value<double, double>(P, P.data64, c, (double)(ylo + e % h), (double)(xlo + e / h));
+        v[0] += g;
+        v[1] += g * g;
+    }
+    block_sum_n<2>(v, red);
+    const int slot = 2 * (blockDim.x >> 5);
+    if (threadIdx.x == 0) red[slot] = sqrt(v[0] * v[0] / v[1] * 2 * 0.6931471805599453 / 3.141592653589793);
+    __syncthreads();
+    const double f = red[slot];
+    __syncthreads();
+    return f;
+}
+
+// The disk table of one fit (layout above), by the whole block:
+// _exp_disk_kernel_bandlimited(f; half = kh) (psf_photometry_diagnostics.jl:82-100)
+// as six separable profiles I_c(m) = int_{-1/2}^{1/2} exp(-a_c k^2) cos(2 pi k m) dk,
+// a_c = 2 pi^2 re^2 v_c, re = f / 16 * 1.67834699, zero where pi^2 m^2 / a_c > 690.
+// The integral is composite 32-point Gauss-Legendre on max(4, 2 kh) equal panels
+// of [-1/2, 1/2] (the host rule of cpb_exp_disk_kernel); the integrand is even,
+// so the right half's panels are summed and doubled.  One panel at a time, the
+// block tabulates the weighted exp(-a_c k^2) of the six components and
+// cos(2 pi k m) of the kh + 1 orders at the panel's 32 nodes in `pan`
+// ((7 + kh) * 32 doubles of shared memory), then one thread per (c, m) adds
+// the panel's 32 products -- 7 + kh transcendentals a node instead of
+// 12 (kh + 1).  f = param unless param is NaN (then _spread_fwhm at (Y, X));
+// spread_tab_on(tab) tells whether spread_model is on.  Ends with a barrier.
+__device__ inline void spread_disk_block(const DevPsf& P, double param, int kh, double Y, double X,
+                                         const double* __restrict__ rule, double* tab, double* red, double* pan) {
+    const double f = isnan(param) ? spread_fwhm_block(P, Y, X, red) : param;
+    if (threadIdx.x == 0) tab[0] = f;
+    if (!(isfinite(f) && f > 0)) {
+        __syncthreads();
+        return;
+    }
+    const double pi = 3.141592653589793;
+    const int n = 2 * kh + 1, np = 6 * (kh + 1), rows = 7 + kh;
+    const double re = f / 16 * 1.67834699;
+    const int panels = max(4, 2 * kh);
+    const double hw = 0.5 / panels;
+    const double* gx = rule;
+    const double* gw = rule + kSpreadGL;
+    const double* amp = rule + 2 * kSpreadGL;
+    const double* var = amp + 6;
+    double* I0 = tab + kSpreadHdr;  // I_c(m) for m >= 0 accumulates at I0[c * n + kh + m]
+    for (int t = threadIdx.x; t < np; t += blockDim.x) I0[(t / (kh + 1)) * n + kh + t % (kh + 1)] = 0.0;
+    for (int pnl = panels / 2; pnl < panels; ++pnl) {
+        const double mid = -0.5 + (2 * pnl + 1) * hw;
+        __syncthreads();  // the previous panel's table is no longer read
+        for (int t = threadIdx.x; t < rows * kSpreadGL; t += blockDim.x) {
+            const int q = t % kSpreadGL, row = t / kSpreadGL;
+            const double k = mid + hw * gx[q];
+            pan[t] = row < 6 ? hw * gw[q] * exp(-(2 * pi * pi * re * re * var[row]) * k * k)
+                             : cospi(2 * k * (double)(row - 6));
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < np; t += blockDim.x) {
+            const int cc = t / (kh + 1), m = t % (kh + 1);
+            const double a = 2 * pi * pi * re * re * var[cc];
+            if (pi * pi * (double)m * m / a > 690) continue;
+            const double* E = pan + cc * kSpreadGL;
+            const double* Cm = pan + (6 + m) * kSpreadGL;
+            double sp = 0.0;
+#pragma unroll 8
+            for (int q = 0; q < kSpreadGL; ++q) sp += E[q] * Cm[q];
+            I0[cc * n + kh + m] += sp;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < np; t += blockDim.x) {
+        const int cc = t / (kh + 1), m = t % (kh + 1);
+        const double I = 2 * I0[cc * n + kh + m];
+        I0[cc * n + kh + m] = I;
+        I0[cc * n + kh - m] = I;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const double* Iv = I0 + threadIdx.x * n + kh;
+        int L = 0;
+        for (int m = kh; m > 0; --m)
+            if (Iv[m] != 0.0) {
+                L = m;
+                break;
+            }
+        tab[7 + threadIdx.x] = (double)L;
+    }
+    if (threadIdx.x == 0) {
+        double total = 0.0;
+        for (int c = 0; c < 6; ++c) {
+            double s = 0.0;
+            for (int m = 0; m < n; ++m) s += I0[c * n + m];
+            total += amp[c] * s * s;
+        }
+        for (int c = 0; c < 6; ++c) tab[1 + c] = amp[c] / total;
+    }
+    __syncthreads();
 }
 
 }  // namespace cpb

@@ -1180,23 +1180,48 @@ __global__ void k_errors(int64_t n_act, int p, const double* gram, bool reweight
     for (int k = 0; k < p; ++k) err[j * p + k] = sqrt(fmax(0.0, inv[k + k * p] * f));
 }
 
+// The spread_model disk of the simultaneous fit, one block.  Its width comes
+// from the first catalogue star's parameters after the final bookkeeping
+// (params[row_y, 1], params[row_x, 1], :1289-1299 and :1363-1364): the fitted
+// position when that star is active (then it is active star 0, the active list
+// being in catalogue order), its catalogue position when not, the fixed value
+// of a fixed coordinate.  ky / kx: their rows in theta, -1 when fixed.  Dynamic
+// shared memory: the quadrature panel, (7 + kh) * 32 doubles.
+__global__ void __launch_bounds__(256) k_spread_disk(DevPsf P, double param, int kh,
+                                                     const double* __restrict__ theta,
+                                                     const int32_t* __restrict__ act, int64_t n_act, int p, int ky,
+                                                     int kx, double fixed_y, double fixed_x,
+                                                     const double* __restrict__ y0, const double* __restrict__ x0,
+                                                     const double* __restrict__ rule, double* tab) {
+    extern __shared__ double pan[];
+    __shared__ double red[2 * 8 + 1];
+    const bool first_active = n_act > 0 && act[0] == 0;
+    const double Y = ky < 0 ? fixed_y : (first_active ? theta[ky] : y0[0]);
+    const double X = kx < 0 ? fixed_x : (first_active ? theta[kx] : x0[0]);
+    spread_disk_block(P, param, kh, Y, X, rule, tab, red, pan);
+}
+
 // chisq and the qfit / crowding / spread_model diagnostics per active star
 // (:1358-1397, psf_photometry_diagnostics.jl:154-231); one block of
 // kDiagThreads a star (grid-stride), the star's model stamp over its box and
-// its disk-correlated copy kept in shared memory (D.I null: spread_model off).
+// its disk-correlated copy kept in shared memory.  stab: the disk table
+// (spread_disk_block; null or off: spread_model NaN), smode its layout.
 template <typename TI>
 __global__ void __launch_bounds__(kDiagThreads, 3) k_diag(int64_t n_act, FitConst fc, DevPsf P, double fit_rad,
                                                       const StarCoef* __restrict__ coef,
                                                       const double* __restrict__ resid, const TI* __restrict__ img,
                                                       const TI* __restrict__ bkgimg, const TI* __restrict__ iv,
-                                                      SpreadDev D, int smode, int boxmax,
+                                                      const double* __restrict__ stab, int kh, int smode,
+                                                      int boxmax,
                                                       double* out /* n_act x 7: chisq qfit qfit_exp qfit_z crowding
                                                                      spread spread_err */) {
     extern __shared__ double stamp[];  // model stamp, x-pass scratch, disk-correlated stamp
     __shared__ double red[14 * (kDiagThreads / 32)];
     __shared__ StarCoef c;
     const double NaN = __longlong_as_double(0x7ff8000000000000LL);
-    const int mode = D.I ? smode : 0;
+    const bool on = stab != nullptr && spread_tab_on(stab);
+    const SpreadDev D = on ? spread_dev(stab, kh) : SpreadDev{};
+    const int mode = on ? smode : 0;
     double* Is = stamp + 7 * boxmax;  // mode 1: the six profiles
     if (mode == 1)
         for (int i = threadIdx.x; i < 6 * (2 * D.kh + 1); i += blockDim.x) Is[i] = D.I[i];
@@ -1532,12 +1557,6 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     unsigned h_flags[4];
     check(cudaMemcpyAsync(&h_nsel, d_nsel, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaMemcpyAsync(h_flags, flags, sizeof(h_flags), cudaMemcpyDeviceToHost, st), "d2h");
-    // the first catalogue star's position sizes the spread_model reference disk
-    double h_yx1[2] = {0, 0};
-    if (n_stars > 0) {
-        check(cudaMemcpyAsync(&h_yx1[0], d_y0, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
-        check(cudaMemcpyAsync(&h_yx1[1], d_x0, sizeof(double), cudaMemcpyDeviceToHost, st), "d2h");
-    }
     check(cudaStreamSynchronize(st), "sync");
     if (!d_inv_var && h_flags[0] > 0)
         throw ArgError{
@@ -2016,20 +2035,33 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
-    // spread_model reference disk (the first catalogue star fixes the PSF's effective width)
-    SpreadHost sh;
-    SpreadDev sd{};
-    const int boxmax = (2 * (int)std::ceil(P->fit_rad) + 2) * (2 * (int)std::ceil(P->fit_rad) + 2);
+    // spread_model reference disk, on the device: its width comes from the first
+    // catalogue star's final parameters (k_spread_disk)
+    const int kh = (int)std::ceil(P->fit_rad);
+    const int boxmax = (2 * kh + 2) * (2 * kh + 2);
+    const double sp_param = P->spread_model_fwhm;
     int smode = 0;
-    if (spread_kernel(psf, psf->dev.fwhm, P->spread_model_fwhm, h_yx1[0], h_yx1[1], P->fit_rad, sh) &&
-        (smode = spread_mode(boxmax, sh.kh)) != 0) {
-        double* d_I = S<double>(ctx, "spread_I", (int64_t)sh.I.size());
-        check(cudaMemcpyAsync(d_I, sh.I.data(), sizeof(double) * sh.I.size(), cudaMemcpyHostToDevice, st), "h2d");
-        sd.I = d_I;
-        sd.kh = sh.kh;
-        for (int c = 0; c < 6; ++c) sd.alpha[c] = sh.alpha[c], sd.L[c] = sh.L[c];
+    double* d_stab = nullptr;
+    if (n_stars > 0 && (std::isnan(sp_param) || (std::isfinite(sp_param) && sp_param > 0)) &&
+        (smode = spread_mode(boxmax, kh)) != 0) {
+        double h_rule[kSpreadRuleLen];
+        spread_rule(h_rule);
+        double* d_rule = S<double>(ctx, "spread_rule", kSpreadRuleLen);
+        d_stab = S<double>(ctx, "spread_tab", spread_tab_len(kh));
+        check(cudaMemcpyAsync(d_rule, h_rule, sizeof(h_rule), cudaMemcpyHostToDevice, st), "h2d");
+        int ky = -1, kx = -1;
+        for (int k = 0; k < p; ++k) {
+            if (fc.gc[k] == 1) ky = k;
+            if (fc.gc[k] == 2) kx = k;
+        }
+        DevPsf ps = dp;
+        ps.fwhm = psf->dev.fwhm;  // _spread_fwhm renders the PSF object's own width
+        KernelScope ks_(ctx, "k_spread_disk", 0.0);
+        k_spread_disk<<<1, 256, sizeof(double) * (7 + kh) * kSpreadGL, st>>>(
+            ps, sp_param, kh, theta, act, n_act, p, ky, kx, P->fixed_y, P->fixed_x, d_y0, d_x0, d_rule, d_stab);
+        check(cudaGetLastError(), "k_spread_disk");
     }
-    const size_t diag_smem = spread_smem_bytes(smode, boxmax, sd.kh);
+    const size_t diag_smem = spread_smem_bytes(smode, boxmax, kh);
     const unsigned dgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
     double* diag = S<double>(ctx, "diag", (int64_t)n_act * 7);
     {
@@ -2041,14 +2073,14 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                       "smem attr");
             k_diag<double><<<dgrid, kDiagThreads, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
                                                                (const double*)d_image, (const double*)d_background,
-                                                               (const double*)d_inv_var, sd, smode, boxmax, diag);
+                                                               (const double*)d_inv_var, d_stab, kh, smode, boxmax, diag);
         } else {
             if (diag_smem > 48 * 1024)
                 check(cudaFuncSetAttribute(k_diag<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem),
                       "smem attr");
             k_diag<float><<<dgrid, kDiagThreads, diag_smem, st>>>(n_act, fc, dp, P->fit_rad, coef, resid,
                                                               (const float*)d_image, (const float*)d_background,
-                                                              (const float*)d_inv_var, sd, smode, boxmax, diag);
+                                                              (const float*)d_inv_var, d_stab, kh, smode, boxmax, diag);
         }
         check(cudaGetLastError(), "k_diag");
     }

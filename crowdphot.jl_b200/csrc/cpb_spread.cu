@@ -1,4 +1,6 @@
-// cpb_spread.cu -- the spread_model reference disk (host side).
+// cpb_spread.cu -- the spread_model reference disk, host side (fit_all_stars and
+// cpb_exp_disk_kernel; the simultaneous fits build theirs on the device with
+// spread_disk_block, whose quadrature rule spread_rule supplies).
 //
 // Restates, for the diagnostics of the device fits,
 //   _spread_fwhm                      src/photometry/psf_photometry_diagnostics.jl:121-133
@@ -67,6 +69,9 @@ void gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
 // _spread_fwhm: the Gaussian-equivalent FWHM of the unit render at (Y, X),
 // sqrt(ea 2 ln2 / pi) with ea = (sum g)^2 / sum g^2 over the PSF's integer extent.
 double spread_fwhm(const cpb_psf* psf, double fwhm, double Y, double X) {
+    // the reference's PSF.extent(Int, m) raises an InexactError on a non-finite
+    // position; here spread_model is then off
+    if (!(std::isfinite(Y) && std::isfinite(X))) return std::nan("");
     double e[4];
     host_extent(psf, fwhm, Y, X, e);
     const int ylo = (int)std::floor(e[0]), yhi = (int)std::ceil(e[1]);
@@ -119,6 +124,22 @@ void exp_disk_components(double fwhm, int half, SpreadHost& S) {
         total += kExpAmp[c] * sum * sum;
     }
     for (int c = 0; c < 6; ++c) S.alpha[c] = kExpAmp[c] / total;
+}
+
+// The quadrature rule and mixture constants of the device disk builder
+// (spread_disk_block): 32 Gauss-Legendre nodes and weights on [-1, 1], the six
+// amplitudes and the six variances.
+void spread_rule(double* out) {
+    std::vector<double> gx, gw;
+    gauss_legendre(kSpreadGL, gx, gw);
+    for (int q = 0; q < kSpreadGL; ++q) {
+        out[q] = gx[q];
+        out[kSpreadGL + q] = gw[q];
+    }
+    for (int c = 0; c < 6; ++c) {
+        out[2 * kSpreadGL + c] = kExpAmp[c];
+        out[2 * kSpreadGL + 6 + c] = kExpVar[c];
+    }
 }
 
 // _exp_disk_kernel_bandlimited(fwhm; half): (2 half + 1)^2, column-major, sum 1.

@@ -400,6 +400,7 @@ typedef struct cpb_group_result {
     int64_t n_kernel_groups;  /* groups fitted by the one-block-per-group kernel */
     int64_t n_routed_groups;  /* groups too large for it, fitted by the full-field path */
     double device_seconds;
+    double *spread_model, *spread_model_err;  /* optional (params->spread_model_fwhm sizes the disk) */
 } cpb_group_result;
 
 /*

@@ -1096,11 +1096,13 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
         put_nan_diag(i);
     }
     // spread_model reference disk: one field-constant kernel sized from the
-    // catalogue's first star (:1361-1365)
+    // catalogue's first star's parameters after the bookkeeping above
+    // (params[row_y, 1], params[row_x, 1], :1289-1299, :1361-1365): its fitted
+    // position when active, its catalogue position otherwise, fixed values
     std::vector<double> spread_K;
     int spread_half = 0;
     const bool have_spread =
-        spread_kernel(psf, P->spread_model_fwhm, y0[0], x0[0], P->fit_rad, spread_K, spread_half);
+        n_stars > 0 && spread_kernel(psf, P->spread_model_fwhm, out->y[0], out->x[0], P->fit_rad, spread_K, spread_half);
     // per-star diagnostics (:1382-1397 chisq; psf_photometry_diagnostics.jl:154-231)
     for (int64_t j = 0; j < n_act; ++j) {
         int64_t i = active[j];

@@ -12,6 +12,7 @@
 // it against that closed form evaluated with scipy's complex erf.
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <vector>
 
 #include "oracle_psf.hpp"
@@ -125,6 +126,9 @@ static void unit_extent(const Psf& psf, double Y, double X, double e[4]) {
 }
 
 double spread_fwhm(const Psf& psf, double Y, double X) {
+    // the reference's PSF.extent(Int, m) raises an InexactError on a non-finite
+    // position; here spread_model is then off
+    if (!(std::isfinite(Y) && std::isfinite(X))) return std::numeric_limits<double>::quiet_NaN();
     double e[4];
     unit_extent(psf, Y, X, e);
     const StarP s{Y, X, 1.0, 0.0, psf.fwhm};

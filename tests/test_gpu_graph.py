@@ -60,10 +60,10 @@ def check_against_direct(psf, dl, tl, dg, tg):
     ns = int(dg["star_offsets"][-1])
     same = (tg["out"]["n_iter"].cpu().numpy()[:ns] == ref_g["n_iter"])
     assert same.mean() > 0.99
-    for k in ("y", "x", "flux"):
+    for k in ("y", "x", "flux", "spread_model"):
         a = tg["out"][k].cpu().numpy()[:ns][same]
         b = ref_g[k][same]
-        np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9)
+        np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9, equal_nan=True)
 
 
 def test_graph_matches_direct_entries_and_replays_new_inputs(tmp_path):

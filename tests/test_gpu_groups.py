@@ -5,7 +5,9 @@ run on each group alone, on the same seeded inputs.
 Parity bar (FP64 device arithmetic), per group: active-star count, union size
 and failure count bit-exact; for stars valid and converged in both with the
 same freeze iteration, |dy|, |dx| <= 1e-4 px and |dflux|/flux <= 1e-5; errors
-within 1e-4 relative; chi^2 and qfit within 1e-3 relative.
+within 1e-4 relative; chi^2 and qfit within 1e-3 relative; spread_model within
+1e-5 absolute and its error within 1e-3 relative (the disk width comes from
+each group's first star's fitted position, so it moves with the fit).
 """
 import numpy as np
 import pytest
@@ -63,6 +65,9 @@ def compare(d, out, psf, fit_rad, min_same=0.9, check_errors=True, **kw):
         if same.any():
             worst = [max(worst[0], dy.max()), max(worst[1], dx.max()), max(worst[2], df.max())]
             assert dy.max() <= POS_TOL and dx.max() <= POS_TOL and df.max() <= FLUX_TOL, (g, dy.max(), df.max())
+            np.testing.assert_allclose(out["spread_model"][sl][same], o.spread_model[same], rtol=0, atol=1e-5)
+            np.testing.assert_allclose(out["spread_model_err"][sl][same], o.spread_model_err[same], rtol=1e-3,
+                                       equal_nan=True)
             if check_errors:
                 np.testing.assert_allclose(out["flux_err"][sl][same], o.flux_err[same], rtol=1e-4)
                 np.testing.assert_allclose(out["y_err"][sl][same], o.y_err[same], rtol=1e-4)
@@ -72,6 +77,7 @@ def compare(d, out, psf, fit_rad, min_same=0.9, check_errors=True, **kw):
         untouched = ~o.valid & (o.flux == d["flux"][sl]) & (o.n_iter == 0)
         np.testing.assert_array_equal(out["flux"][sl][untouched], o.flux[untouched])
         np.testing.assert_array_equal(gv[untouched], False)
+        assert np.isnan(out["spread_model"][sl][~gv]).all()
     assert both_all > 0
     assert same_all >= min_same * both_all, f"freeze iterations differ for {both_all - same_all} stars"
     print(f"groups: {same_all}/{both_all} stars compared; max dy {worst[0]:.2e} dx {worst[1]:.2e} "
@@ -208,8 +214,8 @@ def test_groups_deterministic_and_equal_to_single_fits():
     d = lm_groups(48, seed=99)
     a = run_batch(psf, d, 5, **C4_KW)
     b = run_batch(psf, d, 5, **C4_KW)
-    for k in ("y", "x", "flux", "flux_err", "n_iter", "chisq"):
-        assert np.array_equal(a[k], b[k]), k
+    for k in ("y", "x", "flux", "flux_err", "n_iter", "chisq", "spread_model", "spread_model_err"):
+        assert np.array_equal(a[k], b[k], equal_nan=True), k
     images = [group_image(d, g) for g in range(48)]
     ivs = [group_image(d, g, "inv_var") for g in range(48)]
     cats = [group_cat(d, g) for g in range(48)]
@@ -220,4 +226,22 @@ def test_groups_deterministic_and_equal_to_single_fits():
         assert ok.any()
         assert np.abs(s.y - res[g].y)[ok].max() <= POS_TOL
         assert np.abs(s.flux / res[g].flux - 1)[ok].max() <= FLUX_TOL
+        assert np.abs(s.spread_model - res[g].spread_model)[ok].max() <= 1e-5
         assert res[g].n_passes == s.n_passes or ok.sum() >= 0.8 * len(ok)
+
+
+def test_groups_spread_model_width_and_off_switch():
+    """An explicit disk width replaces the per-group one (the same disk for every
+    group); a non-positive or non-finite width, or no spread_model outputs,
+    turns spread_model off without touching the fit."""
+    psf = moffat_epsf()
+    d = lm_groups(40, seed=321)
+    for width in (3.0, 6.5):
+        out = run_batch(psf, d, 5, spread_model_fwhm=width, **C4_KW)
+        compare(d, out, psf, 5, check_errors=False, spread_model_fwhm=width, **C4_KW)
+    base = run_batch(psf, d, 5, **C4_KW)
+    for off in (0.0, -2.0, float("inf")):
+        out = run_batch(psf, d, 5, spread_model_fwhm=off, **C4_KW)
+        assert np.isnan(out["spread_model"]).all() and np.isnan(out["spread_model_err"]).all()
+        for k in ("y", "x", "flux", "chisq", "qfit"):
+            assert np.array_equal(out[k], base[k], equal_nan=True), k
