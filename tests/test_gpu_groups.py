@@ -245,3 +245,32 @@ def test_groups_spread_model_width_and_off_switch():
         assert np.isnan(out["spread_model"]).all() and np.isnan(out["spread_model_err"]).all()
         for k in ("y", "x", "flux", "chisq", "qfit"):
             assert np.array_equal(out[k], base[k], equal_nan=True), k
+
+
+def test_groups_disk_width_from_each_groups_first_star():
+    """Each group's disk is sized from its own first star's fitted position
+    (psf_photometry_simultaneous.jl:1363-1364): the batch equals, per group, a run
+    given that width explicitly (computed on the host by the oracle's
+    _spread_fwhm); the single-field path does the same."""
+    from oracle import orc_spread_fwhm
+    psf = moffat_epsf()
+    d = lm_groups(12, seed=4242)
+    out = run_batch(psf, d, 5, **C4_KW)
+    for g in range(12):
+        s0, s1 = int(d["star_offsets"][g]), int(d["star_offsets"][g + 1])
+        if not out["valid"][s0:s1].any():
+            continue
+        f = orc_spread_fwhm(psf, out["y"][s0], out["x"][s0])
+        sub = dict(pix=group_image(d, g).ravel(order="F"), inv_var=group_image(d, g, "inv_var").ravel(order="F"),
+                   offsets=np.array([0]), ny=d["ny"][g:g + 1], nx=d["nx"][g:g + 1],
+                   star_offsets=np.array([0, s1 - s0]), y=d["y"][s0:s1], x=d["x"][s0:s1], flux=d["flux"][s0:s1])
+        ex = run_batch(psf, sub, 5, spread_model_fwhm=f, **C4_KW)
+        np.testing.assert_allclose(ex["spread_model"], out["spread_model"][s0:s1], rtol=0, atol=1e-12,
+                                   equal_nan=True)
+        single = cpb.fit_all_stars_simultaneous(group_image(d, g), psf, group_cat(d, g), 5,
+                                                inv_var=group_image(d, g, "inv_var"), **C4_KW)
+        f1 = orc_spread_fwhm(psf, single.y[0], single.x[0])
+        single_ex = cpb.fit_all_stars_simultaneous(group_image(d, g), psf, group_cat(d, g), 5,
+                                                   inv_var=group_image(d, g, "inv_var"), spread_model_fwhm=f1,
+                                                   **C4_KW)
+        np.testing.assert_allclose(single_ex.spread_model, single.spread_model, rtol=0, atol=1e-12, equal_nan=True)

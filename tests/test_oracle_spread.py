@@ -156,3 +156,29 @@ def test_simultaneous_matches_sequential():
     assert rseq.spread_model[3] > 5e-3 and rsim.spread_model[3] > 5e-3
     a, b = rseq.spread_model[3], rsim.spread_model[3]
     assert abs(a - b) <= 0.25 * max(abs(a), abs(b))
+
+
+def test_simultaneous_disk_width_from_the_fitted_first_star():
+    """fit_all_stars_simultaneous sizes the disk after the final bookkeeping, from
+    params[row_y, 1], params[row_x, 1] (psf_photometry_simultaneous.jl:1289-1299,
+    :1363-1364): the first star's fitted position, not its catalogue one (the
+    sequential fit_all_stars takes the catalogue one, psf_photometry_single.jl:324-325)."""
+    img = _img((60, 60), 30.4, 29.7, 3.0, 5000.0) - 20.0
+    iv = np.full(img.shape, 1 / 20.0)
+    cat = dict(y=np.array([30.9]), x=np.array([29.2]), flux=np.array([4000.0]))
+    kw = dict(fixed={"fwhm": FW, "bkg": 0.0}, max_iter=40, inv_var=iv)
+    auto = orc_fit_simultaneous(img, PSF, cat, 7, **kw)
+    assert auto.valid[0] and abs(auto.y[0] - 30.4) < 0.05
+    f_fit = orc_spread_fwhm(PSF, auto.y[0], auto.x[0])
+    f_cat = orc_spread_fwhm(PSF, 30.9, 29.2)
+    assert f_fit != f_cat
+    assert orc_fit_simultaneous(img, PSF, cat, 7, spread_model_fwhm=f_fit, **kw).spread_model[0] == \
+        auto.spread_model[0]
+    assert orc_fit_simultaneous(img, PSF, cat, 7, spread_model_fwhm=f_cat, **kw).spread_model[0] != \
+        auto.spread_model[0]
+    # a fixed position is the position (the bookkeeping writes the fixed value)
+    fx = orc_fit_simultaneous(img, PSF, cat, 7, **dict(kw, fixed={"fwhm": FW, "bkg": 0.0, "y": 30.4}))
+    f_fx = orc_spread_fwhm(PSF, 30.4, fx.x[0])
+    assert orc_fit_simultaneous(img, PSF, cat, 7, spread_model_fwhm=f_fx,
+                                **dict(kw, fixed={"fwhm": FW, "bkg": 0.0, "y": 30.4})).spread_model[0] == \
+        fx.spread_model[0]
