@@ -1183,10 +1183,10 @@ __global__ void k_errors(int64_t n_act, int p, const double* gram, bool reweight
 // The spread_model disk of the simultaneous fit, one block.  Its width comes
 // from the first catalogue star's parameters after the final bookkeeping
 // (params[row_y, 1], params[row_x, 1], :1289-1299 and :1363-1364): the fitted
-// position when that star is active (then it is active star 0, the active list
-// being in catalogue order), its catalogue position when not, the fixed value
-// of a fixed coordinate.  ky / kx: their rows in theta, -1 when fixed.  Dynamic
-// shared memory: the quadrature panel, (7 + kh) * 32 doubles.
+// position when that star is active (the block finds its slot in the
+// Morton-ordered active list), its catalogue position when not, the fixed
+// value of a fixed coordinate.  ky / kx: their rows in theta, -1 when fixed.
+// Dynamic shared memory: the quadrature panel, (7 + kh) * 32 doubles.
 __global__ void __launch_bounds__(256) k_spread_disk(DevPsf P, double param, int kh,
                                                      const double* __restrict__ theta,
                                                      const int32_t* __restrict__ act, int64_t n_act, int p, int ky,
@@ -1195,9 +1195,15 @@ __global__ void __launch_bounds__(256) k_spread_disk(DevPsf P, double param, int
                                                      const double* __restrict__ rule, double* tab) {
     extern __shared__ double pan[];
     __shared__ double red[2 * 8 + 1];
-    const bool first_active = n_act > 0 && act[0] == 0;
-    const double Y = ky < 0 ? fixed_y : (first_active ? theta[ky] : y0[0]);
-    const double X = kx < 0 ? fixed_x : (first_active ? theta[kx] : x0[0]);
+    __shared__ int64_t slot;
+    if (threadIdx.x == 0) slot = -1;
+    __syncthreads();
+    for (int64_t j = threadIdx.x; j < n_act; j += blockDim.x)
+        if (act[j] == 0) slot = j;  // catalogue indices are unique: one writer at most
+    __syncthreads();
+    const int64_t j0 = slot;
+    const double Y = ky < 0 ? fixed_y : (j0 >= 0 ? theta[j0 * p + ky] : y0[0]);
+    const double X = kx < 0 ? fixed_x : (j0 >= 0 ? theta[j0 * p + kx] : x0[0]);
     spread_disk_block(P, param, kh, Y, X, rule, tab, red, pan);
 }
 
