@@ -46,13 +46,16 @@ __device__ __forceinline__ double block_max(double v, double* sh) {
 }
 
 // Grid-wide sum (or max when IS_MAX).  Returns true in every thread of the
-// last block, where *total holds the grid result (also in sh_total[0]).
+// last block, where *total holds the grid result (also in sh_total[0]).  The
+// block's partial goes to slot `slot` (default: blockIdx.x); the partials are
+// summed in slot order, so blocks that work on permuted units keep the sum's
+// order by passing their unit's index.
 template <int NT, bool IS_MAX = false>
-__device__ __forceinline__ bool grid_reduce(double v, Reducer red, double* sh, double* result) {
+__device__ __forceinline__ bool grid_reduce(double v, Reducer red, double* sh, double* result, int slot = -1) {
     double b = IS_MAX ? block_max<NT>(v, sh) : block_sum<NT>(v, sh);
     __shared__ bool is_last;
     if (threadIdx.x == 0) {
-        red.partials[blockIdx.x] = b;
+        red.partials[slot < 0 ? blockIdx.x : (unsigned)slot] = b;
         __threadfence();
         unsigned prev = atomicAdd(red.counter, 1u);
         is_last = (prev == gridDim.x - 1);

@@ -206,6 +206,14 @@ __global__ void k_tile_bounds(int64_t npairs, const uint32_t* keys, int32_t* sta
     if (i == npairs - 1 || keys[i + 1] != k) end[k] = (int32_t)(i + 1);
 }
 
+// Sort keys of the regions by work: the number of (region, star) pairs.
+__global__ void k_tile_work(int64_t ntiles, const int32_t* start, const int32_t* end, uint32_t* key, int32_t* idx) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    key[t] = (uint32_t)(end[t] - start[t]);
+    idx[t] = (int32_t)t;
+}
+
 __global__ void k_tile_pack(int64_t npairs, const int32_t* sorted_j, const int32_t* ay, const int32_t* ax,
                             const int32_t* Rs, int Rconst, int4* packed) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -692,6 +700,7 @@ constexpr int MODE_LSQR = 4;
 template <int KIND, int MODE, typename TS>
 __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
+                                               const int32_t* __restrict__ tord,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
                                                int Rbox, int64_t stride, const int64_t* __restrict__ soff,
                                                const double* __restrict__ vt,
@@ -716,7 +725,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         uscale = u_sign * sc->inv_beta;
     }
     const int p = KIND == KIND_JV ? fc.p : 1;
-    const int reg = blockIdx.x;
+    const int reg = tord[blockIdx.x];
     const int ry = reg % fc.nty, rx = reg / fc.nty;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int y0 = ry * TY + 1, xs0 = rx * TX + wid * SW + 1;
@@ -834,7 +843,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
     }
     if (MODE == MODE_LSQR) {
         double tot;
-        if (grid_reduce<NT>(part, red, sh, &tot) && threadIdx.x == 0) {
+        if (grid_reduce<NT>(part, red, sh, &tot, reg) && threadIdx.x == 0) {
             const double beta = sqrt(tot);
             sc->beta = beta;
             if (beta != 0.0) {
@@ -844,7 +853,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             }
         }
     } else if (MODE == MODE_CUR || MODE == MODE_CAND) {
-        grid_reduce<NT>(part, red, sh, result);
+        grid_reduce<NT>(part, red, sh, result, reg);
     }
 }
 
@@ -1367,7 +1376,8 @@ void launch_k_eval(int64_t S2, unsigned grid, size_t smem, cudaStream_t st, A...
 
 struct TileLists {
     int32_t *start = nullptr, *end = nullptr;
-    int4* list = nullptr;  // (star, anchor y, anchor x, box radius) per (tile, star) pair
+    int4* list = nullptr;     // (star, anchor y, anchor x, box radius) per (tile, star) pair
+    int32_t* order = nullptr; // the regions by decreasing star count: block b of a gather takes order[b]
 };
 
 TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_t* ay, const int32_t* ax,
@@ -1395,6 +1405,7 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
     const int64_t ntiles = (int64_t)nty * ntx;
     tl.start = S<int32_t>(ctx, (t + "_start").c_str(), ntiles);
     tl.end = S<int32_t>(ctx, (t + "_end").c_str(), ntiles);
+    tl.order = S<int32_t>(ctx, (t + "_order").c_str(), ntiles);
     check(cudaMemsetAsync(tl.start, 0, sizeof(int32_t) * ntiles, st), "memset");
     check(cudaMemsetAsync(tl.end, 0, sizeof(int32_t) * ntiles, st), "memset");
     if (npairs > 0) {
@@ -1411,6 +1422,18 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
         k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_j, ay, ax, Rs, Rconst, tl.list);
         check(cudaGetLastError(), "k_tile_pack");
     }
+    // heaviest regions first, so that the last wave of a gather is its lightest
+    // (the radix sort is stable: equal counts keep region order)
+    uint32_t* wkey = S<uint32_t>(ctx, (t + "_wkey").c_str(), 2 * ntiles);
+    int32_t* widx = S<int32_t>(ctx, (t + "_widx").c_str(), ntiles);
+    k_tile_work<<<nblk(ntiles), 256, 0, st>>>(ntiles, tl.start, tl.end, wkey, widx);
+    check(cudaGetLastError(), "k_tile_work");
+    tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, wkey, wkey + ntiles, widx, tl.order, (int)ntiles, 0, 32,
+                                              st);
+    dtmp = scratch(ctx, (t + "_wsort_tmp").c_str(), tmp);
+    cub::DeviceRadixSort::SortPairsDescending(dtmp, tmp, wkey, wkey + ntiles, widx, tl.order, (int)ntiles, 0, 32, st);
+    check(cudaGetLastError(), "region order");
     return tl;
 }
 
@@ -1804,16 +1827,16 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                         (double)npix * px_bytes + (double)nlist * Sm * Sm * bts);
         switch (mode) {
             case MODE_CUR:
-                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_CAND:
-                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             case MODE_FREEZE:
-                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
                 break;
             default:
-                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
+                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
         }
         check(cudaGetLastError(), "k_gather");
     };
@@ -1903,7 +1926,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
                         KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * 8);
-                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, live, V, fc.R, fc.VS, nullptr, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
+                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, tfit.order, live, V, fc.R, fc.VS, nullptr, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
                     }
                     {
                         KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
@@ -2038,7 +2061,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
             check(cudaGetLastError(), "k_eval_model");
         }
         KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
-        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
+        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
     // spread_model reference disk, on the device: its width comes from the first
