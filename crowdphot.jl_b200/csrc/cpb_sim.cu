@@ -590,31 +590,47 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 }
             }
         } else {
+            // one evaluation a stamp entry: the weighted derivatives go to V
+            // unscaled (and the model value to M) while the column norms
+            // accumulate; a second sweep over the star's block, still in L2,
+            // applies the inverse norms
             double acc[6] = {0, 0, 0, 0, 0, 0};
+            T* Vj = gram ? nullptr : V + (int64_t)j * fc.VS;
             int row = lane % Sb, col = lane / Sb;
             for (int m = lane; m < S2b; m += 32) {
                 const int gy = oy + row, gx = ox + col;
-                if (gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx) {
-                    const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
-                    if (w[q] > 0) {
-                        T val, a, b, c;
-                        eval_px(row, col, val, a, b, c);
+                const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
+                const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
+                const bool use = onimg && w[q] > 0;
+                T r0 = 0, r1 = 0, r2 = 0;
+                if (use || (M && !gram)) {
+                    T val, a, b, c;
+                    eval_px(row, col, val, a, b, c);
+                    if (M && !gram) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
+                    if (use) {
                         const T sq = (T)sw[q];
-                        const double r0 = sq * a, r1 = p > 1 ? (double)(sq * b) : 0.0,
-                                     r2 = p > 2 ? (double)(sq * c) : 0.0;
+                        r0 = sq * a;
+                        r1 = sq * b;
+                        r2 = sq * c;
+                        const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
                         if (gram) {
-                            acc[0] += r0 * r0;
-                            acc[1] += r0 * r1;
-                            acc[2] += r0 * r2;
-                            acc[3] += r1 * r1;
-                            acc[4] += r1 * r2;
-                            acc[5] += r2 * r2;
+                            acc[0] += d0 * d0;
+                            acc[1] += d0 * d1;
+                            acc[2] += d0 * d2;
+                            acc[3] += d1 * d1;
+                            acc[4] += d1 * d2;
+                            acc[5] += d2 * d2;
                         } else {
-                            acc[0] += r0 * r0;
-                            acc[1] += r1 * r1;
-                            acc[2] += r2 * r2;
+                            acc[0] += d0 * d0;
+                            acc[1] += d1 * d1;
+                            acc[2] += d2 * d2;
                         }
                     }
+                }
+                if (!gram) {
+                    Vj[m * p] = r0;
+                    if (p > 1) Vj[m * p + 1] = r1;
+                    if (p > 2) Vj[m * p + 2] = r2;
                 }
                 row += r32;
                 col += q32;
@@ -646,35 +662,10 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     inv[k] = (T)(1.0 / cn);
                     if (lane == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
                 }
-                T* Vj = V + (int64_t)j * fc.VS;
-                row = lane % Sb;
-                col = lane / Sb;
-                for (int m = lane; m < S2b; m += 32) {
-                    const int gy = oy + row, gx = ox + col;
-                    T r0 = 0, r1 = 0, r2 = 0;
-                    const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
-                    const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
-                    const bool use = onimg && w[q] > 0;
-                    if (use || M) {
-                        T val, a, b, c;
-                        eval_px(row, col, val, a, b, c);
-                        if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
-                        if (use) {
-                            const T sq = (T)sw[q];
-                            r0 = sq * a;
-                            r1 = sq * b;
-                            r2 = sq * c;
-                        }
-                    }
-                    Vj[m * p] = r0 * inv[0];
-                    if (p > 1) Vj[m * p + 1] = r1 * inv[1];
-                    if (p > 2) Vj[m * p + 2] = r2 * inv[2];
-                    row += r32;
-                    col += q32;
-                    if (row >= Sb) {
-                        row -= Sb;
-                        col += 1;
-                    }
+                for (int m = lane; m < S2b; m += 32) {  // the entries this lane wrote above
+                    Vj[m * p] *= inv[0];
+                    if (p > 1) Vj[m * p + 1] *= inv[1];
+                    if (p > 2) Vj[m * p + 2] *= inv[2];
                 }
             }
         }
