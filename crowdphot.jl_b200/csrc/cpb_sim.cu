@@ -752,52 +752,74 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         }
         __syncthreads();
         if (xs0 <= fc.nx) {
-            for (int e = 0; e < total; ++e) {
-                const int ax_ = s_ax[e], ay_ = s_ay[e];
-                // model renders: each star's own model radius; J v: the fit box
-                const int Rb = KIND == KIND_M ? s_rb[e] : Rbox;
-                const int Sb = 2 * Rb + 1;
-                const int c_lo = max(ax_ - Rb, xs0), c_hi = min(ax_ + Rb, xend);
-                const int r_lo = max(ay_ - Rb, y0), r_hi = min(ay_ + Rb, yend);
-                if (c_lo > c_hi || r_lo > r_hi) continue;  // warp-uniform
-                const int nrows = r_hi - r_lo + 1;
-                const int tot = nrows * (c_hi - c_lo + 1);
-                const float inv_nrows = 1.0f / (float)nrows;
-                const TS* base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride);
-                const int m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
-                const int a0 = (r_lo - y0) + (c_lo - xs0) * TY;
-                double wv0 = 1.0, wv1 = 0.0, wv2 = 0.0;
-                if (KIND == KIND_JV) {
-                    wv0 = s_v[0][e];
-                    if (p > 1) wv1 = s_v[1][e];
-                    if (p > 2) wv2 = s_v[2][e];
+            // The warp walks its stars' entries in 32-entry slots (a slot holds
+            // one star's entries, a star's last slot is padded) and takes four
+            // slots a round -- up to four stars -- loading all of them before
+            // adding any; slots are added in order, so every pixel still sums
+            // its stars in list order, and one add instruction never holds two
+            // stars (no lost updates between lanes).
+            int e = 0, c = 0;  // current star and slot
+            int tot = 0, nrows = 1, m0 = 0, a0 = 0, Sb = 1;
+            float inv_nrows = 1.0f;
+            const TS* base = src;
+            auto seek = [&](int from) {  // the next star meeting the strip, from `from`
+                c = 0;
+                for (e = from; e < total; ++e) {
+                    const int ax_ = s_ax[e], ay_ = s_ay[e];
+                    // model renders: each star's own model radius; J v: the fit box
+                    const int Rb = KIND == KIND_M ? s_rb[e] : Rbox;
+                    Sb = 2 * Rb + 1;
+                    const int c_lo = max(ax_ - Rb, xs0), c_hi = min(ax_ + Rb, xend);
+                    const int r_lo = max(ay_ - Rb, y0), r_hi = min(ay_ + Rb, yend);
+                    if (c_lo > c_hi || r_lo > r_hi) continue;  // warp-uniform
+                    nrows = r_hi - r_lo + 1;
+                    tot = nrows * (c_hi - c_lo + 1);
+                    inv_nrows = 1.0f / (float)nrows;
+                    m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
+                    a0 = (r_lo - y0) + (c_lo - xs0) * TY;
+                    base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride);
+                    return;
                 }
-                for (int t0 = 0; t0 < tot; t0 += 128) {
-                    double val[4];
-                    int dst[4];
+            };
+            seek(0);
+            while (e < total) {
+                TS raw[4][3];
+                int dst[4], eq[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int t = t0 + lane + 32 * q;
-                        dst[q] = -1;
-                        val[q] = 0.0;
+                for (int q = 0; q < 4; ++q) {
+                    dst[q] = -1;
+                    eq[q] = e;
+                    raw[q][0] = raw[q][1] = raw[q][2] = (TS)0;
+                    if (e < total) {
+                        const int t = c * 32 + lane;
                         if (t < tot) {
                             const int cc = (int)(((float)t + 0.5f) * inv_nrows);
                             const int rr = t - cc * nrows;
                             const TS* ptr = base + (int64_t)(m0 + rr + cc * Sb) * p;
+                            raw[q][0] = __ldg(ptr);
                             if (KIND == KIND_JV) {
-                                double v = (double)__ldg(ptr) * wv0;
-                                if (p > 1) v += (double)__ldg(ptr + 1) * wv1;
-                                if (p > 2) v += (double)__ldg(ptr + 2) * wv2;
-                                val[q] = v;
-                            } else {
-                                val[q] = (double)__ldg(ptr);
+                                if (p > 1) raw[q][1] = __ldg(ptr + 1);
+                                if (p > 2) raw[q][2] = __ldg(ptr + 2);
                             }
                             dst[q] = a0 + rr + cc * TY;
                         }
+                        if ((c + 1) * 32 < tot) ++c;
+                        else seek(e + 1);
                     }
+                }
 #pragma unroll
-                    for (int q = 0; q < 4; ++q)
-                        if (dst[q] >= 0) acc[dst[q]] += val[q];
+                for (int q = 0; q < 4; ++q) {
+                    if (dst[q] >= 0) {
+                        double v;
+                        if (KIND == KIND_JV) {
+                            v = (double)raw[q][0] * s_v[0][eq[q]];
+                            if (p > 1) v += (double)raw[q][1] * s_v[1][eq[q]];
+                            if (p > 2) v += (double)raw[q][2] * s_v[2][eq[q]];
+                        } else {
+                            v = (double)raw[q][0];
+                        }
+                        acc[dst[q]] += v;
+                    }
                 }
                 __syncwarp();
             }
