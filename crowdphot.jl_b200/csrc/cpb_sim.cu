@@ -687,6 +687,10 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // :686-693); freeze subtraction (_freeze_star!, :739-754); final residual.
 constexpr int KIND_JV = 0, KIND_M = 1;
 constexpr int MODE_LSQR = 4;
+// 32-entry slots a warp loads per round: 4 measured fastest on the 2048^2 fit
+// (J.v 47.0 ms per fit; 6 slots 58.5 ms and 8 slots 65.1 ms, their registers
+// costing more resident warps than the extra loads in flight gain)
+constexpr int KSLOT = 4;
 
 template <int KIND, int MODE, typename TS>
 __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
@@ -783,10 +787,10 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             };
             seek(0);
             while (e < total) {
-                TS raw[4][3];
-                int dst[4], eq[4];
+                TS raw[KSLOT][3];
+                int dst[KSLOT], eq[KSLOT];
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < KSLOT; ++q) {
                     dst[q] = -1;
                     eq[q] = e;
                     raw[q][0] = raw[q][1] = raw[q][2] = (TS)0;
@@ -808,7 +812,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                     }
                 }
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
+                for (int q = 0; q < KSLOT; ++q) {
                     if (dst[q] >= 0) {
                         double v;
                         if (KIND == KIND_JV) {
