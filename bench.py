@@ -40,10 +40,10 @@ N_STARS = 50_000
 FIT_RAD = 12
 SEED = 1002
 SAMPLE = 512  # CPU sample side (same star density)
-# DRAM bytes moved per algorithmic byte by the J v gather (read + write 230.3 MB against
+# DRAM bytes moved per algorithmic byte by the J v gather (read + write 226.9 MB against
 # 204.6 MB algorithmic), from an ncu capture of the same kernel on a 1024^2 field with
 # the same star density, PSF and radii (its first LSQR launch, every star live)
-JV_TRAFFIC_RATIO = 230.3 / 204.6
+JV_TRAFFIC_RATIO = 226.9 / 204.6
 
 
 def workload_config(ny=NY, nx=NX, n=N_STARS):
@@ -307,7 +307,7 @@ def run_gpu(args):
     if top[0] == "k_gather_Jv":
         roof["traffic"] = JV_TRAFFIC_RATIO * top[1]["bytes"] / max(top[1]["launches"], 1)
         roof["traffic_note"] = ("bytes per launch: this run's algorithmic bytes per launch times the DRAM / "
-                                "algorithmic ratio of an ncu capture of the kernel on a 1024^2 field (1.126)")
+                                "algorithmic ratio of an ncu capture of the kernel on a 1024^2 field (1.109)")
     kernels = {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
                    "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst.items())}
 
