@@ -34,7 +34,7 @@ sys.path[:0] = [ROOT, os.path.join(ROOT, "crowdphot.jl_b200")]
 
 import numpy as np  # noqa: E402
 
-METRIC = "fitted stars/s on 1 B200 (served+mixed vs plain, flux err<=1e-5); p50/p99 ms"
+METRIC = "fitted stars/s on 1 B200 (served+mixed vs plain, flux err\u22641e-5); p50/p99 ms"
 NY = NX = 2048
 N_STARS = 50_000
 FIT_RAD = 12
