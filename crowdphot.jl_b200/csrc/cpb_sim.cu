@@ -690,11 +690,12 @@ constexpr int MODE_LSQR = 4;
 // 32-entry slots a warp loads per round: 4 measured fastest on the 2048^2 fit
 // (J.v 47.0 ms per fit; 3 slots 46.6 ms, 6 slots 58.5 ms and 8 slots 65.1 ms,
 // their registers costing more resident warps than the extra loads in flight
-// gain); J.v is held to 64 registers (8 blocks an SM: 45.7 ms)
+// gain); J.v alone is held to 64 registers (8 blocks an SM: 45.7 ms), the
+// model gathers keep the compiler's choice
 constexpr int KSLOT = 4;
 
 template <int KIND, int MODE, typename TS>
-__global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 1) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
+__global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
                                                const int32_t* __restrict__ tord,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
