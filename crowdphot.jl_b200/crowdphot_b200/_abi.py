@@ -106,7 +106,7 @@ class SimParams(C.Structure):
         ("precision", C.c_int32),
         ("solver", C.c_int32),
         ("damping", C.c_int32),
-        ("reserved", C.c_int32),
+        ("refine_iters", C.c_int32),
         ("spread_model_fwhm", C.c_double),
     ]
 

@@ -274,8 +274,13 @@ def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_itera
                model_rad="auto", model_rad_max=None, model_rad_nsigma=1.0, max_step=0.25, max_trials=8, max_iter=40,
                x_tol=1.0e-5, f_tol=1.0e-4, g_tol=1.0e-4, lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0,
                lambda_min=1.0e-12, lambda_max=1.0e12, damping="marquardt", covariance_estimator=None,
-               precision="fp64", spread_model_fwhm=None):
-    """Keyword arguments -> cpb_sim_params (shared by the device path and the oracle)."""
+               precision="fp64", spread_model_fwhm=None, refine_iters=0):
+    """Keyword arguments -> cpb_sim_params (shared by the device path and the oracle).
+
+    refine_iters (precision="mixed" only): FP64 Gauss-Newton iterations after the
+    FP32-stamp loop, every active star live again from the mixed-precision
+    parameters; 0 keeps the mixed-precision parameters and re-evaluates only the
+    errors, residual and diagnostics in FP64."""
     P = _abi.SimParams()
     P.spread_model_fwhm = spread_fwhm_arg(spread_model_fwhm)
     P.fit_rad = float(fit_rad)
@@ -305,6 +310,9 @@ def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_itera
     P.lambda_init, P.lambda_up, P.lambda_down = float(lambda_init), float(lambda_up), float(lambda_down)
     P.lambda_min, P.lambda_max = float(lambda_min), float(lambda_max)
     P.precision = _PREC[precision]
+    if int(refine_iters) < 0:
+        raise ArgumentError("refine_iters must be >= 0")
+    P.refine_iters = int(refine_iters)
     if solver not in ("lsqr", "lsmr"):
         raise ArgumentError(f"solver must be :lsqr or :lsmr, got :{solver}")
     P.solver = _abi.CPB_SOLVER_LSQR if solver == "lsqr" else _abi.CPB_SOLVER_LSMR
@@ -394,7 +402,7 @@ def fit_all_stars_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_
                                max_trials=8, max_iter=40, x_tol=1.0e-5, f_tol=1.0e-4, g_tol=1.0e-4,
                                lambda_init=1.0e-4, lambda_up=10.0, lambda_down=10.0, lambda_min=1.0e-12,
                                lambda_max=1.0e12, damping="marquardt", show_trace=False, covariance_estimator=None,
-                               precision="fp64", ctx: Context | None = None, debug=False,
+                               precision="fp64", refine_iters=0, ctx: Context | None = None, debug=False,
                                residual=True) -> MultiPassPhotResult:
     """CrowdPhot.fit_all_stars_simultaneous on the B200 (psf_photometry_simultaneous.jl:953-1431)."""
     fixed = dict(fixed or {})
@@ -407,7 +415,7 @@ def fit_all_stars_simultaneous(image, psf, sources, fit_rad, *, fixed=None, inv_
                    max_trials=max_trials, max_iter=max_iter, x_tol=x_tol, f_tol=f_tol, g_tol=g_tol,
                    lambda_init=lambda_init, lambda_up=lambda_up, lambda_down=lambda_down, lambda_min=lambda_min,
                    lambda_max=lambda_max, damping=damping, covariance_estimator=covariance_estimator,
-                   precision=precision, spread_model_fwhm=spread_model_fwhm)
+                   precision=precision, spread_model_fwhm=spread_model_fwhm, refine_iters=refine_iters)
     ny, nx = imgf.shape
     R = int(np.ceil(fit_rad)) if fit_rad > 0 else 0
     S2 = (2 * R + 1) ** 2

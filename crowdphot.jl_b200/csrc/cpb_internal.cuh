@@ -769,6 +769,12 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                          int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out);
 
+// Upper bound of the scratch bytes one simultaneous fit carves from a fixed
+// region (cpb_sim.cu), every catalogue star counted as active; with
+// model_rad = :auto the model stamps are counted at the fit box and checked
+// again inside the fit once the radii are known.
+size_t sim_scratch_bound(const cpb_sim_params* P, int64_t ny, int64_t nx, int64_t n, bool dbg_pixels);
+
 // model_rad = :auto (psf_photometry_simultaneous.jl:192-243), host side
 // (cpb_radii.cu): per-star model radii from the unit PSF's curve of growth and
 // the background noise of the weight sample.

@@ -1,10 +1,11 @@
 // cpb_noalloc.cu -- the simultaneous fit without any device allocation.
 //
-// Some callers cannot call cudaMalloc while they fit: code running between
-// the begin and end of a CUDA stream capture, hosts whose device memory is
-// owned by another allocator (a Julia CUDA.jl or PyTorch memory pool that must
-// not be bypassed), and latency-critical loops where an allocation's implicit
-// synchronisation is not acceptable.  For them
+// Some callers cannot call cudaMalloc while they fit: Julia hosts whose device
+// memory belongs to CUDA.jl's pool allocator (or a PyTorch process whose
+// memory belongs to its caching allocator), where a direct cudaMalloc behind
+// the pool's back can fail once the pool holds most of the GPU or fragment
+// what it holds, and latency-critical loops that cannot take the implicit
+// device synchronisation of cudaMalloc / cudaFree.  For them
 // cpb_fit_simultaneous_device_noalloc runs the same fit as
 // cpb_fit_simultaneous_device, but every scratch buffer (stamps, residuals,
 // LSQR vectors, tile lists, sort temporaries, reduction partials) is carved
@@ -14,7 +15,16 @@
 // Set-up: the array's device address is looked up once per device with
 // cudaGetSymbolAddress (in host code the symbol is only a host-side stand-in,
 // never a device address).  The first call of the entry point on a device
-// does that look-up, so it should come before any stream capture.
+// does that look-up, so it should come before any stream capture.  The
+// address is kept for the life of the process: after a cudaDeviceReset of that
+// device the module is loaded again and the kept address is stale, so do not
+// call this entry point after resetting a device it has used.
+//
+// Sizes: a field is refused with CPB_ERR_ARGUMENT ("too large for the
+// no-allocation entry point") when its scratch bound (sim_scratch_bound, every
+// catalogue star counted as active) exceeds the array; with model_rad = :auto
+// the model stamps are checked again once the per-star radii are known, before
+// the outer loop starts.
 //
 // Sharing: every call uses the same array and finds the previous call's
 // contents there; the fit clears everything that must start at zero.  Calls
@@ -54,28 +64,6 @@ void* noalloc_base(int device) {
     return g_scratch_addr[device];
 }
 
-// Upper bound of the scratch one fit carves (every catalogue star active).
-size_t noalloc_estimate(const cpb_sim_params* P, int64_t ny, int64_t nx, int64_t n, bool dbg_pixels) {
-    const int R = (int)std::ceil(P->fit_rad);
-    const int S = 2 * R + 1;
-    const int64_t S2 = (int64_t)S * S;
-    const int64_t p = 3;
-    const int64_t VS = (p * S2 + 15) / 16 * 16;
-    const int64_t npix = ny * nx;
-    const int64_t ntiles = ((ny + 31) / 32) * ((nx + 7) / 8);
-    const int64_t tiles_per_star = ((S + 31) / 32 + 1) * ((S + 7) / 8 + 1);
-    const int64_t npairs = n * tiles_per_star;
-    size_t b = 0;
-    b += npix * (8 * 7 + 1);                                   // data, data_work, w, sw, wt_resid, u, resid, umask
-    b += n * (4 * 5 + 1 + 8 * 3 + 4);                          // catalogue-order anchors, keys, selection
-    b += n * (4 * 2 + VS * 8 + p * 8 * 10 + 2 * sizeof(StarCoef) + 3 + 4 * 3 + 6 * 8 + 5 * 8);
-    b += 2 * (ntiles * 8 + npairs * 16 + n * 8);               // two tile lists
-    b += (std::max<int64_t>(ntiles, (std::max<int64_t>(3 * n, npix) + 255) / 256 + 1)) * 8;  // partials
-    if (dbg_pixels) b += S2 * n * 4;
-    b += 256 * 80 + (size_t(4) << 20);                         // alignment and sort / scan temporaries
-    return b;
-}
-
 }  // namespace
 
 void* arena_carve(cpb_ctx::Arena* a, const char* name, size_t bytes) {
@@ -110,7 +98,7 @@ extern "C" int cpb_fit_simultaneous_device_noalloc(cpb_ctx* ctx, const cpb_psf* 
         if (!psf || !params || !out || !d_image || (n > 0 && (!d_y0 || !d_x0 || !d_flux0)))
             throw ArgError{"null argument"};
         if (ny <= 0 || nx <= 0) throw ArgError{"image must be non-empty"};
-        const size_t need = noalloc_estimate(params, ny, nx, n, out->dbg_pixels != nullptr);
+        const size_t need = sim_scratch_bound(params, ny, nx, n, out->dbg_pixels != nullptr);
         if (need > kNoAllocScratchBytes)
             throw ArgError{"field too large for the no-allocation entry point: needs about " +
                            std::to_string((need + (1 << 20) - 1) >> 20) + " MiB of scratch, the static region holds " +

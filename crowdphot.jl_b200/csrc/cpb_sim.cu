@@ -5,8 +5,10 @@
 //   * per-pixel vectors (data, data_work, w, sqrt(w), union mask, residual,
 //     LSQR u) are column-major npix arrays, as in the reference;
 //   * stamp derivatives V are star-major: star j owns a contiguous block of
-//     VS >= p*S2 values in the reference's (k fastest, then stamp pixel m)
-//     order (StampDerivatives.values, :19-43), padded to 128 bytes;
+//     p planes (one per free parameter) of the unscaled weighted derivatives
+//     over its fit box (StampDerivatives.values, :19-43, times colnorm), each
+//     plane in the granule layout (gran_rows): box columns padded so that
+//     16-byte granules line up with image rows;
 //   * stamp pixel indices are not stored: they follow from the integer anchor
 //     and the fit-box offset (the reference's `pixels` matrix is rebuilt only
 //     for the bit-exact debug export);
@@ -32,9 +34,8 @@ namespace cpb {
 namespace {
 
 constexpr int TY = 32;   // region rows (y, contiguous in memory)
-constexpr int SW = 8;    // columns of one warp's strip
+constexpr int TX = 32;   // region columns
 constexpr int NT = 128;  // threads of the region kernels (4 warps)
-constexpr int TX = SW * (NT / 32);  // region columns
 constexpr double kEps64 = 2.220446049250313e-16;
 
 enum RenderMode { MODE_CUR = 0, MODE_CAND = 1, MODE_FREEZE = 2, MODE_FINAL = 3 };
@@ -230,11 +231,82 @@ struct FitConst {
     int gc[3];     // grad_col of free param k (1 = dy, 2 = dx, 3 = dflux)
     int ky, kx;    // index of y / x in the free list, -1 if fixed
     double fixed_y, fixed_x, fixed_flux, fixed_bkg;
-    int R, S, S2, VS;
+    int R, S, S2;
+    int SR, PS, VS;  // stamp layout of the fit box: rows per column, plane size, star block (see gran_rows)
     int q32, r32;  // 32 / S and 32 % S: advancing a stamp index by one warp
     int ny, nx;
     int nty, ntx;
 };
+
+// ---- stamp storage ("granule layout") ------------------------------------
+// A star's box of Sb x Sb pixels is stored per plane (one plane per free
+// parameter for the stamp derivatives, one for model values) as Sb columns of
+// SR = gran_rows(Sb, GH) entries.  GH = 16 bytes / element size (4 floats or
+// 2 doubles) is the granule height.  Box row r of column c lives at
+// c * SR + o + r with o = top0 mod GH, top0 the box's first image row
+// (0-based), so storage row 0 of every column sits on an image row that is a
+// multiple of GH.  The pixel regions of the gathers start on rows that are
+// multiples of 32, so every run of a column they need is made of whole
+// 16-byte granules; entries outside the box stay zero.
+template <typename T>
+struct Gran {
+    static constexpr int H = 16 / (int)sizeof(T);
+};
+__host__ __device__ __forceinline__ int gran_rows(int Sb, int gh) { return (Sb + 2 * gh - 2) / gh * gh; }
+__device__ __forceinline__ int gran_base(int top0, int gh) { return top0 & ~(gh - 1); }  // floor to a multiple of gh
+
+// one 16-byte granule; V / model stamps are streamed once per launch (evict first)
+__device__ __forceinline__ void ld_gran(const float* p, float (&o)[4]) {
+    const float4 t = __ldcs((const float4*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+}
+__device__ __forceinline__ void ld_gran(const double* p, double (&o)[2]) {
+    const double2 t = __ldcs((const double2*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+}
+// one 16-byte run of a per-pixel vector (reused, read-only for the launch)
+__device__ __forceinline__ void ld_px16(const float* p, float (&o)[4]) {
+    const float4 t = __ldg((const float4*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+}
+__device__ __forceinline__ void ld_px16(const double* p, double (&o)[2]) {
+    const double2 t = __ldg((const double2*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+}
+
+// a[0 .. n) += v in shared memory, 16 bytes at a time (a is 16-byte aligned)
+template <typename T, int N>
+__device__ __forceinline__ void smem_add_gran(T* a, const T (&v)[N]) {
+    static_assert((N * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int c = 0; c < N; c += 4) {
+            float4 t = *(float4*)(a + c);
+            t.x += v[c];
+            t.y += v[c + 1];
+            t.z += v[c + 2];
+            t.w += v[c + 3];
+            *(float4*)(a + c) = t;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < N; c += 2) {
+            double2 t = *(double2*)(a + c);
+            t.x += v[c];
+            t.y += v[c + 1];
+            *(double2*)(a + c) = t;
+        }
+    }
+}
+
 
 // model_from_vector for star j: theta (+ delta when cand).
 __global__ void k_coef(int64_t n_act, FitConst fc, DevPsf P, const double* theta, const double* delta,
@@ -357,8 +429,9 @@ __device__ __forceinline__ void tab_bicubic(const T* __restrict__ base, const Ax
 // Star-parallel stamp evaluation, one block per star of `list` (grid-stride);
 // the general path (any number of ePSF nodes).
 // GRAD (with gram == nullptr): _fill_stamps! (:342-399, :437-543) -- raw =
-//   sqrt(w) * gradient over the fit box, colnorm = max(||raw||, eps),
-//   V = raw * (1 / colnorm); masked and off-image entries are exactly 0.
+//   sqrt(w) * gradient over the fit box, colnorm = max(||raw||, eps); V keeps
+//   raw (the reference's values[:, m, a] = raw / colnorm; the J products
+//   divide by colnorm per star); masked and off-image entries are exactly 0.
 // GRAD with gram: the unscaled p x p Gram block sum(raw raw') of the error
 //   estimate (:1305-1318), nothing else written.
 // M != nullptr: the model value flux * s + bkg of every box pixel (the
@@ -388,6 +461,11 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
         const int Rb = Rs ? Rs[j] : Rmax;  // this star's box radius (<= Rmax, which sized the tables)
         const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
         const int a_y = ay[j], a_x = ax[j];
+        // granule layout of this star's model stamp and of its derivative planes
+        constexpr int GH = Gran<T>::H;
+        const int top0 = a_y - Rb - 1, go = top0 - gran_base(top0, GH);
+        const int SRb = gran_rows(Sb, GH);
+        T* Mj = M ? M + (moff ? moff[j] : (int64_t)j * MS) : nullptr;
         if (!gauss) {
             for (int e = threadIdx.x; e < 8 * Sb; e += NTF) {
                 const int k = e / (2 * Sb), rem = e % (2 * Sb), axis = rem / Sb, idx = rem % Sb;
@@ -415,7 +493,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             T s = 0, dY = 0, dX = 0, g[3];
             if (gauss) {
                 const T val = gauss_eval<T, GRAD>((T)P.fwhm, c, (T)gy, (T)gx, g[0], g[1], g[2]);
-                if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
+                if (Mj) Mj[col * SRb + go + row] = val;
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -430,7 +508,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                         dX += (T)c.dwdx[k] * pv - (T)c.w[k] * (T)nd.sx * pdu;
                     }
                 }
-                if (M) M[(moff ? moff[j] : (int64_t)j * MS) + m] = (T)c.flux * s + (T)c.bkg;
+                if (Mj) Mj[col * SRb + go + row] = (T)c.flux * s + (T)c.bkg;
                 g[0] = (T)c.flux * dY;
                 g[1] = (T)c.flux * dX;
                 g[2] = s;
@@ -481,12 +559,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             }
             __syncthreads();
             if (!gram) {
-                T inv[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     double cn = sqrt(k < p ? cn_sh[k] : 1.0);
                     cn = cn < kEps64 ? kEps64 : cn;
-                    inv[k] = (T)(1.0 / cn);
                     if (threadIdx.x == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
                 }
                 T* Vj = V + (int64_t)j * fc.VS;
@@ -494,9 +570,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                 for (int e = 0; e < RE; ++e) {
                     const int m = threadIdx.x + e * NTF;
                     if (m >= S2b) continue;
-                    Vj[m * p] = raw[e][0] * inv[0];
-                    if (p > 1) Vj[m * p + 1] = raw[e][1] * inv[1];
-                    if (p > 2) Vj[m * p + 2] = raw[e][2] * inv[2];
+                    const int sidx = (m / Sb) * fc.SR + go + m % Sb;  // the fit box: Sb == fc.S
+                    Vj[sidx] = raw[e][0];
+                    if (p > 1) Vj[fc.PS + sidx] = raw[e][1];
+                    if (p > 2) Vj[2 * fc.PS + sidx] = raw[e][2];
                 }
             }
         }
@@ -506,9 +583,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
 
 // Warp-per-star stamp evaluation for single-node ePSFs and the Gaussian (the
 // common case): no block barriers, each warp keeps its star's row / column
-// tables in its own slice of shared memory, and GRAD runs two passes
-// (colnorm, then the scaled stamp) instead of caching the raw values.
-// Same outputs as k_eval.
+// tables in its own slice of shared memory.  Same outputs as k_eval.
 template <bool GRAD, typename T>
 __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                                       DevPsf P, const StarCoef* __restrict__ coef,
@@ -540,6 +615,10 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const int q32 = 32 / Sb, r32 = 32 % Sb;
         AxisTab<T>* trow = tcol + Sb;
         const int oy = ay[j] - Rb, ox = ax[j] - Rb;
+        // granule layout: column c of the box starts at c * SRb, box row r at go + r
+        constexpr int GH = Gran<T>::H;
+        const int go = (oy - 1) - gran_base(oy - 1, GH), SRb = gran_rows(Sb, GH);
+        T* Mj = M ? M + (moff ? moff[j] : (int64_t)j * MS) : nullptr;
         if (!gauss) {
             for (int idx = lane; idx < 2 * Sb; idx += 32) {
                 if (idx < Sb) axis_tab_x(nd, nd.sx * ((double)(ox + idx) - cx) + nd.ox, tcol[idx]);
@@ -581,7 +660,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             for (int m = lane; m < S2b; m += 32) {
                 T val, a, b, c;
                 eval_px(row, col, val, a, b, c);
-                M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
+                Mj[col * SRb + go + row] = val;
                 row += r32;
                 col += q32;
                 if (row >= Sb) {
@@ -606,7 +685,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 if (use || (M && !gram)) {
                     T val, a, b, c;
                     eval_px(row, col, val, a, b, c);
-                    if (M && !gram) M[(moff ? moff[j] : (int64_t)j * MS) + m] = val;
+                    if (M && !gram) Mj[col * SRb + go + row] = val;
                     if (use) {
                         const T sq = (T)sw[q];
                         r0 = sq * a;
@@ -627,10 +706,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                         }
                     }
                 }
-                if (!gram) {
-                    Vj[m * p] = r0;
-                    if (p > 1) Vj[m * p + 1] = r1;
-                    if (p > 2) Vj[m * p + 2] = r2;
+                if (!gram) {  // the fit box: SRb == fc.SR
+                    const int sidx = col * SRb + go + row;
+                    Vj[sidx] = r0;
+                    if (p > 1) Vj[fc.PS + sidx] = r1;
+                    if (p > 2) Vj[2 * fc.PS + sidx] = r2;
                 }
                 row += r32;
                 col += q32;
@@ -654,18 +734,12 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     }
                 }
             } else {
-                T inv[3];
+                // the stamp keeps the unscaled derivatives; the J products divide by colnorm
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     double cn = sqrt(k < p ? acc[k] : 1.0);
                     cn = cn < kEps64 ? kEps64 : cn;
-                    inv[k] = (T)(1.0 / cn);
                     if (lane == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
-                }
-                for (int m = lane; m < S2b; m += 32) {  // the entries this lane wrote above
-                    Vj[m * p] *= inv[0];
-                    if (p > 1) Vj[m * p + 1] *= inv[1];
-                    if (p > 2) Vj[m * p + 2] *= inv[2];
                 }
             }
         }
@@ -675,44 +749,56 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 
 // Per-region pixel gather over the region's star list (stars in Morton
 // order), the deterministic replacement of the reference's scatter-adds.
-// A block owns a TY x TX pixel region; warp w owns the SW-column strip
-// starting at column w*SW and accumulates it in shared memory.  For each star
-// whose box meets its strip the warp streams the star's stamp entries for
-// those (at most SW) columns -- a contiguous run of the star's block -- and
-// adds them to the strip, one star after another (no atomics, fixed order).
-//   KIND_JV: sum_k V[j, m, k] * v[j, k] / alpha  (apply_J!, :95-137)
-//   KIND_M : sum M[j, m]                         (_render_model!)
+// A block owns a TY x TX pixel region; warp w takes the region's stars
+// w, w + NW, w + 2 NW, ... in list order and adds them into its own copy of
+// the region in shared memory.  A star's part of the region is a rectangle of
+// stamp granules (GH rows of one stamp column, GH = 16 bytes / element): the
+// region's rows and the stamp columns share the GH-row alignment, so every
+// load is a whole 16-byte granule.  The warp walks its stars' granules in
+// 32-granule slots (one star a slot, a star's last slot padded) and loads
+// KSLOT slots -- KSLOT * p granules a lane -- before adding any, slot by slot.
+// Each pixel is the sum of the warps' copies in warp order: a fixed order
+// (no atomics, bitwise reproducible).
+//   KIND_JV: sum_k V[j, k, m] * v[j, k] / (alpha colnorm[j, k])  (apply_J!,
+//            :95-137; V holds the unscaled weighted derivatives)
+//   KIND_M : sum M[j, m]                                          (_render_model!)
 // Epilogues (MODE): LSQR u update + beta (Krylov lsqr step 1); weighted
 // residual + cost (_residual_cost!, :675-684); candidate cost (_cost!,
 // :686-693); freeze subtraction (_freeze_star!, :739-754); final residual.
+// TU: element type of the LSQR pixel vectors (u, weighted residual); all
+// sums are FP64.
 constexpr int KIND_JV = 0, KIND_M = 1;
 constexpr int MODE_LSQR = 4;
-// 32-entry slots a warp loads per round: 4 measured fastest on the 2048^2 fit
-// (J.v 47.0 ms per fit; 3 slots 46.6 ms, 6 slots 58.5 ms and 8 slots 65.1 ms,
-// their registers costing more resident warps than the extra loads in flight
-// gain); J.v alone is held to 64 registers (8 blocks an SM: 45.7 ms), the
-// model gathers keep the compiler's choice
+// slots a warp loads per round before adding
 constexpr int KSLOT = 4;
+// the warps' FP64 region copies (sums are FP64 for either stamp type: FP32
+// sums of the mixed-precision form moved its fit measurably, FP32 storage did not)
+constexpr size_t kGatherSmem = (size_t)(NT / 32) * TX * TY * sizeof(double);
 
-template <int KIND, int MODE, typename TS>
-__global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
+template <int KIND, int MODE, typename TS, typename TU>
+__global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __restrict__ tstart,
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
                                                const int32_t* __restrict__ tord,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
                                                int Rbox, int64_t stride, const int64_t* __restrict__ soff,
-                                               const double* __restrict__ vt,
-                                               const double* u_src, double u_sign,
-                                               double* out, const uint8_t* __restrict__ umask,
+                                               const double* __restrict__ vt, const double* __restrict__ cn,
+                                               const TU* u_src, double u_sign,
+                                               TU* outu, double* outd, const uint8_t* __restrict__ umask,
                                                const double* __restrict__ w, const double* __restrict__ sw,
                                                const double* __restrict__ data_ref, Scalars* sc, Reducer red,
                                                double* result) {
-    __shared__ double s_acc[NT / 32][TY * SW];
+    constexpr int GH = Gran<TS>::H;      // rows of a granule
+    constexpr int NGR = TY / GH;         // granule rows of the region
+    constexpr int NW = NT / 32;
+    constexpr int NPL = KIND == KIND_JV ? 3 : 1;
+    extern __shared__ __align__(16) unsigned char g_smem[];
+    double* parts = (double*)g_smem;     // [NW][TX][TY], column-major per warp
     __shared__ int s_j[NT];
     __shared__ int s_ay[NT];
     __shared__ int s_ax[NT];
     __shared__ int s_rb[NT];
     __shared__ double s_v[3][NT];
-    __shared__ int s_wcnt[NT / 32];
+    __shared__ int s_wcnt[NW];
     __shared__ double sh[32];
     double inv_alpha = 1.0, alpha = 0.0, uscale = 1.0;
     if (KIND == KIND_JV) {
@@ -724,11 +810,11 @@ __global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst
     const int p = KIND == KIND_JV ? fc.p : 1;
     const int reg = tord[blockIdx.x];
     const int ry = reg % fc.nty, rx = reg / fc.nty;
+    const int R0 = ry * TY, C0 = rx * TX;  // 0-based first row / column of the region
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int y0 = ry * TY + 1, xs0 = rx * TX + wid * SW + 1;
-    const int yend = min(y0 + TY - 1, fc.ny), xend = min(xs0 + SW - 1, fc.nx);
-    double* acc = s_acc[wid];
-    for (int t = lane; t < TY * SW; t += 32) acc[t] = 0.0;
+    for (int t = threadIdx.x * 2; t < NW * TX * TY; t += NT * 2) *(double2*)(parts + t) = make_double2(0.0, 0.0);
+    __syncthreads();
+    double* mine = parts + wid * TX * TY;
     const int s0 = tstart[reg], s1 = tend[reg];
     for (int c0 = s0; c0 < s1; c0 += NT) {
         const int li = c0 + threadIdx.x;
@@ -743,7 +829,7 @@ __global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst
         __syncthreads();
         int before = 0, total = 0;
 #pragma unroll
-        for (int q = 0; q < NT / 32; ++q) {
+        for (int q = 0; q < NW; ++q) {
             total += s_wcnt[q];
             if (q < wid) before += s_wcnt[q];
         }
@@ -754,110 +840,133 @@ __global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst
             s_ax[pos] = ent.z;
             s_rb[pos] = ent.w;
             if (KIND == KIND_JV)
-                for (int k = 0; k < fc.p; ++k) s_v[k][pos] = vt[(int64_t)ent.x * fc.p + k] * inv_alpha;
+                for (int k = 0; k < fc.p; ++k)
+                    s_v[k][pos] = vt[(int64_t)ent.x * fc.p + k] * inv_alpha / cn[(int64_t)ent.x * fc.p + k];
         }
         __syncthreads();
-        if (xs0 <= fc.nx) {
-            // The warp walks its stars' entries in 32-entry slots (a slot holds
-            // one star's entries, a star's last slot is padded) and takes four
-            // slots a round -- up to four stars -- loading all of them before
-            // adding any; slots are added in order, so every pixel still sums
-            // its stars in list order, and one add instruction never holds two
-            // stars (no lost updates between lanes).
-            int e = 0, c = 0;  // current star and slot
-            int tot = 0, nrows = 1, m0 = 0, a0 = 0, Sb = 1;
-            float inv_nrows = 1.0f;
-            const TS* base = src;
-            auto seek = [&](int from) {  // the next star meeting the strip, from `from`
-                c = 0;
-                for (e = from; e < total; ++e) {
-                    const int ax_ = s_ax[e], ay_ = s_ay[e];
-                    // model renders: each star's own model radius; J v: the fit box
-                    const int Rb = KIND == KIND_M ? s_rb[e] : Rbox;
-                    Sb = 2 * Rb + 1;
-                    const int c_lo = max(ax_ - Rb, xs0), c_hi = min(ax_ + Rb, xend);
-                    const int r_lo = max(ay_ - Rb, y0), r_hi = min(ay_ + Rb, yend);
-                    if (c_lo > c_hi || r_lo > r_hi) continue;  // warp-uniform
-                    nrows = r_hi - r_lo + 1;
-                    tot = nrows * (c_hi - c_lo + 1);
-                    inv_nrows = 1.0f / (float)nrows;
-                    m0 = (r_lo - ay_ + Rb) + (c_lo - ax_ + Rb) * Sb;
-                    a0 = (r_lo - y0) + (c_lo - xs0) * TY;
-                    base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride);
-                    return;
-                }
-            };
-            seek(0);
-            while (e < total) {
-                TS raw[KSLOT][3];
-                int dst[KSLOT], eq[KSLOT];
+        // the current star's rectangle of granules inside the region
+        int e = wid, c = 0;  // star (staged index) and slot
+        int tot = 0, nga = 1, cl0 = 0, gl0 = 0, SRb = 0, PSb = 0;
+        float inv_nga = 1.0f;
+        const TS* base = src;
+        auto star_geometry = [&]() {
+            if (e >= total) return;
+            // model renders: each star's own model radius; J v: the fit box
+            const int Rb = KIND == KIND_M ? s_rb[e] : Rbox;
+            const int Sb = 2 * Rb + 1;
+            const int left0 = s_ax[e] - Rb - 1, top0 = s_ay[e] - Rb - 1;
+            const int b0 = gran_base(top0, GH);
+            SRb = gran_rows(Sb, GH);
+            PSb = Sb * SRb;
+            cl0 = max(left0, C0) - C0;
+            const int cl1 = min(left0 + Sb - 1, C0 + TX - 1) - C0;
+            const int r_lo = max(b0, R0), r_hi = min(b0 + SRb, R0 + TY);  // multiples of GH
+            gl0 = (r_lo - R0) / GH;
+            nga = max((r_hi - r_lo) / GH, 0);
+            tot = cl1 >= cl0 ? (cl1 - cl0 + 1) * nga : 0;
+            inv_nga = 1.0f / (float)max(nga, 1);
+            // storage offset of the rectangle's first granule
+            base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride) + (int64_t)(C0 + cl0 - left0) * SRb +
+                   (r_lo - b0);
+        };
+        star_geometry();
+        while (e < total && tot == 0) {
+            e += NW;
+            star_geometry();
+        }
+        while (e < total) {
+            TS raw[KSLOT][NPL][GH];
+            int dst[KSLOT], eq[KSLOT];
 #pragma unroll
-                for (int q = 0; q < KSLOT; ++q) {
-                    dst[q] = -1;
-                    eq[q] = e;
-                    raw[q][0] = raw[q][1] = raw[q][2] = (TS)0;
-                    if (e < total) {
-                        const int t = c * 32 + lane;
-                        if (t < tot) {
-                            const int cc = (int)(((float)t + 0.5f) * inv_nrows);
-                            const int rr = t - cc * nrows;
-                            const TS* ptr = base + (int64_t)(m0 + rr + cc * Sb) * p;
-                            raw[q][0] = __ldg(ptr);
-                            if (KIND == KIND_JV) {
-                                if (p > 1) raw[q][1] = __ldg(ptr + 1);
-                                if (p > 2) raw[q][2] = __ldg(ptr + 2);
-                            }
-                            dst[q] = a0 + rr + cc * TY;
-                        }
-                        if ((c + 1) * 32 < tot) ++c;
-                        else seek(e + 1);
+            for (int q = 0; q < KSLOT; ++q) {
+                dst[q] = -1;
+                eq[q] = e;
+                if (e < total) {
+                    const int t = c * 32 + lane;
+                    if (t < tot) {
+                        const int cc = (int)(((float)t + 0.5f) * inv_nga);
+                        const int gg = t - cc * nga;
+                        const TS* g = base + (int64_t)cc * SRb + gg * GH;
+#pragma unroll
+                        for (int k = 0; k < NPL; ++k)
+                            if (k < p) ld_gran(g + (int64_t)k * PSb, raw[q][k]);
+                        dst[q] = (cl0 + cc) * TY + (gl0 + gg) * GH;
+                    }
+                    if ((c + 1) * 32 < tot) {
+                        ++c;
+                    } else {
+                        c = 0;
+                        do {
+                            e += NW;
+                            star_geometry();
+                        } while (e < total && tot == 0);
                     }
                 }
+            }
+            // slots in order; two slots of a round may meet at a pixel (different
+            // lanes), so each slot's adds complete before the next slot's start
 #pragma unroll
-                for (int q = 0; q < KSLOT; ++q) {
-                    if (dst[q] >= 0) {
-                        double v;
+            for (int q = 0; q < KSLOT; ++q) {
+                if (dst[q] >= 0) {
+                    double v[GH];
+#pragma unroll
+                    for (int r = 0; r < GH; ++r) {
+                        double t = (double)raw[q][0][r];
                         if (KIND == KIND_JV) {
-                            v = (double)raw[q][0] * s_v[0][eq[q]];
-                            if (p > 1) v += (double)raw[q][1] * s_v[1][eq[q]];
-                            if (p > 2) v += (double)raw[q][2] * s_v[2][eq[q]];
-                        } else {
-                            v = (double)raw[q][0];
+                            t *= s_v[0][eq[q]];
+                            if (p > 1) t += (double)raw[q][1][r] * s_v[1][eq[q]];
+                            if (p > 2) t += (double)raw[q][2][r] * s_v[2][eq[q]];
                         }
-                        acc[dst[q]] += v;
+                        v[r] = t;
                     }
+                    smem_add_gran(mine + dst[q], v);
                 }
                 __syncwarp();
             }
         }
         __syncthreads();
     }
+    // sum the warps' copies in warp order, then the epilogue, GH pixels at a time
     double part = 0.0;
-    for (int t = lane; t < TY * SW; t += 32) {
-        const int gy = y0 + (t % TY), gx = xs0 + t / TY;
-        if (gy > fc.ny || gx > fc.nx) continue;
-        const int64_t q = (gy - 1) + (int64_t)(gx - 1) * fc.ny;
-        const double a = acc[t];
-        if (MODE == MODE_LSQR) {
-            const double un = a - alpha * (u_src[q] * uscale);
-            out[q] = un;
-            part += un * un;
-        } else if (MODE == MODE_CUR) {
-            double wr = 0.0;
-            if (umask[q]) {
-                wr = sw[q] * (a - data_ref[q]);
-                part += wr * wr;
+    for (int gi = threadIdx.x; gi < TX * NGR; gi += NT) {
+        const int col = gi / NGR, gr = gi % NGR;
+        const int gx = C0 + col;
+        if (gx >= fc.nx) continue;
+        const int off = col * TY + gr * GH;
+        double acc[GH];
+#pragma unroll
+        for (int r = 0; r < GH; ++r) acc[r] = parts[off + r];
+#pragma unroll
+        for (int q = 1; q < NW; ++q)
+#pragma unroll
+            for (int r = 0; r < GH; ++r) acc[r] += parts[q * TX * TY + off + r];
+#pragma unroll
+        for (int r = 0; r < GH; ++r) {
+            const int gy = R0 + gr * GH + r;
+            if (gy >= fc.ny) break;
+            const int64_t q = gy + (int64_t)gx * fc.ny;
+            const double av = acc[r];
+            if (MODE == MODE_LSQR) {
+                const TU un = (TU)(av - alpha * ((double)u_src[q] * uscale));
+                outu[q] = un;
+                part += (double)un * (double)un;
+            } else if (MODE == MODE_CUR) {
+                double wr = 0.0;
+                if (umask[q]) {
+                    wr = sw[q] * (av - data_ref[q]);
+                    part += wr * wr;
+                }
+                outu[q] = (TU)wr;  // wt_resid (zero outside U)
+            } else if (MODE == MODE_CAND) {
+                if (umask[q]) {
+                    const double rr = av - data_ref[q];
+                    part += w[q] * rr * rr;
+                }
+            } else if (MODE == MODE_FREEZE) {
+                outd[q] -= av;  // data_work
+            } else {
+                outd[q] = data_ref[q] - av;  // residual against the original data
             }
-            out[q] = wr;  // wt_resid (zero outside U)
-        } else if (MODE == MODE_CAND) {
-            if (umask[q]) {
-                const double r = a - data_ref[q];
-                part += w[q] * r * r;
-            }
-        } else if (MODE == MODE_FREEZE) {
-            out[q] -= a;  // data_work
-        } else {
-            out[q] = data_ref[q] - a;  // residual against the original data
         }
     }
     if (MODE == MODE_LSQR) {
@@ -876,16 +985,22 @@ __global__ void __launch_bounds__(NT, KIND == KIND_JV ? 8 : 0) k_gather(FitConst
     }
 }
 
-// J^T u for the stars of `list` (apply_JT!, :55-85): one warp per star,
-// coalesced reads of the star's stamp block, gathers of u; stamp indices
-// advance incrementally and four entries per lane are in flight at once.
-// Writes z[j*p+k] = sum_m V[j,m,k] u[pix(m)] * uscale.  LSQR form: v_new =
-// z - beta * v_old / alpha_old and alpha = ||v_new|| (Krylov lsqr step 2).
-template <bool LSQR, typename TS>
-__global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+// J^T u for the stars of `list` (apply_JT!, :55-85): one warp per star.
+// The lanes walk the star's granules (GH rows of one stamp column): the
+// granule of each derivative plane and the matching GH pixels of u, all
+// 16-byte loads, JU granules in flight per lane.  Writes z[j*p+k] =
+// sum_m V[j,k,m] u[pix(m)] * uscale / colnorm[j,k] (V holds the unscaled
+// weighted derivatives).  LSQR form: v_new = z - beta * v_old / alpha_old and
+// alpha = ||v_new|| (Krylov lsqr step 2).  Sums are FP64 for either stamp type.
+template <bool LSQR, typename TS, typename TU>
+__global__ void __launch_bounds__(256, 3) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                             const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                            const TS* __restrict__ V, const double* __restrict__ u,
-                                            double* __restrict__ z, Scalars* sc, Reducer red) {
+                                            const TS* __restrict__ V, const double* __restrict__ cn,
+                                            const TU* __restrict__ u, double* __restrict__ z, Scalars* sc,
+                                            Reducer red) {
+    static_assert(sizeof(TS) == sizeof(TU), "u granules match stamp granules");
+    constexpr int GH = Gran<TS>::H;
+    constexpr int JU = 2;
     __shared__ double sh[32];
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -897,53 +1012,68 @@ __global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list,
         beta = sc->beta;
         inv_alpha = sc->inv_alpha;
     }
-    const int p = fc.p, S = fc.S, S2 = fc.S2, R = fc.R;
+    const int p = fc.p, S = fc.S, R = fc.R, SR = fc.SR, PS = fc.PS;
+    const int NG = SR / GH, G = S * NG;
+    const int dcol = 32 / NG, dgr = 32 % NG;
+    const int ny = fc.ny, nx = fc.nx;
+    const bool uvec = (ny % GH) == 0;
     double part = 0.0;
     for (int64_t li = warp; li < nlist; li += nwarps) {
         const int j = list[li];
-        const int a_y = ay[j] - R, a_x = ax[j] - R;
+        const int top0 = ay[j] - R - 1, left0 = ax[j] - R - 1;
+        const int b0 = gran_base(top0, GH);
         const TS* Vj = V + (int64_t)j * fc.VS;
-        double acc0 = 0, acc1 = 0, acc2 = 0;
-        int r = lane % S, c = lane / S;
-        for (int m0 = 0; m0 < S2; m0 += 128) {
-            double uv[4], v0[4], v1[4], v2[4];
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        int col = lane / NG, gr = lane % NG;
+        for (int g0 = lane; g0 < G; g0 += 32 * JU) {
+            TS v[JU][3][GH];
+            TU uu[JU][GH];
+            bool ok[JU];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int m = m0 + lane + 32 * q;
-                const int gy = a_y + r, gx = a_x + c;
-                const bool ok = m < S2 && gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
-                uv[q] = 0.0;
-                v0[q] = v1[q] = v2[q] = 0.0;
-                if (ok) {
-                    uv[q] = __ldg(u + (gy - 1) + (int64_t)(gx - 1) * fc.ny);
-                    const TS* vm = Vj + m * p;
-                    v0[q] = (double)__ldg(vm);
-                    if (p > 1) v1[q] = (double)__ldg(vm + 1);
-                    if (p > 2) v2[q] = (double)__ldg(vm + 2);
+            for (int q = 0; q < JU; ++q) {
+                const int gx = left0 + col, gy = b0 + gr * GH;
+                ok[q] = g0 + 32 * q < G && gx >= 0 && gx < nx;
+                if (ok[q]) {
+                    const TS* e = Vj + col * SR + gr * GH;
+                    ld_gran(e, v[q][0]);
+                    if (p > 1) ld_gran(e + PS, v[q][1]);
+                    if (p > 2) ld_gran(e + 2 * PS, v[q][2]);
+                    const int64_t pq = gy + (int64_t)gx * ny;
+                    if (uvec && gy >= 0 && gy + GH <= ny) {
+                        ld_px16(u + pq, uu[q]);
+                    } else {
+#pragma unroll
+                        for (int r = 0; r < GH; ++r)
+                            uu[q][r] = (gy + r >= 0 && gy + r < ny) ? __ldg(u + pq + r) : (TU)0;
+                    }
                 }
-                r += fc.r32;
-                c += fc.q32;
-                if (r >= S) {
-                    r -= S;
-                    c += 1;
+                gr += dgr;
+                col += dcol;
+                if (gr >= NG) {
+                    gr -= NG;
+                    col += 1;
                 }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double uq = LSQR ? uv[q] * uscale : uv[q];
-                acc0 += v0[q] * uq;
-                acc1 += v1[q] * uq;
-                acc2 += v2[q] * uq;
+            for (int q = 0; q < JU; ++q) {
+                if (!ok[q]) continue;
+#pragma unroll
+                for (int r = 0; r < GH; ++r) {
+                    const double ur = (double)uu[q][r];
+                    a0 += (double)v[q][0][r] * ur;
+                    if (p > 1) a1 += (double)v[q][1][r] * ur;
+                    if (p > 2) a2 += (double)v[q][2][r] * ur;
+                }
             }
         }
-        acc0 = warp_sum(acc0);
-        acc1 = warp_sum(acc1);
-        acc2 = warp_sum(acc2);
+        const double acc0 = warp_sum(a0) * uscale;
+        const double acc1 = warp_sum(a1) * uscale;
+        const double acc2 = warp_sum(a2) * uscale;
         if (lane == 0) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 if (k >= p) break;
-                double val = k == 0 ? acc0 : (k == 1 ? acc1 : acc2);
+                double val = (k == 0 ? acc0 : (k == 1 ? acc1 : acc2)) / cn[(int64_t)j * p + k];
                 if (LSQR) {
                     val = val - beta * (z[(int64_t)j * p + k] * inv_alpha);
                     part += val * val;
@@ -1459,14 +1589,396 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// scratch bound of one fit (the no-allocation entry point's up-front check)
+// ---------------------------------------------------------------------------
+namespace {
+
+// Bytes arena_carve reserves for one named buffer of `bytes`.
+size_t carve_size(size_t bytes) { return (std::max<size_t>(bytes, 256) + 255) & ~size_t(255); }
+
+// The tile lists of build_tiles for n stars of box radius Rb.
+size_t tiles_bound(int64_t n, int Rb, int64_t ntiles) {
+    const int64_t Sb = 2 * (int64_t)Rb + 1;
+    const int64_t per = ((Sb + TY - 1) / TY + 1) * ((Sb + TX - 1) / TX + 1);
+    const int64_t npairs = std::max<int64_t>(n * per, 1);
+    size_t b = 2 * carve_size(4 * (n + 1));
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, (int32_t*)nullptr, (int32_t*)nullptr, (int)(n + 1));
+    b += carve_size(tmp);
+    b += 4 * carve_size(4 * npairs) + carve_size(16 * npairs);
+    b += 3 * carve_size(4 * ntiles) + carve_size(8 * ntiles) + carve_size(4 * ntiles);
+    int end_bit = 1;
+    while ((1LL << end_bit) < ntiles) ++end_bit;
+    tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, (uint32_t*)nullptr, (uint32_t*)nullptr, (int32_t*)nullptr,
+                                    (int32_t*)nullptr, (int)npairs, 0, end_bit);
+    b += carve_size(tmp);
+    tmp = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                              (int32_t*)nullptr, (int32_t*)nullptr, (int)ntiles, 0, 32);
+    b += carve_size(tmp);
+    return b;
+}
+
+// One precision form (Form<TS, TU>): stamps, model stamps, pixel vectors.
+template <typename TS, typename TU>
+size_t form_bound(int64_t n, int p, int S, int64_t model_entries_per_star, bool per_star_offsets, int64_t npix) {
+    size_t b = carve_size((size_t)p * S * gran_rows(S, Gran<TS>::H) * n * sizeof(TS));
+    b += carve_size((size_t)model_entries_per_star * n * sizeof(TS));
+    if (per_star_offsets) b += carve_size(8 * n);
+    b += 2 * carve_size(npix * sizeof(TU));
+    return b;
+}
+
+}  // namespace
+
+size_t sim_scratch_bound(const cpb_sim_params* P, int64_t ny, int64_t nx, int64_t n, bool dbg_pixels) {
+    const int p = std::max(1, __builtin_popcount((unsigned)(P->free_mask & (CPB_FREE_Y | CPB_FREE_X | CPB_FREE_FLUX))));
+    const int R = (int)std::ceil(std::max(P->fit_rad, 0.0));
+    const int S = 2 * R + 1;
+    const int64_t S2 = (int64_t)S * S;
+    // model boxes: the scalar radius as the driver clamps it; with :auto the
+    // fit box (the driver checks the model buffers again once the radii are known)
+    int Rm = R;
+    if (!P->model_rad_auto) {
+        const int R_cap = (int)std::ceil(std::max(P->model_rad, P->fit_rad));
+        Rm = std::min(std::max((int)std::ceil(P->model_rad), R), R_cap);
+    }
+    const int Sm = 2 * Rm + 1;
+    const int64_t npix = ny * nx;
+    const int64_t ntiles = ((ny + TY - 1) / TY) * ((nx + TX - 1) / TX);
+    const int64_t np = (int64_t)p * n;
+    size_t b = 2 * carve_size(sizeof(Scalars));                                    // scalars, scalars_freeze
+    b += carve_size(8 * std::max<int64_t>(ntiles, nblk(std::max<int64_t>(n * 3, npix)) + 1)) + carve_size(4);
+    b += 4 * carve_size(8 * npix) + carve_size(16);                                // data, data_work, w, sw, flags
+    b += 2 * carve_size(4 * n) + carve_size(n) + carve_size(8 * n);                // ay_c, ax_c, ok, key
+    b += 2 * carve_size(4 * n) + 2 * carve_size(8 * n) + carve_size(4 * n) + carve_size(4);  // iota .. nsel
+    size_t tmp = 0;
+    cub::DeviceSelect::Flagged(nullptr, tmp, (int32_t*)nullptr, (uint8_t*)nullptr, (int32_t*)nullptr, (int*)nullptr,
+                               (int)n);
+    const size_t sel_tmp = tmp;
+    tmp = 0;
+    cub::DeviceSelect::Flagged(nullptr, tmp, (uint64_t*)nullptr, (uint8_t*)nullptr, (uint64_t*)nullptr,
+                               (int*)nullptr, (int)n);
+    b += carve_size(sel_tmp) + carve_size(tmp);
+    tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, (uint64_t*)nullptr, (uint64_t*)nullptr, (int32_t*)nullptr,
+                                    (int32_t*)nullptr, (int)n, 0, 64);
+    b += carve_size(tmp);
+    b += 2 * carve_size(4 * n) + carve_size(8 * np);                              // ay, ax, theta
+    b += carve_size(npix) + carve_size(8);                                         // umask, ucnt
+    if (dbg_pixels) b += carve_size(4 * S2 * n);
+    if (P->model_rad_auto) b += carve_size(4 * n);
+    b += tiles_bound(n, R, ntiles);
+    if (Rm != R || P->model_rad_auto) b += tiles_bound(n, Rm, ntiles);
+    b += 8 * carve_size(8 * np) + 2 * carve_size(sizeof(StarCoef) * n);           // solver state
+    b += 3 * carve_size(n) + 4 * carve_size(4 * n) + carve_size(4);
+    b += 2 * carve_size(sel_tmp);                                                  // live_tmp, newf_tmp
+    const bool per_star = P->model_rad_auto != 0;
+    if (P->precision == CPB_PREC_MIXED) {
+        b += form_bound<float, float>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<float>::H), per_star, npix);
+        if (P->refine_iters > 0)
+            b += form_bound<double, double>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<double>::H), per_star, npix);
+    } else {
+        b += form_bound<double, double>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<double>::H), per_star, npix);
+    }
+    // final pass: gram, err, resid, FP64 model stamps (+ offsets), spread tables, diagnostics
+    b += carve_size(48 * n) + carve_size(8 * np) + carve_size(8 * npix);
+    b += carve_size((size_t)Sm * gran_rows(Sm, Gran<double>::H) * n * 8) + (per_star ? carve_size(8 * n) : 0);
+    b += carve_size(8 * kSpreadRuleLen) + carve_size(8 * spread_tab_len(R)) + carve_size(56 * n);
+    return b;
+}
+
+// ---------------------------------------------------------------------------
 // driver
 // ---------------------------------------------------------------------------
+namespace {
+
+// The buffers of one precision form of the outer loop: stamp derivatives and
+// model stamps stored as TS in the granule layout of TS, the LSQR pixel
+// vectors (weighted residual, u) as TU.
+template <typename TS, typename TU>
+struct Form {
+    FitConst fc;              // the fit constants with TS's stamp layout
+    TS* V = nullptr;          // n_act x fc.VS
+    TS* M = nullptr;          // model stamps: n_act x MS, or per-star blocks at d_moff (model_rad = :auto)
+    int MS = 0;
+    int64_t* d_moff = nullptr;
+    int64_t mtotal = 0;
+    TU* wt_resid = nullptr;
+    TU* u = nullptr;
+    bool m_fresh = false;     // M holds the current-theta model of the live stars (written by the fill)
+};
+
+class SimFit {
+  public:
+    SimFit(cpb_ctx* ctx_, const cpb_psf* psf_, const cpb_sim_params* P_, const void* d_image_, int32_t eltype_,
+           int64_t ny_, int64_t nx_, const void* d_inv_var_, const void* d_background_, int64_t n_stars_,
+           const double* d_y0_, const double* d_x0_, const double* d_flux0_, cpb_sim_result* out_)
+        : ctx(ctx_), psf(psf_), P(P_), d_image(d_image_), eltype(eltype_), ny64(ny_), nx64(nx_),
+          d_inv_var(d_inv_var_), d_background(d_background_), n_stars(n_stars_), d_y0(d_y0_), d_x0(d_x0_),
+          d_flux0(d_flux0_), out(out_), st(ctx_->stream) {}
+
+    int run();
+
+  private:
+    template <typename T>
+    T* S_(const char* name, size_t count) {
+        return (T*)scratch(ctx, name, std::max<size_t>(count, 1) * sizeof(T));
+    }
+    void nan_diag(int64_t i);
+    bool setup();  // false: the fit ended early (no stars, nothing active)
+    template <typename TS, typename TU>
+    Form<TS, TU> make_form(const char* tag);
+    template <typename TS>
+    void model_layout(const char* tag, int& MS, int64_t*& d_moff, int64_t& mtotal);
+    template <typename TS, typename TU>
+    void launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist);
+    template <typename TS>
+    void launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* d_moff, const int32_t* list,
+                           int64_t nlist, const StarCoef* cf);
+    template <typename TS, typename TU>
+    void launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const int32_t* list, int64_t nlist,
+                       const StarCoef* cf, TU* outu, double* outd, const double* ref, double* result);
+    void update_live_list();
+    void read_scalars();
+    template <typename TS, typename TU>
+    void outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial);
+    void finish();
+    void warp_shape(int Sx, size_t tab_size, unsigned& threads, size_t& smem) const;
+    void arena_precheck();
+    void launch_coef(const double* delta, StarCoef* dst);
+
+    // arguments
+    cpb_ctx* ctx;
+    const cpb_psf* psf;
+    const cpb_sim_params* P;
+    const void* d_image;
+    int32_t eltype;
+    int64_t ny64, nx64;
+    const void* d_inv_var;
+    const void* d_background;
+    int64_t n_stars;
+    const double *d_y0, *d_x0, *d_flux0;
+    cpb_sim_result* out;
+    cudaStream_t st;
+    // set-up
+    int ny = 0, nx = 0;
+    int64_t npix = 0, ntiles = 0;
+    bool reweighted = false;
+    FitConst fc{};
+    int p = 0;
+    DevPsf dp{};
+    Scalars* sc = nullptr;
+    Scalars* h_sc = nullptr;
+    Reducer red{};
+    double *data = nullptr, *data_work = nullptr, *w = nullptr, *sw = nullptr;
+    int32_t* act = nullptr;
+    int64_t n_act = 0, n = 0;
+    int n_failed = 0;
+    int32_t *ay = nullptr, *ax = nullptr;
+    double* theta = nullptr;
+    uint8_t* umask = nullptr;
+    int32_t* dbg_pix = nullptr;
+    unsigned long long h_ucnt = 0;
+    int model_R = 0;
+    int32_t* d_modelR = nullptr;
+    std::vector<int32_t> h_modelR;
+    double mean_box = 0, dof = 1;
+    TileLists tfit, tmod;
+    double *cn = nullptr, *D = nullptr, *bsc = nullptr, *delta = nullptr, *dsc = nullptr;
+    double *xl = nullptr, *vt = nullptr, *wl = nullptr;
+    StarCoef *coef = nullptr, *coefc = nullptr;
+    uint8_t *live = nullptr, *newf = nullptr, *conv = nullptr;
+    int32_t *frozen_at = nullptr, *live_list = nullptr, *iota_act = nullptr, *evlist = nullptr;
+    int* d_nlive = nullptr;
+    void* live_tmp = nullptr;
+    size_t live_tmp_bytes = 0;
+    int64_t n_live = 0;
+    bool warp_eval = false;
+    int smem_optin = 0;
+    int Sm = 0;
+    unsigned jt_blocks = 1;
+    // loop state
+    double evals = 0, macs = 0;
+    double lam = 0;
+    int n_run = 0;
+    int64_t n_trials = 0, n_lsqr = 0;
+};
+
+void SimFit::nan_diag(int64_t i) {
+    const double NaN = std::numeric_limits<double>::quiet_NaN();
+    if (out->qfit) out->qfit[i] = NaN;
+    if (out->qfit_expected) out->qfit_expected[i] = NaN;
+    if (out->qfit_z) out->qfit_z[i] = NaN;
+    if (out->crowding) out->crowding[i] = NaN;
+    if (out->spread_model) out->spread_model[i] = NaN;
+    if (out->spread_model_err) out->spread_model_err[i] = NaN;
+}
+
+void SimFit::warp_shape(int Sx, size_t tab_size, unsigned& threads, size_t& smem) const {
+    // warps per block of a k_eval_warp launch whose per-warp axis tables (2 Sx
+    // entries) fit the opt-in shared memory
+    int warps = 8;
+    while (warps > 1 && (size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin) warps /= 2;
+    if ((size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin)
+        throw ArgError{"radius too large for the B200 stamp kernels"};
+    threads = 32u * warps;
+    smem = (size_t)warps * 2 * Sx * tab_size;
+}
+
+void SimFit::launch_coef(const double* dlt, StarCoef* dst) {
+    KernelScope ks_(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8));
+    k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, dlt, dst);
+    check(cudaGetLastError(), "k_coef");
+}
+
+void SimFit::read_scalars() {
+    check(cudaMemcpyAsync(h_sc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+}
+
+void SimFit::update_live_list() {
+    cub::DeviceSelect::Flagged(live_tmp, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
+    int h = 0;
+    check(cudaMemcpyAsync(&h, d_nlive, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    n_live = h;
+}
+
+// Model-stamp layout of element type TS: one block of MS entries a star, or
+// with per-star radii (:auto) each star's own block at d_moff[j].
 template <typename TS>
-int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
-                         int32_t eltype, int64_t ny64, int64_t nx64, const void* d_inv_var, const void* d_background,
-                         int64_t n_stars, const double* d_y0, const double* d_x0, const double* d_flux0,
-                         cpb_sim_result* out) {
-    cudaStream_t st = ctx->stream;
+void SimFit::model_layout(const char* tag, int& MS, int64_t*& d_moff, int64_t& mtotal) {
+    constexpr int GH = Gran<TS>::H;
+    MS = Sm * gran_rows(Sm, GH);
+    d_moff = nullptr;
+    mtotal = (int64_t)MS * n_act;
+    if (d_modelR) {
+        std::vector<int64_t> h_moff(n_act);
+        mtotal = 0;
+        for (int64_t j = 0; j < n_act; ++j) {
+            h_moff[j] = mtotal;
+            const int sj = 2 * h_modelR[j] + 1;
+            mtotal += (int64_t)sj * gran_rows(sj, GH);
+        }
+        d_moff = S_<int64_t>((std::string("model_off") + tag).c_str(), n_act);
+        check(cudaMemcpyAsync(d_moff, h_moff.data(), sizeof(int64_t) * n_act, cudaMemcpyHostToDevice, st), "h2d");
+    }
+}
+
+template <typename TS, typename TU>
+Form<TS, TU> SimFit::make_form(const char* tag) {
+    Form<TS, TU> F;
+    constexpr int GH = Gran<TS>::H;
+    F.fc = fc;
+    F.fc.SR = gran_rows(fc.S, GH);
+    F.fc.PS = fc.S * F.fc.SR;
+    F.fc.VS = p * F.fc.PS;
+    const std::string t(tag);
+    F.V = S_<TS>(("V" + t).c_str(), (int64_t)F.fc.VS * n_act);
+    // entries outside each box stay zero for the whole fit (the anchors are fixed)
+    check(cudaMemsetAsync(F.V, 0, sizeof(TS) * (int64_t)F.fc.VS * n_act, st), "memset");
+    model_layout<TS>(tag, F.MS, F.d_moff, F.mtotal);
+    F.M = S_<TS>(("model_stamps" + t).c_str(), F.mtotal);
+    check(cudaMemsetAsync(F.M, 0, sizeof(TS) * F.mtotal, st), "memset");
+    F.wt_resid = S_<TU>(("wt_resid" + t).c_str(), npix);
+    F.u = S_<TU>(("lsqr_u" + t).c_str(), npix);
+    return F;
+}
+
+// _fill_stamps! at coef for the stars of `list`: V (and, when the model box is
+// the fit box, the model stamps) and colnorm
+template <typename TS, typename TU>
+void SimFit::launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist) {
+    if (nlist <= 0) return;
+    constexpr double bts = sizeof(TS);
+    const bool writeM = model_R == fc.R && !d_modelR;
+    KernelScope ks_(ctx, "k_eval_fill",
+                    (double)nlist * ((double)p * fc.S2 * bts + p * 8 + (writeM ? fc.S2 * bts : 0.0) +
+                                     std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1)) * 16 +
+                                     sizeof(StarCoef)));
+    TS* Mo = writeM ? F.M : nullptr;
+    if (warp_eval) {
+        unsigned thr;
+        size_t sm_bytes;
+        warp_shape(fc.S, sizeof(AxisTab<TS>), thr, sm_bytes);
+        if (sm_bytes > 48 * 1024)
+            check(cudaFuncSetAttribute(k_eval_warp<true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm_bytes), "smem attr");
+        const int wpb = (int)(thr / 32);
+        const unsigned gbw =
+            (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+        k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V, cn,
+                                                         nullptr, Mo, fc.R, F.MS, nullptr, nullptr);
+    } else {
+        const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
+        launch_k_eval<true, TS>(fc.S2, grid, tab_bytes * fc.S, st, list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V,
+                                cn, (double*)nullptr, Mo, fc.R, F.MS, (const int32_t*)nullptr,
+                                (const int64_t*)nullptr);
+    }
+    check(cudaGetLastError(), "k_eval_fill");
+    F.m_fresh = writeM;
+}
+
+// model values at `cf` for the stars of `list` into M (value-only stamp evaluation)
+template <typename TS>
+void SimFit::launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* d_moff, const int32_t* list,
+                               int64_t nlist, const StarCoef* cf) {
+    if (nlist <= 0) return;
+    KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * sizeof(TS) + sizeof(StarCoef)));
+    if (warp_eval) {
+        unsigned thr;
+        size_t sm_bytes;
+        warp_shape(Sm, sizeof(AxisTab<TS>), thr, sm_bytes);
+        if (sm_bytes > 48 * 1024)
+            check(cudaFuncSetAttribute(k_eval_warp<false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm_bytes), "smem attr");
+        const int wpb = (int)(thr / 32);
+        const unsigned gbw =
+            (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+        k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, f, dp, cf, ay, ax, w, sw, (TS*)nullptr, cn,
+                                                          nullptr, M, model_R, MS, d_modelR, d_moff);
+    } else {
+        const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
+        const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
+        launch_k_eval<false, TS>((int64_t)Sm * Sm, grid, tab_bytes * Sm, st, list, nlist, f, dp, cf, ay, ax, w, sw,
+                                 (TS*)nullptr, cn, (double*)nullptr, M, model_R, MS, (const int32_t*)d_modelR,
+                                 d_moff);
+    }
+    check(cudaGetLastError(), "k_eval_model");
+}
+
+template <typename TS, typename TU>
+void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const int32_t* list, int64_t nlist,
+                           const StarCoef* cf, TU* outu, double* outd, const double* ref, double* result) {
+    if (!(mode == MODE_CUR && F.m_fresh)) launch_eval_model<TS>(F.fc, F.M, F.MS, F.d_moff, list, nlist, cf);
+    F.m_fresh = false;
+    const double px_bytes =
+        mode == MODE_CUR ? 17.0 + sizeof(TU) : (mode == MODE_CAND ? 17.0 : 16.0);
+    KernelScope ks_(ctx,
+                    mode == MODE_CUR ? "k_gather_resid"
+                                     : (mode == MODE_CAND ? "k_gather_cost"
+                                                          : (mode == MODE_FREEZE ? "k_gather_freeze" : "k_gather_final")),
+                    (double)npix * px_bytes + (double)nlist * Sm * Sm * sizeof(TS));
+    const unsigned g = (unsigned)ntiles;
+    const auto& tl = tmod;
+#define CPB_RENDER(MD)                                                                                               \
+    k_gather<KIND_M, MD, TS, TU><<<g, NT, kGatherSmem, st>>>(F.fc, tl.start, tl.end, tl.list, tl.order, incl, F.M, model_R,     \
+                                                   F.MS, F.d_moff, nullptr, nullptr, nullptr, 0.0, outu, outd, umask, w, sw, \
+                                                   ref, sc, red, result)
+    switch (mode) {
+        case MODE_CUR: CPB_RENDER(MODE_CUR); break;
+        case MODE_CAND: CPB_RENDER(MODE_CAND); break;
+        case MODE_FREEZE: CPB_RENDER(MODE_FREEZE); break;
+        default: CPB_RENDER(MODE_FINAL);
+    }
+#undef CPB_RENDER
+    check(cudaGetLastError(), "k_gather");
+}
+
+bool SimFit::setup() {
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     // argument checks in the reference's order (:984-997)
     if (!(P->max_iter > 0)) throw ArgError{"max_iter must be positive"};
@@ -1486,10 +1998,13 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     if (!(P->fit_rad > 0)) throw ArgError{"fit_rad must be positive"};
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
     if (ny64 <= 0 || nx64 <= 0 || ny64 * nx64 >= (1LL << 31)) throw ArgError{"image size out of range"};
-    const int ny = (int)ny64, nx = (int)nx64;
-    const int64_t npix = ny64 * nx64;
-    const bool reweighted =
-        P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && d_inv_var == nullptr);
+    if (P->precision != CPB_PREC_FP64 && P->precision != CPB_PREC_MIXED)
+        throw ArgError{"precision must be CPB_PREC_FP64 or CPB_PREC_MIXED"};
+    if (P->refine_iters < 0) throw ArgError{"refine_iters must be >= 0"};
+    ny = (int)ny64;
+    nx = (int)nx64;
+    npix = ny64 * nx64;
+    reweighted = P->covariance == CPB_COV_REWEIGHTED || (P->covariance == CPB_COV_AUTO && d_inv_var == nullptr);
     out->n_active = 0;
     out->n_union = 0;
     out->n_trials = 0;
@@ -1497,22 +2012,13 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     out->model_px_evals = 0;
     out->lsqr_px_macs = 0;
     out->device_seconds = 0;
-    auto nan_diag = [&](int64_t i) {
-        if (out->qfit) out->qfit[i] = NaN;
-        if (out->qfit_expected) out->qfit_expected[i] = NaN;
-        if (out->qfit_z) out->qfit_z[i] = NaN;
-        if (out->crowding) out->crowding[i] = NaN;
-        if (out->spread_model) out->spread_model[i] = NaN;
-        if (out->spread_model_err) out->spread_model_err[i] = NaN;
-    };
     if (n_stars == 0) {
         out->n_passes = 0;
         out->n_failed = 0;
         if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
-        return 0;
+        return false;
     }
     // free set (:1015-1051)
-    FitConst fc{};
     fc.p = 0;
     if (P->free_mask & CPB_FREE_Y) fc.gc[fc.p++] = 1;
     if (P->free_mask & CPB_FREE_X) fc.gc[fc.p++] = 2;
@@ -1522,7 +2028,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
             "fit_all_stars_simultaneous fits only (y, x, flux) per star. Fix `bkg` (subtract the background first "
             "and pass `fixed = (; bkg = zero(eltype(image)))`), and fix all shape parameters."};
     if (fc.p == 0) throw ArgError{"all model parameters are fixed; nothing to fit"};
-    const int p = fc.p;
+    p = fc.p;
     fc.ky = fc.kx = -1;
     for (int k = 0; k < p; ++k) {
         if (fc.gc[k] == 1) fc.ky = k;
@@ -1536,32 +2042,31 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     fc.R = (int)std::ceil(P->fit_rad);
     fc.S = 2 * fc.R + 1;
     fc.S2 = fc.S * fc.S;
-    fc.VS = ((p * fc.S2 + 15) / 16) * 16;
     fc.q32 = 32 / fc.S;
     fc.r32 = 32 % fc.S;
     fc.ny = ny;
     fc.nx = nx;
     fc.nty = (ny + TY - 1) / TY;
     fc.ntx = (nx + TX - 1) / TX;
-    const int64_t ntiles = (int64_t)fc.nty * fc.ntx;
-    DevPsf dp = psf->dev;
+    ntiles = (int64_t)fc.nty * fc.ntx;
+    dp = psf->dev;
     dp.fwhm = P->fixed_fwhm;
 
     check(cudaEventRecord(ctx->ev0, st), "event");
     // device-resident scalars and reducers
-    Scalars* sc = S<Scalars>(ctx, "scalars", 1);
+    sc = S_<Scalars>("scalars", 1);
     check(cudaMemsetAsync(sc, 0, sizeof(Scalars), st), "memset");
     const int64_t max_blocks = std::max<int64_t>(ntiles, nblk(std::max<int64_t>(n_stars * 3, npix)) + 1);
-    Reducer red{S<double>(ctx, "red_partials", max_blocks), S<unsigned>(ctx, "red_counter", 1)};
+    red = Reducer{S_<double>("red_partials", max_blocks), S_<unsigned>("red_counter", 1)};
     check(cudaMemsetAsync(red.counter, 0, sizeof(unsigned), st), "memset");
-    Scalars* h_sc = (Scalars*)ctx->pinned;
+    h_sc = (Scalars*)ctx->pinned;
 
     // ---- data and weights (:1056-1084)
-    double* data = S<double>(ctx, "data", npix);
-    double* data_work = S<double>(ctx, "data_work", npix);
-    double* w = S<double>(ctx, "w", npix);
-    double* sw = S<double>(ctx, "sw", npix);
-    unsigned* flags = S<unsigned>(ctx, "flags", 4);
+    data = S_<double>("data", npix);
+    data_work = S_<double>("data_work", npix);
+    w = S_<double>("w", npix);
+    sw = S_<double>("sw", npix);
+    unsigned* flags = S_<unsigned>("flags", 4);
     check(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned), st), "memset");
     if (eltype == CPB_F64)
         k_prepare<double><<<nblk(npix), 256, 0, st>>>((const double*)d_image, (const double*)d_inv_var,
@@ -1573,20 +2078,20 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     check(cudaGetLastError(), "k_prepare");
 
     // ---- _build_stamps! (:245-323)
-    int32_t* ay_c = S<int32_t>(ctx, "ay_c", n_stars);
-    int32_t* ax_c = S<int32_t>(ctx, "ax_c", n_stars);
-    uint8_t* ok = S<uint8_t>(ctx, "ok", n_stars);
-    uint64_t* key = S<uint64_t>(ctx, "key", n_stars);
+    int32_t* ay_c = S_<int32_t>("ay_c", n_stars);
+    int32_t* ax_c = S_<int32_t>("ax_c", n_stars);
+    uint8_t* ok = S_<uint8_t>("ok", n_stars);
+    uint64_t* key = S_<uint64_t>("key", n_stars);
     k_anchor<<<nblk(n_stars), 256, 0, st>>>(n_stars, d_y0, d_x0, d_flux0, fc.R, ny, nx, w, ay_c, ax_c, ok, key,
                                             flags + 1);
     check(cudaGetLastError(), "k_anchor");
     // compact active stars in catalogue order, then stable radix sort by Morton key
-    int32_t* iota = S<int32_t>(ctx, "iota", n_stars);
-    int32_t* sel = S<int32_t>(ctx, "sel", n_stars);
-    uint64_t* selkey = S<uint64_t>(ctx, "selkey", n_stars);
-    uint64_t* selkey2 = S<uint64_t>(ctx, "selkey2", n_stars);
-    int32_t* act = S<int32_t>(ctx, "act", n_stars);
-    int* d_nsel = S<int>(ctx, "nsel", 1);
+    int32_t* iota = S_<int32_t>("iota", n_stars);
+    int32_t* sel = S_<int32_t>("sel", n_stars);
+    uint64_t* selkey = S_<uint64_t>("selkey", n_stars);
+    uint64_t* selkey2 = S_<uint64_t>("selkey2", n_stars);
+    act = S_<int32_t>("act", n_stars);
+    int* d_nsel = S_<int>("nsel", 1);
     {
         std::vector<int32_t> h_iota(n_stars);
         for (int64_t i = 0; i < n_stars; ++i) h_iota[i] = (int32_t)i;
@@ -1610,14 +2115,15 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         throw ArgError{
             "the image contains non-finite values but `inv_var` was not provided; pass `inv_var` to mask them or "
             "clean the image first"};
-    const int64_t n_act = h_nsel;
-    const int n_failed = (int)(n_stars - n_act);
+    n_act = h_nsel;
+    n_failed = (int)(n_stars - n_act);
     out->n_active = n_act;
     if (n_act == 0) {  // _empty_simultaneous_result (:1433-1445)
         std::vector<double> y(n_stars), x(n_stars), f(n_stars);
-        check(cudaMemcpy(y.data(), d_y0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
-        check(cudaMemcpy(x.data(), d_x0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
-        check(cudaMemcpy(f.data(), d_flux0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost), "d2h");
+        check(cudaMemcpyAsync(y.data(), d_y0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaMemcpyAsync(x.data(), d_x0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaMemcpyAsync(f.data(), d_flux0, sizeof(double) * n_stars, cudaMemcpyDeviceToHost, st), "d2h");
+        check(cudaStreamSynchronize(st), "sync");
         for (int64_t i = 0; i < n_stars; ++i) {
             out->y[i] = y[i];
             out->x[i] = x[i];
@@ -1636,7 +2142,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         out->n_passes = 0;
         out->n_failed = (int32_t)n_stars;
         if (out->residual) std::fill(out->residual, out->residual + npix, 0.0);
-        return 0;
+        return false;
     }
     if (h_flags[1] > 0)
         throw ArgError{"InexactError: a star's integer anchor is negative (Morton key of a negative coordinate)"};
@@ -1647,24 +2153,23 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         cub::DeviceRadixSort::SortPairs(dtmp, tmp, selkey, selkey2, sel, act, (int)n_act, 0, 64, st);
         check(cudaGetLastError(), "sort");
     }
-    const int64_t n = (int64_t)p * n_act;
-    int32_t* ay = S<int32_t>(ctx, "ay", n_act);
-    int32_t* ax = S<int32_t>(ctx, "ax", n_act);
-    double* theta = S<double>(ctx, "theta", n);
+    n = (int64_t)p * n_act;
+    ay = S_<int32_t>("ay", n_act);
+    ax = S_<int32_t>("ax", n_act);
+    theta = S_<double>("theta", n);
     k_gather_active<<<nblk(n_act), 256, 0, st>>>(n_act, act, ay_c, ax_c, d_y0, d_x0, d_flux0, p,
                                                  make_int3(fc.gc[0], fc.gc[1], fc.gc[2]), ay, ax, theta);
     check(cudaGetLastError(), "k_gather_active");
 
     // ---- union of stamp pixels (:329-335)
-    uint8_t* umask = S<uint8_t>(ctx, "umask", npix);
+    umask = S_<uint8_t>("umask", npix);
     check(cudaMemsetAsync(umask, 0, npix, st), "memset");
-    int32_t* dbg_pix = out->dbg_pixels ? S<int32_t>(ctx, "dbg_pix", (int64_t)fc.S2 * n_act) : nullptr;
+    dbg_pix = out->dbg_pixels ? S_<int32_t>("dbg_pix", (int64_t)fc.S2 * n_act) : nullptr;
     k_union<<<(unsigned)n_act, 256, 0, st>>>(n_act, ay, ax, fc.R, ny, nx, w, umask, dbg_pix);
     check(cudaGetLastError(), "k_union");
-    unsigned long long* ucnt = S<unsigned long long>(ctx, "ucnt", 1);
+    unsigned long long* ucnt = S_<unsigned long long>("ucnt", 1);
     check(cudaMemsetAsync(ucnt, 0, sizeof(unsigned long long), st), "memset");
     k_count_u8<<<nblk(npix), 256, 0, st>>>(umask, npix, ucnt);
-    unsigned long long h_ucnt = 0;
     check(cudaMemcpyAsync(&h_ucnt, ucnt, sizeof(h_ucnt), cudaMemcpyDeviceToHost, st), "d2h");
     check(cudaStreamSynchronize(st), "sync");
     out->n_union = (int64_t)h_ucnt;
@@ -1673,10 +2178,7 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     if (P->model_rad_auto && !d_inv_var)
         throw ArgError{
             "model_rad=:auto requires inv_var (it needs a noise scale); pass inv_var or an explicit scalar model_rad"};
-    int model_R;                  // the largest model radius (sizes the model stamps)
-    int32_t* d_modelR = nullptr;  // per active slot when model_rad = :auto
-    std::vector<int32_t> h_modelR;
-    double model_box_sum = 0;     // sum over active stars of (2 R_j + 1)^2
+    double model_box_sum = 0;  // sum over active stars of (2 R_j + 1)^2
     if (P->model_rad_auto) {
         const int R_cap = (int)std::ceil(model_rad_max);
         // the noise sample w[1 : step : end] and the active stars' catalogue fluxes
@@ -1693,211 +2195,131 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         for (int64_t j = 0; j < n_act; ++j) fl[j] = f0[h_act_order[j]];
         model_radii_auto(psf, P->fixed_fwhm, P->model_rad_nsigma, fc.R, R_cap, wsamp, fl, h_modelR);
         model_R = *std::max_element(h_modelR.begin(), h_modelR.end());
-        d_modelR = S<int32_t>(ctx, "model_R", n_act);
+        d_modelR = S_<int32_t>("model_R", n_act);
         check(cudaMemcpyAsync(d_modelR, h_modelR.data(), sizeof(int32_t) * n_act, cudaMemcpyHostToDevice, st),
               "h2d model radii");
+        check(cudaStreamSynchronize(st), "sync");
         for (int32_t r : h_modelR) model_box_sum += (double)(2 * r + 1) * (2 * r + 1);
     } else {
         const int R_cap = (int)std::ceil(std::max(P->model_rad, P->fit_rad));
         model_R = std::min(std::max((int)std::ceil(P->model_rad), fc.R), R_cap);
         model_box_sum = (double)n_act * (2 * model_R + 1) * (2 * model_R + 1);
     }
-    const double mean_box = model_box_sum / (double)n_act;  // per-star render work (instrumentation)
-    const double dof = (double)std::max<int64_t>((int64_t)h_ucnt - n, 1);
+    Sm = 2 * model_R + 1;
+    mean_box = model_box_sum / (double)n_act;  // per-star render work (instrumentation)
+    dof = (double)std::max<int64_t>((int64_t)h_ucnt - n, 1);
 
     // ---- tile lists (fit box for J v; model box for renders)
-    TileLists tfit = build_tiles(ctx, "tfit", n_act, ay, ax, nullptr, fc.R, ny, nx, fc.nty, fc.ntx);
-    TileLists tmod = (model_R == fc.R && !d_modelR)
-                         ? tfit
-                         : build_tiles(ctx, "tmod", n_act, ay, ax, d_modelR, model_R, ny, nx, fc.nty, fc.ntx);
+    tfit = build_tiles(ctx, "tfit", n_act, ay, ax, nullptr, fc.R, ny, nx, fc.nty, fc.ntx);
+    tmod = (model_R == fc.R && !d_modelR)
+               ? tfit
+               : build_tiles(ctx, "tmod", n_act, ay, ax, d_modelR, model_R, ny, nx, fc.nty, fc.ntx);
 
-    // ---- working buffers (:1129-1166)
-    TS* V = S<TS>(ctx, "V", (int64_t)fc.VS * n_act);
-    double* cn = S<double>(ctx, "colnorm", n);
-    double* D = S<double>(ctx, "D", n);
-    double* bsc = S<double>(ctx, "b_scaled", n);
-    double* delta = S<double>(ctx, "delta", n);
-    double* dsc = S<double>(ctx, "delta_scaled", n);
-    double* xl = S<double>(ctx, "lsqr_x", n);
-    double* vt = S<double>(ctx, "lsqr_v", n);
-    double* wl = S<double>(ctx, "lsqr_w", n);
-    double* wt_resid = S<double>(ctx, "wt_resid", npix);
-    double* u = S<double>(ctx, "lsqr_u", npix);
-    StarCoef* coef = S<StarCoef>(ctx, "coef", n_act);
-    StarCoef* coefc = S<StarCoef>(ctx, "coef_cand", n_act);
-    uint8_t* live = S<uint8_t>(ctx, "live", n_act);
-    uint8_t* newf = S<uint8_t>(ctx, "newf", n_act);
-    uint8_t* conv = S<uint8_t>(ctx, "conv", n_act);
-    int32_t* frozen_at = S<int32_t>(ctx, "frozen_at", n_act);
-    int32_t* live_list = S<int32_t>(ctx, "live_list", n_act);
-    int32_t* iota_act = S<int32_t>(ctx, "iota_act", n_act);
-    int* d_nlive = S<int>(ctx, "nlive", 1);
+    // ---- solver state (:1129-1166)
+    cn = S_<double>("colnorm", n);
+    D = S_<double>("D", n);
+    bsc = S_<double>("b_scaled", n);
+    delta = S_<double>("delta", n);
+    dsc = S_<double>("delta_scaled", n);
+    xl = S_<double>("lsqr_x", n);
+    vt = S_<double>("lsqr_v", n);
+    wl = S_<double>("lsqr_w", n);
+    coef = S_<StarCoef>("coef", n_act);
+    coefc = S_<StarCoef>("coef_cand", n_act);
+    live = S_<uint8_t>("live", n_act);
+    newf = S_<uint8_t>("newf", n_act);
+    conv = S_<uint8_t>("conv", n_act);
+    frozen_at = S_<int32_t>("frozen_at", n_act);
+    live_list = S_<int32_t>("live_list", n_act);
+    iota_act = S_<int32_t>("iota_act", n_act);
+    evlist = S_<int32_t>("eval_list", n_act);
+    d_nlive = S_<int>("nlive", 1);
     check(cudaMemsetAsync(live, 1, n_act, st), "memset");
     check(cudaMemsetAsync(conv, 0, n_act, st), "memset");
     check(cudaMemsetAsync(frozen_at, 0, sizeof(int32_t) * n_act, st), "memset");
     check(cudaMemsetAsync(cn, 0, sizeof(double) * n, st), "memset");
-    check(cudaMemsetAsync(V, 0, sizeof(TS) * (int64_t)fc.VS * n_act, st), "memset");
     check(cudaMemcpyAsync(iota_act, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
-    int64_t n_live = n_act;
+    n_live = n_act;
     check(cudaMemcpyAsync(live_list, iota, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
-    size_t live_tmp_bytes = 0;
+    live_tmp_bytes = 0;
     cub::DeviceSelect::Flagged(nullptr, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
-    void* live_tmp = scratch(ctx, "live_tmp", live_tmp_bytes);
+    live_tmp = scratch(ctx, "live_tmp", live_tmp_bytes);
 
-    const int fill_blocks = (int)std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16);
-    // per-star model values of the render box: one block of MS per star, or with
-    // per-star radii (:auto) each star's own (2 R_j + 1)^2 block at moff[j]
-    const int Sm = 2 * model_R + 1;
-    const int MS = ((Sm * Sm + 15) / 16) * 16;
-    int64_t* d_moff = nullptr;
-    int64_t mtotal = (int64_t)MS * n_act;
-    if (d_modelR) {
-        std::vector<int64_t> h_moff(n_act);
-        mtotal = 0;
-        for (int64_t j = 0; j < n_act; ++j) {
-            h_moff[j] = mtotal;
-            const int64_t sj = 2 * (int64_t)h_modelR[j] + 1;
-            mtotal += (sj * sj + 15) / 16 * 16;
-        }
-        d_moff = S<int64_t>(ctx, "model_off", n_act);
-        check(cudaMemcpyAsync(d_moff, h_moff.data(), sizeof(int64_t) * n_act, cudaMemcpyHostToDevice, st), "h2d");
-    }
-    TS* Mbuf = S<TS>(ctx, "model_stamps", mtotal);
-    constexpr double bts = sizeof(TS);  // bytes per stored stamp / model value
-    int32_t* evlist = S<int32_t>(ctx, "eval_list", n_act);
-    const size_t tab_bytes = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN ? 0 : (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
-    bool m_fresh = false;  // Mbuf holds the current-theta model of the live stars (written by the fill)
-    const bool warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
-    // model-value launches of the warp kernel: as many warps a block as their
-    // row / column tables fit in shared memory (large :auto model boxes use fewer)
-    int smem_optin = 0;
+    warp_eval = dp.kind == CPB_PSF_CIRCULAR_GAUSSIAN || dp.n_nodes == 1;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device), "attr");
-    // warps per block of a k_eval_warp launch whose per-warp axis tables (2 Sx
-    // entries) fit the opt-in shared memory
-    auto warp_shape = [&](int Sx, size_t tab_size, unsigned& threads, size_t& smem) {
-        int warps = 8;
-        while (warps > 1 && (size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin) warps /= 2;
-        if ((size_t)warps * 2 * Sx * tab_size > (size_t)smem_optin)
-            throw ArgError{"radius too large for the B200 stamp kernels"};
-        threads = 32u * warps;
-        smem = (size_t)warps * 2 * Sx * tab_size;
-    };
-    auto model_warp_shape = [&](size_t tab_size, unsigned& threads, size_t& smem) {
-        warp_shape(Sm, tab_size, threads, smem);
-    };
-    auto eval_grid = [&](int64_t nlist) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16)); };
-    auto launch_fill = [&](const int32_t* list, int64_t nlist, double* gram) {
-        if (nlist <= 0) return;
-        const bool writeM = !gram && model_R == fc.R && !d_modelR;
-        KernelScope ks_(ctx, gram ? "k_eval_gram" : "k_eval_fill",
-                        (double)nlist * ((gram ? 48.0 : (double)p * fc.S2 * bts + p * 8) + (writeM ? fc.S2 * bts : 0.0) +
-                                         std::min<double>((double)fc.S2, (double)h_ucnt / std::max<int64_t>(n_act, 1)) * 16 +
-                                         sizeof(StarCoef)));
-        const size_t smem = tab_bytes * fc.S;
-        TS* Mo = writeM ? Mbuf : nullptr;
-        if (warp_eval) {
-            unsigned thr;
-            size_t sm_bytes;
-            warp_shape(fc.S, sizeof(AxisTab<TS>), thr, sm_bytes);
-            if (sm_bytes > 48 * 1024)
-                check(cudaFuncSetAttribute(k_eval_warp<true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm_bytes), "smem attr");
-            const int wpb = (int)(thr / 32);
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn, gram, Mo, fc.R, MS, nullptr, nullptr);
-        } else {
-            launch_k_eval<true, TS>(fc.S2, eval_grid(nlist), smem, st, list, nlist, fc, dp, coef, ay, ax, w, sw, V, cn,
-                                    gram, Mo, fc.R, MS, (const int32_t*)nullptr, (const int64_t*)nullptr);
-        }
-        check(cudaGetLastError(), "k_eval_fill");
-        m_fresh = writeM;
-    };
-    (void)fill_blocks;
-    // model values at `cf` for the stars of `list` into Mbuf (value-only stamp evaluation)
-    auto launch_eval_model = [&](const int32_t* list, int64_t nlist, const StarCoef* cf) {
-        if (nlist <= 0) return;
-        KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * bts + sizeof(StarCoef)));
-        const size_t smem = tab_bytes * Sm;
-        const unsigned gb = eval_grid(nlist);
-        if (warp_eval) {
-            unsigned thr;
-            size_t sm_bytes;
-            model_warp_shape(sizeof(AxisTab<TS>), thr, sm_bytes);
-            if (sm_bytes > 48 * 1024)
-                check(cudaFuncSetAttribute(k_eval_warp<false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm_bytes), "smem attr");
-            const int wpb = (int)(thr / 32);
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn, nullptr, Mbuf, model_R, MS, d_modelR, d_moff);
-        } else {
-            launch_k_eval<false, TS>((int64_t)Sm * Sm, gb, smem, st, list, nlist, fc, dp, cf, ay, ax, w, sw, V, cn,
-                                     (double*)nullptr, Mbuf, model_R, MS, (const int32_t*)d_modelR,
-                                     (const int64_t*)d_moff);
-        }
-        check(cudaGetLastError(), "k_eval_model");
-    };
-    auto launch_render = [&](int mode, const uint8_t* incl, const int32_t* list, int64_t nlist, const StarCoef* cf,
-                             double* outp, const double* ref, double* result) {
-        if (!(mode == MODE_CUR && m_fresh)) launch_eval_model(list, nlist, cf);
-        m_fresh = false;
-        const double px_bytes = mode == MODE_CUR ? 25.0 : (mode == MODE_CAND ? 17.0 : 16.0);
-        KernelScope ks_(ctx, mode == MODE_CUR ? "k_gather_resid" : (mode == MODE_CAND ? "k_gather_cost" :
-                                                   (mode == MODE_FREEZE ? "k_gather_freeze" : "k_gather_final")),
-                        (double)npix * px_bytes + (double)nlist * Sm * Sm * bts);
-        switch (mode) {
-            case MODE_CUR:
-                k_gather<KIND_M, MODE_CUR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
-                break;
-            case MODE_CAND:
-                k_gather<KIND_M, MODE_CAND, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
-                break;
-            case MODE_FREEZE:
-                k_gather<KIND_M, MODE_FREEZE, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
-                break;
-            default:
-                k_gather<KIND_M, MODE_FINAL, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, incl, Mbuf, model_R, MS, d_moff, nullptr, nullptr, 0.0, outp, umask, w, sw, ref, sc, red, result);
-        }
-        check(cudaGetLastError(), "k_gather");
-    };
-    auto update_live_list = [&]() {
-        cub::DeviceSelect::Flagged(live_tmp, live_tmp_bytes, iota_act, live, live_list, d_nlive, (int)n_act, st);
-        int h = 0;
-        check(cudaMemcpyAsync(&h, d_nlive, sizeof(int), cudaMemcpyDeviceToHost, st), "d2h");
-        check(cudaStreamSynchronize(st), "sync");
-        n_live = h;
-    };
-    const unsigned jt_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
-    auto read_scalars = [&]() {
-        check(cudaMemcpyAsync(h_sc, sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st), "d2h");
-        check(cudaStreamSynchronize(st), "sync");
-    };
-    double evals = 0.0, macs = 0.0;
+    jt_blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + 7) / 8, (int64_t)ctx->n_sm * 8));
+    lam = P->lambda_init;
+    if (ctx->arena) arena_precheck();
+    return true;
+}
 
-    // ---- initial fill and cost (:1171-1178)
-    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
-    launch_fill(live_list, n_live, nullptr);
-    launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
-    check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
-    evals += (double)n_live * (fc.S2 + mean_box);
-    bool fresh = true;  // V / wt_resid / cost are at the current theta and live set
-    double lam = P->lambda_init;
-    int n_run = 0;
-    int64_t n_trials = 0, n_lsqr = 0;
+// No-allocation entry point: with the active set and the model radii known,
+// the buffers of the precision forms and of the final pass must fit what is
+// left of the fixed region; refuse here, before the outer loop starts.
+void SimFit::arena_precheck() {
+    auto model_entries = [&](int gh) {
+        int64_t t = 0;
+        if (d_modelR) {
+            for (int32_t r : h_modelR) t += (int64_t)(2 * r + 1) * gran_rows(2 * r + 1, gh);
+        } else {
+            t = n_act * (int64_t)Sm * gran_rows(Sm, gh);
+        }
+        return t;
+    };
+    size_t need = 0;
+    auto form = [&](size_t ts, int gh) {
+        need += carve_size((size_t)p * fc.S * gran_rows(fc.S, gh) * n_act * ts) + carve_size(model_entries(gh) * ts) +
+                (d_modelR ? carve_size(8 * n_act) : 0) + 2 * carve_size(npix * ts);
+    };
+    if (P->precision == CPB_PREC_MIXED) {
+        form(sizeof(float), Gran<float>::H);
+        if (P->refine_iters > 0) form(sizeof(double), Gran<double>::H);
+    } else {
+        form(sizeof(double), Gran<double>::H);
+    }
+    need += carve_size(sizeof(Scalars)) + carve_size(live_tmp_bytes);  // scalars_freeze, newf_tmp
+    need += carve_size(48 * n_act) + carve_size(8 * n) + carve_size(8 * npix);
+    need += carve_size(model_entries(Gran<double>::H) * 8) + (d_modelR ? carve_size(8 * n_act) : 0);
+    need += carve_size(8 * kSpreadRuleLen) + carve_size(8 * spread_tab_len(fc.R)) + carve_size(56 * n_act);
+    const size_t used = (ctx->arena->used + 255) & ~size_t(255);
+    if (used + need > ctx->arena->cap)
+        throw ArgError{"field too large for the no-allocation entry point: needs about " +
+                       std::to_string((used + need + (1 << 20) - 1) >> 20) + " MiB of scratch, the static region holds " +
+                       std::to_string(ctx->arena->cap >> 20) + " MiB"};
+}
 
-    // ---- outer loop (:1186-1284)
-    for (int iter = 1; iter <= P->max_iter; ++iter) {
+// The outer Gauss-Newton loop (:1186-1284) over iterations it_first..it_last,
+// with the stamps, model values and LSQR pixel vectors of form F.  `initial`:
+// the first fill and cost of the fit (:1171-1178), which also start D.
+template <typename TS, typename TU>
+void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial) {
+    constexpr double bts = sizeof(TS), btu = sizeof(TU);
+    const FitConst& f = F.fc;
+    bool fresh = false;  // V / wt_resid / cost are at the current theta and live set
+    if (initial) {
+        launch_coef(nullptr, coef);
+        launch_fill(F, live_list, n_live);
+        launch_render(F, MODE_CUR, live, live_list, n_live, coef, F.wt_resid, nullptr, data_work, &sc->cost);
+        check(cudaMemcpyAsync(D, cn, sizeof(double) * n, cudaMemcpyDeviceToDevice, st), "d2d");
+        evals += (double)n_live * (fc.S2 + mean_box);
+        fresh = true;
+    }
+    for (int iter = it_first; iter <= it_last; ++iter) {
         if (!fresh) {
-            KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
-            launch_fill(live_list, n_live, nullptr);
-            launch_render(MODE_CUR, live, live_list, n_live, coef, wt_resid, data_work, &sc->cost);
+            launch_coef(nullptr, coef);
+            launch_fill(F, live_list, n_live);
+            launch_render(F, MODE_CUR, live, live_list, n_live, coef, F.wt_resid, nullptr, data_work, &sc->cost);
             evals += (double)n_live * (fc.S2 + mean_box);
         }
         fresh = false;
         // b_scaled = J' wt_resid (frozen stars stay 0)
         check(cudaMemsetAsync(bsc, 0, sizeof(double) * n, st), "memset");
         {
-            KernelScope ks_(ctx, "k_JT", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
-            k_JT<false, TS><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, wt_resid, bsc, sc, red);
+            KernelScope ks_(ctx, "k_JT",
+                            (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) +
+                                std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * btu);
+            k_JT<false, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, cn, F.wt_resid, bsc,
+                                                           sc, red);
         }
         check(cudaGetLastError(), "k_JT");
         macs += (double)n_live * fc.S2;
@@ -1910,8 +2332,9 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         const double cost = h_sc->cost;
         if (h_sc->gnorm <= P->g_tol) {
             k_freeze_all<<<nblk(n_act), 256, 0, st>>>(n_act, iter - 1, live, frozen_at, conv);
+            check(cudaGetLastError(), "k_freeze_all");
             n_run = iter - 1;
-            break;
+            return;
         }
         bool accepted = false, f_conv = false;
         for (int trial = 1; trial <= P->max_trials; ++trial) {
@@ -1944,12 +2367,20 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 }
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
-                        KernelScope ks_(ctx, "k_gather_Jv", (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * 8);
-                        k_gather<KIND_JV, MODE_LSQR, TS><<<(unsigned)ntiles, NT, 0, st>>>(fc, tfit.start, tfit.end, tfit.list, tfit.order, live, V, fc.R, fc.VS, nullptr, vt, it == 0 ? wt_resid : u, it == 0 ? -1.0 : 1.0, u, umask, w, sw, nullptr, sc, red, nullptr);
+                        KernelScope ks_(ctx, "k_gather_Jv",
+                                        (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * btu);
+                        k_gather<KIND_JV, MODE_LSQR, TS, TU>
+                            <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
+                            f, tfit.start, tfit.end, tfit.list, tfit.order, live, F.V, fc.R, f.VS, nullptr, vt, cn,
+                            it == 0 ? F.wt_resid : F.u, it == 0 ? -1.0 : 1.0, F.u, nullptr, umask, w, sw, nullptr, sc,
+                            red, nullptr);
                     }
                     {
-                        KernelScope ks_(ctx, "k_JT_lsqr", (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) + std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * 8);
-                        k_JT<true, TS><<<jt_blocks, 256, 0, st>>>(live_list, n_live, fc, ay, ax, V, u, vt, sc, red);
+                        KernelScope ks_(ctx, "k_JT_lsqr",
+                                        (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) +
+                                            std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * btu);
+                        k_JT<true, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, cn, F.u, vt,
+                                                                      sc, red);
                     }
                     {
                         KernelScope ks_(ctx, "k_lsqr_update", (double)n * 8 * 5);
@@ -1962,8 +2393,9 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 KernelScope ks_(ctx, "k_step", (double)n * 8 * 4);
                 k_step<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->max_step, xl, cn, delta, dsc);
             }
-            KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, delta, coefc);
-            launch_render(MODE_CAND, live, live_list, n_live, coefc, nullptr, data_work, &sc->cost_cand);
+            launch_coef(delta, coefc);
+            launch_render(F, MODE_CAND, live, live_list, n_live, coefc, (TU*)nullptr, nullptr, data_work,
+                          &sc->cost_cand);
             evals += (double)n_live * mean_box;
             read_scalars();
             n_lsqr += h_sc->iter;
@@ -1981,14 +2413,15 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 *h_sc = s2;
                 check(cudaMemcpyAsync(sc, h_sc, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
                 // C_r of the freeze test uses the cost at the start of this iteration
-                Scalars* scf = S<Scalars>(ctx, "scalars_freeze", 1);
+                Scalars* scf = S_<Scalars>("scalars_freeze", 1);
                 Scalars s3 = s2;
                 s3.cost = cost;
                 check(cudaMemcpyAsync(scf, &s3, sizeof(Scalars), cudaMemcpyHostToDevice, st), "h2d");
                 {
                     KernelScope ks_(ctx, "k_accept_freeze", (double)n * 8 * 7);
-                    k_accept_freeze<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->x_tol, P->g_tol, dof, iter, theta, delta,
-                                                            dsc, cn, D, bsc, live, newf, frozen_at, conv, scf);
+                    k_accept_freeze<<<nblk(n_act), 256, 0, st>>>(n_act, fc, P->x_tol, P->g_tol, dof, iter, theta,
+                                                                delta, dsc, cn, D, bsc, live, newf, frozen_at, conv,
+                                                                scf);
                 }
                 check(cudaGetLastError(), "k_accept_freeze");
                 int h_new = 0;
@@ -2001,14 +2434,15 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                     h_new = 0;
                 }
                 if (h_new > 0) {
-                    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
+                    launch_coef(nullptr, coef);
                     {
                         size_t tb = 0;
                         cub::DeviceSelect::Flagged(nullptr, tb, iota_act, newf, evlist, d_nlive, (int)n_act, st);
                         void* tmpb = scratch(ctx, "newf_tmp", tb);
                         cub::DeviceSelect::Flagged(tmpb, tb, iota_act, newf, evlist, d_nlive, (int)n_act, st);
                     }
-                    launch_render(MODE_FREEZE, newf, evlist, h_new, coef, data_work, nullptr, nullptr);
+                    launch_render(F, MODE_FREEZE, newf, evlist, h_new, coef, (TU*)nullptr, data_work, nullptr,
+                                  nullptr);
                     evals += (double)h_new * mean_box;
                     update_live_list();
                 }
@@ -2020,15 +2454,49 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         n_run = iter;
         if (f_conv) {
             k_freeze_all<<<nblk(n_act), 256, 0, st>>>(n_act, iter, live, frozen_at, conv);
-            break;
+            check(cudaGetLastError(), "k_freeze_all");
+            return;
         }
-        if (accepted && n_live == 0) break;
+        if (accepted && n_live == 0) return;
     }
+}
 
-    // ---- errors at the final theta, every active star (:1302-1329)
-    KernelScope(ctx, "k_coef", (double)n_act * (sizeof(StarCoef) + 3 * 8)), k_coef<<<nblk(n_act), 256, 0, st>>>(n_act, fc, dp, theta, nullptr, coef);
-    double* gram = S<double>(ctx, "gram", (int64_t)n_act * 6);
-    // the final pass (errors, residual, diagnostics) is FP64 for either precision form
+int SimFit::run() {
+    if (!setup()) return 0;
+    const bool mixed = P->precision == CPB_PREC_MIXED;
+    if (mixed) {
+        Form<float, float> F32 = make_form<float, float>("_f32");
+        outer_loop(F32, 1, P->max_iter, true);
+        if (P->refine_iters > 0) {
+            // FP64 refinement: every active star live again on the original
+            // data, from the mixed-precision parameters, with the same damping,
+            // scaling D and convergence tests (converged flags accumulate)
+            Form<double, double> F64 = make_form<double, double>("_f64");
+            check(cudaMemcpyAsync(data_work, data, sizeof(double) * npix, cudaMemcpyDeviceToDevice, st), "d2d");
+            check(cudaMemsetAsync(live, 1, n_act, st), "memset");
+            check(cudaMemcpyAsync(live_list, iota_act, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
+            n_live = n_act;
+            outer_loop(F64, n_run + 1, n_run + P->refine_iters, false);
+        }
+    } else {
+        Form<double, double> F64 = make_form<double, double>("_f64");
+        outer_loop(F64, 1, P->max_iter, true);
+    }
+    finish();
+    return 0;
+}
+
+// Errors (:1302-1329), the final render against the original data
+// (:1344-1356), the diagnostics and the result assembly (:1289-1300,
+// :1331-1337, :1404-1430); FP64 for either precision form.
+void SimFit::finish() {
+    const double NaN = std::numeric_limits<double>::quiet_NaN();
+    launch_coef(nullptr, coef);
+    double* gram = S_<double>("gram", (int64_t)n_act * 6);
+    FitConst f64 = fc;
+    f64.SR = gran_rows(fc.S, Gran<double>::H);
+    f64.PS = fc.S * f64.SR;
+    f64.VS = p * f64.PS;
     {
         KernelScope ks_(ctx, "k_eval_gram", (double)n_act * (48.0 + sizeof(StarCoef)));
         if (warp_eval) {
@@ -2039,48 +2507,39 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
                 check(cudaFuncSetAttribute(k_eval_warp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)sm_bytes), "smem attr");
             const int wpb = (int)(thr / 32);
-            const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, double><<<gbw, thr, sm_bytes, st>>>(
-                nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, gram, nullptr, fc.R, MS, nullptr, nullptr);
+            const unsigned gbw =
+                (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
+            k_eval_warp<true, double><<<gbw, thr, sm_bytes, st>>>(nullptr, n_act, f64, dp, coef, ay, ax, w, sw,
+                                                                  nullptr, cn, gram, nullptr, fc.R, 0, nullptr,
+                                                                  nullptr);
         } else {
-            launch_k_eval<true, double>(fc.S2, eval_grid(n_act), (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S,
-                                        st, (const int32_t*)nullptr, n_act, fc, dp, coef, ay, ax, w, sw, (double*)nullptr,
-                                        cn, gram, (double*)nullptr, fc.R, MS, (const int32_t*)nullptr,
-                                        (const int64_t*)nullptr);
+            const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
+            launch_k_eval<true, double>(fc.S2, grid, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S,
+                                        st, (const int32_t*)nullptr, n_act, f64, dp, coef, ay, ax, w, sw,
+                                        (double*)nullptr, cn, gram, (double*)nullptr, fc.R, 0,
+                                        (const int32_t*)nullptr, (const int64_t*)nullptr);
         }
         check(cudaGetLastError(), "k_eval_gram");
     }
-    double* err = S<double>(ctx, "err", n);
+    double* err = S_<double>("err", n);
     read_scalars();  // final cost
     k_errors<<<nblk(n_act), 256, 0, st>>>(n_act, p, gram, reweighted, dof, sc, err);
     check(cudaGetLastError(), "k_errors");
-    // ---- final render against the original data (:1344-1356) and diagnostics
-    double* resid = S<double>(ctx, "resid", npix);
+    // ---- final render against the original data (:1344-1356)
+    double* resid = S_<double>("resid", npix);
     {
-        double* M64 = std::is_same<TS, double>::value ? (double*)Mbuf : S<double>(ctx, "model_stamps64", mtotal);
-        {
-            KernelScope ks_(ctx, "k_eval_model", (double)n_act * ((double)Sm * Sm * 8 + sizeof(StarCoef)));
-            if (warp_eval) {
-                unsigned thr;
-                size_t sm_bytes;
-                model_warp_shape(sizeof(AxisTab<double>), thr, sm_bytes);
-                if (sm_bytes > 48 * 1024)
-                    check(cudaFuncSetAttribute(k_eval_warp<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)sm_bytes), "smem attr");
-                const int wpb = (int)(thr / 32);
-                const unsigned gbw = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-                k_eval_warp<false, double><<<gbw, thr, sm_bytes, st>>>(
-                    nullptr, n_act, fc, dp, coef, ay, ax, w, sw, nullptr, cn, nullptr, M64, model_R, MS, d_modelR, d_moff);
-            } else {
-                const size_t sm_ = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * Sm;
-                launch_k_eval<false, double>((int64_t)Sm * Sm, eval_grid(n_act), sm_, st, (const int32_t*)nullptr, n_act,
-                                             fc, dp, coef, ay, ax, w, sw, (double*)nullptr, cn, (double*)nullptr, M64,
-                                             model_R, MS, (const int32_t*)d_modelR, (const int64_t*)d_moff);
-            }
-            check(cudaGetLastError(), "k_eval_model");
-        }
+        int MS64;
+        int64_t* moff64;
+        int64_t mtot64;
+        model_layout<double>("_final", MS64, moff64, mtot64);
+        double* M64 = S_<double>("model_stamps_final", mtot64);
+        check(cudaMemsetAsync(M64, 0, sizeof(double) * mtot64, st), "memset");
+        launch_eval_model<double>(f64, M64, MS64, moff64, nullptr, n_act, coef);
         KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
-        k_gather<KIND_M, MODE_FINAL, double><<<(unsigned)ntiles, NT, 0, st>>>(fc, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, MS, d_moff, nullptr, nullptr, 0.0, resid, umask, w, sw, data, sc, red, nullptr);
+        k_gather<KIND_M, MODE_FINAL, double, double>
+            <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
+            f64, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, MS64, moff64, nullptr, nullptr,
+            nullptr, 0.0, nullptr, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
     // spread_model reference disk, on the device: its width comes from the first
@@ -2094,8 +2553,8 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         (smode = spread_mode(boxmax, kh)) != 0) {
         double h_rule[kSpreadRuleLen];
         spread_rule(h_rule);
-        double* d_rule = S<double>(ctx, "spread_rule", kSpreadRuleLen);
-        d_stab = S<double>(ctx, "spread_tab", spread_tab_len(kh));
+        double* d_rule = S_<double>("spread_rule", kSpreadRuleLen);
+        d_stab = S_<double>("spread_tab", spread_tab_len(kh));
         check(cudaMemcpyAsync(d_rule, h_rule, sizeof(h_rule), cudaMemcpyHostToDevice, st), "h2d");
         int ky = -1, kx = -1;
         for (int k = 0; k < p; ++k) {
@@ -2108,10 +2567,11 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
         k_spread_disk<<<1, 256, sizeof(double) * (7 + kh) * kSpreadGL, st>>>(
             ps, sp_param, kh, theta, act, n_act, p, ky, kx, P->fixed_y, P->fixed_x, d_y0, d_x0, d_rule, d_stab);
         check(cudaGetLastError(), "k_spread_disk");
+        check(cudaStreamSynchronize(st), "sync");  // h_rule is a stack buffer
     }
     const size_t diag_smem = spread_smem_bytes(smode, boxmax, kh);
     const unsigned dgrid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
-    double* diag = S<double>(ctx, "diag", (int64_t)n_act * 7);
+    double* diag = S_<double>("diag", (int64_t)n_act * 7);
     {
         KernelScope ks_(ctx, "k_diag",
                         (double)n_act * boxmax * (8.0 + (d_inv_var ? 2.0 : 1.0) * (eltype == CPB_F64 ? 8 : 4)));
@@ -2230,19 +2690,16 @@ int fit_sim_impl(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, cons
     out->n_lsqr_iters = n_lsqr;
     out->model_px_evals = evals;
     out->lsqr_px_macs = macs;
-    return 0;
 }
+
+}  // namespace
 
 int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, const void* d_image,
                          int32_t eltype, int64_t ny, int64_t nx, const void* d_inv_var, const void* d_background,
                          int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out) {
-    if (P->precision == CPB_PREC_MIXED)
-        return fit_sim_impl<float>(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0,
-                                   d_flux0, out);
-    if (P->precision != CPB_PREC_FP64) throw ArgError{"precision must be CPB_PREC_FP64 or CPB_PREC_MIXED"};
-    return fit_sim_impl<double>(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0,
-                                d_flux0, out);
+    SimFit fit(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0, d_flux0, out);
+    return fit.run();
 }
 
 }  // namespace cpb

@@ -132,7 +132,12 @@ typedef struct cpb_sim_params {
     int32_t precision;        /* CPB_PREC_* */
     int32_t solver;           /* CPB_SOLVER_* */
     int32_t damping;          /* CPB_DAMP_* */
-    int32_t reserved;
+    /* precision == CPB_PREC_MIXED only: FP64 refinement iterations after the
+     * FP32-stamp loop (every active star live again on the original data, from
+     * the mixed-precision parameters, same damping and tests; converged flags
+     * accumulate).  0 = none: the final FP64 pass then only re-evaluates
+     * errors, residual and diagnostics at the mixed-precision parameters. */
+    int32_t refine_iters;
     /* spread_model reference disk FWHM: NaN = from the PSF's effective area
      * (the reference default, _spread_fwhm); <= 0 = skip spread_model */
     double spread_model_fwhm;
@@ -296,18 +301,23 @@ CPB_API int cpb_fit_simultaneous_device(cpb_ctx* ctx, const cpb_psf* psf, const 
 
 /*
  * No-allocation form of cpb_fit_simultaneous_device.  It has no counterpart in
- * the reference: it exists for callers that cannot allocate device memory
- * while they fit -- code inside a CUDA stream capture, hosts whose device
- * memory belongs to another allocator's pool, latency-critical loops.  It
+ * the reference.  It exists for callers that cannot allocate device memory
+ * while they fit: hosts whose device memory belongs to another allocator's
+ * pool (CUDA.jl's pool allocator in Julia, PyTorch's caching allocator),
+ * where a cudaMalloc behind the pool's back can fail or fragment the pool,
+ * and loops that cannot take cudaMalloc's implicit device synchronisation.  It
  * allocates nothing: all scratch comes from one static 64 MiB device region
  * the library holds on each GPU that uses it until the process exits.  Fields
  * whose scratch would exceed that region (roughly beyond 512 x 512 pixels with
  * a few thousand 25 x 25 stamps) are rejected with CPB_ERR_ARGUMENT and a
- * message naming the size.  The first call on a device looks up the region's
- * address (cudaGetSymbolAddress); make that call before any stream capture.
- * All calls share the region and find the previous call's contents in it
- * (the fit clears what must start at zero); calls whose GPU work overlaps
- * race on it, so serialise them.  The context must already exist.
+ * message naming the size ("too large for the no-allocation entry point"),
+ * before the fit's outer loop starts.  The first call on a device looks up
+ * the region's address (cudaGetSymbolAddress); make that call before any
+ * stream capture, and do not use this entry point on a device after a
+ * cudaDeviceReset of it (the looked-up address would be stale).  All calls
+ * share the region and find the previous call's contents in it (the fit
+ * clears what must start at zero); calls whose GPU work overlaps race on it,
+ * so serialise them.  The context must already exist.
  */
 CPB_API int cpb_fit_simultaneous_device_noalloc(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* params,
                                                 const void* d_image, int32_t eltype, int64_t ny, int64_t nx,

@@ -1,13 +1,17 @@
 """The no-allocation simultaneous fit (cpb_fit_simultaneous_device_noalloc).
 
-It serves callers that cannot allocate device memory during a fit (inside a
-stream capture, under another allocator's pool); all of its scratch lives in a
-static 64 MiB device region shared by every call.  This checks, through the
-C-ABI, that two calls in a row (the second one finding the first one's data
-in the shared region) give the same stars as the allocating entry point
+It serves callers that cannot allocate device memory during a fit: hosts whose
+GPU memory belongs to another allocator's pool (CUDA.jl, PyTorch), where a
+cudaMalloc behind the pool's back can fail or fragment it, and loops that
+cannot take cudaMalloc's implicit synchronisation.  All of its scratch lives
+in a static 64 MiB device region shared by every call.  This checks, through
+the C-ABI, that two calls in a row (the second one finding the first one's
+data in the shared region) give the same stars as the allocating entry point
 within the parity tolerances used everywhere else (1e-4 px, 1e-5 relative
-flux), and that an oversized field is refused with a clear message.
-Collected last so a failure here never hides the other GPU tests.
+flux), and that fields around the region's limit -- scalar model radii above
+the fit radius and :auto radii included -- either fit or are refused with the
+up-front message, never part-way through carving.  Collected last so a
+failure here never hides the other GPU tests.
 """
 import ctypes as C
 
@@ -106,3 +110,34 @@ def test_noalloc_rejects_oversized_field():
                                                      C.byref(outs.c))
     assert rc == _abi.CPB_ERR_ARGUMENT
     assert "too large for the no-allocation entry point" in ctx.error()
+
+
+@pytest.mark.parametrize("model_rad", [12, 20, "auto"])
+def test_noalloc_fields_around_the_limit_fit_or_are_refused_up_front(model_rad):
+    import torch
+
+    import crowdphot_b200 as cpb
+    from crowdphot_b200 import _abi
+    from crowdphot_b200.photometry import SimOutputs, sim_params
+    from crowdphot_b200.simulate import crowded_field, moffat_epsf
+    ctx = cpb.get_context(0)
+    psf = moffat_epsf()
+    hp = ctx.psf_handle(psf)
+    seen = set()
+    for side, n in ((256, 700), (384, 1500), (448, 2200), (512, 2800), (512, 3600), (640, 5000)):
+        img, bkg, iv, truth, init = crowded_field(side, side, n, seed=3000 + side + n, psf=psf, dtype=np.float32)
+        t = _device_inputs(torch, img, iv, bkg, init)
+        P = sim_params(psf, 12, {"bkg": 0.0}, inv_var_given=True, model_rad=model_rad, max_iter=2)
+        outs = SimOutputs(n, side, side, 625, residual=False)
+        vp = lambda x: C.c_void_p(x.data_ptr())
+        rc = ctx.lib.cpb_fit_simultaneous_device_noalloc(ctx.handle, hp, C.byref(P), vp(t[0]), _abi.CPB_F64, side,
+                                                         side, vp(t[1]), vp(t[2]), n, vp(t[3]), vp(t[4]), vp(t[5]),
+                                                         C.byref(outs.c))
+        if rc == 0:
+            seen.add("fit")
+            assert outs.valid[:n].any()
+        else:
+            assert rc == _abi.CPB_ERR_ARGUMENT, ctx.error()
+            assert "too large for the no-allocation entry point" in ctx.error(), ctx.error()
+            seen.add("refused")
+    assert seen == {"fit", "refused"}, seen
