@@ -40,10 +40,11 @@ N_STARS = 50_000
 FIT_RAD = 12
 SEED = 1002
 SAMPLE = 512  # CPU sample side (same star density)
-# DRAM bytes moved per algorithmic byte by the J v gather (read + write 226.9 MB against
-# 204.6 MB algorithmic), from an ncu capture of the same kernel on a 1024^2 field with
-# the same star density, PSF and radii (its first LSQR launch, every star live)
-JV_TRAFFIC_RATIO = 226.9 / 204.6
+# DRAM bytes moved per algorithmic byte by the FP64 J v gather (read + write 266.8 MB
+# against 204.6 MB algorithmic), from an ncu capture of the same kernel on a 1024^2
+# field with the same star density, PSF and radii (an LSQR launch of the first outer
+# iteration, every star live)
+JV_TRAFFIC_RATIO = 266.8 / 204.6
 
 
 def workload_config(ny=NY, nx=NX, n=N_STARS):
@@ -146,6 +147,44 @@ def cpu_baseline_single():
                       f"{dt:.1f} s"}
 
 
+def _full_field_oracle(ny, nx, n, seed):
+    """The FP64 oracle on the whole bench field (the C2-size parity check); runs in
+    a spawned process while the GPU legs are timed."""
+    from oracle import orc_fit_simultaneous
+    psf, img, bkg, iv, truth, init = make_field(ny, nx, n, seed)
+    t = time.perf_counter()
+    r = orc_fit_simultaneous(img, psf, init, FIT_RAD, inv_var=iv, background=bkg, residual=False, **fit_kwargs())
+    dt = time.perf_counter() - t
+    return dict(y=r.y, x=r.x, flux=r.flux, flux_err=r.flux_err, valid=r.valid, converged=r.converged,
+                n_iter=r.n_iter, n_passes=r.n_passes, n_active=r.stats["n_active"], n_union=r.stats["n_union"],
+                seconds=dt)
+
+
+FLUX_GATE, POS_GATE = 1e-5, 1e-4
+
+
+def deviation(a, b, mask):
+    """Per-output deviation of fit a from fit b over `mask`: relative flux, position
+    (max of |dy|, |dx|) and flux in units of b's flux error."""
+    if not mask.any():
+        return None
+    dfl = np.abs(a["flux"][mask] / b["flux"][mask] - 1)
+    dpos = np.maximum(np.abs(a["y"][mask] - b["y"][mask]), np.abs(a["x"][mask] - b["x"][mask]))
+    dsig = np.abs(a["flux"][mask] - b["flux"][mask]) / b["flux_err"][mask]
+    q = lambda v: {"median": float(np.median(v)), "p99": float(np.percentile(v, 99)), "max": float(v.max())}
+    bad = (dfl > FLUX_GATE) | (dpos > POS_GATE)
+    return {"stars": int(mask.sum()), "flux_rel": dict(q(dfl), frac_within_gate=float(np.mean(dfl <= FLUX_GATE))),
+            "pos_px": dict(q(dpos), frac_within_gate=float(np.mean(dpos <= POS_GATE))),
+            "flux_in_sigma": q(dsig), "violators": int(bad.sum())}
+
+
+def fitted_mask(*rs):
+    m = np.ones_like(rs[0]["valid"], dtype=bool)
+    for r in rs:
+        m &= r["valid"].astype(bool) & r["converged"].astype(bool)
+    return m
+
+
 def run_reference(args):
     import multiprocessing as mp
     cores = os.cpu_count() or 1
@@ -203,6 +242,11 @@ def run_gpu(args):
         torch.cuda.synchronize()
 
     ny, nx, n = args.ny, args.nx, args.n_stars
+    oracle_job = pool = None
+    if world == 1 and not args.quick and not args.no_cpu:
+        import multiprocessing as mp
+        pool = mp.get_context("spawn").Pool(1)
+        oracle_job = pool.apply_async(_full_field_oracle, (ny, nx, n, replica_seed(SEED, rank)))
     psf, img, bkg, iv, truth, init = make_field(ny, nx, n, replica_seed(SEED, rank))
     ctx = cpb.get_context(local)
     hp = ctx.psf_handle(psf)
@@ -259,37 +303,78 @@ def run_gpu(args):
     total_s, fitted_all, launches_all = mx[0], sm[1], int(sm[2])
     value = fitted_all / total_s
 
-    # mixed-precision form: same protocol, and its per-output deviation from the
-    # FP64 form (which tracks the FP64 oracle to ~1e-12 on the parity cases)
-    Pm = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD, precision="mixed")
-    outs_m = SimOutputs(n, ny, nx, S2, residual=False)
-    for _ in range(args.warmup):
-        step_resident(Pm, outs_m)
-        flush.fill_(1.0)
-    barrier()
-    m_fitted, m_times = 0, []
-    for _ in range(args.steps):
+    # the other precision forms, same protocol: the mixed-precision form (FP32
+    # stamps, model values and LSQR pixel vectors, FP64 sums and solver) and the
+    # same followed by two FP64 refinement iterations
+    def take(o):
+        return {k: getattr(o, k)[:n].copy() for k in ("y", "x", "flux", "flux_err", "valid", "converged", "n_iter")}
+
+    def timed_form(Pf, steps):
+        o = SimOutputs(n, ny, nx, S2, residual=False)
+        for _ in range(args.warmup):
+            step_resident(Pf, o)
+            flush.fill_(1.0)
+        barrier()
+        fitted, times = 0, []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            f, s_ = step_resident(Pf, o)
+            fitted += f
+            times.append(s_)
+        barrier()
+        mx_, sm_ = max_and_sum_over_ranks([sum(times), fitted], dev)
+        ms = [1e3 * t for t in times]
+        return o, {"value": sm_[1] / mx_[0], "unit": "stars/s", "ms_per_step": float(np.mean(ms)),
+                   "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99))}
+
+    def kernel_table(Pf):
+        ctx.set_profiling(True)
         flush.fill_(1.0)
         torch.cuda.synchronize()
-        f, s_ = step_resident(Pm, outs_m)
-        m_fitted += f
-        m_times.append(s_)
-    barrier()
-    mx_, sm_ = max_and_sum_over_ranks([sum(m_times), m_fitted], dev)
-    m_value = sm_[1] / mx_[0]
-    ok = (outs.valid[:n] & outs.converged[:n] & outs_m.valid[:n] & outs_m.converged[:n] &
-          (outs.n_iter[:n] == outs_m.n_iter[:n])).astype(bool)
-    dfl = np.abs(outs_m.flux[:n][ok] / outs.flux[:n][ok] - 1)
-    dpos = np.maximum(np.abs(outs_m.y[:n][ok] - outs.y[:n][ok]), np.abs(outs_m.x[:n][ok] - outs.x[:n][ok]))
-    q = lambda a: {"median": float(np.median(a)), "p99": float(np.percentile(a, 99)), "max": float(a.max()),
-                   "frac_within_gate": None} if a.size else None
-    mixed = {"value": m_value, "unit": "stars/s", "ms_per_step": 1e3 * sum(m_times) / args.steps,
-             "p50_ms": float(np.percentile([1e3 * t for t in m_times], 50)),
-             "p99_ms": float(np.percentile([1e3 * t for t in m_times], 99)),
-             "compared_stars": int(ok.sum()), "flux_rel_dev_vs_fp64": q(dfl), "pos_dev_px_vs_fp64": q(dpos)}
-    if mixed["flux_rel_dev_vs_fp64"]:
-        mixed["flux_rel_dev_vs_fp64"]["frac_within_gate"] = float(np.mean(dfl <= 1e-5))
-        mixed["pos_dev_px_vs_fp64"]["frac_within_gate"] = float(np.mean(dpos <= 1e-4))
+        _, secs = step_resident(Pf, SimOutputs(n, ny, nx, S2, residual=False))
+        ctx.set_profiling(False)
+        kst_, _ = ctx.kernel_stats(reset=True)
+        return kst_, secs, {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
+                                "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst_.items())}
+
+    Pm = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD, precision="mixed")
+    outs_m, mixed = timed_form(Pm, args.steps)
+    mixed["kernels"] = kernel_table(Pm)[2]
+    Pr = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD, precision="mixed",
+                    refine_iters=2)
+    outs_r, refined = timed_form(Pr, max(1, min(args.steps, 5)))
+    # How far the FP64 form itself moves when the input moves by its own rounding:
+    # two fits of the image times (1 + 1e-7 N(0, 1)), rounded to the Float32 input
+    # (about one ulp on half of the pixels).  Stars that both move by less than a
+    # tenth of the gates (1e-6 relative flux, 1e-5 px) form the stable set, on which
+    # the other forms are held to the gates.
+    ref = take(outs)
+    pert = []
+    for k in range(2):
+        g = np.random.default_rng(SEED + 700 + k)
+        ip = (img.astype(np.float64) * (1 + 1e-7 * g.standard_normal(img.shape))).astype(img.dtype)
+        t_ip = torch.from_numpy(np.ascontiguousarray(ip.T)).to(dev)
+        o = SimOutputs(n, ny, nx, S2, residual=False)
+        rc = ctx.lib.cpb_fit_simultaneous_device(ctx.handle, hp, C.byref(P), vp(t_ip), _abi.CPB_F32, ny, nx,
+                                                 vp(t_iv), vp(t_bkg), n, vp(t_y), vp(t_x), vp(t_f), C.byref(o.c))
+        ctx.raise_for(rc, "cpb_fit_simultaneous_device")
+        pert.append(take(o))
+        del t_ip
+    fit_all = fitted_mask(ref, *pert)
+    stable = fit_all.copy()
+    for pr in pert:
+        dfl = np.abs(pr["flux"] / ref["flux"] - 1)
+        dpos = np.maximum(np.abs(pr["y"] - ref["y"]), np.abs(pr["x"] - ref["x"]))
+        stable &= (dfl <= 0.1 * FLUX_GATE) & (dpos <= 0.1 * POS_GATE)
+    conditioning = {
+        "perturbation": "image x (1 + 1e-7 N(0,1)) rounded to Float32, two draws, FP64 form",
+        "fitted_in_all": int(fit_all.sum()), "stable_set": int(stable.sum()),
+        "fp64_vs_perturbed": deviation(pert[0], ref, fitted_mask(ref, pert[0]))}
+    for name, o, blk in (("mixed", outs_m, mixed), ("mixed_refine2", outs_r, refined)):
+        r = take(o)
+        blk["vs_fp64_all_fitted"] = deviation(r, ref, fitted_mask(ref, r))
+        blk["vs_fp64_stable_set"] = deviation(r, ref, stable & fitted_mask(r))
 
     # profiling pass (not timed): per-kernel event timing and algorithmic bytes
     ctx.set_profiling(True)
@@ -307,7 +392,8 @@ def run_gpu(args):
     if top[0] == "k_gather_Jv":
         roof["traffic"] = JV_TRAFFIC_RATIO * top[1]["bytes"] / max(top[1]["launches"], 1)
         roof["traffic_note"] = ("bytes per launch: this run's algorithmic bytes per launch times the DRAM / "
-                                "algorithmic ratio of an ncu capture of the kernel on a 1024^2 field (1.109)")
+                                f"algorithmic ratio of an ncu capture of the kernel on a 1024^2 field "
+                                f"({JV_TRAFFIC_RATIO:.3f})")
     kernels = {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
                    "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst.items())}
 
@@ -343,10 +429,28 @@ def run_gpu(args):
                 "model_px_evals_per_s": float(outs.c.model_px_evals) / s_prof,
                 "roofline": roof, "kernels": kernels, "gpu_launches": launches_all, "clocks": clk,
                 "forms": {"plain_fp64": {"value": value, "ms_per_step": 1e3 * total_s / args.steps},
-                          "mixed": mixed},
+                          "mixed": mixed, "mixed_refine2": refined, "conditioning": conditioning},
                 "e2e": {"value": e_value, "unit": "stars/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline_single()
+        if oracle_job is not None:
+            orc = oracle_job.get(timeout=1800)
+            pool.close()
+            both = fitted_mask(ref, orc)
+            same = both & (ref["n_iter"] == orc["n_iter"])
+            line["parity_full_field"] = {
+                "what": "FP64 form vs the FP64 oracle on the whole bench field, same inputs",
+                "n_active_equal": int(outs.c.n_active) == int(orc["n_active"]),
+                "n_union_equal": int(outs.c.n_union) == int(orc["n_union"]),
+                "n_passes": [int(outs.c.n_passes), int(orc["n_passes"])],
+                "fitted_in_both": int(both.sum()), "same_freeze_iteration": int(same.sum()),
+                "same_freeze": deviation(ref, orc, same),
+                "freeze_differs": deviation(ref, orc, both & ~same),
+                "stable_set": deviation(ref, orc, both & stable)}
+            fitted_cpu = int((orc["valid"] & orc["converged"]).sum())
+            line["cpu_baseline"]["full_field"] = {
+                "value": fitted_cpu / orc["seconds"], "unit": "stars/s", "cores": 1,
+                "sample": f"the whole {ny}x{nx} field ({n} stars), one FP64 oracle fit, {orc['seconds']:.0f} s"}
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
