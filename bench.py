@@ -1158,6 +1158,85 @@ def run_gpu_mp(args):
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# The plain CPU-runnable configuration (--workload c1): 256^2 Float64, 200 stars,
+# CircularGaussianPSF FWHM 2.5, 15 x 15 boxes, 20 iterations, linear_tol 1e-8
+# ---------------------------------------------------------------------------
+C1_METRIC = "fitted stars/s on 1 B200, simultaneous fit of the 256^2 Gaussian field"
+C1_SEED = 1001
+
+
+def c1_config():
+    return {"workload": "256x256 Float64, 200 stars, CircularGaussianPSF FWHM 2.5, 15x15 boxes, max_iter 20, "
+                        "linear_tol 1e-8", "image": [256, 256], "n_stars": 200, "fit_rad": 7, "model_rad": 7,
+            "seed": C1_SEED, "l2": "the whole problem is L2-resident; launch and latency bound"}
+
+
+def _c1_kwargs(iv, bkg):
+    return dict(fixed={"fwhm": 2.5, "bkg": 0.0}, inv_var=iv, background=bkg, model_rad=7, max_iter=20,
+                linear_tol=1e-8)
+
+
+def _c1_cpu(seconds=10.0):
+    """The FP64 oracle on the C1 field, repeated for about `seconds` (one core)."""
+    from crowdphot_b200.simulate import c1_field
+    from oracle import orc_fit_simultaneous
+    img, bkg, iv, psf, src, init = c1_field(C1_SEED)
+    fits, fitted, t0 = 0, 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds or fits == 0:
+        r = orc_fit_simultaneous(img, psf, init, 7, residual=False, **_c1_kwargs(iv, bkg))
+        fits += 1
+        fitted += int((r.valid & r.converged).sum())
+    dt = time.perf_counter() - t0
+    return fitted / dt, fits, dt
+
+
+def run_reference_c1(args):
+    rate, fits, dt = _c1_cpu(max(5.0, 0.5 * (args.steps + args.warmup)))
+    line = {"impl": "reference", "metric": C1_METRIC, "value": rate, "unit": "stars/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / fits, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c1_config(),
+            "cpu_baseline": {"value": rate, "unit": "stars/s", "cores": 1, "kind": "port",
+                             "sample": f"{fits} fits of the whole C1 field, FP64 oracle, one core"},
+            "e2e": {"value": rate, "unit": "stars/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_gpu_c1(args):
+    import torch
+
+    import crowdphot_b200 as cpb
+    from crowdphot_b200.simulate import c1_field
+    img, bkg, iv, psf, src, init = c1_field(C1_SEED)
+    ctx = cpb.get_context(0)
+    kw = _c1_kwargs(iv, bkg)
+    for _ in range(args.warmup):
+        cpb.fit_all_stars_simultaneous(img, psf, init, 7, ctx=ctx, residual=False, **kw)
+    ctx.kernel_stats(reset=True)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    dev_s, walls, fitted = [], [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r = cpb.fit_all_stars_simultaneous(img, psf, init, 7, ctx=ctx, residual=False, **kw)
+        walls.append(time.perf_counter() - t0)
+        dev_s.append(r.stats["device_seconds"])
+        fitted += int((r.valid & r.converged).sum())
+    clk = clocks.stop()
+    _, launches = ctx.kernel_stats(reset=True)
+    line = {"metric": C1_METRIC, "value": fitted / sum(dev_s), "unit": "stars/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(dev_s)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c1_config(),
+            "gpu_launches": launches, "clocks": clk, "n_passes": int(r.n_passes),
+            "e2e": {"value": fitted / sum(walls), "unit": "stars/s", "h2d_bytes_per_step": 3 * img.nbytes + 3 * 8 * 200,
+                    "d2h_bytes_per_step": 200 * (12 * 8 + 2 + 4)}}
+    if not args.no_cpu:
+        rate, fits, dt = _c1_cpu()
+        line["cpu_baseline"] = {"value": rate, "unit": "stars/s", "cores": 1, "kind": "port",
+                                "sample": f"{fits} fits of the whole C1 field, FP64 oracle, one core, {dt:.1f} s"}
+    print(json.dumps(line))
+
+
 def C_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -1172,12 +1251,13 @@ def main():
     ap.add_argument("--ny", type=int, default=NY)
     ap.add_argument("--nx", type=int, default=NX)
     ap.add_argument("--n-stars", type=int, default=N_STARS)
-    ap.add_argument("--workload", choices=["crowded-field", "lm-cutouts", "c4", "serve", "multipass"],
+    ap.add_argument("--workload", choices=["crowded-field", "lm-cutouts", "c4", "serve", "multipass", "c1"],
                     default="crowded-field",
                     help="crowded-field: the simultaneous fit (headline); lm-cutouts: batched fit_star; "
                          "c4: fit_star cutouts + blended groups in one CUDA-graph launch; "
                          "serve: a Poisson request stream through the continuous-batching server; "
-                         "multipass: fit_all_stars (sequential passes run as batches of disjoint boxes)")
+                         "multipass: fit_all_stars (sequential passes run as batches of disjoint boxes); "
+                         "c1: the 256^2 Gaussian field of the CPU-runnable configuration")
     ap.add_argument("--n-groups", type=int, default=C4_GROUPS)
     ap.add_argument("--n-requests", type=int, default=24)
     ap.add_argument("--max-inflight", type=int, default=4)
@@ -1187,9 +1267,9 @@ def main():
                     help="only the warm-up and timed resident steps (for profiler captures); prints a short line")
     args = ap.parse_args()
     ref = {"crowded-field": run_reference, "lm-cutouts": run_reference_lm, "c4": run_reference_c4,
-           "serve": run_reference, "multipass": run_reference_mp}
+           "serve": run_reference, "multipass": run_reference_mp, "c1": run_reference_c1}
     gpu = {"crowded-field": run_gpu, "lm-cutouts": run_gpu_lm, "c4": run_gpu_c4, "serve": run_gpu_serve,
-           "multipass": run_gpu_mp}
+           "multipass": run_gpu_mp, "c1": run_gpu_c1}
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return

@@ -13,6 +13,8 @@ CPB_ERR_ARGUMENT = -1
 CPB_ERR_CUDA = -2
 CPB_ERR_OOM = -3
 CPB_ERR_TIMEOUT = -4
+CPB_FAULT_NONE = 0
+CPB_FAULT_HOLD_READY_STAR = 1
 CPB_ERR_INTERNAL = -5
 CPB_ERR_NO_DEVICE = -6
 
@@ -256,6 +258,8 @@ PROTOTYPES = {
     "cpb_last_error": (C.c_char_p, [C.c_void_p]),
     "cpb_version": (C.c_char_p, []),
     "cpb_ctx_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "cpb_ctx_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int64]),
+    "cpb_ctx_inject_fault": (C.c_int, [C.c_void_p, C.c_int32]),
     "cpb_ctx_kernel_stats": (C.c_int, [C.c_void_p, C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int),
                                        C.POINTER(C.c_int64), C.c_int]),
     "cpb_psf_upload": (C.c_int, [C.c_void_p, C.POINTER(PsfDesc), C.POINTER(C.c_void_p)]),

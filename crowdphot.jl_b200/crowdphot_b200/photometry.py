@@ -76,10 +76,21 @@ class Context:
             raise ArgumentError(msg)
         if rc == _abi.CPB_ERR_OOM:
             raise MemoryError(f"{what}: {msg}")
+        if rc == _abi.CPB_ERR_TIMEOUT:
+            raise TimeoutError(f"{what}: {msg}")
         raise CudaError(f"{what} failed ({rc}): {msg}")
 
     def set_profiling(self, enable: bool):
         self.raise_for(self.lib.cpb_ctx_set_profiling(self.handle, int(bool(enable))), "cpb_ctx_set_profiling")
+
+    def set_wait_limit(self, polls: int):
+        """Polls (of >= 64 ns) a bounded device wait makes before the call gives up
+        with CPB_ERR_TIMEOUT; <= 0 restores the default (2^26)."""
+        self.raise_for(self.lib.cpb_ctx_set_wait_limit(self.handle, int(polls)), "cpb_ctx_set_wait_limit")
+
+    def inject_fault(self, fault: int):
+        """One-shot host-side fault injection for tests (CPB_FAULT_*)."""
+        self.raise_for(self.lib.cpb_ctx_inject_fault(self.handle, int(fault)), "cpb_ctx_inject_fault")
 
     def kernel_stats(self, reset: bool = True):
         """Per-kernel launch counts, event-timed seconds and algorithmic bytes, plus
@@ -279,8 +290,9 @@ def sim_params(psf, fit_rad, fixed, *, inv_var_given, solver="lsqr", inner_itera
 
     refine_iters (precision="mixed" only): FP64 Gauss-Newton iterations after the
     FP32-stamp loop, every active star live again from the mixed-precision
-    parameters; 0 keeps the mixed-precision parameters and re-evaluates only the
-    errors, residual and diagnostics in FP64."""
+    parameters and the damping restarted at lambda_init; 0 keeps the
+    mixed-precision parameters and re-evaluates only the errors, residual and
+    diagnostics in FP64."""
     P = _abi.SimParams()
     P.spread_model_fwhm = spread_fwhm_arg(spread_model_fwhm)
     P.fit_rad = float(fit_rad)

@@ -386,3 +386,22 @@ def served_field(side, density, *, seed, psf=None, flux=(1e1, 1e6), flux_power=1
     init = dict(y=ys + rng.normal(0, init_sigma, n), x=xs + rng.normal(0, init_sigma, n),
                 flux=fs * rng.uniform(init_flux[0], init_flux[1], n))
     return img.astype(dtype), bkg.astype(dtype), inv_var.astype(dtype), src, init
+
+
+def c1_field(seed=1001, n=200, shape=(256, 256)):
+    """The plain CPU-runnable configuration: a Float64 image with n stars at
+    uniform sub-pixel positions, fluxes log-uniform 1e2-1e5, a CircularGaussianPSF
+    of FWHM 2.5 (15 x 15 boxes), flat background 100 + Poisson noise and
+    inverse-variance weights; initial guesses perturbed by N(0, 0.3 px) in y / x and
+    x U(0.9, 1.1) in flux.  Returns (image, background, inv_var, psf, sources, init)."""
+    from .psf import CircularGaussianPSF
+    rng = np.random.default_rng(seed)
+    psf = CircularGaussianPSF(fwhm=2.5)
+    src = simulate_sources(shape, n, rng=rng, flux=(1e2, 1e5), flux_distribution="loguniform")
+    model = np.zeros(shape)
+    render_sources(model, psf, src["y"], src["x"], src["flux"], model_radius=7)
+    img = add_noise(model + 100.0, rng=rng, noise="poisson", gain=1.0)
+    iv = 1.0 / (100.0 + model)
+    init = dict(y=src["y"] + rng.normal(0, 0.3, n), x=src["x"] + rng.normal(0, 0.3, n),
+                flux=src["flux"] * rng.uniform(0.9, 1.1, n))
+    return img, np.full(shape, 100.0), iv, psf, src, init

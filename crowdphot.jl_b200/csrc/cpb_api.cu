@@ -155,6 +155,21 @@ int cpb_ctx_set_profiling(cpb_ctx* ctx, int enable) {
     });
 }
 
+int cpb_ctx_set_wait_limit(cpb_ctx* ctx, int64_t polls) {
+    return guarded(ctx, [&]() -> int {
+        ctx->wait_limit = polls;
+        return CPB_OK;
+    });
+}
+
+int cpb_ctx_inject_fault(cpb_ctx* ctx, int32_t fault) {
+    return guarded(ctx, [&]() -> int {
+        if (fault != CPB_FAULT_NONE && fault != CPB_FAULT_HOLD_READY_STAR) throw ArgError{"unknown fault kind"};
+        ctx->fault = fault;
+        return CPB_OK;
+    });
+}
+
 int cpb_ctx_kernel_stats(cpb_ctx* ctx, cpb_kernel_stat* out, int max_out, int* n_out, int64_t* launches, int reset) {
     return guarded(ctx, [&]() -> int {
         resolve_kernel_events(ctx);

@@ -1593,6 +1593,7 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
                    const void* d_bkg, const int64_t* d_soff, const double* d_y0, const double* d_x0,
                    const double* d_f0, int64_t total_pixels, cpb_group_result* out, const int64_t* h_off_opt,
                    const int32_t* h_ny_opt, const int32_t* h_nx_opt, const int64_t* h_soff_opt) {
+    NvtxRange nv_("cpb:group_batch");
     cudaStream_t st = ctx->stream;
     GroupSetup su;
     setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,

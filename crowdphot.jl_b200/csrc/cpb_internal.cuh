@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <algorithm>
@@ -321,6 +322,7 @@ struct DagArgs {
     int* n_failed;
     double* psub;               // per position: the subtracted model
     uint8_t* flag;              // per position: 2 fitted, 1 add-back undone, 0 none
+    long long spin_limit;       // polls of the ready queue before a team gives up
     double* snap;               // last pass: residual box after the subtraction (nullable)
     const int64_t* snap_off;    // per position
 };
@@ -671,6 +673,10 @@ struct cpb_ctx {
     // enabled, CUDA-event timing of every launch on this context's stream
     int64_t launches = 0;
     bool profile = false;
+    // bounded device waits: polls before a persistent kernel gives up (<= 0: default)
+    int64_t wait_limit = 0;
+    // one-shot host-side fault injection for tests (CPB_FAULT_*)
+    int32_t fault = CPB_FAULT_NONE;
     struct KStat {
         int64_t launches = 0;
         double seconds = 0, bytes = 0;
@@ -713,6 +719,15 @@ struct KernelScope {
 };
 // Resolves pending event pairs into ctx->kstats (after a stream sync).
 void resolve_kernel_events(cpb_ctx* ctx);
+
+// A named NVTX range over a host-side phase (set-up, fill, render, LSQR, trial,
+// freeze, final pass, ...), visible in Nsight timelines; free when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct CudaError {
     cudaError_t e;

@@ -1381,7 +1381,7 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
 // brightness order, so the result is the one-star-at-a-time one, but a slow
 // fit only holds back the stars that overlap it.  The residual image is read
 // and written around L1 (ld/st.cg): other SMs change it between uses.
-constexpr long long kDagSpinLimit = 1ll << 26;  // ~64 M polls of >= 64 ns before a team gives up
+constexpr long long kDagSpinLimit = 1ll << 26;  // default: ~64 M polls of >= 64 ns before a team gives up
 // Warps of one team: 4 measured fastest on the 2048^2 field (k_mp_dag 34.6 ms for
 // three passes, against 58.2 ms with 1 and 41.0 ms with 8).
 constexpr int kDagWarps = 4;
@@ -1422,7 +1422,7 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, D
                 for (long long it = 0;; ++it) {
                     k = ((volatile int32_t*)A.queue)[h];
                     if (k >= 0) break;
-                    if (it > kDagSpinLimit || ((volatile int*)errf)[0]) {
+                    if (it > A.spin_limit || ((volatile int*)errf)[0]) {
                         atomicExch(errf, 1);
                         k = -2;
                         break;
@@ -1785,6 +1785,7 @@ void lm_batch_destroy(LMBatch* b) {
 int fit_lm_batch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int64_t n_cut, const int64_t* offsets,
                  const int32_t* ny, const int32_t* nx, const int32_t* y_origin, const int32_t* x_origin,
                  const void* pixels, int32_t eltype, const void* inv_var, const double* init, cpb_lm_result* out) {
+    NvtxRange nv_("cpb:fit_star_batch");
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported pixel eltype"};
     const LMConst L = lm_const(psf, P, inv_var != nullptr);
     if (n_cut <= 0) return 0;
@@ -1935,7 +1936,10 @@ bool mp_dag_supported(const cpb_psf* psf, const cpb_lm_params* P) {
 
 int mp_dag_teams(cpb_ctx* ctx) { return ctx->n_sm * 2 * (kLMThreads / (32 * kDagWarps)); }
 
-void mp_dag_launch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int32_t iv_eltype, const DagArgs& A) {
+void mp_dag_launch(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, int32_t iv_eltype,
+                   const DagArgs& A_in) {
+    DagArgs A = A_in;
+    A.spin_limit = ctx->wait_limit > 0 ? (long long)ctx->wait_limit : kDagSpinLimit;
     const LMConst L = lm_const(psf, P, A.iv != nullptr);
     cudaStream_t st = ctx->stream;
     const bool gauss = psf->dev.kind == CPB_PSF_CIRCULAR_GAUSSIAN;

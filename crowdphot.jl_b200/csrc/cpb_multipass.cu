@@ -637,6 +637,7 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
     std::vector<int64_t> lev_pix;
 
     for (int pass = 1; pass <= n_passes; ++pass) {
+        NvtxRange nv_("cpb:fit_all_stars:pass");
         // ---- plan (:326-348): brightness order, boxes, and the batch (level)
         // of every valid star, all on the device
         check(cudaMemsetAsync(d_ccount, 0, sizeof(int32_t) * (ncell + 1), st), "memset");
@@ -691,6 +692,14 @@ int fit_all_stars_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_lm_params* P, 
                 k_mp_fill<int32_t><<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, -1, d_queue);
                 check(cudaMemsetAsync(d_level, 0, sizeof(int32_t) * npos, st), "memset");
                 check(cudaMemsetAsync(d_dagc, 0, sizeof(int32_t) * 4, st), "memset");
+                if (ctx->fault == CPB_FAULT_HOLD_READY_STAR && pass == 1) {
+                    // test hook: the brightest star (position 0, which waits for nobody) is
+                    // kept out of the ready queue, so the stars behind it never become ready
+                    const int32_t held = 1;
+                    check(cudaMemcpyAsync(d_indeg, &held, sizeof(int32_t), cudaMemcpyHostToDevice, st), "h2d");
+                    check(cudaStreamSynchronize(st), "sync");
+                    ctx->fault = CPB_FAULT_NONE;
+                }
                 counted(ctx);
                 k_dag_queue<<<(unsigned)((npos + 255) / 256), 256, 0, st>>>(npos, d_indeg, d_queue, d_dagc);
                 check(cudaGetLastError(), "k_dag_queue");

@@ -59,27 +59,72 @@ struct Scalars {
 // ---------------------------------------------------------------------------
 // setup kernels
 // ---------------------------------------------------------------------------
-template <typename TI>
-__global__ void k_prepare(const TI* __restrict__ img, const TI* __restrict__ iv, const TI* __restrict__ bkg,
-                          int64_t npix, double* data, double* data_work, double* w, double* sw,
-                          unsigned* nonfinite) {
-    int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (q >= npix) return;
-    double d = (double)img[q] - (bkg ? (double)bkg[q] : 0.0);
+// data and weight sanitisation of one pixel (:1056-1084)
+__device__ __forceinline__ void prepare_px(double d, bool have_iv, double v, double& dout, double& wout,
+                                           unsigned& bad) {
     double wv = 1.0;
-    if (iv) {
-        double v = (double)iv[q];
-        wv = (isfinite(v) && v > 0) ? v : 0.0;
-    }
+    if (have_iv) wv = (isfinite(v) && v > 0) ? v : 0.0;
     if (!isfinite(d)) {
-        if (!iv) atomicAdd(nonfinite, 1u);
+        if (!have_iv) ++bad;
         d = 0.0;
         wv = 0.0;
     }
-    data[q] = d;
-    data_work[q] = d;
-    w[q] = wv;
-    sw[q] = sqrt(wv);
+    dout = d;
+    wout = wv;
+}
+
+// one 16-byte run of a user image (the caller checked its alignment)
+__device__ __forceinline__ void ld_img16(const float* p, double (&o)[4]) {
+    const float4 t = __ldg((const float4*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+}
+__device__ __forceinline__ void ld_img16(const double* p, double (&o)[2]) {
+    const double2 t = __ldg((const double2*)p);
+    o[0] = t.x;
+    o[1] = t.y;
+}
+
+// VEC: each thread takes one 16-byte run of every input (4 floats or 2 doubles)
+// and writes its pixels' vectors with 16-byte stores; otherwise one pixel a thread.
+template <typename TI, bool VEC>
+__global__ void k_prepare(const TI* __restrict__ img, const TI* __restrict__ iv, const TI* __restrict__ bkg,
+                          int64_t npix, double* data, double* data_work, double* w, double* sw,
+                          unsigned* nonfinite) {
+    constexpr int E = VEC ? 16 / (int)sizeof(TI) : 1;
+    const int64_t q0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * E;
+    if (q0 >= npix) return;
+    double d[E], v[E], b[E], dd[E], ww[E];
+    unsigned bad = 0;
+    if constexpr (VEC) {
+        ld_img16(img + q0, d);
+        if (iv) ld_img16(iv + q0, v);
+        if (bkg) ld_img16(bkg + q0, b);
+    } else {
+        d[0] = (double)img[q0];
+        if (iv) v[0] = (double)iv[q0];
+        if (bkg) b[0] = (double)bkg[q0];
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) prepare_px(d[e] - (bkg ? b[e] : 0.0), iv != nullptr, iv ? v[e] : 0.0, dd[e], ww[e], bad);
+#pragma unroll
+    for (int e = 0; e < E; e += 2) {
+        if constexpr (E == 1) {
+            data[q0] = dd[0];
+            data_work[q0] = dd[0];
+            w[q0] = ww[0];
+            sw[q0] = sqrt(ww[0]);
+        } else {
+            const double2 dv = make_double2(dd[e], dd[e + 1]), wv = make_double2(ww[e], ww[e + 1]);
+            *(double2*)(data + q0 + e) = dv;
+            *(double2*)(data_work + q0 + e) = dv;
+            *(double2*)(w + q0 + e) = wv;
+            *(double2*)(sw + q0 + e) = make_double2(sqrt(ww[e]), sqrt(ww[e + 1]));
+        }
+    }
+    if (bad) atomicAdd(nonfinite, bad);
 }
 
 __device__ __forceinline__ uint64_t spread_bits(uint64_t v) {
@@ -1892,6 +1937,7 @@ Form<TS, TU> SimFit::make_form(const char* tag) {
 template <typename TS, typename TU>
 void SimFit::launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist) {
     if (nlist <= 0) return;
+    NvtxRange nv_("cpb:sim:fill");
     constexpr double bts = sizeof(TS);
     const bool writeM = model_R == fc.R && !d_modelR;
     KernelScope ks_(ctx, "k_eval_fill",
@@ -1953,6 +1999,8 @@ void SimFit::launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* 
 template <typename TS, typename TU>
 void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const int32_t* list, int64_t nlist,
                            const StarCoef* cf, TU* outu, double* outd, const double* ref, double* result) {
+    NvtxRange nv_(mode == MODE_CUR ? "cpb:sim:render_residual"
+                                   : (mode == MODE_CAND ? "cpb:sim:render_trial" : "cpb:sim:render_freeze"));
     if (!(mode == MODE_CUR && F.m_fresh)) launch_eval_model<TS>(F.fc, F.M, F.MS, F.d_moff, list, nlist, cf);
     F.m_fresh = false;
     const double px_bytes =
@@ -1979,6 +2027,7 @@ void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const
 }
 
 bool SimFit::setup() {
+    NvtxRange nv_("cpb:sim:setup");
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     // argument checks in the reference's order (:984-997)
     if (!(P->max_iter > 0)) throw ArgError{"max_iter must be positive"};
@@ -2068,14 +2117,28 @@ bool SimFit::setup() {
     sw = S_<double>("sw", npix);
     unsigned* flags = S_<unsigned>("flags", 4);
     check(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned), st), "memset");
-    if (eltype == CPB_F64)
-        k_prepare<double><<<nblk(npix), 256, 0, st>>>((const double*)d_image, (const double*)d_inv_var,
-                                                      (const double*)d_background, npix, data, data_work, w, sw,
-                                                      flags);
-    else
-        k_prepare<float><<<nblk(npix), 256, 0, st>>>((const float*)d_image, (const float*)d_inv_var,
-                                                     (const float*)d_background, npix, data, data_work, w, sw, flags);
-    check(cudaGetLastError(), "k_prepare");
+    {
+        // 16-byte reads of the caller's images when every one of them allows it
+        const int e16 = eltype == CPB_F64 ? 2 : 4;
+        auto al16 = [](const void* q) { return q == nullptr || ((uintptr_t)q & 15) == 0; };
+        const bool vec = npix % e16 == 0 && al16(d_image) && al16(d_inv_var) && al16(d_background);
+        KernelScope ks_(ctx, "k_prepare", (double)npix * ((eltype == CPB_F64 ? 8.0 : 4.0) *
+                                                          (1 + (d_inv_var ? 1 : 0) + (d_background ? 1 : 0)) +
+                                                          32.0));
+#define CPB_PREP(TI, V)                                                                                         \
+    k_prepare<TI, V><<<nblk(V ? npix / e16 : npix), 256, 0, st>>>((const TI*)d_image, (const TI*)d_inv_var,     \
+                                                                  (const TI*)d_background, npix, data,         \
+                                                                  data_work, w, sw, flags)
+        if (eltype == CPB_F64) {
+            if (vec) CPB_PREP(double, true);
+            else CPB_PREP(double, false);
+        } else {
+            if (vec) CPB_PREP(float, true);
+            else CPB_PREP(float, false);
+        }
+#undef CPB_PREP
+        check(cudaGetLastError(), "k_prepare");
+    }
 
     // ---- _build_stamps! (:245-323)
     int32_t* ay_c = S_<int32_t>("ay_c", n_stars);
@@ -2338,6 +2401,7 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
         }
         bool accepted = false, f_conv = false;
         for (int trial = 1; trial <= P->max_trials; ++trial) {
+            NvtxRange nv_trial("cpb:sim:trial");
             ++n_trials;
             // LSQR init (Krylov lsqr: beta1 u1 = b, alpha1 v1 = A'u1)
             Scalars init{};
@@ -2357,6 +2421,7 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
             if (init.beta1 == 0) {
                 check(cudaMemsetAsync(xl, 0, sizeof(double) * n, st), "memset");
             } else {
+                NvtxRange nv_lsqr("cpb:sim:lsqr");
                 {
                     KernelScope ks_(ctx, "k_lsqr_v0", (double)n * 8 * 3);
                     k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red);
@@ -2469,13 +2534,18 @@ int SimFit::run() {
         outer_loop(F32, 1, P->max_iter, true);
         if (P->refine_iters > 0) {
             // FP64 refinement: every active star live again on the original
-            // data, from the mixed-precision parameters, with the same damping,
-            // scaling D and convergence tests (converged flags accumulate)
+            // data, from the mixed-precision parameters, with the same scaling D
+            // and convergence tests (converged flags accumulate) and the damping
+            // restarted at lambda_init: near its end the FP32-stamp loop rejects
+            // steps on cost differences below what FP32 model values resolve, and
+            // the damping those rejections piled up would hold the FP64 steps back
             Form<double, double> F64 = make_form<double, double>("_f64");
+            lam = P->lambda_init;
             check(cudaMemcpyAsync(data_work, data, sizeof(double) * npix, cudaMemcpyDeviceToDevice, st), "d2d");
             check(cudaMemsetAsync(live, 1, n_act, st), "memset");
             check(cudaMemcpyAsync(live_list, iota_act, sizeof(int32_t) * n_act, cudaMemcpyDeviceToDevice, st), "d2d");
             n_live = n_act;
+            NvtxRange nv_("cpb:sim:refine_fp64");
             outer_loop(F64, n_run + 1, n_run + P->refine_iters, false);
         }
     } else {
@@ -2490,6 +2560,7 @@ int SimFit::run() {
 // (:1344-1356), the diagnostics and the result assembly (:1289-1300,
 // :1331-1337, :1404-1430); FP64 for either precision form.
 void SimFit::finish() {
+    NvtxRange nv_("cpb:sim:final");
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     launch_coef(nullptr, coef);
     double* gram = S_<double>("gram", (int64_t)n_act * 6);

@@ -134,9 +134,10 @@ typedef struct cpb_sim_params {
     int32_t damping;          /* CPB_DAMP_* */
     /* precision == CPB_PREC_MIXED only: FP64 refinement iterations after the
      * FP32-stamp loop (every active star live again on the original data, from
-     * the mixed-precision parameters, same damping and tests; converged flags
-     * accumulate).  0 = none: the final FP64 pass then only re-evaluates
-     * errors, residual and diagnostics at the mixed-precision parameters. */
+     * the mixed-precision parameters, damping restarted at lambda_init, same
+     * tests; converged flags accumulate).  0 = none: the final FP64 pass then
+     * only re-evaluates errors, residual and diagnostics at the
+     * mixed-precision parameters. */
     int32_t refine_iters;
     /* spread_model reference disk FWHM: NaN = from the PSF's effective area
      * (the reference default, _spread_fwhm); <= 0 = skip spread_model */
@@ -262,6 +263,25 @@ typedef struct cpb_kernel_stat {
     double bytes;    /* summed algorithmic bytes */
 } cpb_kernel_stat;
 CPB_API int cpb_ctx_set_profiling(cpb_ctx* ctx, int enable);
+
+/*
+ * Bounded device waits (no counterpart in the reference, which runs on one
+ * thread).  The persistent fit_all_stars pass kernel spins on its ready queue
+ * for at most `polls` polls of >= 64 ns per wait (<= 0: the default, 2^26, a few
+ * seconds) before it gives up and the call returns CPB_ERR_TIMEOUT with the
+ * reason in cpb_last_error; the context stays usable.
+ */
+CPB_API int cpb_ctx_set_wait_limit(cpb_ctx* ctx, int64_t polls);
+/*
+ * Host-side fault injection for testing the bounded waits above; no GPU fault
+ * is involved.  CPB_FAULT_HOLD_READY_STAR: the next fit_all_stars call holds the
+ * brightest star of its first pass back from the ready queue, so the stars that
+ * wait for it never become ready and the waits run out (CPB_ERR_TIMEOUT).  The
+ * injection applies to one call and then clears itself.
+ */
+#define CPB_FAULT_NONE 0
+#define CPB_FAULT_HOLD_READY_STAR 1
+CPB_API int cpb_ctx_inject_fault(cpb_ctx* ctx, int32_t fault);
 /* Writes up to max_out per-kernel records, the number available to *n_out and
  * the total launch count to *launches; reset != 0 clears the counters. */
 CPB_API int cpb_ctx_kernel_stats(cpb_ctx* ctx, cpb_kernel_stat* out, int max_out, int* n_out, int64_t* launches,

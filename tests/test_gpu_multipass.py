@@ -120,3 +120,32 @@ def test_batch_level_path_irls_and_four_node_psf():
     cat = dict(y=ys + rng.normal(0, 0.2, 40), x=xs + rng.normal(0, 0.2, 40), flux=fl)
     kw = dict(n_passes=2, max_iter=60, fixed={"bkg": 0.0}, inv_var=iv)
     compare(cpb.fit_all_stars(img, g4, cat, 6, **kw), orc_fit_all_stars(img, g4, cat, 6, **kw))
+
+
+def test_bounded_wait_runs_out_and_the_context_stays_usable():
+    """Every device-side wait of the dependency-driven pass kernel is bounded.  The
+    host holds the brightest star of the first pass back from the ready queue
+    (cpb_ctx_inject_fault; no GPU fault), so the stars behind it never become ready:
+    with a short wait limit the call returns CPB_ERR_TIMEOUT (TimeoutError) with the
+    reason, and the next call on the same context gives the same result as before."""
+    from crowdphot_b200 import _abi
+    psf = moffat_epsf()
+    img, bkg, iv, truth, init = crowded_field(128, 128, 160, seed=3005, psf=psf, dtype=np.float32)
+    data = (img - bkg).astype(np.float32)
+    kw = dict(n_passes=2, fixed={"bkg": 0.0}, inv_var=iv, max_iter=100)
+    ctx = cpb.get_context(0)
+    before = cpb.fit_all_stars(data, psf, init, 8, ctx=ctx, **kw)
+    assert before.valid.sum() > 100
+    try:
+        ctx.set_wait_limit(20_000)  # about a few ms of polling per wait
+        ctx.inject_fault(_abi.CPB_FAULT_HOLD_READY_STAR)
+        with pytest.raises(TimeoutError, match="stalled waiting for ready stars"):
+            cpb.fit_all_stars(data, psf, init, 8, ctx=ctx, **kw)
+    finally:
+        ctx.set_wait_limit(0)
+        ctx.inject_fault(_abi.CPB_FAULT_NONE)
+    after = cpb.fit_all_stars(data, psf, init, 8, ctx=ctx, **kw)
+    for k in ("y", "x", "flux", "flux_err", "valid", "converged", "n_iter"):
+        assert np.array_equal(getattr(after, k), getattr(before, k)), k
+    with pytest.raises(ArgumentError, match="unknown fault"):
+        ctx.inject_fault(7)

@@ -9,7 +9,8 @@ import pytest
 
 import crowdphot_b200 as cpb
 from crowdphot_b200 import ArgumentError, CircularGaussianPSF
-from crowdphot_b200.simulate import (add_noise, crowded_field, moffat_epsf, render_sources, simulate_sources)
+from crowdphot_b200.simulate import (add_noise, c1_field, crowded_field, moffat_epsf, render_sources,
+                                      simulate_sources)
 from oracle import orc_fit_simultaneous
 
 pytestmark = pytest.mark.gpu
@@ -28,27 +29,25 @@ def parity_report(g, o):
     return both, same, dy, dx, df, bad
 
 
-def assert_parity(g, o, min_same_frac=0.9):
-    assert np.array_equal(g.valid, o.valid) or (g.valid != o.valid).sum() <= 0.01 * len(g.valid)
+def assert_parity(g, o, min_same_frac=1.0, max_valid_diff=0, tag=""):
+    """Gates for stars valid and converged in both fits that freeze on the same
+    iteration; `min_same_frac` (just under the measured fraction of each test) bounds
+    how many may freeze on different iterations, and their deviations are printed."""
+    nvd = int((g.valid != o.valid).sum())
+    assert nvd <= max_valid_diff, f"valid flags differ for {nvd} stars"
     both, same, dy, dx, df, bad = parity_report(g, o)
     assert both.sum() > 0
-    assert same.sum() >= min_same_frac * both.sum(), f"freeze iterations differ for {both.sum() - same.sum()} stars"
+    diff = both & ~same
+    msg = (f"parity {tag}: {int(same.sum())}/{int(both.sum())} same freeze iteration "
+           f"({same.sum() / both.sum():.4f}); same: max dy {dy[same].max():.2e} dx {dx[same].max():.2e} "
+           f"dflux {df[same].max():.2e}")
+    if diff.any():
+        msg += (f"; different freeze ({int(diff.sum())}): max dy {dy[diff].max():.2e} dx {dx[diff].max():.2e} "
+                f"dflux {df[diff].max():.2e}")
+    print(msg)
+    assert same.sum() >= min_same_frac * both.sum(), msg
     assert bad.sum() == 0, (f"{bad.sum()} stars outside the gates: max dy {dy[same].max():.3g} "
                             f"dx {dx[same].max():.3g} dflux {df[same].max():.3g}")
-
-
-def c1_field(seed=1001, n=200, shape=(256, 256)):
-    """256^2 Float64, 200 stars, CircularGaussianPSF FWHM 2.5, flat background 100 + Poisson."""
-    rng = np.random.default_rng(seed)
-    psf = CircularGaussianPSF(fwhm=2.5)
-    src = simulate_sources(shape, n, rng=rng, flux=(1e2, 1e5), flux_distribution="loguniform")
-    model = np.zeros(shape)
-    render_sources(model, psf, src["y"], src["x"], src["flux"], model_radius=7)
-    img = add_noise(model + 100.0, rng=rng, noise="poisson", gain=1.0)
-    iv = 1.0 / (100.0 + model)
-    init = dict(y=src["y"] + rng.normal(0, 0.3, n), x=src["x"] + rng.normal(0, 0.3, n),
-                flux=src["flux"] * rng.uniform(0.9, 1.1, n))
-    return img, np.full(shape, 100.0), iv, psf, src, init
 
 
 def test_c1_config_parity():
@@ -62,7 +61,7 @@ def test_c1_config_parity():
     assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
     assert g.stats["n_union"] == o.stats["n_union"]
     assert g.n_failed == o.n_failed
-    assert_parity(g, o)
+    assert_parity(g, o, tag="c1")
 
 
 def test_crowded_epsf_parity_float32():
@@ -74,7 +73,7 @@ def test_crowded_epsf_parity_float32():
     assert np.array_equal(g.debug["active"], o.debug["active"])
     assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
     assert g.stats["n_union"] == o.stats["n_union"]
-    assert_parity(g, o, min_same_frac=0.8)
+    assert_parity(g, o, tag="crowded_f32")
 
 
 def test_edges_masks_and_nan_pixels_bit_exact_structures():
@@ -103,7 +102,7 @@ def test_edges_masks_and_nan_pixels_bit_exact_structures():
     assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
     assert g.stats["n_union"] == o.stats["n_union"]
     assert g.n_failed == o.n_failed and g.n_failed > 0
-    assert_parity(g, o, min_same_frac=0.8)
+    assert_parity(g, o, tag="edges")
 
 
 @pytest.mark.parametrize("kind", ["gaussian", "gridded"])
@@ -175,31 +174,92 @@ def test_deterministic_bitwise():
     assert np.array_equal(a.residual, b.residual)
 
 
-def test_mixed_precision_form_vs_fp64_oracle():
-    """Mixed form (FP32 stamps / model values / products, FP64 solver state) against the
-    FP64 oracle on the crowded ePSF field.  A truncated, freeze-as-you-go fit of a
-    crowded field is sensitive to its trajectory: the oracle itself moves by
-    ~1e-5 (median) when its initial guesses change by 1e-7 relative.  The mixed
-    form must stay within that intrinsic spread (per output, median and p99)."""
+def _perturbed(img, seed):
+    """The image times (1 + 1e-7 N(0, 1)), rounded to its own element type: a change
+    at the input's own rounding (about one ulp of a Float32 image on half the pixels)."""
+    g = np.random.default_rng(seed)
+    return (img.astype(np.float64) * (1 + 1e-7 * g.standard_normal(img.shape))).astype(img.dtype)
+
+
+def test_mixed_precision_form_follows_the_fp64_trajectory():
+    """Mixed form (FP32 stamps, model values and LSQR pixel vectors; FP64 sums,
+    solver state, 3x3 solves and chi^2) against the FP64 oracle on the crowded ePSF
+    field, twelve Gauss-Newton iterations with freezing and the global stops off, so
+    that both take the same steps.  Stars whose result the data do not fix move when
+    the input moves by its own rounding; the stars the oracle reproduces to a tenth of
+    the gates under two such perturbations form the stable set, and there the mixed
+    form meets the gates themselves (1e-4 px, 1e-5 relative flux).  (The default
+    tolerances stop a crowded fit on global tests -- f_tol, the gradient cosine --
+    whose outcome can flip under FP32 rounding and move every star by a step; the
+    bench reports that comparison at full size.)"""
     psf = moffat_epsf()
     img, bkg, iv, truth, init = crowded_field(256, 256, 780, seed=1002, psf=psf, dtype=np.float32)
-    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=12)
+    kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=12, max_iter=12, x_tol=0.0, f_tol=0.0,
+              g_tol=0.0)
     g = cpb.fit_all_stars_simultaneous(img, psf, init, 12, precision="mixed", **kw)
     o = orc_fit_simultaneous(img, psf, init, 12, **kw)
-    rng = np.random.default_rng(0)
-    init2 = {k: v * (1 + 1e-7 * rng.standard_normal(v.size)) for k, v in init.items()}
-    o2 = orc_fit_simultaneous(img, psf, init2, 12, **kw)
-    both, same, dy, dx, df, bad = parity_report(g, o)
-    _, same2, dy2, dx2, df2, _ = parity_report(o2, o)
-    print(f"mixed vs FP64 oracle: {same.sum()}/{both.sum()} same freeze; dflux median/p99/max "
-          f"{np.median(df[same]):.2e}/{np.percentile(df[same], 99):.2e}/{df[same].max():.2e}; dy "
-          f"{np.median(dy[same]):.2e}/{np.percentile(dy[same], 99):.2e}; oracle spread under 1e-7 init "
-          f"perturbation: dflux {np.median(df2[same2]):.2e}/{np.percentile(df2[same2], 99):.2e}, dy "
-          f"{np.median(dy2[same2]):.2e}/{np.percentile(dy2[same2], 99):.2e}")
-    assert same.sum() >= 0.8 * both.sum()
-    for a_, b_ in ((df, df2), (dy, dy2), (dx, dx2)):
-        assert np.median(a_[same]) <= 2 * np.median(b_[same2]) + 1e-7
-        assert np.percentile(a_[same], 99) <= 2 * np.percentile(b_[same2], 99) + 1e-6
+    assert g.n_passes == o.n_passes == 12
+    fitted = o.valid & g.valid
+    stable = fitted.copy()
+    for seed in (11, 12):
+        op = orc_fit_simultaneous(_perturbed(img, seed), psf, init, 12, **kw)
+        stable &= op.valid
+        stable &= np.abs(op.flux / o.flux - 1) <= 0.1 * FLUX_TOL
+        stable &= np.maximum(np.abs(op.y - o.y), np.abs(op.x - o.x)) <= 0.1 * POS_TOL
+    df = np.abs(g.flux / o.flux - 1)
+    dp = np.maximum(np.abs(g.y - o.y), np.abs(g.x - o.x))
+    print(f"mixed vs FP64 oracle, 12 iterations: stable set {int(stable.sum())} of {int(fitted.sum())} valid; on "
+          f"it dflux median/p99/max {np.median(df[stable]):.2e}/{np.percentile(df[stable], 99):.2e}/"
+          f"{df[stable].max():.2e}, dpos max {dp[stable].max():.2e}; all valid: dflux within 1e-5 "
+          f"{np.mean(df[fitted] <= FLUX_TOL):.3f}")
+    assert stable.sum() >= 0.3 * fitted.sum()
+    assert df[stable].max() <= FLUX_TOL and dp[stable].max() <= POS_TOL
+
+
+def test_tight_tolerance_every_valid_star():
+    """The reference's converged-mode comparison (test/photometry/psf_photometry_simultaneous.jl:270-274):
+    with f_tol off and a tight x_tol both fits run to the same minimum, so every
+    valid star -- not only those frozen on the same iteration -- meets the gates."""
+    img, bkg, iv, psf, src, init = c1_field()
+    kw = dict(fixed={"fwhm": 2.5, "bkg": 0.0}, inv_var=iv, background=bkg, model_rad=7, max_iter=60,
+              linear_tol=1e-8, x_tol=1e-10, f_tol=0.0)
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, 7, **kw)
+    o = orc_fit_simultaneous(img, psf, init, 7, **kw)
+    assert np.array_equal(g.valid, o.valid)
+    v = g.valid
+    dy, dx, df = np.abs(g.y - o.y)[v], np.abs(g.x - o.x)[v], np.abs(g.flux / o.flux - 1)[v]
+    print(f"tight: {int(v.sum())} valid, {int((g.converged & v).sum())} converged; max dy {dy.max():.2e} "
+          f"dx {dx.max():.2e} dflux {df.max():.2e}")
+    assert dy.max() <= POS_TOL and dx.max() <= POS_TOL and df.max() <= FLUX_TOL
+
+
+def test_mixed_precision_refinement_reaches_the_fp64_minimum():
+    """refine_iters: FP64 Gauss-Newton iterations after the FP32-stamp loop.  Run to a
+    minimum of the whole field (freezing and the global stops off, 120 iterations,
+    where the FP64 fit no longer moves), the FP32-stamp loop stalls where its accept
+    test no longer resolves the cost (median flux deviation from the oracle ~3e-8);
+    twenty FP64 refinement iterations bring the median to FP64 rounding and every
+    valid star whose nearest neighbour is at least 3 px away (pairs closer than about
+    a FWHM converge slowly at any precision) inside the gates."""
+    img, bkg, iv, psf, src, init = c1_field()
+    kw = dict(fixed={"fwhm": 2.5, "bkg": 0.0}, inv_var=iv, background=bkg, model_rad=7, max_iter=120,
+              linear_tol=1e-10, x_tol=0.0, f_tol=0.0, g_tol=0.0)
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, 7, precision="mixed", refine_iters=20, **kw)
+    m = cpb.fit_all_stars_simultaneous(img, psf, init, 7, precision="mixed", **kw)
+    o = orc_fit_simultaneous(img, psf, init, 7, **kw)
+    assert np.array_equal(g.valid, o.valid) and np.array_equal(m.valid, o.valid)
+    d = np.hypot(src["y"][:, None] - src["y"][None], src["x"][:, None] - src["x"][None]) + 1e9 * np.eye(len(src["y"]))
+    apart = g.valid & (d.min(1) >= 3.0)
+    df = lambda r: np.abs(r.flux / o.flux - 1)
+    dp = lambda r: np.maximum(np.abs(r.y - o.y), np.abs(r.x - o.x))
+    print(f"minimum: mixed median dflux {np.median(df(m)[g.valid]):.1e}, refined {np.median(df(g)[g.valid]):.1e}; "
+          f"{int(apart.sum())} stars >= 3 px apart: refined max dflux {df(g)[apart].max():.1e} dpos "
+          f"{dp(g)[apart].max():.1e}; passes {g.n_passes} (mixed {m.n_passes}, oracle {o.n_passes})")
+    assert np.median(df(g)[g.valid]) <= 1e-12 < np.median(df(m)[g.valid])
+    assert df(g)[apart].max() <= FLUX_TOL and dp(g)[apart].max() <= POS_TOL
+    assert g.n_passes == m.n_passes + 20 == o.n_passes + 20
+    with pytest.raises(ArgumentError, match="refine_iters"):
+        cpb.fit_all_stars_simultaneous(img, psf, init, 7, precision="mixed", refine_iters=-1, **kw)
 
 
 @pytest.mark.parametrize("kind", ["gaussian", "gridded"])
@@ -236,7 +296,7 @@ def test_model_rad_auto_radii_bit_exact_and_parity(case):
     assert np.array_equal(g.debug["active"], o.debug["active"])
     assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
     assert len(np.unique(o.debug["model_R"])) > 1  # radii really vary with flux
-    assert_parity(g, o, min_same_frac=0.8)
+    assert_parity(g, o, tag=f"auto_{case}")
 
 
 def test_spread_model_parity_and_sequential_agreement():
@@ -318,7 +378,7 @@ def test_four_node_gridded_parity_and_large_radii():
     o = orc_fit_simultaneous(img, psf, init, 8, **kw)
     assert np.array_equal(g.debug["active"], o.debug["active"])
     assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
-    assert_parity(g, o, min_same_frac=0.8)
+    assert_parity(g, o, tag="four_node")
     both, same, *_ = parity_report(g, o)
     np.testing.assert_allclose(g.spread_model[same], o.spread_model[same], rtol=0, atol=1e-4)
     sel = {k: np.asarray(v)[:10] for k, v in init.items()}
@@ -327,4 +387,4 @@ def test_four_node_gridded_parity_and_large_radii():
     o = orc_fit_simultaneous(img, psf, sel, 26, **kw)
     assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
     assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
-    assert_parity(g, o, min_same_frac=0.5)
+    assert_parity(g, o, tag="large_radii")
