@@ -229,8 +229,13 @@ __global__ void k_tile_count(int64_t n_act, const int32_t* ay, const int32_t* ax
     cnt[j] = star_tiles(ay[j], ax[j], Rj, ny, nx, a, b, c, d) ? (b - a + 1) * (d - c + 1) : 0;
 }
 
+// A star's (region, star) pairs in emit order: regions column by column
+// (tx0..tx1, then ty0..ty1 within), starting at offs[j]; vals carry the emit
+// index through the sort so that every pair's star and every star's pairs can
+// be found afterwards (emit_j, star_pairs).
 __global__ void k_tile_emit(int64_t n_act, const int32_t* ay, const int32_t* ax, const int32_t* Rs, int Rconst,
-                            int ny, int nx, int nty, const int32_t* offs, uint32_t* keys, int32_t* vals) {
+                            int ny, int nx, int nty, const int32_t* offs, uint32_t* keys, int32_t* vals,
+                            int32_t* emit_j) {
     int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (j >= n_act) return;
     int Rj = Rs ? Rs[j] : Rconst, ty0, ty1, tx0, tx1;
@@ -239,7 +244,8 @@ __global__ void k_tile_emit(int64_t n_act, const int32_t* ay, const int32_t* ax,
     for (int tx = tx0; tx <= tx1; ++tx)
         for (int ty = ty0; ty <= ty1; ++ty) {
             keys[o] = (uint32_t)(ty + tx * nty);
-            vals[o] = (int32_t)j;
+            vals[o] = o;
+            emit_j[o] = (int32_t)j;
             ++o;
         }
 }
@@ -260,13 +266,16 @@ __global__ void k_tile_work(int64_t ntiles, const int32_t* start, const int32_t*
     idx[t] = (int32_t)t;
 }
 
-__global__ void k_tile_pack(int64_t npairs, const int32_t* sorted_j, const int32_t* ay, const int32_t* ax,
-                            const int32_t* Rs, int Rconst, int4* packed) {
+__global__ void k_tile_pack(int64_t npairs, const int32_t* sorted_o, const int32_t* emit_j, const int32_t* ay,
+                            const int32_t* ax, const int32_t* Rs, int Rconst, int4* packed, int32_t* star_pairs) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= npairs) return;
-    const int j = sorted_j[i];
+    const int o = sorted_o[i];
+    const int j = emit_j[o];
     packed[i] = make_int4(j, ay[j], ax[j], Rs ? Rs[j] : Rconst);  // .w: the star's box radius
+    star_pairs[o] = (int32_t)i;
 }
+
 
 // ---------------------------------------------------------------------------
 // per-iteration kernels
@@ -277,7 +286,6 @@ struct FitConst {
     int ky, kx;    // index of y / x in the free list, -1 if fixed
     double fixed_y, fixed_x, fixed_flux, fixed_bkg;
     int R, S, S2;
-    int SR, PS, VS;  // stamp layout of the fit box: rows per column, plane size, star block (see gran_rows)
     int q32, r32;  // 32 / S and 32 % S: advancing a stamp index by one warp
     int ny, nx;
     int nty, ntx;
@@ -325,6 +333,171 @@ __device__ __forceinline__ void ld_px16(const double* p, double (&o)[2]) {
     const double2 t = __ldg((const double2*)p);
     o[0] = t.x;
     o[1] = t.y;
+}
+
+// ---- region-contiguous stamp storage ------------------------------------
+// The stamps are stored per (region, star) pair in the order of the region
+// lists: the pair's rectangle -- the star's granule-layout columns clipped to
+// the region -- is dense (rectangle column c, storage row s at
+// c * nrows + s, one plane after the other), and the rectangles of a region's
+// stars follow one another, so a region's gather reads one contiguous run.
+struct RectGeo {
+    int c_lo, ncols;  // box columns held
+    int s_lo, nrows;  // storage rows held (a multiple of GH)
+};
+
+// The part of the box of radius Rb anchored at (ay, ax) that region (ry, rx)
+// holds, for granules of GH rows.
+__host__ __device__ __forceinline__ RectGeo rect_geo(int ay, int ax, int Rb, int ry, int rx, int GH) {
+    const int Sb = 2 * Rb + 1, left0 = ax - Rb - 1, top0 = ay - Rb - 1;
+    const int b0 = top0 & ~(GH - 1), SRb = gran_rows(Sb, GH);
+    const int C0 = rx * TX, R0 = ry * TY;
+    RectGeo g;
+    const int c0 = left0 > C0 ? left0 : C0, c1 = left0 + Sb - 1 < C0 + TX - 1 ? left0 + Sb - 1 : C0 + TX - 1;
+    const int r_lo = b0 > R0 ? b0 : R0, r_hi = b0 + SRb < R0 + TY ? b0 + SRb : R0 + TY;
+    g.c_lo = c0 - left0;
+    g.ncols = c1 >= c0 ? c1 - c0 + 1 : 0;
+    g.s_lo = r_lo - b0;
+    g.nrows = r_hi > r_lo ? r_hi - r_lo : 0;
+    return g;
+}
+
+// Where one list's stamps live: per star its pairs (soffs, star_pairs), per
+// pair its rectangle's element offset (off), and the planes a rectangle holds.
+struct RectMap {
+    const int32_t* soffs;       // per star: its first emit index
+    const int32_t* star_pairs;  // per emit index: the pair (list position)
+    const int64_t* off;         // per pair: offset of the rectangle's plane 0
+    const int64_t* srect;       // per star, when every box meets at most 2 x 2 regions: its
+                                // rectangles' offsets in emit order (kStarRects a star), else null
+    int planes;
+};
+constexpr int kStarRects = 4;
+
+// srect of a list whose boxes meet at most 2 x 2 regions (box side <= TX + 1).
+__global__ void k_star_rects(int64_t n_act, const int32_t* __restrict__ soffs, const int32_t* __restrict__ star_pairs,
+                             const int64_t* __restrict__ off, int64_t* srect) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n_act * kStarRects) return;
+    const int64_t j = t / kStarRects;
+    const int l = (int)(t % kStarRects);
+    const int o = soffs[j] + l;
+    srect[t] = o < soffs[j + 1] ? off[star_pairs[o]] : -1;
+}
+
+// Element index of box entry (row, col) of star j in plane 0, or -1 when no
+// region holds it (off the image); plane k is k * *pstride further on.
+// ty0..tx1: the star's regions (star_tiles).
+__device__ __forceinline__ int64_t rect_slot(const RectMap& m, int j, int ay, int ax, int Rb, int ty0, int ty1,
+                                             int tx0, int tx1, int row, int col, int GH, int64_t* pstride) {
+    const int y = ay - Rb - 1 + row, x = ax - Rb - 1 + col;
+    if (y < 0 || x < 0) return -1;
+    const int ry = y / TY, rx = x / TX;
+    if (ry < ty0 || ry > ty1 || rx < tx0 || rx > tx1) return -1;
+    const int i = m.star_pairs[m.soffs[j] + (rx - tx0) * (ty1 - ty0 + 1) + (ry - ty0)];
+    const RectGeo g = rect_geo(ay, ax, Rb, ry, rx, GH);
+    const int top0 = ay - Rb - 1, o = top0 - (top0 & ~(GH - 1));
+    *pstride = (int64_t)g.ncols * g.nrows;
+    return m.off[i] + (int64_t)(col - g.c_lo) * g.nrows + (o + row - g.s_lo);
+}
+__device__ __forceinline__ int64_t rect_index(const RectMap& m, int j, int ay, int ax, int Rb, int ty0, int ty1,
+                                              int tx0, int tx1, int row, int col, int k, int GH) {
+    int64_t ps = 0;
+    const int64_t q = rect_slot(m, j, ay, ax, Rb, ty0, ty1, tx0, tx1, row, col, GH, &ps);
+    return q < 0 ? q : q + k * ps;
+}
+
+// A star's rectangles as the stamp kernels store into them: geometry and the
+// offsets in the stamp-derivative (V) and model (M) buffers.
+struct StoreRect {
+    int64_t offV, offM;
+    int c_lo, s_lo, nrows, ps;  // ps = ncols * nrows: the plane stride of V
+};
+constexpr int kFillRects = 16;  // rectangles a stamp kernel tabulates per star (else rect_slot)
+
+__device__ __forceinline__ int64_t star_rect_off(const RectMap& m, int j, int l) {
+    return m.srect ? m.srect[(int64_t)j * kStarRects + l] : m.off[m.star_pairs[m.soffs[j] + l]];
+}
+
+// Threads t = first, first + step, ... < nrect tabulate rectangle t of star j
+// (regions in emit order: column by column, nty_j regions a column).
+__device__ __forceinline__ void store_rect_tab(StoreRect* tab, int first, int step, int nrect, int nty_j, int ty0,
+                                               int tx0, int j, int a_y, int a_x, int Rb, int GH, const RectMap* vmap,
+                                               const RectMap* mmap) {
+    for (int l = first; l < nrect; l += step) {
+        const RectGeo g = rect_geo(a_y, a_x, Rb, ty0 + l % nty_j, tx0 + l / nty_j, GH);
+        StoreRect t;
+        t.c_lo = g.c_lo;
+        t.s_lo = g.s_lo;
+        t.nrows = g.nrows;
+        t.ps = g.ncols * g.nrows;
+        t.offV = vmap ? star_rect_off(*vmap, j, l) : 0;
+        t.offM = mmap ? star_rect_off(*mmap, j, l) : 0;
+        tab[l] = t;
+    }
+}
+
+// Index of box entry (row, col) inside its rectangle (plane 0), and the
+// rectangle, or -1 when no region holds the entry.  o: storage row of box row 0.
+__device__ __forceinline__ int tab_entry(int ty0, int ty1, int tx0, int tx1, int nty_j, int top0, int left0, int o,
+                                         int row, int col, const StoreRect* tab, const StoreRect** rect) {
+    const int y = top0 + row, x = left0 + col;
+    if (y < 0 || x < 0) return -1;
+    const int ry = y / TY, rx = x / TX;
+    if (ry < ty0 || ry > ty1 || rx < tx0 || rx > tx1) return -1;
+    const StoreRect& t = tab[(rx - tx0) * nty_j + (ry - ty0)];
+    *rect = &t;
+    return (col - t.c_lo) * t.nrows + (o + row - t.s_lo);
+}
+
+// The store plan of a star whose box meets at most 2 x 2 regions: box entry
+// (row, col) inside [rmin, rmax) x [cmin, cmax) lies in rectangle
+// rid = (col >= csplit) * nty + (row >= rsplit) at index A + col * nrows + row
+// of plane 0 (A folds the rectangle's offset and origin in), planes ps apart.
+struct StorePlan {
+    int64_t AV[kStarRects], AM[kStarRects];
+    int nrows[kStarRects], ps[kStarRects];
+    int rsplit, csplit, rmin, rmax, cmin, cmax, nty;
+};
+
+// Lane `lane` (< 4) of the warp fills rectangle `lane` of the plan; lane 0 the rest.
+__device__ __forceinline__ void store_plan(StorePlan& sp, int lane, int j, int a_y, int a_x, int Rb, int ty0, int ty1,
+                                           int tx0, int tx1, int GH, const RectMap* vmap, const RectMap* mmap) {
+    const int Sb = 2 * Rb + 1, top0 = a_y - Rb - 1, left0 = a_x - Rb - 1;
+    const int o = top0 - (top0 & ~(GH - 1));
+    const int nty_j = ty1 - ty0 + 1, nrect = nty_j * (tx1 - tx0 + 1);
+    if (lane < nrect) {
+        const RectGeo g = rect_geo(a_y, a_x, Rb, ty0 + lane % nty_j, tx0 + lane / nty_j, GH);
+        const int64_t fold = (int64_t)o - g.s_lo - (int64_t)g.c_lo * g.nrows;
+        sp.AV[lane] = vmap ? star_rect_off(*vmap, j, lane) + fold : 0;
+        sp.AM[lane] = mmap ? star_rect_off(*mmap, j, lane) + fold : 0;
+        sp.nrows[lane] = g.nrows;
+        sp.ps[lane] = g.ncols * g.nrows;
+    }
+    if (lane == 0) {
+        sp.nty = nty_j;
+        sp.rsplit = ty1 > ty0 ? (ty0 + 1) * TY - top0 : Sb;
+        sp.csplit = tx1 > tx0 ? (tx0 + 1) * TX - left0 : Sb;
+        sp.rmin = max(0, ty0 * TY - top0);
+        sp.rmax = min(Sb, (ty1 + 1) * TY - top0);
+        sp.cmin = max(0, tx0 * TX - left0);
+        sp.cmax = min(Sb, (tx1 + 1) * TX - left0);
+    }
+}
+
+// Elements of every pair's rectangle (all planes), for the offsets' prefix sum.
+__global__ void k_rect_size(int64_t npairs, const int4* __restrict__ list, const uint32_t* __restrict__ region,
+                            int nty, int GH, int planes, int64_t* size) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i > npairs) return;
+    if (i == npairs) {
+        size[i] = 0;
+        return;
+    }
+    const int4 e = list[i];
+    const int r = (int)region[i];
+    const RectGeo g = rect_geo(e.y, e.z, e.w, r % nty, r / nty, GH);
+    size[i] = (int64_t)planes * g.ncols * g.nrows;
 }
 
 // a[0 .. n) += v in shared memory, 16 bytes at a time (a is 16-byte aligned)
@@ -486,10 +659,10 @@ template <int NTF, int MAXE, bool GRAD, typename T>
 __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, int64_t nlist, FitConst fc, DevPsf P,
                                               const StarCoef* __restrict__ coef, const int32_t* __restrict__ ay,
                                               const int32_t* __restrict__ ax, const double* __restrict__ w,
-                                              const double* __restrict__ sw, T* __restrict__ V,
+                                              const double* __restrict__ sw, T* __restrict__ V, RectMap vmap,
                                               double* __restrict__ colnorm, double* __restrict__ gram,
-                                              T* __restrict__ M, int Rmax, int MS, const int32_t* __restrict__ Rs,
-                                              const int64_t* __restrict__ moff) {
+                                              T* __restrict__ M, RectMap mmap, int Rmax,
+                                              const int32_t* __restrict__ Rs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     AxisTab<T>* tabs = (AxisTab<T>*)smem_raw;  // [corner][axis][Sb]
     __shared__ double sh[32];
@@ -506,11 +679,13 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
         const int Rb = Rs ? Rs[j] : Rmax;  // this star's box radius (<= Rmax, which sized the tables)
         const int Sb = 2 * Rb + 1, S2b = Sb * Sb;
         const int a_y = ay[j], a_x = ax[j];
-        // granule layout of this star's model stamp and of its derivative planes
+        // the regions holding this star's box (stamp rectangles, rect_index)
         constexpr int GH = Gran<T>::H;
-        const int top0 = a_y - Rb - 1, go = top0 - gran_base(top0, GH);
-        const int SRb = gran_rows(Sb, GH);
-        T* Mj = M ? M + (moff ? moff[j] : (int64_t)j * MS) : nullptr;
+        int ty0 = 0, ty1 = -1, tx0 = 0, tx1 = -1;
+        star_tiles(a_y, a_x, Rb, fc.ny, fc.nx, ty0, ty1, tx0, tx1);
+        auto sidx = [&](const RectMap& m, int row, int col, int k) {
+            return rect_index(m, j, a_y, a_x, Rb, ty0, ty1, tx0, tx1, row, col, k, GH);
+        };
         if (!gauss) {
             for (int e = threadIdx.x; e < 8 * Sb; e += NTF) {
                 const int k = e / (2 * Sb), rem = e % (2 * Sb), axis = rem / Sb, idx = rem % Sb;
@@ -538,7 +713,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
             T s = 0, dY = 0, dX = 0, g[3];
             if (gauss) {
                 const T val = gauss_eval<T, GRAD>((T)P.fwhm, c, (T)gy, (T)gx, g[0], g[1], g[2]);
-                if (Mj) Mj[col * SRb + go + row] = val;
+                if (M) {
+                    const int64_t q = sidx(mmap, row, col, 0);
+                    if (q >= 0) M[q] = val;
+                }
             } else {
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -553,7 +731,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                         dX += (T)c.dwdx[k] * pv - (T)c.w[k] * (T)nd.sx * pdu;
                     }
                 }
-                if (Mj) Mj[col * SRb + go + row] = (T)c.flux * s + (T)c.bkg;
+                if (M) {
+                    const int64_t q = sidx(mmap, row, col, 0);
+                    if (q >= 0) M[q] = (T)c.flux * s + (T)c.bkg;
+                }
                 g[0] = (T)c.flux * dY;
                 g[1] = (T)c.flux * dX;
                 g[2] = s;
@@ -610,15 +791,16 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                     cn = cn < kEps64 ? kEps64 : cn;
                     if (threadIdx.x == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
                 }
-                T* Vj = V + (int64_t)j * fc.VS;
 #pragma unroll
                 for (int e = 0; e < RE; ++e) {
                     const int m = threadIdx.x + e * NTF;
                     if (m >= S2b) continue;
-                    const int sidx = (m / Sb) * fc.SR + go + m % Sb;  // the fit box: Sb == fc.S
-                    Vj[sidx] = raw[e][0];
-                    if (p > 1) Vj[fc.PS + sidx] = raw[e][1];
-                    if (p > 2) Vj[2 * fc.PS + sidx] = raw[e][2];
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        if (k >= p) break;
+                        const int64_t at = sidx(vmap, m % Sb, m / Sb, k);  // the fit box: Sb == fc.S
+                        if (at >= 0) V[at] = raw[e][k];
+                    }
                 }
             }
         }
@@ -634,11 +816,15 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                                                       DevPsf P, const StarCoef* __restrict__ coef,
                                                       const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
                                                       const double* __restrict__ w, const double* __restrict__ sw,
-                                                      T* __restrict__ V, double* __restrict__ colnorm,
-                                                      double* __restrict__ gram, T* __restrict__ M, int Rmax, int MS,
-                                                      const int32_t* __restrict__ Rs, const int64_t* __restrict__ moff) {
+                                                      T* __restrict__ V, RectMap vmap, double* __restrict__ colnorm,
+                                                      double* __restrict__ gram, T* __restrict__ M, RectMap mmap,
+                                                      int Rmax, const int32_t* __restrict__ Rs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ StoreRect rtabs[256 / 32][kFillRects];
+    __shared__ StorePlan plans[256 / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    StoreRect* rtab = rtabs[wid];
+    StorePlan& plan = plans[wid];
     AxisTab<T>* tcol = (AxisTab<T>*)smem_raw + wid * 2 * (2 * Rmax + 1);
     const bool gauss = P.kind == CPB_PSF_CIRCULAR_GAUSSIAN;
     DevNode nd{};
@@ -660,10 +846,42 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const int q32 = 32 / Sb, r32 = 32 % Sb;
         AxisTab<T>* trow = tcol + Sb;
         const int oy = ay[j] - Rb, ox = ax[j] - Rb;
-        // granule layout: column c of the box starts at c * SRb, box row r at go + r
+        // the regions holding this star's box: its stamp rectangles, tabulated
+        // when there are at most kFillRects (else rect_slot per entry)
         constexpr int GH = Gran<T>::H;
-        const int go = (oy - 1) - gran_base(oy - 1, GH), SRb = gran_rows(Sb, GH);
-        T* Mj = M ? M + (moff ? moff[j] : (int64_t)j * MS) : nullptr;
+        int ty0 = 0, ty1 = -1, tx0 = 0, tx1 = -1;
+        const int a_y = ay[j], a_x = ax[j];
+        star_tiles(a_y, a_x, Rb, fc.ny, fc.nx, ty0, ty1, tx0, tx1);
+        const int nty_j = ty1 - ty0 + 1, nrect = nty_j * (tx1 - tx0 + 1);
+        const bool wantV = GRAD && !gram, wantM = M != nullptr && !gram;
+        // a plan when every map has per-star rectangle offsets (boxes within 2 x 2 regions)
+        const bool planned = nrect <= kStarRects && (!wantV || vmap.srect) && (!wantM || mmap.srect);
+        const bool tabbed = !planned && nrect <= kFillRects;
+        if (planned)
+            store_plan(plan, lane, j, a_y, a_x, Rb, ty0, ty1, tx0, tx1, GH, wantV ? &vmap : nullptr,
+                       wantM ? &mmap : nullptr);
+        else if (tabbed)
+            store_rect_tab(rtab, lane, 32, nrect, nty_j, ty0, tx0, j, a_y, a_x, Rb, GH, wantV ? &vmap : nullptr,
+                           wantM ? &mmap : nullptr);
+        __syncwarp();
+        const int top0 = a_y - Rb - 1, left0 = a_x - Rb - 1, so = top0 - gran_base(top0, GH);
+        // element index of entry (row, col) in plane 0 of V (isV) or M, and V's plane stride
+        auto store_at = [&](int row, int col, bool isV, int64_t* ps) -> int64_t {
+            if (planned) {
+                if (row < plan.rmin || row >= plan.rmax || col < plan.cmin || col >= plan.cmax) return -1;
+                const int rid = (col >= plan.csplit ? plan.nty : 0) + (row >= plan.rsplit ? 1 : 0);
+                *ps = plan.ps[rid];
+                return (isV ? plan.AV[rid] : plan.AM[rid]) + (int64_t)col * plan.nrows[rid] + row;
+            }
+            if (tabbed) {
+                const StoreRect* t = nullptr;
+                const int e = tab_entry(ty0, ty1, tx0, tx1, nty_j, top0, left0, so, row, col, rtab, &t);
+                if (e < 0) return -1;
+                *ps = t->ps;
+                return (isV ? t->offV : t->offM) + e;
+            }
+            return rect_slot(isV ? vmap : mmap, j, a_y, a_x, Rb, ty0, ty1, tx0, tx1, row, col, GH, ps);
+        };
         if (!gauss) {
             for (int idx = lane; idx < 2 * Sb; idx += 32) {
                 if (idx < Sb) axis_tab_x(nd, nd.sx * ((double)(ox + idx) - cx) + nd.ox, tcol[idx]);
@@ -705,7 +923,9 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             for (int m = lane; m < S2b; m += 32) {
                 T val, a, b, c;
                 eval_px(row, col, val, a, b, c);
-                Mj[col * SRb + go + row] = val;
+                int64_t ps;
+                const int64_t q = store_at(row, col, false, &ps);
+                if (q >= 0) M[q] = val;
                 row += r32;
                 col += q32;
                 if (row >= Sb) {
@@ -719,7 +939,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             // accumulate; a second sweep over the star's block, still in L2,
             // applies the inverse norms
             double acc[6] = {0, 0, 0, 0, 0, 0};
-            T* Vj = gram ? nullptr : V + (int64_t)j * fc.VS;
+
             int row = lane % Sb, col = lane / Sb;
             for (int m = lane; m < S2b; m += 32) {
                 const int gy = oy + row, gx = ox + col;
@@ -730,7 +950,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 if (use || (M && !gram)) {
                     T val, a, b, c;
                     eval_px(row, col, val, a, b, c);
-                    if (M && !gram) Mj[col * SRb + go + row] = val;
+                    if (M && !gram) {
+                        int64_t ps;
+                        const int64_t q = store_at(row, col, false, &ps);
+                        if (q >= 0) M[q] = val;
+                    }
                     if (use) {
                         const T sq = (T)sw[q];
                         r0 = sq * a;
@@ -751,11 +975,14 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                         }
                     }
                 }
-                if (!gram) {  // the fit box: SRb == fc.SR
-                    const int sidx = col * SRb + go + row;
-                    Vj[sidx] = r0;
-                    if (p > 1) Vj[fc.PS + sidx] = r1;
-                    if (p > 2) Vj[2 * fc.PS + sidx] = r2;
+                if (!gram && onimg) {  // the fit box; off-image entries are not stored
+                    int64_t ps;
+                    const int64_t q = store_at(row, col, true, &ps);
+                    if (q >= 0) {
+                        V[q] = r0;
+                        if (p > 1) V[q + ps] = r1;
+                        if (p > 2) V[q + 2 * ps] = r2;
+                    }
                 }
                 row += r32;
                 col += q32;
@@ -796,10 +1023,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // order), the deterministic replacement of the reference's scatter-adds.
 // A block owns a TY x TX pixel region; warp w takes the region's stars
 // w, w + NW, w + 2 NW, ... in list order and adds them into its own copy of
-// the region in shared memory.  A star's part of the region is a rectangle of
-// stamp granules (GH rows of one stamp column, GH = 16 bytes / element): the
-// region's rows and the stamp columns share the GH-row alignment, so every
-// load is a whole 16-byte granule.  The warp walks its stars' granules in
+// the region in shared memory.  A star's part of the region is a dense
+// rectangle of stamp granules (GH rows of one stamp column, GH = 16 bytes /
+// element) stored at the pair's offset (roff), the rectangles of a region's
+// stars one after another: the region's stamps are one contiguous run, read
+// in whole 16-byte granules.  The warp walks its stars' granules in
 // 32-granule slots (one star a slot, a star's last slot padded) and loads
 // KSLOT slots -- KSLOT * p granules a lane -- before adding any, slot by slot.
 // Each pixel is the sum of the warps' copies in warp order: a fixed order
@@ -825,7 +1053,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
                                                const int32_t* __restrict__ tord,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
-                                               int Rbox, int64_t stride, const int64_t* __restrict__ soff,
+                                               int Rbox, const int64_t* __restrict__ roff,
                                                const double* __restrict__ vt, const double* __restrict__ cn,
                                                const TU* u_src, double u_sign,
                                                TU* outu, double* outd, const uint8_t* __restrict__ umask,
@@ -838,7 +1066,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
     constexpr int NPL = KIND == KIND_JV ? 3 : 1;
     extern __shared__ __align__(16) unsigned char g_smem[];
     double* parts = (double*)g_smem;     // [NW][TX][TY], column-major per warp
-    __shared__ int s_j[NT];
+    __shared__ int64_t s_off[NT];
     __shared__ int s_ay[NT];
     __shared__ int s_ax[NT];
     __shared__ int s_rb[NT];
@@ -880,7 +1108,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         }
         if (keep) {
             const int pos = before + __popc(bal & ((1u << lane) - 1u));
-            s_j[pos] = ent.x;
+            s_off[pos] = roff[li];  // the pair's stamp rectangle
             s_ay[pos] = ent.y;
             s_ax[pos] = ent.z;
             s_rb[pos] = ent.w;
@@ -891,7 +1119,8 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         __syncthreads();
         // the current star's rectangle of granules inside the region
         int e = wid, c = 0;  // star (staged index) and slot
-        int tot = 0, nga = 1, cl0 = 0, gl0 = 0, SRb = 0, PSb = 0;
+        int tot = 0, nga = 1, cl0 = 0, gl0 = 0;
+        int64_t PSb = 0;
         float inv_nga = 1.0f;
         const TS* base = src;
         auto star_geometry = [&]() {
@@ -901,8 +1130,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             const int Sb = 2 * Rb + 1;
             const int left0 = s_ax[e] - Rb - 1, top0 = s_ay[e] - Rb - 1;
             const int b0 = gran_base(top0, GH);
-            SRb = gran_rows(Sb, GH);
-            PSb = Sb * SRb;
+            const int SRb = gran_rows(Sb, GH);
             cl0 = max(left0, C0) - C0;
             const int cl1 = min(left0 + Sb - 1, C0 + TX - 1) - C0;
             const int r_lo = max(b0, R0), r_hi = min(b0 + SRb, R0 + TY);  // multiples of GH
@@ -910,9 +1138,9 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             nga = max((r_hi - r_lo) / GH, 0);
             tot = cl1 >= cl0 ? (cl1 - cl0 + 1) * nga : 0;
             inv_nga = 1.0f / (float)max(nga, 1);
-            // storage offset of the rectangle's first granule
-            base = src + (soff ? soff[s_j[e]] : (int64_t)s_j[e] * stride) + (int64_t)(C0 + cl0 - left0) * SRb +
-                   (r_lo - b0);
+            // the dense rectangle: granule t = cc * nga + gg at t * GH, planes tot * GH apart
+            PSb = (int64_t)tot * GH;
+            base = src + s_off[e];
         };
         star_geometry();
         while (e < total && tot == 0) {
@@ -931,10 +1159,10 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                     if (t < tot) {
                         const int cc = (int)(((float)t + 0.5f) * inv_nga);
                         const int gg = t - cc * nga;
-                        const TS* g = base + (int64_t)cc * SRb + gg * GH;
+                        const TS* g = base + (int64_t)t * GH;
 #pragma unroll
                         for (int k = 0; k < NPL; ++k)
-                            if (k < p) ld_gran(g + (int64_t)k * PSb, raw[q][k]);
+                            if (k < p) ld_gran(g + k * PSb, raw[q][k]);
                         dst[q] = (cl0 + cc) * TY + (gl0 + gg) * GH;
                     }
                     if ((c + 1) * 32 < tot) {
@@ -1031,23 +1259,33 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
 }
 
 // J^T u for the stars of `list` (apply_JT!, :55-85): one warp per star.
-// The lanes walk the star's granules (GH rows of one stamp column): the
-// granule of each derivative plane and the matching GH pixels of u, all
-// 16-byte loads, JU granules in flight per lane.  Writes z[j*p+k] =
-// sum_m V[j,k,m] u[pix(m)] * uscale / colnorm[j,k] (V holds the unscaled
-// weighted derivatives).  LSQR form: v_new = z - beta * v_old / alpha_old and
-// alpha = ||v_new|| (Krylov lsqr step 2).  Sums are FP64 for either stamp type.
+// The star's stamp lives in the rectangles of the regions its box meets
+// (tfit: soffs / star_pairs / off); the lanes walk the granules of those
+// rectangles as one sequence (GH rows of one stamp column: the granule of each
+// derivative plane and the matching GH pixels of u, all 16-byte loads), JU
+// granules in flight per lane.  Writes z[j*p+k] = sum_m V[j,k,m] u[pix(m)] *
+// uscale / colnorm[j,k] (V holds the unscaled weighted derivatives).  LSQR
+// form: v_new = z - beta * v_old / alpha_old and alpha = ||v_new|| (Krylov
+// lsqr step 2).  Sums are FP64 for either stamp type.
+constexpr int kJTRects = 16;  // rectangles a warp tabulates at a time
 template <bool LSQR, typename TS, typename TU>
 __global__ void __launch_bounds__(256, 3) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                             const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
-                                            const TS* __restrict__ V, const double* __restrict__ cn,
+                                            const TS* __restrict__ V, RectMap vmap, const double* __restrict__ cn,
                                             const TU* __restrict__ u, double* __restrict__ z, Scalars* sc,
                                             Reducer red) {
     static_assert(sizeof(TS) == sizeof(TU), "u granules match stamp granules");
     constexpr int GH = Gran<TS>::H;
     constexpr int JU = 2;
+    struct RectTab {
+        int64_t off;
+        int tot, nga, x0, y0;  // granules, granule rows, first image column and row (0-based)
+        float inv_nga;
+    };
+    __shared__ RectTab tabs[256 / 32][kJTRects];
     __shared__ double sh[32];
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    RectTab* tab = tabs[wid];
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = (gridDim.x * (int64_t)blockDim.x) >> 5;
     double uscale = 1.0, beta = 0.0, inv_alpha = 0.0;
@@ -1057,57 +1295,78 @@ __global__ void __launch_bounds__(256, 3) k_JT(const int32_t* __restrict__ list,
         beta = sc->beta;
         inv_alpha = sc->inv_alpha;
     }
-    const int p = fc.p, S = fc.S, R = fc.R, SR = fc.SR, PS = fc.PS;
-    const int NG = SR / GH, G = S * NG;
-    const int dcol = 32 / NG, dgr = 32 % NG;
+    const int p = fc.p, R = fc.R;
     const int ny = fc.ny, nx = fc.nx;
     const bool uvec = (ny % GH) == 0;
     double part = 0.0;
     for (int64_t li = warp; li < nlist; li += nwarps) {
         const int j = list[li];
-        const int top0 = ay[j] - R - 1, left0 = ax[j] - R - 1;
-        const int b0 = gran_base(top0, GH);
-        const TS* Vj = V + (int64_t)j * fc.VS;
+        const int a_y = ay[j], a_x = ax[j];
+        int ty0 = 0, ty1 = -1, tx0 = 0, tx1 = -1;
+        star_tiles(a_y, a_x, R, ny, nx, ty0, ty1, tx0, tx1);
+        const int nty_j = ty1 - ty0 + 1, nrect = (tx1 - tx0 + 1) * nty_j;
+        const int left0 = a_x - R - 1, b0 = gran_base(a_y - R - 1, GH);
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        int col = lane / NG, gr = lane % NG;
-        for (int g0 = lane; g0 < G; g0 += 32 * JU) {
-            TS v[JU][3][GH];
-            TU uu[JU][GH];
-            bool ok[JU];
-#pragma unroll
-            for (int q = 0; q < JU; ++q) {
-                const int gx = left0 + col, gy = b0 + gr * GH;
-                ok[q] = g0 + 32 * q < G && gx >= 0 && gx < nx;
-                if (ok[q]) {
-                    const TS* e = Vj + col * SR + gr * GH;
-                    ld_gran(e, v[q][0]);
-                    if (p > 1) ld_gran(e + PS, v[q][1]);
-                    if (p > 2) ld_gran(e + 2 * PS, v[q][2]);
-                    const int64_t pq = gy + (int64_t)gx * ny;
-                    if (uvec && gy >= 0 && gy + GH <= ny) {
-                        ld_px16(u + pq, uu[q]);
-                    } else {
-#pragma unroll
-                        for (int r = 0; r < GH; ++r)
-                            uu[q][r] = (gy + r >= 0 && gy + r < ny) ? __ldg(u + pq + r) : (TU)0;
-                    }
-                }
-                gr += dgr;
-                col += dcol;
-                if (gr >= NG) {
-                    gr -= NG;
-                    col += 1;
-                }
+        for (int r0 = 0; r0 < nrect; r0 += kJTRects) {
+            const int nr = min(kJTRects, nrect - r0);
+            __syncwarp();  // the previous star's / chunk's table is no longer read
+            if (lane < nr) {
+                const int l = r0 + lane;
+                const int ry = ty0 + l % nty_j, rx = tx0 + l / nty_j;
+                const RectGeo g = rect_geo(a_y, a_x, R, ry, rx, GH);
+                RectTab t;
+                t.off = star_rect_off(vmap, j, l);
+                t.nga = g.nrows / GH;
+                t.inv_nga = 1.0f / (float)max(t.nga, 1);
+                t.tot = g.ncols * t.nga;
+                t.x0 = left0 + g.c_lo;
+                t.y0 = b0 + g.s_lo;
+                tab[lane] = t;
             }
+            __syncwarp();
+            // this lane's granules: lane, lane + 32, ... of the chunk's rectangles in order
+            int r = 0, t = lane;
+            while (r < nr && t >= tab[r].tot) t -= tab[r++].tot;
+            while (r < nr) {
+                TS v[JU][3][GH];
+                TU uu[JU][GH];
+                bool ok[JU];
 #pragma unroll
-            for (int q = 0; q < JU; ++q) {
-                if (!ok[q]) continue;
+                for (int q = 0; q < JU; ++q) {
+                    ok[q] = false;
+                    if (r >= nr) continue;
+                    const RectTab& T = tab[r];
+                    const int cc = (int)(((float)t + 0.5f) * T.inv_nga);
+                    const int gg = t - cc * T.nga;
+                    const int gx = T.x0 + cc, gy = T.y0 + gg * GH;
+                    ok[q] = gx < nx;
+                    if (ok[q]) {
+                        const TS* e = V + T.off + (int64_t)t * GH;
+                        const int64_t ps = (int64_t)T.tot * GH;
+                        ld_gran(e, v[q][0]);
+                        if (p > 1) ld_gran(e + ps, v[q][1]);
+                        if (p > 2) ld_gran(e + 2 * ps, v[q][2]);
+                        const int64_t pq = gy + (int64_t)gx * ny;
+                        if (uvec && gy + GH <= ny) {
+                            ld_px16(u + pq, uu[q]);
+                        } else {
 #pragma unroll
-                for (int r = 0; r < GH; ++r) {
-                    const double ur = (double)uu[q][r];
-                    a0 += (double)v[q][0][r] * ur;
-                    if (p > 1) a1 += (double)v[q][1][r] * ur;
-                    if (p > 2) a2 += (double)v[q][2][r] * ur;
+                            for (int rr = 0; rr < GH; ++rr) uu[q][rr] = gy + rr < ny ? __ldg(u + pq + rr) : (TU)0;
+                        }
+                    }
+                    t += 32;
+                    while (r < nr && t >= tab[r].tot) t -= tab[r++].tot;
+                }
+#pragma unroll
+                for (int q = 0; q < JU; ++q) {
+                    if (!ok[q]) continue;
+#pragma unroll
+                    for (int rr = 0; rr < GH; ++rr) {
+                        const double ur = (double)uu[q][rr];
+                        a0 += (double)v[q][0][rr] * ur;
+                        if (p > 1) a1 += (double)v[q][1][rr] * ur;
+                        if (p > 2) a2 += (double)v[q][2][rr] * ur;
+                    }
                 }
             }
         }
@@ -1572,6 +1831,10 @@ struct TileLists {
     int32_t *start = nullptr, *end = nullptr;
     int4* list = nullptr;     // (star, anchor y, anchor x, box radius) per (tile, star) pair
     int32_t* order = nullptr; // the regions by decreasing star count: block b of a gather takes order[b]
+    uint32_t* region = nullptr;   // per pair: its region (ty + tx * nty)
+    int32_t* soffs = nullptr;     // per star: its first emit index (n_act + 1)
+    int32_t* star_pairs = nullptr;  // per emit index: the pair's list position
+    int64_t npairs = 0;
 };
 
 TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_t* ay, const int32_t* ax,
@@ -1593,8 +1856,13 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
     uint32_t* k0 = S<uint32_t>(ctx, (t + "_k0").c_str(), npairs);
     uint32_t* k1 = S<uint32_t>(ctx, (t + "_k1").c_str(), npairs);
     int32_t* v0 = S<int32_t>(ctx, (t + "_v0").c_str(), npairs);
+    int32_t* emit_j = S<int32_t>(ctx, (t + "_emit_j").c_str(), npairs);
     TileLists tl;
-    int32_t* sorted_j = S<int32_t>(ctx, (t + "_sorted").c_str(), npairs);
+    tl.npairs = npairs;
+    tl.region = k1;
+    tl.soffs = offs;
+    tl.star_pairs = S<int32_t>(ctx, (t + "_star_pairs").c_str(), npairs);
+    int32_t* sorted_o = S<int32_t>(ctx, (t + "_sorted").c_str(), npairs);
     tl.list = S<int4>(ctx, (t + "_list").c_str(), npairs);
     const int64_t ntiles = (int64_t)nty * ntx;
     tl.start = S<int32_t>(ctx, (t + "_start").c_str(), ntiles);
@@ -1603,17 +1871,18 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
     check(cudaMemsetAsync(tl.start, 0, sizeof(int32_t) * ntiles, st), "memset");
     check(cudaMemsetAsync(tl.end, 0, sizeof(int32_t) * ntiles, st), "memset");
     if (npairs > 0) {
-        k_tile_emit<<<nblk(n_act), 256, 0, st>>>(n_act, ay, ax, Rs, Rconst, ny, nx, nty, offs, k0, v0);
+        k_tile_emit<<<nblk(n_act), 256, 0, st>>>(n_act, ay, ax, Rs, Rconst, ny, nx, nty, offs, k0, v0, emit_j);
         check(cudaGetLastError(), "k_tile_emit");
         int end_bit = 1;
         while ((1LL << end_bit) < ntiles) ++end_bit;
         tmp = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, v0, sorted_j, npairs, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp, k0, k1, v0, sorted_o, npairs, 0, end_bit, st);
         dtmp = scratch(ctx, (t + "_sort_tmp").c_str(), tmp);
-        cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, sorted_j, npairs, 0, end_bit, st);
+        cub::DeviceRadixSort::SortPairs(dtmp, tmp, k0, k1, v0, sorted_o, npairs, 0, end_bit, st);
         k_tile_bounds<<<nblk(npairs), 256, 0, st>>>(npairs, k1, tl.start, tl.end);
         check(cudaGetLastError(), "k_tile_bounds");
-        k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_j, ay, ax, Rs, Rconst, tl.list);
+        k_tile_pack<<<nblk(npairs), 256, 0, st>>>(npairs, sorted_o, emit_j, ay, ax, Rs, Rconst, tl.list,
+                                                  tl.star_pairs);
         check(cudaGetLastError(), "k_tile_pack");
     }
     // heaviest regions first, so that the last wave of a gather is its lightest
@@ -1631,6 +1900,25 @@ TileLists build_tiles(cpb_ctx* ctx, const char* tag, int64_t n_act, const int32_
     return tl;
 }
 
+// Element offsets of a list's rectangles for granules of GH rows and `planes`
+// planes: a prefix sum of the rectangle sizes (npairs + 1 entries; the last is
+// the total).  Returns the total.
+int64_t rect_offsets(cpb_ctx* ctx, const char* tag, const TileLists& tl, int nty, int GH, int planes, int64_t* off) {
+    cudaStream_t st = ctx->stream;
+    const std::string t(tag);
+    int64_t* size = S<int64_t>(ctx, (t + "_rsize").c_str(), tl.npairs + 1);
+    k_rect_size<<<nblk(tl.npairs + 1), 256, 0, st>>>(tl.npairs, tl.list, tl.region, nty, GH, planes, size);
+    check(cudaGetLastError(), "k_rect_size");
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, size, off, (int)(tl.npairs + 1), st);
+    void* dtmp = scratch(ctx, (t + "_rscan_tmp").c_str(), tmp);
+    cub::DeviceScan::ExclusiveSum(dtmp, tmp, size, off, (int)(tl.npairs + 1), st);
+    int64_t total = 0;
+    check(cudaMemcpyAsync(&total, off + tl.npairs, sizeof(int64_t), cudaMemcpyDeviceToHost, st), "d2h");
+    check(cudaStreamSynchronize(st), "sync");
+    return total;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1642,15 +1930,28 @@ namespace {
 size_t carve_size(size_t bytes) { return (std::max<size_t>(bytes, 256) + 255) & ~size_t(255); }
 
 // The tile lists of build_tiles for n stars of box radius Rb.
-size_t tiles_bound(int64_t n, int Rb, int64_t ntiles) {
+// Upper bound of the (region, star) pairs of n boxes of radius Rb.
+int64_t pairs_bound(int64_t n, int Rb) {
     const int64_t Sb = 2 * (int64_t)Rb + 1;
-    const int64_t per = ((Sb + TY - 1) / TY + 1) * ((Sb + TX - 1) / TX + 1);
-    const int64_t npairs = std::max<int64_t>(n * per, 1);
+    return std::max<int64_t>(n * ((Sb + TY - 1) / TY + 1) * ((Sb + TX - 1) / TX + 1), 1);
+}
+
+// One rect_map: the offsets, the rectangle sizes, the scan temporaries and the
+// per-star offsets (srect).
+size_t rect_map_bound(int64_t npairs, int64_t n) {
+    size_t tmp = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tmp, (int64_t*)nullptr, (int64_t*)nullptr, (int)(npairs + 1));
+    return 2 * carve_size(8 * (npairs + 1)) + carve_size(tmp) + carve_size(8 * kStarRects * n);
+}
+
+size_t tiles_bound(int64_t n, int Rb, int64_t ntiles) {
+    const int64_t npairs = pairs_bound(n, Rb);
     size_t b = 2 * carve_size(4 * (n + 1));
     size_t tmp = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, tmp, (int32_t*)nullptr, (int32_t*)nullptr, (int)(n + 1));
     b += carve_size(tmp);
-    b += 4 * carve_size(4 * npairs) + carve_size(16 * npairs);
+    // keys (2), values, emit_j, star_pairs, sorted; the packed list
+    b += 6 * carve_size(4 * npairs) + carve_size(16 * npairs);
     b += 3 * carve_size(4 * ntiles) + carve_size(8 * ntiles) + carve_size(4 * ntiles);
     int end_bit = 1;
     while ((1LL << end_bit) < ntiles) ++end_bit;
@@ -1665,12 +1966,14 @@ size_t tiles_bound(int64_t n, int Rb, int64_t ntiles) {
     return b;
 }
 
-// One precision form (Form<TS, TU>): stamps, model stamps, pixel vectors.
+// One precision form (Form<TS, TU>): stamps and model stamps (a star's
+// rectangles hold at most its column storage), their rectangle maps, pixel vectors.
 template <typename TS, typename TU>
-size_t form_bound(int64_t n, int p, int S, int64_t model_entries_per_star, bool per_star_offsets, int64_t npix) {
+size_t form_bound(int64_t n, int p, int S, int64_t model_entries, int64_t npairs_fit, int64_t npairs_mod,
+                  int64_t npix) {
     size_t b = carve_size((size_t)p * S * gran_rows(S, Gran<TS>::H) * n * sizeof(TS));
-    b += carve_size((size_t)model_entries_per_star * n * sizeof(TS));
-    if (per_star_offsets) b += carve_size(8 * n);
+    b += carve_size((size_t)model_entries * sizeof(TS));
+    b += rect_map_bound(npairs_fit, n) + rect_map_bound(npairs_mod, n);
     b += 2 * carve_size(npix * sizeof(TU));
     return b;
 }
@@ -1719,17 +2022,19 @@ size_t sim_scratch_bound(const cpb_sim_params* P, int64_t ny, int64_t nx, int64_
     b += 8 * carve_size(8 * np) + 2 * carve_size(sizeof(StarCoef) * n);           // solver state
     b += 3 * carve_size(n) + 4 * carve_size(4 * n) + carve_size(4);
     b += 2 * carve_size(sel_tmp);                                                  // live_tmp, newf_tmp
-    const bool per_star = P->model_rad_auto != 0;
+    // with :auto the model lists are counted at the fit box here (checked again in the fit)
+    const int64_t pf = pairs_bound(n, R), pm = pairs_bound(n, Rm);
+    const int64_t me32 = (int64_t)Sm * gran_rows(Sm, Gran<float>::H) * n;
+    const int64_t me64 = (int64_t)Sm * gran_rows(Sm, Gran<double>::H) * n;
     if (P->precision == CPB_PREC_MIXED) {
-        b += form_bound<float, float>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<float>::H), per_star, npix);
-        if (P->refine_iters > 0)
-            b += form_bound<double, double>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<double>::H), per_star, npix);
+        b += form_bound<float, float>(n, p, S, me32, pf, pm, npix);
+        if (P->refine_iters > 0) b += form_bound<double, double>(n, p, S, me64, pf, pm, npix);
     } else {
-        b += form_bound<double, double>(n, p, S, (int64_t)Sm * gran_rows(Sm, Gran<double>::H), per_star, npix);
+        b += form_bound<double, double>(n, p, S, me64, pf, pm, npix);
     }
-    // final pass: gram, err, resid, FP64 model stamps (+ offsets), spread tables, diagnostics
+    // final pass: gram, err, resid, FP64 model stamps and their map, spread tables, diagnostics
     b += carve_size(48 * n) + carve_size(8 * np) + carve_size(8 * npix);
-    b += carve_size((size_t)Sm * gran_rows(Sm, Gran<double>::H) * n * 8) + (per_star ? carve_size(8 * n) : 0);
+    b += carve_size(me64 * 8) + rect_map_bound(pm, n);
     b += carve_size(8 * kSpreadRuleLen) + carve_size(8 * spread_tab_len(R)) + carve_size(56 * n);
     return b;
 }
@@ -1744,12 +2049,10 @@ namespace {
 // vectors (weighted residual, u) as TU.
 template <typename TS, typename TU>
 struct Form {
-    FitConst fc;              // the fit constants with TS's stamp layout
-    TS* V = nullptr;          // n_act x fc.VS
-    TS* M = nullptr;          // model stamps: n_act x MS, or per-star blocks at d_moff (model_rad = :auto)
-    int MS = 0;
-    int64_t* d_moff = nullptr;
-    int64_t mtotal = 0;
+    FitConst fc;              // the fit constants
+    TS* V = nullptr;          // stamp derivatives: p planes per rectangle of the fit-box lists (vmap)
+    TS* M = nullptr;          // model stamps: one plane per rectangle of the model-box lists (mmap)
+    RectMap vmap{}, mmap{};
     TU* wt_resid = nullptr;
     TU* u = nullptr;
     bool m_fresh = false;     // M holds the current-theta model of the live stars (written by the fill)
@@ -1775,13 +2078,12 @@ class SimFit {
     bool setup();  // false: the fit ended early (no stars, nothing active)
     template <typename TS, typename TU>
     Form<TS, TU> make_form(const char* tag);
-    template <typename TS>
-    void model_layout(const char* tag, int& MS, int64_t*& d_moff, int64_t& mtotal);
+    RectMap rect_map(const char* tag, const TileLists& tl, int GH, int planes, int Rmax, int64_t& total);
     template <typename TS, typename TU>
     void launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist);
     template <typename TS>
-    void launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* d_moff, const int32_t* list,
-                           int64_t nlist, const StarCoef* cf);
+    void launch_eval_model(const FitConst& f, TS* M, const RectMap& mmap, const int32_t* list, int64_t nlist,
+                           const StarCoef* cf);
     template <typename TS, typename TU>
     void launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const int32_t* list, int64_t nlist,
                        const StarCoef* cf, TU* outu, double* outd, const double* ref, double* result);
@@ -1891,25 +2193,24 @@ void SimFit::update_live_list() {
     n_live = h;
 }
 
-// Model-stamp layout of element type TS: one block of MS entries a star, or
-// with per-star radii (:auto) each star's own block at d_moff[j].
-template <typename TS>
-void SimFit::model_layout(const char* tag, int& MS, int64_t*& d_moff, int64_t& mtotal) {
-    constexpr int GH = Gran<TS>::H;
-    MS = Sm * gran_rows(Sm, GH);
-    d_moff = nullptr;
-    mtotal = (int64_t)MS * n_act;
-    if (d_modelR) {
-        std::vector<int64_t> h_moff(n_act);
-        mtotal = 0;
-        for (int64_t j = 0; j < n_act; ++j) {
-            h_moff[j] = mtotal;
-            const int sj = 2 * h_modelR[j] + 1;
-            mtotal += (int64_t)sj * gran_rows(sj, GH);
-        }
-        d_moff = S_<int64_t>((std::string("model_off") + tag).c_str(), n_act);
-        check(cudaMemcpyAsync(d_moff, h_moff.data(), sizeof(int64_t) * n_act, cudaMemcpyHostToDevice, st), "h2d");
+// The rectangles of list tl with granules of GH rows and `planes` planes each:
+// the pair map and the offsets (total: the elements of every rectangle).
+RectMap SimFit::rect_map(const char* tag, const TileLists& tl, int GH, int planes, int Rmax, int64_t& total) {
+    RectMap m;
+    m.soffs = tl.soffs;
+    m.star_pairs = tl.star_pairs;
+    m.planes = planes;
+    int64_t* off = S_<int64_t>(tag, tl.npairs + 1);
+    total = rect_offsets(ctx, tag, tl, fc.nty, GH, planes, off);
+    m.off = off;
+    m.srect = nullptr;
+    if (2 * Rmax + 1 <= TX + 1 && 2 * Rmax + 1 <= TY + 1) {  // every box meets at most 2 x 2 regions
+        int64_t* sr = S_<int64_t>((std::string(tag) + "_srect").c_str(), n_act * kStarRects);
+        k_star_rects<<<nblk(n_act * kStarRects), 256, 0, st>>>(n_act, tl.soffs, tl.star_pairs, off, sr);
+        check(cudaGetLastError(), "k_star_rects");
+        m.srect = sr;
     }
+    return m;
 }
 
 template <typename TS, typename TU>
@@ -1917,16 +2218,15 @@ Form<TS, TU> SimFit::make_form(const char* tag) {
     Form<TS, TU> F;
     constexpr int GH = Gran<TS>::H;
     F.fc = fc;
-    F.fc.SR = gran_rows(fc.S, GH);
-    F.fc.PS = fc.S * F.fc.SR;
-    F.fc.VS = p * F.fc.PS;
     const std::string t(tag);
-    F.V = S_<TS>(("V" + t).c_str(), (int64_t)F.fc.VS * n_act);
-    // entries outside each box stay zero for the whole fit (the anchors are fixed)
-    check(cudaMemsetAsync(F.V, 0, sizeof(TS) * (int64_t)F.fc.VS * n_act, st), "memset");
-    model_layout<TS>(tag, F.MS, F.d_moff, F.mtotal);
-    F.M = S_<TS>(("model_stamps" + t).c_str(), F.mtotal);
-    check(cudaMemsetAsync(F.M, 0, sizeof(TS) * F.mtotal, st), "memset");
+    int64_t nv = 0, nm = 0;
+    F.vmap = rect_map(("V_off" + t).c_str(), tfit, GH, p, fc.R, nv);
+    F.mmap = rect_map(("M_off" + t).c_str(), tmod, GH, 1, model_R, nm);
+    F.V = S_<TS>(("V" + t).c_str(), nv);
+    F.M = S_<TS>(("model_stamps" + t).c_str(), nm);
+    // rectangle entries outside the boxes stay zero for the whole fit (the anchors are fixed)
+    check(cudaMemsetAsync(F.V, 0, sizeof(TS) * std::max<int64_t>(nv, 1), st), "memset");
+    check(cudaMemsetAsync(F.M, 0, sizeof(TS) * std::max<int64_t>(nm, 1), st), "memset");
     F.wt_resid = S_<TU>(("wt_resid" + t).c_str(), npix);
     F.u = S_<TU>(("lsqr_u" + t).c_str(), npix);
     return F;
@@ -1955,14 +2255,13 @@ void SimFit::launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist) {
         const int wpb = (int)(thr / 32);
         const unsigned gbw =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-        k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V, cn,
-                                                         nullptr, Mo, fc.R, F.MS, nullptr, nullptr);
+        k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V, F.vmap,
+                                                         cn, nullptr, Mo, F.mmap, fc.R, nullptr);
     } else {
         const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
         launch_k_eval<true, TS>(fc.S2, grid, tab_bytes * fc.S, st, list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V,
-                                cn, (double*)nullptr, Mo, fc.R, F.MS, (const int32_t*)nullptr,
-                                (const int64_t*)nullptr);
+                                F.vmap, cn, (double*)nullptr, Mo, F.mmap, fc.R, (const int32_t*)nullptr);
     }
     check(cudaGetLastError(), "k_eval_fill");
     F.m_fresh = writeM;
@@ -1970,8 +2269,8 @@ void SimFit::launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist) {
 
 // model values at `cf` for the stars of `list` into M (value-only stamp evaluation)
 template <typename TS>
-void SimFit::launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* d_moff, const int32_t* list,
-                               int64_t nlist, const StarCoef* cf) {
+void SimFit::launch_eval_model(const FitConst& f, TS* M, const RectMap& mmap, const int32_t* list, int64_t nlist,
+                               const StarCoef* cf) {
     if (nlist <= 0) return;
     KernelScope ks_(ctx, "k_eval_model", (double)nlist * ((double)Sm * Sm * sizeof(TS) + sizeof(StarCoef)));
     if (warp_eval) {
@@ -1984,14 +2283,14 @@ void SimFit::launch_eval_model(const FitConst& f, TS* M, int MS, const int64_t* 
         const int wpb = (int)(thr / 32);
         const unsigned gbw =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-        k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, f, dp, cf, ay, ax, w, sw, (TS*)nullptr, cn,
-                                                          nullptr, M, model_R, MS, d_modelR, d_moff);
+        k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, f, dp, cf, ay, ax, w, sw, (TS*)nullptr,
+                                                          RectMap{}, cn, nullptr, M, mmap, model_R, d_modelR);
     } else {
         const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
         launch_k_eval<false, TS>((int64_t)Sm * Sm, grid, tab_bytes * Sm, st, list, nlist, f, dp, cf, ay, ax, w, sw,
-                                 (TS*)nullptr, cn, (double*)nullptr, M, model_R, MS, (const int32_t*)d_modelR,
-                                 d_moff);
+                                 (TS*)nullptr, RectMap{}, cn, (double*)nullptr, M, mmap, model_R,
+                                 (const int32_t*)d_modelR);
     }
     check(cudaGetLastError(), "k_eval_model");
 }
@@ -2001,7 +2300,7 @@ void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const
                            const StarCoef* cf, TU* outu, double* outd, const double* ref, double* result) {
     NvtxRange nv_(mode == MODE_CUR ? "cpb:sim:render_residual"
                                    : (mode == MODE_CAND ? "cpb:sim:render_trial" : "cpb:sim:render_freeze"));
-    if (!(mode == MODE_CUR && F.m_fresh)) launch_eval_model<TS>(F.fc, F.M, F.MS, F.d_moff, list, nlist, cf);
+    if (!(mode == MODE_CUR && F.m_fresh)) launch_eval_model<TS>(F.fc, F.M, F.mmap, list, nlist, cf);
     F.m_fresh = false;
     const double px_bytes =
         mode == MODE_CUR ? 17.0 + sizeof(TU) : (mode == MODE_CAND ? 17.0 : 16.0);
@@ -2013,9 +2312,9 @@ void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const
     const unsigned g = (unsigned)ntiles;
     const auto& tl = tmod;
 #define CPB_RENDER(MD)                                                                                               \
-    k_gather<KIND_M, MD, TS, TU><<<g, NT, kGatherSmem, st>>>(F.fc, tl.start, tl.end, tl.list, tl.order, incl, F.M, model_R,     \
-                                                   F.MS, F.d_moff, nullptr, nullptr, nullptr, 0.0, outu, outd, umask, w, sw, \
-                                                   ref, sc, red, result)
+    k_gather<KIND_M, MD, TS, TU><<<g, NT, kGatherSmem, st>>>(F.fc, tl.start, tl.end, tl.list, tl.order, incl, F.M,   \
+                                                             model_R, F.mmap.off, nullptr, nullptr, nullptr, 0.0,     \
+                                                             outu, outd, umask, w, sw, ref, sc, red, result)
     switch (mode) {
         case MODE_CUR: CPB_RENDER(MODE_CUR); break;
         case MODE_CAND: CPB_RENDER(MODE_CAND); break;
@@ -2320,6 +2619,8 @@ bool SimFit::setup() {
 // the buffers of the precision forms and of the final pass must fit what is
 // left of the fixed region; refuse here, before the outer loop starts.
 void SimFit::arena_precheck() {
+    // stored model-stamp entries of every active star at granule height gh (a bound:
+    // the rectangles hold at most the stars' column storage)
     auto model_entries = [&](int gh) {
         int64_t t = 0;
         if (d_modelR) {
@@ -2332,7 +2633,7 @@ void SimFit::arena_precheck() {
     size_t need = 0;
     auto form = [&](size_t ts, int gh) {
         need += carve_size((size_t)p * fc.S * gran_rows(fc.S, gh) * n_act * ts) + carve_size(model_entries(gh) * ts) +
-                (d_modelR ? carve_size(8 * n_act) : 0) + 2 * carve_size(npix * ts);
+                rect_map_bound(tfit.npairs, n_act) + rect_map_bound(tmod.npairs, n_act) + 2 * carve_size(npix * ts);
     };
     if (P->precision == CPB_PREC_MIXED) {
         form(sizeof(float), Gran<float>::H);
@@ -2342,7 +2643,7 @@ void SimFit::arena_precheck() {
     }
     need += carve_size(sizeof(Scalars)) + carve_size(live_tmp_bytes);  // scalars_freeze, newf_tmp
     need += carve_size(48 * n_act) + carve_size(8 * n) + carve_size(8 * npix);
-    need += carve_size(model_entries(Gran<double>::H) * 8) + (d_modelR ? carve_size(8 * n_act) : 0);
+    need += carve_size(model_entries(Gran<double>::H) * 8) + rect_map_bound(tmod.npairs, n_act);
     need += carve_size(8 * kSpreadRuleLen) + carve_size(8 * spread_tab_len(fc.R)) + carve_size(56 * n_act);
     const size_t used = (ctx->arena->used + 255) & ~size_t(255);
     if (used + need > ctx->arena->cap)
@@ -2381,8 +2682,8 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
             KernelScope ks_(ctx, "k_JT",
                             (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) +
                                 std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * btu);
-            k_JT<false, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, cn, F.wt_resid, bsc,
-                                                           sc, red);
+            k_JT<false, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, F.vmap, cn, F.wt_resid,
+                                                           bsc, sc, red);
         }
         check(cudaGetLastError(), "k_JT");
         macs += (double)n_live * fc.S2;
@@ -2436,7 +2737,7 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
                                         (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * btu);
                         k_gather<KIND_JV, MODE_LSQR, TS, TU>
                             <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
-                            f, tfit.start, tfit.end, tfit.list, tfit.order, live, F.V, fc.R, f.VS, nullptr, vt, cn,
+                            f, tfit.start, tfit.end, tfit.list, tfit.order, live, F.V, fc.R, F.vmap.off, vt, cn,
                             it == 0 ? F.wt_resid : F.u, it == 0 ? -1.0 : 1.0, F.u, nullptr, umask, w, sw, nullptr, sc,
                             red, nullptr);
                     }
@@ -2444,8 +2745,8 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
                         KernelScope ks_(ctx, "k_JT_lsqr",
                                         (double)n_live * ((double)p * fc.S2 * bts + 2.0 * p * 8) +
                                             std::min<double>((double)h_ucnt, (double)n_live * fc.S2) * btu);
-                        k_JT<true, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, cn, F.u, vt,
-                                                                      sc, red);
+                        k_JT<true, TS, TU><<<jt_blocks, 256, 0, st>>>(live_list, n_live, f, ay, ax, F.V, F.vmap, cn,
+                                                                      F.u, vt, sc, red);
                     }
                     {
                         KernelScope ks_(ctx, "k_lsqr_update", (double)n * 8 * 5);
@@ -2564,10 +2865,7 @@ void SimFit::finish() {
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     launch_coef(nullptr, coef);
     double* gram = S_<double>("gram", (int64_t)n_act * 6);
-    FitConst f64 = fc;
-    f64.SR = gran_rows(fc.S, Gran<double>::H);
-    f64.PS = fc.S * f64.SR;
-    f64.VS = p * f64.PS;
+    const FitConst& f64 = fc;
     {
         KernelScope ks_(ctx, "k_eval_gram", (double)n_act * (48.0 + sizeof(StarCoef)));
         if (warp_eval) {
@@ -2581,14 +2879,14 @@ void SimFit::finish() {
             const unsigned gbw =
                 (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
             k_eval_warp<true, double><<<gbw, thr, sm_bytes, st>>>(nullptr, n_act, f64, dp, coef, ay, ax, w, sw,
-                                                                  nullptr, cn, gram, nullptr, fc.R, 0, nullptr,
-                                                                  nullptr);
+                                                                  nullptr, RectMap{}, cn, gram, nullptr, RectMap{},
+                                                                  fc.R, nullptr);
         } else {
             const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
             launch_k_eval<true, double>(fc.S2, grid, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S,
                                         st, (const int32_t*)nullptr, n_act, f64, dp, coef, ay, ax, w, sw,
-                                        (double*)nullptr, cn, gram, (double*)nullptr, fc.R, 0,
-                                        (const int32_t*)nullptr, (const int64_t*)nullptr);
+                                        (double*)nullptr, RectMap{}, cn, gram, (double*)nullptr, RectMap{}, fc.R,
+                                        (const int32_t*)nullptr);
         }
         check(cudaGetLastError(), "k_eval_gram");
     }
@@ -2599,17 +2897,15 @@ void SimFit::finish() {
     // ---- final render against the original data (:1344-1356)
     double* resid = S_<double>("resid", npix);
     {
-        int MS64;
-        int64_t* moff64;
-        int64_t mtot64;
-        model_layout<double>("_final", MS64, moff64, mtot64);
+        int64_t mtot64 = 0;
+        const RectMap m64 = rect_map("M_off_final", tmod, Gran<double>::H, 1, model_R, mtot64);
         double* M64 = S_<double>("model_stamps_final", mtot64);
-        check(cudaMemsetAsync(M64, 0, sizeof(double) * mtot64, st), "memset");
-        launch_eval_model<double>(f64, M64, MS64, moff64, nullptr, n_act, coef);
+        check(cudaMemsetAsync(M64, 0, sizeof(double) * std::max<int64_t>(mtot64, 1), st), "memset");
+        launch_eval_model<double>(f64, M64, m64, nullptr, n_act, coef);
         KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
         k_gather<KIND_M, MODE_FINAL, double, double>
             <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
-            f64, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, MS64, moff64, nullptr, nullptr,
+            f64, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, m64.off, nullptr, nullptr,
             nullptr, 0.0, nullptr, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
