@@ -450,38 +450,30 @@ __device__ __forceinline__ int tab_entry(int ty0, int ty1, int tx0, int tx1, int
     return (col - t.c_lo) * t.nrows + (o + row - t.s_lo);
 }
 
-// The store plan of a star whose box meets at most 2 x 2 regions: box entry
-// (row, col) inside [rmin, rmax) x [cmin, cmax) lies in rectangle
-// rid = (col >= csplit) * nty + (row >= rsplit) at index A + col * nrows + row
-// of plane 0 (A folds the rectangle's offset and origin in), planes ps apart.
+// The rectangles of a star whose box meets at most 2 x 2 regions, for the stamp
+// kernels' storage-order walk: per rectangle (emit order) its offsets in the
+// stamp-derivative (V) and model (M) buffers, first box column, first storage
+// row, rows and entries (ncols * nrows, also V's plane stride).
 struct StorePlan {
-    int64_t AV[kStarRects], AM[kStarRects];
-    int nrows[kStarRects], ps[kStarRects];
-    int rsplit, csplit, rmin, rmax, cmin, cmax, nty;
+    int64_t offV[kStarRects], offM[kStarRects];
+    int c_lo[kStarRects], s_lo[kStarRects], nrows[kStarRects], ps[kStarRects];
+    float inv_nrows[kStarRects];
 };
 
-// Lane `lane` (< 4) of the warp fills rectangle `lane` of the plan; lane 0 the rest.
-__device__ __forceinline__ void store_plan(StorePlan& sp, int lane, int j, int a_y, int a_x, int Rb, int ty0, int ty1,
-                                           int tx0, int tx1, int GH, const RectMap* vmap, const RectMap* mmap) {
-    const int Sb = 2 * Rb + 1, top0 = a_y - Rb - 1, left0 = a_x - Rb - 1;
-    const int o = top0 - (top0 & ~(GH - 1));
-    const int nty_j = ty1 - ty0 + 1, nrect = nty_j * (tx1 - tx0 + 1);
+// Lanes 0 .. nrect - 1 of the warp fill their rectangle of the plan.
+__device__ __forceinline__ void store_plan(StorePlan& sp, int lane, int nrect, int j, int a_y, int a_x, int Rb,
+                                           int ty0, int ty1, int tx0, int GH, const RectMap* vmap,
+                                           const RectMap* mmap) {
+    const int nty_j = ty1 - ty0 + 1;
     if (lane < nrect) {
         const RectGeo g = rect_geo(a_y, a_x, Rb, ty0 + lane % nty_j, tx0 + lane / nty_j, GH);
-        const int64_t fold = (int64_t)o - g.s_lo - (int64_t)g.c_lo * g.nrows;
-        sp.AV[lane] = vmap ? star_rect_off(*vmap, j, lane) + fold : 0;
-        sp.AM[lane] = mmap ? star_rect_off(*mmap, j, lane) + fold : 0;
+        sp.offV[lane] = vmap ? star_rect_off(*vmap, j, lane) : 0;
+        sp.offM[lane] = mmap ? star_rect_off(*mmap, j, lane) : 0;
+        sp.c_lo[lane] = g.c_lo;
+        sp.s_lo[lane] = g.s_lo;
         sp.nrows[lane] = g.nrows;
         sp.ps[lane] = g.ncols * g.nrows;
-    }
-    if (lane == 0) {
-        sp.nty = nty_j;
-        sp.rsplit = ty1 > ty0 ? (ty0 + 1) * TY - top0 : Sb;
-        sp.csplit = tx1 > tx0 ? (tx0 + 1) * TX - left0 : Sb;
-        sp.rmin = max(0, ty0 * TY - top0);
-        sp.rmax = min(Sb, (ty1 + 1) * TY - top0);
-        sp.cmin = max(0, tx0 * TX - left0);
-        sp.cmax = min(Sb, (tx1 + 1) * TX - left0);
+        sp.inv_nrows[lane] = 1.0f / (float)max(g.nrows, 1);
     }
 }
 
@@ -858,7 +850,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const bool planned = nrect <= kStarRects && (!wantV || vmap.srect) && (!wantM || mmap.srect);
         const bool tabbed = !planned && nrect <= kFillRects;
         if (planned)
-            store_plan(plan, lane, j, a_y, a_x, Rb, ty0, ty1, tx0, tx1, GH, wantV ? &vmap : nullptr,
+            store_plan(plan, lane, nrect, j, a_y, a_x, Rb, ty0, ty1, tx0, GH, wantV ? &vmap : nullptr,
                        wantM ? &mmap : nullptr);
         else if (tabbed)
             store_rect_tab(rtab, lane, 32, nrect, nty_j, ty0, tx0, j, a_y, a_x, Rb, GH, wantV ? &vmap : nullptr,
@@ -867,12 +859,6 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const int top0 = a_y - Rb - 1, left0 = a_x - Rb - 1, so = top0 - gran_base(top0, GH);
         // element index of entry (row, col) in plane 0 of V (isV) or M, and V's plane stride
         auto store_at = [&](int row, int col, bool isV, int64_t* ps) -> int64_t {
-            if (planned) {
-                if (row < plan.rmin || row >= plan.rmax || col < plan.cmin || col >= plan.cmax) return -1;
-                const int rid = (col >= plan.csplit ? plan.nty : 0) + (row >= plan.rsplit ? 1 : 0);
-                *ps = plan.ps[rid];
-                return (isV ? plan.AV[rid] : plan.AM[rid]) + (int64_t)col * plan.nrows[rid] + row;
-            }
             if (tabbed) {
                 const StoreRect* t = nullptr;
                 const int e = tab_entry(ty0, ty1, tx0, tx1, nty_j, top0, left0, so, row, col, rtab, &t);
@@ -918,7 +904,86 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 gcc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
             }
         };
-        if (!GRAD) {
+        if (planned) {
+            // storage order: the star's rectangles one after another, each column
+            // by column, so the stores of a warp are consecutive; pad rows skipped
+            double acc[6] = {0, 0, 0, 0, 0, 0};
+            int l = 0, t = lane;
+            while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
+            while (l < nrect) {
+                const int cc = (int)(((float)t + 0.5f) * plan.inv_nrows[l]);
+                const int row = plan.s_lo[l] + (t - cc * plan.nrows[l]) - so, col = plan.c_lo[l] + cc;
+                if (row >= 0 && row < Sb) {
+                    if (!GRAD) {
+                        T val, a, b, c;
+                        eval_px(row, col, val, a, b, c);
+                        M[plan.offM[l] + t] = val;
+                    } else {
+                        const int gy = oy + row, gx = ox + col;
+                        const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
+                        const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
+                        const bool use = onimg && w[q] > 0;
+                        T r0 = 0, r1 = 0, r2 = 0;
+                        if (use || wantM) {
+                            T val, a, b, c;
+                            eval_px(row, col, val, a, b, c);
+                            if (wantM) M[plan.offM[l] + t] = val;
+                            if (use) {
+                                const T sq = (T)sw[q];
+                                r0 = sq * a;
+                                r1 = sq * b;
+                                r2 = sq * c;
+                                const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
+                                if (gram) {
+                                    acc[0] += d0 * d0;
+                                    acc[1] += d0 * d1;
+                                    acc[2] += d0 * d2;
+                                    acc[3] += d1 * d1;
+                                    acc[4] += d1 * d2;
+                                    acc[5] += d2 * d2;
+                                } else {
+                                    acc[0] += d0 * d0;
+                                    acc[1] += d1 * d1;
+                                    acc[2] += d2 * d2;
+                                }
+                            }
+                        }
+                        if (wantV && onimg) {
+                            T* v = V + plan.offV[l] + t;
+                            v[0] = r0;
+                            if (p > 1) v[plan.ps[l]] = r1;
+                            if (p > 2) v[2 * plan.ps[l]] = r2;
+                        }
+                    }
+                }
+                t += 32;
+                while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
+            }
+            if (GRAD) {
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc[k] = warp_sum(acc[k]);
+                if (gram) {
+                    if (lane == 0) {
+                        double* gj = gram + (int64_t)j * 6;
+                        if (p == 1) gj[0] = acc[0];
+                        else if (p == 2) {
+                            gj[0] = acc[0];
+                            gj[1] = acc[1];
+                            gj[2] = acc[3];
+                        } else {
+                            for (int k = 0; k < 6; ++k) gj[k] = acc[k];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        double cn = sqrt(k < p ? acc[k] : 1.0);
+                        cn = cn < kEps64 ? kEps64 : cn;
+                        if (lane == 0 && k < p) colnorm[(int64_t)j * p + k] = cn;
+                    }
+                }
+            }
+        } else if (!GRAD) {
             int row = lane % Sb, col = lane / Sb;
             for (int m = lane; m < S2b; m += 32) {
                 T val, a, b, c;
