@@ -40,11 +40,11 @@ N_STARS = 50_000
 FIT_RAD = 12
 SEED = 1002
 SAMPLE = 512  # CPU sample side (same star density)
-# DRAM bytes moved per algorithmic byte by the FP64 J v gather (read + write 266.8 MB
-# against 204.6 MB algorithmic), from an ncu capture of the same kernel on a 1024^2
-# field with the same star density, PSF and radii (an LSQR launch of the first outer
-# iteration, every star live)
-JV_TRAFFIC_RATIO = 266.8 / 204.6
+# DRAM bytes moved per algorithmic byte by the FP64 J v gather (read 815.7 MB + write
+# 7.3 MB against 818.3 MB algorithmic), from an ncu capture of one launch of the same
+# kernel on this 2048^2 field (an LSQR launch of the first outer iteration, every star
+# live; one metric pass, no replay)
+JV_TRAFFIC_RATIO = (815.72 + 7.32) / 818.3
 
 
 def workload_config(ny=NY, nx=NX, n=N_STARS):
@@ -392,8 +392,8 @@ def run_gpu(args):
     if top[0] == "k_gather_Jv":
         roof["traffic"] = JV_TRAFFIC_RATIO * top[1]["bytes"] / max(top[1]["launches"], 1)
         roof["traffic_note"] = ("bytes per launch: this run's algorithmic bytes per launch times the DRAM / "
-                                f"algorithmic ratio of an ncu capture of the kernel on a 1024^2 field "
-                                f"({JV_TRAFFIC_RATIO:.3f})")
+                                f"algorithmic ratio of an ncu capture of one launch of the kernel on this "
+                                f"2048^2 field ({JV_TRAFFIC_RATIO:.3f})")
     kernels = {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
                    "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst.items())}
 

@@ -41,8 +41,10 @@ class CudaError(RuntimeError):
 class Context:
     """A device context (cpb_ctx) with an upload cache for PSFs."""
 
-    def __init__(self, device: int = 0):
-        self.lib = _abi.load_library()
+    def __init__(self, device: int = 0, lib: str | None = None):
+        """lib: path of another build of the library (for instance the checked
+        build, lib/libcrowdphot_b200_checked.so); default the package's own."""
+        self.lib = _abi.load_library(lib)
         h = C.c_void_p()
         rc = self.lib.cpb_ctx_create(int(device), C.byref(h))
         if rc != _abi.CPB_OK:

@@ -15,24 +15,33 @@
 
 namespace cpb {
 
+// A named grow-only scratch buffer of at least `bytes`.  Growth frees and
+// allocates in stream order on the context's stream (cudaFreeAsync /
+// cudaMallocAsync from the device's memory pool): no device-wide
+// synchronisation, so contexts sharing the GPU -- the server's slots -- keep
+// running while one of them grows.  The copy stream's work is ordered before
+// the free and after the new allocation.
 void* scratch(cpb_ctx* ctx, const char* name, size_t bytes) {
     if (ctx->arena) return arena_carve(ctx->arena, name, bytes);
     auto& b = ctx->bufs[name];
     if (b.bytes >= bytes && b.p) return b.p;
     if (b.p) {
-        check(cudaStreamSynchronize(ctx->stream), "sync before realloc");
-        cudaFree(b.p);
+        check(cudaEventRecord(ctx->grow_ev, ctx->copy_stream), "grow order");
+        check(cudaStreamWaitEvent(ctx->stream, ctx->grow_ev, 0), "grow order");
+        check(cudaFreeAsync(b.p, ctx->stream), "cudaFreeAsync");
         b.p = nullptr;
         b.bytes = 0;
     }
     size_t want = std::max<size_t>(bytes, 256);
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = cudaMallocAsync(&p, want, ctx->stream);
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
         throw OomError{std::string("device memory exhausted allocating ") + name};
     }
-    check(e, "cudaMalloc");
+    check(e, "cudaMallocAsync");
+    check(cudaEventRecord(ctx->grow_ev, ctx->stream), "grow order");
+    check(cudaStreamWaitEvent(ctx->copy_stream, ctx->grow_ev, 0), "grow order");
     b.p = p;
     b.bytes = want;
     return p;
@@ -102,6 +111,7 @@ int cpb_ctx_create(int device, cpb_ctx** out) {
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->grow_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaMallocHost(&ctx->pinned, 4096) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
@@ -123,10 +133,11 @@ int cpb_ctx_destroy(cpb_ctx* ctx) {
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
+        if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
         for (auto& kv : ctx->bufs)
-            if (kv.second.p) cudaFree(kv.second.p);
+            if (kv.second.p) cudaFreeAsync(kv.second.p, ctx->stream);
         ctx->bufs.clear();
+        cudaStreamSynchronize(ctx->stream);
         if (ctx->pinned) cudaFreeHost(ctx->pinned);
         for (auto e : ctx->event_pool) cudaEventDestroy(e);
         for (auto& p : ctx->pending) {
@@ -135,6 +146,7 @@ int cpb_ctx_destroy(cpb_ctx* ctx) {
         }
         if (ctx->ev0) cudaEventDestroy(ctx->ev0);
         if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+        if (ctx->grow_ev) cudaEventDestroy(ctx->grow_ev);
         if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
         for (auto e : ctx->copy_ev)
             if (e) cudaEventDestroy(e);

@@ -84,10 +84,11 @@ int64_t held_bytes(cpb_ctx* ctx) {
 void release_scratch(cpb_ctx* ctx) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
+    cudaStreamSynchronize(ctx->copy_stream);
     for (auto& kv : ctx->bufs)
-        if (kv.second.p) cudaFree(kv.second.p);
+        if (kv.second.p) cudaFreeAsync(kv.second.p, ctx->stream);
     ctx->bufs.clear();
+    cudaStreamSynchronize(ctx->stream);
 }
 
 }  // namespace

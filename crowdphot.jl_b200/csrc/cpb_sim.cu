@@ -33,6 +33,17 @@
 namespace cpb {
 namespace {
 
+// Checked build (-DCPB_CHECKED): the stamp and pixel accesses of this file's
+// kernels test their indexes against the buffers' lengths; a failed test skips
+// the access and records its site (the first one) in g_check_err, which the
+// host turns into an error return after the fit.  Normal builds test nothing.
+#ifdef CPB_CHECKED
+__device__ unsigned g_check_err;
+#define CPB_CHECK(cond, site) ((cond) || (atomicCAS(&g_check_err, 0u, (unsigned)(site)), false))
+#else
+#define CPB_CHECK(cond, site) true
+#endif
+
 constexpr int TY = 32;   // region rows (y, contiguous in memory)
 constexpr int TX = 32;   // region columns
 constexpr int NT = 128;  // threads of the region kernels (4 warps)
@@ -370,6 +381,7 @@ struct RectMap {
     const int64_t* off;         // per pair: offset of the rectangle's plane 0
     const int64_t* srect;       // per star, when every box meets at most 2 x 2 regions: its
                                 // rectangles' offsets in emit order (kStarRects a star), else null
+    int64_t len;                // elements of the buffer (the checked build tests indexes against it)
     int planes;
 };
 constexpr int kStarRects = 4;
@@ -707,7 +719,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                 const T val = gauss_eval<T, GRAD>((T)P.fwhm, c, (T)gy, (T)gx, g[0], g[1], g[2]);
                 if (M) {
                     const int64_t q = sidx(mmap, row, col, 0);
-                    if (q >= 0) M[q] = val;
+                    if (q >= 0 && CPB_CHECK(q < mmap.len, 0x11)) M[q] = val;
                 }
             } else {
 #pragma unroll
@@ -725,7 +737,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                 }
                 if (M) {
                     const int64_t q = sidx(mmap, row, col, 0);
-                    if (q >= 0) M[q] = (T)c.flux * s + (T)c.bkg;
+                    if (q >= 0 && CPB_CHECK(q < mmap.len, 0x12)) M[q] = (T)c.flux * s + (T)c.bkg;
                 }
                 g[0] = (T)c.flux * dY;
                 g[1] = (T)c.flux * dX;
@@ -791,7 +803,7 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
                     for (int k = 0; k < 3; ++k) {
                         if (k >= p) break;
                         const int64_t at = sidx(vmap, m % Sb, m / Sb, k);  // the fit box: Sb == fc.S
-                        if (at >= 0) V[at] = raw[e][k];
+                        if (at >= 0 && CPB_CHECK(at < vmap.len, 0x13)) V[at] = raw[e][k];
                     }
                 }
             }
@@ -803,7 +815,10 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
 // Warp-per-star stamp evaluation for single-node ePSFs and the Gaussian (the
 // common case): no block barriers, each warp keeps its star's row / column
 // tables in its own slice of shared memory.  Same outputs as k_eval.
-template <bool GRAD, typename T>
+// PLAN: every box meets at most 2 x 2 regions and every map written has
+// per-star rectangle offsets (srect), so only the storage-order walk is
+// compiled (the general paths' registers would otherwise spill in it).
+template <bool GRAD, typename T, bool PLAN>
 __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                                       DevPsf P, const StarCoef* __restrict__ coef,
                                                       const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
@@ -847,8 +862,8 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
         const int nty_j = ty1 - ty0 + 1, nrect = nty_j * (tx1 - tx0 + 1);
         const bool wantV = GRAD && !gram, wantM = M != nullptr && !gram;
         // a plan when every map has per-star rectangle offsets (boxes within 2 x 2 regions)
-        const bool planned = nrect <= kStarRects && (!wantV || vmap.srect) && (!wantM || mmap.srect);
-        const bool tabbed = !planned && nrect <= kFillRects;
+        const bool planned = PLAN || (nrect <= kStarRects && (!wantV || vmap.srect) && (!wantM || mmap.srect));
+        const bool tabbed = !PLAN && !planned && nrect <= kFillRects;
         if (planned)
             store_plan(plan, lane, nrect, j, a_y, a_x, Rb, ty0, ty1, tx0, GH, wantV ? &vmap : nullptr,
                        wantM ? &mmap : nullptr);
@@ -882,14 +897,14 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             gc_.flux = cg.flux;
             gc_.bkg = cg.bkg;
         }
-        // value (and gradient) at stamp entry (row, col)
-        auto eval_px = [&](int row, int col, T& val, T& ga, T& gb, T& gcc) {
+        // value (and gradient) at stamp entry (row, col), the row's table given
+        auto eval_rc = [&](const AxisTab<T>& rtab, int row, int col, T& val, T& ga, T& gb, T& gcc) {
             T g[3];
             if (gauss) {
                 val = gauss_eval<T, GRAD>((T)P.fwhm, gc_, (T)(oy + row), (T)(ox + col), g[0], g[1], g[2]);
             } else {
                 T pv, pdv = 0, pdu = 0;
-                tab_bicubic<GRAD, T>(base, tcol[col], trow[row], nfill, pv, pdv, pdu);
+                tab_bicubic<GRAD, T>(base, tcol[col], rtab, nfill, pv, pdv, pdu);
                 const T s = w0 * pv;
                 val = flux * s + bkg;
                 if (GRAD) {
@@ -904,60 +919,88 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 gcc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
             }
         };
+        auto eval_px = [&](int row, int col, T& val, T& ga, T& gb, T& gcc) {
+            eval_rc(trow[row], row, col, val, ga, gb, gcc);
+        };
         if (planned) {
-            // storage order: the star's rectangles one after another, each column
-            // by column, so the stores of a warp are consecutive; pad rows skipped
+            // column walk: lane = storage row of the star's granule layout (box
+            // row + so), the box columns in order.  The lane's row table stays in
+            // registers, the column's table is one shared-memory broadcast, and at
+            // each column the warp's stores are consecutive rows of one or two
+            // rectangles (the box meets at most 2 x 2 regions).
             double acc[6] = {0, 0, 0, 0, 0, 0};
-            int l = 0, t = lane;
-            while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
-            while (l < nrect) {
-                const int cc = (int)(((float)t + 0.5f) * plan.inv_nrows[l]);
-                const int row = plan.s_lo[l] + (t - cc * plan.nrows[l]) - so, col = plan.c_lo[l] + cc;
-                if (row >= 0 && row < Sb) {
+            const int b0 = top0 - so;            // 0-based image row of storage row 0
+            const int SRb = gran_rows(Sb, GH);
+            const int cx1 = (tx0 + 1) * TX;      // first image column of the second region column
+            for (int s0 = 0; s0 < SRb; s0 += 32) {
+                const int srow = s0 + lane, row = srow - so, y = b0 + srow;
+                const int iy = y >= 0 ? y / TY - ty0 : -1;
+                const bool rowin = srow < SRb && row >= 0 && row < Sb && iy >= 0 && iy < nty_j;
+                // this lane's rectangle in each region column: entry (srow, col) of
+                // plane 0 at base + col * nr, planes ps apart
+                int64_t baseV[2] = {0, 0}, baseM[2] = {0, 0};
+                int nr[2] = {0, 0}, ps[2] = {0, 0};
+#pragma unroll
+                for (int ix = 0; ix < 2; ++ix) {
+                    const int l = min(ix * nty_j + max(iy, 0), nrect - 1);
+                    nr[ix] = plan.nrows[l];
+                    ps[ix] = plan.ps[l];
+                    const int64_t rel = (int64_t)(srow - plan.s_lo[l]) - (int64_t)plan.c_lo[l] * plan.nrows[l];
+                    baseV[ix] = plan.offV[l] + rel;
+                    baseM[ix] = plan.offM[l] + rel;
+                }
+                AxisTab<T> rt{};
+                if (!gauss && rowin) rt = trow[row];
+                const bool ony = rowin && y < fc.ny;
+                for (int col = 0; col < Sb; ++col) {
+                    const int x = left0 + col;
+                    if (x < 0 || x >= (tx1 + 1) * TX) continue;  // no region holds the column (uniform)
+                    const int ix = x >= cx1 ? 1 : 0;
+                    if (!rowin) continue;
+                    const int64_t e = (ix ? baseV[1] : baseV[0]) + (int64_t)col * (ix ? nr[1] : nr[0]);
+                    const int64_t em = (ix ? baseM[1] : baseM[0]) + (int64_t)col * (ix ? nr[1] : nr[0]);
                     if (!GRAD) {
                         T val, a, b, c;
-                        eval_px(row, col, val, a, b, c);
-                        M[plan.offM[l] + t] = val;
+                        eval_rc(rt, row, col, val, a, b, c);
+                        if (CPB_CHECK(em < mmap.len, 0x21)) M[em] = val;
                     } else {
-                        const int gy = oy + row, gx = ox + col;
-                        const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
-                        const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
-                        const bool use = onimg && w[q] > 0;
+                        const bool onimg = ony && x < fc.nx;
+                        const int64_t q = onimg ? y + (int64_t)x * fc.ny : 0;
+                        // the weights load beside the evaluation, not before it
+                        const double wq = onimg ? w[q] : 0.0, swq = onimg ? sw[q] : 0.0;
+                        const bool use = onimg && wq > 0;
+                        T val, a, b, c;
+                        eval_rc(rt, row, col, val, a, b, c);
+                        if (wantM && CPB_CHECK(em < mmap.len, 0x22)) M[em] = val;
                         T r0 = 0, r1 = 0, r2 = 0;
-                        if (use || wantM) {
-                            T val, a, b, c;
-                            eval_px(row, col, val, a, b, c);
-                            if (wantM) M[plan.offM[l] + t] = val;
-                            if (use) {
-                                const T sq = (T)sw[q];
-                                r0 = sq * a;
-                                r1 = sq * b;
-                                r2 = sq * c;
-                                const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
-                                if (gram) {
-                                    acc[0] += d0 * d0;
-                                    acc[1] += d0 * d1;
-                                    acc[2] += d0 * d2;
-                                    acc[3] += d1 * d1;
-                                    acc[4] += d1 * d2;
-                                    acc[5] += d2 * d2;
-                                } else {
-                                    acc[0] += d0 * d0;
-                                    acc[1] += d1 * d1;
-                                    acc[2] += d2 * d2;
-                                }
+                        if (use) {
+                            const T sq = (T)swq;
+                            r0 = sq * a;
+                            r1 = sq * b;
+                            r2 = sq * c;
+                            const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
+                            if (gram) {
+                                acc[0] += d0 * d0;
+                                acc[1] += d0 * d1;
+                                acc[2] += d0 * d2;
+                                acc[3] += d1 * d1;
+                                acc[4] += d1 * d2;
+                                acc[5] += d2 * d2;
+                            } else {
+                                acc[0] += d0 * d0;
+                                acc[1] += d1 * d1;
+                                acc[2] += d2 * d2;
                             }
                         }
-                        if (wantV && onimg) {
-                            T* v = V + plan.offV[l] + t;
+                        const int pst = ix ? ps[1] : ps[0];
+                        if (wantV && onimg && CPB_CHECK(e + (int64_t)(p - 1) * pst < vmap.len, 0x23)) {
+                            T* v = V + e;
                             v[0] = r0;
-                            if (p > 1) v[plan.ps[l]] = r1;
-                            if (p > 2) v[2 * plan.ps[l]] = r2;
+                            if (p > 1) v[pst] = r1;
+                            if (p > 2) v[2 * pst] = r2;
                         }
                     }
                 }
-                t += 32;
-                while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
             }
             if (GRAD) {
 #pragma unroll
@@ -983,6 +1026,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     }
                 }
             }
+        } else if constexpr (PLAN) {
         } else if (!GRAD) {
             int row = lane % Sb, col = lane / Sb;
             for (int m = lane; m < S2b; m += 32) {
@@ -990,7 +1034,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 eval_px(row, col, val, a, b, c);
                 int64_t ps;
                 const int64_t q = store_at(row, col, false, &ps);
-                if (q >= 0) M[q] = val;
+                if (q >= 0 && CPB_CHECK(q < mmap.len, 0x24)) M[q] = val;
                 row += r32;
                 col += q32;
                 if (row >= Sb) {
@@ -1018,7 +1062,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                     if (M && !gram) {
                         int64_t ps;
                         const int64_t q = store_at(row, col, false, &ps);
-                        if (q >= 0) M[q] = val;
+                        if (q >= 0 && CPB_CHECK(q < mmap.len, 0x25)) M[q] = val;
                     }
                     if (use) {
                         const T sq = (T)sw[q];
@@ -1043,7 +1087,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 if (!gram && onimg) {  // the fit box; off-image entries are not stored
                     int64_t ps;
                     const int64_t q = store_at(row, col, true, &ps);
-                    if (q >= 0) {
+                    if (q >= 0 && CPB_CHECK(q + (p - 1) * ps < vmap.len, 0x26)) {
                         V[q] = r0;
                         if (p > 1) V[q + ps] = r1;
                         if (p > 2) V[q + 2 * ps] = r2;
@@ -1118,7 +1162,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                                                const int32_t* __restrict__ tend, const int4* __restrict__ tlist,
                                                const int32_t* __restrict__ tord,
                                                const uint8_t* __restrict__ incl, const TS* __restrict__ src,
-                                               int Rbox, const int64_t* __restrict__ roff,
+                                               int Rbox, const int64_t* __restrict__ roff, int64_t src_len,
                                                const double* __restrict__ vt, const double* __restrict__ cn,
                                                const TU* u_src, double u_sign,
                                                TU* outu, double* outd, const uint8_t* __restrict__ umask,
@@ -1225,10 +1269,13 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                         const int cc = (int)(((float)t + 0.5f) * inv_nga);
                         const int gg = t - cc * nga;
                         const TS* g = base + (int64_t)t * GH;
+                        if (CPB_CHECK(g - src + (p - 1) * PSb + GH <= src_len, 0x31) &&
+                            CPB_CHECK((cl0 + cc) * TY + (gl0 + gg) * GH + GH <= TX * TY, 0x32)) {
 #pragma unroll
-                        for (int k = 0; k < NPL; ++k)
-                            if (k < p) ld_gran(g + k * PSb, raw[q][k]);
-                        dst[q] = (cl0 + cc) * TY + (gl0 + gg) * GH;
+                            for (int k = 0; k < NPL; ++k)
+                                if (k < p) ld_gran(g + k * PSb, raw[q][k]);
+                            dst[q] = (cl0 + cc) * TY + (gl0 + gg) * GH;
+                        }
                     }
                     if ((c + 1) * 32 < tot) {
                         ++c;
@@ -1404,7 +1451,8 @@ __global__ void __launch_bounds__(256, 3) k_JT(const int32_t* __restrict__ list,
                     const int cc = (int)(((float)t + 0.5f) * T.inv_nga);
                     const int gg = t - cc * T.nga;
                     const int gx = T.x0 + cc, gy = T.y0 + gg * GH;
-                    ok[q] = gx < nx;
+                    ok[q] = gx < nx &&
+                            CPB_CHECK(T.off + (int64_t)t * GH + (int64_t)(p - 1) * T.tot * GH + GH <= vmap.len, 0x41);
                     if (ok[q]) {
                         const TS* e = V + T.off + (int64_t)t * GH;
                         const int64_t ps = (int64_t)T.tot * GH;
@@ -1867,6 +1915,19 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t
 // k_eval with the register cache its box needs: 256 threads for boxes up to
 // 2,048 pixels, 512 / 1,024 threads up to 4,096 / 8,192 (ceil(radius) <= 44);
 // the value-only form (no cache) takes any box.  smem: the axis tables.
+// k_eval_warp, the storage-order-walk-only instantiation when `plan` (every
+// box within 2 x 2 regions, every map written with per-star offsets)
+template <bool GRAD, typename TS, typename... A>
+void launch_eval_warp(bool plan, unsigned grid, unsigned thr, size_t smem, cudaStream_t st, A... args) {
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024)
+            check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
+        kern<<<grid, thr, smem, st>>>(args...);
+    };
+    if (plan) go(k_eval_warp<GRAD, TS, true>);
+    else go(k_eval_warp<GRAD, TS, false>);
+}
+
 template <bool GRAD, typename T, typename... A>
 void launch_k_eval(int64_t S2, unsigned grid, size_t smem, cudaStream_t st, A... args) {
     auto go = [&](auto kern, int threads) {
@@ -2267,6 +2328,7 @@ RectMap SimFit::rect_map(const char* tag, const TileLists& tl, int GH, int plane
     m.planes = planes;
     int64_t* off = S_<int64_t>(tag, tl.npairs + 1);
     total = rect_offsets(ctx, tag, tl, fc.nty, GH, planes, off);
+    m.len = total;
     m.off = off;
     m.srect = nullptr;
     if (2 * Rmax + 1 <= TX + 1 && 2 * Rmax + 1 <= TY + 1) {  // every box meets at most 2 x 2 regions
@@ -2314,14 +2376,12 @@ void SimFit::launch_fill(Form<TS, TU>& F, const int32_t* list, int64_t nlist) {
         unsigned thr;
         size_t sm_bytes;
         warp_shape(fc.S, sizeof(AxisTab<TS>), thr, sm_bytes);
-        if (sm_bytes > 48 * 1024)
-            check(cudaFuncSetAttribute(k_eval_warp<true, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm_bytes), "smem attr");
         const int wpb = (int)(thr / 32);
         const unsigned gbw =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-        k_eval_warp<true, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V, F.vmap,
-                                                         cn, nullptr, Mo, F.mmap, fc.R, nullptr);
+        const bool plan = F.vmap.srect && (!Mo || F.mmap.srect);
+        launch_eval_warp<true, TS>(plan, gbw, thr, sm_bytes, st, list, nlist, F.fc, dp, coef, ay, ax, w, sw, F.V,
+                                   F.vmap, cn, (double*)nullptr, Mo, F.mmap, fc.R, (const int32_t*)nullptr);
     } else {
         const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
@@ -2342,14 +2402,12 @@ void SimFit::launch_eval_model(const FitConst& f, TS* M, const RectMap& mmap, co
         unsigned thr;
         size_t sm_bytes;
         warp_shape(Sm, sizeof(AxisTab<TS>), thr, sm_bytes);
-        if (sm_bytes > 48 * 1024)
-            check(cudaFuncSetAttribute(k_eval_warp<false, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm_bytes), "smem attr");
         const int wpb = (int)(thr / 32);
         const unsigned gbw =
             (unsigned)std::max<int64_t>(1, std::min<int64_t>((nlist + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-        k_eval_warp<false, TS><<<gbw, thr, sm_bytes, st>>>(list, nlist, f, dp, cf, ay, ax, w, sw, (TS*)nullptr,
-                                                          RectMap{}, cn, nullptr, M, mmap, model_R, d_modelR);
+        launch_eval_warp<false, TS>(mmap.srect != nullptr, gbw, thr, sm_bytes, st, list, nlist, f, dp, cf, ay, ax,
+                                    w, sw, (TS*)nullptr, RectMap{}, cn, (double*)nullptr, M, mmap, model_R,
+                                    (const int32_t*)d_modelR);
     } else {
         const size_t tab_bytes = (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<TS>);
         const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(nlist, (int64_t)ctx->n_sm * 16));
@@ -2378,7 +2436,8 @@ void SimFit::launch_render(Form<TS, TU>& F, int mode, const uint8_t* incl, const
     const auto& tl = tmod;
 #define CPB_RENDER(MD)                                                                                               \
     k_gather<KIND_M, MD, TS, TU><<<g, NT, kGatherSmem, st>>>(F.fc, tl.start, tl.end, tl.list, tl.order, incl, F.M,   \
-                                                             model_R, F.mmap.off, nullptr, nullptr, nullptr, 0.0,     \
+                                                             model_R, F.mmap.off, F.mmap.len, nullptr, nullptr,      \
+                                                             nullptr, 0.0,                                            \
                                                              outu, outd, umask, w, sw, ref, sc, red, result)
     switch (mode) {
         case MODE_CUR: CPB_RENDER(MODE_CUR); break;
@@ -2802,7 +2861,7 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
                                         (double)n_live * ((double)p * fc.S2 * bts + p * 8) + 2.0 * npix * btu);
                         k_gather<KIND_JV, MODE_LSQR, TS, TU>
                             <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
-                            f, tfit.start, tfit.end, tfit.list, tfit.order, live, F.V, fc.R, F.vmap.off, vt, cn,
+                            f, tfit.start, tfit.end, tfit.list, tfit.order, live, F.V, fc.R, F.vmap.off, F.vmap.len, vt, cn,
                             it == 0 ? F.wt_resid : F.u, it == 0 ? -1.0 : 1.0, F.u, nullptr, umask, w, sw, nullptr, sc,
                             red, nullptr);
                     }
@@ -2937,15 +2996,13 @@ void SimFit::finish() {
             unsigned thr;
             size_t sm_bytes;
             warp_shape(fc.S, sizeof(AxisTab<double>), thr, sm_bytes);
-            if (sm_bytes > 48 * 1024)
-                check(cudaFuncSetAttribute(k_eval_warp<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)sm_bytes), "smem attr");
             const int wpb = (int)(thr / 32);
             const unsigned gbw =
                 (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
-            k_eval_warp<true, double><<<gbw, thr, sm_bytes, st>>>(nullptr, n_act, f64, dp, coef, ay, ax, w, sw,
-                                                                  nullptr, RectMap{}, cn, gram, nullptr, RectMap{},
-                                                                  fc.R, nullptr);
+            const bool plan = 2 * fc.R + 1 <= TX + 1 && 2 * fc.R + 1 <= TY + 1;  // the Gram needs no map
+            launch_eval_warp<true, double>(plan, gbw, thr, sm_bytes, st, (const int32_t*)nullptr, (int64_t)n_act, f64,
+                                           dp, coef, ay, ax, w, sw, (double*)nullptr, RectMap{}, cn, gram,
+                                           (double*)nullptr, RectMap{}, fc.R, (const int32_t*)nullptr);
         } else {
             const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(n_act, (int64_t)ctx->n_sm * 16));
             launch_k_eval<true, double>(fc.S2, grid, (size_t)(dp.n_nodes == 1 ? 2 : 8) * sizeof(AxisTab<double>) * fc.S,
@@ -2970,7 +3027,7 @@ void SimFit::finish() {
         KernelScope ks_(ctx, "k_gather_final", (double)npix * 16.0 + (double)n_act * Sm * Sm * 8);
         k_gather<KIND_M, MODE_FINAL, double, double>
             <<<(unsigned)ntiles, NT, kGatherSmem, st>>>(
-            f64, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, m64.off, nullptr, nullptr,
+            f64, tmod.start, tmod.end, tmod.list, tmod.order, nullptr, M64, model_R, m64.off, m64.len, nullptr, nullptr,
             nullptr, 0.0, nullptr, resid, umask, w, sw, data, sc, red, nullptr);
         check(cudaGetLastError(), "k_gather_final");
     }
@@ -3131,7 +3188,24 @@ int fit_simultaneous_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params*
                          int64_t n, const double* d_y0, const double* d_x0, const double* d_flux0,
                          cpb_sim_result* out) {
     SimFit fit(ctx, psf, P, d_image, eltype, ny, nx, d_inv_var, d_background, n, d_y0, d_x0, d_flux0, out);
-    return fit.run();
+    const int rc = fit.run();
+#ifdef CPB_CHECKED
+    // the checked build: the first index check that failed in any kernel of the fit
+    unsigned site = 0;
+    check(cudaMemcpyFromSymbolAsync(&site, g_check_err, sizeof(site), 0, cudaMemcpyDeviceToHost, ctx->stream),
+          "check flag");
+    check(cudaStreamSynchronize(ctx->stream), "check flag");
+    if (site) {
+        const unsigned zero = 0;
+        check(cudaMemcpyToSymbolAsync(g_check_err, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, ctx->stream),
+              "check flag");
+        check(cudaStreamSynchronize(ctx->stream), "check flag");
+        char msg[96];
+        snprintf(msg, sizeof msg, "index check 0x%x failed in the simultaneous fit (access skipped)", site);
+        throw std::runtime_error(msg);
+    }
+#endif
+    return rc;
 }
 
 }  // namespace cpb

@@ -42,7 +42,7 @@ extern "C" {
 #define CPB_ERR_CUDA (-2)      /* CUDA runtime / launch error */
 #define CPB_ERR_OOM (-3)       /* device memory exhausted or admission refused */
 #define CPB_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
-#define CPB_ERR_INTERNAL (-5)
+#define CPB_ERR_INTERNAL (-5)  /* also: a device index check failed (libcrowdphot_b200_checked.so) */
 #define CPB_ERR_NO_DEVICE (-6) /* no CUDA device / library built without GPU */
 
 /* ---- element types ----------------------------------------------------- */

@@ -25,10 +25,11 @@ def test_header_declares_prototyped_symbols():
     assert set(names) == set(_abi.PROTOTYPES), (set(names) ^ set(_abi.PROTOTYPES))
 
 
-def test_library_exports_every_declared_symbol():
-    if not os.path.exists(_abi.LIB_PATH):
-        pytest.fail(f"library not built: {_abi.LIB_PATH}")
-    lib = C.CDLL(_abi.LIB_PATH)
+@pytest.mark.parametrize("path", [_abi.LIB_PATH, _abi.CHECKED_LIB_PATH], ids=["production", "checked"])
+def test_library_exports_every_declared_symbol(path):
+    if not os.path.exists(path):
+        pytest.fail(f"library not built: {path}")
+    lib = C.CDLL(path)
     for name in declared():
         assert hasattr(lib, name), name
     lib.cpb_version.restype = C.c_char_p
