@@ -250,7 +250,9 @@ def run_gpu(args):
     psf, img, bkg, iv, truth, init = make_field(ny, nx, n, replica_seed(SEED, rank))
     ctx = cpb.get_context(local)
     hp = ctx.psf_handle(psf)
-    P = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD)
+    # the timed form: the plain FP64 form, or (--quick only, for profiler captures) the mixed form
+    P = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD,
+                   precision=args.precision if args.quick else "fp64")
 
     # device-resident inputs (column-major images = torch (nx, ny) contiguous)
     t_img = torch.from_numpy(np.ascontiguousarray(img.T)).to(dev)
@@ -291,11 +293,30 @@ def run_gpu(args):
     clk = clocks.stop() if clocks else None
     _, launches = ctx.kernel_stats(reset=True)
     total_s = float(sum(dev_times))
+    def kernel_table(Pf):
+        ctx.set_profiling(True)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        _, secs = step_resident(Pf, SimOutputs(n, ny, nx, S2, residual=False))
+        ctx.set_profiling(False)
+        kst_, _ = ctx.kernel_stats(reset=True)
+        return kst_, secs, {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
+                                "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst_.items())}
+
     if args.quick:
+        # one more step with per-launch events (not timed above): the kernel table and
+        # the render-path kernels' algorithmic bandwidth
+        _, _, ktab = kernel_table(P)
+        peak = peaks()[0]
+        render = {k: dict(v, frac=v["GB_s"] / peak) for k, v in ktab.items()
+                  if k in ("k_gather_resid", "k_gather_cost", "k_gather_freeze", "k_eval_model", "k_gather_Jv",
+                           "k_JT_lsqr", "k_JT", "k_eval_fill")}
         if rank == 0:
-            print(json.dumps({"quick": True, "value": fitted_total / total_s, "unit": "stars/s",
+            print(json.dumps({"quick": True, "precision": args.precision, "value": fitted_total / total_s,
+                              "unit": "stars/s",
                               "ms_per_step": 1e3 * total_s / args.steps, "gpu_launches": launches,
-                              "config": workload_config(ny, nx, n)}))
+                              "config": workload_config(ny, nx, n), "kernels": ktab,
+                              "roofline_by_kernel": render, "peak_gbs": peak}))
         if world > 1:
             dist.destroy_process_group()
         return
@@ -327,16 +348,6 @@ def run_gpu(args):
         ms = [1e3 * t for t in times]
         return o, {"value": sm_[1] / mx_[0], "unit": "stars/s", "ms_per_step": float(np.mean(ms)),
                    "p50_ms": float(np.percentile(ms, 50)), "p99_ms": float(np.percentile(ms, 99))}
-
-    def kernel_table(Pf):
-        ctx.set_profiling(True)
-        flush.fill_(1.0)
-        torch.cuda.synchronize()
-        _, secs = step_resident(Pf, SimOutputs(n, ny, nx, S2, residual=False))
-        ctx.set_profiling(False)
-        kst_, _ = ctx.kernel_stats(reset=True)
-        return kst_, secs, {k: {"launches": v["launches"], "ms": 1e3 * v["seconds"],
-                                "GB_s": v["bytes"] / max(v["seconds"], 1e-12) / 1e9} for k, v in sorted(kst_.items())}
 
     Pm = sim_params(psf, FIT_RAD, {"bkg": 0.0}, inv_var_given=True, model_rad=FIT_RAD, precision="mixed")
     outs_m, mixed = timed_form(Pm, args.steps)
@@ -1265,6 +1276,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--quick", action="store_true",
                     help="only the warm-up and timed resident steps (for profiler captures); prints a short line")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="with --quick: the form the resident steps run")
     args = ap.parse_args()
     ref = {"crowded-field": run_reference, "lm-cutouts": run_reference_lm, "c4": run_reference_c4,
            "serve": run_reference, "multipass": run_reference_mp, "c1": run_reference_c1}

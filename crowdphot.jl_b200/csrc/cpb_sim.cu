@@ -818,7 +818,8 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
 // PLAN: every box meets at most 2 x 2 regions and every map written has
 // per-star rectangle offsets (srect), so only the storage-order walk is
 // compiled (the general paths' registers would otherwise spill in it).
-template <bool GRAD, typename T, bool PLAN>
+// GRAM: the Gram blocks (gram non-null) rather than the stamps.
+template <bool GRAD, typename T, bool PLAN, bool GRAM>
 __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                                       DevPsf P, const StarCoef* __restrict__ coef,
                                                       const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
@@ -827,6 +828,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                                                       double* __restrict__ gram, T* __restrict__ M, RectMap mmap,
                                                       int Rmax, const int32_t* __restrict__ Rs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if constexpr (!GRAM) gram = nullptr;  // the stamp instantiations carry no Gram code
     __shared__ StoreRect rtabs[256 / 32][kFillRects];
     __shared__ StorePlan plans[256 / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -897,14 +899,14 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
             gc_.flux = cg.flux;
             gc_.bkg = cg.bkg;
         }
-        // value (and gradient) at stamp entry (row, col), the row's table given
-        auto eval_rc = [&](const AxisTab<T>& rtab, int row, int col, T& val, T& ga, T& gb, T& gcc) {
+        // value (and gradient) at stamp entry (row, col)
+        auto eval_px = [&](int row, int col, T& val, T& ga, T& gb, T& gcc) {
             T g[3];
             if (gauss) {
                 val = gauss_eval<T, GRAD>((T)P.fwhm, gc_, (T)(oy + row), (T)(ox + col), g[0], g[1], g[2]);
             } else {
                 T pv, pdv = 0, pdu = 0;
-                tab_bicubic<GRAD, T>(base, tcol[col], rtab, nfill, pv, pdv, pdu);
+                tab_bicubic<GRAD, T>(base, tcol[col], trow[row], nfill, pv, pdv, pdu);
                 const T s = w0 * pv;
                 val = flux * s + bkg;
                 if (GRAD) {
@@ -919,88 +921,62 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
                 gcc = g2 == 0 ? g[0] : (g2 == 1 ? g[1] : g[2]);
             }
         };
-        auto eval_px = [&](int row, int col, T& val, T& ga, T& gb, T& gcc) {
-            eval_rc(trow[row], row, col, val, ga, gb, gcc);
-        };
         if (planned) {
-            // column walk: lane = storage row of the star's granule layout (box
-            // row + so), the box columns in order.  The lane's row table stays in
-            // registers, the column's table is one shared-memory broadcast, and at
-            // each column the warp's stores are consecutive rows of one or two
-            // rectangles (the box meets at most 2 x 2 regions).
+            // storage order: the star's rectangles one after another, each column
+            // by column, so the stores of a warp are consecutive; pad rows skipped
             double acc[6] = {0, 0, 0, 0, 0, 0};
-            const int b0 = top0 - so;            // 0-based image row of storage row 0
-            const int SRb = gran_rows(Sb, GH);
-            const int cx1 = (tx0 + 1) * TX;      // first image column of the second region column
-            for (int s0 = 0; s0 < SRb; s0 += 32) {
-                const int srow = s0 + lane, row = srow - so, y = b0 + srow;
-                const int iy = y >= 0 ? y / TY - ty0 : -1;
-                const bool rowin = srow < SRb && row >= 0 && row < Sb && iy >= 0 && iy < nty_j;
-                // this lane's rectangle in each region column: entry (srow, col) of
-                // plane 0 at base + col * nr, planes ps apart
-                int64_t baseV[2] = {0, 0}, baseM[2] = {0, 0};
-                int nr[2] = {0, 0}, ps[2] = {0, 0};
-#pragma unroll
-                for (int ix = 0; ix < 2; ++ix) {
-                    const int l = min(ix * nty_j + max(iy, 0), nrect - 1);
-                    nr[ix] = plan.nrows[l];
-                    ps[ix] = plan.ps[l];
-                    const int64_t rel = (int64_t)(srow - plan.s_lo[l]) - (int64_t)plan.c_lo[l] * plan.nrows[l];
-                    baseV[ix] = plan.offV[l] + rel;
-                    baseM[ix] = plan.offM[l] + rel;
-                }
-                AxisTab<T> rt{};
-                if (!gauss && rowin) rt = trow[row];
-                const bool ony = rowin && y < fc.ny;
-                for (int col = 0; col < Sb; ++col) {
-                    const int x = left0 + col;
-                    if (x < 0 || x >= (tx1 + 1) * TX) continue;  // no region holds the column (uniform)
-                    const int ix = x >= cx1 ? 1 : 0;
-                    if (!rowin) continue;
-                    const int64_t e = (ix ? baseV[1] : baseV[0]) + (int64_t)col * (ix ? nr[1] : nr[0]);
-                    const int64_t em = (ix ? baseM[1] : baseM[0]) + (int64_t)col * (ix ? nr[1] : nr[0]);
+            int l = 0, t = lane;
+            while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
+            while (l < nrect) {
+                const int cc = (int)(((float)t + 0.5f) * plan.inv_nrows[l]);
+                const int row = plan.s_lo[l] + (t - cc * plan.nrows[l]) - so, col = plan.c_lo[l] + cc;
+                if (row >= 0 && row < Sb) {
                     if (!GRAD) {
                         T val, a, b, c;
-                        eval_rc(rt, row, col, val, a, b, c);
-                        if (CPB_CHECK(em < mmap.len, 0x21)) M[em] = val;
+                        eval_px(row, col, val, a, b, c);
+                        if (CPB_CHECK(plan.offM[l] + t < mmap.len, 0x21)) M[plan.offM[l] + t] = val;
                     } else {
-                        const bool onimg = ony && x < fc.nx;
-                        const int64_t q = onimg ? y + (int64_t)x * fc.ny : 0;
-                        // the weights load beside the evaluation, not before it
+                        const int gy = oy + row, gx = ox + col;
+                        const bool onimg = gy >= 1 && gy <= fc.ny && gx >= 1 && gx <= fc.nx;
+                        const int64_t q = onimg ? (gy - 1) + (int64_t)(gx - 1) * fc.ny : 0;
+                        // the weights load beside the evaluation (no branch on them before it)
                         const double wq = onimg ? w[q] : 0.0, swq = onimg ? sw[q] : 0.0;
                         const bool use = onimg && wq > 0;
-                        T val, a, b, c;
-                        eval_rc(rt, row, col, val, a, b, c);
-                        if (wantM && CPB_CHECK(em < mmap.len, 0x22)) M[em] = val;
                         T r0 = 0, r1 = 0, r2 = 0;
-                        if (use) {
-                            const T sq = (T)swq;
-                            r0 = sq * a;
-                            r1 = sq * b;
-                            r2 = sq * c;
-                            const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
-                            if (gram) {
-                                acc[0] += d0 * d0;
-                                acc[1] += d0 * d1;
-                                acc[2] += d0 * d2;
-                                acc[3] += d1 * d1;
-                                acc[4] += d1 * d2;
-                                acc[5] += d2 * d2;
-                            } else {
-                                acc[0] += d0 * d0;
-                                acc[1] += d1 * d1;
-                                acc[2] += d2 * d2;
+                        if (onimg || wantM) {
+                            T val, a, b, c;
+                            eval_px(row, col, val, a, b, c);
+                            if (wantM && CPB_CHECK(plan.offM[l] + t < mmap.len, 0x22)) M[plan.offM[l] + t] = val;
+                            if (use) {
+                                const T sq = (T)swq;
+                                r0 = sq * a;
+                                r1 = sq * b;
+                                r2 = sq * c;
+                                const double d0 = r0, d1 = p > 1 ? (double)r1 : 0.0, d2 = p > 2 ? (double)r2 : 0.0;
+                                if (gram) {
+                                    acc[0] += d0 * d0;
+                                    acc[1] += d0 * d1;
+                                    acc[2] += d0 * d2;
+                                    acc[3] += d1 * d1;
+                                    acc[4] += d1 * d2;
+                                    acc[5] += d2 * d2;
+                                } else {
+                                    acc[0] += d0 * d0;
+                                    acc[1] += d1 * d1;
+                                    acc[2] += d2 * d2;
+                                }
                             }
                         }
-                        const int pst = ix ? ps[1] : ps[0];
-                        if (wantV && onimg && CPB_CHECK(e + (int64_t)(p - 1) * pst < vmap.len, 0x23)) {
-                            T* v = V + e;
+                        if (wantV && onimg && CPB_CHECK(plan.offV[l] + t + (int64_t)(p - 1) * plan.ps[l] < vmap.len, 0x23)) {
+                            T* v = V + plan.offV[l] + t;
                             v[0] = r0;
-                            if (p > 1) v[pst] = r1;
-                            if (p > 2) v[2 * pst] = r2;
+                            if (p > 1) v[plan.ps[l]] = r1;
+                            if (p > 2) v[2 * plan.ps[l]] = r2;
                         }
                     }
                 }
+                t += 32;
+                while (l < nrect && t >= plan.ps[l]) t -= plan.ps[l++];
             }
             if (GRAD) {
 #pragma unroll
@@ -1917,15 +1893,15 @@ inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)std::max<int64_t
 // the value-only form (no cache) takes any box.  smem: the axis tables.
 // k_eval_warp, the storage-order-walk-only instantiation when `plan` (every
 // box within 2 x 2 regions, every map written with per-star offsets)
-template <bool GRAD, typename TS, typename... A>
+template <bool GRAD, typename TS, bool GRAM = false, typename... A>
 void launch_eval_warp(bool plan, unsigned grid, unsigned thr, size_t smem, cudaStream_t st, A... args) {
     auto go = [&](auto kern) {
         if (smem > 48 * 1024)
             check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attr");
         kern<<<grid, thr, smem, st>>>(args...);
     };
-    if (plan) go(k_eval_warp<GRAD, TS, true>);
-    else go(k_eval_warp<GRAD, TS, false>);
+    if (plan) go(k_eval_warp<GRAD, TS, true, GRAM>);
+    else go(k_eval_warp<GRAD, TS, false, GRAM>);
 }
 
 template <bool GRAD, typename T, typename... A>
@@ -3000,7 +2976,7 @@ void SimFit::finish() {
             const unsigned gbw =
                 (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_act + wpb - 1) / wpb, (int64_t)ctx->n_sm * 8));
             const bool plan = 2 * fc.R + 1 <= TX + 1 && 2 * fc.R + 1 <= TY + 1;  // the Gram needs no map
-            launch_eval_warp<true, double>(plan, gbw, thr, sm_bytes, st, (const int32_t*)nullptr, (int64_t)n_act, f64,
+            launch_eval_warp<true, double, true>(plan, gbw, thr, sm_bytes, st, (const int32_t*)nullptr, (int64_t)n_act, f64,
                                            dp, coef, ay, ax, w, sw, (double*)nullptr, RectMap{}, cn, gram,
                                            (double*)nullptr, RectMap{}, fc.R, (const int32_t*)nullptr);
         } else {
