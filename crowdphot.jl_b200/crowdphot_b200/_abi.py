@@ -314,7 +314,8 @@ PROTOTYPES = {
 }
 
 PACKAGE_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PACKAGE_DIR, "lib", "libcrowdphot_b200.so")
+# CROWDPHOT_B200_LIB (as for the Julia binding) selects another build of the library
+LIB_PATH = os.environ.get("CROWDPHOT_B200_LIB") or os.path.join(PACKAGE_DIR, "lib", "libcrowdphot_b200.so")
 # the same library with every stamp and pixel index of the simultaneous fit
 # tested against its buffer (a failed test skips the access and fails the call)
 CHECKED_LIB_PATH = os.path.join(PACKAGE_DIR, "lib", "libcrowdphot_b200_checked.so")

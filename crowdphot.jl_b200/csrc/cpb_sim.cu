@@ -504,32 +504,6 @@ __global__ void k_rect_size(int64_t npairs, const int4* __restrict__ list, const
     size[i] = (int64_t)planes * g.ncols * g.nrows;
 }
 
-// a[0 .. n) += v in shared memory, 16 bytes at a time (a is 16-byte aligned)
-template <typename T, int N>
-__device__ __forceinline__ void smem_add_gran(T* a, const T (&v)[N]) {
-    static_assert((N * sizeof(T)) % 16 == 0, "whole 16-byte chunks");
-    if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int c = 0; c < N; c += 4) {
-            float4 t = *(float4*)(a + c);
-            t.x += v[c];
-            t.y += v[c + 1];
-            t.z += v[c + 2];
-            t.w += v[c + 3];
-            *(float4*)(a + c) = t;
-        }
-    } else {
-#pragma unroll
-        for (int c = 0; c < N; c += 2) {
-            double2 t = *(double2*)(a + c);
-            t.x += v[c];
-            t.y += v[c + 1];
-            *(double2*)(a + c) = t;
-        }
-    }
-}
-
-
 // model_from_vector for star j: theta (+ delta when cand).
 __global__ void k_coef(int64_t n_act, FitConst fc, DevPsf P, const double* theta, const double* delta,
                        StarCoef* coef) {
@@ -1114,7 +1088,8 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // stars one after another: the region's stamps are one contiguous run, read
 // in whole 16-byte granules.  The warp walks its stars' granules in
 // 32-granule slots (one star a slot, a star's last slot padded) and loads
-// KSLOT slots -- KSLOT * p granules a lane -- before adding any, slot by slot.
+// gather_slots<KIND>() slots -- 12 granules a lane -- before adding any, slot
+// by slot.
 // Each pixel is the sum of the warps' copies in warp order: a fixed order
 // (no atomics, bitwise reproducible).
 //   KIND_JV: sum_k V[j, k, m] * v[j, k] / (alpha colnorm[j, k])  (apply_J!,
@@ -1127,8 +1102,11 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // sums are FP64.
 constexpr int KIND_JV = 0, KIND_M = 1;
 constexpr int MODE_LSQR = 4;
-// slots a warp loads per round before adding
+// slots a warp loads per round before adding: J v (three planes) 4, the model
+// renders (one plane) 12, so that either keeps 12 granules a lane in flight
 constexpr int KSLOT = 4;
+template <int KIND>
+constexpr int gather_slots() { return KIND == KIND_JV ? KSLOT : 3 * KSLOT; }
 // the warps' FP64 region copies (sums are FP64 for either stamp type: FP32
 // sums of the mixed-precision form moved its fit measurably, FP32 storage did not)
 constexpr size_t kGatherSmem = (size_t)(NT / 32) * TX * TY * sizeof(double);
@@ -1150,7 +1128,12 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
     constexpr int NW = NT / 32;
     constexpr int NPL = KIND == KIND_JV ? 3 : 1;
     extern __shared__ __align__(16) unsigned char g_smem[];
-    double* parts = (double*)g_smem;     // [NW][TX][TY], column-major per warp
+    // the warps' region copies, [NW][TX * TY] doubles each: granule g (= column *
+    // NGR + granule row) keeps its rows 0-1 at 2 g and rows 2-3 (4-row granules)
+    // at kHalf + 2 g, so a warp's 16-byte accesses to consecutive granules are
+    // consecutive (no bank conflicts for either granule height)
+    constexpr int kHalf = TX * TY / 2;
+    double* parts = (double*)g_smem;
     __shared__ int64_t s_off[NT];
     __shared__ int s_ay[NT];
     __shared__ int s_ax[NT];
@@ -1233,10 +1216,11 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             star_geometry();
         }
         while (e < total) {
-            TS raw[KSLOT][NPL][GH];
-            int dst[KSLOT], eq[KSLOT];
+            constexpr int KS = gather_slots<KIND>();
+            TS raw[KS][NPL][GH];
+            int dst[KS], eq[KS];
 #pragma unroll
-            for (int q = 0; q < KSLOT; ++q) {
+            for (int q = 0; q < KS; ++q) {
                 dst[q] = -1;
                 eq[q] = e;
                 if (e < total) {
@@ -1246,11 +1230,11 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                         const int gg = t - cc * nga;
                         const TS* g = base + (int64_t)t * GH;
                         if (CPB_CHECK(g - src + (p - 1) * PSb + GH <= src_len, 0x31) &&
-                            CPB_CHECK((cl0 + cc) * TY + (gl0 + gg) * GH + GH <= TX * TY, 0x32)) {
+                            CPB_CHECK((cl0 + cc) * NGR + (gl0 + gg) < TX * NGR, 0x32)) {
 #pragma unroll
                             for (int k = 0; k < NPL; ++k)
                                 if (k < p) ld_gran(g + k * PSb, raw[q][k]);
-                            dst[q] = (cl0 + cc) * TY + (gl0 + gg) * GH;
+                            dst[q] = (cl0 + cc) * NGR + (gl0 + gg);  // granule index in the region
                         }
                     }
                     if ((c + 1) * 32 < tot) {
@@ -1267,7 +1251,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             // slots in order; two slots of a round may meet at a pixel (different
             // lanes), so each slot's adds complete before the next slot's start
 #pragma unroll
-            for (int q = 0; q < KSLOT; ++q) {
+            for (int q = 0; q < KS; ++q) {
                 if (dst[q] >= 0) {
                     double v[GH];
 #pragma unroll
@@ -1280,7 +1264,14 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
                         }
                         v[r] = t;
                     }
-                    smem_add_gran(mine + dst[q], v);
+#pragma unroll
+                    for (int h = 0; h < GH; h += 2) {
+                        double2* a = (double2*)(mine + (h >> 1) * kHalf + 2 * dst[q]);
+                        double2 t = *a;
+                        t.x += v[h];
+                        t.y += v[h + 1];
+                        *a = t;
+                    }
                 }
                 __syncwarp();
             }
@@ -1293,14 +1284,13 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
         const int col = gi / NGR, gr = gi % NGR;
         const int gx = C0 + col;
         if (gx >= fc.nx) continue;
-        const int off = col * TY + gr * GH;
         double acc[GH];
 #pragma unroll
-        for (int r = 0; r < GH; ++r) acc[r] = parts[off + r];
+        for (int r = 0; r < GH; ++r) acc[r] = parts[(r >> 1) * kHalf + 2 * gi + (r & 1)];
 #pragma unroll
         for (int q = 1; q < NW; ++q)
 #pragma unroll
-            for (int r = 0; r < GH; ++r) acc[r] += parts[q * TX * TY + off + r];
+            for (int r = 0; r < GH; ++r) acc[r] += parts[q * TX * TY + (r >> 1) * kHalf + 2 * gi + (r & 1)];
 #pragma unroll
         for (int r = 0; r < GH; ++r) {
             const int gy = R0 + gr * GH + r;
