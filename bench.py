@@ -40,11 +40,11 @@ N_STARS = 50_000
 FIT_RAD = 12
 SEED = 1002
 SAMPLE = 512  # CPU sample side (same star density)
-# DRAM bytes moved per algorithmic byte by the FP64 J v gather (read 815.7 MB + write
-# 7.3 MB against 818.3 MB algorithmic), from an ncu capture of one launch of the same
-# kernel on this 2048^2 field (an LSQR launch of the first outer iteration, every star
-# live; one metric pass, no replay)
-JV_TRAFFIC_RATIO = (815.72 + 7.32) / 818.3
+# DRAM bytes moved per algorithmic byte by the FP64 J v gather (read 816.8 MB + write
+# 5.9 MB against 818.3 MB algorithmic: 50,000 live stars x (3 x 625 x 8 + 24) B + two
+# 2048^2 FP64 pixel vectors), from an ncu capture of the first launch of the kernel on
+# this 2048^2 field (every star live; one metric pass, no replay)
+JV_TRAFFIC_RATIO = (816.78 + 5.90) / 818.3
 
 
 def workload_config(ny=NY, nx=NX, n=N_STARS):

@@ -65,60 +65,6 @@ struct DevPsf {
     int64_t total_elems;      // sum of padded node sizes
 };
 
-// ---------------------------------------------------------------------------
-// bulk staging of a table into shared memory
-// ---------------------------------------------------------------------------
-// Polls of the staging mbarrier before a block gives up on its bulk copy.
-constexpr long long kStageWaitLimit = 1ll << 22;
-
-// Copies `bytes` (a multiple of 16) from global `src` to shared `dst` (both
-// 16-byte aligned) with one bulk asynchronous copy (cp.async.bulk, the tensor
-// memory accelerator's 1-D form; this GPU's own memory, no multicast) that
-// completes on the shared-memory mbarrier *bar.  Every thread of the block
-// calls it and waits, boundedly, for the copy; false when its wait ran out.
-__device__ __forceinline__ bool bulk_stage(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    const unsigned mb = (unsigned)__cvta_generic_to_shared(bar);
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the init, seen by the copy engine
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                (unsigned)__cvta_generic_to_shared(dst)),
-            "l"(src), "r"(bytes), "r"(mb)
-            : "memory");
-    }
-    for (long long it = 0; it < kStageWaitLimit; ++it) {
-        unsigned done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(mb)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// A node table of `nel` doubles into shared memory: the 16-byte-aligned bulk
-// with bulk_stage, the remainder (or all of it, for an unaligned source) with
-// plain loads.  Returns whether the shared copy can be read (a bulk copy whose
-// wait ran out leaves the caller on the global table; the block then keeps its
-// shared memory until it exits, so a late copy lands where nothing reads).
-__device__ __forceinline__ bool stage_node_table(double* dst, const double* src, int nel, unsigned long long* bar) {
-    const bool aligned = ((uintptr_t)src & 15) == 0 && ((uintptr_t)dst & 15) == 0;
-    const int nbulk = aligned ? (nel & ~1) : 0;
-    for (int k = nbulk + (int)threadIdx.x; k < nel; k += (int)blockDim.x) dst[k] = src[k];
-    bool ok = true;
-    if (nbulk > 0) ok = bulk_stage(dst, src, (unsigned)nbulk * 8u, bar);
-    __syncthreads();
-    return ok;
-}
-
 // Per-star model coefficients for one parameter vector (theta or theta+delta).
 struct StarCoef {
     double y, x, flux, bkg;

@@ -1304,16 +1304,19 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_lm_t(int64_t n_cut, LMConst L
     __shared__ LMState<NP, NF> states[kLMThreads / TS];
     __shared__ double red_all[(kLMThreads / 32) * KR];
     __shared__ unsigned long long cut_sh[kLMThreads / TS];
-    extern __shared__ __align__(16) double node_smem[];
+    extern __shared__ double node_smem[];
     const int team = threadIdx.x / TS;
     LMState<NP, NF>& S = states[team];
     double* red = red_all + team * WPC * KR;
     const int lane = threadIdx.x % TS;  // index within the team (lane 0 stores the team's state)
-    // the node's polyphase samples, staged once per (persistent) block by a bulk copy
+    // the node's polyphase samples, staged once per (persistent) block (plain
+    // loads: a 1-D bulk asynchronous copy measured 4.5 % slower for the whole kernel)
     const double* pp = N.pp;
     if (SMEM && NP == 4) {
-        __shared__ unsigned long long stage_bar;
-        if (stage_node_table(node_smem, N.pp, N.plane * N.nd.isy * N.nd.isx, &stage_bar)) pp = node_smem;
+        const int nel = N.plane * N.nd.isy * N.nd.isx;
+        for (int k = threadIdx.x; k < nel; k += blockDim.x) node_smem[k] = N.pp[k];
+        __syncthreads();
+        pp = node_smem;
     }
     for (;;) {
         unsigned long long cc = 0;
@@ -1391,7 +1394,7 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, D
     __shared__ LMState<NP, NF> states[kLMThreads / TS];
     __shared__ double red_all[(kLMThreads / 32) * KR];
     __shared__ int pos_sh[kLMThreads / TS];
-    extern __shared__ __align__(16) double node_smem[];
+    extern __shared__ double node_smem[];
     const int team = threadIdx.x / TS;
     LMState<NP, NF>& S = states[team];
     double* red = red_all + team * WPC * KR;
@@ -1401,9 +1404,11 @@ __global__ void __launch_bounds__(kLMThreads, 2) k_mp_dag(LMConst L, PPNode N, D
     double* civ = A.civ ? A.civ + (int64_t)gteam * A.box_max : nullptr;
     const TIV* ivimg = (const TIV*)A.iv;
     const double* pp = N.pp;
-    if (SMEM && NP == 4) {  // the node's polyphase samples, staged once per block by a bulk copy
-        __shared__ unsigned long long stage_bar;
-        if (stage_node_table(node_smem, N.pp, N.plane * N.nd.isy * N.nd.isx, &stage_bar)) pp = node_smem;
+    if (SMEM && NP == 4) {  // the node's polyphase samples, staged once per block
+        const int nel = N.plane * N.nd.isy * N.nd.isx;
+        for (int k = threadIdx.x; k < nel; k += blockDim.x) node_smem[k] = N.pp[k];
+        __syncthreads();
+        pp = node_smem;
     }
     int* head = A.counters;
     int* tail = A.counters + 1;

@@ -1088,8 +1088,7 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // stars one after another: the region's stamps are one contiguous run, read
 // in whole 16-byte granules.  The warp walks its stars' granules in
 // 32-granule slots (one star a slot, a star's last slot padded) and loads
-// gather_slots<KIND>() slots -- 12 granules a lane -- before adding any, slot
-// by slot.
+// KSLOT slots -- KSLOT * p granules a lane -- before adding any, slot by slot.
 // Each pixel is the sum of the warps' copies in warp order: a fixed order
 // (no atomics, bitwise reproducible).
 //   KIND_JV: sum_k V[j, k, m] * v[j, k] / (alpha colnorm[j, k])  (apply_J!,
@@ -1102,11 +1101,9 @@ __global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict_
 // sums are FP64.
 constexpr int KIND_JV = 0, KIND_M = 1;
 constexpr int MODE_LSQR = 4;
-// slots a warp loads per round before adding: J v (three planes) 4, the model
-// renders (one plane) 12, so that either keeps 12 granules a lane in flight
+// slots a warp loads per round before adding (J v: 12 granules a lane in flight;
+// the one-plane model renders measured slower with 12 slots than with 4)
 constexpr int KSLOT = 4;
-template <int KIND>
-constexpr int gather_slots() { return KIND == KIND_JV ? KSLOT : 3 * KSLOT; }
 // the warps' FP64 region copies (sums are FP64 for either stamp type: FP32
 // sums of the mixed-precision form moved its fit measurably, FP32 storage did not)
 constexpr size_t kGatherSmem = (size_t)(NT / 32) * TX * TY * sizeof(double);
@@ -1216,11 +1213,10 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             star_geometry();
         }
         while (e < total) {
-            constexpr int KS = gather_slots<KIND>();
-            TS raw[KS][NPL][GH];
-            int dst[KS], eq[KS];
+            TS raw[KSLOT][NPL][GH];
+            int dst[KSLOT], eq[KSLOT];
 #pragma unroll
-            for (int q = 0; q < KS; ++q) {
+            for (int q = 0; q < KSLOT; ++q) {
                 dst[q] = -1;
                 eq[q] = e;
                 if (e < total) {
@@ -1251,7 +1247,7 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
             // slots in order; two slots of a round may meet at a pixel (different
             // lanes), so each slot's adds complete before the next slot's start
 #pragma unroll
-            for (int q = 0; q < KS; ++q) {
+            for (int q = 0; q < KSLOT; ++q) {
                 if (dst[q] >= 0) {
                     double v[GH];
 #pragma unroll
