@@ -1680,9 +1680,12 @@ int fit_groups_dev(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, in
             kind = e.msg.find("non-finite") != std::string::npos ? 1 : 2;
             std::vector<double> hy(ng), hx(ng), hf(ng);
             if (ng > 0) {
-                check(cudaMemcpy(hy.data(), d_y0 + s0, 8 * ng, cudaMemcpyDeviceToHost), "d2h");
-                check(cudaMemcpy(hx.data(), d_x0 + s0, 8 * ng, cudaMemcpyDeviceToHost), "d2h");
-                check(cudaMemcpy(hf.data(), d_f0 + s0, 8 * ng, cudaMemcpyDeviceToHost), "d2h");
+                // on the context's stream (non-blocking: a legacy-stream copy would not
+                // wait for the catalogue's upload)
+                check(cudaMemcpyAsync(hy.data(), d_y0 + s0, 8 * ng, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+                check(cudaMemcpyAsync(hx.data(), d_x0 + s0, 8 * ng, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+                check(cudaMemcpyAsync(hf.data(), d_f0 + s0, 8 * ng, cudaMemcpyDeviceToHost, ctx->stream), "d2h");
+                check(cudaStreamSynchronize(ctx->stream), "d2h");
             }
             const double NaN = std::numeric_limits<double>::quiet_NaN();
             for (int64_t i = 0; i < ng; ++i) {

@@ -792,9 +792,11 @@ __global__ void __launch_bounds__(NTF) k_eval(const int32_t* __restrict__ list, 
 // PLAN: every box meets at most 2 x 2 regions and every map written has
 // per-star rectangle offsets (srect), so only the storage-order walk is
 // compiled (the general paths' registers would otherwise spill in it).
-// GRAM: the Gram blocks (gram non-null) rather than the stamps.
+// GRAM: the Gram blocks (gram non-null) rather than the stamps.  Four blocks
+// an SM for FP32 stamps, three for FP64 (four measured slower there: the FP64
+// taps' registers spill).
 template <bool GRAD, typename T, bool PLAN, bool GRAM>
-__global__ void __launch_bounds__(256, 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3) k_eval_warp(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                                       DevPsf P, const StarCoef* __restrict__ coef,
                                                       const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
                                                       const double* __restrict__ w, const double* __restrict__ sw,
@@ -1342,8 +1344,9 @@ __global__ void __launch_bounds__(NT) k_gather(FitConst fc, const int32_t* __res
 // form: v_new = z - beta * v_old / alpha_old and alpha = ||v_new|| (Krylov
 // lsqr step 2).  Sums are FP64 for either stamp type.
 constexpr int kJTRects = 16;  // rectangles a warp tabulates at a time
+// four blocks an SM (64 registers; three with 80 and five with 48 measured slower)
 template <bool LSQR, typename TS, typename TU>
-__global__ void __launch_bounds__(256, 3) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
+__global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list, int64_t nlist, FitConst fc,
                                             const int32_t* __restrict__ ay, const int32_t* __restrict__ ax,
                                             const TS* __restrict__ V, RectMap vmap, const double* __restrict__ cn,
                                             const TU* __restrict__ u, double* __restrict__ z, Scalars* sc,
