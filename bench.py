@@ -433,6 +433,21 @@ def run_gpu(args):
     h2d = 3 * img.nbytes + 3 * 8 * n
     d2h = n * (12 * 8 + 2 + 4) + ny * nx * 8
 
+    # the comparison the headline metric names: the served stream (C5) through the
+    # served mixed form against the plain FP64 form, same requests (one GPU; it runs
+    # while the spawned oracle fit is still going)
+    served = None
+    if world == 1 and not args.no_serve:
+        out_s, acc_s, specs_s, _, _ = serve_stream(args.n_requests, args.max_inflight, 1, rank, local,
+                                                   sample_clocks=False)
+        keep = ("value", "fitted", "makespan_s", "p50_ms", "p99_ms", "slots_used")
+        served = {"workload": serve_config(args.n_requests, specs_s)["workload"],
+                  "served_mixed": {k: out_s["served_mixed"][k] for k in keep},
+                  "plain": {k: out_s["plain"][k] for k in keep},
+                  "speedup_vs_plain": out_s["served_mixed"]["value"] / out_s["plain"]["value"],
+                  "accuracy": acc_s, "unit": "stars/s",
+                  "timer": "host wall clock from the first arrival to the last result"}
+
     if rank == 0:
         ms = sorted(1e3 * t for t in dev_times)
         line = {"metric": METRIC, "value": value, "unit": "stars/s", "n_gpus": world, "steps": args.steps,
@@ -444,7 +459,8 @@ def run_gpu(args):
                 "model_px_evals_per_s": float(outs.c.model_px_evals) / s_prof,
                 "roofline": roof, "kernels": kernels, "gpu_launches": launches_all, "clocks": clk,
                 "forms": {"plain_fp64": {"value": value, "ms_per_step": 1e3 * total_s / args.steps},
-                          "mixed": mixed, "mixed_refine2": refined, "conditioning": conditioning},
+                          "mixed": mixed, "mixed_refine2": refined, "conditioning": conditioning,
+                          "served_stream": served},
                 "e2e": {"value": e_value, "unit": "stars/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_baseline_single()
@@ -941,17 +957,18 @@ def _run_stream(sv, psf, reqs, arrivals, precision):
     return results, infos, makespan
 
 
-def run_gpu_serve(args):
+def serve_stream(n_requests, max_inflight, warmup, rank, local, sample_clocks=True):
+    """The served stream (C5) run twice on one GPU: the plain FP64 form one request
+    at a time and the served mixed form with `max_inflight` slots.  Returns the
+    per-form summaries (with the results), the accuracy of the served form against
+    the plain one, the request specs and inputs, and the clock record."""
     import torch
 
     import crowdphot_b200 as cpb
     from crowdphot_b200.simulate import moffat_epsf, served_field
 
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
     psf = moffat_epsf()
-    arrivals, specs = serve_requests(args.n_requests, 5000 + 1000 * rank)
+    arrivals, specs = serve_requests(n_requests, 5000 + 1000 * rank)
     reqs = []
     for side, dens, sd in specs:
         img, bkg, iv, truth, init = served_field(side, dens, seed=sd, psf=psf)
@@ -960,12 +977,12 @@ def run_gpu_serve(args):
     warm = reqs[int(np.argmin([s for s, _, _ in specs]))]
     clocks, clk = None, None
     out = {}
-    for form, slots, prec in (("plain", 1, "fp64"), ("served_mixed", args.max_inflight, "mixed")):
+    for form, slots, prec in (("plain", 1, "fp64"), ("served_mixed", max_inflight, "mixed")):
         with cpb.Server(device=local, max_inflight=slots) as sv:
-            for _ in range(max(args.warmup, 1)):
+            for _ in range(max(warmup, 1)):
                 sv.submit(warm[0], psf, warm[3], FIT_RAD, inv_var=warm[2], background=warm[1], precision=prec,
                           **fit_kwargs()).result(timeout=600)
-            if form == "served_mixed" and rank == 0:
+            if form == "served_mixed" and rank == 0 and sample_clocks:
                 clocks = ClockSampler(torch.cuda.current_device())
             res, infos, makespan = _run_stream(sv, psf, reqs, arrivals, prec)
             if form == "served_mixed" and clocks is not None:
@@ -988,6 +1005,16 @@ def run_gpu_serve(args):
                                     "frac_within_1e-5": float(np.mean(dfl <= 1e-5))},
            "pos_dev_px_vs_fp64": {"median": float(np.median(dpos)), "p99": float(np.percentile(dpos, 99)),
                                   "frac_within_1e-4": float(np.mean(dpos <= 1e-4))}}
+    return out, acc, specs, reqs, clk
+
+
+def run_gpu_serve(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    out, acc, specs, reqs, clk = serve_stream(args.n_requests, args.max_inflight, args.warmup, rank, local)
     sm, pl = out["served_mixed"], out["plain"]
     h2d = sum(r[0].nbytes * 3 + 24 * r[3]["y"].size for r in reqs)
     d2h = sum(r[3]["y"].size * (12 * 8 + 2 + 4) for r in reqs)
@@ -1278,6 +1305,8 @@ def main():
     ap.add_argument("--max-inflight", type=int, default=4)
     ap.add_argument("--n-cutouts", type=int, default=LM_CUTOUTS)
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="default workload: skip the served-stream comparison in forms.served_stream")
     ap.add_argument("--quick", action="store_true",
                     help="only the warm-up and timed resident steps (for profiler captures); prints a short line")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",

@@ -4,17 +4,20 @@
 // (src/photometry/psf_photometry_simultaneous.jl:953-1431).  Layout in HBM:
 //   * per-pixel vectors (data, data_work, w, sqrt(w), union mask, residual,
 //     LSQR u) are column-major npix arrays, as in the reference;
-//   * stamp derivatives V are star-major: star j owns a contiguous block of
-//     p planes (one per free parameter) of the unscaled weighted derivatives
-//     over its fit box (StampDerivatives.values, :19-43, times colnorm), each
-//     plane in the granule layout (gran_rows): box columns padded so that
-//     16-byte granules line up with image rows;
+//   * stamp derivatives V (the unscaled weighted derivatives over each fit
+//     box, StampDerivatives.values, :19-43, times colnorm) and the model
+//     stamps are stored region-contiguously: the image is cut into 32 x 32
+//     pixel regions, the part of a star's box inside one region is a dense
+//     rectangle (p planes, one per free parameter, each column in 16-byte
+//     granules aligned with image rows: gran_rows), and a region's rectangles
+//     follow one another in its star-list order, so a region's stamps are one
+//     contiguous run (RectMap);
 //   * stamp pixel indices are not stored: they follow from the integer anchor
 //     and the fit-box offset (the reference's `pixels` matrix is rebuilt only
 //     for the bit-exact debug export);
-//   * per-tile star lists (32 x 8 pixel tiles, stars in Morton order) turn the
-//     reference's scatter-adds (apply_J!, _render_model!) into deterministic
-//     pixel gathers with no atomics.
+//   * per-region star lists (stars in Morton order) turn the reference's
+//     scatter-adds (apply_J!, _render_model!) into deterministic pixel
+//     gathers with no atomics.
 // Control flow per outer iteration follows :1186-1284; the LSQR inner solve
 // runs entirely on the device with its stopping tests evaluated in-kernel.
 #include <cub/cub.cuh>
