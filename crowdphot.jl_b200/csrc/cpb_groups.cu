@@ -1343,7 +1343,6 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
     if (!(model_rad_max >= P->fit_rad)) throw ArgError{"model_rad_max must be >= fit_rad"};
     if (!(P->model_rad_nsigma > 0)) throw ArgError{"model_rad_nsigma must be positive"};
     if (P->solver != CPB_SOLVER_LSQR && P->solver != CPB_SOLVER_LSMR) throw ArgError{"solver must be :lsqr or :lsmr"};
-    if (P->solver == CPB_SOLVER_LSMR) throw ArgError{"solver :lsmr is not supported by the B200 path; use :lsqr"};
     if (P->damping == CPB_DAMP_LEVENBERG)
         throw ArgError{
             "LevenbergDamping is not supported by fit_all_stars_simultaneous: it conflicts with the "
@@ -1473,13 +1472,16 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
         return ng > 32 ? layout_bytes<uint64_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn)
                        : layout_bytes<uint32_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn);
     };
-    // a group runs in the kernel when it has <= 64 stars and its own layout fits
+    // a group runs in the kernel when it has <= 64 stars and its own layout fits;
+    // the kernel's in-block solver is LSQR, so solver = :lsmr routes every group
+    // to the full-field fit
+    const bool lsmr = P->solver == CPB_SOLVER_LSMR;
     std::vector<Bucket> bk(kNumBuckets);
     for (int64_t g = 0; g < G; ++g) {
         const int ng = (int)(h_soff[g + 1] - h_soff[g]);
         const int um = (int)std::min<int64_t>((int64_t)ng * C.S2, (int64_t)h_ny[g] * h_nx[g]);
         const int kn = next_pow2(std::max(ng * C.S2, 2));
-        if (ng > kMaxGroupStars || need_of(ng, um, kn) > cap) {
+        if (lsmr || ng > kMaxGroupStars || need_of(ng, um, kn) > cap) {
             plan.routed_groups.push_back((int32_t)g);
             continue;
         }
@@ -1770,6 +1772,9 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
             setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,
                          total_pixels, out, nullptr, nullptr, nullptr, nullptr, b->su);
         const GroupPlan& plan = b->su.plan;
+        if (!plan.routed_groups.empty() && P->solver == CPB_SOLVER_LSMR)
+            throw ArgError{"solver :lsmr groups are fitted one by one by the full-field fit; use "
+                           "cpb_fit_simultaneous_batch instead of a captured batch"};
         if (!plan.routed_groups.empty())
             throw ArgError{"group " + std::to_string(plan.routed_groups[0]) +
                            " is too large for one thread block (more than 64 stars, or a working set beyond shared "

@@ -65,6 +65,9 @@ struct Scalars {
     double Anorm2, dNorm2, xNorm, xNorm2, c2, s2, z, xENorm2, res2, rhobar, phibar, ArNorm0;
     double err_vec[5];
     double wnorm2;
+    // LSMR state (solver = :lsmr; Fong & Saunders 2011 recurrences)
+    double m_alphabar, m_rho, m_rhobar, m_cbar, m_sbar, m_zeta, m_zetabar;
+    double m_betadd, m_betad, m_rhodold, m_tautildeold, m_thetatilde, m_d, m_maxrbar, m_minrbar;
     double lambda, atol, btol;
     int iter, itmax, stopped, status;
     int n_new_frozen;
@@ -1480,7 +1483,8 @@ __global__ void __launch_bounds__(256, 4) k_JT(const int32_t* __restrict__ list,
 
 // LSQR init after b_scaled: v1 = A'u1 = -b_scaled / beta1 (the first
 // adjoint product reuses the gradient pass), alpha1 = ||v1||, x = 0.
-__global__ void k_lsqr_v0(int64_t n, const double* b_scaled, double* vt, double* x, Scalars* sc, Reducer red) {
+__global__ void k_lsqr_v0(int64_t n, const double* b_scaled, double* vt, double* x, Scalars* sc, Reducer red,
+                          bool lsmr) {
     __shared__ double sh[32];
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const double inv_b1 = sc->inv_beta;
@@ -1503,7 +1507,7 @@ __global__ void k_lsqr_v0(int64_t n, const double* b_scaled, double* vt, double*
         if (alpha == 0.0) {
             sc->stopped = 1;
             sc->status = 4;
-        } else {
+        } else if (!lsmr) {  // lsqr's test before the first iteration (lsmr has none)
             double Anorm = alpha, rNorm = sc->beta1;
             double t = sc->ArNorm0 / (Anorm * rNorm);
             if (t <= 1.4901161193847656e-08 || 1.0 + t <= 1.0) {
@@ -1606,6 +1610,126 @@ __global__ void k_lsqr_update(int64_t n, const double* vt, double* x, double* wl
         sc->z = z;
         sc->res2 = res2;
         sc->wnorm2 = tot;
+        sc->iter = iter;
+        if (solved || tired || ill) {
+            sc->stopped = 1;
+            sc->status = solved ? (zr ? 2 : 1) : (ill ? 3 : 0);
+        }
+    }
+}
+
+// LSMR start (solver = :lsmr) after k_lsqr_v0: h = v1, hbar = 0 and the
+// recurrence state of Fong & Saunders' algorithm (zetabar = alpha1 beta1, ...).
+__global__ void k_lsmr_init(int64_t n, const double* vt, double* h, double* hbar, Scalars* sc) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double ia = sc->inv_alpha;
+    if (i < n) {
+        h[i] = vt[i] * ia;
+        hbar[i] = 0.0;
+    }
+    if (i == 0) {
+        sc->m_alphabar = sc->alpha;
+        sc->m_rho = 1.0;
+        sc->m_rhobar = 1.0;
+        sc->m_cbar = 1.0;
+        sc->m_sbar = 0.0;
+        sc->m_zeta = 0.0;
+        sc->m_zetabar = sc->alpha * sc->beta1;
+        sc->m_betadd = sc->beta1;
+        sc->m_betad = 0.0;
+        sc->m_rhodold = 1.0;
+        sc->m_tautildeold = 0.0;
+        sc->m_thetatilde = 0.0;
+        sc->m_d = 0.0;
+        sc->m_maxrbar = 0.0;
+        sc->m_minrbar = 1e100;
+    }
+}
+
+// One LSMR iteration after the Golub-Kahan step (Krylov lsmr main loop): the
+// rotations eliminating the damping and turning B into R and R' into Rbar,
+// hbar / x / h updates with ||x||^2 reduced over the grid, then (last block)
+// the ||r||, ||A|| and cond(A) estimates and the stopping tests.  Every
+// thread evaluates the same rotations from the state; the last block commits.
+__global__ void k_lsmr_update(int64_t n, const double* vt, double* x, double* h, double* hbar, Scalars* sc,
+                              Reducer red) {
+    __shared__ double sh[32];
+    if (sc->stopped) return;
+    const double alpha = sc->alpha, beta = sc->beta, lambda = sc->lambda;
+    double chat, shat, alphahat;
+    sym_givens(sc->m_alphabar, lambda, chat, shat, alphahat);
+    const double rhoold = sc->m_rho;
+    double c, s, rho;
+    sym_givens(alphahat, beta, c, s, rho);
+    const double thetanew = s * alpha;
+    const double rhobarold = sc->m_rhobar, zetaold = sc->m_zeta;
+    const double thetabar = sc->m_sbar * rho, rhotemp = sc->m_cbar * rho;
+    double cbar, sbar, rhobar;
+    sym_givens(sc->m_cbar * rho, thetanew, cbar, sbar, rhobar);
+    const double zeta = cbar * sc->m_zetabar, zetabar = -sbar * sc->m_zetabar;
+    const double kh = thetabar * rho / (rhoold * rhobarold), kx = zeta / (rho * rhobar), kv = thetanew / rho;
+    const double ia = sc->inv_alpha;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double part = 0.0;
+    if (i < n) {
+        const double hb = h[i] - kh * hbar[i];
+        hbar[i] = hb;
+        const double xi = x[i] + kx * hb;
+        x[i] = xi;
+        h[i] = vt[i] * ia - kv * h[i];
+        part = xi * xi;
+    }
+    double tot;
+    if (grid_reduce<256>(part, red, sh, &tot) && threadIdx.x == 0) {
+        const double axtol = 1.4901161193847656e-08, ctol = axtol;
+        const int iter = sc->iter + 1;
+        // ||r|| estimate
+        const double betaacute = chat * sc->m_betadd, betacheck = -shat * sc->m_betadd;
+        const double betahat = c * betaacute, betadd = -s * betaacute;
+        const double thetatildeold = sc->m_thetatilde;
+        double ctildeold, stildeold, rhotildeold;
+        sym_givens(sc->m_rhodold, thetabar, ctildeold, stildeold, rhotildeold);
+        const double thetatilde = stildeold * rhobar, rhodold = ctildeold * rhobar;
+        const double betad = -stildeold * sc->m_betad + ctildeold * betahat;
+        const double tautildeold = (zetaold - thetatildeold * sc->m_tautildeold) / rhotildeold;
+        const double taud = (zeta - thetatilde * tautildeold) / rhodold;
+        const double dsum = sc->m_d + betacheck * betacheck;
+        const double rNorm = sqrt(dsum + (betad - taud) * (betad - taud) + betadd * betadd);
+        // ||A||, cond(A)
+        double Anorm2 = sc->Anorm2 + beta * beta;
+        const double Anorm = sqrt(Anorm2);
+        Anorm2 += alpha * alpha;
+        const double maxrbar = fmax(sc->m_maxrbar, rhobarold);
+        const double minrbar = iter > 1 ? fmin(sc->m_minrbar, rhobarold) : sc->m_minrbar;
+        const double Acond = fmax(maxrbar, rhotemp) / fmin(minrbar, rhotemp);
+        // stopping tests
+        const double ArNorm = fabs(zetabar), xNorm = sqrt(tot);
+        const double test1 = rNorm / sc->beta1;
+        const double test2 = ArNorm / (Anorm * rNorm);
+        const double test3 = 1.0 / Acond;
+        const double t1 = test1 / (1.0 + Anorm * xNorm / sc->beta1);
+        const double rNormtol = sc->btol + axtol * Anorm * xNorm / sc->beta1;
+        const bool ill = (1.0 + test3 <= 1.0) || (test3 <= ctol);
+        const bool zr = (1.0 + t1 <= 1.0) || (test1 <= rNormtol);
+        const bool solved = (1.0 + test2 <= 1.0) || (test2 <= axtol) || (ArNorm <= sc->atol) || zr;
+        const bool tired = iter >= sc->itmax;
+        sc->m_alphabar = c * alpha;
+        sc->m_rho = rho;
+        sc->m_rhobar = rhobar;
+        sc->m_cbar = cbar;
+        sc->m_sbar = sbar;
+        sc->m_zeta = zeta;
+        sc->m_zetabar = zetabar;
+        sc->m_betadd = betadd;
+        sc->m_betad = betad;
+        sc->m_rhodold = rhodold;
+        sc->m_tautildeold = tautildeold;
+        sc->m_thetatilde = thetatilde;
+        sc->m_d = dsum;
+        sc->m_maxrbar = maxrbar;
+        sc->m_minrbar = minrbar;
+        sc->Anorm2 = Anorm2;
+        sc->xNorm = xNorm;
         sc->iter = iter;
         if (solved || tired || ill) {
             sc->stopped = 1;
@@ -2113,7 +2237,8 @@ size_t sim_scratch_bound(const cpb_sim_params* P, int64_t ny, int64_t nx, int64_
     if (P->model_rad_auto) b += carve_size(4 * n);
     b += tiles_bound(n, R, ntiles);
     if (Rm != R || P->model_rad_auto) b += tiles_bound(n, Rm, ntiles);
-    b += 8 * carve_size(8 * np) + 2 * carve_size(sizeof(StarCoef) * n);           // solver state
+    b += (P->solver == CPB_SOLVER_LSMR ? 9 : 8) * carve_size(8 * np) +           // solver state (lsmr: hbar)
+         2 * carve_size(sizeof(StarCoef) * n);
     b += 3 * carve_size(n) + 4 * carve_size(4 * n) + carve_size(4);
     b += 2 * carve_size(sel_tmp);                                                  // live_tmp, newf_tmp
     // with :auto the model lists are counted at the fit box here (checked again in the fit)
@@ -2228,7 +2353,7 @@ class SimFit {
     double mean_box = 0, dof = 1;
     TileLists tfit, tmod;
     double *cn = nullptr, *D = nullptr, *bsc = nullptr, *delta = nullptr, *dsc = nullptr;
-    double *xl = nullptr, *vt = nullptr, *wl = nullptr;
+    double *xl = nullptr, *vt = nullptr, *wl = nullptr, *hbar = nullptr;
     StarCoef *coef = nullptr, *coefc = nullptr;
     uint8_t *live = nullptr, *newf = nullptr, *conv = nullptr;
     int32_t *frozen_at = nullptr, *live_list = nullptr, *iota_act = nullptr, *evlist = nullptr;
@@ -2430,7 +2555,6 @@ bool SimFit::setup() {
     if (!(model_rad_max >= P->fit_rad)) throw ArgError{"model_rad_max must be >= fit_rad"};
     if (!(P->model_rad_nsigma > 0)) throw ArgError{"model_rad_nsigma must be positive"};
     if (P->solver != CPB_SOLVER_LSQR && P->solver != CPB_SOLVER_LSMR) throw ArgError{"solver must be :lsqr or :lsmr"};
-    if (P->solver == CPB_SOLVER_LSMR) throw ArgError{"solver :lsmr is not supported by the B200 path; use :lsqr"};
     if (P->damping == CPB_DAMP_LEVENBERG)
         throw ArgError{
             "LevenbergDamping is not supported by fit_all_stars_simultaneous: it conflicts with the "
@@ -2677,7 +2801,8 @@ bool SimFit::setup() {
     dsc = S_<double>("delta_scaled", n);
     xl = S_<double>("lsqr_x", n);
     vt = S_<double>("lsqr_v", n);
-    wl = S_<double>("lsqr_w", n);
+    wl = S_<double>("lsqr_w", n);  // lsqr's w, or lsmr's h
+    if (P->solver == CPB_SOLVER_LSMR) hbar = S_<double>("lsmr_hbar", n);
     coef = S_<StarCoef>("coef", n_act);
     coefc = S_<StarCoef>("coef_cand", n_act);
     live = S_<uint8_t>("live", n_act);
@@ -2751,6 +2876,7 @@ template <typename TS, typename TU>
 void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial) {
     constexpr double bts = sizeof(TS), btu = sizeof(TU);
     const FitConst& f = F.fc;
+    const bool lsmr = P->solver == CPB_SOLVER_LSMR;  // krylov_solve! with the :lsmr workspace
     bool fresh = false;  // V / wt_resid / cost are at the current theta and live set
     if (initial) {
         launch_coef(nullptr, coef);
@@ -2817,11 +2943,12 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
                 NvtxRange nv_lsqr("cpb:sim:lsqr");
                 {
                     KernelScope ks_(ctx, "k_lsqr_v0", (double)n * 8 * 3);
-                    k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red);
+                    k_lsqr_v0<<<nblk(n), 256, 0, st>>>(n, bsc, vt, xl, sc, red, lsmr);
                 }
                 {
-                    KernelScope ks_(ctx, "k_lsqr_w0", (double)n * 8 * 2);
-                    k_lsqr_w0<<<nblk(n), 256, 0, st>>>(n, vt, wl, sc, red);
+                    KernelScope ks_(ctx, lsmr ? "k_lsmr_init" : "k_lsqr_w0", (double)n * 8 * 2);
+                    if (lsmr) k_lsmr_init<<<nblk(n), 256, 0, st>>>(n, vt, wl, hbar, sc);
+                    else k_lsqr_w0<<<nblk(n), 256, 0, st>>>(n, vt, wl, sc, red);
                 }
                 for (int it = 0; it < P->inner_iterations; ++it) {
                     {
@@ -2841,8 +2968,9 @@ void SimFit::outer_loop(Form<TS, TU>& F, int it_first, int it_last, bool initial
                                                                       F.u, vt, sc, red);
                     }
                     {
-                        KernelScope ks_(ctx, "k_lsqr_update", (double)n * 8 * 5);
-                        k_lsqr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, sc, red);
+                        KernelScope ks_(ctx, lsmr ? "k_lsmr_update" : "k_lsqr_update", (double)n * 8 * (lsmr ? 7 : 5));
+                        if (lsmr) k_lsmr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, hbar, sc, red);
+                        else k_lsqr_update<<<nblk(n), 256, 0, st>>>(n, vt, xl, wl, sc, red);
                     }
                 }
                 check(cudaGetLastError(), "lsqr");

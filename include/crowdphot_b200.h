@@ -103,7 +103,7 @@ typedef struct cpb_psf_desc {
 
 /* inner Krylov solver of the simultaneous fit */
 #define CPB_SOLVER_LSQR 0
-#define CPB_SOLVER_LSMR 1 /* accepted by the reference; rejected here */
+#define CPB_SOLVER_LSMR 1 /* LSMR (Fong & Saunders); batched groups run through the full-field fit */
 
 /*
  * Keyword arguments of fit_all_stars_simultaneous

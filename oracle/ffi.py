@@ -55,6 +55,9 @@ def load():
         lib.orc_lsqr_dense.restype = C.c_int
         lib.orc_lsqr_dense.argtypes = [C.c_int64, C.c_int64, _dp, _dp, C.c_double, C.c_int, C.c_double, C.c_double,
                                        _dp]
+        lib.orc_lsmr_dense.restype = C.c_int
+        lib.orc_lsmr_dense.argtypes = [C.c_int64, C.c_int64, _dp, _dp, C.c_double, C.c_int, C.c_double, C.c_double,
+                                       _dp]
         lib.orc_ring_offsets.restype = C.c_int
         lib.orc_ring_offsets.argtypes = [C.c_int, _i32p, _i32p]
         lib.orc_morton2d.restype = C.c_uint64
@@ -208,6 +211,17 @@ def orc_lsqr_dense(A, b, lam, itmax, atol, btol):
     bb = _f64(b)
     x = np.zeros(n)
     it = lib.orc_lsqr_dense(m, n, Af.ctypes.data_as(_dp), bb.ctypes.data_as(_dp), lam, itmax, atol, btol,
+                            x.ctypes.data_as(_dp))
+    return x, it
+
+
+def orc_lsmr_dense(A, b, lam, itmax, atol, btol):
+    lib = load()
+    m, n = A.shape
+    Af = np.asfortranarray(A, dtype=np.float64)
+    bb = _f64(b)
+    x = np.zeros(n)
+    it = lib.orc_lsmr_dense(m, n, Af.ctypes.data_as(_dp), bb.ctypes.data_as(_dp), lam, itmax, atol, btol,
                             x.ctypes.data_as(_dp))
     return x, it
 

@@ -136,4 +136,124 @@ LsqrStats lsqr(int64_t m, int64_t n, const std::function<void(const double*, dou
     return st;
 }
 
+LsqrStats lsmr(int64_t m, int64_t n, const std::function<void(const double*, double*)>& Av,
+               const std::function<void(const double*, double*)>& Atu, const double* b, double lambda,
+               int itmax, double atol, double btol, double* x) {
+    const double eps = std::numeric_limits<double>::epsilon();
+    const double axtol = std::sqrt(eps), conlim = 1.0 / std::sqrt(eps);
+    const double ctol = conlim > 0 ? 1.0 / conlim : 0.0, rtol = 0.0;
+    LsqrStats st;
+    std::fill(x, x + n, 0.0);
+    std::vector<double> u(b, b + m), v(n), h(n), hbar(n, 0.0), tmpm(m), tmpn(n);
+    double beta1 = 0;
+    for (int64_t i = 0; i < m; ++i) beta1 += u[i] * u[i];
+    beta1 = std::sqrt(beta1);
+    if (beta1 == 0) {
+        st.status = 4;
+        return st;
+    }
+    double beta = beta1;
+    for (auto& e : u) e *= 1.0 / beta1;
+    Atu(u.data(), v.data());
+    double alpha = 0;
+    for (int64_t i = 0; i < n; ++i) alpha += v[i] * v[i];
+    alpha = std::sqrt(alpha);
+    if (alpha == 0) {
+        st.status = 4;
+        return st;
+    }
+    for (auto& e : v) e *= 1.0 / alpha;
+    // QR factorisation state (Fong & Saunders, section 2)
+    double zetabar = alpha * beta, alphabar = alpha, rho = 1, rhobar = 1, cbar = 1, sbar = 0, zeta = 0;
+    h = v;
+    // ||r|| estimate state (section 3.4)
+    double betadd = beta, betad = 0, rhodold = 1, tautildeold = 0, thetatilde = 0, d = 0;
+    // ||A||, cond(A) estimates (section 4)
+    double Anorm2 = alpha * alpha, maxrbar = 0, minrbar = 1e100;
+    const double ArNorm0 = alpha * beta;
+    bool solved = false, tired = (0 >= itmax), ill_cond = false;
+    int iter = 0;
+    while (!(solved || tired || ill_cond)) {
+        ++iter;
+        // Golub-Kahan step, as in lsqr
+        Av(v.data(), tmpm.data());
+        for (int64_t i = 0; i < m; ++i) u[i] = tmpm[i] - alpha * u[i];
+        beta = 0;
+        for (int64_t i = 0; i < m; ++i) beta += u[i] * u[i];
+        beta = std::sqrt(beta);
+        if (beta != 0) {
+            for (auto& e : u) e *= 1.0 / beta;
+            Atu(u.data(), tmpn.data());
+            for (int64_t i = 0; i < n; ++i) v[i] = tmpn[i] - beta * v[i];
+            alpha = 0;
+            for (int64_t i = 0; i < n; ++i) alpha += v[i] * v[i];
+            alpha = std::sqrt(alpha);
+            if (alpha != 0)
+                for (auto& e : v) e *= 1.0 / alpha;
+        }
+        // rotation eliminating the damping, then the one turning B into R
+        double chat, shat, alphahat;
+        sym_givens(alphabar, lambda, chat, shat, alphahat);
+        const double rhoold = rho;
+        double c, s;
+        sym_givens(alphahat, beta, c, s, rho);
+        const double thetanew = s * alpha;
+        alphabar = c * alpha;
+        // rotation turning R' into Rbar
+        const double rhobarold = rhobar, zetaold = zeta;
+        const double thetabar = sbar * rho, rhotemp = cbar * rho;
+        sym_givens(cbar * rho, thetanew, cbar, sbar, rhobar);
+        zeta = cbar * zetabar;
+        zetabar = -sbar * zetabar;
+        // h, hbar, x
+        const double kh = thetabar * rho / (rhoold * rhobarold);
+        const double kx = zeta / (rho * rhobar);
+        const double kv = thetanew / rho;
+        double xx = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            hbar[i] = h[i] - kh * hbar[i];
+            x[i] += kx * hbar[i];
+            h[i] = v[i] - kv * h[i];
+            xx += x[i] * x[i];
+        }
+        // ||r|| estimate
+        const double betaacute = chat * betadd, betacheck = -shat * betadd;
+        const double betahat = c * betaacute;
+        betadd = -s * betaacute;
+        const double thetatildeold = thetatilde;
+        double ctildeold, stildeold, rhotildeold;
+        sym_givens(rhodold, thetabar, ctildeold, stildeold, rhotildeold);
+        thetatilde = stildeold * rhobar;
+        rhodold = ctildeold * rhobar;
+        betad = -stildeold * betad + ctildeold * betahat;
+        tautildeold = (zetaold - thetatildeold * tautildeold) / rhotildeold;
+        const double taud = (zeta - thetatilde * tautildeold) / rhodold;
+        d += betacheck * betacheck;
+        const double rNorm = std::sqrt(d + (betad - taud) * (betad - taud) + betadd * betadd);
+        // ||A|| and cond(A)
+        Anorm2 += beta * beta;
+        const double Anorm = std::sqrt(Anorm2);
+        Anorm2 += alpha * alpha;
+        maxrbar = std::max(maxrbar, rhobarold);
+        if (iter > 1) minrbar = std::min(minrbar, rhobarold);
+        const double Acond = std::max(maxrbar, rhotemp) / std::min(minrbar, rhotemp);
+        // stopping tests
+        const double ArNorm = std::fabs(zetabar);
+        const double xNorm = std::sqrt(xx);
+        const double test1 = rNorm / beta1;
+        const double test2 = ArNorm / (Anorm * rNorm);
+        const double test3 = 1.0 / Acond;
+        const double t1 = test1 / (1.0 + Anorm * xNorm / beta1);
+        const double rNormtol = btol + axtol * Anorm * xNorm / beta1;
+        tired = iter >= itmax;
+        ill_cond = (1.0 + test3 <= 1.0) || (test3 <= ctol);
+        const bool zr = (1.0 + t1 <= 1.0) || (test1 <= rNormtol);
+        solved = (1.0 + test2 <= 1.0) || (test2 <= axtol) || (ArNorm <= atol + rtol * ArNorm0) || zr;
+        if (solved) st.status = zr ? 2 : 1;
+        else if (ill_cond) st.status = 3;
+    }
+    st.iters = iter;
+    return st;
+}
+
 }  // namespace orc

@@ -55,4 +55,15 @@ LsqrStats lsqr(int64_t m, int64_t n, const std::function<void(const double*, dou
                const std::function<void(const double*, double*)>& Atu, const double* b, double lambda,
                int itmax, double atol, double btol, double* x);
 
+// The same problem by LSMR (solver = :lsmr): Fong & Saunders 2011 (SIAM J. Sci.
+// Comput. 33:2950-2971), the damping rotation of their section 3 and the norm /
+// condition estimates of their section 4, with Krylov.jl's lsmr stopping rules
+// and default tolerances (axtol = btol_default = sqrt(eps), conlim = 1/sqrt(eps),
+// rtol = 0; atol and btol from the caller).  Iterates pinned against
+// scipy.sparse.linalg.lsmr in tests/test_oracle_operator.py; Krylov.jl's exact
+// early-exit iteration for a truncated solve is unpinned.
+LsqrStats lsmr(int64_t m, int64_t n, const std::function<void(const double*, double*)>& Av,
+               const std::function<void(const double*, double*)>& Atu, const double* b, double lambda,
+               int itmax, double atol, double btol, double* x);
+
 }  // namespace orc

@@ -9,8 +9,8 @@
 //     of raising Julia's InexactError from round(Int, NaN);
 //   * a negative Morton anchor raises CPB_ERR_ARGUMENT (Julia raises
 //     InexactError from UInt64(negative)) -- same outcome: the call fails;
-//   * solver = :lsmr is rejected with ArgumentError text (the GPU path
-//     implements LSQR); model_rad = :auto follows _model_radii with the unit
+//   * solver = :lsmr runs the LSMR restatement (oracle_lsqr.hpp) in place of
+//     LSQR, as krylov_solve! does; model_rad = :auto follows _model_radii with the unit
 //     PSF's curve of growth (analytic for the Gaussian, exact-overlap apertures
 //     otherwise), in FP64 whatever the image eltype;
 //   * spread_model / spread_model_err are not computed (NaN).
@@ -394,6 +394,27 @@ int orc_lsqr_dense(int64_t m, int64_t n, const double* A, const double* b, doubl
         }
     };
     LsqrStats s = lsqr(m, n, Av, Atu, b, lambda, itmax, atol, btol, x);
+    return s.iters;
+}
+
+// Dense LSMR (tests against scipy): A is m x n column-major.
+int orc_lsmr_dense(int64_t m, int64_t n, const double* A, const double* b, double lambda, int itmax, double atol,
+                   double btol, double* x) {
+    auto Av = [&](const double* v, double* y) {
+        for (int64_t i = 0; i < m; ++i) {
+            double s = 0;
+            for (int64_t j = 0; j < n; ++j) s += A[i + j * m] * v[j];
+            y[i] = s;
+        }
+    };
+    auto Atu = [&](const double* u, double* z) {
+        for (int64_t j = 0; j < n; ++j) {
+            double s = 0;
+            for (int64_t i = 0; i < m; ++i) s += A[i + j * m] * u[i];
+            z[j] = s;
+        }
+    };
+    LsqrStats s = lsmr(m, n, Av, Atu, b, lambda, itmax, atol, btol, x);
     return s.iters;
 }
 
@@ -948,8 +969,10 @@ int orc_fit_simultaneous(const cpb_psf_desc* desc, const cpb_sim_params* P, cons
         for (int trial = 1; trial <= P->max_trials; ++trial) {
             out->n_trials += 1;
             double lam_solve = std::sqrt(lam);
-            LsqrStats ls = lsqr(npix, n, Av, Atu, mrhs.data(), lam_solve, P->inner_iterations, P->linear_tol,
-                                P->linear_tol, d_scaled.data());
+            // krylov_solve!(ws, J_op, mrhs; λ, itmax, atol, btol) with the workspace of `solver` (:1222-1224)
+            LsqrStats ls = (P->solver == CPB_SOLVER_LSMR ? lsmr : lsqr)(
+                npix, n, Av, Atu, mrhs.data(), lam_solve, P->inner_iterations, P->linear_tol, P->linear_tol,
+                d_scaled.data());
             out->n_lsqr_iters += ls.iters;
             out->lsqr_px_macs += 2.0 * ls.iters * nl * S2 + (double)nl * S2;
             for (int64_t i = 0; i < n; ++i) delta[i] = d_scaled[i] / st.colnorm[i];

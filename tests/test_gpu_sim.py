@@ -388,3 +388,53 @@ def test_four_node_gridded_parity_and_large_radii():
     assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
     assert np.array_equal(g.debug["model_R"], o.debug["model_R"])
     assert_parity(g, o, tag="large_radii")
+
+
+@pytest.mark.parametrize("case", ["c1", "crowded_epsf"])
+def test_lsmr_solver_parity(case):
+    """solver = :lsmr (krylov_solve! with the LSMR workspace, :1222-1224): the same
+    Golub-Kahan kernels as LSQR with LSMR's rotations and h / hbar / x updates,
+    against the oracle's LSMR restatement -- integer structures bit-exact, the same
+    parity gates as LSQR, and a result that differs from the LSQR fit (the solver
+    really changed)."""
+    if case == "c1":
+        img, bkg, iv, psf, src, init = c1_field()
+        kw = dict(fixed={"fwhm": 2.5, "bkg": 0.0}, inv_var=iv, background=bkg, model_rad=7, max_iter=20,
+                  linear_tol=1e-8, debug=True)
+        R = 7
+    else:
+        psf = moffat_epsf()
+        img, bkg, iv, truth, init = crowded_field(256, 256, 780, seed=1002, psf=psf, dtype=np.float32)
+        kw = dict(fixed={"bkg": 0.0}, inv_var=iv, background=bkg, model_rad=12, debug=True)
+        R = 12
+    g = cpb.fit_all_stars_simultaneous(img, psf, init, R, solver="lsmr", **kw)
+    o = orc_fit_simultaneous(img, psf, init, R, solver="lsmr", **kw)
+    assert np.array_equal(g.debug["active"], o.debug["active"])
+    assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
+    assert_parity(g, o, tag=f"lsmr_{case}")
+    q = cpb.fit_all_stars_simultaneous(img, psf, init, R, **kw)
+    assert np.max(np.abs(q.flux / g.flux - 1)[g.valid & q.valid]) > 0
+
+
+def test_lsmr_groups_route_to_the_full_field_fit():
+    """The batched group kernel's in-block solver is LSQR, so solver = :lsmr fits
+    every group through the full-field path: each group equals its own single fit."""
+    from crowdphot_b200.simulate import lm_groups
+    psf = moffat_epsf()
+    d = lm_groups(6, seed=77, psf=psf, kmax=5)
+    offs, so = d["offsets"], d["star_offsets"]
+    images, cats, ivs = [], [], []
+    for gi in range(6):
+        ny, nx = int(d["ny"][gi]), int(d["nx"][gi])
+        a, b = int(so[gi]), int(so[gi + 1])
+        images.append(d["pix"][offs[gi]:offs[gi] + ny * nx].reshape((ny, nx), order="F"))
+        ivs.append(d["inv_var"][offs[gi]:offs[gi] + ny * nx].reshape((ny, nx), order="F"))
+        cats.append(dict(y=d["y"][a:b], x=d["x"][a:b], flux=d["flux"][a:b]))
+    kw = dict(fixed={"bkg": 0.0}, model_rad=12, solver="lsmr")
+    res = cpb.fit_all_stars_simultaneous_batch(images, psf, cats, 5, inv_vars=ivs, **kw)
+    for gi in range(6):
+        s = cpb.fit_all_stars_simultaneous(images[gi], psf, cats[gi], 5, inv_var=ivs[gi], **kw)
+        assert np.array_equal(s.valid, res[gi].valid)
+        ok = s.valid
+        np.testing.assert_allclose(res[gi].flux[ok], s.flux[ok], rtol=1e-12)
+        np.testing.assert_allclose(res[gi].y[ok], s.y[ok], rtol=0, atol=1e-12)

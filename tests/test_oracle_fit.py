@@ -30,14 +30,15 @@ def isolated_field(psf, seed=42, shape=(128, 128), n=5):
     return img, src
 
 
+@pytest.mark.parametrize("solver", ["lsqr", "lsmr"])
 @pytest.mark.parametrize("kind", ["gaussian", "gridded"])
-def test_isolated_noiseless_recovers_truth(kind):
+def test_isolated_noiseless_recovers_truth(kind, solver):
     psf = CircularGaussianPSF(fwhm=2.0) if kind == "gaussian" else gaussian_node_psf()
     fixed = {"fwhm": 2.0, "bkg": 0.0} if kind == "gaussian" else {"bkg": 0.0}
     img, src = isolated_field(psf)
     cat = dict(y=src["y"], x=src["x"], flux=np.full(5, 400.0))
     r = orc_fit_simultaneous(img, psf, cat, 5, fixed=fixed, max_iter=40, inner_iterations=10, x_tol=1e-8,
-                             model_rad=5)
+                             model_rad=5, solver=solver)
     assert r.valid.all()
     np.testing.assert_allclose(r.flux, src["flux"], rtol=1e-10)
     np.testing.assert_allclose(r.y, src["y"], atol=1e-10)

@@ -9,8 +9,8 @@ import pytest
 import scipy.sparse.linalg as spla
 
 from crowdphot_b200 import CircularGaussianPSF
-from oracle import (orc_apply_J, orc_apply_JT, orc_fill_stamps, orc_lsqr_dense, orc_lsqr_stamp, orc_morton2d,
-                    orc_ring_offsets)
+from oracle import (orc_apply_J, orc_apply_JT, orc_fill_stamps, orc_lsmr_dense, orc_lsqr_dense, orc_lsqr_stamp,
+                    orc_morton2d, orc_ring_offsets)
 
 
 def dense_J(values, pixels, npix):
@@ -103,6 +103,35 @@ def test_lsqr_iterates_match_scipy(damp, itmax):
     ref = spla.lsqr(A, b, damp=damp, atol=0, btol=0, conlim=0, iter_lim=itmax)
     assert it == itmax == ref[2]
     np.testing.assert_allclose(x, ref[0], rtol=1e-10, atol=1e-12)
+
+
+@pytest.mark.parametrize("damp", [0.0, 0.03, 1.0])
+@pytest.mark.parametrize("itmax", [1, 3, 10])
+def test_lsmr_iterates_match_scipy(damp, itmax):
+    # solver = :lsmr: truncated iterates agree with scipy.sparse.linalg.lsmr (Fong &
+    # Saunders 2011), damped and undamped
+    rng = np.random.default_rng(12)
+    A = rng.standard_normal((60, 12))
+    b = rng.standard_normal(60)
+    x, it = orc_lsmr_dense(A, b, damp, itmax, 0.0, 0.0)
+    ref = spla.lsmr(A, b, damp=damp, atol=0, btol=0, conlim=0, maxiter=itmax)
+    assert it == itmax == ref[2]
+    np.testing.assert_allclose(x, ref[0], rtol=1e-10, atol=1e-12)
+
+
+def test_lsmr_converged_solution_matches_normal_equations():
+    # run to convergence with Krylov's default tolerances: the damped least-squares
+    # solution (A'A + damp^2 I) x = A'b, as for lsqr
+    rng = np.random.default_rng(13)
+    A = rng.standard_normal((80, 10))
+    b = rng.standard_normal(80)
+    for damp in (0.0, 0.5):
+        x, it = orc_lsmr_dense(A, b, damp, 200, 1e-12, 1e-12)
+        want = np.linalg.solve(A.T @ A + damp ** 2 * np.eye(10), A.T @ b)
+        assert 0 < it < 200
+        np.testing.assert_allclose(x, want, rtol=1e-6, atol=1e-9)
+    x, it = orc_lsmr_dense(A, np.zeros(80), 0.1, 10, 1e-6, 1e-6)
+    assert it == 0 and np.all(x == 0)
 
 
 def test_lsqr_zero_rhs_returns_zero():
