@@ -1349,12 +1349,9 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
             "column-equilibrated x_tol scaling. Use MarquardtDamping."};
     if (!(P->fit_rad > 0)) throw ArgError{"fit_rad must be positive"};
     if (eltype != CPB_F32 && eltype != CPB_F64) throw ArgError{"unsupported image eltype"};
-    if (P->precision != CPB_PREC_FP64)
-        throw ArgError{"the batched group fitter computes in FP64 only (precision must be CPB_PREC_FP64)"};
     if (P->model_rad_auto && !d_iv)
         throw ArgError{
             "model_rad=:auto requires inv_var (it needs a noise scale); pass inv_var or an explicit scalar model_rad"};
-    if (P->model_rad_auto) throw ArgError{"model_rad=:auto is not supported by the B200 path; pass a scalar model_rad"};
     if (G < 0) throw ArgError{"n_groups must be >= 0"};
     if (!out->y || !out->x || !out->flux || !out->y_err || !out->x_err || !out->flux_err || !out->converged ||
         !out->valid || !out->n_iter || !out->n_passes || !out->n_failed || !out->status)
@@ -1473,15 +1470,16 @@ void setup_groups(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_params* P, int
                        : layout_bytes<uint32_t>(std::max(ng, 1), C.S2, std::max(um, 1), kn);
     };
     // a group runs in the kernel when it has <= 64 stars and its own layout fits;
-    // the kernel's in-block solver is LSQR, so solver = :lsmr routes every group
-    // to the full-field fit
-    const bool lsmr = P->solver == CPB_SOLVER_LSMR;
+    // the kernel computes in FP64 with LSQR and one scalar model radius, so
+    // solver = :lsmr, model_rad = :auto or the mixed form route every group to
+    // the full-field fit
+    const bool route_all = P->solver == CPB_SOLVER_LSMR || P->model_rad_auto || P->precision != CPB_PREC_FP64;
     std::vector<Bucket> bk(kNumBuckets);
     for (int64_t g = 0; g < G; ++g) {
         const int ng = (int)(h_soff[g + 1] - h_soff[g]);
         const int um = (int)std::min<int64_t>((int64_t)ng * C.S2, (int64_t)h_ny[g] * h_nx[g]);
         const int kn = next_pow2(std::max(ng * C.S2, 2));
-        if (lsmr || ng > kMaxGroupStars || need_of(ng, um, kn) > cap) {
+        if (route_all || ng > kMaxGroupStars || need_of(ng, um, kn) > cap) {
             plan.routed_groups.push_back((int32_t)g);
             continue;
         }
@@ -1772,9 +1770,10 @@ GroupBatch* group_batch_create(cpb_ctx* ctx, const cpb_psf* psf, const cpb_sim_p
             setup_groups(ctx, psf, P, G, d_off, d_ny, d_nx, d_pix, eltype, d_iv, d_bkg, d_soff, d_y0, d_x0, d_f0,
                          total_pixels, out, nullptr, nullptr, nullptr, nullptr, b->su);
         const GroupPlan& plan = b->su.plan;
-        if (!plan.routed_groups.empty() && P->solver == CPB_SOLVER_LSMR)
-            throw ArgError{"solver :lsmr groups are fitted one by one by the full-field fit; use "
-                           "cpb_fit_simultaneous_batch instead of a captured batch"};
+        if (!plan.routed_groups.empty() &&
+            (P->solver == CPB_SOLVER_LSMR || P->model_rad_auto || P->precision != CPB_PREC_FP64))
+            throw ArgError{"groups with solver :lsmr, model_rad = :auto or mixed precision are fitted one by one "
+                           "by the full-field fit; use cpb_fit_simultaneous_batch instead of a captured batch"};
         if (!plan.routed_groups.empty())
             throw ArgError{"group " + std::to_string(plan.routed_groups[0]) +
                            " is too large for one thread block (more than 64 stars, or a working set beyond shared "

@@ -205,8 +205,13 @@ def test_group_argument_errors_are_per_group():
     assert abs(out["flux"][0] / o.flux[0] - 1) < FLUX_TOL
     with pytest.raises(ArgumentError, match="non-finite"):
         cpb.fit_all_stars_simultaneous_batch([good, bad], psf, [dict(y=[15.0], x=[15.0], flux=[700.0])] * 2, 5, **kw)
-    with pytest.raises(ArgumentError, match="only the batched|FP64 only"):
-        run_batch(psf, d, 5, precision="mixed", **kw)
+    # the mixed form routes every group to the full-field fit: the same per-group
+    # statuses, and group 0 equals its own single mixed fit
+    outm = run_batch(psf, d, 5, precision="mixed", **kw)
+    assert list(outm["status"]) == [0, -1, -1]
+    sm = cpb.fit_all_stars_simultaneous(good, psf, dict(y=[15.0], x=[15.0], flux=[700.0]), 5, precision="mixed",
+                                        **kw)
+    np.testing.assert_allclose(outm["flux"][0], sm.flux[0], rtol=1e-12)
 
 
 def test_groups_deterministic_and_equal_to_single_fits():

@@ -416,9 +416,13 @@ def test_lsmr_solver_parity(case):
     assert np.max(np.abs(q.flux / g.flux - 1)[g.valid & q.valid]) > 0
 
 
-def test_lsmr_groups_route_to_the_full_field_fit():
-    """The batched group kernel's in-block solver is LSQR, so solver = :lsmr fits
-    every group through the full-field path: each group equals its own single fit."""
+@pytest.mark.parametrize("variant", [{"solver": "lsmr"}, {"model_rad": "auto"}, {"precision": "mixed"}],
+                         ids=["lsmr", "auto_radii", "mixed"])
+def test_routed_group_variants_equal_single_fits(variant):
+    """The block-per-group kernel computes in FP64 with LSQR and one scalar model
+    radius; solver = :lsmr, model_rad = :auto and the mixed form fit every group of
+    a batch through the full-field path instead: each group equals its own single
+    fit."""
     from crowdphot_b200.simulate import lm_groups
     psf = moffat_epsf()
     d = lm_groups(6, seed=77, psf=psf, kmax=5)
@@ -430,7 +434,7 @@ def test_lsmr_groups_route_to_the_full_field_fit():
         images.append(d["pix"][offs[gi]:offs[gi] + ny * nx].reshape((ny, nx), order="F"))
         ivs.append(d["inv_var"][offs[gi]:offs[gi] + ny * nx].reshape((ny, nx), order="F"))
         cats.append(dict(y=d["y"][a:b], x=d["x"][a:b], flux=d["flux"][a:b]))
-    kw = dict(fixed={"bkg": 0.0}, model_rad=12, solver="lsmr")
+    kw = dict({"fixed": {"bkg": 0.0}, "model_rad": 12}, **variant)
     res = cpb.fit_all_stars_simultaneous_batch(images, psf, cats, 5, inv_vars=ivs, **kw)
     for gi in range(6):
         s = cpb.fit_all_stars_simultaneous(images[gi], psf, cats[gi], 5, inv_var=ivs[gi], **kw)
