@@ -387,10 +387,10 @@ class SimOutputs:
         n = self.n
         r = self.c
         valid = self.valid[:n].astype(bool)
-        msgs = [f"star {i + 1}: excluded before the solve (no usable pixels or non-finite initial parameters)"
-                for i in range(n) if not valid[i] and r.n_active < n]
-        if r.n_active == n:
-            msgs = []
+        msgs = []
+        if r.n_active < n:
+            msgs = [f"star {i + 1}: excluded before the solve (no usable pixels or non-finite initial parameters)"
+                    for i in np.flatnonzero(~valid).tolist()]
         res = MultiPassPhotResult(
             y=self.y[:n].copy(), x=self.x[:n].copy(), y_err=self.y_err[:n].copy(), x_err=self.x_err[:n].copy(),
             flux=self.flux[:n].copy(), flux_err=self.flux_err[:n].copy(), bkg=self.bkg[:n].copy(),
