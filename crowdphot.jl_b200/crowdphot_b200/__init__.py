@@ -16,12 +16,12 @@ from .photometry import (BatchGraph, Context, CudaError, Request, Server, LMResu
                          fit_all_stars, fit_all_stars_simultaneous_batch, fit_groups_packed, fit_star, fit_star_batch,
                          fit_star_packed, get_context, lm_params, psf_descriptor, sim_params)
 from ._abi import LIB_PATH, load_library
-from .robust import FixedScale, HuberLoss, L2DistLoss, MADScale, MScale, TukeyLoss
+from .robust import FixedScale, HuberLoss, L2DistLoss, LogitDistLoss, MADScale, MScale, TukeyLoss
 
 __all__ = [
     "AbstractPSFModel", "ArgumentError", "CircularGaussianPSF", "CircularMoffatPSF", "GriddedPSFModel", "ImagePSF",
     "replace_params", "BatchGraph", "Context", "Request", "Server", "CudaError", "LMResult", "MultiPassPhotResult", "fit_all_stars_simultaneous",
     "fit_all_stars", "fit_all_stars_simultaneous_batch", "fit_groups_packed",
     "fit_star", "fit_star_batch", "fit_star_packed", "get_context", "lm_params", "psf_descriptor", "sim_params", "LIB_PATH",
-    "load_library", "L2DistLoss", "HuberLoss", "TukeyLoss", "MADScale", "FixedScale", "MScale",
+    "load_library", "L2DistLoss", "HuberLoss", "TukeyLoss", "LogitDistLoss", "MADScale", "FixedScale", "MScale",
 ]

@@ -49,6 +49,7 @@ CPB_LOSS_NONE = 0
 CPB_LOSS_L2DIST = 1
 CPB_LOSS_HUBER = 2
 CPB_LOSS_TUKEY = 3
+CPB_LOSS_LOGITDIST = 4
 CPB_SCALE_AUTO = 0
 CPB_SCALE_MAD = 1
 CPB_SCALE_FIXED = 2

@@ -12,7 +12,7 @@ Differences from the Julia API, all deliberate:
   * the device computes in FP64 and results are returned as float64 arrays
     (Float32 cannot hold 1e-4 px at 2048 px);
   * ``background`` (image-shaped, optional) is subtracted on the device;
-  * IRLS losses other than L2DistLoss / HuberLoss / TukeyLoss and PSF types
+  * IRLS losses other than L2DistLoss / HuberLoss / TukeyLoss / LogitDistLoss and PSF types
     other than CircularGaussianPSF / ImagePSF / GriddedPSFModel{ImagePSF} raise
     ArgumentError -- there is no CPU fallback;
   * ``solver=:lsmr`` groups of the batched fitter run one by one through the

@@ -32,6 +32,12 @@ class TukeyLoss:
 
 
 @dataclass(frozen=True)
+class LogitDistLoss:
+    """LossFunctions.jl's logistic distance loss, -log(4 e^r / (1 + e^r)^2): weight
+    tanh(r/2) / (r/2) (psi(r) = tanh(r/2), psi'(0) = 1/2)."""
+
+
+@dataclass(frozen=True)
 class MADScale:
     """1.4826 * median(|r - median(r)|)."""
 
@@ -66,9 +72,11 @@ def set_irls(P, reweight, scale_estimator, weight_reset_tol):
         P.reweight, P.loss_param = _abi.CPB_LOSS_HUBER, float(reweight.d)
     elif isinstance(reweight, TukeyLoss):
         P.reweight, P.loss_param = _abi.CPB_LOSS_TUKEY, float(reweight.c)
+    elif isinstance(reweight, LogitDistLoss):
+        P.reweight = _abi.CPB_LOSS_LOGITDIST
     else:
         raise ArgumentError(f"reweight loss {type(reweight).__name__} is not supported by the B200 path "
-                            "(L2DistLoss, HuberLoss and TukeyLoss are)")
+                            "(L2DistLoss, HuberLoss, TukeyLoss and LogitDistLoss are)")
     if scale_estimator is None:
         P.scale_estimator = _abi.CPB_SCALE_AUTO
     elif isinstance(scale_estimator, MADScale):
@@ -84,4 +92,4 @@ def set_irls(P, reweight, scale_estimator, weight_reset_tol):
     return P
 
 
-__all__ = ["L2DistLoss", "HuberLoss", "TukeyLoss", "MADScale", "FixedScale", "MScale", "set_irls"]
+__all__ = ["L2DistLoss", "HuberLoss", "TukeyLoss", "LogitDistLoss", "MADScale", "FixedScale", "MScale", "set_irls"]

@@ -496,6 +496,7 @@ __device__ __forceinline__ double irls_weight(const LMConst& L, double r) {
         const double psi0 = 0.0 <= c ? 1.0 : 0.0;
         return psi / (r * psi0);
     }
+    if (L.irls == CPB_LOSS_LOGITDIST) return tanh(r / 2) / (r * 0.5);  // psi = tanh(r/2), psi'(0) = 1/2
     // TukeyLoss
     double psi = 0.0;
     if (fabs(r) <= c) {
@@ -1543,7 +1544,7 @@ LMConst lm_const(const cpb_psf* psf, const cpb_lm_params* P, bool have_iv) {
     L.max_iter = P->max_iter;
     if (!(P->weight_reset_tol >= 0) && P->reweight != CPB_LOSS_NONE)
         throw ArgError{"`weight_reset_tol` must be non-negative"};
-    if (P->reweight < CPB_LOSS_NONE || P->reweight > CPB_LOSS_TUKEY) throw ArgError{"unknown IRLS loss"};
+    if (P->reweight < CPB_LOSS_NONE || P->reweight > CPB_LOSS_LOGITDIST) throw ArgError{"unknown IRLS loss"};
     if (P->scale_estimator < CPB_SCALE_AUTO || P->scale_estimator > CPB_SCALE_MSCALE)
         throw ArgError{"unknown IRLS scale estimator"};
     L.irls = P->reweight;

@@ -213,6 +213,7 @@ typedef struct cpb_lm_params {
 #define CPB_LOSS_L2DIST 1
 #define CPB_LOSS_HUBER 2
 #define CPB_LOSS_TUKEY 3
+#define CPB_LOSS_LOGITDIST 4 /* LossFunctions.jl LogitDistLoss: psi(r) = tanh(r/2), psi'(0) = 1/2 */
 #define CPB_SCALE_AUTO 0
 #define CPB_SCALE_MAD 1
 #define CPB_SCALE_FIXED 2

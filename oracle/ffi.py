@@ -441,7 +441,7 @@ def orc_estimate_scale(estimator, r):
 
 
 def orc_irls_weight(loss, r):
-    """weight(loss, r) for L2DistLoss / HuberLoss / TukeyLoss."""
+    """weight(loss, r) for L2DistLoss / HuberLoss / TukeyLoss / LogitDistLoss."""
     from crowdphot_b200 import CircularGaussianPSF
     P = lm_params(CircularGaussianPSF(fwhm=1.0), {}, reweight=loss)
     return float(load().orc_irls_weight(P.reweight, P.loss_param, float(r)))

@@ -196,7 +196,9 @@ double estimate_scale(int kind, const cpb_lm_params* P, double fixed_sigma, cons
 }
 
 // weight(loss, r) = psi(r) / (r psi'(0)) (:337-345) for L2DistLoss (psi = 2r),
-// HuberLoss(d) (psi = r inside d, d sign(r) beyond) and TukeyLoss(c) (:289-313).
+// HuberLoss(d) (psi = r inside d, d sign(r) beyond), TukeyLoss(c) (:289-313) and
+// LossFunctions.jl's LogitDistLoss (loss -log(4 e^r / (1 + e^r)^2): psi = tanh(r/2),
+// psi'(0) = 1/2; a third-party loss the reference's generic weight accepts).
 double irls_weight(int loss, double c, double r) {
     if (std::fabs(r) < kEps * 10) return 1.0;
     if (loss == CPB_LOSS_L2DIST) return (2 * r) / (r * 2.0);
@@ -205,6 +207,7 @@ double irls_weight(int loss, double c, double r) {
         const double psi0 = 0.0 <= c ? 1.0 : 0.0;
         return psi / (r * psi0);
     }
+    if (loss == CPB_LOSS_LOGITDIST) return std::tanh(r / 2) / (r * 0.5);
     double psi = 0.0;
     if (std::fabs(r) <= c) {
         const double rc2 = (r / c) * (r / c);

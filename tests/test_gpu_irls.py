@@ -1,6 +1,6 @@
 """fit_star with IRLS reweighting on the device (k_lm_irls) against the oracle's
 lm_irls, cutout by cutout, on the same seeded inputs: every loss (L2DistLoss,
-HuberLoss, TukeyLoss) and scale estimator (the default, MADScale, FixedScale,
+HuberLoss, TukeyLoss, LogitDistLoss) and scale estimator (the default, MADScale, FixedScale,
 MScale), with and without inv_var, for the ePSF, a four-node gridded PSF and
 the Gaussian (free FWHM).  The weights are recomputed from residuals divided by
 a median-based scale, so the device's rounding (fused multiply-adds, warp
@@ -10,8 +10,8 @@ import numpy as np
 import pytest
 
 import crowdphot_b200 as cpb
-from crowdphot_b200 import (ArgumentError, CircularGaussianPSF, FixedScale, HuberLoss, L2DistLoss, MADScale, MScale,
-                            TukeyLoss)
+from crowdphot_b200 import (ArgumentError, CircularGaussianPSF, FixedScale, HuberLoss, L2DistLoss, LogitDistLoss,
+                            MADScale, MScale, TukeyLoss)
 from crowdphot_b200.simulate import lm_cutouts, moffat_epsf
 from oracle import orc_fit_star
 from oracle.ffi import orc_fit_star_packed
@@ -35,7 +35,7 @@ def compare(g, o, np_pos=2):
 
 
 CASES = [(HuberLoss(1.0), None), (TukeyLoss(), None), (L2DistLoss(), MADScale()), (HuberLoss(1.5), MScale()),
-         (TukeyLoss(4.0), FixedScale(1.3))]
+         (TukeyLoss(4.0), FixedScale(1.3)), (LogitDistLoss(), MADScale())]
 
 
 @pytest.mark.parametrize("loss,scale", CASES)

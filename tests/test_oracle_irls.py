@@ -9,8 +9,8 @@ restated with numpy random draws in place of StableRNG.
 import numpy as np
 import pytest
 
-from crowdphot_b200 import (ArgumentError, CircularGaussianPSF, FixedScale, HuberLoss, L2DistLoss, MADScale,
-                            MScale, TukeyLoss)
+from crowdphot_b200 import (ArgumentError, CircularGaussianPSF, FixedScale, HuberLoss, L2DistLoss, LogitDistLoss,
+                            MADScale, MScale, TukeyLoss)
 from oracle import orc_estimate_scale, orc_fit_star, orc_irls_weight, orc_lm_irls_line
 
 
@@ -36,6 +36,15 @@ def test_weight_functions():
     # psi(3) for Tukey at c = 4.685 is 3 (1 - (3/c)^2)^2; the weight divides by r
     assert orc_irls_weight(TukeyLoss(), 3.0) == pytest.approx((1 - (3 / 4.685) ** 2) ** 2, rel=1e-12)
     assert orc_irls_weight(TukeyLoss(), 1e-20) == 1.0  # |r| < 10 eps
+    # LogitDistLoss: psi(r) = tanh(r/2) (the derivative of -log(4 e^r / (1 + e^r)^2)),
+    # psi'(0) = 1/2, checked here by finite differences of the loss itself
+    loss = lambda r: -np.log(4 * np.exp(r) / (1 + np.exp(r)) ** 2)
+    h = 1e-5
+    for r in (0.3, 1.0, 2.5, -4.0):
+        psi = (loss(r + h) - loss(r - h)) / (2 * h)
+        psi0 = (loss(h) - 2 * loss(0.0) + loss(-h)) / h ** 2
+        assert orc_irls_weight(LogitDistLoss(), r) == pytest.approx(psi / (r * psi0), rel=1e-5)
+    assert orc_irls_weight(LogitDistLoss(), 1e-20) == 1.0
 
 
 def test_weight_reset_threshold():
