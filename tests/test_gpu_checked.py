@@ -64,6 +64,17 @@ def test_edges_and_masks_checked(checked, precision):
     a = cpb.fit_all_stars_simultaneous(img, psf, cat, 4, ctx=checked, **kw)
     b = cpb.fit_all_stars_simultaneous(img, psf, cat, 4, **kw)
     same_results(a, b)
+    if precision == "fp64":
+        # element-wise against the CPU oracle as well: structures bit-exact, parity gates
+        from oracle import orc_fit_simultaneous
+        from test_gpu_sim import assert_parity
+        kwd = dict(kw, debug=True)
+        kwd.pop("precision")
+        g = cpb.fit_all_stars_simultaneous(img, psf, cat, 4, ctx=checked, **kwd)
+        o = orc_fit_simultaneous(img, psf, cat, 4, **kwd)
+        assert np.array_equal(g.debug["active"], o.debug["active"])
+        assert np.array_equal(g.debug["pixels"], o.debug["pixels"])
+        assert_parity(g, o, tag="checked_edges")
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
